@@ -1,0 +1,1109 @@
+// CPU restatement of the reference's search, walks, rate snapshot and decode.
+//
+// TEST INFRASTRUCTURE ONLY: the parity checker for the CUDA library and the timed CPU
+// baseline.  Nothing in the product (mars_b200/) links or calls this file.
+//
+// Every function below restates one reference function of daleobrien/mars (Rust), in the
+// same operation order, so that the f64 results are bit-identical.  Paths are relative to
+// the reference project root.  Build flags keep that order: -ffp-contract=off and no
+// fast-math (gcc would otherwise fuse a*b+c into an FMA, which Rust never does).
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <utility>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ------------------------------------------------------------------ fit and quantise
+
+// quantise_f64 (crates/mars-codec/src/encode.rs:446-448): trunc(0.5 + x) clamped to
+// [0, max], then `as u32` (NaN -> 0).
+inline uint32_t quantise_f64(double x, uint32_t max) {
+    double y = std::trunc(0.5 + x);
+    if (std::isnan(y)) return 0;
+    if (y < 0.0) y = 0.0;
+    if (y > (double)max) y = (double)max;
+    return (uint32_t)y;
+}
+
+// fit_f64 (encode.rs:247-289).
+void fit_f64(const orc_moments& m, double max_alfa, uint32_t bits_alfa, uint32_t bits_beta,
+             uint32_t* qalfa_out, uint32_t* qbeta_out, double* rms_out) {
+    const double s0 = (double)m.s0;
+    const double s1 = (double)m.s1_x4 / 4.0;
+    const double s2 = (double)m.s2_x16 / 16.0;
+    const double t0 = (double)m.t0;
+    const double t1 = (double)m.t1_x4 / 4.0;
+    const double t2 = (double)m.t2;
+
+    const double det = s0 * s2 - s1 * s1;
+    double alfa = (det == 0.0) ? 0.0 : (s0 * t1 - s1 * t0) / det;
+    if (alfa < 0.0) alfa = 0.0;
+
+    const uint32_t max_qalfa = (1u << bits_alfa) - 1;
+    const uint32_t qalfa = quantise_f64(alfa / max_alfa * (double)(1u << bits_alfa), max_qalfa);
+    const double alfa2 = (double)qalfa / (double)(1u << bits_alfa) * max_alfa;
+
+    double beta = (t0 - alfa2 * s1) / s0;
+    if (alfa2 > 0.0) beta += alfa2 * 255.0;
+    const uint32_t max_qbeta = (1u << bits_beta) - 1;
+    const uint32_t qbeta = quantise_f64(
+        beta / ((1.0 + std::fabs(alfa2)) * 255.0) * (double)max_qbeta, max_qbeta);
+    double beta2 = (double)qbeta / (double)max_qbeta * ((1.0 + std::fabs(alfa2)) * 255.0);
+    if (alfa2 > 0.0) beta2 -= alfa2 * 255.0;
+
+    const double sum = t2 - 2.0 * alfa2 * t1 - 2.0 * beta2 * t0 + alfa2 * alfa2 * s2 +
+                       2.0 * alfa2 * beta2 * s1 + s0 * beta2 * beta2;
+    double q = sum / s0;
+    // f64::max(0.0): the non-NaN operand wins.
+    if (!(q >= 0.0)) q = 0.0;
+    *qalfa_out = qalfa;
+    *qbeta_out = qbeta;
+    *rms_out = std::sqrt(q);
+}
+
+// best_beta (encode.rs:456-460).
+uint32_t best_beta(int64_t range_sum, int64_t pixel_count, uint32_t bits_beta) {
+    const double mean = (double)range_sum / (double)pixel_count;
+    const uint32_t max_qbeta = (1u << bits_beta) - 1;
+    return quantise_f64(mean / 255.0 * (double)max_qbeta, max_qbeta);
+}
+
+// isometry::map (crates/mars-codec/src/isometry.rs:7-19).
+inline void iso_map(uint32_t k, uint32_t u, uint32_t v, uint32_t size, uint32_t* i, uint32_t* j) {
+    switch (k) {
+        case 0: *i = u; *j = v; break;
+        case 1: *i = size - 1 - v; *j = u; break;
+        case 2: *i = v; *j = size - 1 - u; break;
+        case 3: *i = size - 1 - u; *j = size - 1 - v; break;
+        case 4: *i = u; *j = size - 1 - v; break;
+        case 5: *i = size - 1 - u; *j = v; break;
+        case 6: *i = v; *j = u; break;
+        default: *i = size - 1 - v; *j = size - 1 - u; break;
+    }
+}
+
+// ------------------------------------------------------------------ the plane types
+
+struct Image {
+    const uint8_t* px;
+    uint32_t w, h;
+};
+
+// Contracted::build (encode.rs:478-502): D(r, c) = sum of the 2x2 block at (2r, 2c).
+struct Contracted {
+    std::vector<int32_t> data;
+    size_t stride = 0;
+    static Contracted build(const Image& im) {
+        Contracted c;
+        const size_t w = im.w, h = im.h;
+        c.stride = w / 2;
+        const size_t rows = h / 2;
+        c.data.assign(c.stride * rows, 0);
+        for (size_t i = 0; i < rows; ++i) {
+            const size_t r0 = 2 * i;
+            for (size_t j = 0; j < c.stride; ++j) {
+                const size_t c0 = 2 * j;
+                c.data[i * c.stride + j] = (int32_t)im.px[r0 * w + c0] +
+                                           (int32_t)im.px[r0 * w + c0 + 1] +
+                                           (int32_t)im.px[(r0 + 1) * w + c0] +
+                                           (int32_t)im.px[(r0 + 1) * w + c0 + 1];
+            }
+        }
+        return c;
+    }
+};
+
+// domain_sums (encode.rs:800-802 -> mars-simd/src/moments.rs:20-36, the scalar form).
+inline void domain_sums(const Contracted& c, size_t dr, size_t dc, size_t size, int64_t* s1,
+                        int64_t* s2) {
+    int64_t a = 0, b = 0;
+    for (size_t u = 0; u < size; ++u) {
+        const int32_t* row = &c.data[(dr + u) * c.stride + dc];
+        for (size_t v = 0; v < size; ++v) {
+            const int64_t d = row[v];
+            a += d;
+            b += d * d;
+        }
+    }
+    *s1 = a;
+    *s2 = b;
+}
+
+// cross_term_permuted (encode.rs:849-864 -> moments.rs dot_u8_i32_window).
+inline int64_t cross_term_permuted(const Contracted& c, size_t dr, size_t dc, size_t size,
+                                   const uint8_t* range_k) {
+    int64_t acc = 0;
+    for (size_t u = 0; u < size; ++u) {
+        const int32_t* row = &c.data[(dr + u) * c.stride + dc];
+        const uint8_t* rr = range_k + u * size;
+        for (size_t v = 0; v < size; ++v) acc += (int64_t)rr[v] * (int64_t)row[v];
+    }
+    return acc;
+}
+
+// permute_range (encode.rs:833-842).
+void permute_range(const uint8_t* range, uint32_t k, uint32_t size, uint8_t* out) {
+    for (uint32_t u = 0; u < size; ++u)
+        for (uint32_t v = 0; v < size; ++v) {
+            uint32_t i, j;
+            iso_map(k, u, v, size, &i, &j);
+            out[u * size + v] = range[i * size + j];
+        }
+}
+
+// retain_top_k (encode.rs:676-685): strict `<`, so equal-rms candidates keep encounter
+// order.
+void retain_top_k(std::vector<orc_candidate>& top, const orc_candidate& cand, size_t k) {
+    size_t pos = top.size();
+    for (size_t i = 0; i < top.size(); ++i)
+        if (cand.rms < top[i].rms) {
+            pos = i;
+            break;
+        }
+    if (pos < k) {
+        top.insert(top.begin() + (long)pos, cand);
+        if (top.size() > k) top.resize(k);
+    }
+}
+
+// search_top_k (encode.rs:695-788): every domain position (dom_row outer, dom_col inner,
+// step `shift`) x the 8 isometries, integer moments, fit_f64, strict-< retention.
+uint64_t search_top_k(const Image& im, const Contracted& c, uint32_t row, uint32_t col,
+                      uint32_t size, uint32_t shift, const orc_params& p, size_t k,
+                      std::vector<orc_candidate>& top) {
+    top.clear();
+    const size_t su = size;
+    std::vector<uint8_t> range(su * su);
+    int64_t t0 = 0, t2 = 0;
+    for (size_t i = 0; i < su; ++i) {
+        const size_t src = (row + i) * (size_t)im.w + col;
+        for (size_t j = 0; j < su; ++j) {
+            const uint8_t r = im.px[src + j];
+            range[i * su + j] = r;
+            t0 += r;
+            t2 += (int64_t)r * r;
+        }
+    }
+    const int64_t s0 = (int64_t)size * size;
+    std::vector<uint8_t> by_iso(8 * su * su);
+    for (uint32_t kk = 0; kk < 8; ++kk) permute_range(range.data(), kk, size, &by_iso[kk * su * su]);
+
+    if (im.h < 2 * size || im.w < 2 * size) return 0;
+    const uint32_t max_dom_row = im.h - 2 * size, max_dom_col = im.w - 2 * size;
+    uint64_t evals = 0;
+    for (uint32_t dom_row = 0; dom_row <= max_dom_row; dom_row += shift) {
+        for (uint32_t dom_col = 0; dom_col <= max_dom_col; dom_col += shift) {
+            const size_t drh = dom_row / 2, dch = dom_col / 2;
+            int64_t s1_x4, s2_x16;
+            domain_sums(c, drh, dch, su, &s1_x4, &s2_x16);
+            for (uint32_t kk = 0; kk < 8; ++kk) {
+                const int64_t t1_x4 = cross_term_permuted(c, drh, dch, su, &by_iso[kk * su * su]);
+                orc_candidate cand;
+                cand.dom_row = dom_row;
+                cand.dom_col = dom_col;
+                cand.isometry = kk;
+                cand.valid = 1;
+                cand.m = orc_moments{s0, s1_x4, s2_x16, t0, t1_x4, t2};
+                fit_f64(cand.m, p.max_alfa, p.bits_alfa, p.bits_beta, &cand.qalfa, &cand.qbeta,
+                        &cand.rms);
+                evals += 1;
+                retain_top_k(top, cand, k);
+            }
+        }
+    }
+    return evals;
+}
+
+// ------------------------------------------------------------------ rate snapshot
+
+// AdaptiveModel (crates/mars-entropy/src/lib.rs:36-121).
+constexpr uint32_t PRECISION = 24;
+constexpr uint64_t PRECISION_TOTAL = 1ull << PRECISION;
+constexpr uint64_t RESCALE_THRESHOLD = 1ull << 16;
+
+struct AdaptiveModel {
+    std::vector<uint32_t> counts;
+    uint64_t total = 0;
+    explicit AdaptiveModel(uint32_t alphabet = 2) : counts(alphabet, 1u), total(alphabet) {}
+    void update(uint32_t symbol) {
+        counts[symbol] += 32;
+        total += 32;
+        if (total >= RESCALE_THRESHOLD) {
+            uint64_t t = 0;
+            for (auto& c : counts) {
+                c = std::max<uint32_t>(c >> 1, 1u);
+                t += c;
+            }
+            total = t;
+        }
+    }
+    uint32_t scaled(uint64_t c) const {
+        const uint64_t free_weight = PRECISION_TOTAL - counts.size();
+        return (uint32_t)(((unsigned __int128)c * free_weight) / total);
+    }
+    uint32_t prob(uint32_t symbol) const {
+        uint64_t before = 0;
+        for (uint32_t i = 0; i < symbol; ++i) before += counts[i];
+        const uint64_t after = before + counts[symbol];
+        const uint32_t left = scaled(before) + symbol;
+        const uint32_t right = scaled(after) + symbol + 1;
+        return right - left;
+    }
+    // bits_for (lib.rs:98-101).
+    double bits_for(uint32_t symbol) const {
+        return -std::log2((double)prob(symbol) / (double)PRECISION_TOTAL);
+    }
+};
+
+using ContextKey = std::pair<uint8_t, uint32_t>;
+struct Event {
+    ContextKey ctx;
+    uint32_t alphabet, symbol;
+};
+
+// Field ids (crates/mars-codec/src/mars_format.rs:113-128) and MODE_ALPHABET (:133).
+constexpr uint8_t FIELD_SPLIT = 0, FIELD_MODE = 1, FIELD_QALFA = 2, FIELD_QBETA = 3,
+                  FIELD_QBETA_DC = 4, FIELD_ISOMETRY = 5, FIELD_DOM_ROW = 6, FIELD_DOM_COL = 7,
+                  FIELD_GX = 8, FIELD_GY = 9;
+constexpr uint32_t MODE_ALPHABET = 4;
+// AFFINE_GRAD_SCALE / AFFINE_GRAD_CLAMP (encode.rs:353-360).
+constexpr double AFFINE_GRAD_SCALE = 64.0;
+constexpr int32_t AFFINE_GRAD_CLAMP = 2048;
+
+uint32_t ceil_log2(uint32_t q) { return q <= 1 ? 0 : 32 - (uint32_t)__builtin_clz(q - 1); }
+uint32_t virtual_size(const orc_header& h) {
+    return 1u << ceil_log2(std::max(h.width, h.height));
+}
+uint32_t bits_coord_row(const orc_header& h) { return ceil_log2(h.height / h.shift); }
+uint32_t bits_coord_col(const orc_header& h) { return ceil_log2(h.width / h.shift); }
+uint32_t zigzag(int64_t x) { return (uint32_t)((x << 1) ^ (x >> 63)); }
+uint32_t size_class_of(uint32_t size) { return (uint32_t)__builtin_ctz(size); }
+
+struct Predictor {
+    int64_t prev_row_units = 0, prev_col_units = 0;
+};
+
+// emit_leaf (mars_format.rs:515-595), modes 0/1/2.
+void emit_leaf(const orc_header& hdr, const orc_leaf& leaf, uint32_t sc, Predictor& pred,
+               std::vector<Event>& ev) {
+    ev.push_back({{FIELD_MODE, sc}, MODE_ALPHABET, leaf.mode});
+    if (leaf.mode == 0) {
+        ev.push_back({{FIELD_QBETA_DC, sc}, 1u << hdr.bits_beta, leaf.qbeta});
+    } else if (leaf.mode == 1) {
+        ev.push_back({{FIELD_QBETA_DC, sc}, 1u << hdr.bits_beta, leaf.qbeta});
+        const uint32_t alph = (uint32_t)(2 * (int64_t)AFFINE_GRAD_CLAMP + 1);
+        ev.push_back({{FIELD_GX, sc}, alph, zigzag(leaf.qgx)});
+        ev.push_back({{FIELD_GY, sc}, alph, zigzag(leaf.qgy)});
+    } else {
+        ev.push_back({{FIELD_QALFA, sc}, (1u << hdr.bits_alfa) - 1, leaf.qalfa - 1});
+        ev.push_back({{FIELD_QBETA, sc}, 1u << hdr.bits_beta, leaf.qbeta});
+        ev.push_back({{FIELD_ISOMETRY, sc}, 8, leaf.isometry});
+        const int64_t row_units = leaf.dom_row / hdr.shift;
+        const int64_t col_units = leaf.dom_col / hdr.shift;
+        const int64_t row_range = 1ll << bits_coord_row(hdr);
+        const int64_t col_range = 1ll << bits_coord_col(hdr);
+        ev.push_back({{FIELD_DOM_ROW, sc}, (uint32_t)(2 * row_range),
+                      zigzag(row_units - pred.prev_row_units)});
+        ev.push_back({{FIELD_DOM_COL, sc}, (uint32_t)(2 * col_range),
+                      zigzag(col_units - pred.prev_col_units)});
+        pred.prev_row_units = row_units;
+        pred.prev_col_units = col_units;
+    }
+}
+
+using LeafMap = std::map<std::tuple<uint32_t, uint32_t, uint32_t>, const orc_leaf*>;
+
+// walk_write (mars_format.rs:460-512): canonical NW, SW, NE, SE traversal.
+bool walk_write(const orc_header& hdr, uint32_t row, uint32_t col, uint32_t size,
+                const LeafMap& by_pos, Predictor& pred, std::vector<Event>& ev) {
+    if (row >= hdr.height || col >= hdr.width) return true;
+    const uint32_t half = size / 2;
+    const bool forced = size > hdr.max_size || row + size > hdr.height || col + size > hdr.width;
+    const uint32_t sc = size_class_of(size);
+    auto it = by_pos.find({row, col, size});
+    if (it != by_pos.end()) {
+        if (!forced && size > hdr.min_size) ev.push_back({{FIELD_SPLIT, sc}, 2, 0});
+        emit_leaf(hdr, *it->second, sc, pred, ev);
+        return true;
+    }
+    if (!forced) {
+        if (size <= hdr.min_size) return false;
+        ev.push_back({{FIELD_SPLIT, sc}, 2, 1});
+    }
+    return walk_write(hdr, row, col, half, by_pos, pred, ev) &&
+           walk_write(hdr, row + half, col, half, by_pos, pred, ev) &&
+           walk_write(hdr, row, col + half, half, by_pos, pred, ev) &&
+           walk_write(hdr, row + half, col + half, half, by_pos, pred, ev);
+}
+
+// RateModels (crates/mars-codec/src/rate.rs:55-80) over build_models
+// (mars-entropy/src/lib.rs:269-278).
+struct RateModels {
+    std::map<ContextKey, AdaptiveModel> models;
+    static bool from_leaves(const orc_header& hdr, const std::vector<orc_leaf>& leaves,
+                            RateModels& out) {
+        LeafMap by_pos;
+        for (const auto& l : leaves) by_pos[{l.row, l.col, l.size}] = &l;
+        std::vector<Event> ev;
+        Predictor pred;
+        if (!walk_write(hdr, 0, 0, virtual_size(hdr), by_pos, pred, ev)) return false;
+        for (const auto& e : ev) {
+            auto it = out.models.find(e.ctx);
+            if (it == out.models.end()) it = out.models.emplace(e.ctx, AdaptiveModel(e.alphabet)).first;
+            it->second.update(e.symbol);
+        }
+        return true;
+    }
+    double bits_for(ContextKey ctx, uint32_t alphabet, uint32_t symbol) const {
+        auto it = models.find(ctx);
+        if (it != models.end()) return it->second.bits_for(symbol);
+        return AdaptiveModel(std::max<uint32_t>(alphabet, 2)).bits_for(symbol);
+    }
+};
+
+// event_bits (encode.rs:1513-1518) over leaf_events (mars_format.rs:453-458).
+double leaf_bits(const RateModels& rate, const orc_header& hdr, const orc_leaf& leaf,
+                 uint32_t sc) {
+    std::vector<Event> ev;
+    Predictor pred;
+    emit_leaf(hdr, leaf, sc, pred, ev);
+    double s = -0.0;
+    for (const auto& e : ev) s += rate.bits_for(e.ctx, e.alphabet, e.symbol);
+    return s;
+}
+
+// ------------------------------------------------------------------ partition walks
+
+struct Ctx {
+    Image im;
+    const Contracted* contracted;
+    orc_header hdr;
+    orc_params params;
+    const RateModels* rate;
+    uint8_t allowed[4];
+    bool adaptive_density;
+};
+
+orc_leaf make_leaf(uint32_t row, uint32_t col, uint32_t size) {
+    orc_leaf l;
+    std::memset(&l, 0, sizeof l);
+    l.row = row;
+    l.col = col;
+    l.size = size;
+    return l;
+}
+
+uint32_t pixel_at(const Image& im, uint32_t row, uint32_t col) {
+    return im.px[(size_t)row * im.w + col];
+}
+
+int64_t range_sum(const Image& im, uint32_t row, uint32_t col, uint32_t size) {
+    int64_t s = 0;
+    for (uint32_t i = 0; i < size; ++i)
+        for (uint32_t j = 0; j < size; ++j) s += pixel_at(im, row + i, col + j);
+    return s;
+}
+
+struct WalkResult {
+    std::vector<orc_leaf> leaves;
+    uint64_t evals = 0;
+};
+
+constexpr uint32_t PARALLEL_SIZE_CUTOFF = 8;  // encode.rs:1321
+
+WalkResult walk(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size);
+
+// split (encode.rs:1442-1468): TL, BL, TR, BR, concatenated in that order.
+WalkResult split(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t half) {
+    WalkResult q[4];
+    const uint32_t rs[4] = {row, row + half, row, row + half};
+    const uint32_t cs[4] = {col, col, col + half, col + half};
+    if (half >= PARALLEL_SIZE_CUTOFF) {
+        for (int i = 0; i < 4; ++i) {
+#pragma omp task shared(q, ctx) firstprivate(i)
+            q[i] = walk(ctx, rs[i], cs[i], half);
+        }
+#pragma omp taskwait
+    } else {
+        for (int i = 0; i < 4; ++i) q[i] = walk(ctx, rs[i], cs[i], half);
+    }
+    WalkResult out;
+    for (auto& r : q) {
+        out.leaves.insert(out.leaves.end(), r.leaves.begin(), r.leaves.end());
+        out.evals += r.evals;
+    }
+    return out;
+}
+
+// walk (encode.rs:1330-1435): the top-down threshold walk with the §8.1 zero-alfa refit.
+WalkResult walk(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size) {
+    const orc_header& hdr = ctx.hdr;
+    if (row >= hdr.height || col >= hdr.width) return {};
+    const bool forced = size > hdr.max_size || row + size > hdr.height || col + size > hdr.width;
+    if (forced) return split(ctx, row, col, size / 2);
+    if (size == 1) {
+        orc_leaf l = make_leaf(row, col, 1);
+        l.qbeta = best_beta(pixel_at(ctx.im, row, col), 1, hdr.bits_beta);
+        WalkResult r;
+        r.leaves.push_back(l);
+        return r;
+    }
+    std::vector<orc_candidate> top;
+    const uint64_t block_evals =
+        search_top_k(ctx.im, *ctx.contracted, row, col, size, ctx.params.shift, ctx.params, 1, top);
+    const double best_rms = top.empty() ? INFINITY : top[0].rms;
+    if (best_rms > ctx.params.t_rms && size > hdr.min_size) {
+        WalkResult r = split(ctx, row, col, size / 2);
+        r.evals += block_evals;
+        return r;
+    }
+    orc_leaf leaf = make_leaf(row, col, size);
+    if (!top.empty()) {
+        const orc_candidate& c = top[0];
+        leaf.mode = 2;
+        leaf.qalfa = c.qalfa;
+        leaf.qbeta = c.qbeta;
+        leaf.isometry = c.isometry;
+        leaf.dom_row = c.dom_row;
+        leaf.dom_col = c.dom_col;
+    }
+    const uint32_t diff = leaf.qalfa;  // qalfa.abs_diff(0)
+    if (diff <= ctx.params.zero_threshold) {
+        leaf.qbeta = best_beta(range_sum(ctx.im, row, col, size), (int64_t)size * size,
+                               hdr.bits_beta);
+        leaf.qalfa = 0;
+        leaf.mode = 0;
+        leaf.isometry = 0;
+        leaf.dom_row = 0;
+        leaf.dom_col = 0;
+    }
+    WalkResult r;
+    r.leaves.push_back(leaf);
+    r.evals = block_evals;
+    return r;
+}
+
+// affine_fit (encode.rs:1724-1781), mode 1.
+void affine_fit(const std::vector<double>& block, uint32_t size, uint32_t bits_beta,
+                uint32_t* qbeta_out, int32_t* qgx_out, int32_t* qgy_out, double* sse_out) {
+    const double n = (double)size * (double)size;
+    double t0 = 0.0, tu = 0.0, tv = 0.0;
+    for (uint32_t u = 0; u < size; ++u)
+        for (uint32_t v = 0; v < size; ++v) {
+            const double p = block[u * size + v];
+            t0 += p;
+            tu += p * (double)u;
+            tv += p * (double)v;
+        }
+    double su = -0.0, suu = -0.0;
+    for (uint32_t u = 0; u < size; ++u) su += (double)u;
+    for (uint32_t u = 0; u < size; ++u) suu += (double)u * (double)u;
+    const double s0 = n;
+    const double s_u = (double)size * su;
+    const double s_v = s_u;
+    const double s_uu = (double)size * suu;
+    const double s_vv = s_uu;
+    const double s_uv = su * su;
+    auto det3 = [](const double m[3][3]) {
+        return m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
+               m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+               m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+    };
+    const double a[3][3] = {{s0, s_u, s_v}, {s_u, s_uu, s_uv}, {s_v, s_uv, s_vv}};
+    const double det_a = det3(a);
+    double b0, gx, gy;
+    if (std::fabs(det_a) < 1e-9) {
+        b0 = t0 / s0;
+        gx = 0.0;
+        gy = 0.0;
+    } else {
+        const double a_b0[3][3] = {{t0, s_u, s_v}, {tu, s_uu, s_uv}, {tv, s_uv, s_vv}};
+        const double a_gx[3][3] = {{s0, t0, s_v}, {s_u, tu, s_uv}, {s_v, tv, s_vv}};
+        const double a_gy[3][3] = {{s0, s_u, t0}, {s_u, s_uu, tu}, {s_v, s_uv, tv}};
+        b0 = det3(a_b0) / det_a;
+        gx = det3(a_gx) / det_a;
+        gy = det3(a_gy) / det_a;
+    }
+    const uint32_t max_qbeta = (1u << bits_beta) - 1;
+    const uint32_t qbeta = quantise_f64(std::max(b0 / 255.0 * (double)max_qbeta, 0.0), max_qbeta);
+    auto qgrad = [](double g) {
+        double r = std::round(g * AFFINE_GRAD_SCALE);
+        if (r < -(double)AFFINE_GRAD_CLAMP) r = -(double)AFFINE_GRAD_CLAMP;
+        if (r > (double)AFFINE_GRAD_CLAMP) r = (double)AFFINE_GRAD_CLAMP;
+        return (int32_t)r;
+    };
+    const int32_t qgx = qgrad(gx), qgy = qgrad(gy);
+    const double b0q = (double)qbeta / (double)max_qbeta * 255.0;
+    const double gxq = (double)qgx / AFFINE_GRAD_SCALE;
+    const double gyq = (double)qgy / AFFINE_GRAD_SCALE;
+    double sse = 0.0;
+    for (uint32_t u = 0; u < size; ++u)
+        for (uint32_t v = 0; v < size; ++v) {
+            const double pred = b0q + gxq * (double)u + gyq * (double)v;
+            const double diff = block[u * size + v] - pred;
+            sse += diff * diff;
+        }
+    *qbeta_out = qbeta;
+    *qgx_out = qgx;
+    *qgy_out = qgy;
+    *sse_out = sse;
+}
+
+struct Priced {
+    orc_leaf leaf;
+    double d, r;
+};
+
+// best_mode_leaf (encode.rs:1536-1714), modes 0, 1 and 2.
+Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
+                      const std::vector<orc_candidate>& ranked, double lambda, uint32_t sc) {
+    const orc_header& hdr = ctx.hdr;
+    std::vector<double> block((size_t)size * size);
+    int64_t rsum = 0;
+    for (uint32_t i = 0; i < size; ++i)
+        for (uint32_t j = 0; j < size; ++j) {
+            const uint32_t v = pixel_at(ctx.im, row + i, col + j);
+            block[i * size + j] = (double)v;
+            rsum += v;
+        }
+    const int64_t s0 = (int64_t)size * size;
+    std::vector<Priced> cands;
+    auto mode0 = [&]() {
+        orc_leaf l = make_leaf(row, col, size);
+        l.qbeta = best_beta(rsum, s0, hdr.bits_beta);
+        const uint32_t max_qbeta = (1u << hdr.bits_beta) - 1;
+        const double beta2 = (double)l.qbeta / (double)max_qbeta * 255.0;
+        double sse = -0.0;
+        for (double p : block) sse += (p - beta2) * (p - beta2);
+        const double r = leaf_bits(*ctx.rate, hdr, l, sc);
+        cands.push_back({l, sse, r});
+    };
+    if (ctx.allowed[0]) mode0();
+    if (ctx.allowed[1]) {
+        orc_leaf l = make_leaf(row, col, size);
+        l.mode = 1;
+        double sse;
+        affine_fit(block, size, hdr.bits_beta, &l.qbeta, &l.qgx, &l.qgy, &sse);
+        const double r = leaf_bits(*ctx.rate, hdr, l, sc);
+        cands.push_back({l, sse, r});
+    }
+    for (const auto& c : ranked) {
+        if (c.qalfa < 1) continue;
+        if (ctx.allowed[2]) {
+            orc_leaf l = make_leaf(row, col, size);
+            l.mode = 2;
+            l.qalfa = c.qalfa;
+            l.qbeta = c.qbeta;
+            l.isometry = c.isometry;
+            l.dom_row = c.dom_row;
+            l.dom_col = c.dom_col;
+            const double sse2 = c.rms * c.rms * (double)size * (double)size;
+            const double r2 = leaf_bits(*ctx.rate, hdr, l, sc);
+            cands.push_back({l, sse2, r2});
+        }
+    }
+    if (cands.empty()) mode0();
+    size_t best = 0;
+    for (size_t i = 1; i < cands.size(); ++i) {
+        const double jb = cands[best].d + lambda * cands[best].r;
+        const double ji = cands[i].d + lambda * cands[i].r;
+        if (ji < jb) best = i;  // min_by keeps the first of equal minima
+    }
+    return cands[best];
+}
+
+// block_rms (encode.rs:386-403) and adaptive_shift (:431-437).
+double block_rms(const Image& im, uint32_t row, uint32_t col, uint32_t size) {
+    int64_t t0 = 0, t2 = 0;
+    for (uint32_t i = 0; i < size; ++i)
+        for (uint32_t j = 0; j < size; ++j) {
+            const int64_t v = pixel_at(im, row + i, col + j);
+            t0 += v;
+            t2 += v * v;
+        }
+    const int64_t s0 = (int64_t)size * size;
+    const double mean = (double)t0 / (double)s0;
+    double variance = (double)t2 / (double)s0 - mean * mean;
+    if (!(variance >= 0.0)) variance = 0.0;
+    return std::sqrt(variance);
+}
+constexpr double DENSITY_LOW_RMS = 4.0;  // encode.rs:376
+uint32_t adaptive_shift(uint32_t base, double rms) {
+    if (rms <= DENSITY_LOW_RMS) {
+        const uint64_t d = (uint64_t)base * 2;
+        return d > 0xffffffffull ? 0xffffffffu : (uint32_t)d;
+    }
+    return base;
+}
+
+struct RdResult {
+    std::vector<orc_leaf> leaves;
+    uint64_t evals = 0;
+    double d = 0.0, r = 0.0;
+};
+
+RdResult walk_rd(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, double lambda);
+
+// split_rd (encode.rs:2033-2071).
+RdResult split_rd(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t half, double lambda) {
+    RdResult q[4];
+    const uint32_t rs[4] = {row, row + half, row, row + half};
+    const uint32_t cs[4] = {col, col, col + half, col + half};
+    if (half >= PARALLEL_SIZE_CUTOFF) {
+        for (int i = 0; i < 4; ++i) {
+#pragma omp task shared(q, ctx) firstprivate(i)
+            q[i] = walk_rd(ctx, rs[i], cs[i], half, lambda);
+        }
+#pragma omp taskwait
+    } else {
+        for (int i = 0; i < 4; ++i) q[i] = walk_rd(ctx, rs[i], cs[i], half, lambda);
+    }
+    RdResult out;
+    for (auto& x : q) {
+        out.leaves.insert(out.leaves.end(), x.leaves.begin(), x.leaves.end());
+        out.evals += x.evals;
+        out.d += x.d;
+        out.r += x.r;
+    }
+    return out;
+}
+
+// walk_rd (encode.rs:1865-2027): bottom-up J = D + lambda*R, no lambda regions.
+RdResult walk_rd(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, double lambda) {
+    const orc_header& hdr = ctx.hdr;
+    if (row >= hdr.height || col >= hdr.width) return {};
+    const bool forced = size > hdr.max_size || row + size > hdr.height || col + size > hdr.width;
+    if (forced) return split_rd(ctx, row, col, size / 2, lambda);
+    const RateModels& rate = *ctx.rate;
+    const uint32_t sc = size_class_of(size);
+    if (size == 1) {
+        const uint32_t pixel = pixel_at(ctx.im, row, col);
+        orc_leaf l = make_leaf(row, col, 1);
+        l.qbeta = best_beta(pixel, 1, hdr.bits_beta);
+        double dv = 0.5 + (double)l.qbeta / (double)((1u << hdr.bits_beta) - 1) * 255.0;
+        if (dv < 0.0) dv = 0.0;
+        if (dv > 255.0) dv = 255.0;
+        const uint8_t decoded = (uint8_t)dv;
+        const double diff = (double)pixel - (double)decoded;
+        RdResult r;
+        r.leaves.push_back(l);
+        r.d = diff * diff;
+        r.r = leaf_bits(rate, hdr, l, sc);
+        return r;
+    }
+    const double node_lambda = lambda * 1.0;
+    const uint32_t shift = ctx.adaptive_density
+                               ? adaptive_shift(ctx.params.shift, block_rms(ctx.im, row, col, size))
+                               : ctx.params.shift;
+    std::vector<orc_candidate> top;
+    const uint64_t block_evals =
+        search_top_k(ctx.im, *ctx.contracted, row, col, size, shift, ctx.params, 1, top);
+    Priced leaf = best_mode_leaf(ctx, row, col, size, top, node_lambda, sc);
+    if (size <= hdr.min_size) {
+        RdResult r;
+        r.leaves.push_back(leaf.leaf);
+        r.evals = block_evals;
+        r.d = leaf.d;
+        r.r = leaf.r;
+        return r;
+    }
+    RdResult children = split_rd(ctx, row, col, size / 2, lambda);
+    const uint64_t total_evals = block_evals + children.evals;
+    const double split0 = rate.bits_for({FIELD_SPLIT, sc}, 2, 0);
+    const double split1 = rate.bits_for({FIELD_SPLIT, sc}, 2, 1);
+    const double leaf_j = leaf.d + node_lambda * (leaf.r + split0);
+    const double split_j = children.d + node_lambda * (children.r + split1);
+    if (leaf_j <= split_j) {
+        RdResult r;
+        r.leaves.push_back(leaf.leaf);
+        r.evals = total_evals;
+        r.d = leaf.d;
+        r.r = leaf.r + split0;
+        return r;
+    }
+    children.evals = total_evals;
+    children.r = children.r + split1;
+    return children;
+}
+
+// build_header (encode.rs:1033-1047).
+orc_header build_header(uint32_t w, uint32_t h, const orc_params& p) {
+    orc_header hdr;
+    hdr.bits_alfa = p.bits_alfa;
+    hdr.bits_beta = p.bits_beta;
+    hdr.min_size = p.min_size;
+    hdr.max_size = p.max_size;
+    hdr.shift = p.shift;
+    hdr.width = w;
+    hdr.height = h;
+    hdr.int_max_alfa = quantise_f64(p.max_alfa / 8.0 * 256.0, 255);
+    return hdr;
+}
+
+template <class F>
+void run_parallel(int nthreads, F&& f) {
+#ifdef _OPENMP
+    const int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel num_threads(nt)
+#pragma omp single
+    f();
+#else
+    (void)nthreads;
+    f();
+#endif
+}
+
+// ------------------------------------------------------------------ decode
+
+double max_alfa_of(const orc_header& h) { return (double)h.int_max_alfa / 256.0 * 8.0; }
+
+// decode_leaf (ifs.rs:406-484), modes 0/1/2.
+void decode_leaf(const orc_header& hdr, const orc_leaf& leaf, const uint8_t* img, size_t stride,
+                 uint8_t* next) {
+    const uint32_t size = leaf.size;
+    if (leaf.mode == 1) {
+        const double b0 = (double)leaf.qbeta / (double)((1u << hdr.bits_beta) - 1) * 255.0;
+        const double gx = (double)leaf.qgx / AFFINE_GRAD_SCALE;
+        const double gy = (double)leaf.qgy / AFFINE_GRAD_SCALE;
+        for (uint32_t u = 0; u < size; ++u)
+            for (uint32_t v = 0; v < size; ++v) {
+                double value = std::round(b0 + gx * (double)u + gy * (double)v);
+                if (value < 0.0) value = 0.0;
+                if (value > 255.0) value = 255.0;
+                next[(leaf.row + u) * stride + leaf.col + v] = (uint8_t)value;
+            }
+        return;
+    }
+    const double alfa = (double)leaf.qalfa / (double)(1u << hdr.bits_alfa) * max_alfa_of(hdr);
+    double beta = (double)leaf.qbeta / (double)((1u << hdr.bits_beta) - 1) *
+                  ((1.0 + std::fabs(alfa)) * 255.0);
+    if (alfa > 0.0) beta -= alfa * 255.0;
+    for (uint32_t u = 0; u < size; ++u)
+        for (uint32_t v = 0; v < size; ++v) {
+            double d = 0.0;
+            if (leaf.qalfa != 0) {
+                const size_t dr = leaf.dom_row + 2 * u, dc = leaf.dom_col + 2 * v;
+                d = ((double)img[dr * stride + dc] + (double)img[(dr + 1) * stride + dc] +
+                     (double)img[dr * stride + dc + 1] + (double)img[(dr + 1) * stride + dc + 1]) /
+                    4.0;
+            }
+            uint32_t i, j;
+            iso_map(leaf.isometry, u, v, size, &i, &j);
+            double value = (0.5 + d * alfa) + beta;
+            if (value < 0.0) value = 0.0;
+            if (value > 255.0) value = 255.0;
+            next[(leaf.row + i) * stride + leaf.col + j] = (uint8_t)value;
+        }
+}
+
+// ------------------------------------------------------------------ .ifs bits
+
+struct BitReader {
+    const uint8_t* data;
+    size_t len, pos = 0;
+    bool bit(uint32_t* b) {
+        if ((pos >> 3) >= len) return false;
+        *b = (data[pos >> 3] >> (7 - (pos & 7))) & 1;
+        ++pos;
+        return true;
+    }
+    bool read(uint32_t n, uint32_t* v) {
+        uint32_t x = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t b;
+            if (!bit(&b)) return false;
+            x |= b << i;
+        }
+        *v = x;
+        return true;
+    }
+};
+
+// ifs walk (ifs.rs:221-279).
+int ifs_walk(BitReader& r, const orc_header& hdr, uint32_t row, uint32_t col, uint32_t size,
+             std::vector<orc_leaf>& leaves) {
+    if (row >= hdr.height || col >= hdr.width) return 0;
+    const bool forced = size > hdr.max_size || row + size > hdr.height || col + size > hdr.width;
+    uint32_t flag = 0;
+    if (!forced && size > hdr.min_size) {
+        if (!r.read(1, &flag)) return -1;
+    }
+    if (forced || flag == 1) {
+        const uint32_t half = size / 2;
+        int e;
+        if ((e = ifs_walk(r, hdr, row, col, half, leaves))) return e;
+        if ((e = ifs_walk(r, hdr, row + half, col, half, leaves))) return e;
+        if ((e = ifs_walk(r, hdr, row, col + half, half, leaves))) return e;
+        return ifs_walk(r, hdr, row + half, col + half, half, leaves);
+    }
+    orc_leaf l = make_leaf(row, col, size);
+    if (!r.read(hdr.bits_alfa, &l.qalfa) || !r.read(hdr.bits_beta, &l.qbeta)) return -1;
+    if (l.qalfa != 0) {
+        uint32_t iso, dr, dc;
+        if (!r.read(3, &iso) || !r.read(bits_coord_row(hdr), &dr) ||
+            !r.read(bits_coord_col(hdr), &dc))
+            return -1;
+        l.isometry = iso;
+        l.dom_row = hdr.shift * dr;
+        l.dom_col = hdr.shift * dc;
+        if (l.dom_row + 2 * size > hdr.height || l.dom_col + 2 * size > hdr.width) return -2;
+        l.mode = 2;
+    }
+    leaves.push_back(l);
+    return 0;
+}
+
+struct BitWriter {
+    std::vector<uint8_t> bits;
+    void write(uint32_t n, uint32_t v) {
+        for (uint32_t i = 0; i < n; ++i) bits.push_back((v >> i) & 1);
+    }
+    std::vector<uint8_t> finish() const {
+        std::vector<uint8_t> out((bits.size() + 7) / 8, 0);
+        for (size_t i = 0; i < bits.size(); ++i)
+            if (bits[i]) out[i / 8] |= (uint8_t)(1u << (7 - (i % 8)));
+        return out;
+    }
+};
+
+// write_walk (ifs.rs:555-599).
+bool ifs_write_walk(BitWriter& w, const orc_header& hdr, uint32_t row, uint32_t col,
+                    uint32_t size, const LeafMap& by_pos) {
+    if (row >= hdr.height || col >= hdr.width) return true;
+    const uint32_t half = size / 2;
+    const bool forced = size > hdr.max_size || row + size > hdr.height || col + size > hdr.width;
+    auto quads = [&]() {
+        return ifs_write_walk(w, hdr, row, col, half, by_pos) &&
+               ifs_write_walk(w, hdr, row + half, col, half, by_pos) &&
+               ifs_write_walk(w, hdr, row, col + half, half, by_pos) &&
+               ifs_write_walk(w, hdr, row + half, col + half, half, by_pos);
+    };
+    if (forced) return quads();
+    auto it = by_pos.find({row, col, size});
+    if (it == by_pos.end()) {
+        if (size <= hdr.min_size) return false;
+        w.write(1, 1);
+        return quads();
+    }
+    const orc_leaf& l = *it->second;
+    if (size > hdr.min_size) w.write(1, 0);
+    w.write(hdr.bits_alfa, l.qalfa);
+    w.write(hdr.bits_beta, l.qbeta);
+    if (l.qalfa != 0) {
+        w.write(3, l.isometry);
+        w.write(bits_coord_row(hdr), l.dom_row / hdr.shift);
+        w.write(bits_coord_col(hdr), l.dom_col / hdr.shift);
+    }
+    return true;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+
+extern "C" {
+
+void orc_contract(const uint8_t* px, uint32_t w, uint32_t h, int32_t* out) {
+    Contracted c = Contracted::build(Image{px, w, h});
+    std::memcpy(out, c.data.data(), c.data.size() * sizeof(int32_t));
+}
+
+void orc_fit_f64(const orc_moments* m, double max_alfa, uint32_t bits_alfa, uint32_t bits_beta,
+                 uint32_t* qalfa, uint32_t* qbeta, double* rms) {
+    fit_f64(*m, max_alfa, bits_alfa, bits_beta, qalfa, qbeta, rms);
+}
+
+uint32_t orc_best_beta(int64_t range_sum_, int64_t pixel_count, uint32_t bits_beta) {
+    return best_beta(range_sum_, pixel_count, bits_beta);
+}
+
+int orc_search(const uint8_t* px, uint32_t w, uint32_t h, const int32_t* contracted,
+               uint32_t row, uint32_t col, uint32_t size, uint32_t shift, const orc_params* p,
+               uint32_t k, orc_candidate* out, uint32_t* nout, uint64_t* evals) {
+    if (!px || !p || k == 0 || row + size > h || col + size > w || shift == 0) return -1;
+    Image im{px, w, h};
+    Contracted c;
+    if (contracted) {
+        c.stride = w / 2;
+        c.data.assign(contracted, contracted + (size_t)(w / 2) * (h / 2));
+    } else {
+        c = Contracted::build(im);
+    }
+    std::vector<orc_candidate> top;
+    *evals = search_top_k(im, c, row, col, size, shift, *p, k, top);
+    *nout = (uint32_t)top.size();
+    for (size_t i = 0; i < top.size(); ++i) out[i] = top[i];
+    return 0;
+}
+
+int orc_search_blocks(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size, uint32_t shift,
+                      const orc_params* p, const uint32_t* rows, const uint32_t* cols, size_t n,
+                      orc_candidate* out, uint64_t* evals_per_block, int nthreads) {
+    if (!px || !p || size == 0 || shift == 0) return -1;
+    for (size_t i = 0; i < n; ++i)
+        if (rows[i] + size > h || cols[i] + size > w) return -1;
+    Image im{px, w, h};
+    Contracted c = Contracted::build(im);
+#ifdef _OPENMP
+    const int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+#else
+    (void)nthreads;
+#endif
+    for (long i = 0; i < (long)n; ++i) {
+        std::vector<orc_candidate> top;
+        evals_per_block[i] = search_top_k(im, c, rows[i], cols[i], size, shift, *p, 1, top);
+        if (top.empty()) {
+            std::memset(&out[i], 0, sizeof(orc_candidate));
+        } else {
+            out[i] = top[0];
+        }
+    }
+    return 0;
+}
+
+int orc_search_grid(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size, uint32_t shift,
+                    const orc_params* p, orc_candidate* out, uint64_t* evals_per_block,
+                    int nthreads) {
+    if (size == 0) return -1;
+    const uint32_t by = h / size, bx = w / size;
+    std::vector<uint32_t> rows((size_t)by * bx), cols((size_t)by * bx);
+    for (uint32_t i = 0; i < by; ++i)
+        for (uint32_t j = 0; j < bx; ++j) {
+            rows[(size_t)i * bx + j] = i * size;
+            cols[(size_t)i * bx + j] = j * size;
+        }
+    return orc_search_blocks(px, w, h, size, shift, p, rows.data(), cols.data(), rows.size(), out,
+                             evals_per_block, nthreads);
+}
+
+int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
+               const orc_options* o, orc_header* hdr_out, orc_leaf** leaves, size_t* nleaves,
+               uint64_t* search_evals, uint64_t* warmup_evals, int nthreads) {
+    if (!px || !p || !o || w == 0 || h == 0 || p->shift == 0) return -1;
+    if (p->has_lambda && !(std::isfinite(p->lambda) && p->lambda >= 0.0)) return -1;
+    if (o->allowed_modes[3]) return -3;  // mode 3 (DCT residual) is not restated here
+    Image im{px, w, h};
+    const orc_header hdr = build_header(w, h, *p);
+    Contracted c = Contracted::build(im);
+    std::vector<orc_leaf> out;
+    uint64_t sev = 0, wev = 0;
+    int status = 0;
+    run_parallel(nthreads, [&]() {
+        if (p->has_lambda) {
+            // build_rate_snapshot (encode.rs:1139-1169): exhaustive threshold walk at t_rms 8.
+            Ctx warm{im, &c, hdr, *p, nullptr, {1, 1, 1, 1}, false};
+            warm.params.t_rms = 8.0;
+            warm.params.has_lambda = 0;
+            WalkResult wr = walk(warm, 0, 0, virtual_size(hdr));
+            RateModels rate;
+            if (!RateModels::from_leaves(hdr, wr.leaves, rate)) {
+                status = -4;
+                return;
+            }
+            wev = wr.evals;
+            Ctx ctx{im, &c, hdr, *p, &rate, {o->allowed_modes[0], o->allowed_modes[1],
+                                             o->allowed_modes[2], o->allowed_modes[3]},
+                    o->adaptive_density != 0};
+            RdResult rr = walk_rd(ctx, 0, 0, virtual_size(hdr), p->lambda);
+            out = std::move(rr.leaves);
+            sev = rr.evals;
+        } else {
+            Ctx ctx{im, &c, hdr, *p, nullptr, {1, 1, 1, 1}, false};
+            WalkResult wr = walk(ctx, 0, 0, virtual_size(hdr));
+            out = std::move(wr.leaves);
+            sev = wr.evals;
+        }
+    });
+    if (status) return status;
+    *hdr_out = hdr;
+    *nleaves = out.size();
+    *leaves = (orc_leaf*)std::malloc(std::max<size_t>(1, out.size()) * sizeof(orc_leaf));
+    std::memcpy(*leaves, out.data(), out.size() * sizeof(orc_leaf));
+    *search_evals = sev;
+    *warmup_evals = wev;
+    return 0;
+}
+
+void orc_free(void* ptr) { std::free(ptr); }
+
+int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, uint32_t iterations,
+               uint8_t* out) {
+    const size_t w = hdr->width, h = hdr->height;
+    std::vector<uint8_t> img(w * h, 128), next(w * h, 0);
+    for (uint32_t it = 0; it < iterations; ++it) {
+        std::fill(next.begin(), next.end(), 0);
+        for (size_t i = 0; i < n; ++i) decode_leaf(*hdr, leaves[i], img.data(), w, next.data());
+        img.swap(next);
+    }
+    std::memcpy(out, img.data(), w * h);
+    return 0;
+}
+
+int orc_ifs_parse(const uint8_t* data, size_t len, orc_header* hdr, orc_leaf** leaves,
+                  size_t* nleaves) {
+    BitReader r{data, len};
+    orc_header h;
+    if (!r.read(4, &h.bits_alfa) || !r.read(4, &h.bits_beta) || !r.read(7, &h.min_size) ||
+        !r.read(7, &h.max_size) || !r.read(6, &h.shift) || !r.read(12, &h.width) ||
+        !r.read(12, &h.height) || !r.read(8, &h.int_max_alfa))
+        return -1;
+    if (h.width == 0 || h.height == 0 || h.shift == 0) return -3;
+    std::vector<orc_leaf> out;
+    const int e = ifs_walk(r, h, 0, 0, virtual_size(h), out);
+    if (e) return e;
+    const size_t left = len * 8 - r.pos;
+    if (left >= 8) return -4;
+    if (left > 0 && (data[len - 1] & ((1u << left) - 1)) != 0) return -5;
+    *hdr = h;
+    *nleaves = out.size();
+    *leaves = (orc_leaf*)std::malloc(std::max<size_t>(1, out.size()) * sizeof(orc_leaf));
+    std::memcpy(*leaves, out.data(), out.size() * sizeof(orc_leaf));
+    return 0;
+}
+
+int orc_ifs_write(const orc_header* hdr, const orc_leaf* leaves, size_t n, uint8_t** out,
+                  size_t* len) {
+    LeafMap by_pos;
+    for (size_t i = 0; i < n; ++i) {
+        if (!by_pos.emplace(std::make_tuple(leaves[i].row, leaves[i].col, leaves[i].size), &leaves[i])
+                 .second)
+            return -2;
+    }
+    BitWriter w;
+    w.write(4, hdr->bits_alfa);
+    w.write(4, hdr->bits_beta);
+    w.write(7, hdr->min_size);
+    w.write(7, hdr->max_size);
+    w.write(6, hdr->shift);
+    w.write(12, hdr->width);
+    w.write(12, hdr->height);
+    w.write(8, hdr->int_max_alfa);
+    if (!ifs_write_walk(w, *hdr, 0, 0, virtual_size(*hdr), by_pos)) return -3;
+    std::vector<uint8_t> bytes = w.finish();
+    *len = bytes.size();
+    *out = (uint8_t*)std::malloc(std::max<size_t>(1, bytes.size()));
+    std::memcpy(*out, bytes.data(), bytes.size());
+    return 0;
+}
+
+double orc_leaf_bits(const orc_header* warm_hdr, const orc_leaf* warm_leaves, size_t nwarm,
+                     const orc_leaf* leaf) {
+    RateModels rate;
+    std::vector<orc_leaf> wl(warm_leaves, warm_leaves + nwarm);
+    if (!RateModels::from_leaves(*warm_hdr, wl, rate)) return NAN;
+    return leaf_bits(rate, *warm_hdr, *leaf, size_class_of(leaf->size));
+}
+
+}  // extern "C"

@@ -1,0 +1,232 @@
+"""ctypes wrapper for the CPU oracle (oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg as the parity checker; the product package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("min_size", C.c_uint32), ("max_size", C.c_uint32), ("shift", C.c_uint32),
+        ("bits_alfa", C.c_uint32), ("bits_beta", C.c_uint32), ("zero_threshold", C.c_uint32),
+        ("max_alfa", C.c_double), ("t_rms", C.c_double), ("has_lambda", C.c_int32),
+        ("pad_", C.c_int32), ("lambda_", C.c_double),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [("allowed_modes", C.c_uint8 * 4), ("adaptive_density", C.c_int32)]
+
+
+class Moments(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("s0", "s1_x4", "s2_x16", "t0", "t1_x4", "t2")]
+
+
+class Candidate(C.Structure):
+    _fields_ = [
+        ("dom_row", C.c_uint32), ("dom_col", C.c_uint32), ("isometry", C.c_uint32),
+        ("qalfa", C.c_uint32), ("qbeta", C.c_uint32), ("valid", C.c_uint32),
+        ("rms", C.c_double), ("m", Moments),
+    ]
+
+
+class Leaf(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in (
+        "row", "col", "size", "mode", "qalfa", "qbeta", "isometry", "dom_row", "dom_col")] + [
+        ("qgx", C.c_int32), ("qgy", C.c_int32)]
+
+
+class Header(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in (
+        "bits_alfa", "bits_beta", "min_size", "max_size", "shift", "width", "height",
+        "int_max_alfa")]
+
+
+CANDIDATE_DTYPE = np.dtype([
+    ("dom_row", "<u4"), ("dom_col", "<u4"), ("isometry", "<u4"), ("qalfa", "<u4"),
+    ("qbeta", "<u4"), ("valid", "<u4"), ("rms", "<f8"), ("s0", "<i8"), ("s1_x4", "<i8"),
+    ("s2_x16", "<i8"), ("t0", "<i8"), ("t1_x4", "<i8"), ("t2", "<i8")])
+LEAF_DTYPE = np.dtype([(n, "<u4") for n in (
+    "row", "col", "size", "mode", "qalfa", "qbeta", "isometry", "dom_row", "dom_col")] + [
+    ("qgx", "<i4"), ("qgy", "<i4")])
+assert CANDIDATE_DTYPE.itemsize == C.sizeof(Candidate)
+assert LEAF_DTYPE.itemsize == C.sizeof(Leaf)
+
+_lib = None
+
+
+def build() -> None:
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        P = C.POINTER
+        L.orc_contract.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
+        L.orc_fit_f64.argtypes = [P(Moments), C.c_double, C.c_uint32, C.c_uint32,
+                                  P(C.c_uint32), P(C.c_uint32), P(C.c_double)]
+        L.orc_best_beta.argtypes = [C.c_int64, C.c_int64, C.c_uint32]
+        L.orc_best_beta.restype = C.c_uint32
+        L.orc_search.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
+                                 C.c_uint32, C.c_uint32, C.c_uint32, P(Params), C.c_uint32,
+                                 C.c_void_p, P(C.c_uint32), P(C.c_uint64)]
+        L.orc_search_grid.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                      P(Params), C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_search_blocks.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                        C.c_uint32, P(Params), C.c_void_p, C.c_void_p, C.c_size_t,
+                                        C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_encode.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, P(Params), P(Options),
+                                 P(Header), P(C.c_void_p), P(C.c_size_t), P(C.c_uint64),
+                                 P(C.c_uint64), C.c_int]
+        L.orc_free.argtypes = [C.c_void_p]
+        L.orc_decode.argtypes = [P(Header), C.c_void_p, C.c_size_t, C.c_uint32, C.c_void_p]
+        L.orc_ifs_parse.argtypes = [C.c_void_p, C.c_size_t, P(Header), P(C.c_void_p),
+                                    P(C.c_size_t)]
+        L.orc_ifs_write.argtypes = [P(Header), C.c_void_p, C.c_size_t, P(C.c_void_p),
+                                    P(C.c_size_t)]
+        L.orc_leaf_bits.argtypes = [P(Header), C.c_void_p, C.c_size_t, P(Leaf)]
+        L.orc_leaf_bits.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def make_params(min_size=4, max_size=16, shift=4, bits_alfa=4, bits_beta=7, max_alfa=1.0,
+                t_rms=8.0, zero_threshold=0, lam=None) -> Params:
+    return Params(min_size, max_size, shift, bits_alfa, bits_beta, zero_threshold, max_alfa,
+                  t_rms, 0 if lam is None else 1, 0, 0.0 if lam is None else float(lam))
+
+
+def _u8(img: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(img, dtype=np.uint8)
+    assert a.ndim == 2
+    return a
+
+
+def contract(img: np.ndarray) -> np.ndarray:
+    a = _u8(img)
+    h, w = a.shape
+    out = np.zeros((h // 2, w // 2), dtype=np.int32)
+    lib().orc_contract(a.ctypes.data, w, h, out.ctypes.data)
+    return out
+
+
+def fit_f64(s0, s1_x4, s2_x16, t0, t1_x4, t2, max_alfa=1.0, bits_alfa=4, bits_beta=7):
+    m = Moments(s0, s1_x4, s2_x16, t0, t1_x4, t2)
+    qa, qb, rms = C.c_uint32(), C.c_uint32(), C.c_double()
+    lib().orc_fit_f64(C.byref(m), max_alfa, bits_alfa, bits_beta, C.byref(qa), C.byref(qb),
+                      C.byref(rms))
+    return qa.value, qb.value, rms.value
+
+
+def best_beta(range_sum: int, pixel_count: int, bits_beta: int = 7) -> int:
+    return lib().orc_best_beta(range_sum, pixel_count, bits_beta)
+
+
+def search(img, row, col, size, shift, params: Params, k=1):
+    """search_top_k for one block: (candidates structured array, evals)."""
+    a = _u8(img)
+    h, w = a.shape
+    out = np.zeros(k, dtype=CANDIDATE_DTYPE)
+    n, ev = C.c_uint32(), C.c_uint64()
+    rc = lib().orc_search(a.ctypes.data, w, h, None, row, col, size, shift, C.byref(params), k,
+                          out.ctypes.data, C.byref(n), C.byref(ev))
+    if rc:
+        raise ValueError(f"orc_search failed: {rc}")
+    return out[: n.value], ev.value
+
+
+def search_grid(img, size, shift, params: Params, nthreads=0):
+    """search_block over every aligned size x size block, row-major."""
+    a = _u8(img)
+    h, w = a.shape
+    nb = (h // size) * (w // size)
+    out = np.zeros(nb, dtype=CANDIDATE_DTYPE)
+    ev = np.zeros(nb, dtype=np.uint64)
+    rc = lib().orc_search_grid(a.ctypes.data, w, h, size, shift, C.byref(params), out.ctypes.data,
+                               ev.ctypes.data, nthreads)
+    if rc:
+        raise ValueError(f"orc_search_grid failed: {rc}")
+    return out, ev
+
+
+def search_blocks(img, size, shift, params: Params, rows, cols, nthreads=0):
+    a = _u8(img)
+    h, w = a.shape
+    rows = np.ascontiguousarray(rows, dtype=np.uint32)
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    out = np.zeros(len(rows), dtype=CANDIDATE_DTYPE)
+    ev = np.zeros(len(rows), dtype=np.uint64)
+    rc = lib().orc_search_blocks(a.ctypes.data, w, h, size, shift, C.byref(params),
+                                 rows.ctypes.data, cols.ctypes.data, len(rows), out.ctypes.data,
+                                 ev.ctypes.data, nthreads)
+    if rc:
+        raise ValueError(f"orc_search_blocks failed: {rc}")
+    return out, ev
+
+
+def encode(img, params: Params, allowed_modes=(1, 0, 1, 0), adaptive_density=False, nthreads=0):
+    """encode_image_with_search(.., ExhaustiveSearch): (header, leaves, search_evals, warmup)."""
+    a = _u8(img)
+    h, w = a.shape
+    opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density))
+    hdr = Header()
+    ptr, n = C.c_void_p(), C.c_size_t()
+    sev, wev = C.c_uint64(), C.c_uint64()
+    rc = lib().orc_encode(a.ctypes.data, w, h, C.byref(params), C.byref(opts), C.byref(hdr),
+                          C.byref(ptr), C.byref(n), C.byref(sev), C.byref(wev), nthreads)
+    if rc:
+        raise ValueError(f"orc_encode failed: {rc}")
+    leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize), dtype=LEAF_DTYPE).copy()
+    lib().orc_free(ptr)
+    return hdr, leaves, sev.value, wev.value
+
+
+def decode(hdr: Header, leaves: np.ndarray, iterations: int = 10) -> np.ndarray:
+    leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    out = np.zeros((hdr.height, hdr.width), dtype=np.uint8)
+    lib().orc_decode(C.byref(hdr), leaves.ctypes.data, len(leaves), iterations, out.ctypes.data)
+    return out
+
+
+def ifs_parse(data: bytes):
+    buf = np.frombuffer(data, dtype=np.uint8)
+    hdr = Header()
+    ptr, n = C.c_void_p(), C.c_size_t()
+    rc = lib().orc_ifs_parse(buf.ctypes.data, len(data), C.byref(hdr), C.byref(ptr), C.byref(n))
+    if rc:
+        raise ValueError(f"orc_ifs_parse failed: {rc}")
+    leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize), dtype=LEAF_DTYPE).copy()
+    lib().orc_free(ptr)
+    return hdr, leaves
+
+
+def ifs_write(hdr: Header, leaves: np.ndarray) -> bytes:
+    leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    ptr, n = C.c_void_p(), C.c_size_t()
+    rc = lib().orc_ifs_write(C.byref(hdr), leaves.ctypes.data, len(leaves), C.byref(ptr),
+                             C.byref(n))
+    if rc:
+        raise ValueError(f"orc_ifs_write failed: {rc}")
+    data = C.string_at(ptr, n.value)
+    lib().orc_free(ptr)
+    return data
+
+
+def pgm_bytes(img: np.ndarray) -> bytes:
+    h, w = img.shape
+    return b"P5\n%d %d\n255\n" % (w, h) + np.ascontiguousarray(img, dtype=np.uint8).tobytes()
