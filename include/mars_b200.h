@@ -1,0 +1,174 @@
+/*
+ * mars_b200 -- B200 (sm_100a) domain-range block search and decode for the Mars fractal
+ * codec, behind a plain C ABI.
+ *
+ * This is the drop-in boundary a host encoder binds.  It replaces, entry point by entry
+ * point, the reference's (daleobrien/mars, Rust) search-provider boundary:
+ *
+ *   SearchProvider factory    crates/mars-codec/src/encode.rs:1054-1076
+ *     (make_search(&Contracted) -> Box<dyn SearchProvider>)   -> mars_search_table_build
+ *   SearchProvider::search    encode.rs:558-560, ExhaustiveSearch encode.rs:582-596
+ *                                                              -> mars_search_table_lookup
+ *   search_block              encode.rs:610-619 (the fixed-grid GPU differential of
+ *                             crates/mars-bench/src/gpu_search.rs:124-193) -> mars_search_blocks
+ *   encode_image_with_search  encode.rs:1054-1126 with build_rate_snapshot :1139-1169
+ *                                                              -> mars_encode
+ *   decode_iterative          crates/mars-codec/src/ifs.rs:281-309   -> mars_decode
+ *   ifs::parse / ifs::write   ifs.rs:186-217, 525-552           -> mars_ifs_parse / _write
+ *
+ * Conventions: every call returns MARS_OK (0) or a negative MARS_E* status; the text of the
+ * last error on the calling thread is available from mars_last_error().  There is no CPU
+ * fallback: without a usable CUDA device every compute call returns MARS_ENODEV.
+ * Host pointers are caller-owned; tables and leaf arrays returned by the library are freed
+ * with the matching *_free call.  Lookups on a built table are thread-safe.
+ */
+#ifndef MARS_B200_H
+#define MARS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    MARS_OK = 0,
+    MARS_EINVAL = -1,    /* bad argument or geometry */
+    MARS_ENODEV = -2,    /* no usable CUDA device */
+    MARS_ECUDA = -3,     /* a CUDA runtime call failed */
+    MARS_ENOMEM = -4,    /* host or device allocation failed */
+    MARS_ENOTFOUND = -5, /* lookup of a node the table does not hold */
+    MARS_ETIMEOUT = -6,  /* a bounded device wait expired */
+    MARS_EFORMAT = -7,   /* malformed bitstream */
+    MARS_EUNSUPPORTED = -8
+};
+
+/* EncodeParams, crates/mars-codec/src/encode.rs:27-52 (lambda: Option<f64>). */
+typedef struct mars_params {
+    uint32_t min_size, max_size, shift, bits_alfa, bits_beta, zero_threshold;
+    double max_alfa;
+    double t_rms;
+    int32_t has_lambda;
+    int32_t reserved;
+    double lambda;
+} mars_params;
+
+/* The EncodeOptions fields supported (encode.rs:78-109): allowed_modes (modes 0, 1 and 2;
+ * mode 3 is rejected with MARS_EUNSUPPORTED) and adaptive_density. */
+typedef struct mars_options {
+    uint8_t allowed_modes[4];
+    int32_t adaptive_density;
+} mars_options;
+
+/* RawMoments, encode.rs:225-232. */
+typedef struct mars_moments {
+    int64_t s0, s1_x4, s2_x16, t0, t1_x4, t2;
+} mars_moments;
+
+/* Candidate, encode.rs:236-244; valid = 0 stands for None (no legal domain). */
+typedef struct mars_candidate {
+    uint32_t dom_row, dom_col, isometry, qalfa, qbeta, valid;
+    double rms;
+    mars_moments moments;
+} mars_candidate;
+
+/* ifs::Leaf, crates/mars-codec/src/ifs.rs:101-117 (modes 0, 1, 2). */
+typedef struct mars_leaf {
+    uint32_t row, col, size, mode, qalfa, qbeta, isometry, dom_row, dom_col;
+    int32_t qgx, qgy;
+} mars_leaf;
+
+/* ifs::Header, ifs.rs:13-22. */
+typedef struct mars_header {
+    uint32_t bits_alfa, bits_beta, min_size, max_size, shift, width, height, int_max_alfa;
+} mars_header;
+
+/* EncodeCounters, encode.rs:1011-1021. */
+typedef struct mars_counters {
+    uint64_t search_evals, warmup_evals;
+} mars_counters;
+
+typedef struct mars_ctx mars_ctx;
+typedef struct mars_table mars_table;
+
+const char* mars_last_error(void);
+const char* mars_version(void);
+
+/* One context per device; a context owns a CUDA stream and cached device buffers.
+ * A context serialises its own calls: use one context per host thread for concurrency. */
+int mars_ctx_create(mars_ctx** out, int device);
+void mars_ctx_destroy(mars_ctx* ctx);
+/* Use `stream` (a cudaStream_t) for all of this context's work; NULL restores its own. */
+int mars_ctx_set_stream(mars_ctx* ctx, void* stream);
+/* Kernel launches made by this context since creation (instrumentation). */
+uint64_t mars_ctx_launch_count(const mars_ctx* ctx);
+
+/* The provider factory (encode.rs:1076): search every quadtree node an encode of this
+ * plane can request -- every aligned block of size min_size..max_size, plus the smaller
+ * border blocks reached through forced splits -- at `params->shift`, and also at
+ * 2*shift for the nodes adaptive density routes there when `adaptive_density` is set.
+ * `plane` is a host pointer to width*height bytes, row-major. */
+int mars_search_table_build(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
+                            const mars_params* params, int32_t adaptive_density,
+                            mars_table** out);
+/* SearchProvider::search for one node: the winning candidate (valid = 0 when the node has
+ * no legal domain) and the eval count the reference reports for it. */
+int mars_search_table_lookup(const mars_table* table, uint32_t row, uint32_t col, uint32_t size,
+                             uint32_t shift, mars_candidate* out, uint64_t* evals);
+/* Total evals the table's searches stand for (all nodes, all shifts, counted as the
+ * reference counts them: domain positions x 8 per node). */
+uint64_t mars_search_table_evals(const mars_table* table);
+/* How many of those candidates survived the exact-bound filter and took the exact f64 fit
+ * (instrumentation). */
+uint64_t mars_search_table_exact_fits(const mars_table* table);
+void mars_search_table_free(mars_table* table);
+
+/* search_block over an explicit list of block origins at one size and shift (host
+ * buffers).  out[i] / evals[i] belong to (rows[i], cols[i]). */
+int mars_search_blocks(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
+                       uint32_t size, uint32_t shift, const mars_params* params,
+                       const uint32_t* rows, const uint32_t* cols, size_t n,
+                       mars_candidate* out, uint64_t* evals);
+
+/* Device-resident form for callers that keep the plane in HBM: `d_plane` is a device
+ * pointer; results stay on the device in `d_out` (n candidates).  Asynchronous on the
+ * context's stream. */
+int mars_search_blocks_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t width,
+                              uint32_t height, uint32_t size, uint32_t shift,
+                              const mars_params* params, const uint32_t* d_rows,
+                              const uint32_t* d_cols, size_t n, mars_candidate* d_out);
+
+/* The searches of mars_search_table_build (every node an encode can request, at
+ * params->shift) with the plane already in device memory and the results left on the
+ * device, in the node order the table uses.  *n_nodes receives the node count and
+ * *total_evals the reference eval count; call with d_out = NULL to query only.
+ * Asynchronous on the context's stream. */
+int mars_search_nodes_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t width,
+                             uint32_t height, const mars_params* params, mars_candidate* d_out,
+                             size_t capacity, size_t* n_nodes, uint64_t* total_evals);
+
+/* encode_image_with_search with this library as the provider: the threshold walk when
+ * params->has_lambda == 0, else the exhaustive t_rms = 8 warm-up (served from the same
+ * table) followed by the bottom-up RD walk.  *leaves is freed with mars_leaves_free. */
+int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
+                const mars_params* params, const mars_options* options, mars_header* header,
+                mars_leaf** leaves, size_t* nleaves, mars_counters* counters);
+void mars_leaves_free(mars_leaf* leaves);
+
+/* decode_iterative: `iterations` fixed-point steps from the flat-128 seed (modes 0/1/2).
+ * `out` is a host buffer of width*height bytes. */
+int mars_decode(mars_ctx* ctx, const mars_header* header, const mars_leaf* leaves, size_t n,
+                uint32_t iterations, uint8_t* out);
+
+/* .ifs bitstream.  Buffers returned here are freed with mars_bytes_free / mars_leaves_free. */
+int mars_ifs_parse(const uint8_t* data, size_t len, mars_header* header, mars_leaf** leaves,
+                   size_t* nleaves);
+int mars_ifs_write(const mars_header* header, const mars_leaf* leaves, size_t n, uint8_t** out,
+                   size_t* len);
+void mars_bytes_free(uint8_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MARS_B200_H */

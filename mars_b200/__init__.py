@@ -1,0 +1,305 @@
+"""mars_b200: the Mars fractal codec's domain-range block search and decode on B200.
+
+Python mirror of the reference's search-provider boundary (daleobrien/mars,
+crates/mars-codec/src/encode.rs:530-602): `Context.search_provider(plane, params)` plays
+the provider factory `make_search(&Contracted)`, and the returned `GpuSearch.search()` is
+`SearchProvider::search` -- same request (row, col, size, shift), same outcome (winning
+candidate or None, evals).  Everything runs through libmars_b200.so (include/mars_b200.h);
+there is no CPU path: without a CUDA device the calls raise `MarsError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import build as _build
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+MARS_OK = 0
+ERRORS = {-1: "EINVAL", -2: "ENODEV", -3: "ECUDA", -4: "ENOMEM", -5: "ENOTFOUND",
+          -6: "ETIMEOUT", -7: "EFORMAT", -8: "EUNSUPPORTED"}
+
+
+class MarsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    """EncodeParams (encode.rs:27-52)."""
+    _fields_ = [
+        ("min_size", C.c_uint32), ("max_size", C.c_uint32), ("shift", C.c_uint32),
+        ("bits_alfa", C.c_uint32), ("bits_beta", C.c_uint32), ("zero_threshold", C.c_uint32),
+        ("max_alfa", C.c_double), ("t_rms", C.c_double), ("has_lambda", C.c_int32),
+        ("reserved", C.c_int32), ("lambda_", C.c_double),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [("allowed_modes", C.c_uint8 * 4), ("adaptive_density", C.c_int32)]
+
+
+class Header(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in (
+        "bits_alfa", "bits_beta", "min_size", "max_size", "shift", "width", "height",
+        "int_max_alfa")]
+
+
+class Counters(C.Structure):
+    _fields_ = [("search_evals", C.c_uint64), ("warmup_evals", C.c_uint64)]
+
+
+CANDIDATE_DTYPE = np.dtype([
+    ("dom_row", "<u4"), ("dom_col", "<u4"), ("isometry", "<u4"), ("qalfa", "<u4"),
+    ("qbeta", "<u4"), ("valid", "<u4"), ("rms", "<f8"), ("s0", "<i8"), ("s1_x4", "<i8"),
+    ("s2_x16", "<i8"), ("t0", "<i8"), ("t1_x4", "<i8"), ("t2", "<i8")])
+LEAF_DTYPE = np.dtype([(n, "<u4") for n in (
+    "row", "col", "size", "mode", "qalfa", "qbeta", "isometry", "dom_row", "dom_col")] + [
+    ("qgx", "<i4"), ("qgy", "<i4")])
+
+# Every symbol include/mars_b200.h declares (tests check the library exports them all).
+EXPORTS = (
+    "mars_last_error", "mars_version", "mars_ctx_create", "mars_ctx_destroy",
+    "mars_ctx_set_stream", "mars_ctx_launch_count", "mars_search_table_build",
+    "mars_search_table_lookup", "mars_search_table_evals", "mars_search_table_exact_fits",
+    "mars_search_table_free", "mars_search_blocks", "mars_search_blocks_device",
+    "mars_search_nodes_device", "mars_encode", "mars_leaves_free", "mars_decode",
+    "mars_ifs_parse", "mars_ifs_write", "mars_bytes_free",
+)
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def lib():
+    """Load libmars_b200.so (building it first if the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_build.LIB) or _build.stale():
+        _build.build()
+    L = C.CDLL(_build.LIB)
+    P, vp, u32, u64, sz = C.POINTER, C.c_void_p, C.c_uint32, C.c_uint64, C.c_size_t
+    L.mars_last_error.restype = C.c_char_p
+    L.mars_version.restype = C.c_char_p
+    L.mars_ctx_create.argtypes = [P(vp), C.c_int]
+    L.mars_ctx_destroy.argtypes = [vp]
+    L.mars_ctx_destroy.restype = None
+    L.mars_ctx_set_stream.argtypes = [vp, vp]
+    L.mars_ctx_launch_count.argtypes = [vp]
+    L.mars_ctx_launch_count.restype = u64
+    L.mars_search_table_build.argtypes = [vp, vp, u32, u32, P(Params), C.c_int32, P(vp)]
+    L.mars_search_table_lookup.argtypes = [vp, u32, u32, u32, u32, vp, P(u64)]
+    L.mars_search_table_evals.argtypes = [vp]
+    L.mars_search_table_evals.restype = u64
+    L.mars_search_table_exact_fits.argtypes = [vp]
+    L.mars_search_table_exact_fits.restype = u64
+    L.mars_search_table_free.argtypes = [vp]
+    L.mars_search_table_free.restype = None
+    L.mars_search_blocks.argtypes = [vp, vp, u32, u32, u32, u32, P(Params), vp, vp, sz, vp, vp]
+    L.mars_search_blocks_device.argtypes = [vp, vp, u32, u32, u32, u32, P(Params), vp, vp, sz, vp]
+    L.mars_search_nodes_device.argtypes = [vp, vp, u32, u32, P(Params), vp, sz, P(sz), P(u64)]
+    L.mars_encode.argtypes = [vp, vp, u32, u32, P(Params), P(Options), P(Header), P(vp), P(sz),
+                              P(Counters)]
+    L.mars_leaves_free.argtypes = [vp]
+    L.mars_leaves_free.restype = None
+    L.mars_decode.argtypes = [vp, P(Header), vp, sz, u32, vp]
+    L.mars_ifs_parse.argtypes = [vp, sz, P(Header), P(vp), P(sz)]
+    L.mars_ifs_write.argtypes = [P(Header), vp, sz, P(vp), P(sz)]
+    L.mars_bytes_free.argtypes = [vp]
+    L.mars_bytes_free.restype = None
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != MARS_OK:
+        raise MarsError(rc, (lib().mars_last_error() or b"").decode())
+
+
+def make_params(min_size=4, max_size=16, shift=4, bits_alfa=4, bits_beta=7, max_alfa=1.0,
+                t_rms=8.0, zero_threshold=0, lam: Optional[float] = None) -> Params:
+    """EncodeParams with the encmars defaults (crates/mars-cli/src/bin/encmars.rs:185-205)."""
+    return Params(min_size, max_size, shift, bits_alfa, bits_beta, zero_threshold, max_alfa,
+                  t_rms, 0 if lam is None else 1, 0, 0.0 if lam is None else float(lam))
+
+
+def _plane(img) -> np.ndarray:
+    a = np.ascontiguousarray(img, dtype=np.uint8)
+    if a.ndim != 2:
+        raise ValueError("a plane is a 2-D uint8 array")
+    return a
+
+
+@dataclass
+class Candidate:
+    """Candidate (encode.rs:236-244)."""
+    dom_row: int
+    dom_col: int
+    isometry: int
+    qalfa: int
+    qbeta: int
+    rms: float
+    moments: tuple
+
+
+@dataclass
+class SearchOutcome:
+    """SearchOutcome (encode.rs:543-546)."""
+    candidate: Optional[Candidate]
+    evals: int
+
+
+class GpuSearch:
+    """SearchProvider over a table the GPU filled for every node of one plane."""
+
+    def __init__(self, ctx: "Context", handle: int, width: int, height: int):
+        self._ctx = ctx
+        self._h = C.c_void_p(handle)
+        self.width, self.height = width, height
+
+    def search(self, row: int, col: int, size: int, shift: int) -> SearchOutcome:
+        out = np.zeros(1, dtype=CANDIDATE_DTYPE)
+        ev = C.c_uint64()
+        check(lib().mars_search_table_lookup(self._h, row, col, size, shift, out.ctypes.data,
+                                             C.byref(ev)))
+        c = out[0]
+        if not c["valid"]:
+            return SearchOutcome(None, ev.value)
+        return SearchOutcome(Candidate(int(c["dom_row"]), int(c["dom_col"]), int(c["isometry"]),
+                                       int(c["qalfa"]), int(c["qbeta"]), float(c["rms"]),
+                                       tuple(int(c[k]) for k in ("s0", "s1_x4", "s2_x16", "t0",
+                                                                 "t1_x4", "t2"))), ev.value)
+
+    @property
+    def evals(self) -> int:
+        return lib().mars_search_table_evals(self._h)
+
+    @property
+    def exact_fits(self) -> int:
+        return lib().mars_search_table_exact_fits(self._h)
+
+    def close(self) -> None:
+        if self._h:
+            lib().mars_search_table_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """One device context (a CUDA stream plus cached device memory)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().mars_ctx_create(C.byref(h), device))
+        self._h = h
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def close(self) -> None:
+        if self._h:
+            lib().mars_ctx_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int) -> None:
+        check(lib().mars_ctx_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    @property
+    def launches(self) -> int:
+        return lib().mars_ctx_launch_count(self._h)
+
+    def search_provider(self, img, params: Params, adaptive_density: bool = False) -> GpuSearch:
+        a = _plane(img)
+        h, w = a.shape
+        t = C.c_void_p()
+        check(lib().mars_search_table_build(self._h, a.ctypes.data, w, h, C.byref(params),
+                                            int(adaptive_density), C.byref(t)))
+        return GpuSearch(self, t.value, w, h)
+
+    def search_blocks(self, img, size: int, shift: int, params: Params, rows, cols):
+        """search_block for each (rows[i], cols[i]): (candidates, evals) arrays."""
+        a = _plane(img)
+        h, w = a.shape
+        rows = np.ascontiguousarray(rows, dtype=np.uint32)
+        cols = np.ascontiguousarray(cols, dtype=np.uint32)
+        out = np.zeros(len(rows), dtype=CANDIDATE_DTYPE)
+        ev = np.zeros(len(rows), dtype=np.uint64)
+        check(lib().mars_search_blocks(self._h, a.ctypes.data, w, h, size, shift, C.byref(params),
+                                       rows.ctypes.data, cols.ctypes.data, len(rows),
+                                       out.ctypes.data, ev.ctypes.data))
+        return out, ev
+
+    def search_grid(self, img, size: int, shift: int, params: Params):
+        a = _plane(img)
+        h, w = a.shape
+        rr, cc = np.meshgrid(np.arange(h // size) * size, np.arange(w // size) * size, indexing="ij")
+        return self.search_blocks(a, size, shift, params, rr.ravel(), cc.ravel())
+
+    def encode(self, img, params: Params, allowed_modes=(1, 0, 1, 0), adaptive_density=False):
+        """encode_image_with_search with the GPU provider: (header, leaves, counters)."""
+        a = _plane(img)
+        h, w = a.shape
+        opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density))
+        hdr, cnt = Header(), Counters()
+        ptr, n = C.c_void_p(), C.c_size_t()
+        check(lib().mars_encode(self._h, a.ctypes.data, w, h, C.byref(params), C.byref(opts),
+                                C.byref(hdr), C.byref(ptr), C.byref(n), C.byref(cnt)))
+        leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize),
+                               dtype=LEAF_DTYPE).copy()
+        lib().mars_leaves_free(ptr)
+        return hdr, leaves, cnt
+
+    def decode(self, hdr: Header, leaves: np.ndarray, iterations: int = 10) -> np.ndarray:
+        leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+        out = np.zeros((hdr.height, hdr.width), dtype=np.uint8)
+        check(lib().mars_decode(self._h, C.byref(hdr), leaves.ctypes.data, len(leaves),
+                                iterations, out.ctypes.data))
+        return out
+
+
+def ifs_parse(data: bytes):
+    buf = np.frombuffer(data, dtype=np.uint8)
+    hdr = Header()
+    ptr, n = C.c_void_p(), C.c_size_t()
+    check(lib().mars_ifs_parse(buf.ctypes.data, len(data), C.byref(hdr), C.byref(ptr), C.byref(n)))
+    leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize), dtype=LEAF_DTYPE).copy()
+    lib().mars_leaves_free(ptr)
+    return hdr, leaves
+
+
+def ifs_write(hdr: Header, leaves: np.ndarray) -> bytes:
+    leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    ptr, n = C.c_void_p(), C.c_size_t()
+    check(lib().mars_ifs_write(C.byref(hdr), leaves.ctypes.data, len(leaves), C.byref(ptr),
+                               C.byref(n)))
+    data = C.string_at(ptr, n.value)
+    lib().mars_bytes_free(ptr)
+    return data

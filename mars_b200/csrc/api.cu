@@ -1,0 +1,652 @@
+// The C ABI of include/mars_b200.h: contexts, the per-plane search table (the provider
+// factory of crates/mars-codec/src/encode.rs:1054-1076), fixed-grid block search, the
+// encode driver and the decode iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/mars_b200.h"
+#include "codec.hpp"
+#include "kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define MARS_CUDA(call)                                                                   \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(MARS_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
+
+}  // namespace
+
+struct mars_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::atomic<uint64_t> launches{0};
+    std::mutex mu;
+    unsigned long long* d_counter = nullptr;  // survivors that took the exact f64 fit
+};
+
+struct mars_table {
+    uint32_t width = 0, height = 0;
+    std::unordered_map<uint64_t, uint32_t> index;
+    std::vector<mars_candidate> cands;
+    std::vector<uint64_t> evals;
+    uint64_t total_evals = 0;
+    uint64_t exact_fits = 0;
+};
+
+namespace {
+
+static_assert(sizeof(mars_candidate) == sizeof(mars::CandidateOut), "candidate layout");
+
+uint64_t node_key(uint32_t row, uint32_t col, uint32_t size, uint32_t shift) {
+    return (uint64_t)row | ((uint64_t)col << 16) | ((uint64_t)size << 32) |
+           ((uint64_t)shift << 48);
+}
+
+// Device waits are bounded: poll an event until it completes or the deadline passes.
+int sync_bounded(mars_ctx* ctx) {
+    static const double limit_s = [] {
+        const char* e = std::getenv("MARS_SYNC_TIMEOUT_S");
+        return e ? std::atof(e) : 300.0;
+    }();
+    cudaEvent_t ev;
+    MARS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    MARS_CUDA(cudaEventRecord(ev, ctx->stream));
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(ev);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) {
+            cudaEventDestroy(ev);
+            return fail(MARS_ECUDA, std::string("device error: ") + cudaGetErrorString(q));
+        }
+        const double el =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > limit_s) {
+            cudaEventDestroy(ev);
+            return fail(MARS_ETIMEOUT, "device work did not finish within MARS_SYNC_TIMEOUT_S");
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 20 : 500));
+    }
+    cudaEventDestroy(ev);
+    return MARS_OK;
+}
+
+int check_params(const mars_params* p) {
+    if (!p) return fail(MARS_EINVAL, "params is NULL");
+    if (p->bits_alfa < 1 || p->bits_alfa > 16 || p->bits_beta < 1 || p->bits_beta > 16)
+        return fail(MARS_EINVAL, "bits_alfa/bits_beta must be in 1..16");
+    if (!(p->max_alfa > 0.0) || !std::isfinite(p->max_alfa))
+        return fail(MARS_EINVAL, "max_alfa must be finite and positive");
+    if (p->shift == 0 || (p->shift & 1))
+        return fail(MARS_EUNSUPPORTED, "the domain stride must be even (the reference CLI "
+                                       "enforces an even shift in 2..=254)");
+    if (!is_pow2(p->min_size) || !is_pow2(p->max_size) || p->min_size > p->max_size)
+        return fail(MARS_EINVAL, "min_size/max_size must be powers of two, min <= max");
+    if (p->max_size > 64)
+        return fail(MARS_EUNSUPPORTED, "block sizes above 64 are not supported on the GPU path");
+    if (p->has_lambda && !(std::isfinite(p->lambda) && p->lambda >= 0.0))
+        return fail(MARS_EINVAL, "lambda must be finite and nonnegative");
+    return MARS_OK;
+}
+
+mars::FitParams make_fit_params(const mars_params& p) {
+    mars::FitParams fp;
+    fp.max_alfa = p.max_alfa;
+    fp.bits_alfa = p.bits_alfa;
+    fp.bits_beta = p.bits_beta;
+    const double a = p.max_alfa / (double)(1u << p.bits_alfa);  // exact (power-of-two scale)
+    float af = (float)a;
+    if ((double)af > a) af = std::nextafter(af, 0.0f);
+    fp.a_min = af;
+    fp.two_a = 2.0f * af;
+    fp.a_half = 0.5f * af;
+    fp.eta_per_n = 1e-6 * (1.0 + p.max_alfa) * (1.0 + p.max_alfa);
+    return fp;
+}
+
+mars::LevelGeom level_geom(uint32_t w, uint32_t h, uint32_t size, uint32_t shift) {
+    mars::LevelGeom g;
+    g.size = (int)size;
+    g.shift = (int)shift;
+    g.step_c = (int)(shift / 2);
+    g.dw = (int)(w / 2);
+    g.dh = (int)(h / 2);
+    g.w = (int)w;
+    g.h = (int)h;
+    g.nrow_d = h >= 2 * size ? (int)((h - 2 * size) / shift + 1) : 0;
+    g.ncol_d = w >= 2 * size ? (int)((w - 2 * size) / shift + 1) : 0;
+    return g;
+}
+
+// Grow-nothing scratch: every buffer is taken from the stream-ordered pool and returned
+// to it at the end of the call (the pool keeps the memory cached between calls).
+struct Scratch {
+    cudaStream_t st;
+    std::vector<void*> ptrs;
+    explicit Scratch(cudaStream_t s) : st(s) {}
+    template <class T>
+    cudaError_t get(T** p, size_t count) {
+        void* v = nullptr;
+        const cudaError_t e = cudaMallocAsync(&v, std::max<size_t>(count, 1) * sizeof(T), st);
+        if (e == cudaSuccess) ptrs.push_back(v);
+        *p = (T*)v;
+        return e;
+    }
+    ~Scratch() {
+        for (void* v : ptrs) cudaFreeAsync(v, st);
+    }
+};
+
+// Search every block of one (size, shift) level.  rows/cols/out are device pointers.
+int run_level(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t* d_D,
+              uint32_t w, uint32_t h, uint32_t size, uint32_t shift, const mars::FitParams& fp,
+              const uint32_t* d_rows, const uint32_t* d_cols, size_t n,
+              mars::CandidateOut* d_out) {
+    if (n == 0) return MARS_OK;
+    const cudaStream_t st = ctx->stream;
+    const mars::LevelGeom g = level_geom(w, h, size, shift);
+    if (g.nrow_d <= 0 || g.ncol_d <= 0) {
+        // No legal domain: every candidate is None (encode.rs:734-739).
+        MARS_CUDA(cudaMemsetAsync(d_out, 0, n * sizeof(mars::CandidateOut), st));
+        return MARS_OK;
+    }
+    const size_t ndom = (size_t)g.nrow_d * g.ncol_d;
+    mars::RangeStats rs;
+    mars::DomainStats ds;
+    MARS_CUDA(sc.get(&rs.t0, n));
+    MARS_CUDA(sc.get(&rs.t2, n));
+    MARS_CUDA(sc.get(&rs.nrr, n));
+    MARS_CUDA(sc.get(&rs.sum0, n));
+    MARS_CUDA(sc.get(&rs.rms0, n));
+    MARS_CUDA(sc.get(&ds.s1x4, ndom));
+    MARS_CUDA(sc.get(&ds.s2x16, ndom));
+    MARS_CUDA(sc.get(&ds.detf, ndom));
+    MARS_CUDA(sc.get(&ds.sdetf, ndom));
+    const int nsplit = mars::search_simt_splits(g, (int)n, ctx->num_sms);
+    mars::Partial* partials;
+    MARS_CUDA(sc.get(&partials, (size_t)nsplit * n));
+    MARS_CUDA(mars::launch_range_stats(d_plane, (int)w, (int)h, d_rows, d_cols, (int)n,
+                                       (int)size, fp, rs, st));
+    MARS_CUDA(mars::launch_domain_stats(d_D, g, ds, st));
+    MARS_CUDA(mars::launch_search_simt(d_D, d_plane, (int)w, d_rows, d_cols, (int)n, g, rs, ds,
+                                       fp, partials, nsplit, ctx->d_counter, st));
+    MARS_CUDA(mars::launch_reduce(partials, nsplit, (int)n, g, rs, ds, d_out, st));
+    ctx->launches += 4;
+    return MARS_OK;
+}
+
+// Quadtree nodes an encode can request a search for (walk / walk_rd, encode.rs:1330-1468,
+// 1865-2071): every non-forced node of size >= 2, and the children of non-forced nodes
+// above min_size; forced nodes split unconditionally.
+void enumerate_nodes(uint32_t w, uint32_t h, uint32_t min_size, uint32_t max_size,
+                     uint32_t row, uint32_t col, uint32_t size,
+                     std::vector<std::vector<std::pair<uint32_t, uint32_t>>>& by_log2) {
+    if (row >= h || col >= w || size == 0) return;
+    const bool forced = size > max_size || row + size > h || col + size > w;
+    const uint32_t half = size / 2;
+    if (!forced) {
+        if (size >= 2) by_log2[__builtin_ctz(size)].push_back({row, col});
+        if (size <= min_size) return;
+    }
+    if (half == 0) return;
+    enumerate_nodes(w, h, min_size, max_size, row, col, half, by_log2);
+    enumerate_nodes(w, h, min_size, max_size, row + half, col, half, by_log2);
+    enumerate_nodes(w, h, min_size, max_size, row, col + half, half, by_log2);
+    enumerate_nodes(w, h, min_size, max_size, row + half, col + half, half, by_log2);
+}
+
+struct Job {
+    uint32_t size, shift;
+    std::vector<uint32_t> rows, cols;
+};
+
+std::vector<Job> plan_jobs(const uint8_t* plane, uint32_t w, uint32_t h, const mars_params& p,
+                           bool adaptive) {
+    mars_header hdr = mars::codec::build_header(w, h, p);
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> by_log2(32);
+    enumerate_nodes(w, h, p.min_size, p.max_size, 0, 0, mars::codec::virtual_size(hdr), by_log2);
+    std::vector<Job> jobs;
+    for (uint32_t lg = 1; lg < 32; ++lg) {
+        if (by_log2[lg].empty()) continue;
+        Job base{1u << lg, p.shift, {}, {}};
+        Job dense{1u << lg, std::min<uint32_t>(p.shift * 2, 0xffffu), {}, {}};
+        for (const auto& rc : by_log2[lg]) {
+            base.rows.push_back(rc.first);
+            base.cols.push_back(rc.second);
+            if (adaptive) {
+                const mars::codec::Image im{plane, w, h};
+                const double rms = mars::codec::block_rms(im, rc.first, rc.second, 1u << lg);
+                if (mars::codec::adaptive_shift(p.shift, rms) != p.shift) {
+                    dense.rows.push_back(rc.first);
+                    dense.cols.push_back(rc.second);
+                }
+            }
+        }
+        jobs.push_back(std::move(base));
+        if (!dense.rows.empty()) jobs.push_back(std::move(dense));
+    }
+    return jobs;
+}
+
+uint64_t level_evals(uint32_t w, uint32_t h, uint32_t size, uint32_t shift) {
+    const mars::LevelGeom g = level_geom(w, h, size, shift);
+    if (g.nrow_d <= 0 || g.ncol_d <= 0) return 0;
+    return (uint64_t)g.nrow_d * (uint64_t)g.ncol_d * 8ull;
+}
+
+// Runs all jobs on the device plane; results land in d_out (concatenated in job order).
+int run_jobs(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uint32_t h,
+             const mars::FitParams& fp, const std::vector<Job>& jobs, mars::CandidateOut* d_out) {
+    const cudaStream_t st = ctx->stream;
+    int32_t* d_D = nullptr;
+    MARS_CUDA(sc.get(&d_D, (size_t)(w / 2) * (h / 2)));
+    MARS_CUDA(mars::launch_contract(d_plane, (int)w, (int)h, d_D, st));
+    ctx->launches += 1;
+    size_t total = 0;
+    for (const Job& j : jobs) total += j.rows.size();
+    std::vector<uint32_t> rc(2 * total);
+    size_t off = 0;
+    for (const Job& j : jobs) {
+        std::copy(j.rows.begin(), j.rows.end(), rc.begin() + (long)off);
+        std::copy(j.cols.begin(), j.cols.end(), rc.begin() + (long)(total + off));
+        off += j.rows.size();
+    }
+    uint32_t* d_rc = nullptr;
+    MARS_CUDA(sc.get(&d_rc, rc.size()));
+    MARS_CUDA(cudaMemcpyAsync(d_rc, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice, st));
+    off = 0;
+    for (const Job& j : jobs) {
+        const int e = run_level(ctx, sc, d_plane, d_D, w, h, j.size, j.shift, fp, d_rc + off,
+                                d_rc + total + off, j.rows.size(), d_out + off);
+        if (e) return e;
+        off += j.rows.size();
+    }
+    return MARS_OK;
+}
+
+int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, uint32_t w,
+                uint32_t h, const mars_params* params, bool adaptive, mars_table** out) {
+    if (!ctx || !out) return fail(MARS_EINVAL, "NULL argument");
+    if (int e = check_params(params)) return e;
+    if (w == 0 || h == 0 || w > 65535 || h > 65535)
+        return fail(MARS_EINVAL, "plane dimensions must be in 1..65535");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    const mars::FitParams fp = make_fit_params(*params);
+    std::vector<uint8_t> host_plane;
+    if (!plane && adaptive) {
+        host_plane.resize((size_t)w * h);
+        MARS_CUDA(cudaMemcpy(host_plane.data(), d_plane_in, host_plane.size(),
+                             cudaMemcpyDeviceToHost));
+        plane = host_plane.data();
+    }
+    const std::vector<Job> jobs = plan_jobs(plane, w, h, *params, adaptive);
+    size_t total = 0;
+    for (const Job& j : jobs) total += j.rows.size();
+    if (total > 0xffffffffull) return fail(MARS_EINVAL, "too many quadtree nodes");
+    auto* t = new (std::nothrow) mars_table;
+    if (!t) return fail(MARS_ENOMEM, "table allocation failed");
+    std::unique_ptr<mars_table> guard(t);
+    t->width = w;
+    t->height = h;
+    t->cands.resize(total);
+    t->evals.resize(total);
+    {
+        Scratch sc(ctx->stream);
+        const uint8_t* d_plane = d_plane_in;
+        if (!d_plane) {
+            uint8_t* dp = nullptr;
+            MARS_CUDA(sc.get(&dp, (size_t)w * h));
+            MARS_CUDA(cudaMemcpyAsync(dp, plane, (size_t)w * h, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+            d_plane = dp;
+        }
+        mars::CandidateOut* d_out = nullptr;
+        MARS_CUDA(sc.get(&d_out, total));
+        MARS_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), ctx->stream));
+        if (int e = run_jobs(ctx, sc, d_plane, w, h, fp, jobs, d_out)) return e;
+        MARS_CUDA(cudaMemcpyAsync(t->cands.data(), d_out, total * sizeof(mars_candidate),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+        unsigned long long exact = 0;
+        MARS_CUDA(cudaMemcpyAsync(&exact, ctx->d_counter, sizeof exact, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+        if (int e = sync_bounded(ctx)) return e;
+        t->exact_fits = exact;
+    }
+    size_t off = 0;
+    t->index.reserve(total * 2);
+    for (const Job& j : jobs) {
+        const uint64_t ev = level_evals(w, h, j.size, j.shift);
+        for (size_t i = 0; i < j.rows.size(); ++i) {
+            t->index[node_key(j.rows[i], j.cols[i], j.size, j.shift)] = (uint32_t)(off + i);
+            t->evals[off + i] = ev;
+            t->total_evals += ev;
+        }
+        off += j.rows.size();
+    }
+    *out = guard.release();
+    return MARS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mars_last_error(void) { return g_err.c_str(); }
+const char* mars_version(void) { return "mars_b200 0.1 (sm_100a)"; }
+
+int mars_ctx_create(mars_ctx** out, int device) {
+    if (!out) return fail(MARS_EINVAL, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+        return fail(MARS_ENODEV, "no CUDA device is available");
+    if (device < 0 || device >= n) return fail(MARS_EINVAL, "device index out of range");
+    cudaDeviceProp prop;
+    MARS_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+        return fail(MARS_ENODEV, "mars_b200 is built for sm_100a (B200); this device is sm_" +
+                                     std::to_string(prop.major) + std::to_string(prop.minor));
+    auto* c = new (std::nothrow) mars_ctx;
+    if (!c) return fail(MARS_ENOMEM, "context allocation failed");
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_counter, sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    if (e != cudaSuccess) {
+        if (c->own_stream) cudaStreamDestroy(c->own_stream);
+        delete c;
+        return fail(MARS_ECUDA, std::string("context setup: ") + cudaGetErrorString(e));
+    }
+    c->stream = c->own_stream;
+    *out = c;
+    return MARS_OK;
+}
+
+void mars_ctx_destroy(mars_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->d_counter) cudaFree(ctx->d_counter);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+}
+
+int mars_ctx_set_stream(mars_ctx* ctx, void* stream) {
+    if (!ctx) return fail(MARS_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return MARS_OK;
+}
+
+uint64_t mars_ctx_launch_count(const mars_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
+
+int mars_search_table_build(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
+                            const mars_params* params, int32_t adaptive_density,
+                            mars_table** out) {
+    if (!plane) return fail(MARS_EINVAL, "plane is NULL");
+    return build_table(ctx, plane, nullptr, width, height, params, adaptive_density != 0, out);
+}
+
+int mars_search_table_lookup(const mars_table* t, uint32_t row, uint32_t col, uint32_t size,
+                             uint32_t shift, mars_candidate* out, uint64_t* evals) {
+    if (!t || !out) return fail(MARS_EINVAL, "NULL argument");
+    auto it = t->index.find(node_key(row, col, size, shift));
+    if (it == t->index.end())
+        return fail(MARS_ENOTFOUND, "node (" + std::to_string(row) + "," + std::to_string(col) +
+                                        "," + std::to_string(size) + ") at shift " +
+                                        std::to_string(shift) + " is not in the table");
+    *out = t->cands[it->second];
+    if (evals) *evals = t->evals[it->second];
+    return MARS_OK;
+}
+
+uint64_t mars_search_table_evals(const mars_table* t) { return t ? t->total_evals : 0; }
+uint64_t mars_search_table_exact_fits(const mars_table* t) { return t ? t->exact_fits : 0; }
+
+void mars_search_table_free(mars_table* t) { delete t; }
+
+int mars_search_blocks(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
+                       uint32_t size, uint32_t shift, const mars_params* params,
+                       const uint32_t* rows, const uint32_t* cols, size_t n,
+                       mars_candidate* out, uint64_t* evals) {
+    if (!ctx || !plane || (n && (!rows || !cols || !out))) return fail(MARS_EINVAL, "NULL argument");
+    if (int e = check_params(params)) return e;
+    if (!is_pow2(size) || size < 2 || size > 64)
+        return fail(size > 64 ? MARS_EUNSUPPORTED : MARS_EINVAL, "size must be a power of two in 2..64");
+    if (shift == 0 || (shift & 1)) return fail(MARS_EUNSUPPORTED, "shift must be even");
+    for (size_t i = 0; i < n; ++i)
+        if (rows[i] + size > height || cols[i] + size > width)
+            return fail(MARS_EINVAL, "block " + std::to_string(i) + " runs past the plane");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    const mars::FitParams fp = make_fit_params(*params);
+    Job job{size, shift, std::vector<uint32_t>(rows, rows + n), std::vector<uint32_t>(cols, cols + n)};
+    {
+        Scratch sc(ctx->stream);
+        uint8_t* dp = nullptr;
+        mars::CandidateOut* d_out = nullptr;
+        MARS_CUDA(sc.get(&dp, (size_t)width * height));
+        MARS_CUDA(sc.get(&d_out, n));
+        MARS_CUDA(cudaMemcpyAsync(dp, plane, (size_t)width * height, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+        if (int e = run_jobs(ctx, sc, dp, width, height, fp, {job}, d_out)) return e;
+        MARS_CUDA(cudaMemcpyAsync(out, d_out, n * sizeof(mars_candidate), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+        if (int e = sync_bounded(ctx)) return e;
+    }
+    const uint64_t ev = level_evals(width, height, size, shift);
+    if (evals)
+        for (size_t i = 0; i < n; ++i) evals[i] = ev;
+    return MARS_OK;
+}
+
+int mars_search_blocks_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t width,
+                              uint32_t height, uint32_t size, uint32_t shift,
+                              const mars_params* params, const uint32_t* d_rows,
+                              const uint32_t* d_cols, size_t n, mars_candidate* d_out) {
+    if (!ctx || !d_plane || (n && (!d_rows || !d_cols || !d_out)))
+        return fail(MARS_EINVAL, "NULL argument");
+    if (int e = check_params(params)) return e;
+    if (!is_pow2(size) || size < 2 || size > 64)
+        return fail(size > 64 ? MARS_EUNSUPPORTED : MARS_EINVAL, "size must be a power of two in 2..64");
+    if (shift == 0 || (shift & 1)) return fail(MARS_EUNSUPPORTED, "shift must be even");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    const mars::FitParams fp = make_fit_params(*params);
+    Scratch sc(ctx->stream);
+    int32_t* d_D = nullptr;
+    MARS_CUDA(sc.get(&d_D, (size_t)(width / 2) * (height / 2)));
+    MARS_CUDA(mars::launch_contract(d_plane, (int)width, (int)height, d_D, ctx->stream));
+    ctx->launches += 1;
+    return run_level(ctx, sc, d_plane, d_D, width, height, size, shift, fp, d_rows, d_cols, n,
+                     (mars::CandidateOut*)d_out);
+}
+
+int mars_search_nodes_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t width,
+                             uint32_t height, const mars_params* params, mars_candidate* d_out,
+                             size_t capacity, size_t* n_nodes, uint64_t* total_evals) {
+    if (!ctx || !d_plane || !n_nodes) return fail(MARS_EINVAL, "NULL argument");
+    if (int e = check_params(params)) return e;
+    if (width == 0 || height == 0 || width > 65535 || height > 65535)
+        return fail(MARS_EINVAL, "plane dimensions must be in 1..65535");
+    const std::vector<Job> jobs = plan_jobs(nullptr, width, height, *params, false);
+    size_t total = 0;
+    uint64_t ev = 0;
+    for (const Job& j : jobs) {
+        total += j.rows.size();
+        ev += level_evals(width, height, j.size, j.shift) * j.rows.size();
+    }
+    *n_nodes = total;
+    if (total_evals) *total_evals = ev;
+    if (!d_out) return MARS_OK;
+    if (capacity < total) return fail(MARS_EINVAL, "d_out holds fewer entries than nodes");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    Scratch sc(ctx->stream);
+    return run_jobs(ctx, sc, d_plane, width, height, make_fit_params(*params), jobs,
+                    (mars::CandidateOut*)d_out);
+}
+
+int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
+                const mars_params* params, const mars_options* options, mars_header* header,
+                mars_leaf** leaves, size_t* nleaves, mars_counters* counters) {
+    if (!ctx || !plane || !options || !header || !leaves || !nleaves || !counters)
+        return fail(MARS_EINVAL, "NULL argument");
+    if (int e = check_params(params)) return e;
+    if (options->allowed_modes[3])
+        return fail(MARS_EUNSUPPORTED, "mode 3 (DCT residual) is not supported");
+    mars_table* table = nullptr;
+    const bool adaptive = params->has_lambda && options->adaptive_density;
+    if (int e = build_table(ctx, plane, nullptr, width, height, params, adaptive, &table)) return e;
+    std::unique_ptr<mars_table, void (*)(mars_table*)> guard(table, mars_search_table_free);
+    mars::codec::Provider provider = [table](uint32_t row, uint32_t col, uint32_t size,
+                                             uint32_t shift, mars::codec::SearchAnswer* ans) {
+        return mars_search_table_lookup(table, row, col, size, shift, &ans->cand, &ans->evals);
+    };
+    std::vector<mars_leaf> out;
+    const mars::codec::Image im{plane, width, height};
+    if (int e = mars::codec::encode(im, *params, *options, provider, header, &out, counters))
+        return e;
+    *nleaves = out.size();
+    *leaves = (mars_leaf*)std::malloc(std::max<size_t>(1, out.size()) * sizeof(mars_leaf));
+    if (!*leaves) return fail(MARS_ENOMEM, "leaf array allocation failed");
+    std::memcpy(*leaves, out.data(), out.size() * sizeof(mars_leaf));
+    return MARS_OK;
+}
+
+void mars_leaves_free(mars_leaf* leaves) { std::free(leaves); }
+void mars_bytes_free(uint8_t* bytes) { std::free(bytes); }
+
+int mars_decode(mars_ctx* ctx, const mars_header* hdr, const mars_leaf* leaves, size_t n,
+                uint32_t iterations, uint8_t* out) {
+    if (!ctx || !hdr || !out || (n && !leaves)) return fail(MARS_EINVAL, "NULL argument");
+    const uint32_t w = hdr->width, h = hdr->height;
+    if (w == 0 || h == 0) return fail(MARS_EINVAL, "empty plane");
+    if (hdr->bits_alfa > 16 || hdr->bits_beta < 1 || hdr->bits_beta > 16)
+        return fail(MARS_EINVAL, "header bit widths out of range");
+    // Host-side validation: every read and write the gather makes stays inside the plane.
+    std::vector<int32_t> owner((size_t)w * h, -1);
+    std::vector<mars::DecodeLeaf> dl(n);
+    const double max_alfa = (double)hdr->int_max_alfa / 256.0 * 8.0;
+    for (size_t k = 0; k < n; ++k) {
+        const mars_leaf& L = leaves[k];
+        if (L.size == 0 || L.row + L.size > h || L.col + L.size > w || L.isometry > 7)
+            return fail(MARS_EINVAL, "leaf " + std::to_string(k) + " lies outside the plane");
+        if (L.mode > 2) return fail(MARS_EUNSUPPORTED, "leaf mode 3 is not supported");
+        if (L.mode != 1 && L.qalfa != 0 &&
+            (L.dom_row + 2 * L.size > h || L.dom_col + 2 * L.size > w))
+            return fail(MARS_EINVAL, "leaf " + std::to_string(k) + " domain runs past the plane");
+        mars::DecodeLeaf& d = dl[k];
+        d.row = L.row;
+        d.col = L.col;
+        d.size = L.size;
+        d.mode = L.mode;
+        d.iso = L.isometry;
+        d.dom_row = L.dom_row;
+        d.dom_col = L.dom_col;
+        d.qalfa = L.qalfa;
+        d.gx = d.gy = 0.0;
+        if (L.mode == 1) {
+            // ifs.rs:416-431
+            d.alfa = (double)L.qbeta / (double)((1u << hdr->bits_beta) - 1) * 255.0;
+            d.beta = 0.0;
+            d.gx = (double)L.qgx / 64.0;
+            d.gy = (double)L.qgy / 64.0;
+        } else {
+            // ifs.rs:433-439
+            d.alfa = (double)L.qalfa / (double)(1u << hdr->bits_alfa) * max_alfa;
+            d.beta = (double)L.qbeta / (double)((1u << hdr->bits_beta) - 1) *
+                     ((1.0 + std::fabs(d.alfa)) * 255.0);
+            if (d.alfa > 0.0) d.beta -= d.alfa * 255.0;
+        }
+        for (uint32_t i = 0; i < L.size; ++i)
+            std::fill_n(owner.begin() + (long)((size_t)(L.row + i) * w + L.col), L.size, (int32_t)k);
+    }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    Scratch sc(ctx->stream);
+    uint8_t *a = nullptr, *b = nullptr;
+    int32_t* d_owner = nullptr;
+    mars::DecodeLeaf* d_leaves = nullptr;
+    const size_t px = (size_t)w * h;
+    MARS_CUDA(sc.get(&a, px));
+    MARS_CUDA(sc.get(&b, px));
+    MARS_CUDA(sc.get(&d_owner, px));
+    MARS_CUDA(sc.get(&d_leaves, n));
+    MARS_CUDA(cudaMemcpyAsync(d_owner, owner.data(), px * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if (n)
+        MARS_CUDA(cudaMemcpyAsync(d_leaves, dl.data(), n * sizeof(mars::DecodeLeaf),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    MARS_CUDA(cudaMemsetAsync(a, 128, px, ctx->stream));
+    for (uint32_t it = 0; it < iterations; ++it) {
+        MARS_CUDA(mars::launch_decode_step(a, b, (int)w, (int)h, d_owner, d_leaves, ctx->stream));
+        ctx->launches += 1;
+        std::swap(a, b);
+    }
+    MARS_CUDA(cudaMemcpyAsync(out, a, px, cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_bounded(ctx);
+}
+
+int mars_ifs_parse(const uint8_t* data, size_t len, mars_header* header, mars_leaf** leaves,
+                   size_t* nleaves) {
+    if (!data || !header || !leaves || !nleaves) return fail(MARS_EINVAL, "NULL argument");
+    std::vector<mars_leaf> out;
+    if (int e = mars::codec::ifs_parse(data, len, header, &out))
+        return fail(e, "malformed .ifs bitstream");
+    *nleaves = out.size();
+    *leaves = (mars_leaf*)std::malloc(std::max<size_t>(1, out.size()) * sizeof(mars_leaf));
+    if (!*leaves) return fail(MARS_ENOMEM, "leaf array allocation failed");
+    std::memcpy(*leaves, out.data(), out.size() * sizeof(mars_leaf));
+    return MARS_OK;
+}
+
+int mars_ifs_write(const mars_header* header, const mars_leaf* leaves, size_t n, uint8_t** out,
+                   size_t* len) {
+    if (!header || (n && !leaves) || !out || !len) return fail(MARS_EINVAL, "NULL argument");
+    std::vector<mars_leaf> v(leaves, leaves + n);
+    std::vector<uint8_t> bytes;
+    if (int e = mars::codec::ifs_write(*header, v, &bytes))
+        return fail(e, "leaves do not tile the quadtree");
+    *len = bytes.size();
+    *out = (uint8_t*)std::malloc(std::max<size_t>(1, bytes.size()));
+    if (!*out) return fail(MARS_ENOMEM, "byte buffer allocation failed");
+    std::memcpy(*out, bytes.data(), bytes.size());
+    return MARS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// Device-side data layouts and launch entry points shared by the search and decode kernels.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "fit.cuh"
+
+namespace mars {
+
+// Per-level domain pool statistics (struct of arrays, one entry per domain position,
+// row-major over the (nrow_d x ncol_d) position grid of that level).
+struct DomainStats {
+    int32_t* s1x4;   // sum of D over the s x s window (D = 2x2 box sum), exact
+    int64_t* s2x16;  // sum of D^2, exact
+    float* detf;     // Ndd = n*s2 - s1^2 (= the reference's det), rounded down; +huge if 0
+    float* sdetf;    // sqrt(Ndd) rounded down; +huge if Ndd == 0
+};
+
+// Per-level range block statistics (one entry per requested block).
+struct RangeStats {
+    int32_t* t0;   // sum r
+    int32_t* t2;   // sum r^2
+    int64_t* nrr;  // n*t2 - t0^2
+    double* sum0;  // f64 sum of any qalfa == 0 fit (domain independent)
+    double* rms0;  // its rms
+};
+
+// One champion per (range, domain tile): the best candidate that tile saw.
+struct Partial {
+    double rms;
+    double sum;
+    uint32_t idx;  // dom_linear * 8 + isometry; UINT32_MAX when the tile saw nothing
+    int32_t t1x4;
+    uint16_t qalfa, qbeta;
+    uint32_t pad;
+};
+static_assert(sizeof(Partial) == 32, "Partial layout");
+
+struct LevelGeom {
+    int size;      // range block side s (a power of two)
+    int shift;     // domain stride in image pixels (even)
+    int nrow_d;    // domain positions per column
+    int ncol_d;    // domain positions per row
+    int step_c;    // domain stride in contracted samples (shift / 2)
+    int dw, dh;    // contracted plane width/height
+    int w, h;      // plane width/height (range blocks outside it are reported invalid)
+};
+
+// Output record, bit-compatible with mars_candidate in include/mars_b200.h.
+struct CandidateOut {
+    uint32_t dom_row, dom_col, isometry, qalfa, qbeta, valid;
+    double rms;
+    int64_t s0, s1_x4, s2_x16, t0, t1_x4, t2;
+};
+
+// ---- launchers (search.cu) ----
+cudaError_t launch_contract(const uint8_t* plane, int w, int h, int32_t* d_out,
+                            cudaStream_t st);
+cudaError_t launch_domain_stats(const int32_t* D, const LevelGeom& g, DomainStats ds,
+                                cudaStream_t st);
+cudaError_t launch_range_stats(const uint8_t* plane, int w, int h, const uint32_t* rows,
+                               const uint32_t* cols, int nranges, int size, const FitParams& fp,
+                               RangeStats rs, cudaStream_t st);
+// The partial array is nsplit x nranges; nsplit from search_simt_splits().
+cudaError_t launch_search_simt(const int32_t* D, const uint8_t* plane, int w,
+                               const uint32_t* rows, const uint32_t* cols, int nranges,
+                               const LevelGeom& g, RangeStats rs, DomainStats ds,
+                               const FitParams& fp, Partial* partials, int nsplit,
+                               unsigned long long* exact_counter, cudaStream_t st);
+int search_simt_tiles(const LevelGeom& g);
+int search_simt_splits(const LevelGeom& g, int nranges, int num_sms);
+cudaError_t launch_reduce(const Partial* partials, int ntiles, int nranges, const LevelGeom& g,
+                          RangeStats rs, DomainStats ds, CandidateOut* out, cudaStream_t st);
+
+// ---- decode (decode.cu) ----
+struct DecodeLeaf {
+    double alfa, beta;     // dequantised contrast / brightness (mode 0/2), or b0 (mode 1)
+    double gx, gy;         // mode-1 gradients
+    uint32_t row, col, size, mode;
+    uint32_t iso, dom_row, dom_col, qalfa;
+};
+cudaError_t launch_decode_step(const uint8_t* src, uint8_t* dst, int w, int h,
+                               const int32_t* leaf_of_pixel, const DecodeLeaf* leaves,
+                               cudaStream_t st);
+
+}  // namespace mars

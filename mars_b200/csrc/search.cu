@@ -1,0 +1,380 @@
+// Exhaustive domain-range block search for one quadtree level (one block size s and one
+// domain stride), sm_100a.
+//
+// Data flow per level (all device-resident, one stream):
+//   contract      : D(r, c) = 2x2 box sum of the plane          (Contracted::build,
+//                   crates/mars-codec/src/encode.rs:478-502)
+//   domain_stats  : per domain position, exact s1_x4 = sum D, s2_x16 = sum D^2 and the
+//                   rounded-down Ndd / sqrt(Ndd) the pruning bound needs
+//                   (domain_sums, encode.rs:800-802)
+//   range_stats   : per range block t0, t2, Nrr and the domain-independent qalfa == 0 fit
+//   search        : per (range block, domain tile) the 8 isometry correlations
+//                   t1_x4 = sum range[map(k,u,v)] * D[u][v] (cross_term_permuted,
+//                   encode.rs:849-864), the exact-bound filter of fit.cuh, and the exact f64
+//                   fit of every survivor; keeps the tile champion under the reference's
+//                   strict-< / encounter-order rule (retain_top_k, encode.rs:676-685)
+//   reduce        : per range block, the champion over tiles by (rms, reference index).
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+
+#include "kernels.cuh"
+
+namespace mars {
+namespace {
+
+constexpr float kHugeDet = 1.0e30f;
+constexpr float kHugeSqrtDet = 1.0e15f;
+constexpr int kTileRows = 16;  // domain positions per tile, vertically
+constexpr int kTileCols = 32;  // and horizontally
+
+// isometry::map (crates/mars-codec/src/isometry.rs:7-19) as a flat range index i*S + j.
+__host__ __device__ constexpr int iso_src(int k, int u, int v, int S) {
+    return k == 0   ? u * S + v
+           : k == 1 ? (S - 1 - v) * S + u
+           : k == 2 ? v * S + (S - 1 - u)
+           : k == 3 ? (S - 1 - u) * S + (S - 1 - v)
+           : k == 4 ? u * S + (S - 1 - v)
+           : k == 5 ? (S - 1 - u) * S + v
+           : k == 6 ? v * S + u
+                    : (S - 1 - v) * S + (S - 1 - u);
+}
+
+__global__ void contract_kernel(const uint8_t* __restrict__ plane, int w, int dw, int dh,
+                                int32_t* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    if (c >= dw || r >= dh) return;
+    const uint8_t* p0 = plane + (size_t)(2 * r) * w + 2 * c;
+    const uint8_t* p1 = p0 + w;
+    out[(size_t)r * dw + c] = (int32_t)p0[0] + (int32_t)p0[1] + (int32_t)p1[0] + (int32_t)p1[1];
+}
+
+__global__ void domain_stats_kernel(const int32_t* __restrict__ D, LevelGeom g, DomainStats ds) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ndom = g.nrow_d * g.ncol_d;
+    if (idx >= ndom) return;
+    const int a = idx / g.ncol_d, b = idx % g.ncol_d;
+    const int32_t* base = D + (size_t)(a * g.step_c) * g.dw + b * g.step_c;
+    int64_t s1 = 0, s2 = 0;
+    for (int u = 0; u < g.size; ++u) {
+        const int32_t* row = base + (size_t)u * g.dw;
+        for (int v = 0; v < g.size; ++v) {
+            const int64_t d = row[v];
+            s1 += d;
+            s2 += d * d;
+        }
+    }
+    const int64_t n = (int64_t)g.size * g.size;
+    const int64_t det16 = n * s2 - s1 * s1;  // 16 * Ndd, exact
+    ds.s1x4[idx] = (int32_t)s1;
+    ds.s2x16[idx] = s2;
+    if (det16 == 0) {
+        ds.detf[idx] = kHugeDet;
+        ds.sdetf[idx] = kHugeSqrtDet;
+    } else {
+        const float df = __double2float_rd((double)det16 * 0.0625);
+        ds.detf[idx] = df;
+        ds.sdetf[idx] = __fsqrt_rd(df);
+    }
+}
+
+__global__ void range_stats_kernel(const uint8_t* __restrict__ plane, int w, int h,
+                                   const uint32_t* __restrict__ rows,
+                                   const uint32_t* __restrict__ cols, int nranges, int size,
+                                   FitParams fp, RangeStats rs) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nranges) return;
+    if (rows[r] + (uint32_t)size > (uint32_t)h || cols[r] + (uint32_t)size > (uint32_t)w) {
+        // A block outside the plane is never read; the search skips it (result invalid).
+        rs.t0[r] = 0;
+        rs.t2[r] = 0;
+        rs.nrr[r] = 0;
+        rs.sum0[r] = 0.0;
+        rs.rms0[r] = 0.0;
+        return;
+    }
+    const uint8_t* base = plane + (size_t)rows[r] * w + cols[r];
+    int32_t t0 = 0, t2 = 0;
+    for (int i = 0; i < size; ++i)
+        for (int j = 0; j < size; ++j) {
+            const int32_t p = base[(size_t)i * w + j];
+            t0 += p;
+            t2 += p * p;
+        }
+    const int64_t n = (int64_t)size * size;
+    rs.t0[r] = t0;
+    rs.t2[r] = t2;
+    rs.nrr[r] = n * (int64_t)t2 - (int64_t)t0 * t0;
+    // Any candidate whose fit quantises to qalfa == 0 has exactly this f64 sum: with
+    // alfa2 == 0 every domain term of fit_f64 is an exact zero.
+    const FitResult f0 = fit_exact(n, 0, 0, t0, 0, t2, fp);
+    rs.sum0[r] = f0.sum;
+    rs.rms0[r] = f0.rms;
+}
+
+// One CTA = RPB range blocks (one per thread) x a strided subset of the domain tiles
+// (tile = blockIdx.y, blockIdx.y + gridDim.y, ...).  Per tile the contracted strip and the
+// domain statistics are staged in shared memory; every thread correlates its range block
+// with each domain of the tile under all 8 isometries, applies the exact-bound filter and
+// runs the exact f64 fit on survivors only.
+template <int S, int RPB>
+__global__ void __launch_bounds__(RPB) search_simt_kernel(
+    const int32_t* __restrict__ D, LevelGeom g, const uint8_t* __restrict__ plane, int w,
+    const uint32_t* __restrict__ rows, const uint32_t* __restrict__ cols, int nranges,
+    RangeStats rs, DomainStats ds, FitParams fp, Partial* __restrict__ partials, int tiles_c,
+    int ntiles, unsigned long long* __restrict__ exact_counter) {
+    constexpr int N = S * S;
+    constexpr bool kRegs = S <= 8;
+    extern __shared__ __align__(16) unsigned char smem[];
+
+    const int step = g.step_c;
+    const int strip_ld = (kTileCols - 1) * step + S;
+    const int strip_rows_max = (kTileRows - 1) * step + S;
+    int32_t* Ds = reinterpret_cast<int32_t*>(smem);
+    float* s1s = reinterpret_cast<float*>(Ds + strip_rows_max * strip_ld);
+    float* dets = s1s + kTileRows * kTileCols;
+    float* sdets = dets + kTileRows * kTileCols;
+    uint8_t* Rs = reinterpret_cast<uint8_t*>(sdets + kTileRows * kTileCols);
+
+    const int tid = threadIdx.x;
+    const int r = blockIdx.x * RPB + tid;
+    const bool active = r < nranges && rows[r] + (uint32_t)S <= (uint32_t)g.h &&
+                        cols[r] + (uint32_t)S <= (uint32_t)g.w;
+    const bool in_grid = r < nranges;
+
+    int rr[kRegs ? N : 1];
+    {
+        const uint8_t* base = active ? plane + (size_t)rows[r] * w + cols[r] : nullptr;
+        if constexpr (kRegs) {
+#pragma unroll
+            for (int p = 0; p < N; ++p) rr[p] = active ? base[(size_t)(p / S) * w + (p % S)] : 0;
+        } else {
+            for (int p = 0; p < N; ++p)
+                Rs[p * RPB + tid] = active ? base[(size_t)(p / S) * w + (p % S)] : 0;
+        }
+    }
+
+    int32_t t0 = 0, t2 = 0;
+    int64_t nrr = 0;
+    double rms0 = 0.0;
+    if (active) {
+        t0 = rs.t0[r];
+        t2 = rs.t2[r];
+        nrr = rs.nrr[r];
+        rms0 = rs.rms0[r];
+    }
+    const float t0f = (float)t0;
+    const float inv_n = 1.0f / (float)N;  // exact: N is a power of four
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    double ch_rms = inf, ch_sum = inf;
+    uint32_t ch_idx = UINT32_MAX;
+    int32_t ch_t1 = 0;
+    uint32_t ch_qa = 0, ch_qb = 0;
+    Threshold th = make_threshold(ch_sum, ch_rms, UINT32_MAX, rms0, nrr, N, fp);
+    unsigned long long exact = 0;
+
+    for (int tile = blockIdx.y; tile < ntiles; tile += gridDim.y) {
+        const int a0 = (tile / tiles_c) * kTileRows, b0 = (tile % tiles_c) * kTileCols;
+        const int na = min(kTileRows, g.nrow_d - a0), nb = min(kTileCols, g.ncol_d - b0);
+        const int strip_h = (na - 1) * step + S, strip_w = (nb - 1) * step + S;
+        __syncthreads();
+        for (int i = tid; i < strip_h * strip_w; i += RPB) {
+            const int y = i / strip_w, x = i % strip_w;
+            Ds[y * strip_ld + x] = D[(size_t)(a0 * step + y) * g.dw + b0 * step + x];
+        }
+        for (int i = tid; i < na * nb; i += RPB) {
+            const int da = i / nb, db = i % nb;
+            const int dom = (a0 + da) * g.ncol_d + (b0 + db);
+            s1s[da * kTileCols + db] = (float)ds.s1x4[dom];
+            dets[da * kTileCols + db] = ds.detf[dom];
+            sdets[da * kTileCols + db] = ds.sdetf[dom];
+        }
+        __syncthreads();
+        if (!active) continue;
+
+        for (int da = 0; da < na; ++da) {
+            for (int db = 0; db < nb; ++db) {
+                const int32_t* Dw = Ds + (da * step) * strip_ld + db * step;
+                int acc[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) acc[k] = 0;
+                if constexpr (kRegs) {
+#pragma unroll
+                    for (int u = 0; u < S; ++u)
+#pragma unroll
+                        for (int v = 0; v < S; ++v) {
+                            const int d = Dw[u * strip_ld + v];
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) acc[k] += rr[iso_src(k, u, v, S)] * d;
+                        }
+                } else {
+                    for (int u = 0; u < S; ++u) {
+#pragma unroll 4
+                        for (int v = 0; v < S; ++v) {
+                            const int d = Dw[u * strip_ld + v];
+#pragma unroll
+                            for (int k = 0; k < 8; ++k)
+                                acc[k] += (int)Rs[iso_src(k, u, v, S) * RPB + tid] * d;
+                        }
+                    }
+                }
+                const int li = da * kTileCols + db;
+                const uint32_t dom = (uint32_t)((a0 + da) * g.ncol_d + (b0 + db));
+                const int32_t lim = prune_below(th, dom, s1s[li], t0f, dets[li], sdets[li], inv_n, fp);
+                int mx = acc[0];
+#pragma unroll
+                for (int k = 1; k < 8; ++k) mx = max(mx, acc[k]);
+                if (mx < lim) continue;
+                const int32_t s1 = ds.s1x4[dom];
+                const int64_t s2 = ds.s2x16[dom];
+#pragma unroll 1
+                for (int k = 0; k < 8; ++k) {
+                    if (acc[k] < lim) continue;
+                    ++exact;
+                    const FitResult f = fit_exact(N, s1, s2, t0, acc[k], t2, fp);
+                    const uint32_t idx = dom * 8u + (uint32_t)k;
+                    if (f.rms < ch_rms || (f.rms == ch_rms && idx < ch_idx)) {
+                        ch_rms = f.rms;
+                        ch_sum = f.sum;
+                        ch_idx = idx;
+                        ch_t1 = acc[k];
+                        ch_qa = f.qalfa;
+                        ch_qb = f.qbeta;
+                        th = make_threshold(ch_sum, ch_rms, dom, rms0, nrr, N, fp);
+                    }
+                }
+            }
+        }
+    }
+    if (!in_grid) return;
+    Partial p;
+    p.rms = ch_rms;
+    p.sum = ch_sum;
+    p.idx = ch_idx;
+    p.t1x4 = ch_t1;
+    p.qalfa = (uint16_t)ch_qa;
+    p.qbeta = (uint16_t)ch_qb;
+    p.pad = 0;
+    partials[(size_t)blockIdx.y * nranges + r] = p;
+    if (exact_counter && exact) atomicAdd(exact_counter, exact);
+}
+
+__global__ void reduce_kernel(const Partial* __restrict__ partials, int ntiles, int nranges,
+                              LevelGeom g, RangeStats rs, DomainStats ds,
+                              CandidateOut* __restrict__ out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nranges) return;
+    Partial best = partials[r];
+    for (int t = 1; t < ntiles; ++t) {
+        const Partial p = partials[(size_t)t * nranges + r];
+        if (p.rms < best.rms || (p.rms == best.rms && p.idx < best.idx)) best = p;
+    }
+    CandidateOut c;
+    const int64_t n = (int64_t)g.size * g.size;
+    if (best.idx == UINT32_MAX) {
+        c = CandidateOut{0, 0, 0, 0, 0, 0, 0.0, 0, 0, 0, 0, 0, 0};
+    } else {
+        const uint32_t dom = best.idx >> 3;
+        c.dom_row = (dom / g.ncol_d) * g.shift;
+        c.dom_col = (dom % g.ncol_d) * g.shift;
+        c.isometry = best.idx & 7u;
+        c.qalfa = best.qalfa;
+        c.qbeta = best.qbeta;
+        c.valid = 1;
+        c.rms = best.rms;
+        c.s0 = n;
+        c.s1_x4 = ds.s1x4[dom];
+        c.s2_x16 = ds.s2x16[dom];
+        c.t0 = rs.t0[r];
+        c.t1_x4 = best.t1x4;
+        c.t2 = rs.t2[r];
+    }
+    out[r] = c;
+}
+
+template <int S, int RPB>
+cudaError_t launch_simt_t(const int32_t* D, const uint8_t* plane, int w, const uint32_t* rows,
+                          const uint32_t* cols, int nranges, const LevelGeom& g, RangeStats rs,
+                          DomainStats ds, const FitParams& fp, Partial* partials, int nsplit,
+                          unsigned long long* counter, cudaStream_t st) {
+    const int tiles_c = (g.ncol_d + kTileCols - 1) / kTileCols;
+    const int ntiles = search_simt_tiles(g);
+    const int strip_ld = (kTileCols - 1) * g.step_c + S;
+    const int strip_rows = (kTileRows - 1) * g.step_c + S;
+    size_t smem = (size_t)strip_ld * strip_rows * 4 + 3 * kTileRows * kTileCols * 4;
+    if (S > 8) smem += (size_t)S * S * RPB;
+    auto kern = search_simt_kernel<S, RPB>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((nranges + RPB - 1) / RPB, nsplit);
+    kern<<<grid, RPB, smem, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, partials,
+                                  tiles_c, ntiles, counter);
+    return cudaGetLastError();
+}
+
+int rpb_for(int size) { return size <= 16 ? 64 : (size == 32 ? 32 : 16); }
+
+}  // namespace
+
+cudaError_t launch_contract(const uint8_t* plane, int w, int h, int32_t* d_out, cudaStream_t st) {
+    const int dw = w / 2, dh = h / 2;
+    if (dw == 0 || dh == 0) return cudaSuccess;
+    dim3 grid((dw + 127) / 128, dh);
+    contract_kernel<<<grid, 128, 0, st>>>(plane, w, dw, dh, d_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_domain_stats(const int32_t* D, const LevelGeom& g, DomainStats ds,
+                                cudaStream_t st) {
+    const int ndom = g.nrow_d * g.ncol_d;
+    if (ndom == 0) return cudaSuccess;
+    domain_stats_kernel<<<(ndom + 255) / 256, 256, 0, st>>>(D, g, ds);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_range_stats(const uint8_t* plane, int w, int h, const uint32_t* rows,
+                               const uint32_t* cols, int nranges, int size, const FitParams& fp,
+                               RangeStats rs, cudaStream_t st) {
+    if (nranges == 0) return cudaSuccess;
+    range_stats_kernel<<<(nranges + 127) / 128, 128, 0, st>>>(plane, w, h, rows, cols, nranges,
+                                                               size, fp, rs);
+    return cudaGetLastError();
+}
+
+int search_simt_tiles(const LevelGeom& g) {
+    return ((g.nrow_d + kTileRows - 1) / kTileRows) * ((g.ncol_d + kTileCols - 1) / kTileCols);
+}
+
+int search_simt_splits(const LevelGeom& g, int nranges, int num_sms) {
+    const int groups = (nranges + rpb_for(g.size) - 1) / rpb_for(g.size);
+    const int want = (num_sms * 16 + groups - 1) / groups;
+    return std::max(1, std::min(want, search_simt_tiles(g)));
+}
+
+cudaError_t launch_search_simt(const int32_t* D, const uint8_t* plane, int w,
+                               const uint32_t* rows, const uint32_t* cols, int nranges,
+                               const LevelGeom& g, RangeStats rs, DomainStats ds,
+                               const FitParams& fp, Partial* partials, int nsplit,
+                               unsigned long long* counter, cudaStream_t st) {
+    if (nranges == 0 || g.nrow_d <= 0 || g.ncol_d <= 0) return cudaSuccess;
+    switch (g.size) {
+        case 2: return launch_simt_t<2, 64>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
+        case 4: return launch_simt_t<4, 64>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
+        case 8: return launch_simt_t<8, 64>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
+        case 16: return launch_simt_t<16, 64>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
+        case 32: return launch_simt_t<32, 32>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
+        case 64: return launch_simt_t<64, 16>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_reduce(const Partial* partials, int ntiles, int nranges, const LevelGeom& g,
+                          RangeStats rs, DomainStats ds, CandidateOut* out, cudaStream_t st) {
+    if (nranges == 0) return cudaSuccess;
+    reduce_kernel<<<(nranges + 127) / 128, 128, 0, st>>>(partials, ntiles, nranges, g, rs, ds, out);
+    return cudaGetLastError();
+}
+
+}  // namespace mars
