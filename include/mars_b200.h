@@ -103,6 +103,10 @@ void mars_ctx_destroy(mars_ctx* ctx);
 int mars_ctx_set_stream(mars_ctx* ctx, void* stream);
 /* Kernel launches made by this context since creation (instrumentation). */
 uint64_t mars_ctx_launch_count(const mars_ctx* ctx);
+/* Correlation kernel selection for A/B checks: 0 = automatic (tensor cores wherever the
+ * level allows, CUDA cores otherwise), 1 = CUDA cores only, 2 = automatic as well (the
+ * tensor-core path never serves a level it does not support).  Results are identical. */
+int mars_ctx_set_search_path(mars_ctx* ctx, int32_t path);
 
 /* The provider factory (encode.rs:1076): search every quadtree node an encode of this
  * plane can request -- every aligned block of size min_size..max_size, plus the smaller

@@ -66,7 +66,8 @@ LEAF_DTYPE = np.dtype([(n, "<u4") for n in (
 # Every symbol include/mars_b200.h declares (tests check the library exports them all).
 EXPORTS = (
     "mars_last_error", "mars_version", "mars_ctx_create", "mars_ctx_destroy",
-    "mars_ctx_set_stream", "mars_ctx_launch_count", "mars_search_table_build",
+    "mars_ctx_set_stream", "mars_ctx_launch_count", "mars_ctx_set_search_path",
+    "mars_search_table_build",
     "mars_search_table_lookup", "mars_search_table_evals", "mars_search_table_exact_fits",
     "mars_search_table_free", "mars_search_blocks", "mars_search_blocks_device",
     "mars_search_nodes_device", "mars_encode", "mars_leaves_free", "mars_decode",
@@ -97,6 +98,7 @@ def lib():
     L.mars_ctx_set_stream.argtypes = [vp, vp]
     L.mars_ctx_launch_count.argtypes = [vp]
     L.mars_ctx_launch_count.restype = u64
+    L.mars_ctx_set_search_path.argtypes = [vp, C.c_int32]
     L.mars_search_table_build.argtypes = [vp, vp, u32, u32, P(Params), C.c_int32, P(vp)]
     L.mars_search_table_lookup.argtypes = [vp, u32, u32, u32, u32, vp, P(u64)]
     L.mars_search_table_evals.argtypes = [vp]
@@ -231,6 +233,10 @@ class Context:
 
     def set_stream(self, stream_ptr: int) -> None:
         check(lib().mars_ctx_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def set_search_path(self, path: str) -> None:
+        """'auto' (tensor cores wherever a level allows) or 'simt' (CUDA cores only)."""
+        check(lib().mars_ctx_set_search_path(self._h, {"auto": 0, "simt": 1, "tc": 2}[path]))
 
     @property
     def launches(self) -> int:

@@ -19,6 +19,9 @@
 #include "../../include/mars_b200.h"
 #include "codec.hpp"
 #include "kernels.cuh"
+#include "tc.cuh"
+
+#include <cudaTypedefs.h>
 
 namespace {
 
@@ -48,6 +51,9 @@ struct mars_ctx {
     std::atomic<uint64_t> launches{0};
     std::mutex mu;
     unsigned long long* d_counter = nullptr;  // survivors that took the exact f64 fit
+    int* d_err = nullptr;                     // kernel-side error bits (bounded waits)
+    int search_path = 0;                      // 0 auto, 1 CUDA cores only, 2 tensor cores
+    PFN_cuTensorMapEncodeTiled_v12000 encode_tiled = nullptr;
 };
 
 struct mars_table {
@@ -94,6 +100,13 @@ int sync_bounded(mars_ctx* ctx) {
         std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 20 : 500));
     }
     cudaEventDestroy(ev);
+    int kerr = 0;
+    MARS_CUDA(cudaMemcpy(&kerr, ctx->d_err, sizeof kerr, cudaMemcpyDeviceToHost));
+    if (kerr) {
+        cudaMemset(ctx->d_err, 0, sizeof(int));
+        return fail(MARS_ETIMEOUT, "a bounded wait inside the search kernel expired (code " +
+                                       std::to_string(kerr) + ")");
+    }
     return MARS_OK;
 }
 
@@ -163,6 +176,78 @@ struct Scratch {
     }
 };
 
+// Which correlation kernel serves a level: the tcgen05 path wherever it applies (block
+// sizes 4..64, domain stride 2, 4, 8 or 16), the CUDA-core path otherwise.
+// mars_ctx_set_search_path (or the MARS_SEARCH_PATH environment variable, simt / tc)
+// pins the CUDA-core path for A/B checks.
+bool use_tc(const mars_ctx* ctx, uint32_t size, uint32_t shift) {
+    static const int env = [] {
+        const char* e = std::getenv("MARS_SEARCH_PATH");
+        if (!e) return 0;
+        if (std::string(e) == "simt") return 1;
+        if (std::string(e) == "tc") return 2;
+        return 0;
+    }();
+    const int forced = ctx->search_path ? ctx->search_path : env;
+    if (forced == 1) return false;
+    return mars::tc::supported((int)size, (int)shift);
+}
+
+int make_maps(mars_ctx* ctx, const uint8_t* d_phases, uint32_t w, uint32_t h, uint32_t shift,
+              mars::tc::TcMaps* maps) {
+    if (!ctx->encode_tiled) return fail(MARS_ECUDA, "cuTensorMapEncodeTiled is unavailable");
+    std::memset(maps, 0, sizeof(*maps));
+    const int P = mars::tc::phase_count((int)shift);
+    const uint64_t wp = (uint64_t)mars::tc::row_pitch((int)w);
+    for (int p = 0; p < P; ++p) {
+        const cuuint64_t dims[2] = {wp, h};
+        const cuuint64_t strides[1] = {wp};
+        const cuuint32_t box[2] = {128, 8};
+        const cuuint32_t estr[2] = {1, 1};
+        void* addr = (void*)(d_phases + (size_t)p * h * wp);
+        const CUresult r = ctx->encode_tiled(&maps->m[p], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, addr,
+                                             dims, strides, box, estr,
+                                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+            return fail(MARS_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    }
+    return MARS_OK;
+}
+
+// The tcgen05 path for one level: phase copies of the plane, the B operand, seed
+// champions, the correlation + exact-bound kernel, and the final champion per block.
+int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t* d_D,
+                 uint32_t w, uint32_t h, const mars::LevelGeom& g, const mars::FitParams& fp,
+                 const uint32_t* d_rows, const uint32_t* d_cols, size_t n, mars::RangeStats rs,
+                 mars::DomainStats ds, mars::CandidateOut* d_out) {
+    const cudaStream_t st = ctx->stream;
+    const int P = mars::tc::phase_count(g.shift);
+    uint8_t* d_phases = nullptr;
+    uint8_t* d_b = nullptr;
+    mars::tc::SeedOut* d_seed = nullptr;
+    MARS_CUDA(sc.get(&d_phases, (size_t)P * h * mars::tc::row_pitch((int)w)));
+    MARS_CUDA(sc.get(&d_b, mars::tc::b_bytes(g.size, (int)n)));
+    MARS_CUDA(sc.get(&d_seed, n));
+    const int msplit = mars::tc::msplit_for(g, (int)n, ctx->num_sms);
+    mars::Partial* partials = nullptr;
+    MARS_CUDA(sc.get(&partials, (size_t)msplit * n));
+    mars::tc::TcMaps maps;
+    if (int e = make_maps(ctx, d_phases, w, h, (uint32_t)g.shift, &maps)) return e;
+    MARS_CUDA(mars::tc::launch_phase_planes(d_plane, (int)w, (int)h, g.shift, d_phases, st));
+    MARS_CUDA(mars::tc::launch_build_b(g.size, d_plane, (int)w, (int)h, d_rows, d_cols, (int)n,
+                                       d_b, st));
+    MARS_CUDA(mars::tc::launch_seed(d_D, g, d_plane, (int)w, d_rows, d_cols, (int)n, rs, ds, fp,
+                                    d_seed, st));
+    MARS_CUDA(mars::tc::launch_corr(maps, d_b, g, (int)n, rs, ds, fp, d_seed, partials, msplit,
+                                    ctx->d_err, ctx->d_counter, st));
+    MARS_CUDA(mars::tc::launch_finish(partials, msplit, (int)n, g, d_D, d_plane, (int)w, d_rows,
+                                      d_cols, rs, ds, fp, d_out, st));
+    ctx->launches += 5;
+    return MARS_OK;
+}
+
 // Search every block of one (size, shift) level.  rows/cols/out are device pointers.
 int run_level(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t* d_D,
               uint32_t w, uint32_t h, uint32_t size, uint32_t shift, const mars::FitParams& fp,
@@ -188,16 +273,19 @@ int run_level(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t*
     MARS_CUDA(sc.get(&ds.s2x16, ndom));
     MARS_CUDA(sc.get(&ds.detf, ndom));
     MARS_CUDA(sc.get(&ds.sdetf, ndom));
-    const int nsplit = mars::search_simt_splits(g, (int)n, ctx->num_sms);
-    mars::Partial* partials;
-    MARS_CUDA(sc.get(&partials, (size_t)nsplit * n));
     MARS_CUDA(mars::launch_range_stats(d_plane, (int)w, (int)h, d_rows, d_cols, (int)n,
                                        (int)size, fp, rs, st));
     MARS_CUDA(mars::launch_domain_stats(d_D, g, ds, st));
+    ctx->launches += 2;
+    if (use_tc(ctx, size, shift))
+        return run_level_tc(ctx, sc, d_plane, d_D, w, h, g, fp, d_rows, d_cols, n, rs, ds, d_out);
+    const int nsplit = mars::search_simt_splits(g, (int)n, ctx->num_sms);
+    mars::Partial* partials;
+    MARS_CUDA(sc.get(&partials, (size_t)nsplit * n));
     MARS_CUDA(mars::launch_search_simt(d_D, d_plane, (int)w, d_rows, d_cols, (int)n, g, rs, ds,
                                        fp, partials, nsplit, ctx->d_counter, st));
     MARS_CUDA(mars::launch_reduce(partials, nsplit, (int)n, g, rs, ds, d_out, st));
-    ctx->launches += 4;
+    ctx->launches += 2;
     return MARS_OK;
 }
 
@@ -380,6 +468,16 @@ int mars_ctx_create(mars_ctx** out, int device) {
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_counter, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            c->encode_tiled = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
     if (e == cudaSuccess) {
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -402,6 +500,7 @@ void mars_ctx_destroy(mars_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
+    if (ctx->d_err) cudaFree(ctx->d_err);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }
@@ -414,6 +513,13 @@ int mars_ctx_set_stream(mars_ctx* ctx, void* stream) {
 }
 
 uint64_t mars_ctx_launch_count(const mars_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
+
+int mars_ctx_set_search_path(mars_ctx* ctx, int32_t path) {
+    if (!ctx || path < 0 || path > 2) return fail(MARS_EINVAL, "path must be 0, 1 or 2");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->search_path = path;
+    return MARS_OK;
+}
 
 int mars_search_table_build(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
                             const mars_params* params, int32_t adaptive_density,

@@ -1,0 +1,843 @@
+// Tensor-core (tcgen05, sm_100a) domain-range correlation with the fused exact-bound
+// epilogue.
+//
+// For one quadtree level (block size S, domain stride `shift` in {2, 4, 8, 16}) the
+// correlations t1'(domain, range, isometry) = sum_{y,x} P[dom_row+y][dom_col+x] *
+// (r[map_k(y/2, x/2)] - 128) over the 2S x 2S pixel block of a domain are one exact int8
+// GEMM with INT32 accumulation:
+//   A (M = 128 lanes)  = 128 consecutive domain positions of one domain row, K-major:
+//                        each domain's pixels, grouped in 16-byte K-groups (pixel row y,
+//                        16-pixel column group j); u8.
+//   B (N = 256)        = 32 range blocks x 8 isometries: the range pixel r[map_k(u, v)]
+//                        minus 128, upsampled 2x2 onto the same K positions; s8.  Zero on
+//                        K positions past 2S (S = 4 pads each pixel row to 16 bytes).
+//   D (TMEM, 128 x 256 int32) = t1' = t1_x4 - 128 * s1_x4, exact (|t1'| < 2^31).
+// The pixel sum over the 2x2 box that the reference folds into D = 4d
+// (Contracted::build, crates/mars-codec/src/encode.rs:478-502) is folded into K instead,
+// so every operand is a plain u8 pixel or an s8 range sample and nothing rounds.
+//
+// A is fed by TMA from `shift`-phase copies of the plane: copy p holds the plane shifted
+// left by shift*p pixels, so the P = 16/shift domains of one 16-byte column group start on
+// 16-byte boundaries and 8 consecutive same-phase domains' K-group is one contiguous
+// 128-byte row segment -- exactly one 8 x 16 B core matrix of the SWIZZLE_NONE K-major
+// canonical layout.  A 128 B x 8-row TMA box therefore lands as 8 core matrices along K
+// (LBO = 128 B), and the 16 boxes of a stage are 16 row groups (SBO = 1024 B).  B is
+// pre-built in global memory in the same core-matrix order and copied with 1-D bulk
+// copies.
+//
+// Warp roles (256 threads): warp 0 issues the loads, warp 1 owns TMEM and issues the MMAs
+// (one elected lane), warps 4-7 are the epilogue (TMEM lane quadrant = warp % 4).  The
+// accumulator is double-buffered in TMEM (2 x 256 columns).  The epilogue runs the
+// pruning test of fit.cuh once per (domain lane, range) -- shared by the 8 isometry
+// columns -- and queues survivors per range in shared memory; one warp per range then
+// runs the exact f64 fit on them and updates that range's champion and threshold.
+// Every mbarrier wait is bounded (clock64 deadline): on expiry the kernel records an
+// error, stops issuing work, waits (bounded) for its own loads, frees TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "tc.cuh"
+
+namespace mars {
+namespace tc {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kM = 128;
+constexpr int kN = 256;
+constexpr int kRangesPerTile = kN / 8;     // 32
+constexpr int kStageA = 16 * 1024;         // 16 row groups x 8 K-groups x 128 B
+constexpr int kStageB = 32 * 1024;         // 32 row groups x 8 K-groups x 128 B
+constexpr int kQueueCap = kM * 8;          // survivors of one range in one 32-column chunk
+constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 1.965 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false when the deadline passed or another warp already gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          int* err_global, int code) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > kWaitCycles) {
+            *abort_flag = 1;
+            atomicOr(err_global, code);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// SWIZZLE_NONE K-major shared-memory matrix descriptor: core matrices of 8 rows x 16 B,
+// LBO = 128 B between K-adjacent core matrices, SBO = 1024 B between 8-row groups.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)(128u >> 4) << 16;
+    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+    return d;                // base offset 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor, kind::i8: D = s32, A = u8, B = s8, both K-major, M = 128, N = 256.
+constexpr uint32_t kIdesc = (2u << 4) | (0u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) |
+                            ((uint32_t)(kM >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+          "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+          "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+          "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void epi_barrier() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Named barrier over the 4 epilogue warps that also ANDs a predicate across them, so the
+// warps always agree on whether to go on.
+__device__ __forceinline__ bool epi_barrier_and(bool pred) {
+    uint32_t out;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, 1, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(out)
+        : "r"((uint32_t)pred)
+        : "memory");
+    return out != 0;
+}
+
+// Per-range state shared by the epilogue warps.
+struct RangeRec {
+    double rms;      // champion rms (reference order: smaller rms, then smaller idx)
+    double sum;      // champion f64 sum
+    double rms0;     // rms of any qalfa == 0 fit of this range
+    int64_t nrr;
+    uint32_t idx;    // champion reference index dom * 8 + isometry
+    int32_t t0, t2;
+    float c;         // t0 / n - 128 (exact)
+    Threshold th;
+    int32_t valid;
+};
+
+struct __align__(8) QEntry {
+    int32_t t1;     // t1' = t1_x4 - 128 * s1_x4
+    uint32_t code;  // lane << 3 | isometry
+};
+
+struct Smem {
+    uint64_t full[kStages];
+    uint64_t empty[kStages];
+    uint64_t tfull[2];
+    uint64_t tempty[2];
+    uint64_t bres;
+    uint32_t tmem_base;
+    int abort_flag;
+    int qcount[2][4];
+    RangeRec rec[kRangesPerTile];
+    QEntry queue[4][kQueueCap];
+};
+
+__device__ __forceinline__ void domain_of_lane(int m, int P, int tile_q0, int* c) {
+    const int g = m >> 3, r8 = m & 7;
+    const int per_phase = 16 / P;
+    const int p = g / per_phase, h = g % per_phase;
+    *c = P * (tile_q0 + 8 * h + r8) + p;
+}
+
+template <int S>
+__global__ void __launch_bounds__(kThreads, 1)
+    corr_tc_kernel(const __grid_constant__ TcMaps maps, const uint8_t* __restrict__ bglob,
+                   LevelGeom g, int nranges, RangeStats rs, DomainStats ds, FitParams fp,
+                   const SeedOut* __restrict__ seeds, int m_tiles, int m_per_cta,
+                   Partial* __restrict__ partials, int* __restrict__ err,
+                   unsigned long long* __restrict__ exact_counter) {
+    constexpr int N = S * S;
+    constexpr int J = S >= 8 ? S / 8 : 1;  // 16-byte column groups per pixel row
+    constexpr int ROWS = 2 * S;            // pixel rows of a domain block
+    constexpr int KST = J * ROWS / 8;      // 128-byte K stages per tile
+    constexpr bool kBRes = KST <= 2;       // B tile stays resident in shared memory
+    constexpr uint32_t kTxA = kStageA;
+    constexpr uint32_t kTxStage = kBRes ? kTxA : kTxA + kStageB;
+
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* stA = base;                                  // kStages x 16 KB
+    unsigned char* stB = stA + kStages * kStageA;               // kStages x 32 KB or resident
+    unsigned char* after_b = stB + (kBRes ? KST * kStageB : kStages * kStageB);
+    Smem& sm = *reinterpret_cast<Smem*>(after_b);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntile = blockIdx.x;
+    const int m_begin = blockIdx.y * m_per_cta;
+    const int m_end = min(m_tiles, m_begin + m_per_cta);
+    const int P = 16 / g.shift;
+    const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
+    const uint8_t* btile = bglob + (size_t)ntile * KST * kStageB;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&sm.tfull[b], 1);
+            mbar_init(&sm.tempty[b], 128);
+        }
+        mbar_init(&sm.bres, 1);
+        sm.abort_flag = 0;
+        for (int q = 0; q < 4; ++q) sm.qcount[0][q] = sm.qcount[1][q] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (threadIdx.x < kRangesPerTile) {
+        RangeRec& R = sm.rec[threadIdx.x];
+        const int r = ntile * kRangesPerTile + threadIdx.x;
+        R.valid = r < nranges && seeds[r].idx != UINT32_MAX;
+        if (R.valid) {
+            R.t0 = rs.t0[r];
+            R.t2 = rs.t2[r];
+            R.nrr = rs.nrr[r];
+            R.rms0 = rs.rms0[r];
+            R.c = (float)R.t0 / (float)N - 128.0f;  // exact: t0 < 2^24, N a power of four
+            const SeedOut sd = seeds[r];
+            R.rms = sd.rms;
+            R.sum = sd.sum;
+            R.idx = sd.idx;
+            R.th = make_threshold(R.sum, R.rms, R.idx >> 3, R.rms0, R.nrr, N, fp);
+        } else {
+            R.rms = 0.0;
+            R.idx = 0;
+        }
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&sm.tmem_base)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+    const uint32_t tmem = sm.tmem_base;
+    volatile int* abort_flag = &sm.abort_flag;
+
+    if (warp == 0) {
+        // ---------------------------------------------------------------- loads
+        if (lane == 0) {
+            int s = 0;
+            uint32_t ph = 0;
+            int issued = 0;
+            if (kBRes) {
+                mbar_expect_tx(&sm.bres, KST * kStageB);
+                for (int t = 0; t < KST; ++t)
+                    bulk_load(stB + t * kStageB, btile + (size_t)t * kStageB, kStageB, &sm.bres);
+            }
+            for (int mt = m_begin; mt < m_end && !*abort_flag; ++mt) {
+                const int a = mt / tiles_per_row;
+                const int q0 = (mt % tiles_per_row) * (kM / P);
+                const int dom_row = a * g.shift;
+                for (int t = 0; t < KST; ++t) {
+                    if (issued >= kStages && !mbar_wait(&sm.empty[s], ph ^ 1, abort_flag, err, 1)) break;
+                    mbar_expect_tx(&sm.full[s], kTxStage);
+                    const int kg0 = t * 8;
+                    const int j = kg0 / ROWS, y0 = kg0 % ROWS;
+                    unsigned char* dstA = stA + s * kStageA;
+#pragma unroll 1
+                    for (int gg = 0; gg < 16; ++gg) {
+                        const int per_phase = 16 / P;
+                        const int p = gg / per_phase, h = gg % per_phase;
+                        tma_load_2d(dstA + gg * 1024, &maps.m[p], 16 * (q0 + 8 * h + j),
+                                    dom_row + y0, &sm.full[s]);
+                    }
+                    if (!kBRes)
+                        bulk_load(stB + s * kStageB, btile + (size_t)t * kStageB, kStageB, &sm.full[s]);
+                    ++issued;
+                    if (++s == kStages) {
+                        s = 0;
+                        ph ^= 1;
+                    }
+                }
+            }
+            // Drain: wait (bounded) for the loads still in flight before leaving.
+            if (*abort_flag) {
+                int s2 = s;
+                uint32_t ph2 = ph;
+                for (int i = 0; i < kStages && i < issued; ++i) {
+                    if (--s2 < 0) {
+                        s2 = kStages - 1;
+                        ph2 ^= 1;
+                    }
+                    const long long t0 = clock64();
+                    while (!mbar_try_wait(&sm.full[s2], ph2) && clock64() - t0 < kWaitCycles) {
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------------------- MMA
+        if (lane == 0) {
+            int s = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            if (kBRes) ok = mbar_wait(&sm.bres, 0, abort_flag, err, 2);
+            int i = 0;
+            for (int mt = m_begin; ok && mt < m_end; ++mt, ++i) {
+                const int b = i & 1;
+                const uint32_t bph = (uint32_t)((i >> 1) & 1);
+                if (i >= 2 && !mbar_wait(&sm.tempty[b], bph ^ 1, abort_flag, err, 4)) break;
+                tmem_fence_after();
+                const uint32_t dcol = tmem + (uint32_t)(b * kN);
+                for (int t = 0; t < KST; ++t) {
+                    if (!mbar_wait(&sm.full[s], ph, abort_flag, err, 8)) {
+                        ok = false;
+                        break;
+                    }
+                    tmem_fence_after();
+                    const uint32_t a_addr = smem_u32(stA + s * kStageA);
+                    const uint32_t b_addr = smem_u32(kBRes ? stB + t * kStageB : stB + s * kStageB);
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk)
+                        mma_i8(dcol, smem_desc(a_addr + kk * 256), smem_desc(b_addr + kk * 256),
+                               (t > 0 || kk > 0) ? 1u : 0u);
+                    mma_commit(&sm.empty[s]);
+                    if (++s == kStages) {
+                        s = 0;
+                        ph ^= 1;
+                    }
+                }
+                if (!ok) break;
+                mma_commit(&sm.tfull[b]);
+            }
+        }
+        __syncwarp();
+    } else if (warp >= 4) {
+        // ---------------------------------------------------------------- epilogue
+        const int e = warp - 4;  // TMEM lane quadrant
+        const int m = e * 32 + lane;
+        const float inv_n = 1.0f / (float)N;
+        const float four_inv_n = 4.0f / (float)N;
+        unsigned long long exact = 0;
+        int i = 0;
+        for (int mt = m_begin; mt < m_end; ++mt, ++i) {
+            const int b = i & 1;
+            const uint32_t bph = (uint32_t)((i >> 1) & 1);
+            const bool got = mbar_wait(&sm.tfull[b], bph, abort_flag, err, 16);
+            if (!epi_barrier_and(got)) break;
+            tmem_fence_after();
+            const int a = mt / tiles_per_row;
+            const int q0 = (mt % tiles_per_row) * (kM / P);
+            int c;
+            domain_of_lane(m, P, q0, &c);
+            const bool dvalid = c < g.ncol_d;
+            const uint32_t dom = (uint32_t)(a * g.ncol_d + (dvalid ? c : 0));
+            float s1f = 0.f, detf = 0.f, sdetf = 0.f;
+            if (dvalid) {
+                s1f = (float)ds.s1x4[dom];
+                detf = ds.detf[dom];
+                sdetf = ds.sdetf[dom];
+            }
+            const float ad = __fmul_rd(fp.a_min, detf);
+            const float ahd = __fmul_rd(fp.a_half, detf);
+            const uint32_t tcol = tmem + ((uint32_t)(e * 32) << 16) + (uint32_t)(b * kN);
+            for (int ch = 0; ch < kN / 32; ++ch) {
+                int32_t v[32];
+                tmem_ld32(tcol + (uint32_t)(ch * 32), v);
+                if (ch == kN / 32 - 1) {
+                    // All of this accumulator is in registers: hand it back to the MMA warp.
+                    tmem_fence_before();
+                    mbar_arrive(&sm.tempty[b]);
+                }
+#pragma unroll
+                for (int rr = 0; rr < 4; ++rr) {
+                    const RangeRec& R = sm.rec[ch * 4 + rr];
+                    if (!dvalid || !R.valid) continue;
+                    const Threshold th = R.th;
+                    float tau;
+                    if (th.mode == 2 || (th.mode == 1 && dom > th.tie_dom)) {
+                        const float g1 = __fmul_rd(th.sqrt_w, sdetf);
+                        const float g2 = __fadd_rd(th.w2a, ahd);
+                        tau = fminf(g2, fmaxf(g1, ad));
+                    } else if (th.wpos) {
+                        tau = __fmul_rd(th.sqrt_w, sdetf);
+                    } else {
+                        tau = -INFINITY;
+                    }
+                    const float num = __fadd_rd(__fmul_rd(s1f, R.c), __fmul_rd(tau, four_inv_n));
+                    const int32_t thr = __float2int_rd(num);
+                    int mx = v[rr * 8];
+#pragma unroll
+                    for (int k = 1; k < 8; ++k) mx = max(mx, v[rr * 8 + k]);
+                    if (mx >= thr) {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            if (v[rr * 8 + k] >= thr) {
+                                const int slot = atomicAdd(&sm.qcount[ch & 1][rr], 1);
+                                sm.queue[rr][slot] = QEntry{v[rr * 8 + k], (uint32_t)(m << 3 | k)};
+                            }
+                        }
+                    }
+                }
+                // Counters alternate with the chunk parity: the next chunk's pushes can never
+                // be mistaken for this chunk's survivors by a warp that reads late.
+                epi_barrier();
+                const int* qc = sm.qcount[ch & 1];
+                const int cnt = qc[e];
+                const bool any = (qc[0] | qc[1] | qc[2] | qc[3]) != 0;
+                if (any) {
+                    // Warp e owns range ch*4 + e: exact fits of its survivors, then the
+                    // champion update under the reference's (rms, index) order.
+                    RangeRec& R = sm.rec[ch * 4 + e];
+                    double best_rms = INFINITY, best_sum = 0.0;
+                    uint32_t best_idx = UINT32_MAX;
+                    for (int qi = lane; qi < cnt; qi += 32) {
+                        const QEntry q = sm.queue[e][qi];
+                        int cc;
+                        domain_of_lane((int)(q.code >> 3), P, q0, &cc);
+                        const uint32_t d2 = (uint32_t)(a * g.ncol_d + cc);
+                        const int32_t s1 = ds.s1x4[d2];
+                        const int64_t t1x4 = (int64_t)q.t1 + 128ll * s1;
+                        const FitResult f = fit_exact(N, s1, ds.s2x16[d2], R.t0, t1x4, R.t2, fp);
+                        const uint32_t idx = d2 * 8u + (q.code & 7u);
+                        ++exact;
+                        if (f.rms < best_rms || (f.rms == best_rms && idx < best_idx)) {
+                            best_rms = f.rms;
+                            best_sum = f.sum;
+                            best_idx = idx;
+                        }
+                    }
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) {
+                        const double orms = __shfl_xor_sync(0xffffffffu, best_rms, off);
+                        const double osum = __shfl_xor_sync(0xffffffffu, best_sum, off);
+                        const uint32_t oidx = __shfl_xor_sync(0xffffffffu, best_idx, off);
+                        if (orms < best_rms || (orms == best_rms && oidx < best_idx)) {
+                            best_rms = orms;
+                            best_sum = osum;
+                            best_idx = oidx;
+                        }
+                    }
+                    if (lane == 0 && best_idx != UINT32_MAX &&
+                        (best_rms < R.rms || (best_rms == R.rms && best_idx < R.idx))) {
+                        R.rms = best_rms;
+                        R.sum = best_sum;
+                        R.idx = best_idx;
+                        R.th = make_threshold(R.sum, R.rms, R.idx >> 3, R.rms0, R.nrr, N, fp);
+                    }
+                    epi_barrier();
+                    if (threadIdx.x == 128) {
+                        int* w = sm.qcount[ch & 1];
+                        w[0] = w[1] = w[2] = w[3] = 0;
+                    }
+                    epi_barrier();
+                }
+            }
+        }
+        if (exact_counter && exact) atomicAdd(exact_counter, exact);
+        (void)inv_n;
+    }
+
+    tmem_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tmem_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+    }
+    if (threadIdx.x < kRangesPerTile) {
+        const RangeRec& R = sm.rec[threadIdx.x];
+        const int r = ntile * kRangesPerTile + threadIdx.x;
+        if (r < nranges) {
+            Partial p;
+            p.rms = R.rms;
+            p.sum = R.sum;
+            p.idx = R.idx;
+            p.t1x4 = 0;
+            p.qalfa = 0;
+            p.qbeta = 0;
+            p.pad = 0;
+            partials[(size_t)blockIdx.y * nranges + r] = p;
+        }
+    }
+}
+
+// B operand of one level: rows n = range * 8 + isometry; for each 256-row N tile and each
+// 128-byte K stage, 32 row groups x 8 K-groups x (8 rows x 16 B).
+template <int S>
+__global__ void build_b_kernel(const uint8_t* __restrict__ plane, int w, int h,
+                               const uint32_t* rows, const uint32_t* cols, int nranges,
+                               int ntiles, uint8_t* __restrict__ out) {
+    constexpr int J = S >= 8 ? S / 8 : 1;
+    constexpr int ROWS = 2 * S;
+    constexpr int KG = J * ROWS;
+    constexpr int KST = KG / 8;
+    // one thread per (n, kg): writes one 16-byte K-group of one B row
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)ntiles * kN * KG;
+    if (tid >= total) return;
+    const int kg = (int)(tid % KG);
+    const long long nglob = tid / KG;
+    const int nt = (int)(nglob / kN), n = (int)(nglob % kN);
+    const int r = nt * kRangesPerTile + n / 8, k = n % 8;
+    const int j = kg / ROWS, y = kg % ROWS;
+    const int t = kg / 8, kgl = kg % 8;
+    const bool inside = r < nranges && rows[r] + (uint32_t)S <= (uint32_t)h &&
+                        cols[r] + (uint32_t)S <= (uint32_t)w;
+    uint8_t bytes[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        const int x = 16 * j + e;
+        int8_t val = 0;
+        if (inside && x < 2 * S) {
+            const int u = y >> 1, vv = x >> 1;
+            int i, jj;
+            switch (k) {
+                case 0: i = u; jj = vv; break;
+                case 1: i = S - 1 - vv; jj = u; break;
+                case 2: i = vv; jj = S - 1 - u; break;
+                case 3: i = S - 1 - u; jj = S - 1 - vv; break;
+                case 4: i = u; jj = S - 1 - vv; break;
+                case 5: i = S - 1 - u; jj = vv; break;
+                case 6: i = vv; jj = u; break;
+                default: i = S - 1 - vv; jj = S - 1 - u; break;
+            }
+            val = (int8_t)((int)plane[(size_t)(rows[r] + i) * w + cols[r] + jj] - 128);
+        }
+        bytes[e] = (uint8_t)val;
+    }
+    const size_t off = (((size_t)nt * KST + t) * 32 + (n >> 3)) * 1024 + (size_t)kgl * 128 +
+                       (size_t)(n & 7) * 16;
+    uint4 pk;
+    pk.x = bytes[0] | bytes[1] << 8 | bytes[2] << 16 | (uint32_t)bytes[3] << 24;
+    pk.y = bytes[4] | bytes[5] << 8 | bytes[6] << 16 | (uint32_t)bytes[7] << 24;
+    pk.z = bytes[8] | bytes[9] << 8 | bytes[10] << 16 | (uint32_t)bytes[11] << 24;
+    pk.w = bytes[12] | bytes[13] << 8 | bytes[14] << 16 | (uint32_t)bytes[15] << 24;
+    *reinterpret_cast<uint4*>(out + off) = pk;
+}
+
+// Phase copies of the plane: copy p (of P = 16 / shift) is the plane shifted left by
+// shift * p pixels, zero past the right edge; row pitch wp (a multiple of 16).
+__global__ void phase_planes_kernel(const uint8_t* __restrict__ plane, int w, int h, int wp,
+                                    int shift, int P, uint8_t* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int p = blockIdx.z;
+    if (x >= wp || y >= h || p >= P) return;
+    const int sx = x + shift * p;
+    out[((size_t)p * h + y) * wp + x] = sx < w ? plane[(size_t)y * w + sx] : 0;
+}
+
+// Seed champion of each range: the exact best of the 8 isometries at the 3 x 3 domain
+// positions around the range's own position (any real candidate is a valid champion; a
+// good one makes the filter tight from the first tile).  One warp per range.
+__global__ void seed_kernel(const int32_t* __restrict__ D, LevelGeom g, const uint8_t* __restrict__ plane,
+                            int w, const uint32_t* rows, const uint32_t* cols, int nranges,
+                            RangeStats rs, DomainStats ds, FitParams fp, SeedOut* __restrict__ out) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= nranges) return;
+    const int S = g.size, N = S * S;
+    if (rows[r] + (uint32_t)S > (uint32_t)g.h || cols[r] + (uint32_t)S > (uint32_t)g.w) {
+        if (lane == 0) out[r] = SeedOut{INFINITY, 0.0, UINT32_MAX, 0};
+        return;
+    }
+    const int ac = min(max(((int)rows[r] - S / 2 + g.shift / 2) / g.shift, 0), g.nrow_d - 1);
+    const int bc = min(max(((int)cols[r] - S / 2 + g.shift / 2) / g.shift, 0), g.ncol_d - 1);
+    double best_rms = INFINITY, best_sum = 0.0;
+    uint32_t best_idx = UINT32_MAX;
+    const uint8_t* rb = plane + (size_t)rows[r] * w + cols[r];
+    for (int cand = lane; cand < 72; cand += 32) {
+        const int k = cand & 7, nb = cand >> 3;
+        const int a = min(max(ac + nb / 3 - 1, 0), g.nrow_d - 1);
+        const int bb = min(max(bc + nb % 3 - 1, 0), g.ncol_d - 1);
+        const int32_t* db = D + (size_t)(a * g.step_c) * g.dw + bb * g.step_c;
+        int64_t t1 = 0;
+        for (int u = 0; u < S; ++u)
+            for (int v = 0; v < S; ++v) {
+                int i, j;
+                switch (k) {
+                    case 0: i = u; j = v; break;
+                    case 1: i = S - 1 - v; j = u; break;
+                    case 2: i = v; j = S - 1 - u; break;
+                    case 3: i = S - 1 - u; j = S - 1 - v; break;
+                    case 4: i = u; j = S - 1 - v; break;
+                    case 5: i = S - 1 - u; j = v; break;
+                    case 6: i = v; j = u; break;
+                    default: i = S - 1 - v; j = S - 1 - u; break;
+                }
+                t1 += (int64_t)rb[(size_t)i * w + j] * db[(size_t)u * g.dw + v];
+            }
+        const uint32_t dom = (uint32_t)(a * g.ncol_d + bb);
+        const FitResult f = fit_exact(N, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], t1, rs.t2[r], fp);
+        const uint32_t idx = dom * 8u + (uint32_t)k;
+        if (f.rms < best_rms || (f.rms == best_rms && idx < best_idx)) {
+            best_rms = f.rms;
+            best_sum = f.sum;
+            best_idx = idx;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double orms = __shfl_xor_sync(0xffffffffu, best_rms, off);
+        const double osum = __shfl_xor_sync(0xffffffffu, best_sum, off);
+        const uint32_t oidx = __shfl_xor_sync(0xffffffffu, best_idx, off);
+        if (orms < best_rms || (orms == best_rms && oidx < best_idx)) {
+            best_rms = orms;
+            best_sum = osum;
+            best_idx = oidx;
+        }
+    }
+    if (lane == 0) out[r] = SeedOut{best_rms, best_sum, best_idx, 0};
+}
+
+// Final champion over the M-splits, with the winner's moments recomputed exactly.
+__global__ void finish_kernel(const Partial* __restrict__ partials, int nsplit, int nranges,
+                              LevelGeom g, const int32_t* __restrict__ D,
+                              const uint8_t* __restrict__ plane, int w, const uint32_t* rows,
+                              const uint32_t* cols, RangeStats rs, DomainStats ds, FitParams fp,
+                              CandidateOut* __restrict__ out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nranges) return;
+    Partial best = partials[r];
+    for (int t = 1; t < nsplit; ++t) {
+        const Partial p = partials[(size_t)t * nranges + r];
+        if (p.rms < best.rms || (p.rms == best.rms && p.idx < best.idx)) best = p;
+    }
+    const int S = g.size;
+    if (best.idx == UINT32_MAX) {
+        out[r] = CandidateOut{0, 0, 0, 0, 0, 0, 0.0, 0, 0, 0, 0, 0, 0};
+        return;
+    }
+    const uint32_t dom = best.idx >> 3, k = best.idx & 7u;
+    const int a = (int)(dom / (uint32_t)g.ncol_d), bb = (int)(dom % (uint32_t)g.ncol_d);
+    const int32_t* db = D + (size_t)(a * g.step_c) * g.dw + bb * g.step_c;
+    const uint8_t* rb = plane + (size_t)rows[r] * w + cols[r];
+    int64_t t1 = 0;
+    for (int u = 0; u < S; ++u)
+        for (int v = 0; v < S; ++v) {
+            int i, j;
+            switch (k) {
+                case 0: i = u; j = v; break;
+                case 1: i = S - 1 - v; j = u; break;
+                case 2: i = v; j = S - 1 - u; break;
+                case 3: i = S - 1 - u; j = S - 1 - v; break;
+                case 4: i = u; j = S - 1 - v; break;
+                case 5: i = S - 1 - u; j = v; break;
+                case 6: i = v; j = u; break;
+                default: i = S - 1 - v; j = S - 1 - u; break;
+            }
+            t1 += (int64_t)rb[(size_t)i * w + j] * db[(size_t)u * g.dw + v];
+        }
+    const int64_t n = (int64_t)S * S;
+    const FitResult f = fit_exact(n, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], t1, rs.t2[r], fp);
+    CandidateOut c;
+    c.dom_row = (uint32_t)a * (uint32_t)g.shift;
+    c.dom_col = (uint32_t)bb * (uint32_t)g.shift;
+    c.isometry = k;
+    c.qalfa = f.qalfa;
+    c.qbeta = f.qbeta;
+    c.valid = 1;
+    c.rms = f.rms;
+    c.s0 = n;
+    c.s1_x4 = ds.s1x4[dom];
+    c.s2_x16 = ds.s2x16[dom];
+    c.t0 = rs.t0[r];
+    c.t1_x4 = t1;
+    c.t2 = rs.t2[r];
+    out[r] = c;
+}
+
+template <int S>
+size_t smem_bytes() {
+    constexpr int J = S >= 8 ? S / 8 : 1;
+    constexpr int KST = J * 2 * S / 8;
+    constexpr bool kBRes = KST <= 2;
+    return 1024 + (size_t)kStages * kStageA + (kBRes ? (size_t)KST * kStageB : (size_t)kStages * kStageB) +
+           sizeof(Smem);
+}
+
+template <int S>
+cudaError_t launch_t(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
+                     RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
+                     Partial* partials, int msplit, int* err, unsigned long long* counter,
+                     cudaStream_t st) {
+    const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
+    const int m_tiles = g.nrow_d * tiles_per_row;
+    const int m_per_cta = (m_tiles + msplit - 1) / msplit;
+    const int ntiles = (nranges + kRangesPerTile - 1) / kRangesPerTile;
+    const size_t smem = smem_bytes<S>();
+    auto kern = corr_tc_kernel<S>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(ntiles, msplit);
+    kern<<<grid, kThreads, smem, st>>>(maps, bglob, g, nranges, rs, ds, fp, seeds, m_tiles,
+                                      m_per_cta, partials, err, counter);
+    return cudaGetLastError();
+}
+
+template <int S>
+cudaError_t build_b_t(const uint8_t* plane, int w, int h, const uint32_t* rows,
+                      const uint32_t* cols, int nranges, uint8_t* out, cudaStream_t st) {
+    constexpr int J = S >= 8 ? S / 8 : 1;
+    constexpr int KG = J * 2 * S;
+    const int ntiles = (nranges + kRangesPerTile - 1) / kRangesPerTile;
+    const long long total = (long long)ntiles * kN * KG;
+    build_b_kernel<S><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(plane, w, h, rows, cols,
+                                                                       nranges, ntiles, out);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool supported(int size, int shift) {
+    return (size == 4 || size == 8 || size == 16 || size == 32 || size == 64) &&
+           (shift == 2 || shift == 4 || shift == 8 || shift == 16);
+}
+
+size_t b_bytes(int size, int nranges) {
+    const int J = size >= 8 ? size / 8 : 1;
+    const int KG = J * 2 * size;
+    const size_t ntiles = (size_t)(nranges + kRangesPerTile - 1) / kRangesPerTile;
+    return ntiles * (size_t)kN * (size_t)KG * 16;
+}
+
+int phase_count(int shift) { return 16 / shift; }
+int row_pitch(int w) { return ((w + 15) / 16) * 16 + 16; }
+
+cudaError_t launch_phase_planes(const uint8_t* plane, int w, int h, int shift, uint8_t* out,
+                                cudaStream_t st) {
+    const int P = phase_count(shift), wp = row_pitch(w);
+    dim3 grid((wp + 255) / 256, h, P);
+    phase_planes_kernel<<<grid, 256, 0, st>>>(plane, w, h, wp, shift, P, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_b(int size, const uint8_t* plane, int w, int h, const uint32_t* rows,
+                           const uint32_t* cols, int nranges, uint8_t* out, cudaStream_t st) {
+    switch (size) {
+        case 4: return build_b_t<4>(plane, w, h, rows, cols, nranges, out, st);
+        case 8: return build_b_t<8>(plane, w, h, rows, cols, nranges, out, st);
+        case 16: return build_b_t<16>(plane, w, h, rows, cols, nranges, out, st);
+        case 32: return build_b_t<32>(plane, w, h, rows, cols, nranges, out, st);
+        case 64: return build_b_t<64>(plane, w, h, rows, cols, nranges, out, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_seed(const int32_t* D, const LevelGeom& g, const uint8_t* plane, int w,
+                        const uint32_t* rows, const uint32_t* cols, int nranges, RangeStats rs,
+                        DomainStats ds, const FitParams& fp, SeedOut* out, cudaStream_t st) {
+    const long long threads = (long long)nranges * 32;
+    seed_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(D, g, plane, w, rows, cols,
+                                                                   nranges, rs, ds, fp, out);
+    return cudaGetLastError();
+}
+
+int msplit_for(const LevelGeom& g, int nranges, int num_sms) {
+    const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
+    const int m_tiles = g.nrow_d * tiles_per_row;
+    const int ntiles = (nranges + kRangesPerTile - 1) / kRangesPerTile;
+    const int want = (2 * num_sms + ntiles - 1) / ntiles;
+    return want < 1 ? 1 : (want > m_tiles ? m_tiles : want);
+}
+
+cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
+                        RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
+                        Partial* partials, int msplit, int* err, unsigned long long* counter,
+                        cudaStream_t st) {
+    switch (g.size) {
+        case 4: return launch_t<4>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st);
+        case 8: return launch_t<8>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st);
+        case 16: return launch_t<16>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st);
+        case 32: return launch_t<32>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st);
+        case 64: return launch_t<64>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,
+                          const int32_t* D, const uint8_t* plane, int w, const uint32_t* rows,
+                          const uint32_t* cols, RangeStats rs, DomainStats ds, const FitParams& fp,
+                          CandidateOut* out, cudaStream_t st) {
+    finish_kernel<<<(nranges + 127) / 128, 128, 0, st>>>(partials, nsplit, nranges, g, D, plane, w,
+                                                         rows, cols, rs, ds, fp, out);
+    return cudaGetLastError();
+}
+
+}  // namespace tc
+}  // namespace mars

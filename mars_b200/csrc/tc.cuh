@@ -1,0 +1,49 @@
+// Launch interface of the tcgen05 correlation path (search_tc.cu).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace mars {
+namespace tc {
+
+constexpr int kStages = 3;     // shared-memory pipeline depth (A, and B when streamed)
+constexpr int kMaxPhases = 8;  // 16 / shift for shift = 2
+
+// One 2-D TMA descriptor per phase copy of the plane (u8, row pitch a multiple of 16,
+// box 128 B x 8 rows, no swizzle, zero fill out of bounds).
+struct alignas(64) TcMaps {
+    CUtensorMap m[kMaxPhases];
+};
+
+struct SeedOut {
+    double rms, sum;
+    uint32_t idx, pad;
+};
+
+bool supported(int size, int shift);
+int phase_count(int shift);
+int row_pitch(int w);
+size_t b_bytes(int size, int nranges);
+int msplit_for(const LevelGeom& g, int nranges, int num_sms);
+
+cudaError_t launch_phase_planes(const uint8_t* plane, int w, int h, int shift, uint8_t* out,
+                                cudaStream_t st);
+cudaError_t launch_build_b(int size, const uint8_t* plane, int w, int h, const uint32_t* rows,
+                           const uint32_t* cols, int nranges, uint8_t* out, cudaStream_t st);
+cudaError_t launch_seed(const int32_t* D, const LevelGeom& g, const uint8_t* plane, int w,
+                        const uint32_t* rows, const uint32_t* cols, int nranges, RangeStats rs,
+                        DomainStats ds, const FitParams& fp, SeedOut* out, cudaStream_t st);
+cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
+                        RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
+                        Partial* partials, int msplit, int* err, unsigned long long* counter,
+                        cudaStream_t st);
+cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,
+                          const int32_t* D, const uint8_t* plane, int w, const uint32_t* rows,
+                          const uint32_t* cols, RangeStats rs, DomainStats ds, const FitParams& fp,
+                          CandidateOut* out, cudaStream_t st);
+
+}  // namespace tc
+}  // namespace mars

@@ -197,3 +197,47 @@ def test_invalid_arguments_are_rejected(ctx):
     bad[0] = (0, 0, 8, 2, 3, 10, 0, 60, 0, 0, 0)  # domain runs past a 64x64 plane
     with pytest.raises(mb.MarsError):
         ctx.decode(mb.Header(4, 7, 4, 16, 4, 64, 64, 32), bad, 2)
+
+
+@pytest.mark.parametrize("shift", [2, 4, 8, 16])
+def test_tensor_core_path_equals_cuda_core_path(ctx, shift):
+    # Same blocks through the tcgen05 correlation and through the CUDA-core correlation:
+    # identical records, and identical to the oracle.
+    img = synthetic.gray(288, 224, 9)
+    simt = mb.Context(0)
+    simt.set_search_path("simt")
+    try:
+        for size in (4, 8, 16, 32, 64):
+            if 2 * size > 224:
+                continue
+            p = mb.make_params(shift=shift)
+            a, aev = ctx.search_grid(img, size, shift, p)
+            b, bev = simt.search_grid(img, size, shift, p)
+            assert np.array_equal(aev, bev)
+            assert a.tobytes() == b.tobytes(), (size, shift)
+    finally:
+        simt.close()
+    o, _ = orc.search_grid(img, 8, shift, orc.make_params(shift=shift))
+    a, _ = ctx.search_grid(img, 8, shift, mb.make_params(shift=shift))
+    assert a.tobytes() == o.tobytes()
+
+
+def test_device_entry_rejects_blocks_outside_the_plane(ctx):
+    # Out-of-plane origins handed to the device-pointer entry are never read and come
+    # back invalid, on both correlation paths.
+    import torch
+    img = synthetic.gray(128, 128, 3)
+    d_img = torch.from_numpy(img).cuda()
+    rows = torch.tensor([0, 124, 120], dtype=torch.int32, device="cuda")
+    cols = torch.tensor([0, 0, 124], dtype=torch.int32, device="cuda")
+    out = torch.zeros((3, 80), dtype=torch.uint8, device="cuda")
+    p = mb.make_params(shift=2)
+    torch.cuda.synchronize()
+    mb.check(mb.lib().mars_search_blocks_device(ctx.handle, d_img.data_ptr(), 128, 128, 8, 2,
+                                                mb.C.byref(p), rows.data_ptr(), cols.data_ptr(),
+                                                3, out.data_ptr()))
+    torch.cuda.synchronize()
+    rec = out.cpu().numpy().view(mb.CANDIDATE_DTYPE).ravel()
+    assert rec[0]["valid"] == 1 and rec[1]["valid"] == 0 and rec[2]["valid"] == 0
+    o, _ = orc.search(img, 0, 0, 8, 2, orc.make_params(shift=2))
+    assert rec[0].tobytes() == o[0].tobytes()
