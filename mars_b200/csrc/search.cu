@@ -25,8 +25,9 @@ namespace {
 
 constexpr float kHugeDet = 1.0e30f;
 constexpr float kHugeSqrtDet = 1.0e15f;
-constexpr int kTileRows = 16;  // domain positions per tile, vertically
-constexpr int kTileCols = 32;  // and horizontally
+constexpr int kTileRowsMax = 16;  // domain positions per tile, vertically
+constexpr int kTileColsMax = 32;  // and horizontally
+constexpr size_t kSmemBudget = 200 * 1024;
 
 // isometry::map (crates/mars-codec/src/isometry.rs:7-19) as a flat range index i*S + j.
 __host__ __device__ constexpr int iso_src(int k, int u, int v, int S) {
@@ -123,19 +124,19 @@ __global__ void __launch_bounds__(RPB) search_simt_kernel(
     const int32_t* __restrict__ D, LevelGeom g, const uint8_t* __restrict__ plane, int w,
     const uint32_t* __restrict__ rows, const uint32_t* __restrict__ cols, int nranges,
     RangeStats rs, DomainStats ds, FitParams fp, Partial* __restrict__ partials, int tiles_c,
-    int ntiles, unsigned long long* __restrict__ exact_counter) {
+    int ntiles, int tile_rows, int tile_cols, unsigned long long* __restrict__ exact_counter) {
     constexpr int N = S * S;
     constexpr bool kRegs = S <= 8;
     extern __shared__ __align__(16) unsigned char smem[];
 
     const int step = g.step_c;
-    const int strip_ld = (kTileCols - 1) * step + S;
-    const int strip_rows_max = (kTileRows - 1) * step + S;
+    const int strip_ld = (tile_cols - 1) * step + S;
+    const int strip_rows_max = (tile_rows - 1) * step + S;
     int32_t* Ds = reinterpret_cast<int32_t*>(smem);
     float* s1s = reinterpret_cast<float*>(Ds + strip_rows_max * strip_ld);
-    float* dets = s1s + kTileRows * kTileCols;
-    float* sdets = dets + kTileRows * kTileCols;
-    uint8_t* Rs = reinterpret_cast<uint8_t*>(sdets + kTileRows * kTileCols);
+    float* dets = s1s + tile_rows * tile_cols;
+    float* sdets = dets + tile_rows * tile_cols;
+    uint8_t* Rs = reinterpret_cast<uint8_t*>(sdets + tile_rows * tile_cols);
 
     const int tid = threadIdx.x;
     const int r = blockIdx.x * RPB + tid;
@@ -175,8 +176,8 @@ __global__ void __launch_bounds__(RPB) search_simt_kernel(
     unsigned long long exact = 0;
 
     for (int tile = blockIdx.y; tile < ntiles; tile += gridDim.y) {
-        const int a0 = (tile / tiles_c) * kTileRows, b0 = (tile % tiles_c) * kTileCols;
-        const int na = min(kTileRows, g.nrow_d - a0), nb = min(kTileCols, g.ncol_d - b0);
+        const int a0 = (tile / tiles_c) * tile_rows, b0 = (tile % tiles_c) * tile_cols;
+        const int na = min(tile_rows, g.nrow_d - a0), nb = min(tile_cols, g.ncol_d - b0);
         const int strip_h = (na - 1) * step + S, strip_w = (nb - 1) * step + S;
         __syncthreads();
         for (int i = tid; i < strip_h * strip_w; i += RPB) {
@@ -186,9 +187,9 @@ __global__ void __launch_bounds__(RPB) search_simt_kernel(
         for (int i = tid; i < na * nb; i += RPB) {
             const int da = i / nb, db = i % nb;
             const int dom = (a0 + da) * g.ncol_d + (b0 + db);
-            s1s[da * kTileCols + db] = (float)ds.s1x4[dom];
-            dets[da * kTileCols + db] = ds.detf[dom];
-            sdets[da * kTileCols + db] = ds.sdetf[dom];
+            s1s[da * tile_cols + db] = (float)ds.s1x4[dom];
+            dets[da * tile_cols + db] = ds.detf[dom];
+            sdets[da * tile_cols + db] = ds.sdetf[dom];
         }
         __syncthreads();
         if (!active) continue;
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(RPB) search_simt_kernel(
                         }
                     }
                 }
-                const int li = da * kTileCols + db;
+                const int li = da * tile_cols + db;
                 const uint32_t dom = (uint32_t)((a0 + da) * g.ncol_d + (b0 + db));
                 const int32_t lim = prune_below(th, dom, s1s[li], t0f, dets[li], sdets[li], inv_n, fp);
                 int mx = acc[0];
@@ -293,16 +294,34 @@ __global__ void reduce_kernel(const Partial* __restrict__ partials, int ntiles, 
     out[r] = c;
 }
 
+int rpb_for(int size) { return size <= 16 ? 64 : (size == 32 ? 32 : 16); }
+
+// Domain tile of the CUDA-core kernel: as large as 16 x 32 positions while the staged
+// strip, the per-domain statistics and the range pixels stay within the budget.
+void simt_tile(int S, int step, int rpb, int* tr, int* tcn) {
+    int r = kTileRowsMax, c = kTileColsMax;
+    for (;;) {
+        const size_t strip = (size_t)((c - 1) * step + S) * ((r - 1) * step + S) * 4;
+        const size_t smem = strip + 3 * (size_t)r * c * 4 + (S > 8 ? (size_t)S * S * rpb : 0);
+        if (smem <= kSmemBudget || (r == 1 && c == 1)) break;
+        if (c >= r && c > 1) c /= 2; else r /= 2;
+    }
+    *tr = r;
+    *tcn = c;
+}
+
 template <int S, int RPB>
 cudaError_t launch_simt_t(const int32_t* D, const uint8_t* plane, int w, const uint32_t* rows,
                           const uint32_t* cols, int nranges, const LevelGeom& g, RangeStats rs,
                           DomainStats ds, const FitParams& fp, Partial* partials, int nsplit,
                           unsigned long long* counter, cudaStream_t st) {
-    const int tiles_c = (g.ncol_d + kTileCols - 1) / kTileCols;
-    const int ntiles = search_simt_tiles(g);
-    const int strip_ld = (kTileCols - 1) * g.step_c + S;
-    const int strip_rows = (kTileRows - 1) * g.step_c + S;
-    size_t smem = (size_t)strip_ld * strip_rows * 4 + 3 * kTileRows * kTileCols * 4;
+    int tr, tcn;
+    simt_tile(S, g.step_c, RPB, &tr, &tcn);
+    const int tiles_c = (g.ncol_d + tcn - 1) / tcn;
+    const int ntiles = ((g.nrow_d + tr - 1) / tr) * tiles_c;
+    const int strip_ld = (tcn - 1) * g.step_c + S;
+    const int strip_rows = (tr - 1) * g.step_c + S;
+    size_t smem = (size_t)strip_ld * strip_rows * 4 + 3 * (size_t)tr * tcn * 4;
     if (S > 8) smem += (size_t)S * S * RPB;
     auto kern = search_simt_kernel<S, RPB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -310,11 +329,9 @@ cudaError_t launch_simt_t(const int32_t* D, const uint8_t* plane, int w, const u
     if (e != cudaSuccess) return e;
     dim3 grid((nranges + RPB - 1) / RPB, nsplit);
     kern<<<grid, RPB, smem, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, partials,
-                                  tiles_c, ntiles, counter);
+                                  tiles_c, ntiles, tr, tcn, counter);
     return cudaGetLastError();
 }
-
-int rpb_for(int size) { return size <= 16 ? 64 : (size == 32 ? 32 : 16); }
 
 }  // namespace
 
@@ -344,7 +361,9 @@ cudaError_t launch_range_stats(const uint8_t* plane, int w, int h, const uint32_
 }
 
 int search_simt_tiles(const LevelGeom& g) {
-    return ((g.nrow_d + kTileRows - 1) / kTileRows) * ((g.ncol_d + kTileCols - 1) / kTileCols);
+    int tr, tcn;
+    simt_tile(g.size, g.step_c, rpb_for(g.size), &tr, &tcn);
+    return ((g.nrow_d + tr - 1) / tr) * ((g.ncol_d + tcn - 1) / tcn);
 }
 
 int search_simt_splits(const LevelGeom& g, int nranges, int num_sms) {

@@ -282,8 +282,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             R.idx = sd.idx;
             R.th = make_threshold(R.sum, R.rms, R.idx >> 3, R.rms0, R.nrr, N, fp);
         } else {
-            R.rms = 0.0;
-            R.idx = 0;
+            // Padding of the last N tile, or a block outside the plane: no candidate.
+            R.rms = INFINITY;
+            R.sum = 0.0;
+            R.idx = UINT32_MAX;
         }
     }
     if (warp == 1) {
