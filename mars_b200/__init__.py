@@ -235,8 +235,10 @@ class Context:
         check(lib().mars_ctx_set_stream(self._h, C.c_void_p(stream_ptr)))
 
     def set_search_path(self, path: str) -> None:
-        """'auto' (tensor cores wherever a level allows) or 'simt' (CUDA cores only)."""
-        check(lib().mars_ctx_set_search_path(self._h, {"auto": 0, "simt": 1, "tc": 2}[path]))
+        """'auto' (tensor cores wherever a level allows), 'simt' (CUDA cores only) or
+        'boxes' (tensor cores, operand stages loaded as per-phase boxes)."""
+        check(lib().mars_ctx_set_search_path(self._h, {"auto": 0, "simt": 1, "tc": 2,
+                                                       "boxes": 3}[path]))
 
     @property
     def launches(self) -> int:

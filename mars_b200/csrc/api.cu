@@ -53,6 +53,7 @@ struct mars_ctx {
     unsigned long long* d_counter = nullptr;  // survivors that took the exact f64 fit
     int* d_err = nullptr;                     // kernel-side error bits (bounded waits)
     int search_path = 0;                      // 0 auto, 1 CUDA cores only, 2 tensor cores
+    bool tma_16_boxes = false;                // load A stages as 16 2-D boxes (A/B checks)
     PFN_cuTensorMapEncodeTiled_v12000 encode_tiled = nullptr;
 };
 
@@ -213,6 +214,18 @@ int make_maps(mars_ctx* ctx, const uint8_t* d_phases, uint32_t w, uint32_t h, ui
         if (r != CUDA_SUCCESS)
             return fail(MARS_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
     }
+    // One box for the whole stage: (bytes, pixel rows, same-phase 128-byte groups, phases).
+    const uint32_t per_phase = 16u / (uint32_t)P;
+    const cuuint64_t dims4[4] = {wp, h, per_phase, (cuuint64_t)P};
+    const cuuint64_t strides4[3] = {wp, 128, (cuuint64_t)h * wp};
+    const cuuint32_t box4[4] = {128, 8, per_phase, (cuuint32_t)P};
+    const cuuint32_t estr4[4] = {1, 1, 1, 1};
+    const CUresult r4 = ctx->encode_tiled(&maps->all, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4,
+                                          (void*)d_phases, dims4, strides4, box4, estr4,
+                                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    maps->use_all = (r4 == CUDA_SUCCESS && !ctx->tma_16_boxes) ? 1 : 0;
     return MARS_OK;
 }
 
@@ -227,7 +240,7 @@ int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32
     uint8_t* d_phases = nullptr;
     uint8_t* d_b = nullptr;
     mars::tc::SeedOut* d_seed = nullptr;
-    MARS_CUDA(sc.get(&d_phases, (size_t)P * h * mars::tc::row_pitch((int)w)));
+    MARS_CUDA(sc.get(&d_phases, mars::tc::phase_bytes((int)w, (int)h, g.shift)));
     MARS_CUDA(sc.get(&d_b, mars::tc::b_bytes(g.size, (int)n)));
     MARS_CUDA(sc.get(&d_seed, n));
     const int msplit = mars::tc::msplit_for(g, (int)n, ctx->num_sms);
@@ -515,9 +528,10 @@ int mars_ctx_set_stream(mars_ctx* ctx, void* stream) {
 uint64_t mars_ctx_launch_count(const mars_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
 
 int mars_ctx_set_search_path(mars_ctx* ctx, int32_t path) {
-    if (!ctx || path < 0 || path > 2) return fail(MARS_EINVAL, "path must be 0, 1 or 2");
+    if (!ctx || path < 0 || path > 3) return fail(MARS_EINVAL, "path must be 0, 1, 2 or 3");
     std::lock_guard<std::mutex> lock(ctx->mu);
-    ctx->search_path = path;
+    ctx->search_path = path == 3 ? 0 : path;
+    ctx->tma_16_boxes = path == 3;
     return MARS_OK;
 }
 

@@ -25,12 +25,13 @@
 // pre-built in global memory in the same core-matrix order and copied with 1-D bulk
 // copies.
 //
-// Warp roles (256 threads): warp 0 issues the loads, warp 1 owns TMEM and issues the MMAs
-// (one elected lane), warps 4-7 are the epilogue (TMEM lane quadrant = warp % 4).  The
-// accumulator is double-buffered in TMEM (2 x 256 columns).  The epilogue runs the
-// pruning test of fit.cuh once per (domain lane, range) -- shared by the 8 isometry
-// columns -- and queues survivors per range in shared memory; one warp per range then
-// runs the exact f64 fit on them and updates that range's champion and threshold.
+// Warp roles (320 threads): warp 0 issues the loads, warp 1 owns TMEM and issues the MMAs
+// (one elected lane), warps 2-9 are the epilogue (TMEM lane quadrant = warp % 4, two warps
+// per quadrant splitting the 256 columns).  The accumulator is double-buffered in TMEM
+// (2 x 256 columns).  The epilogue runs the pruning test of fit.cuh once per (domain
+// lane, range) -- shared by the 8 isometry columns -- and queues survivors in shared
+// memory; batches of survivors get the exact f64 fit and update the ranges' champions
+// and thresholds.
 // Every mbarrier wait is bounded (clock64 deadline): on expiry the kernel records an
 // error, stops issuing work, waits (bounded) for its own loads, frees TMEM and returns.
 #include <cuda.h>
@@ -45,14 +46,20 @@ namespace mars {
 namespace tc {
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 320;                   // 10 warps: load, MMA, 8 epilogue
+constexpr int kEpiThreads = 256;
 constexpr int kM = 128;
 constexpr int kN = 256;
-constexpr int kRangesPerTile = kN / 8;     // 32
-constexpr int kStageA = 16 * 1024;         // 16 row groups x 8 K-groups x 128 B
-constexpr int kStageB = 32 * 1024;         // 32 row groups x 8 K-groups x 128 B
-constexpr int kQueueCap = kM * 8;          // survivors of one range in one 32-column chunk
+constexpr int kRangesPerTile = kN / 8;         // 32
+constexpr int kStageA = 16 * 1024;             // 16 row groups x 8 K-groups x 128 B
+constexpr int kStageB = 32 * 1024;             // 32 row groups x 8 K-groups x 128 B
+constexpr int kQueueCap = 2048;                // survivors the queue can hold
+constexpr int kFlush = 256;                    // drain the queue once it holds this many
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 1.965 GHz
+
+// Pipeline depth: as many A stages as fit beside the resident B tile (S <= 8), otherwise
+// three stages of A + B.
+__host__ __device__ constexpr int stages_for(int S) { return S == 4 ? 6 : (S == 8 ? 4 : 3); }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -72,14 +79,17 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// One bounded poll of an mbarrier phase.  The suspend-time hint lets the hardware park
+// the waiting thread until the phase completes (or ~20 us pass) instead of spinning, so
+// waiting warps leave the issue slots to the epilogue warps sharing their scheduler.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
         : "memory");
     return ok != 0;
 }
@@ -105,6 +115,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
         " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
         "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(0), "r"(0), "r"(smem_u32(bar))
         : "memory");
 }
 
@@ -153,6 +172,9 @@ __device__ __forceinline__ void tmem_fence_after() {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
+// TMEM -> registers, 32 columns of this warp's 32 lanes.  The load completes
+// asynchronously: tmem_wait() names the destination registers as read-write operands so
+// no consumer can be scheduled ahead of it.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int32_t (&v)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
@@ -164,19 +186,30 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int32_t (&v)[32]) {
           "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
           "=r"(v[31])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ void epi_barrier() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait(int32_t (&v)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]),
+                   "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]),
+                   "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15]), "+r"(v[16]), "+r"(v[17]),
+                   "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]), "+r"(v[22]), "+r"(v[23]),
+                   "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]), "+r"(v[29]),
+                   "+r"(v[30]), "+r"(v[31])
+                 :
+                 : "memory");
+}
 
-// Named barrier over the 4 epilogue warps that also ANDs a predicate across them, so the
+__device__ __forceinline__ void epi_barrier() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+// Named barrier over the 8 epilogue warps that also ANDs a predicate across them, so the
 // warps always agree on whether to go on.
 __device__ __forceinline__ bool epi_barrier_and(bool pred) {
     uint32_t out;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.and.pred q, 1, 128, p;\n\t"
+        "bar.red.and.pred q, 1, 256, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}"
         : "=r"(out)
         : "r"((uint32_t)pred)
@@ -184,42 +217,138 @@ __device__ __forceinline__ bool epi_barrier_and(bool pred) {
     return out != 0;
 }
 
-// Per-range state shared by the epilogue warps.
-struct RangeRec {
-    double rms;      // champion rms (reference order: smaller rms, then smaller idx)
-    double sum;      // champion f64 sum
-    double rms0;     // rms of any qalfa == 0 fit of this range
+// Champion of one range block (reference order: smaller rms, then smaller index).
+struct Champ {
+    double rms, sum, rms0;
     int64_t nrr;
-    uint32_t idx;    // champion reference index dom * 8 + isometry
-    int32_t t0, t2;
-    float c;         // t0 / n - 128 (exact)
-    Threshold th;
-    int32_t valid;
+    uint32_t idx;
+    int32_t t0, t2, valid;
 };
 
+// The per-range pruning record the epilogue reads for every (domain lane, range) pair,
+// branch-free form of prune_below (fit.cuh):
+//   g1 = sqrt_w * sqrt(Ndd);  tau_z = min(w2a + a_half*Ndd, max(g1, a_min*Ndd));
+//   tau = (dom > tie) ? tau_z : g1 + neg;   prune  <=>  t1' < s1_x4 * c + 4 tau / n.
+// tie = -1 puts every domain in the Z-form, INT32_MAX none; neg = 0 or -inf (W <= 0).
+struct __align__(16) ThrRec {
+    float sqrt_w, w2a, neg, c;  // sqrt_w, w2a, neg pre-scaled by 4 / n (exact: n = 4^k)
+    int32_t tie, pad0, pad1, pad2;
+};
+
+// A survivor waiting for its exact fit.  Survivors of several tiles are batched: the
+// queue is drained when it holds kFlush entries, when a tile overflows it, and at the end.
 struct __align__(8) QEntry {
     int32_t t1;     // t1' = t1_x4 - 128 * s1_x4
-    uint32_t code;  // lane << 3 | isometry
+    uint32_t dom;   // domain position index (row-major)
+    uint32_t code;  // tile tag << 16 | lane << 8 | tile column (range * 8 + iso)
+    uint32_t pad;
+    double rms, sum;
 };
 
 struct Smem {
-    uint64_t full[kStages];
-    uint64_t empty[kStages];
+    uint64_t full[kMaxStages];
+    uint64_t empty[kMaxStages];
     uint64_t tfull[2];
     uint64_t tempty[2];
     uint64_t bres;
     uint32_t tmem_base;
     int abort_flag;
-    int qcount[2][4];
-    RangeRec rec[kRangesPerTile];
-    QEntry queue[4][kQueueCap];
+    int qcount;
+    int overflow_seen;
+    unsigned long long key_rms[kRangesPerTile];  // per-pass winner: f64 bits (rms >= 0)
+    uint32_t key_idx[kRangesPerTile];
+    double key_sum[kRangesPerTile];
+    ThrRec thr[kRangesPerTile];
+    Champ ch[kRangesPerTile];
+    uint32_t evaluated[kM * kN / 32];           // candidates already fitted in this tile
+    QEntry queue[kQueueCap];
 };
 
-__device__ __forceinline__ void domain_of_lane(int m, int P, int tile_q0, int* c) {
+__device__ __forceinline__ int domain_of_lane(int m, int P, int tile_q0) {
     const int g = m >> 3, r8 = m & 7;
     const int per_phase = 16 / P;
     const int p = g / per_phase, h = g % per_phase;
-    *c = P * (tile_q0 + 8 * h + r8) + p;
+    return P * (tile_q0 + 8 * h + r8) + p;
+}
+
+__device__ __forceinline__ void publish_threshold(Smem& sm, int rl, const FitParams& fp, int n) {
+    const Champ& C = sm.ch[rl];
+    ThrRec t;
+    if (!C.valid) {
+        // An invalid range never survives: c = +huge makes every threshold unreachable.
+        t = ThrRec{0.0f, 0.0f, 0.0f, 3.0e38f, INT32_MAX, 0, 0, 0};
+        sm.thr[rl] = t;
+        return;
+    }
+    const Threshold th = make_threshold(C.sum, C.rms, C.idx >> 3, C.rms0, C.nrr, n, fp);
+    // Scaling by 4 / n (a power of two) is exact, so folding it in keeps every bound
+    // rounded toward -inf.
+    const float four_inv_n = 4.0f / (float)n;
+    t.sqrt_w = th.sqrt_w * four_inv_n;
+    t.w2a = th.w2a * four_inv_n;
+    t.neg = th.wpos ? 0.0f : -INFINITY;
+    t.c = (float)C.t0 / (float)n - 128.0f;  // exact: t0 < 2^24, n a power of four
+    t.tie = th.mode == 2 ? -1 : (th.mode == 1 ? (int32_t)th.tie_dom : INT32_MAX);
+    t.pad0 = t.pad1 = t.pad2 = 0;
+    sm.thr[rl] = t;
+}
+
+// Exact fits of every queued survivor, then the per-range winners of the batch (atomic
+// min on the f64 bit pattern of rms >= 0, then on the reference index) and the champion /
+// threshold update.  All 256 epilogue threads call this together.
+template <int N>
+__device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t tag, int et,
+                                         const DomainStats& ds, const FitParams& fp,
+                                         unsigned long long& exact) {
+    for (int qi = et; qi < n; qi += kEpiThreads) {
+        QEntry& q = sm.queue[qi];
+        const int rl = (int)(q.code & 255u) >> 3;
+        const Champ& C = sm.ch[rl];
+        const int32_t s1 = ds.s1x4[q.dom];
+        const int64_t t1x4 = (int64_t)q.t1 + 128ll * s1;
+        const FitResult f = fit_exact(N, s1, ds.s2x16[q.dom], C.t0, t1x4, C.t2, fp);
+        q.rms = f.rms;
+        q.sum = f.sum;
+        ++exact;
+        atomicMin(&sm.key_rms[rl], (unsigned long long)__double_as_longlong(f.rms));
+    }
+    epi_barrier();
+    for (int qi = et; qi < n; qi += kEpiThreads) {
+        const QEntry& q = sm.queue[qi];
+        const int col = (int)(q.code & 255u), rl = col >> 3;
+        if ((unsigned long long)__double_as_longlong(q.rms) == sm.key_rms[rl])
+            atomicMin(&sm.key_idx[rl], q.dom * 8u + (uint32_t)(col & 7));
+    }
+    epi_barrier();
+    for (int qi = et; qi < n; qi += kEpiThreads) {
+        const QEntry& q = sm.queue[qi];
+        const int col = (int)(q.code & 255u), rl = col >> 3;
+        if ((unsigned long long)__double_as_longlong(q.rms) == sm.key_rms[rl] &&
+            q.dom * 8u + (uint32_t)(col & 7) == sm.key_idx[rl])
+            sm.key_sum[rl] = q.sum;
+        if (mark && (q.code >> 16) == tag) {
+            // The tile overflowed the queue: remember what was fitted so the next pass
+            // over the same accumulator only queues candidates not yet seen.
+            const int qm = (int)(q.code >> 8) & 127;
+            atomicOr(&sm.evaluated[(qm * kN + col) >> 5], 1u << (col & 31));
+        }
+    }
+    epi_barrier();
+    if (et < kRangesPerTile && sm.key_rms[et] != ~0ull) {
+        Champ& C = sm.ch[et];
+        const double r2 = __longlong_as_double((long long)sm.key_rms[et]);
+        const uint32_t i2 = sm.key_idx[et];
+        if (r2 < C.rms || (r2 == C.rms && i2 < C.idx)) {
+            C.rms = r2;
+            C.idx = i2;
+            C.sum = sm.key_sum[et];
+            publish_threshold(sm, et, fp, N);
+        }
+        sm.key_rms[et] = ~0ull;
+        sm.key_idx[et] = UINT32_MAX;
+    }
+    if (et == 0) sm.qcount = 0;
+    epi_barrier();
 }
 
 template <int S>
@@ -234,8 +363,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr int ROWS = 2 * S;            // pixel rows of a domain block
     constexpr int KST = J * ROWS / 8;      // 128-byte K stages per tile
     constexpr bool kBRes = KST <= 2;       // B tile stays resident in shared memory
-    constexpr uint32_t kTxA = kStageA;
-    constexpr uint32_t kTxStage = kBRes ? kTxA : kTxA + kStageB;
+    constexpr int kStages = stages_for(S);
+    constexpr uint32_t kTxStage = kBRes ? kStageA : kStageA + kStageB;
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -259,34 +388,37 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&sm.tfull[b], 1);
-            mbar_init(&sm.tempty[b], 128);
+            mbar_init(&sm.tempty[b], kEpiThreads);
         }
         mbar_init(&sm.bres, 1);
         sm.abort_flag = 0;
-        for (int q = 0; q < 4; ++q) sm.qcount[0][q] = sm.qcount[1][q] = 0;
+        sm.qcount = 0;
+        sm.overflow_seen = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    for (int i = threadIdx.x; i < kM * kN / 32; i += kThreads) sm.evaluated[i] = 0u;
     if (threadIdx.x < kRangesPerTile) {
-        RangeRec& R = sm.rec[threadIdx.x];
+        Champ& C = sm.ch[threadIdx.x];
         const int r = ntile * kRangesPerTile + threadIdx.x;
-        R.valid = r < nranges && seeds[r].idx != UINT32_MAX;
-        if (R.valid) {
-            R.t0 = rs.t0[r];
-            R.t2 = rs.t2[r];
-            R.nrr = rs.nrr[r];
-            R.rms0 = rs.rms0[r];
-            R.c = (float)R.t0 / (float)N - 128.0f;  // exact: t0 < 2^24, N a power of four
+        C.valid = r < nranges && seeds[r].idx != UINT32_MAX;
+        if (C.valid) {
+            C.t0 = rs.t0[r];
+            C.t2 = rs.t2[r];
+            C.nrr = rs.nrr[r];
+            C.rms0 = rs.rms0[r];
             const SeedOut sd = seeds[r];
-            R.rms = sd.rms;
-            R.sum = sd.sum;
-            R.idx = sd.idx;
-            R.th = make_threshold(R.sum, R.rms, R.idx >> 3, R.rms0, R.nrr, N, fp);
+            C.rms = sd.rms;
+            C.sum = sd.sum;
+            C.idx = sd.idx;
         } else {
             // Padding of the last N tile, or a block outside the plane: no candidate.
-            R.rms = INFINITY;
-            R.sum = 0.0;
-            R.idx = UINT32_MAX;
+            C.rms = INFINITY;
+            C.sum = 0.0;
+            C.idx = UINT32_MAX;
         }
+        sm.key_rms[threadIdx.x] = ~0ull;
+        sm.key_idx[threadIdx.x] = UINT32_MAX;
+        publish_threshold(sm, threadIdx.x, fp, N);
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -321,12 +453,16 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const int kg0 = t * 8;
                     const int j = kg0 / ROWS, y0 = kg0 % ROWS;
                     unsigned char* dstA = stA + s * kStageA;
-#pragma unroll 1
-                    for (int gg = 0; gg < 16; ++gg) {
+                    if (maps.use_all) {
+                        tma_load_4d(dstA, &maps.all, 16 * (q0 + j), dom_row + y0, &sm.full[s]);
+                    } else {
                         const int per_phase = 16 / P;
-                        const int p = gg / per_phase, h = gg % per_phase;
-                        tma_load_2d(dstA + gg * 1024, &maps.m[p], 16 * (q0 + 8 * h + j),
-                                    dom_row + y0, &sm.full[s]);
+#pragma unroll 1
+                        for (int gg = 0; gg < 16; ++gg) {
+                            const int p = gg / per_phase, h = gg % per_phase;
+                            tma_load_2d(dstA + gg * 1024, &maps.m[p], 16 * (q0 + 8 * h + j),
+                                        dom_row + y0, &sm.full[s]);
+                        }
                     }
                     if (!kBRes)
                         bulk_load(stB + s * kStageB, btile + (size_t)t * kStageB, kStageB, &sm.full[s]);
@@ -389,130 +525,155 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
         }
         __syncwarp();
-    } else if (warp >= 4) {
+    } else {
         // ---------------------------------------------------------------- epilogue
-        const int e = warp - 4;  // TMEM lane quadrant
-        const int m = e * 32 + lane;
-        const float inv_n = 1.0f / (float)N;
+        // Warps 2..9: TMEM lane quadrant = warp % 4 (each quadrant twice), column half
+        // (ranges [16*half, 16*half + 16)) = which of the two warps of that quadrant.
+        const int et = threadIdx.x - 64;         // 0..255
+        const int e = warp & 3;
+        const int half = (warp - 2) >> 2;
+        const int m = e * 32 + lane;             // this thread's domain lane
         const float four_inv_n = 4.0f / (float)N;
         unsigned long long exact = 0;
+
+        // This lane's domain statistics, prefetched one tile ahead.
+        auto load_dom = [&](int mt, float& s1f, float& detf, float& sdetf, int& dom) {
+            if (mt >= m_end) return;
+            const int a = mt / tiles_per_row;
+            const int c = domain_of_lane(m, P, (mt % tiles_per_row) * (kM / P));
+            if (c < g.ncol_d) {
+                dom = a * g.ncol_d + c;
+                s1f = (float)ds.s1x4[dom];
+                detf = ds.detf[dom];
+                sdetf = ds.sdetf[dom];
+            } else {
+                dom = -1;
+            }
+        };
+        float n_s1 = 0.f, n_det = 0.f, n_sdet = 0.f;
+        int n_dom = -1;
+        load_dom(m_begin, n_s1, n_det, n_sdet, n_dom);
+
         int i = 0;
         for (int mt = m_begin; mt < m_end; ++mt, ++i) {
             const int b = i & 1;
             const uint32_t bph = (uint32_t)((i >> 1) & 1);
+            const float s1f = n_s1, detf = n_det, sdetf = n_sdet;
+            const int dom = n_dom;
+            load_dom(mt + 1, n_s1, n_det, n_sdet, n_dom);
+            // a_min * Ndd and a_min/2 * Ndd, pre-scaled by 4 / n like the range records.
+            const float ad = __fmul_rd(fp.a_min, detf) * four_inv_n;
+            const float ahd = __fmul_rd(fp.a_half, detf) * four_inv_n;
+            const uint32_t tcol = tmem + ((uint32_t)(e * 32) << 16) + (uint32_t)(b * kN + half * 128);
+            bool rescan = false;
+
+            auto max8 = [](const int32_t (&v)[32], int o) {
+                return max(max(max(v[o], v[o + 1]), max(v[o + 2], v[o + 3])),
+                           max(max(v[o + 4], v[o + 5]), max(v[o + 6], v[o + 7])));
+            };
+            const uint32_t tag = (uint32_t)(mt & 0xFFFF);
+            // Thresholds of this lane's domain against its 16 ranges (fit.cuh, branch-free
+            // form).  They do not depend on the accumulator; each stage below runs over all
+            // 16 ranges so the independent chains overlap.
+            int32_t thr[16];
+            auto all_thresholds = [&]() {
+                float4 ra[16];
+                int4 rb[16];
+                const float4* rec = reinterpret_cast<const float4*>(sm.thr);
+#pragma unroll
+                for (int r = 0; r < 16; ++r) {
+                    ra[r] = rec[2 * (half * 16 + r)];
+                    rb[r] = reinterpret_cast<const int4*>(rec)[2 * (half * 16 + r) + 1];
+                }
+                float tau[16];
+#pragma unroll
+                for (int r = 0; r < 16; ++r) {
+                    const float g1 = __fmul_rd(ra[r].x, sdetf);
+                    const float tz = fminf(__fadd_rd(ra[r].y, ahd), fmaxf(g1, ad));
+                    tau[r] = dom > rb[r].x ? tz : __fadd_rd(g1, ra[r].z);
+                }
+#pragma unroll
+                for (int r = 0; r < 16; ++r) {
+                    const float num = __fadd_rd(__fmul_rd(s1f, ra[r].w), tau[r]);
+                    thr[r] = dom < 0 ? INT32_MAX : __float2int_rd(num);
+                }
+            };
+            auto test_chunk = [&](const int32_t (&v)[32], int ch) {
+                const int32_t t0 = thr[ch * 4], t1 = thr[ch * 4 + 1];
+                const int32_t t2 = thr[ch * 4 + 2], t3 = thr[ch * 4 + 3];
+                const bool any = (max8(v, 0) >= t0) | (max8(v, 8) >= t1) | (max8(v, 16) >= t2) |
+                                 (max8(v, 24) >= t3);
+                if (any) {
+                    // Rare: bit c of `mask` = column c of this chunk survives (and was not
+                    // fitted by an earlier pass over this accumulator).
+                    uint32_t mask = 0u;
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) {
+                        const int32_t tc = c < 8 ? t0 : (c < 16 ? t1 : (c < 24 ? t2 : t3));
+                        mask |= (v[c] >= tc ? 1u : 0u) << c;
+                    }
+                    const int col0 = half * 128 + ch * 32;
+                    if (rescan) mask &= ~sm.evaluated[(m * kN + col0) >> 5];
+                    int slot = atomicAdd(&sm.qcount, __popc(mask));
+                    while (mask) {
+                        const int c = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        int32_t val = v[0];
+#pragma unroll
+                        for (int q = 1; q < 32; ++q) val = c == q ? v[q] : val;
+                        if (slot < kQueueCap)
+                            sm.queue[slot] = QEntry{val, (uint32_t)dom,
+                                                    (uint32_t)(tag << 16 | m << 8 | (col0 + c)), 0u, 0.0, 0.0};
+                        ++slot;
+                    }
+                }
+            };
+            all_thresholds();  // overlaps the MMAs of this tile
             const bool got = mbar_wait(&sm.tfull[b], bph, abort_flag, err, 16);
             if (!epi_barrier_and(got)) break;
             tmem_fence_after();
-            const int a = mt / tiles_per_row;
-            const int q0 = (mt % tiles_per_row) * (kM / P);
-            int c;
-            domain_of_lane(m, P, q0, &c);
-            const bool dvalid = c < g.ncol_d;
-            const uint32_t dom = (uint32_t)(a * g.ncol_d + (dvalid ? c : 0));
-            float s1f = 0.f, detf = 0.f, sdetf = 0.f;
-            if (dvalid) {
-                s1f = (float)ds.s1x4[dom];
-                detf = ds.detf[dom];
-                sdetf = ds.sdetf[dom];
-            }
-            const float ad = __fmul_rd(fp.a_min, detf);
-            const float ahd = __fmul_rd(fp.a_half, detf);
-            const uint32_t tcol = tmem + ((uint32_t)(e * 32) << 16) + (uint32_t)(b * kN);
-            for (int ch = 0; ch < kN / 32; ++ch) {
-                int32_t v[32];
-                tmem_ld32(tcol + (uint32_t)(ch * 32), v);
-                if (ch == kN / 32 - 1) {
-                    // All of this accumulator is in registers: hand it back to the MMA warp.
-                    tmem_fence_before();
-                    mbar_arrive(&sm.tempty[b]);
-                }
-#pragma unroll
-                for (int rr = 0; rr < 4; ++rr) {
-                    const RangeRec& R = sm.rec[ch * 4 + rr];
-                    if (!dvalid || !R.valid) continue;
-                    const Threshold th = R.th;
-                    float tau;
-                    if (th.mode == 2 || (th.mode == 1 && dom > th.tie_dom)) {
-                        const float g1 = __fmul_rd(th.sqrt_w, sdetf);
-                        const float g2 = __fadd_rd(th.w2a, ahd);
-                        tau = fminf(g2, fmaxf(g1, ad));
-                    } else if (th.wpos) {
-                        tau = __fmul_rd(th.sqrt_w, sdetf);
-                    } else {
-                        tau = -INFINITY;
-                    }
-                    const float num = __fadd_rd(__fmul_rd(s1f, R.c), __fmul_rd(tau, four_inv_n));
-                    const int32_t thr = __float2int_rd(num);
-                    int mx = v[rr * 8];
-#pragma unroll
-                    for (int k = 1; k < 8; ++k) mx = max(mx, v[rr * 8 + k]);
-                    if (mx >= thr) {
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) {
-                            if (v[rr * 8 + k] >= thr) {
-                                const int slot = atomicAdd(&sm.qcount[ch & 1][rr], 1);
-                                sm.queue[rr][slot] = QEntry{v[rr * 8 + k], (uint32_t)(m << 3 | k)};
-                            }
-                        }
-                    }
-                }
-                // Counters alternate with the chunk parity: the next chunk's pushes can never
-                // be mistaken for this chunk's survivors by a warp that reads late.
+            for (;;) {
+                // ---- scan: this thread's 128 accumulator columns, loads overlapped with tests
+                int32_t va[32], vb[32];
+                __syncwarp();
+                tmem_ld32(tcol, va);
+                tmem_wait(va);
+                tmem_ld32(tcol + 32u, vb);
+                test_chunk(va, 0);
+                __syncwarp();
+                tmem_wait(vb);
+                tmem_ld32(tcol + 64u, va);
+                test_chunk(vb, 1);
+                __syncwarp();
+                tmem_wait(va);
+                tmem_ld32(tcol + 96u, vb);
+                test_chunk(va, 2);
+                __syncwarp();
+                tmem_wait(vb);
+                test_chunk(vb, 3);
+
                 epi_barrier();
-                const int* qc = sm.qcount[ch & 1];
-                const int cnt = qc[e];
-                const bool any = (qc[0] | qc[1] | qc[2] | qc[3]) != 0;
-                if (any) {
-                    // Warp e owns range ch*4 + e: exact fits of its survivors, then the
-                    // champion update under the reference's (rms, index) order.
-                    RangeRec& R = sm.rec[ch * 4 + e];
-                    double best_rms = INFINITY, best_sum = 0.0;
-                    uint32_t best_idx = UINT32_MAX;
-                    for (int qi = lane; qi < cnt; qi += 32) {
-                        const QEntry q = sm.queue[e][qi];
-                        int cc;
-                        domain_of_lane((int)(q.code >> 3), P, q0, &cc);
-                        const uint32_t d2 = (uint32_t)(a * g.ncol_d + cc);
-                        const int32_t s1 = ds.s1x4[d2];
-                        const int64_t t1x4 = (int64_t)q.t1 + 128ll * s1;
-                        const FitResult f = fit_exact(N, s1, ds.s2x16[d2], R.t0, t1x4, R.t2, fp);
-                        const uint32_t idx = d2 * 8u + (q.code & 7u);
-                        ++exact;
-                        if (f.rms < best_rms || (f.rms == best_rms && idx < best_idx)) {
-                            best_rms = f.rms;
-                            best_sum = f.sum;
-                            best_idx = idx;
-                        }
-                    }
-#pragma unroll
-                    for (int off = 16; off > 0; off >>= 1) {
-                        const double orms = __shfl_xor_sync(0xffffffffu, best_rms, off);
-                        const double osum = __shfl_xor_sync(0xffffffffu, best_sum, off);
-                        const uint32_t oidx = __shfl_xor_sync(0xffffffffu, best_idx, off);
-                        if (orms < best_rms || (orms == best_rms && oidx < best_idx)) {
-                            best_rms = orms;
-                            best_sum = osum;
-                            best_idx = oidx;
-                        }
-                    }
-                    if (lane == 0 && best_idx != UINT32_MAX &&
-                        (best_rms < R.rms || (best_rms == R.rms && best_idx < R.idx))) {
-                        R.rms = best_rms;
-                        R.sum = best_sum;
-                        R.idx = best_idx;
-                        R.th = make_threshold(R.sum, R.rms, R.idx >> 3, R.rms0, R.nrr, N, fp);
-                    }
-                    epi_barrier();
-                    if (threadIdx.x == 128) {
-                        int* w = sm.qcount[ch & 1];
-                        w[0] = w[1] = w[2] = w[3] = 0;
-                    }
-                    epi_barrier();
+                const int queued = sm.qcount;
+                const bool last = mt + 1 == m_end;
+                if (queued > kQueueCap) {
+                    drain_queue<N>(sm, kQueueCap, true, tag, et, ds, fp, exact);
+                    rescan = true;
+                    all_thresholds();
+                    continue;  // pass again over the same accumulator
                 }
+                if (queued >= kFlush || (last && queued > 0))
+                    drain_queue<N>(sm, queued, false, tag, et, ds, fp, exact);
+                break;
             }
+            if (rescan) {
+                for (int w2 = et; w2 < kM * kN / 32; w2 += kEpiThreads) sm.evaluated[w2] = 0u;
+                epi_barrier();
+            }
+            // The accumulator has been read completely: hand it back to the MMA warp.
+            tmem_fence_before();
+            mbar_arrive(&sm.tempty[b]);
         }
         if (exact_counter && exact) atomicAdd(exact_counter, exact);
-        (void)inv_n;
     }
 
     tmem_fence_before();
@@ -522,13 +683,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
     }
     if (threadIdx.x < kRangesPerTile) {
-        const RangeRec& R = sm.rec[threadIdx.x];
+        const Champ& C = sm.ch[threadIdx.x];
         const int r = ntile * kRangesPerTile + threadIdx.x;
         if (r < nranges) {
             Partial p;
-            p.rms = R.rms;
-            p.sum = R.sum;
-            p.idx = R.idx;
+            p.rms = C.rms;
+            p.sum = C.sum;
+            p.idx = C.idx;
             p.t1x4 = 0;
             p.qalfa = 0;
             p.qbeta = 0;
@@ -729,6 +890,8 @@ size_t smem_bytes() {
     constexpr int J = S >= 8 ? S / 8 : 1;
     constexpr int KST = J * 2 * S / 8;
     constexpr bool kBRes = KST <= 2;
+    constexpr int kStages = stages_for(S);
+    static_assert(kStages <= kMaxStages, "pipeline depth");
     return 1024 + (size_t)kStages * kStageA + (kBRes ? (size_t)KST * kStageB : (size_t)kStages * kStageB) +
            sizeof(Smem);
 }
@@ -780,6 +943,11 @@ size_t b_bytes(int size, int nranges) {
 
 int phase_count(int shift) { return 16 / shift; }
 int row_pitch(int w) { return ((w + 15) / 16) * 16 + 16; }
+// The 4-D view reads up to (16/P - 1) * 128 bytes past a row's end (columns no valid
+// domain uses); the allocation carries that much slack after the last phase copy.
+size_t phase_bytes(int w, int h, int shift) {
+    return (size_t)phase_count(shift) * h * row_pitch(w) + 2048;
+}
 
 cudaError_t launch_phase_planes(const uint8_t* plane, int w, int h, int shift, uint8_t* out,
                                 cudaStream_t st) {

@@ -9,13 +9,18 @@
 namespace mars {
 namespace tc {
 
-constexpr int kStages = 3;     // shared-memory pipeline depth (A, and B when streamed)
+constexpr int kMaxStages = 6;  // shared-memory pipeline depth bound (see stages_for)
 constexpr int kMaxPhases = 8;  // 16 / shift for shift = 2
 
-// One 2-D TMA descriptor per phase copy of the plane (u8, row pitch a multiple of 16,
-// box 128 B x 8 rows, no swizzle, zero fill out of bounds).
+// TMA descriptors of the phase copies of the plane (u8, row pitch a multiple of 16, no
+// swizzle, zero fill out of bounds).  `all` is one 4-D view -- bytes x pixel rows x
+// same-phase 128-byte column groups x phases -- whose 128 x 8 x (16/P) x P box is a whole
+// 16 KB A stage in core-matrix order; when the driver rejects that view (`use_all` = 0)
+// the stage is loaded as 16 boxes of 128 B x 8 rows through the per-phase 2-D maps.
 struct alignas(64) TcMaps {
+    CUtensorMap all;
     CUtensorMap m[kMaxPhases];
+    int32_t use_all;
 };
 
 struct SeedOut {
@@ -26,6 +31,7 @@ struct SeedOut {
 bool supported(int size, int shift);
 int phase_count(int shift);
 int row_pitch(int w);
+size_t phase_bytes(int w, int h, int shift);
 size_t b_bytes(int size, int nranges);
 int msplit_for(const LevelGeom& g, int nranges, int num_sms);
 

@@ -206,6 +206,8 @@ def test_tensor_core_path_equals_cuda_core_path(ctx, shift):
     img = synthetic.gray(288, 224, 9)
     simt = mb.Context(0)
     simt.set_search_path("simt")
+    boxes = mb.Context(0)
+    boxes.set_search_path("boxes")  # tensor cores, A stages loaded as per-phase 2-D boxes
     try:
         for size in (4, 8, 16, 32, 64):
             if 2 * size > 224:
@@ -213,10 +215,13 @@ def test_tensor_core_path_equals_cuda_core_path(ctx, shift):
             p = mb.make_params(shift=shift)
             a, aev = ctx.search_grid(img, size, shift, p)
             b, bev = simt.search_grid(img, size, shift, p)
+            c, _ = boxes.search_grid(img, size, shift, p)
             assert np.array_equal(aev, bev)
             assert a.tobytes() == b.tobytes(), (size, shift)
+            assert c.tobytes() == a.tobytes(), (size, shift)
     finally:
         simt.close()
+        boxes.close()
     o, _ = orc.search_grid(img, 8, shift, orc.make_params(shift=shift))
     a, _ = ctx.search_grid(img, 8, shift, mb.make_params(shift=shift))
     assert a.tobytes() == o.tobytes()
