@@ -255,8 +255,7 @@ int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32
                                     d_seed, st));
     MARS_CUDA(mars::tc::launch_corr(maps, d_b, g, (int)n, rs, ds, fp, d_seed, partials, msplit,
                                     ctx->d_err, ctx->d_counter, st));
-    MARS_CUDA(mars::tc::launch_finish(partials, msplit, (int)n, g, d_D, d_plane, (int)w, d_rows,
-                                      d_cols, rs, ds, fp, d_out, st));
+    MARS_CUDA(mars::tc::launch_finish(partials, msplit, (int)n, g, rs, ds, fp, d_out, st));
     ctx->launches += 5;
     return MARS_OK;
 }

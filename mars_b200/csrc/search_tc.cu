@@ -223,6 +223,7 @@ struct Champ {
     int64_t nrr;
     uint32_t idx;
     int32_t t0, t2, valid;
+    int32_t t1x4;  // the champion's exact correlation, handed to the finish kernel
 };
 
 // The per-range pruning record the epilogue reads for every (domain lane, range) pair,
@@ -258,6 +259,7 @@ struct Smem {
     unsigned long long key_rms[kRangesPerTile];  // per-pass winner: f64 bits (rms >= 0)
     uint32_t key_idx[kRangesPerTile];
     double key_sum[kRangesPerTile];
+    int32_t key_t1[kRangesPerTile];
     ThrRec thr[kRangesPerTile];
     Champ ch[kRangesPerTile];
     uint32_t evaluated[kM * kN / 32];           // candidates already fitted in this tile
@@ -324,8 +326,10 @@ __device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t ta
         const QEntry& q = sm.queue[qi];
         const int col = (int)(q.code & 255u), rl = col >> 3;
         if ((unsigned long long)__double_as_longlong(q.rms) == sm.key_rms[rl] &&
-            q.dom * 8u + (uint32_t)(col & 7) == sm.key_idx[rl])
+            q.dom * 8u + (uint32_t)(col & 7) == sm.key_idx[rl]) {
             sm.key_sum[rl] = q.sum;
+            sm.key_t1[rl] = q.t1 + 128 * ds.s1x4[q.dom];  // t1_x4, exact in int32 (S <= 64)
+        }
         if (mark && (q.code >> 16) == tag) {
             // The tile overflowed the queue: remember what was fitted so the next pass
             // over the same accumulator only queues candidates not yet seen.
@@ -342,6 +346,7 @@ __device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t ta
             C.rms = r2;
             C.idx = i2;
             C.sum = sm.key_sum[et];
+            C.t1x4 = sm.key_t1[et];
             publish_threshold(sm, et, fp, N);
         }
         sm.key_rms[et] = ~0ull;
@@ -410,11 +415,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             C.rms = sd.rms;
             C.sum = sd.sum;
             C.idx = sd.idx;
+            C.t1x4 = sd.t1x4;
         } else {
             // Padding of the last N tile, or a block outside the plane: no candidate.
             C.rms = INFINITY;
             C.sum = 0.0;
             C.idx = UINT32_MAX;
+            C.t1x4 = 0;
         }
         sm.key_rms[threadIdx.x] = ~0ull;
         sm.key_idx[threadIdx.x] = UINT32_MAX;
@@ -690,7 +697,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             p.rms = C.rms;
             p.sum = C.sum;
             p.idx = C.idx;
-            p.t1x4 = 0;
+            p.t1x4 = C.t1x4;
             p.qalfa = 0;
             p.qbeta = 0;
             p.pad = 0;
@@ -765,9 +772,25 @@ __global__ void phase_planes_kernel(const uint8_t* __restrict__ plane, int w, in
     out[((size_t)p * h + y) * wp + x] = sx < w ? plane[(size_t)y * w + sx] : 0;
 }
 
+// isometry::map (crates/mars-codec/src/isometry.rs:7-19) as a flat range index i*S + j.
+__device__ __forceinline__ int iso_src_rt(int k, int u, int v, int S) {
+    switch (k) {
+        case 0: return u * S + v;
+        case 1: return (S - 1 - v) * S + u;
+        case 2: return v * S + (S - 1 - u);
+        case 3: return (S - 1 - u) * S + (S - 1 - v);
+        case 4: return u * S + (S - 1 - v);
+        case 5: return (S - 1 - u) * S + v;
+        case 6: return v * S + u;
+        default: return (S - 1 - v) * S + (S - 1 - u);
+    }
+}
+
 // Seed champion of each range: the exact best of the 8 isometries at the 3 x 3 domain
 // positions around the range's own position (any real candidate is a valid champion; a
-// good one makes the filter tight from the first tile).  One warp per range.
+// good one makes the filter tight from the first tile).  One warp per range: the 32 lanes
+// share each candidate's correlation (S*S terms), then each lane fits the candidates it
+// owns.
 __global__ void seed_kernel(const int32_t* __restrict__ D, LevelGeom g, const uint8_t* __restrict__ plane,
                             int w, const uint32_t* rows, const uint32_t* cols, int nranges,
                             RangeStats rs, DomainStats ds, FitParams fp, SeedOut* __restrict__ out) {
@@ -781,37 +804,42 @@ __global__ void seed_kernel(const int32_t* __restrict__ D, LevelGeom g, const ui
     }
     const int ac = min(max(((int)rows[r] - S / 2 + g.shift / 2) / g.shift, 0), g.nrow_d - 1);
     const int bc = min(max(((int)cols[r] - S / 2 + g.shift / 2) / g.shift, 0), g.ncol_d - 1);
+    const uint8_t* rb = plane + (size_t)rows[r] * w + cols[r];
     double best_rms = INFINITY, best_sum = 0.0;
     uint32_t best_idx = UINT32_MAX;
-    const uint8_t* rb = plane + (size_t)rows[r] * w + cols[r];
-    for (int cand = lane; cand < 72; cand += 32) {
-        const int k = cand & 7, nb = cand >> 3;
-        const int a = min(max(ac + nb / 3 - 1, 0), g.nrow_d - 1);
-        const int bb = min(max(bc + nb % 3 - 1, 0), g.ncol_d - 1);
-        const int32_t* db = D + (size_t)(a * g.step_c) * g.dw + bb * g.step_c;
-        int64_t t1 = 0;
-        for (int u = 0; u < S; ++u)
-            for (int v = 0; v < S; ++v) {
-                int i, j;
-                switch (k) {
-                    case 0: i = u; j = v; break;
-                    case 1: i = S - 1 - v; j = u; break;
-                    case 2: i = v; j = S - 1 - u; break;
-                    case 3: i = S - 1 - u; j = S - 1 - v; break;
-                    case 4: i = u; j = S - 1 - v; break;
-                    case 5: i = S - 1 - u; j = v; break;
-                    case 6: i = v; j = u; break;
-                    default: i = S - 1 - v; j = S - 1 - u; break;
-                }
-                t1 += (int64_t)rb[(size_t)i * w + j] * db[(size_t)u * g.dw + v];
+    int32_t best_t1 = 0;
+    for (int base = 0; base < 72; base += 32) {
+        // Correlations of candidates base .. base+31; lane (cand - base) keeps its own.
+        int64_t mine = 0;
+        const int ncand = min(32, 72 - base);
+        for (int ci = 0; ci < ncand; ++ci) {
+            const int cand = base + ci, k = cand & 7, nb = cand >> 3;
+            const int a = min(max(ac + nb / 3 - 1, 0), g.nrow_d - 1);
+            const int bb = min(max(bc + nb % 3 - 1, 0), g.ncol_d - 1);
+            const int32_t* db = D + (size_t)(a * g.step_c) * g.dw + bb * g.step_c;
+            int64_t part = 0;
+            for (int t = lane; t < N; t += 32) {
+                const int u = t / S, v = t % S;
+                const int src = iso_src_rt(k, u, v, S);
+                part += (int64_t)rb[(size_t)(src / S) * w + (src % S)] * db[(size_t)u * g.dw + v];
             }
-        const uint32_t dom = (uint32_t)(a * g.ncol_d + bb);
-        const FitResult f = fit_exact(N, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], t1, rs.t2[r], fp);
-        const uint32_t idx = dom * 8u + (uint32_t)k;
-        if (f.rms < best_rms || (f.rms == best_rms && idx < best_idx)) {
-            best_rms = f.rms;
-            best_sum = f.sum;
-            best_idx = idx;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+            if (lane == ci) mine = part;
+        }
+        if (lane < ncand) {
+            const int cand = base + lane, k = cand & 7, nb = cand >> 3;
+            const int a = min(max(ac + nb / 3 - 1, 0), g.nrow_d - 1);
+            const int bb = min(max(bc + nb % 3 - 1, 0), g.ncol_d - 1);
+            const uint32_t dom = (uint32_t)(a * g.ncol_d + bb);
+            const FitResult f = fit_exact(N, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], mine, rs.t2[r], fp);
+            const uint32_t idx = dom * 8u + (uint32_t)k;
+            if (f.rms < best_rms || (f.rms == best_rms && idx < best_idx)) {
+                best_rms = f.rms;
+                best_sum = f.sum;
+                best_idx = idx;
+                best_t1 = (int32_t)mine;
+            }
         }
     }
 #pragma unroll
@@ -819,20 +847,21 @@ __global__ void seed_kernel(const int32_t* __restrict__ D, LevelGeom g, const ui
         const double orms = __shfl_xor_sync(0xffffffffu, best_rms, off);
         const double osum = __shfl_xor_sync(0xffffffffu, best_sum, off);
         const uint32_t oidx = __shfl_xor_sync(0xffffffffu, best_idx, off);
+        const int32_t ot1 = __shfl_xor_sync(0xffffffffu, best_t1, off);
         if (orms < best_rms || (orms == best_rms && oidx < best_idx)) {
             best_rms = orms;
             best_sum = osum;
             best_idx = oidx;
+            best_t1 = ot1;
         }
     }
-    if (lane == 0) out[r] = SeedOut{best_rms, best_sum, best_idx, 0};
+    if (lane == 0) out[r] = SeedOut{best_rms, best_sum, best_idx, best_t1};
 }
 
-// Final champion over the M-splits, with the winner's moments recomputed exactly.
+// Final champion over the M-splits; its exact correlation travels with it, so only the
+// (cheap) exact fit is redone here to fill in qalfa / qbeta.
 __global__ void finish_kernel(const Partial* __restrict__ partials, int nsplit, int nranges,
-                              LevelGeom g, const int32_t* __restrict__ D,
-                              const uint8_t* __restrict__ plane, int w, const uint32_t* rows,
-                              const uint32_t* cols, RangeStats rs, DomainStats ds, FitParams fp,
+                              LevelGeom g, RangeStats rs, DomainStats ds, FitParams fp,
                               CandidateOut* __restrict__ out) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nranges) return;
@@ -841,32 +870,14 @@ __global__ void finish_kernel(const Partial* __restrict__ partials, int nsplit, 
         const Partial p = partials[(size_t)t * nranges + r];
         if (p.rms < best.rms || (p.rms == best.rms && p.idx < best.idx)) best = p;
     }
-    const int S = g.size;
     if (best.idx == UINT32_MAX) {
         out[r] = CandidateOut{0, 0, 0, 0, 0, 0, 0.0, 0, 0, 0, 0, 0, 0};
         return;
     }
     const uint32_t dom = best.idx >> 3, k = best.idx & 7u;
     const int a = (int)(dom / (uint32_t)g.ncol_d), bb = (int)(dom % (uint32_t)g.ncol_d);
-    const int32_t* db = D + (size_t)(a * g.step_c) * g.dw + bb * g.step_c;
-    const uint8_t* rb = plane + (size_t)rows[r] * w + cols[r];
-    int64_t t1 = 0;
-    for (int u = 0; u < S; ++u)
-        for (int v = 0; v < S; ++v) {
-            int i, j;
-            switch (k) {
-                case 0: i = u; j = v; break;
-                case 1: i = S - 1 - v; j = u; break;
-                case 2: i = v; j = S - 1 - u; break;
-                case 3: i = S - 1 - u; j = S - 1 - v; break;
-                case 4: i = u; j = S - 1 - v; break;
-                case 5: i = S - 1 - u; j = v; break;
-                case 6: i = v; j = u; break;
-                default: i = S - 1 - v; j = S - 1 - u; break;
-            }
-            t1 += (int64_t)rb[(size_t)i * w + j] * db[(size_t)u * g.dw + v];
-        }
-    const int64_t n = (int64_t)S * S;
+    const int64_t n = (int64_t)g.size * g.size;
+    const int64_t t1 = best.t1x4;
     const FitResult f = fit_exact(n, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], t1, rs.t2[r], fp);
     CandidateOut c;
     c.dom_row = (uint32_t)a * (uint32_t)g.shift;
@@ -978,12 +989,27 @@ cudaError_t launch_seed(const int32_t* D, const LevelGeom& g, const uint8_t* pla
     return cudaGetLastError();
 }
 
+// M-split of a level: the grid is (N tiles) x msplit CTAs, one CTA per SM at a time, each
+// CTA sweeping ceil(m_tiles / msplit) domain tiles after a fixed set-up (B load, range
+// records, pipeline fill) worth about kSetupTiles tiles.  Pick the split with the fewest
+// tile-times over all waves.
 int msplit_for(const LevelGeom& g, int nranges, int num_sms) {
+    constexpr long long kSetupTiles = 4;
     const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
     const int m_tiles = g.nrow_d * tiles_per_row;
     const int ntiles = (nranges + kRangesPerTile - 1) / kRangesPerTile;
-    const int want = (2 * num_sms + ntiles - 1) / ntiles;
-    return want < 1 ? 1 : (want > m_tiles ? m_tiles : want);
+    int best = 1;
+    long long best_cost = -1;
+    for (int ms = 1; ms <= m_tiles; ++ms) {
+        const long long waves = ((long long)ntiles * ms + num_sms - 1) / num_sms;
+        const long long per_cta = (m_tiles + ms - 1) / ms + kSetupTiles;
+        const long long cost = waves * per_cta;
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = ms;
+        }
+    }
+    return best;
 }
 
 cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
@@ -1001,11 +1027,10 @@ cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeo
 }
 
 cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,
-                          const int32_t* D, const uint8_t* plane, int w, const uint32_t* rows,
-                          const uint32_t* cols, RangeStats rs, DomainStats ds, const FitParams& fp,
-                          CandidateOut* out, cudaStream_t st) {
-    finish_kernel<<<(nranges + 127) / 128, 128, 0, st>>>(partials, nsplit, nranges, g, D, plane, w,
-                                                         rows, cols, rs, ds, fp, out);
+                          RangeStats rs, DomainStats ds, const FitParams& fp, CandidateOut* out,
+                          cudaStream_t st) {
+    finish_kernel<<<(nranges + 127) / 128, 128, 0, st>>>(partials, nsplit, nranges, g, rs, ds, fp,
+                                                         out);
     return cudaGetLastError();
 }
 

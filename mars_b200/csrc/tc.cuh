@@ -25,7 +25,8 @@ struct alignas(64) TcMaps {
 
 struct SeedOut {
     double rms, sum;
-    uint32_t idx, pad;
+    uint32_t idx;
+    int32_t t1x4;  // the seed champion's exact correlation (fits int32 for S <= 64)
 };
 
 bool supported(int size, int shift);
@@ -47,9 +48,8 @@ cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeo
                         Partial* partials, int msplit, int* err, unsigned long long* counter,
                         cudaStream_t st);
 cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,
-                          const int32_t* D, const uint8_t* plane, int w, const uint32_t* rows,
-                          const uint32_t* cols, RangeStats rs, DomainStats ds, const FitParams& fp,
-                          CandidateOut* out, cudaStream_t st);
+                          RangeStats rs, DomainStats ds, const FitParams& fp, CandidateOut* out,
+                          cudaStream_t st);
 
 }  // namespace tc
 }  // namespace mars
