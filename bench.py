@@ -50,6 +50,21 @@ def rank_info():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def rank_seeds(rank):
+    """The 8 planes a rank cycles through: seeds 1-8, rank r starting at seed r % 8 + 1."""
+    return [1 + (rank + k) % 8 for k in range(8)]
+
+
+def reduce_max(value, dist=None, device=None):
+    """Max of a per-rank float over all ranks (the identity without a process group)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def level_nodes(size):
     rows, cols = np.meshgrid(np.arange(H // size) * size, np.arange(W // size) * size, indexing="ij")
     return rows.ravel().astype(np.uint32), cols.ravel().astype(np.uint32)
@@ -220,7 +235,7 @@ def run_gpu(args):
     ctx.set_stream(stream.cuda_stream)
 
     params = mb.make_params(min_size=4, max_size=32, shift=SHIFT)
-    seeds = [1 + (rank * 8 + k) % 8 for k in range(8)]
+    seeds = rank_seeds(rank)
     planes = [torch.from_numpy(synthetic.gray(W, H, s)).to(dev) for s in seeds]
     levels = {}
     for size in SIZES:
@@ -262,11 +277,7 @@ def run_gpu(args):
                 per_level[s] += timers[s][0].elapsed_time(timers[s][1]) / 1e3
     torch.cuda.synchronize(dev)
     launches = ctx.launches - launches0
-    t_total = sum(per_level.values())
-    if dist:
-        t = torch.tensor([t_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_total = float(t.item())
+    t_total = reduce_max(sum(per_level.values()), dist, dev)
     ev_step = evals_per_step()
     value = ev_step * args.steps * world / t_total
 
