@@ -153,6 +153,26 @@ int mars_search_nodes_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t wid
                              uint32_t height, const mars_params* params, mars_candidate* d_out,
                              size_t capacity, size_t* n_nodes, uint64_t* total_evals);
 
+/* The level search of mars_search_blocks_device for callers that cannot allocate device
+ * memory -- real-time pipelines that forbid allocation once they are running, plug-ins
+ * whose host application owns every device allocation, hosts with a fixed device-memory
+ * budget.  It has no
+ * counterpart in the reference.  It needs no context (creating one allocates) and calls no
+ * allocator: its scratch is one 16 MiB device array inside the library, which every GPU
+ * that loads the library holds until the process exits.  A search that needs more scratch
+ * (roughly: planes beyond 512 x 512 at the smallest block sizes) is rejected with
+ * MARS_EINVAL.  It runs on the current device and on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream), with the CUDA-core correlation kernel; results are identical to
+ * the other entry points.  The first call on each device looks up the array's device
+ * address, so make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other host threads) race and must
+ * be serialised by the caller.  Inputs and outputs are device pointers, as in
+ * mars_search_blocks_device; the call is asynchronous. */
+int mars_search_blocks_noalloc(const uint8_t* d_plane, uint32_t width, uint32_t height,
+                               uint32_t size, uint32_t shift, const mars_params* params,
+                               const uint32_t* d_rows, const uint32_t* d_cols, size_t n,
+                               mars_candidate* d_out, void* stream);
+
 /* encode_image_with_search with this library as the provider: the threshold walk when
  * params->has_lambda == 0, else the exhaustive t_rms = 8 warm-up (served from the same
  * table) followed by the bottom-up RD walk.  *leaves is freed with mars_leaves_free. */

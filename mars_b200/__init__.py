@@ -71,7 +71,7 @@ EXPORTS = (
     "mars_search_table_lookup", "mars_search_table_evals", "mars_search_table_exact_fits",
     "mars_search_table_free", "mars_search_blocks", "mars_search_blocks_device",
     "mars_search_nodes_device", "mars_encode", "mars_leaves_free", "mars_decode",
-    "mars_ifs_parse", "mars_ifs_write", "mars_bytes_free",
+    "mars_ifs_parse", "mars_ifs_write", "mars_bytes_free", "mars_search_blocks_noalloc",
 )
 
 _lib = None
@@ -110,6 +110,7 @@ def lib():
     L.mars_search_blocks.argtypes = [vp, vp, u32, u32, u32, u32, P(Params), vp, vp, sz, vp, vp]
     L.mars_search_blocks_device.argtypes = [vp, vp, u32, u32, u32, u32, P(Params), vp, vp, sz, vp]
     L.mars_search_nodes_device.argtypes = [vp, vp, u32, u32, P(Params), vp, sz, P(sz), P(u64)]
+    L.mars_search_blocks_noalloc.argtypes = [vp, u32, u32, u32, u32, P(Params), vp, vp, sz, vp, vp]
     L.mars_encode.argtypes = [vp, vp, u32, u32, P(Params), P(Options), P(Header), P(vp), P(sz),
                               P(Counters)]
     L.mars_leaves_free.argtypes = [vp]

@@ -43,6 +43,11 @@ bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
 
 }  // namespace
 
+namespace mars {
+// The message mars_last_error() reports, for entry points defined in other files.
+int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace mars
+
 struct mars_ctx {
     int device = 0;
     int num_sms = 148;
