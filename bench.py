@@ -45,6 +45,11 @@ WORKLOAD = ("exhaustive search of every RD quadtree node of a 512x512 synthetic 
             "block sizes 32..4, domain stride 2, 8 isometries, seeds 1-8")
 
 
+# DRAM bytes (read + write) per launch of the dominant search kernel, from one ncu capture
+# of this workload's s=4 level (profiles/corr_tc_s4_512x512_ncu.md).
+NCU_TRAFFIC = {4: 21_066_496 + 12_032}
+
+
 def rank_info():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
@@ -187,6 +192,89 @@ def cpu_baseline(budget_s=12.0, seed=1):
     return value, cores, desc
 
 
+DECODE_SIDE = 16384
+DECODE_ITERS = 10
+
+
+def decode_header(mb, side):
+    """Header of the synthetic decode map: encmars defaults (bits 4/7, sizes 4..32, stride 2,
+    max_alfa 1.0 -> int_max_alfa 32)."""
+    return mb.Header(bits_alfa=4, bits_beta=7, min_size=4, max_size=32, shift=2, width=side,
+                     height=side, int_max_alfa=32)
+
+
+def decode_cpu_baseline(side=2048, seed=1):
+    """The oracle's decode_iterative (single-threaded, as the reference's) on a smaller
+    plane of the same synthetic map."""
+    from oracle import oracle as orc
+    leaves = synthetic.quadtree_leaves(side, side, seed)
+    hdr = orc.Header(bits_alfa=4, bits_beta=7, min_size=4, max_size=32, shift=2, width=side,
+                     height=side, int_max_alfa=32)
+    t0 = time.perf_counter()
+    orc.decode(hdr, leaves, DECODE_ITERS)
+    el = time.perf_counter() - t0
+    return {"value": side * side * DECODE_ITERS / el, "unit": "pixel-iterations/s", "cores": 1,
+            "kind": "port",
+            "sample": f"oracle decode of a {side}x{side} synthetic quadtree map, "
+                      f"{DECODE_ITERS} iterations"}
+
+
+def run_decode(args, mb, ctx, stream, dev, peaks, with_cpu):
+    """Fixed-point decode: DECODE_ITERS iterations of the gather over a synthetic quadtree
+    map of a DECODE_SIDE^2 plane (both ping-pong planes larger than L2)."""
+    import torch
+    side = DECODE_SIDE
+    leaves = synthetic.quadtree_leaves(side, side, 1)
+    hdr = decode_header(mb, side)
+    plan = ctx.decode_plan(hdr, leaves)
+    out = torch.empty(side * side, dtype=torch.uint8, device=dev)
+    for _ in range(max(3, args.warmup)):
+        plan.run(DECODE_ITERS, out.data_ptr())
+    torch.cuda.synchronize(dev)
+    steps = max(3, min(args.steps, 10))
+    launches0 = ctx.launches
+    t = 0.0
+    with ClockSampler(dev.index) as clocks:
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.run(DECODE_ITERS, out.data_ptr())
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            t += e0.elapsed_time(e1) / 1e3
+    launches = ctx.launches - launches0
+    plan.close()
+    t_dec = t / steps
+    px = side * side
+    algo = DECODE_ITERS * (2 * px + 16 * len(leaves))
+    achieved = algo / t_dec / 1e9
+    try:
+        peak, src = float(peaks["hbm_gbs"]), "measured copy bandwidth"
+    except Exception:
+        peak, src = 6650.0, "fallback 6.65 TB/s"
+    # End to end through mars_decode: host leaves in, host image out.
+    t0 = time.perf_counter()
+    ctx.decode(hdr, leaves, DECODE_ITERS)
+    t_e2e = time.perf_counter() - t0
+    del out
+    return {
+        "workload": f"decode_iterative of a {side}x{side} synthetic quadtree map "
+                    f"({len(leaves)} leaves, sizes 32..4, modes 0/1/2), {DECODE_ITERS} iterations "
+                    "from the flat-128 seed",
+        "value": px * DECODE_ITERS / t_dec, "unit": "pixel-iterations/s",
+        "ms_per_decode": 1e3 * t_dec, "steps": steps, "gpu_launches": launches,
+        "l2": "not flushed: both 268 MB planes exceed L2", "clocks": clocks.summary(),
+        "roofline": {"bound": "hbm", "kernel": "decode_step4_kernel", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": src,
+                     "bytes_per_launch": algo / DECODE_ITERS,
+                     "launch_ms": 1e3 * t_dec / DECODE_ITERS},
+        "e2e": {"value": px * DECODE_ITERS / t_e2e, "unit": "pixel-iterations/s",
+                "h2d_bytes_per_step": len(leaves) * 44, "d2h_bytes_per_step": px},
+        "cpu_baseline": decode_cpu_baseline() if with_cpu else None,
+    }
+
+
 def run_reference(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -313,6 +401,11 @@ def run_gpu(args):
         h2d = W * H + nodes * 8
         d2h = nodes * 80 + 8
 
+    decode = None
+    if not args.no_decode:
+        decode = run_decode(args, mb, ctx, stream, dev, peaks,
+                            with_cpu=rank == 0 and world == 1 and not args.no_cpu)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, desc = cpu_baseline()
@@ -329,7 +422,9 @@ def run_gpu(args):
                        "parallelism": f"replicas{world}", "l2": "flushed between steps (256 MiB write)"},
             "roofline": {"bound": "tensor", "kernel": f"search level s={dom}",
                          "achieved": achieved, "peak": peak_tops, "unit": "TOP/s",
-                         "frac": achieved / peak_tops, "traffic": None, "peak_source": peak_src,
+                         "frac": achieved / peak_tops, "traffic": NCU_TRAFFIC.get(dom),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum",
+                         "peak_source": peak_src,
                          "ops_per_launch": ops, "launch_ms": 1e3 * t_launch},
             "per_level_ms": {str(s): 1e3 * per_level[s] / args.steps for s in SIZES},
             "cpu_baseline": cpu,
@@ -337,6 +432,7 @@ def run_gpu(args):
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
+            "decode": decode,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -353,6 +449,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-decode", action="store_true", help="skip the decode leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -15,6 +15,10 @@
  *                                                              -> mars_encode
  *   decode_iterative          crates/mars-codec/src/ifs.rs:281-309   -> mars_decode
  *   ifs::parse / ifs::write   ifs.rs:186-217, 525-552           -> mars_ifs_parse / _write
+ *   mars_format::write / read crates/mars-codec/src/mars_format.rs:232-400
+ *                                                              -> mars_format_write / _read
+ *   mars_entropy::encode / Decoder  crates/mars-entropy/src/lib.rs:200-335
+ *                                                              -> mars_entropy_encode / _decode
  *
  * Conventions: every call returns MARS_OK (0) or a negative MARS_E* status; the text of the
  * last error on the calling thread is available from mars_last_error().  There is no CPU
@@ -91,6 +95,7 @@ typedef struct mars_counters {
 
 typedef struct mars_ctx mars_ctx;
 typedef struct mars_table mars_table;
+typedef struct mars_decode_plan mars_decode_plan;
 
 const char* mars_last_error(void);
 const char* mars_version(void);
@@ -186,12 +191,43 @@ void mars_leaves_free(mars_leaf* leaves);
 int mars_decode(mars_ctx* ctx, const mars_header* header, const mars_leaf* leaves, size_t n,
                 uint32_t iterations, uint8_t* out);
 
+/* Repeated decodes of one leaf list (progressive display, the attractor's forward map):
+ * the leaf table and the owner map are validated and uploaded once; each run writes
+ * `iterations` steps from the flat-128 seed into the device buffer d_out (width*height
+ * bytes), asynchronously on the context's stream. */
+int mars_decode_plan_create(mars_ctx* ctx, const mars_header* header, const mars_leaf* leaves,
+                            size_t n, mars_decode_plan** out);
+int mars_decode_plan_run(mars_decode_plan* plan, uint32_t iterations, uint8_t* d_out);
+void mars_decode_plan_free(mars_decode_plan* plan);
+
 /* .ifs bitstream.  Buffers returned here are freed with mars_bytes_free / mars_leaves_free. */
 int mars_ifs_parse(const uint8_t* data, size_t len, mars_header* header, mars_leaf** leaves,
                    size_t* nleaves);
 int mars_ifs_write(const mars_header* header, const mars_leaf* leaves, size_t n, uint8_t** out,
                    size_t* len);
 void mars_bytes_free(uint8_t* bytes);
+
+/* .mars v0 plane container (mars_format.rs:232-400): 24-byte header carrying the residual
+ * step as binary32, then the TREE section entropy-coded with adaptive models over the rANS
+ * stack coder.  Leaves of modes 0/1/2; mode 3 is refused with MARS_EUNSUPPORTED.  Format
+ * errors (bad magic, truncation, degenerate header, out-of-image domain, ...) return
+ * MARS_EFORMAT on read and MARS_EINVAL on write, with the reference's message text. */
+int mars_format_write(const mars_header* header, float residual_qstep, const mars_leaf* leaves,
+                      size_t n, uint8_t** out, size_t* len);
+int mars_format_read(const uint8_t* data, size_t len, mars_header* header, float* residual_qstep,
+                     mars_leaf** leaves, size_t* nleaves);
+
+/* mars_entropy::Event (lib.rs:188-193): context = (field, disambiguator). */
+typedef struct mars_event {
+    uint8_t field;
+    uint8_t pad[3];
+    uint32_t disambiguator, alphabet, symbol;
+} mars_event;
+/* mars_entropy::encode (lib.rs:200-202); bytes freed with mars_bytes_free. */
+int mars_entropy_encode(const mars_event* events, size_t n, uint8_t** out, size_t* len);
+/* Decoder::next once per entry of `shape` (its symbol fields are ignored), lib.rs:303-335. */
+int mars_entropy_decode(const uint8_t* data, size_t len, const mars_event* shape, size_t n,
+                        uint32_t* symbols);
 
 #ifdef __cplusplus
 }

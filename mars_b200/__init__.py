@@ -10,6 +10,7 @@ there is no CPU path: without a CUDA device the calls raise `MarsError`.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 from dataclasses import dataclass
 from typing import Optional
@@ -72,6 +73,8 @@ EXPORTS = (
     "mars_search_table_free", "mars_search_blocks", "mars_search_blocks_device",
     "mars_search_nodes_device", "mars_encode", "mars_leaves_free", "mars_decode",
     "mars_ifs_parse", "mars_ifs_write", "mars_bytes_free", "mars_search_blocks_noalloc",
+    "mars_decode_plan_create", "mars_decode_plan_run", "mars_decode_plan_free",
+    "mars_format_write", "mars_format_read", "mars_entropy_encode", "mars_entropy_decode",
 )
 
 _lib = None
@@ -116,10 +119,18 @@ def lib():
     L.mars_leaves_free.argtypes = [vp]
     L.mars_leaves_free.restype = None
     L.mars_decode.argtypes = [vp, P(Header), vp, sz, u32, vp]
+    L.mars_decode_plan_create.argtypes = [vp, P(Header), vp, sz, P(vp)]
+    L.mars_decode_plan_run.argtypes = [vp, u32, vp]
+    L.mars_decode_plan_free.argtypes = [vp]
+    L.mars_decode_plan_free.restype = None
     L.mars_ifs_parse.argtypes = [vp, sz, P(Header), P(vp), P(sz)]
     L.mars_ifs_write.argtypes = [P(Header), vp, sz, P(vp), P(sz)]
     L.mars_bytes_free.argtypes = [vp]
     L.mars_bytes_free.restype = None
+    L.mars_format_write.argtypes = [P(Header), C.c_float, vp, sz, P(vp), P(sz)]
+    L.mars_format_read.argtypes = [vp, sz, P(Header), P(C.c_float), P(vp), P(sz)]
+    L.mars_entropy_encode.argtypes = [vp, sz, P(vp), P(sz)]
+    L.mars_entropy_decode.argtypes = [vp, sz, vp, sz, vp]
     _lib = L
     return L
 
@@ -286,12 +297,40 @@ class Context:
         lib().mars_leaves_free(ptr)
         return hdr, leaves, cnt
 
+    def decode_plan(self, hdr: Header, leaves: np.ndarray) -> "DecodePlan":
+        leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+        h = C.c_void_p()
+        check(lib().mars_decode_plan_create(self._h, C.byref(hdr), leaves.ctypes.data,
+                                            len(leaves), C.byref(h)))
+        return DecodePlan(h.value)
+
     def decode(self, hdr: Header, leaves: np.ndarray, iterations: int = 10) -> np.ndarray:
         leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
         out = np.zeros((hdr.height, hdr.width), dtype=np.uint8)
         check(lib().mars_decode(self._h, C.byref(hdr), leaves.ctypes.data, len(leaves),
                                 iterations, out.ctypes.data))
         return out
+
+
+class DecodePlan:
+    """A leaf list prepared for repeated device decodes (mars_decode_plan_*)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    def run(self, iterations: int, d_out_ptr: int) -> None:
+        check(lib().mars_decode_plan_run(self._h, iterations, C.c_void_p(d_out_ptr)))
+
+    def close(self) -> None:
+        if self._h:
+            lib().mars_decode_plan_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def ifs_parse(data: bytes):
@@ -302,6 +341,65 @@ def ifs_parse(data: bytes):
     leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize), dtype=LEAF_DTYPE).copy()
     lib().mars_leaves_free(ptr)
     return hdr, leaves
+
+
+EVENT_DTYPE = np.dtype([("field", "u1"), ("pad", "u1", 3), ("disambiguator", "<u4"),
+                        ("alphabet", "<u4"), ("symbol", "<u4")])
+
+LEGACY_QSTEP = 8.0
+
+
+def qstep_from_lambda(lam: float) -> float:
+    """ResidualQstep::from_lambda (crates/mars-codec/src/quant.rs:36-52), as binary32."""
+    step = math.sqrt(max(lam, 0.0)) * math.sqrt(6.0 / math.log(2.0))
+    return float(np.float32(min(max(step, 1.0), 65535.0)))
+
+
+def format_write(hdr: Header, leaves: np.ndarray, residual_qstep: float = LEGACY_QSTEP) -> bytes:
+    """mars_format::write (mars_format.rs:232-300): the .mars v0 bytes of (hdr, leaves)."""
+    leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    ptr, n = C.c_void_p(), C.c_size_t()
+    check(lib().mars_format_write(C.byref(hdr), float(np.float32(residual_qstep)),
+                                  leaves.ctypes.data, len(leaves), C.byref(ptr), C.byref(n)))
+    data = C.string_at(ptr, n.value)
+    lib().mars_bytes_free(ptr)
+    return data
+
+
+def format_read(data: bytes):
+    """mars_format::read (mars_format.rs:302-400) -> (header, residual_qstep, leaves)."""
+    buf = np.frombuffer(data, dtype=np.uint8)
+    hdr, q = Header(), C.c_float()
+    ptr, n = C.c_void_p(), C.c_size_t()
+    check(lib().mars_format_read(buf.ctypes.data, len(data), C.byref(hdr), C.byref(q),
+                                 C.byref(ptr), C.byref(n)))
+    leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize), dtype=LEAF_DTYPE).copy()
+    lib().mars_leaves_free(ptr)
+    return hdr, q.value, leaves
+
+
+def entropy_encode(events) -> bytes:
+    """mars_entropy::encode over (field, disambiguator, alphabet, symbol) tuples."""
+    ev = np.zeros(len(events), EVENT_DTYPE)
+    for i, (f, d, a, s) in enumerate(events):
+        ev[i]["field"], ev[i]["disambiguator"], ev[i]["alphabet"], ev[i]["symbol"] = f, d, a, s
+    ptr, n = C.c_void_p(), C.c_size_t()
+    check(lib().mars_entropy_encode(ev.ctypes.data, len(ev), C.byref(ptr), C.byref(n)))
+    data = C.string_at(ptr, n.value)
+    lib().mars_bytes_free(ptr)
+    return data
+
+
+def entropy_decode(data: bytes, shape) -> list:
+    """Decoder::next for each (field, disambiguator, alphabet) of `shape`, in order."""
+    ev = np.zeros(len(shape), EVENT_DTYPE)
+    for i, (f, d, a) in enumerate(shape):
+        ev[i]["field"], ev[i]["disambiguator"], ev[i]["alphabet"] = f, d, a
+    out = np.zeros(len(shape), np.uint32)
+    buf = np.frombuffer(data, dtype=np.uint8)
+    check(lib().mars_entropy_decode(buf.ctypes.data, len(data), ev.ctypes.data, len(ev),
+                                    out.ctypes.data))
+    return [int(x) for x in out]
 
 
 def ifs_write(hdr: Header, leaves: np.ndarray) -> bytes:

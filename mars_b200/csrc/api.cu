@@ -676,51 +676,94 @@ int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t he
 void mars_leaves_free(mars_leaf* leaves) { std::free(leaves); }
 void mars_bytes_free(uint8_t* bytes) { std::free(bytes); }
 
-int mars_decode(mars_ctx* ctx, const mars_header* hdr, const mars_leaf* leaves, size_t n,
-                uint32_t iterations, uint8_t* out) {
-    if (!ctx || !hdr || !out || (n && !leaves)) return fail(MARS_EINVAL, "NULL argument");
+}  // extern "C"
+
+namespace {
+
+// Leaf table and owner map of one leaf list, validated on the host so that every read and
+// write the gather kernel makes stays inside the plane.  Leaves are packed into 16 bytes
+// (the layout is documented beside DecodeLeaf), which bounds plane sides to 65535, leaf
+// sizes to 4095 and qalfa to 2^bits_alfa, qbeta to 2^bits_beta - 1 -- the ranges every
+// .ifs stream and every encoder output lie in.  The owner map's cell is the largest power
+// of two dividing every leaf's row, column and size (4 for the usual quadtree with
+// min_size 4), capped at 32; later leaves overwrite earlier ones, as in the reference.
+int prepare_decode(const mars_header* hdr, const mars_leaf* leaves, size_t n,
+                   std::vector<mars::DecodeLeaf>* dl, std::vector<int32_t>* owner, int* lg_out,
+                   mars::DecodeConsts* consts) {
     const uint32_t w = hdr->width, h = hdr->height;
     if (w == 0 || h == 0) return fail(MARS_EINVAL, "empty plane");
+    if (w > 65535 || h > 65535) return fail(MARS_EINVAL, "plane sides must be at most 65535");
     if (hdr->bits_alfa > 16 || hdr->bits_beta < 1 || hdr->bits_beta > 16)
         return fail(MARS_EINVAL, "header bit widths out of range");
-    // Host-side validation: every read and write the gather makes stays inside the plane.
-    std::vector<int32_t> owner((size_t)w * h, -1);
-    std::vector<mars::DecodeLeaf> dl(n);
-    const double max_alfa = (double)hdr->int_max_alfa / 256.0 * 8.0;
+    dl->assign(n, mars::DecodeLeaf{});
+    uint32_t align_bits = 32u;
+    const uint32_t qalfa_max = 1u << hdr->bits_alfa, qbeta_max = (1u << hdr->bits_beta) - 1;
     for (size_t k = 0; k < n; ++k) {
         const mars_leaf& L = leaves[k];
         if (L.size == 0 || L.row + L.size > h || L.col + L.size > w || L.isometry > 7)
             return fail(MARS_EINVAL, "leaf " + std::to_string(k) + " lies outside the plane");
+        if (L.size > 4095)
+            return fail(MARS_EUNSUPPORTED, "leaf " + std::to_string(k) + " is wider than 4095");
         if (L.mode > 2) return fail(MARS_EUNSUPPORTED, "leaf mode 3 is not supported");
+        if (L.qbeta > qbeta_max || (L.mode != 1 && L.qalfa > qalfa_max))
+            return fail(MARS_EINVAL, "leaf " + std::to_string(k) +
+                                         " has coefficients wider than the header's bits");
         if (L.mode != 1 && L.qalfa != 0 &&
             (L.dom_row + 2 * L.size > h || L.dom_col + 2 * L.size > w))
             return fail(MARS_EINVAL, "leaf " + std::to_string(k) + " domain runs past the plane");
-        mars::DecodeLeaf& d = dl[k];
-        d.row = L.row;
-        d.col = L.col;
-        d.size = L.size;
-        d.mode = L.mode;
-        d.iso = L.isometry;
-        d.dom_row = L.dom_row;
-        d.dom_col = L.dom_col;
-        d.qalfa = L.qalfa;
-        d.gx = d.gy = 0.0;
+        align_bits |= L.row | L.col | L.size;
+        mars::DecodeLeaf& d = (*dl)[k];
+        d.x = L.row | (L.col << 16);
+        d.y = L.size | (L.mode << 12) | (L.qbeta << 16);
         if (L.mode == 1) {
-            // ifs.rs:416-431
-            d.alfa = (double)L.qbeta / (double)((1u << hdr->bits_beta) - 1) * 255.0;
-            d.beta = 0.0;
-            d.gx = (double)L.qgx / 64.0;
-            d.gy = (double)L.qgy / 64.0;
+            d.z = (uint32_t)L.qgx;
+            d.w = (uint32_t)L.qgy;
         } else {
-            // ifs.rs:433-439
-            d.alfa = (double)L.qalfa / (double)(1u << hdr->bits_alfa) * max_alfa;
-            d.beta = (double)L.qbeta / (double)((1u << hdr->bits_beta) - 1) *
-                     ((1.0 + std::fabs(d.alfa)) * 255.0);
-            if (d.alfa > 0.0) d.beta -= d.alfa * 255.0;
+            d.z = L.dom_row | (L.dom_col << 16);
+            d.w = L.qalfa | (L.isometry << 24);
         }
-        for (uint32_t i = 0; i < L.size; ++i)
-            std::fill_n(owner.begin() + (long)((size_t)(L.row + i) * w + L.col), L.size, (int32_t)k);
     }
+    consts->max_alfa = (double)hdr->int_max_alfa / 256.0 * 8.0;
+    consts->alfa_den = (double)qalfa_max;
+    consts->beta_den = (double)qbeta_max;
+    const int lg = __builtin_ctz(align_bits);
+    const uint32_t cell = 1u << lg;
+    const uint32_t mw = (w + cell - 1) >> lg, mh = (h + cell - 1) >> lg;
+    owner->assign((size_t)mw * mh, -1);
+    for (size_t k = 0; k < n; ++k) {
+        const mars_leaf& L = leaves[k];
+        for (uint32_t i = 0; i < (L.size >> lg); ++i)
+            std::fill_n(owner->begin() + (long)((size_t)((L.row >> lg) + i) * mw + (L.col >> lg)),
+                        L.size >> lg, (int32_t)k);
+    }
+    *lg_out = lg;
+    return MARS_OK;
+}
+
+}  // namespace
+
+struct mars_decode_plan {
+    mars_ctx* ctx = nullptr;
+    uint32_t w = 0, h = 0;
+    int lg = 0;
+    mars::DecodeConsts consts{};
+    size_t nleaves = 0;
+    int32_t* d_owner = nullptr;
+    mars::DecodeLeaf* d_leaves = nullptr;
+    uint8_t* d_tmp = nullptr;  // ping-pong partner of the caller's output buffer
+};
+
+extern "C" {
+
+int mars_decode(mars_ctx* ctx, const mars_header* hdr, const mars_leaf* leaves, size_t n,
+                uint32_t iterations, uint8_t* out) {
+    if (!ctx || !hdr || !out || (n && !leaves)) return fail(MARS_EINVAL, "NULL argument");
+    std::vector<mars::DecodeLeaf> dl;
+    std::vector<int32_t> owner;
+    int lg = 0;
+    mars::DecodeConsts consts;
+    if (int e = prepare_decode(hdr, leaves, n, &dl, &owner, &lg, &consts)) return e;
+    const uint32_t w = hdr->width, h = hdr->height;
     std::lock_guard<std::mutex> lock(ctx->mu);
     MARS_CUDA(cudaSetDevice(ctx->device));
     Scratch sc(ctx->stream);
@@ -730,20 +773,86 @@ int mars_decode(mars_ctx* ctx, const mars_header* hdr, const mars_leaf* leaves, 
     const size_t px = (size_t)w * h;
     MARS_CUDA(sc.get(&a, px));
     MARS_CUDA(sc.get(&b, px));
-    MARS_CUDA(sc.get(&d_owner, px));
+    MARS_CUDA(sc.get(&d_owner, owner.size()));
     MARS_CUDA(sc.get(&d_leaves, n));
-    MARS_CUDA(cudaMemcpyAsync(d_owner, owner.data(), px * 4, cudaMemcpyHostToDevice, ctx->stream));
+    MARS_CUDA(cudaMemcpyAsync(d_owner, owner.data(), owner.size() * 4, cudaMemcpyHostToDevice,
+                              ctx->stream));
     if (n)
         MARS_CUDA(cudaMemcpyAsync(d_leaves, dl.data(), n * sizeof(mars::DecodeLeaf),
                                   cudaMemcpyHostToDevice, ctx->stream));
     MARS_CUDA(cudaMemsetAsync(a, 128, px, ctx->stream));
     for (uint32_t it = 0; it < iterations; ++it) {
-        MARS_CUDA(mars::launch_decode_step(a, b, (int)w, (int)h, d_owner, d_leaves, ctx->stream));
+        MARS_CUDA(mars::launch_decode_step(a, b, (int)w, (int)h, lg, d_owner, d_leaves, consts,
+                                           ctx->stream));
         ctx->launches += 1;
         std::swap(a, b);
     }
     MARS_CUDA(cudaMemcpyAsync(out, a, px, cudaMemcpyDeviceToHost, ctx->stream));
     return sync_bounded(ctx);
+}
+
+int mars_decode_plan_create(mars_ctx* ctx, const mars_header* hdr, const mars_leaf* leaves,
+                            size_t n, mars_decode_plan** out) {
+    if (!ctx || !hdr || !out || (n && !leaves)) return fail(MARS_EINVAL, "NULL argument");
+    std::vector<mars::DecodeLeaf> dl;
+    std::vector<int32_t> owner;
+    int lg = 0;
+    mars::DecodeConsts consts;
+    if (int e = prepare_decode(hdr, leaves, n, &dl, &owner, &lg, &consts)) return e;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    auto* p = new (std::nothrow) mars_decode_plan;
+    if (!p) return fail(MARS_ENOMEM, "plan allocation failed");
+    p->ctx = ctx;
+    p->w = hdr->width;
+    p->h = hdr->height;
+    p->lg = lg;
+    p->consts = consts;
+    p->nleaves = n;
+    cudaError_t e = cudaMalloc(&p->d_owner, std::max<size_t>(1, owner.size()) * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_leaves, std::max<size_t>(1, n) * sizeof(mars::DecodeLeaf));
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_tmp, (size_t)p->w * p->h);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->d_owner, owner.data(), owner.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n)
+        e = cudaMemcpy(p->d_leaves, dl.data(), n * sizeof(mars::DecodeLeaf), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(p->d_owner);
+        cudaFree(p->d_leaves);
+        cudaFree(p->d_tmp);
+        delete p;
+        return fail(MARS_ECUDA, std::string("decode plan: ") + cudaGetErrorString(e));
+    }
+    *out = p;
+    return MARS_OK;
+}
+
+int mars_decode_plan_run(mars_decode_plan* p, uint32_t iterations, uint8_t* d_out) {
+    if (!p || !d_out) return fail(MARS_EINVAL, "NULL argument");
+    mars_ctx* ctx = p->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    // Ping-pong so that the last iteration lands in d_out.
+    uint8_t* a = (iterations & 1) ? p->d_tmp : d_out;
+    uint8_t* b = (iterations & 1) ? d_out : p->d_tmp;
+    MARS_CUDA(cudaMemsetAsync(a, 128, (size_t)p->w * p->h, ctx->stream));
+    for (uint32_t it = 0; it < iterations; ++it) {
+        MARS_CUDA(mars::launch_decode_step(a, b, (int)p->w, (int)p->h, p->lg, p->d_owner,
+                                           p->d_leaves, p->consts, ctx->stream));
+        ctx->launches += 1;
+        std::swap(a, b);
+    }
+    return MARS_OK;
+}
+
+void mars_decode_plan_free(mars_decode_plan* p) {
+    if (!p) return;
+    cudaSetDevice(p->ctx->device);
+    cudaStreamSynchronize(p->ctx->stream);
+    cudaFree(p->d_owner);
+    cudaFree(p->d_leaves);
+    cudaFree(p->d_tmp);
+    delete p;
 }
 
 int mars_ifs_parse(const uint8_t* data, size_t len, mars_header* header, mars_leaf** leaves,

@@ -39,11 +39,13 @@ void iso_map(uint32_t k, uint32_t u, uint32_t v, uint32_t size, uint32_t* i, uin
     }
 }
 
-static uint32_t ceil_log2(uint32_t q) { return q <= 1 ? 0 : 32 - (uint32_t)__builtin_clz(q - 1); }
+// ceil_log2, virtual_size, bits_coord_* (ifs.rs:58-84); zigzag / unzigzag (mars_format.rs:183-189).
+uint32_t ceil_log2(uint32_t q) { return q <= 1 ? 0 : 32 - (uint32_t)__builtin_clz(q - 1); }
 uint32_t virtual_size(const mars_header& h) { return 1u << ceil_log2(std::max(h.width, h.height)); }
-static uint32_t bits_coord_row(const mars_header& h) { return ceil_log2(h.height / h.shift); }
-static uint32_t bits_coord_col(const mars_header& h) { return ceil_log2(h.width / h.shift); }
-static uint32_t zigzag(int64_t x) { return (uint32_t)((x << 1) ^ (x >> 63)); }
+uint32_t bits_coord_row(const mars_header& h) { return ceil_log2(h.height / h.shift); }
+uint32_t bits_coord_col(const mars_header& h) { return ceil_log2(h.width / h.shift); }
+uint32_t zigzag(int64_t x) { return (uint32_t)((x << 1) ^ (x >> 63)); }
+int64_t unzigzag(uint32_t z) { return (int64_t)(z >> 1) ^ -(int64_t)(z & 1); }
 static uint32_t size_class_of(uint32_t size) { return (uint32_t)__builtin_ctz(size); }
 
 // build_header (encode.rs:1033-1047).
@@ -89,60 +91,6 @@ uint32_t adaptive_shift(uint32_t base, double rms) {
     return base;
 }
 
-namespace {
-
-// ---------------------------------------------------------------- rate snapshot
-
-// AdaptiveModel (crates/mars-entropy/src/lib.rs:36-121): Laplace-seeded counts, +32 per
-// observation, halving above 2^16, 24-bit fixed-point CDF by integer division.
-constexpr uint64_t kPrecisionTotal = 1ull << 24;
-struct AdaptiveModel {
-    std::vector<uint32_t> counts;
-    uint64_t total = 0;
-    explicit AdaptiveModel(uint32_t alphabet = 2) : counts(alphabet, 1u), total(alphabet) {}
-    void update(uint32_t s) {
-        counts[s] += 32;
-        total += 32;
-        if (total >= (1ull << 16)) {
-            uint64_t t = 0;
-            for (auto& c : counts) {
-                c = std::max<uint32_t>(c >> 1, 1u);
-                t += c;
-            }
-            total = t;
-        }
-    }
-    uint32_t scaled(uint64_t c) const {
-        return (uint32_t)(((unsigned __int128)c * (kPrecisionTotal - counts.size())) / total);
-    }
-    double bits_for(uint32_t s) const {
-        uint64_t before = 0;
-        for (uint32_t i = 0; i < s; ++i) before += counts[i];
-        const uint32_t left = scaled(before) + s;
-        const uint32_t right = scaled(before + counts[s]) + s + 1;
-        return -std::log2((double)(right - left) / (double)kPrecisionTotal);
-    }
-};
-
-using ContextKey = std::pair<uint8_t, uint32_t>;
-struct Event {
-    ContextKey ctx;
-    uint32_t alphabet, symbol;
-};
-
-// Field ids and MODE_ALPHABET (crates/mars-codec/src/mars_format.rs:113-133);
-// AFFINE_GRAD_SCALE / _CLAMP (encode.rs:348-353).
-constexpr uint8_t FIELD_SPLIT = 0, FIELD_MODE = 1, FIELD_QALFA = 2, FIELD_QBETA = 3,
-                  FIELD_QBETA_DC = 4, FIELD_ISOMETRY = 5, FIELD_DOM_ROW = 6, FIELD_DOM_COL = 7,
-                  FIELD_GX = 8, FIELD_GY = 9;
-constexpr uint32_t MODE_ALPHABET = 4;
-constexpr double AFFINE_GRAD_SCALE = 64.0;
-constexpr int32_t AFFINE_GRAD_CLAMP = 2048;
-
-struct Predictor {
-    int64_t row = 0, col = 0;
-};
-
 // emit_leaf (mars_format.rs:515-595), modes 0/1/2.
 void emit_leaf(const mars_header& hdr, const mars_leaf& leaf, uint32_t sc, Predictor& pred,
                std::vector<Event>& ev) {
@@ -168,8 +116,6 @@ void emit_leaf(const mars_header& hdr, const mars_leaf& leaf, uint32_t sc, Predi
     }
 }
 
-using LeafMap = std::map<std::tuple<uint32_t, uint32_t, uint32_t>, const mars_leaf*>;
-
 // walk_write (mars_format.rs:460-512).
 bool walk_write(const mars_header& hdr, uint32_t row, uint32_t col, uint32_t size,
                 const LeafMap& by_pos, Predictor& pred, std::vector<Event>& ev) {
@@ -192,6 +138,10 @@ bool walk_write(const mars_header& hdr, uint32_t row, uint32_t col, uint32_t siz
            walk_write(hdr, row, col + half, half, by_pos, pred, ev) &&
            walk_write(hdr, row + half, col + half, half, by_pos, pred, ev);
 }
+
+namespace {
+
+// ---------------------------------------------------------------- rate snapshot
 
 // RateModels (crates/mars-codec/src/rate.rs:55-80) over build_models (lib.rs:269-278).
 struct RateModels {

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/mars_b200.h"
+#include "entropy.hpp"
 
 namespace mars {
 namespace codec {
@@ -50,6 +51,34 @@ int ifs_write(const mars_header& hdr, const std::vector<mars_leaf>& leaves,
 
 // The isometry map of isometry.rs:7-19.
 void iso_map(uint32_t k, uint32_t u, uint32_t v, uint32_t size, uint32_t* i, uint32_t* j);
+
+// .mars event vocabulary (mars_format.rs:113-133, 453-595).
+using entropy::AdaptiveModel;
+using entropy::ContextKey;
+using entropy::Event;
+constexpr uint8_t FIELD_SPLIT = 0, FIELD_MODE = 1, FIELD_QALFA = 2, FIELD_QBETA = 3,
+                  FIELD_QBETA_DC = 4, FIELD_ISOMETRY = 5, FIELD_DOM_ROW = 6, FIELD_DOM_COL = 7,
+                  FIELD_GX = 8, FIELD_GY = 9;
+constexpr uint32_t MODE_ALPHABET = 4;
+constexpr double AFFINE_GRAD_SCALE = 64.0;
+constexpr int32_t AFFINE_GRAD_CLAMP = 2048;
+
+// The domain-position predictor threaded through traversal order (mars_format.rs:386-395).
+struct Predictor {
+    int64_t row = 0, col = 0;
+};
+using LeafMap = std::map<std::tuple<uint32_t, uint32_t, uint32_t>, const mars_leaf*>;
+
+uint32_t ceil_log2(uint32_t q);
+uint32_t bits_coord_row(const mars_header& h);
+uint32_t bits_coord_col(const mars_header& h);
+uint32_t zigzag(int64_t x);
+int64_t unzigzag(uint32_t z);
+
+void emit_leaf(const mars_header& hdr, const mars_leaf& leaf, uint32_t sc, Predictor& pred,
+               std::vector<Event>& ev);
+bool walk_write(const mars_header& hdr, uint32_t row, uint32_t col, uint32_t size,
+                const LeafMap& by_pos, Predictor& pred, std::vector<Event>& ev);
 
 }  // namespace codec
 }  // namespace mars

@@ -75,14 +75,23 @@ cudaError_t launch_reduce(const Partial* partials, int ntiles, int nranges, cons
                           RangeStats rs, DomainStats ds, CandidateOut* out, cudaStream_t st);
 
 // ---- decode (decode.cu) ----
+// One leaf of the decode map in 16 bytes, dequantised on the device:
+//   x: row | col << 16
+//   y: size (bits 0-11) | mode (bits 12-13) | qbeta << 16
+//   z: modes 0/2: dom_row | dom_col << 16;            mode 1: qgx
+//   w: modes 0/2: qalfa (bits 0-16) | isometry << 24;  mode 1: qgy
 struct DecodeLeaf {
-    double alfa, beta;     // dequantised contrast / brightness (mode 0/2), or b0 (mode 1)
-    double gx, gy;         // mode-1 gradients
-    uint32_t row, col, size, mode;
-    uint32_t iso, dom_row, dom_col, qalfa;
+    uint32_t x, y, z, w;
 };
-cudaError_t launch_decode_step(const uint8_t* src, uint8_t* dst, int w, int h,
-                               const int32_t* leaf_of_pixel, const DecodeLeaf* leaves,
+// Header constants of the dequantisation (ifs.rs:416-439).
+struct DecodeConsts {
+    double max_alfa;   // Header::max_alfa()
+    double alfa_den;   // 2^bits_alfa
+    double beta_den;   // 2^bits_beta - 1
+};
+// owner: leaf index (or -1) per cell of 2^lg x 2^lg pixels, row-major, ceil(w/2^lg) wide.
+cudaError_t launch_decode_step(const uint8_t* src, uint8_t* dst, int w, int h, int lg,
+                               const int32_t* owner, const DecodeLeaf* leaves, DecodeConsts c,
                                cudaStream_t st);
 
 }  // namespace mars

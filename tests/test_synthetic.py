@@ -34,3 +34,19 @@ def test_value_statistics():
     img = synthetic.gray(512, 512, 1).astype(np.int64)
     assert img.min() == 0 or img.max() == 255
     assert 40 < img.std() < 100
+
+
+def test_quadtree_leaves_pinned_and_valid():
+    leaves = synthetic.quadtree_leaves(512, 512, 3)
+    assert synthetic.sha256(leaves) == (
+        "20e9e7684f2a54ad953c4c9137a03e3d256b8166345b32156f5dd632a58f1e4d")
+    cover = np.zeros((512, 512), np.int32)
+    for r, c, s in zip(leaves["row"], leaves["col"], leaves["size"]):
+        cover[r:r + s, c:c + s] += 1
+    assert (cover == 1).all()  # a partition of the plane
+    frac = leaves["qalfa"] > 0
+    assert (leaves["mode"][frac] == 2).all()
+    assert (leaves["dom_row"][frac] + 2 * leaves["size"][frac] <= 512).all()
+    assert (leaves["dom_col"][frac] + 2 * leaves["size"][frac] <= 512).all()
+    assert (leaves["dom_row"] % 2 == 0).all() and (leaves["dom_col"] % 2 == 0).all()
+    assert set(np.unique(leaves["mode"])) == {0, 1, 2}
