@@ -48,6 +48,8 @@ WORKLOAD = ("exhaustive search of every RD quadtree node of a 512x512 synthetic 
 # DRAM bytes (read + write) per launch of the dominant search kernel, from one ncu capture
 # of this workload's s=4 level (profiles/corr_tc_s4_512x512_ncu.md).
 NCU_TRAFFIC = {4: 21_066_496 + 12_032}
+# The same for one decode iteration, by plane side (profiles/decode_cell_*_ncu.md).
+NCU_DECODE_TRAFFIC = {4096: 34_837_248 + 706_816}
 
 
 def rank_info():
@@ -192,7 +194,8 @@ def cpu_baseline(budget_s=12.0, seed=1):
     return value, cores, desc
 
 
-DECODE_SIDE = 16384
+DECODE_SIDE = 4096         # the decode GB/s figure: both planes (2 x 16.8 MB) fit in L2
+DECODE_SIDE_LARGE = 16384  # both planes (2 x 268 MB) exceed L2: the HBM-resident case
 DECODE_ITERS = 10
 
 
@@ -219,11 +222,11 @@ def decode_cpu_baseline(side=2048, seed=1):
                       f"{DECODE_ITERS} iterations"}
 
 
-def run_decode(args, mb, ctx, stream, dev, peaks, with_cpu):
+def run_decode(args, mb, ctx, stream, dev, peaks, side, with_cpu, flush=None):
     """Fixed-point decode: DECODE_ITERS iterations of the gather over a synthetic quadtree
-    map of a DECODE_SIDE^2 plane (both ping-pong planes larger than L2)."""
+    map of a side x side plane, from the flat-128 seed.  `flush` (a device buffer larger
+    than L2) is rewritten between timed decodes when the planes would otherwise stay in L2."""
     import torch
-    side = DECODE_SIDE
     leaves = synthetic.quadtree_leaves(side, side, 1)
     hdr = decode_header(mb, side)
     plan = ctx.decode_plan(hdr, leaves)
@@ -235,7 +238,9 @@ def run_decode(args, mb, ctx, stream, dev, peaks, with_cpu):
     launches0 = ctx.launches
     t = 0.0
     with ClockSampler(dev.index) as clocks:
-        for _ in range(steps):
+        for k in range(steps):
+            if flush is not None:
+                flush.fill_(k & 0xFF)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             plan.run(DECODE_ITERS, out.data_ptr())
@@ -257,16 +262,20 @@ def run_decode(args, mb, ctx, stream, dev, peaks, with_cpu):
     ctx.decode(hdr, leaves, DECODE_ITERS)
     t_e2e = time.perf_counter() - t0
     del out
+    resident = 2 * px < 126e6
     return {
         "workload": f"decode_iterative of a {side}x{side} synthetic quadtree map "
                     f"({len(leaves)} leaves, sizes 32..4, modes 0/1/2), {DECODE_ITERS} iterations "
                     "from the flat-128 seed",
         "value": px * DECODE_ITERS / t_dec, "unit": "pixel-iterations/s",
         "ms_per_decode": 1e3 * t_dec, "steps": steps, "gpu_launches": launches,
-        "l2": "not flushed: both 268 MB planes exceed L2", "clocks": clocks.summary(),
-        "roofline": {"bound": "hbm", "kernel": "decode_step4_kernel", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                     "peak_source": src,
+        "l2": ("planes L2-resident across the iterations of one decode; L2 flushed between "
+               "timed decodes (256 MiB write)") if resident else
+              "not flushed: both planes exceed L2",
+        "clocks": clocks.summary(),
+        "roofline": {"bound": "hbm", "kernel": "decode_cell_kernel", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": NCU_DECODE_TRAFFIC.get(side), "peak_source": src,
                      "bytes_per_launch": algo / DECODE_ITERS,
                      "launch_ms": 1e3 * t_dec / DECODE_ITERS},
         "e2e": {"value": px * DECODE_ITERS / t_e2e, "unit": "pixel-iterations/s",
@@ -401,10 +410,11 @@ def run_gpu(args):
         h2d = W * H + nodes * 8
         d2h = nodes * 80 + 8
 
-    decode = None
+    decode = decode_large = None
     if not args.no_decode:
-        decode = run_decode(args, mb, ctx, stream, dev, peaks,
-                            with_cpu=rank == 0 and world == 1 and not args.no_cpu)
+        with_cpu = rank == 0 and world == 1 and not args.no_cpu
+        decode = run_decode(args, mb, ctx, stream, dev, peaks, DECODE_SIDE, with_cpu, flush)
+        decode_large = run_decode(args, mb, ctx, stream, dev, peaks, DECODE_SIDE_LARGE, False)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -433,6 +443,7 @@ def run_gpu(args):
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "decode": decode,
+            "decode_large": decode_large,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

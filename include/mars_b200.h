@@ -58,11 +58,15 @@ typedef struct mars_params {
     double lambda;
 } mars_params;
 
-/* The EncodeOptions fields supported (encode.rs:78-109): allowed_modes (modes 0, 1 and 2;
- * mode 3 is rejected with MARS_EUNSUPPORTED) and adaptive_density. */
+/* The EncodeOptions fields supported (encode.rs:78-109): allowed_modes (modes 0-3),
+ * adaptive_density and residual_quantisation: residual_adaptive != 0 is LambdaAdaptive
+ * (the step from lambda, 8 without one), else Fixed(residual_qstep) with 0 meaning the
+ * default step 8 (ResidualQstep::LEGACY). */
 typedef struct mars_options {
     uint8_t allowed_modes[4];
     int32_t adaptive_density;
+    int32_t residual_adaptive;
+    float residual_qstep;
 } mars_options;
 
 /* RawMoments, encode.rs:225-232. */
@@ -77,15 +81,19 @@ typedef struct mars_candidate {
     mars_moments moments;
 } mars_candidate;
 
-/* ifs::Leaf, crates/mars-codec/src/ifs.rs:101-117 (modes 0, 1, 2). */
+/* ifs::Leaf, crates/mars-codec/src/ifs.rs:101-117.  A mode-3 leaf's `residual` (size*size
+ * quantised DCT levels) travels outside the struct: calls that take or return leaves take or
+ * return a residual pool with the levels of every mode-3 leaf, concatenated in leaf order. */
 typedef struct mars_leaf {
     uint32_t row, col, size, mode, qalfa, qbeta, isometry, dom_row, dom_col;
     int32_t qgx, qgy;
 } mars_leaf;
 
-/* ifs::Header, ifs.rs:13-22. */
+/* mars_format::Header (mars_format.rs:62-67): the ifs::Header geometry (ifs.rs:13-22) and
+ * the residual step, binary32; 0 stands for the default step 8 (ResidualQstep::LEGACY). */
 typedef struct mars_header {
     uint32_t bits_alfa, bits_beta, min_size, max_size, shift, width, height, int_max_alfa;
+    float residual_qstep;
 } mars_header;
 
 /* EncodeCounters, encode.rs:1011-1021. */
@@ -180,23 +188,27 @@ int mars_search_blocks_noalloc(const uint8_t* d_plane, uint32_t width, uint32_t 
 
 /* encode_image_with_search with this library as the provider: the threshold walk when
  * params->has_lambda == 0, else the exhaustive t_rms = 8 warm-up (served from the same
- * table) followed by the bottom-up RD walk.  *leaves is freed with mars_leaves_free. */
+ * table) followed by the bottom-up RD walk over modes 0-3.  *leaves is freed with
+ * mars_leaves_free, *residuals (the mode-3 levels) with mars_residuals_free. */
 int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
                 const mars_params* params, const mars_options* options, mars_header* header,
-                mars_leaf** leaves, size_t* nleaves, mars_counters* counters);
+                mars_leaf** leaves, size_t* nleaves, int32_t** residuals, size_t* nresiduals,
+                mars_counters* counters);
 void mars_leaves_free(mars_leaf* leaves);
+void mars_residuals_free(int32_t* residuals);
 
-/* decode_iterative: `iterations` fixed-point steps from the flat-128 seed (modes 0/1/2).
+/* decode_iterative: `iterations` fixed-point steps from the flat-128 seed (modes 0-3).
  * `out` is a host buffer of width*height bytes. */
 int mars_decode(mars_ctx* ctx, const mars_header* header, const mars_leaf* leaves, size_t n,
-                uint32_t iterations, uint8_t* out);
+                const int32_t* residuals, size_t nresiduals, uint32_t iterations, uint8_t* out);
 
 /* Repeated decodes of one leaf list (progressive display, the attractor's forward map):
  * the leaf table and the owner map are validated and uploaded once; each run writes
  * `iterations` steps from the flat-128 seed into the device buffer d_out (width*height
  * bytes), asynchronously on the context's stream. */
 int mars_decode_plan_create(mars_ctx* ctx, const mars_header* header, const mars_leaf* leaves,
-                            size_t n, mars_decode_plan** out);
+                            size_t n, const int32_t* residuals, size_t nresiduals,
+                            mars_decode_plan** out);
 int mars_decode_plan_run(mars_decode_plan* plan, uint32_t iterations, uint8_t* d_out);
 void mars_decode_plan_free(mars_decode_plan* plan);
 
@@ -209,13 +221,14 @@ void mars_bytes_free(uint8_t* bytes);
 
 /* .mars v0 plane container (mars_format.rs:232-400): 24-byte header carrying the residual
  * step as binary32, then the TREE section entropy-coded with adaptive models over the rANS
- * stack coder.  Leaves of modes 0/1/2; mode 3 is refused with MARS_EUNSUPPORTED.  Format
- * errors (bad magic, truncation, degenerate header, out-of-image domain, ...) return
- * MARS_EFORMAT on read and MARS_EINVAL on write, with the reference's message text. */
-int mars_format_write(const mars_header* header, float residual_qstep, const mars_leaf* leaves,
-                      size_t n, uint8_t** out, size_t* len);
-int mars_format_read(const uint8_t* data, size_t len, mars_header* header, float* residual_qstep,
-                     mars_leaf** leaves, size_t* nleaves);
+ * stack coder, modes 0-3.  Format errors (bad magic, truncation, degenerate header,
+ * out-of-image domain, ...) return MARS_EFORMAT on read and MARS_EINVAL on write, with the
+ * reference's message text.  Read output is freed with mars_leaves_free and
+ * mars_residuals_free. */
+int mars_format_write(const mars_header* header, const mars_leaf* leaves, size_t n,
+                      const int32_t* residuals, size_t nresiduals, uint8_t** out, size_t* len);
+int mars_format_read(const uint8_t* data, size_t len, mars_header* header, mars_leaf** leaves,
+                     size_t* nleaves, int32_t** residuals, size_t* nresiduals);
 
 /* mars_entropy::Event (lib.rs:188-193): context = (field, disambiguator). */
 typedef struct mars_event {

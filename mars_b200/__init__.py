@@ -43,13 +43,17 @@ class Params(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = [("allowed_modes", C.c_uint8 * 4), ("adaptive_density", C.c_int32)]
+    """EncodeOptions (encode.rs:78-109): allowed modes, adaptive density, residual
+    quantisation (LambdaAdaptive when residual_adaptive, else Fixed(residual_qstep), 0 = 8)."""
+    _fields_ = [("allowed_modes", C.c_uint8 * 4), ("adaptive_density", C.c_int32),
+                ("residual_adaptive", C.c_int32), ("residual_qstep", C.c_float)]
 
 
 class Header(C.Structure):
+    """mars_format::Header: the ifs geometry plus the binary32 residual step (0 = 8)."""
     _fields_ = [(n, C.c_uint32) for n in (
         "bits_alfa", "bits_beta", "min_size", "max_size", "shift", "width", "height",
-        "int_max_alfa")]
+        "int_max_alfa")] + [("residual_qstep", C.c_float)]
 
 
 class Counters(C.Structure):
@@ -75,6 +79,7 @@ EXPORTS = (
     "mars_ifs_parse", "mars_ifs_write", "mars_bytes_free", "mars_search_blocks_noalloc",
     "mars_decode_plan_create", "mars_decode_plan_run", "mars_decode_plan_free",
     "mars_format_write", "mars_format_read", "mars_entropy_encode", "mars_entropy_decode",
+    "mars_residuals_free",
 )
 
 _lib = None
@@ -115,11 +120,11 @@ def lib():
     L.mars_search_nodes_device.argtypes = [vp, vp, u32, u32, P(Params), vp, sz, P(sz), P(u64)]
     L.mars_search_blocks_noalloc.argtypes = [vp, u32, u32, u32, u32, P(Params), vp, vp, sz, vp, vp]
     L.mars_encode.argtypes = [vp, vp, u32, u32, P(Params), P(Options), P(Header), P(vp), P(sz),
-                              P(Counters)]
+                              P(vp), P(sz), P(Counters)]
     L.mars_leaves_free.argtypes = [vp]
     L.mars_leaves_free.restype = None
-    L.mars_decode.argtypes = [vp, P(Header), vp, sz, u32, vp]
-    L.mars_decode_plan_create.argtypes = [vp, P(Header), vp, sz, P(vp)]
+    L.mars_decode.argtypes = [vp, P(Header), vp, sz, vp, sz, u32, vp]
+    L.mars_decode_plan_create.argtypes = [vp, P(Header), vp, sz, vp, sz, P(vp)]
     L.mars_decode_plan_run.argtypes = [vp, u32, vp]
     L.mars_decode_plan_free.argtypes = [vp]
     L.mars_decode_plan_free.restype = None
@@ -127,8 +132,10 @@ def lib():
     L.mars_ifs_write.argtypes = [P(Header), vp, sz, P(vp), P(sz)]
     L.mars_bytes_free.argtypes = [vp]
     L.mars_bytes_free.restype = None
-    L.mars_format_write.argtypes = [P(Header), C.c_float, vp, sz, P(vp), P(sz)]
-    L.mars_format_read.argtypes = [vp, sz, P(Header), P(C.c_float), P(vp), P(sz)]
+    L.mars_format_write.argtypes = [P(Header), vp, sz, vp, sz, P(vp), P(sz)]
+    L.mars_format_read.argtypes = [vp, sz, P(Header), P(vp), P(sz), P(vp), P(sz)]
+    L.mars_residuals_free.argtypes = [vp]
+    L.mars_residuals_free.restype = None
     L.mars_entropy_encode.argtypes = [vp, sz, P(vp), P(sz)]
     L.mars_entropy_decode.argtypes = [vp, sz, vp, sz, vp]
     _lib = L
@@ -283,33 +290,49 @@ class Context:
         rr, cc = np.meshgrid(np.arange(h // size) * size, np.arange(w // size) * size, indexing="ij")
         return self.search_blocks(a, size, shift, params, rr.ravel(), cc.ravel())
 
-    def encode(self, img, params: Params, allowed_modes=(1, 0, 1, 0), adaptive_density=False):
-        """encode_image_with_search with the GPU provider: (header, leaves, counters)."""
+    def encode(self, img, params: Params, allowed_modes=(1, 0, 1, 0), adaptive_density=False,
+               residual_adaptive=False, residual_qstep=0.0):
+        """encode_image_with_search with the GPU provider: (header, leaves, residuals,
+        counters); `residuals` holds the levels of the mode-3 leaves, size*size each, in
+        leaf order."""
         a = _plane(img)
         h, w = a.shape
-        opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density))
+        opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density),
+                       int(residual_adaptive), float(residual_qstep))
         hdr, cnt = Header(), Counters()
         ptr, n = C.c_void_p(), C.c_size_t()
+        rptr, rn = C.c_void_p(), C.c_size_t()
         check(lib().mars_encode(self._h, a.ctypes.data, w, h, C.byref(params), C.byref(opts),
-                                C.byref(hdr), C.byref(ptr), C.byref(n), C.byref(cnt)))
+                                C.byref(hdr), C.byref(ptr), C.byref(n), C.byref(rptr),
+                                C.byref(rn), C.byref(cnt)))
         leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize),
                                dtype=LEAF_DTYPE).copy()
+        resid = np.frombuffer(C.string_at(rptr, rn.value * 4), dtype=np.int32).copy()
         lib().mars_leaves_free(ptr)
-        return hdr, leaves, cnt
+        lib().mars_residuals_free(rptr)
+        return hdr, leaves, resid, cnt
 
-    def decode_plan(self, hdr: Header, leaves: np.ndarray) -> "DecodePlan":
+    def decode_plan(self, hdr: Header, leaves: np.ndarray, residuals=None) -> "DecodePlan":
         leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+        res = _residuals(residuals)
         h = C.c_void_p()
         check(lib().mars_decode_plan_create(self._h, C.byref(hdr), leaves.ctypes.data,
-                                            len(leaves), C.byref(h)))
+                                            len(leaves), res.ctypes.data, len(res), C.byref(h)))
         return DecodePlan(h.value)
 
-    def decode(self, hdr: Header, leaves: np.ndarray, iterations: int = 10) -> np.ndarray:
+    def decode(self, hdr: Header, leaves: np.ndarray, iterations: int = 10,
+               residuals=None) -> np.ndarray:
         leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+        res = _residuals(residuals)
         out = np.zeros((hdr.height, hdr.width), dtype=np.uint8)
         check(lib().mars_decode(self._h, C.byref(hdr), leaves.ctypes.data, len(leaves),
-                                iterations, out.ctypes.data))
+                                res.ctypes.data, len(res), iterations, out.ctypes.data))
         return out
+
+
+def _residuals(residuals) -> np.ndarray:
+    return np.ascontiguousarray(residuals if residuals is not None else np.zeros(0),
+                                dtype=np.int32)
 
 
 class DecodePlan:
@@ -355,27 +378,32 @@ def qstep_from_lambda(lam: float) -> float:
     return float(np.float32(min(max(step, 1.0), 65535.0)))
 
 
-def format_write(hdr: Header, leaves: np.ndarray, residual_qstep: float = LEGACY_QSTEP) -> bytes:
-    """mars_format::write (mars_format.rs:232-300): the .mars v0 bytes of (hdr, leaves)."""
+def format_write(hdr: Header, leaves: np.ndarray, residuals=None) -> bytes:
+    """mars_format::write (mars_format.rs:232-300): the .mars v0 bytes of (hdr, leaves);
+    the residual step is the header's (0 = 8)."""
     leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    res = _residuals(residuals)
     ptr, n = C.c_void_p(), C.c_size_t()
-    check(lib().mars_format_write(C.byref(hdr), float(np.float32(residual_qstep)),
-                                  leaves.ctypes.data, len(leaves), C.byref(ptr), C.byref(n)))
+    check(lib().mars_format_write(C.byref(hdr), leaves.ctypes.data, len(leaves), res.ctypes.data,
+                                  len(res), C.byref(ptr), C.byref(n)))
     data = C.string_at(ptr, n.value)
     lib().mars_bytes_free(ptr)
     return data
 
 
 def format_read(data: bytes):
-    """mars_format::read (mars_format.rs:302-400) -> (header, residual_qstep, leaves)."""
+    """mars_format::read (mars_format.rs:302-400) -> (header, leaves, residuals)."""
     buf = np.frombuffer(data, dtype=np.uint8)
-    hdr, q = Header(), C.c_float()
+    hdr = Header()
     ptr, n = C.c_void_p(), C.c_size_t()
-    check(lib().mars_format_read(buf.ctypes.data, len(data), C.byref(hdr), C.byref(q),
-                                 C.byref(ptr), C.byref(n)))
+    rptr, rn = C.c_void_p(), C.c_size_t()
+    check(lib().mars_format_read(buf.ctypes.data, len(data), C.byref(hdr), C.byref(ptr),
+                                 C.byref(n), C.byref(rptr), C.byref(rn)))
     leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize), dtype=LEAF_DTYPE).copy()
+    resid = np.frombuffer(C.string_at(rptr, rn.value * 4), dtype=np.int32).copy()
     lib().mars_leaves_free(ptr)
-    return hdr, q.value, leaves
+    lib().mars_residuals_free(rptr)
+    return hdr, leaves, resid
 
 
 def entropy_encode(events) -> bytes:

@@ -18,6 +18,7 @@
 
 #include "../../include/mars_b200.h"
 #include "codec.hpp"
+#include "residual.hpp"
 #include "kernels.cuh"
 #include "tc.cuh"
 
@@ -648,32 +649,47 @@ int mars_search_nodes_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t wid
 
 int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
                 const mars_params* params, const mars_options* options, mars_header* header,
-                mars_leaf** leaves, size_t* nleaves, mars_counters* counters) {
-    if (!ctx || !plane || !options || !header || !leaves || !nleaves || !counters)
+                mars_leaf** leaves, size_t* nleaves, int32_t** residuals, size_t* nresiduals,
+                mars_counters* counters) {
+    if (!ctx || !plane || !options || !header || !leaves || !nleaves || !residuals ||
+        !nresiduals || !counters)
         return fail(MARS_EINVAL, "NULL argument");
     if (int e = check_params(params)) return e;
-    if (options->allowed_modes[3])
-        return fail(MARS_EUNSUPPORTED, "mode 3 (DCT residual) is not supported");
+    if (!options->residual_adaptive && options->residual_qstep != 0.0f &&
+        !(std::isfinite(options->residual_qstep) && options->residual_qstep >= 1.0f &&
+          options->residual_qstep <= 65535.0f))
+        return fail(MARS_EINVAL, "residual qstep must be finite and in [1, 65535]");
     mars_table* table = nullptr;
     const bool adaptive = params->has_lambda && options->adaptive_density;
     if (int e = build_table(ctx, plane, nullptr, width, height, params, adaptive, &table)) return e;
     std::unique_ptr<mars_table, void (*)(mars_table*)> guard(table, mars_search_table_free);
-    mars::codec::Provider provider = [table](uint32_t row, uint32_t col, uint32_t size,
-                                             uint32_t shift, mars::codec::SearchAnswer* ans) {
+    const mars::codec::Provider provider = [table](uint32_t row, uint32_t col, uint32_t size,
+                                                   uint32_t shift, mars::codec::SearchAnswer* ans) {
         return mars_search_table_lookup(table, row, col, size, shift, &ans->cand, &ans->evals);
     };
     std::vector<mars_leaf> out;
+    std::vector<int32_t> res;
     const mars::codec::Image im{plane, width, height};
-    if (int e = mars::codec::encode(im, *params, *options, provider, header, &out, counters))
+    if (int e = mars::codec::encode(im, *params, *options, provider, provider, header, &out, &res,
+                                    counters))
         return e;
     *nleaves = out.size();
     *leaves = (mars_leaf*)std::malloc(std::max<size_t>(1, out.size()) * sizeof(mars_leaf));
     if (!*leaves) return fail(MARS_ENOMEM, "leaf array allocation failed");
     std::memcpy(*leaves, out.data(), out.size() * sizeof(mars_leaf));
+    *nresiduals = res.size();
+    *residuals = (int32_t*)std::malloc(std::max<size_t>(1, res.size()) * sizeof(int32_t));
+    if (!*residuals) {
+        std::free(*leaves);
+        *leaves = nullptr;
+        return fail(MARS_ENOMEM, "residual array allocation failed");
+    }
+    if (!res.empty()) std::memcpy(*residuals, res.data(), res.size() * sizeof(int32_t));
     return MARS_OK;
 }
 
 void mars_leaves_free(mars_leaf* leaves) { std::free(leaves); }
+void mars_residuals_free(int32_t* residuals) { std::free(residuals); }
 void mars_bytes_free(uint8_t* bytes) { std::free(bytes); }
 
 }  // extern "C"
@@ -687,9 +703,13 @@ namespace {
 // .ifs stream and every encoder output lie in.  The owner map's cell is the largest power
 // of two dividing every leaf's row, column and size (4 for the usual quadtree with
 // min_size 4), capped at 32; later leaves overwrite earlier ones, as in the reference.
+// Mode-3 residuals are rebuilt here on the host exactly as decode_leaf does
+// (ifs.rs:441-456) -- the inverse DCT uses the C library's cosine, as the reference's
+// does -- in domain-local (u, v) order, and their offsets are returned per leaf.
 int prepare_decode(const mars_header* hdr, const mars_leaf* leaves, size_t n,
-                   std::vector<mars::DecodeLeaf>* dl, std::vector<int32_t>* owner, int* lg_out,
-                   mars::DecodeConsts* consts) {
+                   const int32_t* residuals, size_t nresiduals, std::vector<mars::DecodeLeaf>* dl,
+                   std::vector<int32_t>* owner, int* lg_out, mars::DecodeConsts* consts,
+                   std::vector<int32_t>* resid_off, std::vector<double>* resid_values) {
     const uint32_t w = hdr->width, h = hdr->height;
     if (w == 0 || h == 0) return fail(MARS_EINVAL, "empty plane");
     if (w > 65535 || h > 65535) return fail(MARS_EINVAL, "plane sides must be at most 65535");
@@ -704,7 +724,7 @@ int prepare_decode(const mars_header* hdr, const mars_leaf* leaves, size_t n,
             return fail(MARS_EINVAL, "leaf " + std::to_string(k) + " lies outside the plane");
         if (L.size > 4095)
             return fail(MARS_EUNSUPPORTED, "leaf " + std::to_string(k) + " is wider than 4095");
-        if (L.mode > 2) return fail(MARS_EUNSUPPORTED, "leaf mode 3 is not supported");
+        if (L.mode > 3) return fail(MARS_EINVAL, "leaf " + std::to_string(k) + " has mode > 3");
         if (L.qbeta > qbeta_max || (L.mode != 1 && L.qalfa > qalfa_max))
             return fail(MARS_EINVAL, "leaf " + std::to_string(k) +
                                          " has coefficients wider than the header's bits");
@@ -726,6 +746,23 @@ int prepare_decode(const mars_header* hdr, const mars_leaf* leaves, size_t n,
     consts->max_alfa = (double)hdr->int_max_alfa / 256.0 * 8.0;
     consts->alfa_den = (double)qalfa_max;
     consts->beta_den = (double)qbeta_max;
+    std::vector<int64_t> offs;
+    if (!mars::codec::residual_offsets(leaves, n, nresiduals, &offs) || (nresiduals && !residuals))
+        return fail(MARS_EINVAL, "the residual pool does not hold size*size levels per mode-3 leaf");
+    resid_off->clear();
+    resid_values->clear();
+    if (nresiduals) {
+        if (nresiduals > 0x7fffffffull) return fail(MARS_EINVAL, "residual pool too large");
+        resid_off->assign(n, -1);
+        const double step = mars::codec::qstep_of(*hdr);
+        for (size_t k = 0; k < n; ++k) {
+            if (offs[k] < 0) continue;
+            (*resid_off)[k] = (int32_t)resid_values->size();
+            const std::vector<double> v =
+                mars::residual::values(residuals + offs[k], leaves[k].size, step);
+            resid_values->insert(resid_values->end(), v.begin(), v.end());
+        }
+    }
     const int lg = __builtin_ctz(align_bits);
     const uint32_t cell = 1u << lg;
     const uint32_t mw = (w + cell - 1) >> lg, mh = (h + cell - 1) >> lg;
@@ -746,23 +783,26 @@ struct mars_decode_plan {
     mars_ctx* ctx = nullptr;
     uint32_t w = 0, h = 0;
     int lg = 0;
-    mars::DecodeConsts consts{};
     size_t nleaves = 0;
     int32_t* d_owner = nullptr;
-    mars::DecodeLeaf* d_leaves = nullptr;
-    uint8_t* d_tmp = nullptr;  // ping-pong partner of the caller's output buffer
+    mars::DecodeMap* d_maps = nullptr;
+    double* d_rvals = nullptr;  // mode-3 residual values, or null
+    uint8_t* d_tmp = nullptr;   // ping-pong partner of the caller's output buffer
 };
 
 extern "C" {
 
 int mars_decode(mars_ctx* ctx, const mars_header* hdr, const mars_leaf* leaves, size_t n,
-                uint32_t iterations, uint8_t* out) {
+                const int32_t* residuals, size_t nresiduals, uint32_t iterations, uint8_t* out) {
     if (!ctx || !hdr || !out || (n && !leaves)) return fail(MARS_EINVAL, "NULL argument");
     std::vector<mars::DecodeLeaf> dl;
-    std::vector<int32_t> owner;
+    std::vector<int32_t> owner, roff;
+    std::vector<double> rvals;
     int lg = 0;
     mars::DecodeConsts consts;
-    if (int e = prepare_decode(hdr, leaves, n, &dl, &owner, &lg, &consts)) return e;
+    if (int e = prepare_decode(hdr, leaves, n, residuals, nresiduals, &dl, &owner, &lg, &consts,
+                               &roff, &rvals))
+        return e;
     const uint32_t w = hdr->width, h = hdr->height;
     std::lock_guard<std::mutex> lock(ctx->mu);
     MARS_CUDA(cudaSetDevice(ctx->device));
@@ -770,19 +810,34 @@ int mars_decode(mars_ctx* ctx, const mars_header* hdr, const mars_leaf* leaves, 
     uint8_t *a = nullptr, *b = nullptr;
     int32_t* d_owner = nullptr;
     mars::DecodeLeaf* d_leaves = nullptr;
+    mars::DecodeMap* d_maps = nullptr;
+    int32_t* d_roff = nullptr;
+    double* d_rvals = nullptr;
     const size_t px = (size_t)w * h;
     MARS_CUDA(sc.get(&a, px));
     MARS_CUDA(sc.get(&b, px));
     MARS_CUDA(sc.get(&d_owner, owner.size()));
     MARS_CUDA(sc.get(&d_leaves, n));
+    MARS_CUDA(sc.get(&d_maps, n));
     MARS_CUDA(cudaMemcpyAsync(d_owner, owner.data(), owner.size() * 4, cudaMemcpyHostToDevice,
                               ctx->stream));
-    if (n)
+    if (!rvals.empty()) {
+        MARS_CUDA(sc.get(&d_roff, n));
+        MARS_CUDA(sc.get(&d_rvals, rvals.size()));
+        MARS_CUDA(cudaMemcpyAsync(d_roff, roff.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream));
+        MARS_CUDA(cudaMemcpyAsync(d_rvals, rvals.data(), rvals.size() * 8, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    }
+    if (n) {
         MARS_CUDA(cudaMemcpyAsync(d_leaves, dl.data(), n * sizeof(mars::DecodeLeaf),
                                   cudaMemcpyHostToDevice, ctx->stream));
+        MARS_CUDA(mars::launch_decode_expand(d_leaves, d_roff, (int)n, consts, d_maps,
+                                             ctx->stream));
+        ctx->launches += 1;
+    }
     MARS_CUDA(cudaMemsetAsync(a, 128, px, ctx->stream));
     for (uint32_t it = 0; it < iterations; ++it) {
-        MARS_CUDA(mars::launch_decode_step(a, b, (int)w, (int)h, lg, d_owner, d_leaves, consts,
+        MARS_CUDA(mars::launch_decode_step(a, b, (int)w, (int)h, lg, d_owner, d_maps, d_rvals,
                                            ctx->stream));
         ctx->launches += 1;
         std::swap(a, b);
@@ -792,13 +847,17 @@ int mars_decode(mars_ctx* ctx, const mars_header* hdr, const mars_leaf* leaves, 
 }
 
 int mars_decode_plan_create(mars_ctx* ctx, const mars_header* hdr, const mars_leaf* leaves,
-                            size_t n, mars_decode_plan** out) {
+                            size_t n, const int32_t* residuals, size_t nresiduals,
+                            mars_decode_plan** out) {
     if (!ctx || !hdr || !out || (n && !leaves)) return fail(MARS_EINVAL, "NULL argument");
     std::vector<mars::DecodeLeaf> dl;
-    std::vector<int32_t> owner;
+    std::vector<int32_t> owner, roff;
+    std::vector<double> rvals;
     int lg = 0;
     mars::DecodeConsts consts;
-    if (int e = prepare_decode(hdr, leaves, n, &dl, &owner, &lg, &consts)) return e;
+    if (int e = prepare_decode(hdr, leaves, n, residuals, nresiduals, &dl, &owner, &lg, &consts,
+                               &roff, &rvals))
+        return e;
     std::lock_guard<std::mutex> lock(ctx->mu);
     MARS_CUDA(cudaSetDevice(ctx->device));
     auto* p = new (std::nothrow) mars_decode_plan;
@@ -807,18 +866,39 @@ int mars_decode_plan_create(mars_ctx* ctx, const mars_header* hdr, const mars_le
     p->w = hdr->width;
     p->h = hdr->height;
     p->lg = lg;
-    p->consts = consts;
     p->nleaves = n;
+    mars::DecodeLeaf* d_leaves = nullptr;
+    int32_t* d_roff = nullptr;
     cudaError_t e = cudaMalloc(&p->d_owner, std::max<size_t>(1, owner.size()) * 4);
-    if (e == cudaSuccess) e = cudaMalloc(&p->d_leaves, std::max<size_t>(1, n) * sizeof(mars::DecodeLeaf));
+    if (e == cudaSuccess) e = cudaMalloc(&d_leaves, std::max<size_t>(1, n) * sizeof(mars::DecodeLeaf));
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_maps, std::max<size_t>(1, n) * sizeof(mars::DecodeMap));
     if (e == cudaSuccess) e = cudaMalloc(&p->d_tmp, (size_t)p->w * p->h);
+    if (e == cudaSuccess && !rvals.empty()) {
+        e = cudaMalloc(&d_roff, n * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_rvals, rvals.size() * 8);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_roff, roff.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(p->d_rvals, rvals.data(), rvals.size() * 8, cudaMemcpyHostToDevice,
+                                ctx->stream);
+    }
     if (e == cudaSuccess)
-        e = cudaMemcpy(p->d_owner, owner.data(), owner.size() * 4, cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(p->d_owner, owner.data(), owner.size() * 4, cudaMemcpyHostToDevice,
+                            ctx->stream);
     if (e == cudaSuccess && n)
-        e = cudaMemcpy(p->d_leaves, dl.data(), n * sizeof(mars::DecodeLeaf), cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(d_leaves, dl.data(), n * sizeof(mars::DecodeLeaf),
+                            cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && n) {
+        e = mars::launch_decode_expand(d_leaves, d_roff, (int)n, consts, p->d_maps, ctx->stream);
+        ctx->launches += 1;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_leaves);
+    cudaFree(d_roff);
     if (e != cudaSuccess) {
         cudaFree(p->d_owner);
-        cudaFree(p->d_leaves);
+        cudaFree(p->d_maps);
+        cudaFree(p->d_rvals);
         cudaFree(p->d_tmp);
         delete p;
         return fail(MARS_ECUDA, std::string("decode plan: ") + cudaGetErrorString(e));
@@ -838,7 +918,7 @@ int mars_decode_plan_run(mars_decode_plan* p, uint32_t iterations, uint8_t* d_ou
     MARS_CUDA(cudaMemsetAsync(a, 128, (size_t)p->w * p->h, ctx->stream));
     for (uint32_t it = 0; it < iterations; ++it) {
         MARS_CUDA(mars::launch_decode_step(a, b, (int)p->w, (int)p->h, p->lg, p->d_owner,
-                                           p->d_leaves, p->consts, ctx->stream));
+                                           p->d_maps, p->d_rvals, ctx->stream));
         ctx->launches += 1;
         std::swap(a, b);
     }
@@ -850,7 +930,8 @@ void mars_decode_plan_free(mars_decode_plan* p) {
     cudaSetDevice(p->ctx->device);
     cudaStreamSynchronize(p->ctx->stream);
     cudaFree(p->d_owner);
-    cudaFree(p->d_leaves);
+    cudaFree(p->d_maps);
+    cudaFree(p->d_rvals);
     cudaFree(p->d_tmp);
     delete p;
 }

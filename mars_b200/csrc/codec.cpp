@@ -2,6 +2,7 @@
 // Every function cites the reference function it restates (paths relative to the
 // daleobrien/mars root).  Compiled with -ffp-contract=off: Rust never fuses a*b+c.
 #include "codec.hpp"
+#include "residual.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -59,6 +60,7 @@ mars_header build_header(uint32_t w, uint32_t h, const mars_params& p) {
     hdr.width = w;
     hdr.height = h;
     hdr.int_max_alfa = quantise_f64(p.max_alfa / 8.0 * 256.0, 255);
+    hdr.residual_qstep = 8.0f;
     return hdr;
 }
 
@@ -91,9 +93,9 @@ uint32_t adaptive_shift(uint32_t base, double rms) {
     return base;
 }
 
-// emit_leaf (mars_format.rs:515-595), modes 0/1/2.
-void emit_leaf(const mars_header& hdr, const mars_leaf& leaf, uint32_t sc, Predictor& pred,
-               std::vector<Event>& ev) {
+// emit_leaf (mars_format.rs:515-595); mode 3 appends residual::encode_events.
+void emit_leaf(const mars_header& hdr, const mars_leaf& leaf, const int32_t* levels, uint32_t sc,
+               Predictor& pred, std::vector<Event>& ev) {
     ev.push_back({{FIELD_MODE, sc}, MODE_ALPHABET, leaf.mode});
     if (leaf.mode == 0) {
         ev.push_back({{FIELD_QBETA_DC, sc}, 1u << hdr.bits_beta, leaf.qbeta});
@@ -113,6 +115,8 @@ void emit_leaf(const mars_header& hdr, const mars_leaf& leaf, uint32_t sc, Predi
                       zigzag(cu - pred.col)});
         pred.row = ru;
         pred.col = cu;
+        if (leaf.mode == 3)
+            residual::encode_events(levels, (size_t)leaf.size * leaf.size, sc, ev);
     }
 }
 
@@ -126,7 +130,7 @@ bool walk_write(const mars_header& hdr, uint32_t row, uint32_t col, uint32_t siz
     auto it = by_pos.find({row, col, size});
     if (it != by_pos.end()) {
         if (!forced && size > hdr.min_size) ev.push_back({{FIELD_SPLIT, sc}, 2, 0});
-        emit_leaf(hdr, *it->second, sc, pred, ev);
+        emit_leaf(hdr, *it->second.leaf, it->second.levels, sc, pred, ev);
         return true;
     }
     if (!forced) {
@@ -148,7 +152,7 @@ struct RateModels {
     std::map<ContextKey, AdaptiveModel> models;
     bool build(const mars_header& hdr, const std::vector<mars_leaf>& leaves) {
         LeafMap by_pos;
-        for (const auto& l : leaves) by_pos[{l.row, l.col, l.size}] = &l;
+        for (const auto& l : leaves) by_pos[{l.row, l.col, l.size}] = LeafRef{&l, nullptr};
         std::vector<Event> ev;
         Predictor pred;
         if (!walk_write(hdr, 0, 0, virtual_size(hdr), by_pos, pred, ev)) return false;
@@ -168,10 +172,10 @@ struct RateModels {
 
 // event_bits over leaf_events (encode.rs:1513-1518, mars_format.rs:453-458).
 double leaf_bits(const RateModels& rate, const mars_header& hdr, const mars_leaf& leaf,
-                 uint32_t sc) {
+                 uint32_t sc, const int32_t* levels = nullptr) {
     std::vector<Event> ev;
     Predictor pred;
-    emit_leaf(hdr, leaf, sc, pred, ev);
+    emit_leaf(hdr, leaf, levels, sc, pred, ev);
     double s = -0.0;
     for (const auto& e : ev) s += rate.bits_for(e.ctx, e.alphabet, e.symbol);
     return s;
@@ -339,9 +343,64 @@ void affine_fit(const std::vector<double>& block, uint32_t size, uint32_t bits_b
 struct Priced {
     mars_leaf leaf;
     double d, r;
+    std::vector<int32_t> levels;  // mode 3
 };
 
-// best_mode_leaf (encode.rs:1536-1714), modes 0, 1 and 2 with the single-winner list.
+// residual_for_candidate (encode.rs:1783-1851): the mode-2 prediction's error in
+// domain-local (u, v) order, forward DCT, dead-zone quantised and clamped, then priced by
+// the SSE of the pixels the decoder will produce.
+std::vector<int32_t> residual_for_candidate(const Ctx& ctx, const std::vector<double>& block,
+                                            uint32_t size, const mars_candidate& c,
+                                            double* sse_out) {
+    const mars_header& hdr = ctx.hdr;
+    const double alfa = (double)c.qalfa / (double)(1u << ctx.params.bits_alfa) * ctx.params.max_alfa;
+    double beta = (double)c.qbeta / (double)((1u << hdr.bits_beta) - 1) *
+                  ((1.0 + std::fabs(alfa)) * 255.0);
+    if (alfa > 0.0) beta -= alfa * 255.0;
+    const size_t n = (size_t)size * size;
+    std::vector<double> resid(n), prediction(n);
+    for (uint32_t u = 0; u < size; ++u)
+        for (uint32_t v = 0; v < size; ++v) {
+            const uint32_t dr = c.dom_row + 2 * u, dc = c.dom_col + 2 * v;
+            const double d = ((double)pixel_at(ctx.im, dr, dc) + (double)pixel_at(ctx.im, dr + 1, dc) +
+                              (double)pixel_at(ctx.im, dr, dc + 1) +
+                              (double)pixel_at(ctx.im, dr + 1, dc + 1)) /
+                             4.0;
+            uint32_t i, j;
+            iso_map(c.isometry, u, v, size, &i, &j);
+            const double pred = 0.5 + d * alfa + beta;
+            prediction[u * size + v] = pred;
+            resid[u * size + v] = block[i * size + j] - pred;
+        }
+    const std::vector<double> coeffs = residual::forward_dct2d(resid, size);
+    const double step = qstep_of(hdr);
+    std::vector<int32_t> levels(n);
+    std::vector<double> deq(n);
+    for (size_t k = 0; k < n; ++k) {
+        int32_t l = residual::dead_zone_quantize(coeffs[k], step, residual::kDeadZone);
+        if (l < -residual::kLevelClamp) l = -residual::kLevelClamp;
+        if (l > residual::kLevelClamp) l = residual::kLevelClamp;
+        levels[k] = l;
+        deq[k] = residual::dead_zone_dequantize(l, step, residual::kDeadZone);
+    }
+    const std::vector<double> recon = residual::inverse_dct2d(deq, size);
+    double sse = 0.0;
+    for (uint32_t u = 0; u < size; ++u)
+        for (uint32_t v = 0; v < size; ++v) {
+            const size_t k = u * size + v;
+            uint32_t i, j;
+            iso_map(c.isometry, u, v, size, &i, &j);
+            double pv = prediction[k] + recon[k];
+            if (pv < 0.0) pv = 0.0;
+            if (pv > 255.0) pv = 255.0;
+            const double diff = block[i * size + j] - (double)(uint8_t)pv;
+            sse += diff * diff;
+        }
+    *sse_out = sse;
+    return levels;
+}
+
+// best_mode_leaf (encode.rs:1536-1714), modes 0-3 with the single-winner list.
 Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
                       const SearchAnswer& ans, double lambda, uint32_t sc) {
     const mars_header& hdr = ctx.hdr;
@@ -361,7 +420,7 @@ Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
         const double beta2 = (double)l.qbeta / (double)((1u << hdr.bits_beta) - 1) * 255.0;
         double sse = -0.0;
         for (double p : block) sse += (p - beta2) * (p - beta2);
-        cands.push_back({l, sse, leaf_bits(*ctx.rate, hdr, l, sc)});
+        cands.push_back({l, sse, leaf_bits(*ctx.rate, hdr, l, sc), {}});
     };
     if (ctx.allowed[0]) mode0();
     if (ctx.allowed[1]) {
@@ -369,7 +428,7 @@ Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
         l.mode = 1;
         double sse;
         affine_fit(block, size, hdr.bits_beta, &l.qbeta, &l.qgx, &l.qgy, &sse);
-        cands.push_back({l, sse, leaf_bits(*ctx.rate, hdr, l, sc)});
+        cands.push_back({l, sse, leaf_bits(*ctx.rate, hdr, l, sc), {}});
     }
     if (ans.cand.valid && ans.cand.qalfa >= 1 && ctx.allowed[2]) {
         const mars_candidate& c = ans.cand;
@@ -381,7 +440,21 @@ Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
         l.dom_row = c.dom_row;
         l.dom_col = c.dom_col;
         const double sse2 = c.rms * c.rms * (double)size * (double)size;
-        cands.push_back({l, sse2, leaf_bits(*ctx.rate, hdr, l, sc)});
+        cands.push_back({l, sse2, leaf_bits(*ctx.rate, hdr, l, sc), {}});
+    }
+    if (ans.cand.valid && ans.cand.qalfa >= 1 && ctx.allowed[3]) {
+        const mars_candidate& c = ans.cand;
+        mars_leaf l = make_leaf(row, col, size);
+        l.mode = 3;
+        l.qalfa = c.qalfa;
+        l.qbeta = c.qbeta;
+        l.isometry = c.isometry;
+        l.dom_row = c.dom_row;
+        l.dom_col = c.dom_col;
+        double sse3;
+        std::vector<int32_t> levels = residual_for_candidate(ctx, block, size, c, &sse3);
+        const double r3 = leaf_bits(*ctx.rate, hdr, l, sc, levels.data());
+        cands.push_back({l, sse3, r3, std::move(levels)});
     }
     if (cands.empty()) mode0();
     size_t best = 0;
@@ -390,11 +463,12 @@ Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
         const double ji = cands[i].d + lambda * cands[i].r;
         if (ji < jb) best = i;
     }
-    return cands[best];
+    return std::move(cands[best]);
 }
 
 struct RdResult {
     std::vector<mars_leaf> leaves;
+    std::vector<int32_t> resid;  // levels of the mode-3 leaves, in leaf order
     uint64_t evals = 0;
     double d = 0.0, r = 0.0;
 };
@@ -409,6 +483,7 @@ RdResult split_rd(Ctx& ctx, uint32_t row, uint32_t col, uint32_t half, double la
     for (int i = 0; i < 4; ++i) {
         RdResult q = walk_rd(ctx, rs[i], cs[i], half, lambda);
         out.leaves.insert(out.leaves.end(), q.leaves.begin(), q.leaves.end());
+        out.resid.insert(out.resid.end(), q.resid.begin(), q.resid.end());
         out.evals += q.evals;
         out.d += q.d;
         out.r += q.r;
@@ -452,6 +527,7 @@ RdResult walk_rd(Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, double lam
     if (size <= hdr.min_size) {
         RdResult r;
         r.leaves.push_back(leaf.leaf);
+        r.resid = std::move(leaf.levels);
         r.evals = ans.evals;
         r.d = leaf.d;
         r.r = leaf.r;
@@ -466,6 +542,7 @@ RdResult walk_rd(Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, double lam
     if (leaf_j <= split_j) {
         RdResult r;
         r.leaves.push_back(leaf.leaf);
+        r.resid = std::move(leaf.levels);
         r.evals = total;
         r.d = leaf.d;
         r.r = leaf.r + split0;
@@ -550,7 +627,7 @@ bool ifs_write_walk(BitWriter& w, const mars_header& hdr, uint32_t row, uint32_t
         w.write(1, 1);
         return quads();
     }
-    const mars_leaf& l = *it->second;
+    const mars_leaf& l = *it->second.leaf;
     if (size > hdr.min_size) w.write(1, 0);
     w.write(hdr.bits_alfa, l.qalfa);
     w.write(hdr.bits_beta, l.qbeta);
@@ -564,13 +641,52 @@ bool ifs_write_walk(BitWriter& w, const mars_header& hdr, uint32_t row, uint32_t
 
 }  // namespace
 
+double qstep_of(const mars_header& h) {
+    return h.residual_qstep == 0.0f ? 8.0 : (double)h.residual_qstep;
+}
+
+bool qstep_new(double step, float* out) {
+    if (!(std::isfinite(step) && step >= 1.0 && step <= 65535.0)) return false;
+    *out = (float)step;
+    return true;
+}
+
+float qstep_from_lambda(double lambda) {
+    double step = std::sqrt(std::max(lambda, 0.0)) * std::sqrt(6.0 / 0.693147180559945309417232121458176568);
+    if (!(step >= 1.0)) step = 1.0;  // NaN and below-range map to MIN
+    if (step > 65535.0) step = 65535.0;
+    return (float)step;
+}
+
+bool residual_offsets(const mars_leaf* leaves, size_t n, size_t npool, std::vector<int64_t>* offs) {
+    offs->assign(n, -1);
+    size_t at = 0;
+    for (size_t k = 0; k < n; ++k)
+        if (leaves[k].mode == 3) {
+            const size_t need = (size_t)leaves[k].size * leaves[k].size;
+            if (need > npool - at) return false;
+            (*offs)[k] = (int64_t)at;
+            at += need;
+        }
+    return at == npool;
+}
+
 int encode(const Image& im, const mars_params& p, const mars_options& o, const Provider& provider,
-           mars_header* hdr_out, std::vector<mars_leaf>* leaves, mars_counters* counters) {
-    const mars_header hdr = build_header(im.w, im.h, p);
+           const Provider& warmup, mars_header* hdr_out, std::vector<mars_leaf>* leaves,
+           std::vector<int32_t>* residuals, mars_counters* counters) {
+    mars_header hdr = build_header(im.w, im.h, p);
+    // encode.rs:1066-1071: LambdaAdaptive -> from_lambda (8 without lambda); Fixed(step).
+    if (o.residual_adaptive)
+        hdr.residual_qstep = p.has_lambda ? qstep_from_lambda(p.lambda) : 8.0f;
+    else if (o.residual_qstep == 0.0f)
+        hdr.residual_qstep = 8.0f;
+    else if (!qstep_new((double)o.residual_qstep, &hdr.residual_qstep))
+        return MARS_EINVAL;
+    residuals->clear();
     if (p.has_lambda) {
         // build_rate_snapshot (encode.rs:1139-1169): the t_rms = 8 threshold walk with the
         // exhaustive search, here answered by the same provider (it is exhaustive too).
-        Ctx warm{im, hdr, p, &provider, nullptr, {1, 1, 1, 1}, false};
+        Ctx warm{im, hdr, p, &warmup, nullptr, {1, 1, 1, 1}, false};
         warm.params.t_rms = 8.0;
         warm.params.has_lambda = 0;
         WalkResult wr = walk(warm, 0, 0, virtual_size(hdr));
@@ -583,6 +699,7 @@ int encode(const Image& im, const mars_params& p, const mars_options& o, const P
         RdResult rr = walk_rd(ctx, 0, 0, virtual_size(hdr), p.lambda);
         if (ctx.status) return ctx.status;
         *leaves = std::move(rr.leaves);
+        *residuals = std::move(rr.resid);
         counters->search_evals = rr.evals;
         counters->warmup_evals = wr.evals;
     } else {
@@ -599,7 +716,8 @@ int encode(const Image& im, const mars_params& p, const mars_options& o, const P
 
 int ifs_parse(const uint8_t* data, size_t len, mars_header* hdr, std::vector<mars_leaf>* leaves) {
     BitReader r{data, len};
-    mars_header h;
+    mars_header h{};
+    h.residual_qstep = 8.0f;
     if (!r.read(4, &h.bits_alfa) || !r.read(4, &h.bits_beta) || !r.read(7, &h.min_size) ||
         !r.read(7, &h.max_size) || !r.read(6, &h.shift) || !r.read(12, &h.width) ||
         !r.read(12, &h.height) || !r.read(8, &h.int_max_alfa))
@@ -619,7 +737,8 @@ int ifs_write(const mars_header& hdr, const std::vector<mars_leaf>& leaves,
               std::vector<uint8_t>* out) {
     LeafMap by_pos;
     for (const auto& l : leaves)
-        if (!by_pos.emplace(std::make_tuple(l.row, l.col, l.size), &l).second) return MARS_EINVAL;
+        if (!by_pos.emplace(std::make_tuple(l.row, l.col, l.size), LeafRef{&l, nullptr}).second)
+            return MARS_EINVAL;
     BitWriter w;
     w.write(4, hdr.bits_alfa);
     w.write(4, hdr.bits_beta);

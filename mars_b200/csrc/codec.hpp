@@ -41,8 +41,23 @@ double block_rms(const Image& im, uint32_t row, uint32_t col, uint32_t size);
 uint32_t adaptive_shift(uint32_t base, double rms);
 
 // encode_image_with_search (encode.rs:1054-1126): returns MARS_OK or an error status.
+// `residuals` receives the levels of the mode-3 leaves, size*size each, in leaf order.
+// `warmup` answers the exhaustive t_rms = 8 warm-up walk of an RD encode
+// (build_rate_snapshot searches exhaustively whatever the provider is); `provider` answers
+// the final walk.
 int encode(const Image& im, const mars_params& p, const mars_options& o, const Provider& provider,
-           mars_header* hdr, std::vector<mars_leaf>* leaves, mars_counters* counters);
+           const Provider& warmup, mars_header* hdr, std::vector<mars_leaf>* leaves,
+           std::vector<int32_t>* residuals, mars_counters* counters);
+
+// The residual step of a header as f64 (ResidualQstep::get, quant.rs:54-56); 0 in the
+// struct stands for the default step 8.
+double qstep_of(const mars_header& h);
+// ResidualQstep::new / from_lambda (quant.rs:29-52), as binary32; false when out of range.
+bool qstep_new(double step, float* out);
+float qstep_from_lambda(double lambda);
+// Offsets of each mode-3 leaf's levels in a residual pool of `npool` values (-1 for other
+// leaves); false when the pool size does not match the leaves.
+bool residual_offsets(const mars_leaf* leaves, size_t n, size_t npool, std::vector<int64_t>* offs);
 
 // .ifs (ifs.rs:186-279 parse, 525-599 write).
 int ifs_parse(const uint8_t* data, size_t len, mars_header* hdr, std::vector<mars_leaf>* leaves);
@@ -67,7 +82,11 @@ constexpr int32_t AFFINE_GRAD_CLAMP = 2048;
 struct Predictor {
     int64_t row = 0, col = 0;
 };
-using LeafMap = std::map<std::tuple<uint32_t, uint32_t, uint32_t>, const mars_leaf*>;
+struct LeafRef {
+    const mars_leaf* leaf;
+    const int32_t* levels;  // mode 3: size*size residual levels, else null
+};
+using LeafMap = std::map<std::tuple<uint32_t, uint32_t, uint32_t>, LeafRef>;
 
 uint32_t ceil_log2(uint32_t q);
 uint32_t bits_coord_row(const mars_header& h);
@@ -75,8 +94,8 @@ uint32_t bits_coord_col(const mars_header& h);
 uint32_t zigzag(int64_t x);
 int64_t unzigzag(uint32_t z);
 
-void emit_leaf(const mars_header& hdr, const mars_leaf& leaf, uint32_t sc, Predictor& pred,
-               std::vector<Event>& ev);
+void emit_leaf(const mars_header& hdr, const mars_leaf& leaf, const int32_t* levels, uint32_t sc,
+               Predictor& pred, std::vector<Event>& ev);
 bool walk_write(const mars_header& hdr, uint32_t row, uint32_t col, uint32_t size,
                 const LeafMap& by_pos, Predictor& pred, std::vector<Event>& ev);
 

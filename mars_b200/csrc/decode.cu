@@ -1,45 +1,39 @@
-// Fixed-point decode iteration as a gather: each thread produces output pixels.
+// Fixed-point decode iteration as a gather.
 //
 // decode_step / decode_leaf (crates/mars-codec/src/ifs.rs:299-309, 406-484) scatter each
 // leaf's (u, v) domain samples to range positions (i, j) = map(iso, u, v).  Every output
 // pixel belongs to exactly one leaf, so the same map is computed here as a gather: the
-// thread for pixel (y, x) finds its leaf through an owner map kept at the granularity of
-// the smallest leaf (cell = 2^lg x 2^lg pixels: one 4-byte entry per 16 pixels for the
-// usual 4x4 minimum), inverts the isometry to get (u, v), reads the 2x2 domain block of the
-// previous iterate and applies the leaf's affine map with the reference's f64 association,
-// (0.5 + d*alfa) + beta.  Leaves are 16 bytes and carry the quantised coefficients; alfa and
-// beta are dequantised here with the reference's operations in its order, so the doubles
-// are the ones decode_leaf computes.  Pixels no leaf covers are written 0, as the
-// reference's zero-filled `next` buffer is.  When cells are at least 4 pixels wide, a thread
-// produces 4 consecutive pixels of one leaf and stores them as one word.
+// owner map (one leaf index per 2^lg x 2^lg cell, lg the largest power of two dividing
+// every leaf's row, column and size) names the leaf of each pixel, and the inverse
+// isometry names its domain sample.  Values use the reference's f64 association,
+// (0.5 + d*alfa) + beta (+ the mode-3 residual); pixels no leaf covers are written 0, as
+// the reference's zero-filled `next` buffer is.
+//
+// The 16-byte packed leaves are expanded once per leaf list (decode_expand_kernel): alfa
+// and beta are dequantised with the reference's operations in its order, so the doubles
+// are the ones decode_leaf computes.
+//
+// decode_cell_kernel (lg >= 2, width % 4 == 0): one thread per 4x4 output cell.  A cell lies
+// in one leaf, and the inverse isometry maps it onto a 4x4 set of domain samples, i.e. one
+// 8x8 byte window of the previous iterate: the thread reads it as eight 8-byte rows, forms
+// the sixteen 2x2 sums with byte-pair SIMD adds in 16-bit lanes, evaluates the sixteen
+// values in sample order, moves them to output order with byte permutes (row reversal,
+// byte reversal, 4x4 transpose) and stores four 4-byte rows.  decode_pixel_kernel covers
+// any other geometry.
 #include "kernels.cuh"
 
 namespace mars {
 namespace {
 
-// Inverse of isometry::map (isometry.rs:7-19): the (u, v) whose image is (i, j).
-__device__ __forceinline__ void iso_inverse(uint32_t k, int i, int j, int S, int* u, int* v) {
-    switch (k) {
-        case 0: *u = i; *v = j; break;
-        case 1: *u = j; *v = S - 1 - i; break;
-        case 2: *u = S - 1 - j; *v = i; break;
-        case 3: *u = S - 1 - i; *v = S - 1 - j; break;
-        case 4: *u = i; *v = S - 1 - j; break;
-        case 5: *u = S - 1 - i; *v = j; break;
-        case 6: *u = j; *v = i; break;
-        default: *u = S - 1 - j; *v = S - 1 - i; break;
-    }
-}
-
-// A leaf unpacked and dequantised (ifs.rs:416-439).
-struct LeafMap {
+struct Unpacked {
     double alfa, beta, gx, gy;  // mode 1: alfa holds b0
     int row, col, size, mode, iso, dom_row, dom_col;
-    bool domain;                // qalfa != 0: the leaf reads a domain block
+    bool domain;                // qalfa != 0 and mode != 1: the leaf reads a domain block
 };
 
-__device__ __forceinline__ LeafMap unpack(const DecodeLeaf p, const DecodeConsts& c) {
-    LeafMap L;
+// ifs.rs:416-439.
+__device__ __forceinline__ Unpacked unpack(const DecodeLeaf p, const DecodeConsts& c) {
+    Unpacked L;
     L.row = (int)(p.x & 0xFFFFu);
     L.col = (int)(p.x >> 16);
     L.size = (int)(p.y & 0xFFFu);
@@ -68,79 +62,247 @@ __device__ __forceinline__ LeafMap unpack(const DecodeLeaf p, const DecodeConsts
     return L;
 }
 
-__device__ __forceinline__ uint8_t leaf_pixel(const uint8_t* __restrict__ src, int w,
-                                              const LeafMap& L, int y, int x) {
-    const int i = y - L.row, j = x - L.col;
-    double value;
-    if (L.mode == 1) {
-        // Mode 1: round(b0 + gx*u + gy*v) with (u, v) = (i, j) (ifs.rs:416-431);
-        // f64::round and CUDA's round() both round half away from zero.
-        value = round(__dadd_rn(__dadd_rn(L.alfa, __dmul_rn(L.gx, (double)i)),
-                                __dmul_rn(L.gy, (double)j)));
-    } else {
-        double d = 0.0;
-        if (L.domain) {
-            int u, v;
-            iso_inverse(L.iso, i, j, L.size, &u, &v);
-            const size_t dr = L.dom_row + 2 * u, dc = L.dom_col + 2 * v;
-            const double p00 = src[dr * w + dc], p10 = src[(dr + 1) * w + dc];
-            const double p01 = src[dr * w + dc + 1], p11 = src[(dr + 1) * w + dc + 1];
-            d = __dmul_rn(__dadd_rn(__dadd_rn(__dadd_rn(p00, p10), p01), p11), 0.25);
-        }
-        value = __dadd_rn(__dadd_rn(0.5, __dmul_rn(d, L.alfa)), L.beta);
-    }
+__device__ __forceinline__ uint32_t clamp_u8(double value) {
     if (!(value >= 0.0)) value = 0.0;
     if (value > 255.0) value = 255.0;
-    return (uint8_t)value;
+    return (uint32_t)value;
 }
 
-// One pixel per thread (any owner-map granularity).
-__global__ void decode_step_kernel(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst,
-                                   int w, int h, int lg, int mw,
-                                   const int32_t* __restrict__ owner,
-                                   const DecodeLeaf* __restrict__ leaves, DecodeConsts c) {
+// clamp(0, 255) then truncation: truncating first and clamping the integer gives the same
+// byte (a NaN converts to 0 either way).
+__device__ __forceinline__ uint32_t to_u8(double value) {
+    return (uint32_t)min(max(__double2int_rz(value), 0), 255);
+}
+
+// (u, v) = (cu + ai*i + aj*j, cv + bi*i + bj*j): the inverse of isometry::map
+// (isometry.rs:7-19) as an affine map of the range position (i, j), with S1 = size - 1.
+// Three bits describe it: tr (u follows j and v follows i: isometries 1, 2, 6, 7), uneg (u
+// counts down from S1: 2, 3, 5, 7) and vneg (v counts down: 1, 3, 4, 7).
+struct IsoInv {
+    int cu, ai, aj, cv, bi, bj;
+};
+__device__ __forceinline__ IsoInv iso_inverse(int k, int S1) {
+    const bool tr = (0xC6u >> k) & 1u, uneg = (0xACu >> k) & 1u, vneg = (0x9Au >> k) & 1u;
+    const int su = uneg ? -1 : 1, sv = vneg ? -1 : 1;
+    return {uneg ? S1 : 0, tr ? 0 : su, tr ? su : 0, vneg ? S1 : 0, tr ? sv : 0, tr ? 0 : sv};
+}
+
+// A 4x4 byte tile in four row words (byte q of word p = element (p, q)): transposed.
+__device__ __forceinline__ void transpose4x4(uint32_t& r0, uint32_t& r1, uint32_t& r2,
+                                             uint32_t& r3) {
+    // 2x2 blocks of bytes first, then bytes within each block.
+    const uint32_t a0 = __byte_perm(r0, r2, 0x5410), a1 = __byte_perm(r1, r3, 0x5410);
+    const uint32_t a2 = __byte_perm(r0, r2, 0x7632), a3 = __byte_perm(r1, r3, 0x7632);
+    r0 = __byte_perm(a0, a1, 0x6240);
+    r1 = __byte_perm(a0, a1, 0x7351);
+    r2 = __byte_perm(a2, a3, 0x6240);
+    r3 = __byte_perm(a2, a3, 0x7351);
+}
+
+__global__ void decode_expand_kernel(const DecodeLeaf* __restrict__ leaves,
+                                     const int32_t* __restrict__ resid_off, int n,
+                                     DecodeConsts c, DecodeMap* __restrict__ maps) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const Unpacked L = unpack(leaves[k], c);
+    DecodeMap m;
+    // Domain kinds keep alfa / 4: (sum / 4) * alfa == sum * (alfa / 4) exactly, both
+    // scalings by 1/4 being exact.
+    m.a = L.mode == 1 ? L.alfa : __dmul_rn(L.alfa, 0.25);
+    m.b = L.beta;
+    m.gx = L.gx;
+    m.gy = L.gy;
+    m.rc = (uint32_t)L.row | ((uint32_t)L.col << 16);
+    m.dom = (uint32_t)L.dom_row | ((uint32_t)L.dom_col << 16);
+    m.roff = -1;
+    uint32_t kind, cbyte = 0;
+    if (L.mode == 1) {
+        kind = kLeafAffine;
+    } else if (!L.domain) {
+        // d = 0: (0.5 + 0*alfa) + beta, the same for every pixel of the leaf.
+        kind = kLeafConst;
+        cbyte = clamp_u8(__dadd_rn(__dadd_rn(0.5, __dmul_rn(0.0, L.alfa)), L.beta));
+    } else if (L.mode == 3 && resid_off && resid_off[k] >= 0) {
+        kind = kLeafResidual;
+        m.roff = resid_off[k];
+    } else {
+        kind = kLeafDomain;
+    }
+    m.info = (uint32_t)L.size | (kind << 12) | ((uint32_t)L.iso << 14) | (cbyte << 24);
+    maps[k] = m;
+}
+
+__device__ __forceinline__ double domain_value(int sum, const DecodeMap& m) {
+    // The four samples are small integers, so their f64 sum in the reference's order is
+    // the integer sum exactly, and d * alfa = (sum / 4) * alfa = sum * (alfa / 4).
+    return __dadd_rn(__dadd_rn(0.5, __dmul_rn((double)sum, m.a)), m.b);
+}
+
+// Mode 1: round(b0 + gx*u + gy*v) with (u, v) = (i, j) (ifs.rs:416-431); f64::round and
+// CUDA's round() both round half away from zero.
+__device__ __forceinline__ uint32_t affine_pixel(const DecodeMap& m, int i, int j) {
+    return clamp_u8(round(__dadd_rn(__dadd_rn(m.a, __dmul_rn(m.gx, (double)i)),
+                                    __dmul_rn(m.gy, (double)j))));
+}
+
+// One pixel per thread (any owner-map granularity or width).
+__global__ void decode_pixel_kernel(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst,
+                                    int w, int h, int lg, int mw,
+                                    const int32_t* __restrict__ owner,
+                                    const DecodeMap* __restrict__ maps,
+                                    const double* __restrict__ resid) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= w || y >= h) return;
     const int32_t li = owner[(size_t)(y >> lg) * mw + (x >> lg)];
-    uint8_t out = 0;
+    uint32_t out = 0;
     if (li >= 0) {
-        const LeafMap L = unpack(leaves[li], c);
-        out = leaf_pixel(src, w, L, y, x);
+        const DecodeMap m = maps[li];
+        const uint32_t kind = (m.info >> 12) & 3u;
+        const int i = y - (int)(m.rc & 0xFFFFu), j = x - (int)(m.rc >> 16);
+        if (kind == kLeafConst) {
+            out = m.info >> 24;
+        } else if (kind == kLeafAffine) {
+            out = affine_pixel(m, i, j);
+        } else {
+            const int S = (int)(m.info & 0xFFFu);
+            const IsoInv t = iso_inverse((int)((m.info >> 14) & 7u), S - 1);
+            const int u = t.cu + t.ai * i + t.aj * j, v = t.cv + t.bi * i + t.bj * j;
+            const size_t p = ((size_t)(m.dom & 0xFFFFu) + 2 * u) * w + (m.dom >> 16) + 2 * v;
+            const int sum = (int)src[p] + (int)src[p + w] + (int)src[p + 1] + (int)src[p + w + 1];
+            double value = domain_value(sum, m);
+            if (kind == kLeafResidual) value = __dadd_rn(value, resid[m.roff + u * S + v]);
+            out = to_u8(value);
+        }
     }
-    dst[(size_t)y * w + x] = out;
+    dst[(size_t)y * w + x] = (uint8_t)out;
 }
 
-// Four consecutive pixels of one owner cell per thread (granularity >= 4, w % 4 == 0).
-__global__ void decode_step4_kernel(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst,
-                                    int w, int h, int lg, int mw,
-                                    const int32_t* __restrict__ owner,
-                                    const DecodeLeaf* __restrict__ leaves, DecodeConsts c) {
-    const int x = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
-    const int y = blockIdx.y;
-    if (x >= w || y >= h) return;
-    const int32_t li = owner[(size_t)(y >> lg) * mw + (x >> lg)];
-    uint32_t packed = 0;
-    if (li >= 0) {
-        const LeafMap L = unpack(leaves[li], c);
+// Eight bytes of the plane from byte offset `off` (off + 8 <= total), through aligned
+// 8-byte loads where they stay inside the plane.
+__device__ __forceinline__ uint64_t load8(const uint8_t* __restrict__ src, size_t off,
+                                          size_t total) {
+    const size_t a = off & ~(size_t)7;
+    const unsigned s = (unsigned)(off & 7);
+    const uint64_t* p = reinterpret_cast<const uint64_t*>(src + a);
+    if (s == 0) return __ldg(p);
+    if (a + 16 <= total) return (__ldg(p) >> (8 * s)) | (__ldg(p + 1) << (64 - 8 * s));
+    uint64_t v = 0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) packed |= (uint32_t)leaf_pixel(src, w, L, y, x + q) << (8 * q);
+    for (int k = 0; k < 8; ++k) v |= (uint64_t)__ldg(src + off + k) << (8 * k);
+    return v;
+}
+
+// Byte-pair sums of a 4-byte word in two 16-bit lanes: [b0 + b1, b2 + b3].
+__device__ __forceinline__ uint32_t pair_sums(uint32_t x) {
+    return (x & 0x00FF00FFu) + ((x >> 8) & 0x00FF00FFu);
+}
+
+__global__ void __launch_bounds__(128) decode_cell_kernel(
+    const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int w, int h, int lg, int mw,
+    const int32_t* __restrict__ owner, const DecodeMap* __restrict__ maps,
+    const double* __restrict__ resid) {
+    const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int y0 = 4 * blockIdx.y;
+    if (x0 >= w || y0 >= h) return;
+    const int32_t li = owner[(size_t)(y0 >> lg) * mw + (x0 >> lg)];
+    uint64_t lo = 0, hi = 0;  // output rows 0-1 and 2-3, byte 4*a + b = pixel (y0 + a, x0 + b)
+    if (li >= 0) {
+        const DecodeMap m = maps[li];
+        const uint32_t kind = (m.info >> 12) & 3u;
+        const int i0 = y0 - (int)(m.rc & 0xFFFFu), j0 = x0 - (int)(m.rc >> 16);
+        if (kind == kLeafConst) {
+            lo = hi = 0x0101010101010101ull * (uint64_t)(m.info >> 24);
+        } else if (kind == kLeafAffine) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const uint64_t v = affine_pixel(m, i0 + a, j0 + b);
+                    if (a < 2) lo |= v << (8 * (4 * a + b));
+                    else hi |= v << (8 * (4 * (a - 2) + b));
+                }
+        } else {
+            const int S = (int)(m.info & 0xFFFu);
+            const int k = (int)((m.info >> 14) & 7u);
+            const IsoInv t = iso_inverse(k, S - 1);
+            const int u00 = t.cu + t.ai * i0 + t.aj * j0, v00 = t.cv + t.bi * i0 + t.bj * j0;
+            const int umin = u00 - 3 * ((t.ai < 0) | (t.aj < 0));
+            const int vmin = v00 - 3 * ((t.bi < 0) | (t.bj < 0));
+            const size_t total = (size_t)w * h;
+            size_t off = ((size_t)(m.dom & 0xFFFFu) + 2 * umin) * w + (m.dom >> 16) + 2 * vmin;
+            uint32_t sums[4][2];  // 2x2 sums of sample (umin + p, vmin + q), 16-bit lanes
+#pragma unroll
+            for (int r = 0; r < 8; ++r, off += w) {
+                const uint64_t row = load8(src, off, total);
+                const uint32_t s0 = pair_sums((uint32_t)row), s1 = pair_sums((uint32_t)(row >> 32));
+                if (r & 1) {
+                    sums[r >> 1][0] += s0;
+                    sums[r >> 1][1] += s1;
+                } else {
+                    sums[r >> 1][0] = s0;
+                    sums[r >> 1][1] = s1;
+                }
+            }
+            // Values in sample order: byte q of word p is sample (umin + p, vmin + q).
+            uint32_t rw[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int sum = (int)((sums[p][q >> 1] >> (16 * (q & 1))) & 0xFFFFu);
+                    double value = domain_value(sum, m);
+                    if (kind == kLeafResidual)
+                        value = __dadd_rn(value, __ldg(resid + m.roff + (umin + p) * S + vmin + q));
+                    rw[p] |= to_u8(value) << (8 * q);
+                }
+            // Sample (p, q) is output pixel (a, b) with a = p (or 3 - p when u counts down)
+            // and b = q (or 3 - q when v counts down), transposed for isometries 1, 2, 6, 7.
+            const bool tr = (0xC6u >> k) & 1u, uneg = (0xACu >> k) & 1u, vneg = (0x9Au >> k) & 1u;
+            if (vneg) {
+#pragma unroll
+                for (int p = 0; p < 4; ++p) rw[p] = __byte_perm(rw[p], 0, 0x0123);
+            }
+            if (uneg) {
+                const uint32_t t0 = rw[0], t1 = rw[1];
+                rw[0] = rw[3];
+                rw[1] = rw[2];
+                rw[2] = t1;
+                rw[3] = t0;
+            }
+            if (tr) transpose4x4(rw[0], rw[1], rw[2], rw[3]);
+            lo = (uint64_t)rw[0] | ((uint64_t)rw[1] << 32);
+            hi = (uint64_t)rw[2] | ((uint64_t)rw[3] << 32);
+        }
     }
-    *reinterpret_cast<uint32_t*>(dst + (size_t)y * w + x) = packed;
+    uint8_t* out = dst + (size_t)y0 * w + x0;
+    *reinterpret_cast<uint32_t*>(out) = (uint32_t)lo;
+    if (y0 + 1 < h) *reinterpret_cast<uint32_t*>(out + w) = (uint32_t)(lo >> 32);
+    if (y0 + 2 < h) *reinterpret_cast<uint32_t*>(out + 2 * (size_t)w) = (uint32_t)hi;
+    if (y0 + 3 < h) *reinterpret_cast<uint32_t*>(out + 3 * (size_t)w) = (uint32_t)(hi >> 32);
 }
 
 }  // namespace
 
+cudaError_t launch_decode_expand(const DecodeLeaf* leaves, const int32_t* resid_off, int n,
+                                 DecodeConsts c, DecodeMap* maps, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    decode_expand_kernel<<<(n + 255) / 256, 256, 0, st>>>(leaves, resid_off, n, c, maps);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_decode_step(const uint8_t* src, uint8_t* dst, int w, int h, int lg,
-                               const int32_t* owner, const DecodeLeaf* leaves, DecodeConsts c,
+                               const int32_t* owner, const DecodeMap* maps, const double* resid,
                                cudaStream_t st) {
     const int mw = (w + (1 << lg) - 1) >> lg;
-    if (lg >= 2 && (w % 4) == 0) {
-        dim3 grid((w / 4 + 127) / 128, h);
-        decode_step4_kernel<<<grid, 128, 0, st>>>(src, dst, w, h, lg, mw, owner, leaves, c);
+    const bool aligned =
+        ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 7) == 0;
+    if (lg >= 2 && (w % 4) == 0 && aligned) {
+        dim3 grid((w / 4 + 127) / 128, (h + 3) / 4);
+        decode_cell_kernel<<<grid, 128, 0, st>>>(src, dst, w, h, lg, mw, owner, maps, resid);
     } else {
         dim3 grid((w + 255) / 256, h);
-        decode_step_kernel<<<grid, 256, 0, st>>>(src, dst, w, h, lg, mw, owner, leaves, c);
+        decode_pixel_kernel<<<grid, 256, 0, st>>>(src, dst, w, h, lg, mw, owner, maps, resid);
     }
     return cudaGetLastError();
 }

@@ -13,6 +13,7 @@
 #include <string>
 
 #include "codec.hpp"
+#include "residual.hpp"
 
 namespace mars {
 int set_last_error(int code, const std::string& msg);  // api.cu
@@ -49,6 +50,7 @@ struct ReadState {
     ent::Decoder& dec;
     Predictor pred;
     std::vector<mars_leaf>& leaves;
+    std::vector<int32_t>& resid;
     std::string err;
     int code = MARS_OK;
 };
@@ -60,7 +62,7 @@ bool next(ReadState& st, ContextKey ctx, uint32_t alphabet, uint32_t* sym) {
     return false;
 }
 
-// walk_read (mars_format.rs:597-731), modes 0/1/2.
+// walk_read (mars_format.rs:597-731).
 bool walk_read(ReadState& st, uint32_t row, uint32_t col, uint32_t size) {
     const mars_header& hdr = st.hdr;
     if (row >= hdr.height || col >= hdr.width) return true;
@@ -95,11 +97,6 @@ bool walk_read(ReadState& st, uint32_t row, uint32_t col, uint32_t size) {
         st.leaves.push_back(L);
         return true;
     }
-    if (L.mode == 3) {
-        st.code = MARS_EUNSUPPORTED;
-        st.err = "mode 3 (DCT residual) leaves are not supported";
-        return false;
-    }
     uint32_t qa, dz_r, dz_c;
     if (!next(st, {FIELD_QALFA, sc}, (1u << hdr.bits_alfa) - 1, &qa) ||
         !next(st, {FIELD_QBETA, sc}, 1u << hdr.bits_beta, &L.qbeta) ||
@@ -127,12 +124,19 @@ bool walk_read(ReadState& st, uint32_t row, uint32_t col, uint32_t size) {
     L.dom_col = hdr.shift * (uint32_t)cu;
     if (L.dom_row + 2 * size > hdr.height || L.dom_col + 2 * size > hdr.width)
         return out_of_bounds();
+    if (L.mode == 3 &&
+        !mars::residual::decode_values(st.dec, sc, (size_t)size * size, &st.resid)) {
+        st.code = MARS_EFORMAT;
+        st.err = "residual alphabet out of range";
+        return false;
+    }
     st.leaves.push_back(L);
     return true;
 }
 
-int format_write(const mars_header& hdr, float qstep, const mars_leaf* leaves, size_t n,
-                 std::vector<uint8_t>* out) {
+int format_write(const mars_header& hdr, const mars_leaf* leaves, size_t n, const int32_t* resid,
+                 size_t nresid, std::vector<uint8_t>* out) {
+    const float qstep = hdr.residual_qstep == 0.0f ? 8.0f : hdr.residual_qstep;
     if (!header_ok(hdr))
         return fail(MARS_EINVAL,
                     "degenerate header: width, height and shift must be nonzero, bits_alfa "
@@ -142,12 +146,15 @@ int format_write(const mars_header& hdr, float qstep, const mars_leaf* leaves, s
     if (hdr.min_size > 255 || hdr.max_size > 255 || hdr.shift > 255)
         return fail(MARS_EINVAL, "min_size/max_size/shift do not fit in the format's 8-bit fields");
     if (!qstep_ok(qstep)) return fail(MARS_EINVAL, "residual qstep must be finite and in [1, 65535]");
+    std::vector<int64_t> offs;
+    if (!residual_offsets(leaves, n, nresid, &offs) || (nresid && !resid))
+        return fail(MARS_EINVAL, "the residual pool does not hold size*size levels per mode-3 leaf");
     LeafMap by_pos;
     for (size_t k = 0; k < n; ++k) {
         const mars_leaf& l = leaves[k];
-        if (l.mode > 2)
-            return fail(MARS_EUNSUPPORTED, "mode 3 (DCT residual) leaves are not supported");
-        if (!by_pos.emplace(std::make_tuple(l.row, l.col, l.size), &l).second)
+        if (l.mode > 3) return fail(MARS_EINVAL, "leaf mode must be 0..3");
+        const int32_t* lv = offs[k] >= 0 ? resid + offs[k] : nullptr;
+        if (!by_pos.emplace(std::make_tuple(l.row, l.col, l.size), LeafRef{&l, lv}).second)
             return fail(MARS_EINVAL, "two leaves claim the same position (" + std::to_string(l.row) +
                                          "," + std::to_string(l.col) + "," +
                                          std::to_string(l.size) + ")");
@@ -182,8 +189,8 @@ int format_write(const mars_header& hdr, float qstep, const mars_leaf* leaves, s
     return MARS_OK;
 }
 
-int format_read(const uint8_t* d, size_t len, mars_header* hdr, float* qstep,
-                std::vector<mars_leaf>* leaves) {
+int format_read(const uint8_t* d, size_t len, mars_header* hdr, std::vector<mars_leaf>* leaves,
+                std::vector<int32_t>* resid) {
     if (len < kHeaderLen) return fail(MARS_EFORMAT, "header truncated");
     if (std::memcmp(d, "MARS", 4) != 0) return fail(MARS_EFORMAT, "not a .mars file: bad magic");
     if (d[4] != 0) return fail(MARS_EFORMAT, "unsupported .mars version " + std::to_string(d[4]));
@@ -227,10 +234,11 @@ int format_read(const uint8_t* d, size_t len, mars_header* hdr, float* qstep,
     if (!dec.init(tree, tree_len))
         return fail(MARS_EFORMAT, "compressed tree payload ends in an all-zero word");
     leaves->clear();
-    ReadState st{h, dec, Predictor{}, *leaves, std::string(), MARS_OK};
+    resid->clear();
+    ReadState st{h, dec, Predictor{}, *leaves, *resid, std::string(), MARS_OK};
     if (!walk_read(st, 0, 0, virtual_size(h))) return fail(st.code, st.err);
+    h.residual_qstep = q;
     *hdr = h;
-    *qstep = q;
     return MARS_OK;
 }
 
@@ -247,21 +255,28 @@ int copy_out(const std::vector<T>& v, T** out, size_t* n) {
 
 extern "C" {
 
-int mars_format_write(const mars_header* header, float residual_qstep, const mars_leaf* leaves,
-                      size_t n, uint8_t** out, size_t* len) {
+int mars_format_write(const mars_header* header, const mars_leaf* leaves, size_t n,
+                      const int32_t* residuals, size_t nresiduals, uint8_t** out, size_t* len) {
     if (!header || (n && !leaves) || !out || !len) return fail(MARS_EINVAL, "NULL argument");
     std::vector<uint8_t> bytes;
-    if (int e = format_write(*header, residual_qstep, leaves, n, &bytes)) return e;
+    if (int e = format_write(*header, leaves, n, residuals, nresiduals, &bytes)) return e;
     return copy_out(bytes, out, len);
 }
 
-int mars_format_read(const uint8_t* data, size_t len, mars_header* header, float* residual_qstep,
-                     mars_leaf** leaves, size_t* nleaves) {
-    if ((len && !data) || !header || !residual_qstep || !leaves || !nleaves)
+int mars_format_read(const uint8_t* data, size_t len, mars_header* header, mars_leaf** leaves,
+                     size_t* nleaves, int32_t** residuals, size_t* nresiduals) {
+    if ((len && !data) || !header || !leaves || !nleaves || !residuals || !nresiduals)
         return fail(MARS_EINVAL, "NULL argument");
     std::vector<mars_leaf> out;
-    if (int e = format_read(data, len, header, residual_qstep, &out)) return e;
-    return copy_out(out, leaves, nleaves);
+    std::vector<int32_t> res;
+    if (int e = format_read(data, len, header, &out, &res)) return e;
+    if (int e = copy_out(out, leaves, nleaves)) return e;
+    if (int e = copy_out(res, residuals, nresiduals)) {
+        std::free(*leaves);
+        *leaves = nullptr;
+        return e;
+    }
+    return MARS_OK;
 }
 
 int mars_entropy_encode(const mars_event* events, size_t n, uint8_t** out, size_t* len) {

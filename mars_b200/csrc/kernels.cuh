@@ -78,8 +78,8 @@ cudaError_t launch_reduce(const Partial* partials, int ntiles, int nranges, cons
 // One leaf of the decode map in 16 bytes, dequantised on the device:
 //   x: row | col << 16
 //   y: size (bits 0-11) | mode (bits 12-13) | qbeta << 16
-//   z: modes 0/2: dom_row | dom_col << 16;            mode 1: qgx
-//   w: modes 0/2: qalfa (bits 0-16) | isometry << 24;  mode 1: qgy
+//   z: modes 0/2/3: dom_row | dom_col << 16;            mode 1: qgx
+//   w: modes 0/2/3: qalfa (bits 0-16) | isometry << 24;  mode 1: qgy
 struct DecodeLeaf {
     uint32_t x, y, z, w;
 };
@@ -89,9 +89,29 @@ struct DecodeConsts {
     double alfa_den;   // 2^bits_alfa
     double beta_den;   // 2^bits_beta - 1
 };
+// Kinds of expanded leaf.
+enum : uint32_t { kLeafConst = 0, kLeafAffine = 1, kLeafDomain = 2, kLeafResidual = 3 };
+// A leaf expanded for the gather (built once per leaf list by launch_decode_expand):
+//   const:    qalfa == 0 (modes 0/2): every pixel is the byte in info bits 24-31;
+//   affine:   mode 1: round((a + gx*i) + gy*j), (i, j) = (y - row, x - col);
+//   domain:   qalfa != 0 (modes 0/2): (0.5 + sum*a) + b, sum the 2x2 sum at
+//             (dom_row + 2u, dom_col + 2v), (u, v) the inverse isometry of (i, j), a = alfa/4;
+//   residual: mode 3: the domain value + res[roff + u*size + v], res the residual pool.
+struct __align__(16) DecodeMap {
+    double a, b, gx, gy;
+    uint32_t rc;    // row | col << 16
+    uint32_t info;  // size (bits 0-11) | kind (12-13) | isometry (14-16) | const byte (24-31)
+    uint32_t dom;   // dom_row | dom_col << 16
+    int32_t roff;   // residual pool offset (kind residual), else -1
+};
+// resid_off: per leaf, the offset of its size*size residual values in the pool (or -1);
+// may be null when no leaf is mode 3.
+cudaError_t launch_decode_expand(const DecodeLeaf* leaves, const int32_t* resid_off, int n,
+                                 DecodeConsts c, DecodeMap* maps, cudaStream_t st);
 // owner: leaf index (or -1) per cell of 2^lg x 2^lg pixels, row-major, ceil(w/2^lg) wide.
+// resid: the residual pool (f64), or null.
 cudaError_t launch_decode_step(const uint8_t* src, uint8_t* dst, int w, int h, int lg,
-                               const int32_t* owner, const DecodeLeaf* leaves, DecodeConsts c,
+                               const int32_t* owner, const DecodeMap* maps, const double* resid,
                                cudaStream_t st);
 
 }  // namespace mars

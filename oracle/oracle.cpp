@@ -294,9 +294,28 @@ struct Predictor {
     int64_t prev_row_units = 0, prev_col_units = 0;
 };
 
-// emit_leaf (mars_format.rs:515-595), modes 0/1/2.
-void emit_leaf(const orc_header& hdr, const orc_leaf& leaf, uint32_t sc, Predictor& pred,
-               std::vector<Event>& ev) {
+// residual::encode_events (crates/mars-codec/src/residual.rs): FIELD_RESID_NZ = 10,
+// FIELD_RESID_MAG = 11, LEVEL_CLAMP = 63, 4 bands over the coefficient index.
+constexpr uint8_t FIELD_RESID_NZ = 10, FIELD_RESID_MAG = 11;
+constexpr int32_t LEVEL_CLAMP = 63;
+constexpr uint32_t RESID_BANDS = 4;
+uint32_t resid_band(size_t index, size_t n) {
+    return std::min<uint32_t>((uint32_t)((index * RESID_BANDS) / n), RESID_BANDS - 1);
+}
+void residual_events(const int32_t* levels, size_t n, uint32_t sc, std::vector<Event>& ev) {
+    for (size_t i = 0; i < n; ++i) {
+        const uint32_t band = resid_band(i, n);
+        const int32_t c = std::max(-LEVEL_CLAMP, std::min(LEVEL_CLAMP, levels[i]));
+        ev.push_back({{FIELD_RESID_NZ, sc * RESID_BANDS + band}, 2, c != 0 ? 1u : 0u});
+        if (c != 0)
+            ev.push_back({{FIELD_RESID_MAG, sc * RESID_BANDS + band}, (uint32_t)(2 * LEVEL_CLAMP + 1),
+                          (uint32_t)((c << 1) ^ (c >> 31))});
+    }
+}
+
+// emit_leaf (mars_format.rs:515-595); `levels` is the mode-3 residual (else unused).
+void emit_leaf(const orc_header& hdr, const orc_leaf& leaf, const int32_t* levels, uint32_t sc,
+               Predictor& pred, std::vector<Event>& ev) {
     ev.push_back({{FIELD_MODE, sc}, MODE_ALPHABET, leaf.mode});
     if (leaf.mode == 0) {
         ev.push_back({{FIELD_QBETA_DC, sc}, 1u << hdr.bits_beta, leaf.qbeta});
@@ -319,10 +338,12 @@ void emit_leaf(const orc_header& hdr, const orc_leaf& leaf, uint32_t sc, Predict
                       zigzag(col_units - pred.prev_col_units)});
         pred.prev_row_units = row_units;
         pred.prev_col_units = col_units;
+        if (leaf.mode == 3) residual_events(levels, (size_t)leaf.size * leaf.size, sc, ev);
     }
 }
 
-using LeafMap = std::map<std::tuple<uint32_t, uint32_t, uint32_t>, const orc_leaf*>;
+using LeafMap = std::map<std::tuple<uint32_t, uint32_t, uint32_t>,
+                         std::pair<const orc_leaf*, const int32_t*>>;
 
 // walk_write (mars_format.rs:460-512): canonical NW, SW, NE, SE traversal.
 bool walk_write(const orc_header& hdr, uint32_t row, uint32_t col, uint32_t size,
@@ -334,7 +355,7 @@ bool walk_write(const orc_header& hdr, uint32_t row, uint32_t col, uint32_t size
     auto it = by_pos.find({row, col, size});
     if (it != by_pos.end()) {
         if (!forced && size > hdr.min_size) ev.push_back({{FIELD_SPLIT, sc}, 2, 0});
-        emit_leaf(hdr, *it->second, sc, pred, ev);
+        emit_leaf(hdr, *it->second.first, it->second.second, sc, pred, ev);
         return true;
     }
     if (!forced) {
@@ -354,7 +375,7 @@ struct RateModels {
     static bool from_leaves(const orc_header& hdr, const std::vector<orc_leaf>& leaves,
                             RateModels& out) {
         LeafMap by_pos;
-        for (const auto& l : leaves) by_pos[{l.row, l.col, l.size}] = &l;
+        for (const auto& l : leaves) by_pos[{l.row, l.col, l.size}] = {&l, nullptr};
         std::vector<Event> ev;
         Predictor pred;
         if (!walk_write(hdr, 0, 0, virtual_size(hdr), by_pos, pred, ev)) return false;
@@ -374,10 +395,10 @@ struct RateModels {
 
 // event_bits (encode.rs:1513-1518) over leaf_events (mars_format.rs:453-458).
 double leaf_bits(const RateModels& rate, const orc_header& hdr, const orc_leaf& leaf,
-                 uint32_t sc) {
+                 uint32_t sc, const int32_t* levels = nullptr) {
     std::vector<Event> ev;
     Predictor pred;
-    emit_leaf(hdr, leaf, sc, pred, ev);
+    emit_leaf(hdr, leaf, levels, sc, pred, ev);
     double s = -0.0;
     for (const auto& e : ev) s += rate.bits_for(e.ctx, e.alphabet, e.symbol);
     return s;
@@ -560,12 +581,145 @@ void affine_fit(const std::vector<double>& block, uint32_t size, uint32_t bits_b
     *sse_out = sse;
 }
 
+// ------------------------------------------------------------------ mode 3 (residual)
+
+// basis (crates/mars-codec/src/dct.rs:13-20), evaluated at every use as there.
+double dct_basis(size_t n_size, size_t k, size_t n) {
+    const double c_k = k == 0 ? 0.707106781186547524400844362104849039 : 1.0;
+    const double pi = 3.14159265358979323846264338327950288;
+    return std::sqrt(2.0 / (double)n_size) * c_k *
+           std::cos(pi / (double)n_size * ((double)n + 0.5) * (double)k);
+}
+// dct1d / idct1d (dct.rs:22-36): Iterator::sum folds from -0.0 (Rust >= 1.83).
+std::vector<double> dct1d(const std::vector<double>& x) {
+    const size_t n = x.size();
+    std::vector<double> out(n);
+    for (size_t k = 0; k < n; ++k) {
+        double s = -0.0;
+        for (size_t i = 0; i < n; ++i) s += x[i] * dct_basis(n, k, i);
+        out[k] = s;
+    }
+    return out;
+}
+std::vector<double> idct1d(const std::vector<double>& c) {
+    const size_t n = c.size();
+    std::vector<double> out(n);
+    for (size_t i = 0; i < n; ++i) {
+        double s = -0.0;
+        for (size_t k = 0; k < n; ++k) s += c[k] * dct_basis(n, k, i);
+        out[i] = s;
+    }
+    return out;
+}
+// forward_dct2d (dct.rs:38-58): rows then columns.
+std::vector<double> forward_dct2d(const std::vector<double>& block, size_t size) {
+    std::vector<double> tmp(size * size), out(size * size), row(size), col(size);
+    for (size_t r = 0; r < size; ++r) {
+        for (size_t c = 0; c < size; ++c) row[c] = block[r * size + c];
+        const auto t = dct1d(row);
+        for (size_t c = 0; c < size; ++c) tmp[r * size + c] = t[c];
+    }
+    for (size_t c = 0; c < size; ++c) {
+        for (size_t r = 0; r < size; ++r) col[r] = tmp[r * size + c];
+        const auto t = dct1d(col);
+        for (size_t r = 0; r < size; ++r) out[r * size + c] = t[r];
+    }
+    return out;
+}
+// inverse_dct2d (dct.rs:60-80): columns then rows.
+std::vector<double> inverse_dct2d(const std::vector<double>& coeffs, size_t size) {
+    std::vector<double> tmp(size * size), out(size * size), row(size), col(size);
+    for (size_t c = 0; c < size; ++c) {
+        for (size_t r = 0; r < size; ++r) col[r] = coeffs[r * size + c];
+        const auto t = idct1d(col);
+        for (size_t r = 0; r < size; ++r) tmp[r * size + c] = t[r];
+    }
+    for (size_t r = 0; r < size; ++r) {
+        for (size_t c = 0; c < size; ++c) row[c] = tmp[r * size + c];
+        const auto t = idct1d(row);
+        for (size_t c = 0; c < size; ++c) out[r * size + c] = t[c];
+    }
+    return out;
+}
+// dead_zone_quantize / dead_zone_dequantize (crates/mars-codec/src/quant.rs:76-103).
+int32_t dz_quantize(double x, double step, double dz_frac) {
+    const double threshold = dz_frac * step;
+    const double ax = std::fabs(x);
+    if (ax <= threshold) return 0;
+    const double level = std::floor((ax - threshold) / step) + 1.0;
+    const double signed_level = x < 0.0 ? -level : level;
+    if (std::isnan(signed_level)) return 0;  // `as i32` saturates, NaN -> 0
+    if (signed_level >= 2147483647.0) return INT32_MAX;
+    if (signed_level <= -2147483648.0) return INT32_MIN;
+    return (int32_t)signed_level;
+}
+double dz_dequantize(int32_t level, double step, double dz_frac) {
+    if (level == 0) return 0.0;
+    const double threshold = dz_frac * step;
+    const double mag = threshold + ((double)(uint32_t)std::abs((int64_t)level) - 1.0 + 0.5) * step;
+    return level < 0 ? -mag : mag;
+}
+constexpr double RESIDUAL_DEAD_ZONE = 0.5;  // encode.rs:442
+double qstep_get(const orc_header& h) {
+    return h.residual_qstep == 0.0f ? 8.0 : (double)h.residual_qstep;
+}
+
+// residual_for_candidate (encode.rs:1783-1851).
+std::vector<int32_t> residual_for_candidate(const Ctx& ctx, const std::vector<double>& block,
+                                            uint32_t size, const orc_candidate& c, double* sse_out) {
+    const orc_header& hdr = ctx.hdr;
+    const double alfa =
+        (double)c.qalfa / (double)(1u << ctx.params.bits_alfa) * ctx.params.max_alfa;
+    double beta = (double)c.qbeta / (double)((1u << hdr.bits_beta) - 1) *
+                  ((1.0 + std::fabs(alfa)) * 255.0);
+    if (alfa > 0.0) beta -= alfa * 255.0;
+    const size_t n = (size_t)size * size;
+    std::vector<double> resid(n, 0.0), prediction(n, 0.0);
+    for (uint32_t u = 0; u < size; ++u)
+        for (uint32_t v = 0; v < size; ++v) {
+            const uint32_t dr = c.dom_row + 2 * u, dc = c.dom_col + 2 * v;
+            const double d = ((double)pixel_at(ctx.im, dr, dc) + (double)pixel_at(ctx.im, dr + 1, dc) +
+                              (double)pixel_at(ctx.im, dr, dc + 1) +
+                              (double)pixel_at(ctx.im, dr + 1, dc + 1)) /
+                             4.0;
+            uint32_t i, j;
+            iso_map(c.isometry, u, v, size, &i, &j);
+            const double pred = 0.5 + d * alfa + beta;
+            prediction[u * size + v] = pred;
+            resid[u * size + v] = block[i * size + j] - pred;
+        }
+    const auto coeffs = forward_dct2d(resid, size);
+    const double step = qstep_get(hdr);
+    std::vector<int32_t> levels(n);
+    std::vector<double> deq(n);
+    for (size_t k = 0; k < n; ++k) {
+        levels[k] = std::max(-LEVEL_CLAMP,
+                             std::min(LEVEL_CLAMP, dz_quantize(coeffs[k], step, RESIDUAL_DEAD_ZONE)));
+        deq[k] = dz_dequantize(levels[k], step, RESIDUAL_DEAD_ZONE);
+    }
+    const auto recon = inverse_dct2d(deq, size);
+    double sse = 0.0;
+    for (uint32_t u = 0; u < size; ++u)
+        for (uint32_t v = 0; v < size; ++v) {
+            const size_t k = u * size + v;
+            uint32_t i, j;
+            iso_map(c.isometry, u, v, size, &i, &j);
+            const double cl = std::min(255.0, std::max(0.0, prediction[k] + recon[k]));
+            const uint8_t pixel = (uint8_t)cl;
+            const double e = block[i * size + j] - (double)pixel;
+            sse += e * e;
+        }
+    *sse_out = sse;
+    return levels;
+}
+
 struct Priced {
     orc_leaf leaf;
     double d, r;
+    std::vector<int32_t> levels;  // mode 3
 };
 
-// best_mode_leaf (encode.rs:1536-1714), modes 0, 1 and 2.
+// best_mode_leaf (encode.rs:1536-1714), modes 0-3.
 Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
                       const std::vector<orc_candidate>& ranked, double lambda, uint32_t sc) {
     const orc_header& hdr = ctx.hdr;
@@ -587,7 +741,7 @@ Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
         double sse = -0.0;
         for (double p : block) sse += (p - beta2) * (p - beta2);
         const double r = leaf_bits(*ctx.rate, hdr, l, sc);
-        cands.push_back({l, sse, r});
+        cands.push_back({l, sse, r, {}});
     };
     if (ctx.allowed[0]) mode0();
     if (ctx.allowed[1]) {
@@ -596,7 +750,7 @@ Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
         double sse;
         affine_fit(block, size, hdr.bits_beta, &l.qbeta, &l.qgx, &l.qgy, &sse);
         const double r = leaf_bits(*ctx.rate, hdr, l, sc);
-        cands.push_back({l, sse, r});
+        cands.push_back({l, sse, r, {}});
     }
     for (const auto& c : ranked) {
         if (c.qalfa < 1) continue;
@@ -610,7 +764,20 @@ Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
             l.dom_col = c.dom_col;
             const double sse2 = c.rms * c.rms * (double)size * (double)size;
             const double r2 = leaf_bits(*ctx.rate, hdr, l, sc);
-            cands.push_back({l, sse2, r2});
+            cands.push_back({l, sse2, r2, {}});
+        }
+        if (ctx.allowed[3]) {
+            orc_leaf l = make_leaf(row, col, size);
+            l.mode = 3;
+            l.qalfa = c.qalfa;
+            l.qbeta = c.qbeta;
+            l.isometry = c.isometry;
+            l.dom_row = c.dom_row;
+            l.dom_col = c.dom_col;
+            double sse3;
+            std::vector<int32_t> levels = residual_for_candidate(ctx, block, size, c, &sse3);
+            const double r3 = leaf_bits(*ctx.rate, hdr, l, sc, levels.data());
+            cands.push_back({l, sse3, r3, std::move(levels)});
         }
     }
     if (cands.empty()) mode0();
@@ -620,7 +787,7 @@ Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
         const double ji = cands[i].d + lambda * cands[i].r;
         if (ji < jb) best = i;  // min_by keeps the first of equal minima
     }
-    return cands[best];
+    return std::move(cands[best]);
 }
 
 // block_rms (encode.rs:386-403) and adaptive_shift (:431-437).
@@ -649,6 +816,7 @@ uint32_t adaptive_shift(uint32_t base, double rms) {
 
 struct RdResult {
     std::vector<orc_leaf> leaves;
+    std::vector<int32_t> resid;  // mode-3 levels in leaf order
     uint64_t evals = 0;
     double d = 0.0, r = 0.0;
 };
@@ -672,6 +840,7 @@ RdResult split_rd(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t half, dou
     RdResult out;
     for (auto& x : q) {
         out.leaves.insert(out.leaves.end(), x.leaves.begin(), x.leaves.end());
+        out.resid.insert(out.resid.end(), x.resid.begin(), x.resid.end());
         out.evals += x.evals;
         out.d += x.d;
         out.r += x.r;
@@ -713,6 +882,7 @@ RdResult walk_rd(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, doub
     if (size <= hdr.min_size) {
         RdResult r;
         r.leaves.push_back(leaf.leaf);
+        r.resid = std::move(leaf.levels);
         r.evals = block_evals;
         r.d = leaf.d;
         r.r = leaf.r;
@@ -727,6 +897,7 @@ RdResult walk_rd(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, doub
     if (leaf_j <= split_j) {
         RdResult r;
         r.leaves.push_back(leaf.leaf);
+        r.resid = std::move(leaf.levels);
         r.evals = total_evals;
         r.d = leaf.d;
         r.r = leaf.r + split0;
@@ -748,6 +919,7 @@ orc_header build_header(uint32_t w, uint32_t h, const orc_params& p) {
     hdr.width = w;
     hdr.height = h;
     hdr.int_max_alfa = quantise_f64(p.max_alfa / 8.0 * 256.0, 255);
+    hdr.residual_qstep = 8.0f;  // ResidualQstep::LEGACY
     return hdr;
 }
 
@@ -768,9 +940,9 @@ void run_parallel(int nthreads, F&& f) {
 
 double max_alfa_of(const orc_header& h) { return (double)h.int_max_alfa / 256.0 * 8.0; }
 
-// decode_leaf (ifs.rs:406-484), modes 0/1/2.
-void decode_leaf(const orc_header& hdr, const orc_leaf& leaf, const uint8_t* img, size_t stride,
-                 uint8_t* next) {
+// decode_leaf (ifs.rs:406-484); `levels` is a mode-3 leaf's residual (else null).
+void decode_leaf(const orc_header& hdr, const orc_leaf& leaf, const int32_t* levels,
+                 const uint8_t* img, size_t stride, uint8_t* next) {
     const uint32_t size = leaf.size;
     if (leaf.mode == 1) {
         const double b0 = (double)leaf.qbeta / (double)((1u << hdr.bits_beta) - 1) * 255.0;
@@ -789,6 +961,13 @@ void decode_leaf(const orc_header& hdr, const orc_leaf& leaf, const uint8_t* img
     double beta = (double)leaf.qbeta / (double)((1u << hdr.bits_beta) - 1) *
                   ((1.0 + std::fabs(alfa)) * 255.0);
     if (alfa > 0.0) beta -= alfa * 255.0;
+    std::vector<double> residual;
+    if (leaf.mode == 3 && levels && size > 0) {
+        std::vector<double> deq((size_t)size * size);
+        for (size_t k = 0; k < deq.size(); ++k)
+            deq[k] = dz_dequantize(levels[k], qstep_get(hdr), RESIDUAL_DEAD_ZONE);
+        residual = inverse_dct2d(deq, size);
+    }
     for (uint32_t u = 0; u < size; ++u)
         for (uint32_t v = 0; v < size; ++v) {
             double d = 0.0;
@@ -801,6 +980,7 @@ void decode_leaf(const orc_header& hdr, const orc_leaf& leaf, const uint8_t* img
             uint32_t i, j;
             iso_map(leaf.isometry, u, v, size, &i, &j);
             double value = (0.5 + d * alfa) + beta;
+            if (!residual.empty()) value += residual[u * size + v];
             if (value < 0.0) value = 0.0;
             if (value > 255.0) value = 255.0;
             next[(leaf.row + i) * stride + leaf.col + j] = (uint8_t)value;
@@ -896,7 +1076,7 @@ bool ifs_write_walk(BitWriter& w, const orc_header& hdr, uint32_t row, uint32_t 
         w.write(1, 1);
         return quads();
     }
-    const orc_leaf& l = *it->second;
+    const orc_leaf& l = *it->second.first;
     if (size > hdr.min_size) w.write(1, 0);
     w.write(hdr.bits_alfa, l.qalfa);
     w.write(hdr.bits_beta, l.qbeta);
@@ -990,14 +1170,29 @@ int orc_search_grid(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size, ui
 
 int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
                const orc_options* o, orc_header* hdr_out, orc_leaf** leaves, size_t* nleaves,
-               uint64_t* search_evals, uint64_t* warmup_evals, int nthreads) {
+               int32_t** residuals, size_t* nresiduals, uint64_t* search_evals,
+               uint64_t* warmup_evals, int nthreads) {
     if (!px || !p || !o || w == 0 || h == 0 || p->shift == 0) return -1;
     if (p->has_lambda && !(std::isfinite(p->lambda) && p->lambda >= 0.0)) return -1;
-    if (o->allowed_modes[3]) return -3;  // mode 3 (DCT residual) is not restated here
     Image im{px, w, h};
-    const orc_header hdr = build_header(w, h, *p);
+    orc_header hdr = build_header(w, h, *p);
+    // encode.rs:1066-1071 with ResidualQstep::from_lambda (quant.rs:36-52).
+    if (o->residual_adaptive) {
+        if (p->has_lambda) {
+            double step = std::sqrt(std::max(p->lambda, 0.0)) *
+                          std::sqrt(6.0 / 0.693147180559945309417232121458176568);
+            step = std::min(65535.0, std::max(1.0, step));
+            hdr.residual_qstep = (float)step;
+        }
+    } else if (o->residual_qstep != 0.0f) {
+        if (!(std::isfinite(o->residual_qstep) && o->residual_qstep >= 1.0f &&
+              o->residual_qstep <= 65535.0f))
+            return -1;
+        hdr.residual_qstep = o->residual_qstep;
+    }
     Contracted c = Contracted::build(im);
     std::vector<orc_leaf> out;
+    std::vector<int32_t> res;
     uint64_t sev = 0, wev = 0;
     int status = 0;
     run_parallel(nthreads, [&]() {
@@ -1018,6 +1213,7 @@ int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
                     o->adaptive_density != 0};
             RdResult rr = walk_rd(ctx, 0, 0, virtual_size(hdr), p->lambda);
             out = std::move(rr.leaves);
+            res = std::move(rr.resid);
             sev = rr.evals;
         } else {
             Ctx ctx{im, &c, hdr, *p, nullptr, {1, 1, 1, 1}, false};
@@ -1031,6 +1227,9 @@ int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
     *nleaves = out.size();
     *leaves = (orc_leaf*)std::malloc(std::max<size_t>(1, out.size()) * sizeof(orc_leaf));
     std::memcpy(*leaves, out.data(), out.size() * sizeof(orc_leaf));
+    *nresiduals = res.size();
+    *residuals = (int32_t*)std::malloc(std::max<size_t>(1, res.size()) * sizeof(int32_t));
+    if (!res.empty()) std::memcpy(*residuals, res.data(), res.size() * sizeof(int32_t));
     *search_evals = sev;
     *warmup_evals = wev;
     return 0;
@@ -1038,13 +1237,34 @@ int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
 
 void orc_free(void* ptr) { std::free(ptr); }
 
-int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, uint32_t iterations,
-               uint8_t* out) {
+void orc_forward_dct2d(const double* block, uint32_t size, double* out) {
+    const auto r = forward_dct2d(std::vector<double>(block, block + (size_t)size * size), size);
+    std::copy(r.begin(), r.end(), out);
+}
+void orc_inverse_dct2d(const double* coeffs, uint32_t size, double* out) {
+    const auto r = inverse_dct2d(std::vector<double>(coeffs, coeffs + (size_t)size * size), size);
+    std::copy(r.begin(), r.end(), out);
+}
+int32_t orc_dead_zone_quantize(double x, double step, double dz) { return dz_quantize(x, step, dz); }
+double orc_dead_zone_dequantize(int32_t level, double step, double dz) {
+    return dz_dequantize(level, step, dz);
+}
+
+int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, const int32_t* residuals,
+               size_t nresiduals, uint32_t iterations, uint8_t* out) {
     const size_t w = hdr->width, h = hdr->height;
+    std::vector<const int32_t*> lv(n, nullptr);
+    size_t at = 0;
+    for (size_t i = 0; i < n; ++i)
+        if (leaves[i].mode == 3) {
+            lv[i] = residuals + at;
+            at += (size_t)leaves[i].size * leaves[i].size;
+        }
+    if (at != nresiduals) return -1;
     std::vector<uint8_t> img(w * h, 128), next(w * h, 0);
     for (uint32_t it = 0; it < iterations; ++it) {
         std::fill(next.begin(), next.end(), 0);
-        for (size_t i = 0; i < n; ++i) decode_leaf(*hdr, leaves[i], img.data(), w, next.data());
+        for (size_t i = 0; i < n; ++i) decode_leaf(*hdr, leaves[i], lv[i], img.data(), w, next.data());
         img.swap(next);
     }
     std::memcpy(out, img.data(), w * h);
@@ -1054,7 +1274,8 @@ int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, uint32_t
 int orc_ifs_parse(const uint8_t* data, size_t len, orc_header* hdr, orc_leaf** leaves,
                   size_t* nleaves) {
     BitReader r{data, len};
-    orc_header h;
+    orc_header h{};
+    h.residual_qstep = 8.0f;
     if (!r.read(4, &h.bits_alfa) || !r.read(4, &h.bits_beta) || !r.read(7, &h.min_size) ||
         !r.read(7, &h.max_size) || !r.read(6, &h.shift) || !r.read(12, &h.width) ||
         !r.read(12, &h.height) || !r.read(8, &h.int_max_alfa))
@@ -1077,7 +1298,7 @@ int orc_ifs_write(const orc_header* hdr, const orc_leaf* leaves, size_t n, uint8
                   size_t* len) {
     LeafMap by_pos;
     for (size_t i = 0; i < n; ++i) {
-        if (!by_pos.emplace(std::make_tuple(leaves[i].row, leaves[i].col, leaves[i].size), &leaves[i])
+        if (!by_pos.emplace(std::make_tuple(leaves[i].row, leaves[i].col, leaves[i].size), std::make_pair(&leaves[i], (const int32_t*)nullptr))
                  .second)
             return -2;
     }

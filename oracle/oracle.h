@@ -35,6 +35,9 @@ typedef struct orc_params {
 typedef struct orc_options {
     uint8_t allowed_modes[4];
     int32_t adaptive_density;
+    int32_t residual_adaptive; /* ResidualQuantisation::LambdaAdaptive */
+    float residual_qstep;      /* Fixed(step); 0 = ResidualQstep::LEGACY (8) */
+    int32_t method;            /* 0 ExhaustiveSearch, 1 Fisher (IndexedSearchProvider) */
 } orc_options;
 
 /* RawMoments (encode.rs:225-232). */
@@ -58,6 +61,7 @@ typedef struct orc_leaf {
 /* ifs::Header (ifs.rs:13-22). */
 typedef struct orc_header {
     uint32_t bits_alfa, bits_beta, min_size, max_size, shift, width, height, int_max_alfa;
+    float residual_qstep; /* binary32 wire value; 0 = 8 */
 } orc_header;
 
 void orc_contract(const uint8_t* px, uint32_t w, uint32_t h, int32_t* out);
@@ -81,14 +85,22 @@ int orc_search_blocks(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size, 
                       size_t n, orc_candidate* out, uint64_t* evals_per_block, int nthreads);
 
 /* encode_image_with_search(.., ExhaustiveSearch): header, leaves, counters. */
+/* residuals: the size*size levels of every mode-3 leaf, in leaf order (freed with orc_free). */
 int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
                const orc_options* o, orc_header* hdr, orc_leaf** leaves, size_t* nleaves,
-               uint64_t* search_evals, uint64_t* warmup_evals, int nthreads);
+               int32_t** residuals, size_t* nresiduals, uint64_t* search_evals,
+               uint64_t* warmup_evals, int nthreads);
 void orc_free(void* ptr);
 
 /* decode_iterative from the flat-128 seed, modes 0/1/2. */
-int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, uint32_t iterations,
-               uint8_t* out);
+int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, const int32_t* residuals,
+               size_t nresiduals, uint32_t iterations, uint8_t* out);
+
+/* dct.rs forward_dct2d / inverse_dct2d and quant.rs dead-zone quantiser, for tests. */
+void orc_forward_dct2d(const double* block, uint32_t size, double* out);
+void orc_inverse_dct2d(const double* coeffs, uint32_t size, double* out);
+int32_t orc_dead_zone_quantize(double x, double step, double dz);
+double orc_dead_zone_dequantize(int32_t level, double step, double dz);
 
 /* .ifs bitstream (ifs.rs:186-260 parse, 525-599 write). */
 int orc_ifs_parse(const uint8_t* data, size_t len, orc_header* hdr, orc_leaf** leaves,

@@ -25,7 +25,12 @@ class Params(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = [("allowed_modes", C.c_uint8 * 4), ("adaptive_density", C.c_int32)]
+    _fields_ = [("allowed_modes", C.c_uint8 * 4), ("adaptive_density", C.c_int32),
+                ("residual_adaptive", C.c_int32), ("residual_qstep", C.c_float),
+                ("method", C.c_int32)]
+
+
+METHODS = {"exhaustive": 0, "fisher": 1}
 
 
 class Moments(C.Structure):
@@ -49,7 +54,7 @@ class Leaf(C.Structure):
 class Header(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in (
         "bits_alfa", "bits_beta", "min_size", "max_size", "shift", "width", "height",
-        "int_max_alfa")]
+        "int_max_alfa")] + [("residual_qstep", C.c_float)]
 
 
 CANDIDATE_DTYPE = np.dtype([
@@ -91,10 +96,17 @@ def lib():
                                         C.c_uint32, P(Params), C.c_void_p, C.c_void_p, C.c_size_t,
                                         C.c_void_p, C.c_void_p, C.c_int]
         L.orc_encode.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, P(Params), P(Options),
-                                 P(Header), P(C.c_void_p), P(C.c_size_t), P(C.c_uint64),
-                                 P(C.c_uint64), C.c_int]
+                                 P(Header), P(C.c_void_p), P(C.c_size_t), P(C.c_void_p),
+                                 P(C.c_size_t), P(C.c_uint64), P(C.c_uint64), C.c_int]
         L.orc_free.argtypes = [C.c_void_p]
-        L.orc_decode.argtypes = [P(Header), C.c_void_p, C.c_size_t, C.c_uint32, C.c_void_p]
+        L.orc_decode.argtypes = [P(Header), C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                 C.c_uint32, C.c_void_p]
+        L.orc_forward_dct2d.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        L.orc_inverse_dct2d.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        L.orc_dead_zone_quantize.argtypes = [C.c_double, C.c_double, C.c_double]
+        L.orc_dead_zone_quantize.restype = C.c_int32
+        L.orc_dead_zone_dequantize.argtypes = [C.c_int32, C.c_double, C.c_double]
+        L.orc_dead_zone_dequantize.restype = C.c_double
         L.orc_ifs_parse.argtypes = [C.c_void_p, C.c_size_t, P(Header), P(C.c_void_p),
                                     P(C.c_size_t)]
         L.orc_ifs_write.argtypes = [P(Header), C.c_void_p, C.c_size_t, P(C.c_void_p),
@@ -179,28 +191,62 @@ def search_blocks(img, size, shift, params: Params, rows, cols, nthreads=0):
     return out, ev
 
 
-def encode(img, params: Params, allowed_modes=(1, 0, 1, 0), adaptive_density=False, nthreads=0):
-    """encode_image_with_search(.., ExhaustiveSearch): (header, leaves, search_evals, warmup)."""
+def encode(img, params: Params, allowed_modes=(1, 0, 1, 0), adaptive_density=False, nthreads=0,
+           residual_adaptive=False, residual_qstep=0.0, method="exhaustive"):
+    """encode_image_with_search with ExhaustiveSearch (or the Fisher provider):
+    (header, leaves, residuals, search_evals, warmup_evals); `residuals` holds the levels of
+    the mode-3 leaves, size*size each, in leaf order."""
     a = _u8(img)
     h, w = a.shape
-    opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density))
+    opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density), int(residual_adaptive),
+                   float(residual_qstep), METHODS[method])
     hdr = Header()
     ptr, n = C.c_void_p(), C.c_size_t()
+    rptr, rn = C.c_void_p(), C.c_size_t()
     sev, wev = C.c_uint64(), C.c_uint64()
     rc = lib().orc_encode(a.ctypes.data, w, h, C.byref(params), C.byref(opts), C.byref(hdr),
-                          C.byref(ptr), C.byref(n), C.byref(sev), C.byref(wev), nthreads)
+                          C.byref(ptr), C.byref(n), C.byref(rptr), C.byref(rn), C.byref(sev),
+                          C.byref(wev), nthreads)
     if rc:
         raise ValueError(f"orc_encode failed: {rc}")
     leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize), dtype=LEAF_DTYPE).copy()
+    resid = np.frombuffer(C.string_at(rptr, rn.value * 4), dtype=np.int32).copy()
     lib().orc_free(ptr)
-    return hdr, leaves, sev.value, wev.value
+    lib().orc_free(rptr)
+    return hdr, leaves, resid, sev.value, wev.value
 
 
-def decode(hdr: Header, leaves: np.ndarray, iterations: int = 10) -> np.ndarray:
+def decode(hdr: Header, leaves: np.ndarray, iterations: int = 10, residuals=None) -> np.ndarray:
     leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    res = np.ascontiguousarray(residuals if residuals is not None else np.zeros(0), dtype=np.int32)
     out = np.zeros((hdr.height, hdr.width), dtype=np.uint8)
-    lib().orc_decode(C.byref(hdr), leaves.ctypes.data, len(leaves), iterations, out.ctypes.data)
+    rc = lib().orc_decode(C.byref(hdr), leaves.ctypes.data, len(leaves), res.ctypes.data, len(res),
+                          iterations, out.ctypes.data)
+    if rc:
+        raise ValueError(f"orc_decode failed: {rc}")
     return out
+
+
+def forward_dct2d(block: np.ndarray) -> np.ndarray:
+    b = np.ascontiguousarray(block, dtype=np.float64)
+    out = np.empty_like(b)
+    lib().orc_forward_dct2d(b.ctypes.data, b.shape[0], out.ctypes.data)
+    return out
+
+
+def inverse_dct2d(coeffs: np.ndarray) -> np.ndarray:
+    c = np.ascontiguousarray(coeffs, dtype=np.float64)
+    out = np.empty_like(c)
+    lib().orc_inverse_dct2d(c.ctypes.data, c.shape[0], out.ctypes.data)
+    return out
+
+
+def dead_zone_quantize(x: float, step: float, dz: float) -> int:
+    return int(lib().orc_dead_zone_quantize(x, step, dz))
+
+
+def dead_zone_dequantize(level: int, step: float, dz: float) -> float:
+    return float(lib().orc_dead_zone_dequantize(level, step, dz))
 
 
 def ifs_parse(data: bytes):

@@ -115,10 +115,14 @@ def test_decode_rejects_out_of_range_leaves(ctx):
         ctx.decode(hdr, bad, 2)
     assert e.value.code == -1
     bad = leaves.copy()
-    bad["mode"][k] = 3
+    bad["mode"][k] = 3  # a mode-3 leaf without its residual levels
+    with pytest.raises(mb.MarsError, match="residual pool") as e:
+        ctx.decode(hdr, bad, 2)
+    assert e.value.code == -1
+    bad["mode"][k] = 4
     with pytest.raises(mb.MarsError) as e:
         ctx.decode(hdr, bad, 2)
-    assert e.value.code == -8
+    assert e.value.code == -1
     with pytest.raises(mb.MarsError) as e:
         ctx.decode_plan(_hdr(70000, 8), np.zeros(0, dtype=mb.LEAF_DTYPE))
     assert e.value.code == -1

@@ -95,14 +95,15 @@ def test_no_legal_domain_is_none(ctx):
     assert len(o) == 0 and oev == 0
 
 
-def _encode_parity(ctx, img, params_kw, modes=(1, 0, 1, 0), adaptive=False):
-    gh, gl, gc = ctx.encode(img, mb.make_params(**params_kw), allowed_modes=modes,
-                            adaptive_density=adaptive)
-    oh, ol, osev, owev = orc.encode(img, orc.make_params(**params_kw), allowed_modes=modes,
-                                    adaptive_density=adaptive)
+def _encode_parity(ctx, img, params_kw, modes=(1, 0, 1, 0), adaptive=False, **resid):
+    gh, gl, gr, gc = ctx.encode(img, mb.make_params(**params_kw), allowed_modes=modes,
+                                adaptive_density=adaptive, **resid)
+    oh, ol, orr, osev, owev = orc.encode(img, orc.make_params(**params_kw), allowed_modes=modes,
+                                         adaptive_density=adaptive, **resid)
     assert bytes(gh) == bytes(oh)
     assert (gc.search_evals, gc.warmup_evals) == (osev, owev)
     assert gl.tobytes() == ol.tobytes()
+    assert gr.tobytes() == orr.tobytes()
     return gh, gl
 
 
@@ -111,15 +112,25 @@ def test_provider_pattern_encodes(ctx):
     img = provider_pattern_16()
     base = dict(min_size=4, max_size=8, shift=4, t_rms=8.0)
     _encode_parity(ctx, img, base)
-    _encode_parity(ctx, img, dict(base, lam=2.0), modes=(1, 1, 1, 0))
-    _encode_parity(ctx, img, dict(base, lam=2.0), modes=(1, 1, 1, 0), adaptive=True)
-    _encode_parity(ctx, img, dict(base, lam=50.0))
+    _encode_parity(ctx, img, dict(base, lam=2.0), modes=(1, 1, 1, 1))
+    _encode_parity(ctx, img, dict(base, lam=2.0), modes=(1, 1, 1, 1), adaptive=True,
+                   residual_adaptive=True)
+    _encode_parity(ctx, img, dict(base, lam=50.0), residual_qstep=17.123456789)
 
 
 @pytest.mark.parametrize("lam", [None, 50.0, 200.0, 800.0])
 def test_config1_encode_parity(ctx, lam):
     img = synthetic.gray(256, 256, 0)
     _encode_parity(ctx, img, dict(min_size=4, max_size=16, shift=4, lam=lam))
+
+
+@pytest.mark.parametrize("lam", [50.0, 200.0])
+def test_all_modes_encode_parity(ctx, lam):
+    # The reference's default EncodeOptions: all four modes, residual step 8.
+    img = synthetic.gray(128, 128, 5)
+    _encode_parity(ctx, img, dict(min_size=4, max_size=16, shift=4, lam=lam), modes=(1, 1, 1, 1))
+    _encode_parity(ctx, img, dict(min_size=4, max_size=16, shift=2, lam=lam), modes=(1, 1, 1, 1),
+                   adaptive=True, residual_adaptive=True)
 
 
 def test_forced_border_splits_encode_parity(ctx):
@@ -135,7 +146,7 @@ def test_ifs_bytes_identical_through_gpu_encode(ctx):
     img = synthetic.gray(128, 128, 11)
     p = dict(min_size=4, max_size=16, shift=4, t_rms=8.0)
     gh, gl = _encode_parity(ctx, img, p)
-    oh, ol, _, _ = orc.encode(img, orc.make_params(**p))
+    oh, ol, _, _, _ = orc.encode(img, orc.make_params(**p))
     assert mb.ifs_write(gh, gl) == orc.ifs_write(oh, ol)
 
 
@@ -172,12 +183,27 @@ def test_gpu_decode_matches_pinned_hash(ctx, entry):
 
 def test_gpu_decode_modes_0_1_2_match_oracle(ctx):
     img = synthetic.gray(128, 128, 2)
-    hdr, leaves, _ = ctx.encode(img, mb.make_params(min_size=4, max_size=16, shift=4, lam=100.0),
-                                allowed_modes=(1, 1, 1, 0))
+    hdr, leaves, _, _ = ctx.encode(img, mb.make_params(min_size=4, max_size=16, shift=4,
+                                                       lam=100.0), allowed_modes=(1, 1, 1, 0))
     assert set(np.unique(leaves["mode"])) <= {0, 1, 2}
     oh = orc.Header(*[getattr(hdr, f) for f, _ in orc.Header._fields_])
     for iters in (1, 3, 12):
         assert np.array_equal(ctx.decode(hdr, leaves, iters), orc.decode(oh, leaves, iters))
+
+
+@pytest.mark.parametrize("qstep", [0.0, 3.5, 17.123456789])
+def test_gpu_decode_mode_3_matches_oracle(ctx, qstep):
+    # decode_leaf with the DCT residual (ifs.rs:441-456): the residual is rebuilt on the host
+    # and added in the gather.
+    img = synthetic.gray(160, 128, 6)
+    hdr, leaves, res, _ = ctx.encode(img, mb.make_params(min_size=4, max_size=16, shift=2,
+                                                         lam=20.0), allowed_modes=(1, 1, 1, 1),
+                                     residual_qstep=qstep)
+    assert 3 in set(leaves["mode"].tolist()) and len(res) > 0
+    oh = orc.Header(*[getattr(hdr, f) for f, _ in orc.Header._fields_])
+    for iters in (1, 2, 10):
+        assert np.array_equal(ctx.decode(hdr, leaves, iters, res),
+                              orc.decode(oh, leaves, iters, res))
 
 
 def test_invalid_arguments_are_rejected(ctx):
@@ -191,8 +217,8 @@ def test_invalid_arguments_are_rejected(ctx):
     with pytest.raises(mb.MarsError):
         ctx.encode(img, mb.make_params(lam=float("nan")))
     with pytest.raises(mb.MarsError) as e:
-        ctx.encode(img, mb.make_params(lam=10.0), allowed_modes=(1, 1, 1, 1))
-    assert e.value.code == -8
+        ctx.encode(img, mb.make_params(lam=10.0), residual_qstep=0.5)
+    assert e.value.code == -1
     bad = np.zeros(1, dtype=mb.LEAF_DTYPE)
     bad[0] = (0, 0, 8, 2, 3, 10, 0, 60, 0, 0, 0)  # domain runs past a 64x64 plane
     with pytest.raises(mb.MarsError):

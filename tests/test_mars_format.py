@@ -1,11 +1,11 @@
 """The .mars v0 container and its rANS entropy coder (host code, no GPU).
 
 Pinned by the reference's own SHA-256s of encoder output
-(crates/mars-codec/tests/search_provider.rs:180-227) -- the two cases that need no mode 3 --
-and by the unit tests of crates/mars-entropy/src/lib.rs:366-465 and
-crates/mars-codec/src/mars_format.rs:764-905, restated.  Leaves come from the CPU oracle's
-encode, so these run without a GPU; the GPU encode path is pinned to the same bytes in
-test_gpu_mars_format.py.
+(crates/mars-codec/tests/search_provider.rs:180-227: all four streams, two of them with mode-3
+DCT residuals) and by the unit tests of crates/mars-entropy/src/lib.rs:366-465,
+crates/mars-codec/src/mars_format.rs:764-905, dct.rs and quant.rs, restated.  Leaves come
+from the CPU oracle's encode, so these run without a GPU; the GPU encode path is pinned to
+the same bytes in test_gpu_mars_format.py.
 """
 import hashlib
 
@@ -16,25 +16,30 @@ import mars_b200 as mb
 from oracle import oracle as orc
 from tests.golden_data import provider_pattern_16
 
-# (lambda, allowed_modes, residual step, .mars length, search evals, SHA-256), from
-# search_provider.rs:43-66 (cases 1 and 4) and :180-227.
+# search_provider.rs:43-66 (the four cases) and :180-227 (length, evals, SHA-256): threshold;
+# RD lambda 2 with every mode; RD lambda 2 + adaptive density + lambda-adaptive residual step;
+# RD lambda 50, modes {0, 2}, fixed step 17.123456789.
 PINNED = [
-    (None, (1, 0, 1, 0), mb.LEGACY_QSTEP, 53, 608,
+    (None, (1, 1, 1, 1), {}, 53, 608,
      "bb480414035f577917542c7f972cb302f904cecbc79449568d05ad74345e98d8"),
-    (50.0, (1, 0, 1, 0), 17.123456789, 53, 1184,
+    (2.0, (1, 1, 1, 1), {}, 149, 1184,
+     "5069a669a65b6926bc8a597099e0c40c36ac94f038138480226c9b0385b6ae1c"),
+    (2.0, (1, 1, 1, 1), dict(adaptive_density=True, residual_adaptive=True), 161, 864,
+     "afbb23207c8e98b70a1b23639701a8c02d46bd10e7299c58cebe60d52cee76d8"),
+    (50.0, (1, 0, 1, 0), dict(residual_qstep=17.123456789), 53, 1184,
      "44fd4f749006cddd0054b817ba5afd630f356bfa6c18f5b68473e4a300c3885f"),
 ]
+PINNED_IDS = ["threshold", "rd2_all_modes", "rd2_density_adaptive", "rd50_modes02_qstep"]
 
 
 def _mb_header(hdr):
     return mb.Header(*[getattr(hdr, f) for f, _ in mb.Header._fields_])
 
 
-def _encode(img, **kw):
-    modes = kw.pop("modes", (1, 0, 1, 0))
-    p = orc.make_params(**kw)
-    hdr, leaves, sev, _ = orc.encode(img, p, allowed_modes=modes)
-    return _mb_header(hdr), leaves, sev
+def _encode(img, modes=(1, 0, 1, 0), opts=None, **kw):
+    hdr, leaves, res, sev, _ = orc.encode(img, orc.make_params(**kw), allowed_modes=modes,
+                                          **(opts or {}))
+    return _mb_header(hdr), leaves, res, sev
 
 
 def _ramp_image(w, h):
@@ -51,20 +56,18 @@ def _textured_gradient(w, h):
     return np.clip(base + texture, 0, 255).astype(np.uint8)
 
 
-@pytest.mark.parametrize("case", PINNED, ids=["threshold", "rd50_modes02_qstep"])
+@pytest.mark.parametrize("case", PINNED, ids=PINNED_IDS)
 def test_pinned_pre_provider_streams(case):
-    lam, modes, qstep, length, evals, digest = case
-    hdr, leaves, sev = _encode(provider_pattern_16(), min_size=4, max_size=8, shift=4, lam=lam,
-                               modes=modes)
+    lam, modes, opts, length, evals, digest = case
+    hdr, leaves, res, sev = _encode(provider_pattern_16(), modes, opts, min_size=4, max_size=8,
+                                    shift=4, lam=lam)
     assert sev == evals
-    data = mb.format_write(hdr, leaves, qstep)
+    data = mb.format_write(hdr, leaves, res)
     assert len(data) == length
     assert hashlib.sha256(data).hexdigest() == digest
-    h2, q2, l2 = mb.format_read(data)
-    assert [getattr(h2, f) for f, _ in mb.Header._fields_] == \
-        [getattr(hdr, f) for f, _ in mb.Header._fields_]
-    assert q2 == float(np.float32(qstep))
-    assert np.array_equal(l2, leaves)
+    h2, l2, r2 = mb.format_read(data)
+    assert bytes(h2) == bytes(hdr)
+    assert np.array_equal(l2, leaves) and np.array_equal(r2, res)
 
 
 def test_qstep_from_lambda():
@@ -72,26 +75,31 @@ def test_qstep_from_lambda():
     assert mb.qstep_from_lambda(0.0) == 1.0
     assert mb.qstep_from_lambda(1e30) == 65535.0
     assert mb.qstep_from_lambda(200.0) == float(np.float32(np.sqrt(200.0) * np.sqrt(6 / np.log(2))))
+    hdr, _, _, _ = _encode(provider_pattern_16(), (1, 1, 1, 1), dict(residual_adaptive=True),
+                           min_size=4, max_size=8, shift=4, lam=2.0)
+    assert hdr.residual_qstep == mb.qstep_from_lambda(2.0)
 
 
 def test_round_trips_a_real_encode():
-    hdr, leaves, _ = _encode(_ramp_image(64, 48), min_size=4, max_size=16, shift=4)
-    h2, _, l2 = mb.format_read(mb.format_write(hdr, leaves))
+    hdr, leaves, _, _ = _encode(_ramp_image(64, 48), min_size=4, max_size=16, shift=4)
+    h2, l2, _ = mb.format_read(mb.format_write(hdr, leaves))
     assert (h2.width, h2.height, h2.min_size, h2.max_size) == (64, 48, 4, 16)
     assert np.array_equal(np.sort(l2, order=["row", "col", "size"]),
                           np.sort(leaves, order=["row", "col", "size"]))
 
 
 def test_every_mode_the_rd_search_picks_round_trips():
-    hdr, leaves, _ = _encode(_textured_gradient(96, 96), min_size=4, max_size=16, shift=4,
-                             lam=40.0, modes=(1, 1, 1, 0))
+    # mars_format.rs:816-851: a lambda-40 RD encode of the textured gradient uses several
+    # modes, mode 3's residual included, and every field round-trips.
+    hdr, leaves, res, _ = _encode(_textured_gradient(96, 96), (1, 1, 1, 1), min_size=4,
+                                  max_size=16, shift=4, lam=40.0)
     assert len(set(leaves["mode"].tolist())) > 1
-    _, _, l2 = mb.format_read(mb.format_write(hdr, leaves))
-    assert np.array_equal(l2, leaves)
+    h2, l2, r2 = mb.format_read(mb.format_write(hdr, leaves, res))
+    assert np.array_equal(l2, leaves) and np.array_equal(r2, res)
 
 
 def test_compresses_smaller_than_the_raw_ifs_bitstream():
-    hdr, leaves, _ = _encode(_ramp_image(128, 96), min_size=4, max_size=16, shift=4)
+    hdr, leaves, _, _ = _encode(_ramp_image(128, 96), min_size=4, max_size=16, shift=4)
     assert len(mb.format_write(hdr, leaves)) < len(mb.ifs_write(hdr, leaves))
 
 
@@ -107,7 +115,7 @@ def test_rejects_malformed_containers():
     _expect(bytes(bad), "bad magic")
     _expect(b"", "truncated")
     _expect(b"MARS", "truncated")
-    hdr, leaves, _ = _encode(_ramp_image(32, 32), min_size=4, max_size=16, shift=4)
+    hdr, leaves, _, _ = _encode(_ramp_image(32, 32), min_size=4, max_size=16, shift=4)
     data = bytearray(mb.format_write(hdr, leaves))
     data[25:29] = (0xFFFFFFFF).to_bytes(4, "little")
     _expect(bytes(data), "section table claims")
@@ -132,8 +140,9 @@ def test_rejects_malformed_containers():
 def test_corrupted_payloads_never_crash():
     # mars_format::read must reject or decode arbitrary bytes without faulting (the reference
     # fuzzes it, fuzz/fuzz_targets/mars_format_read.rs).
-    hdr, leaves, _ = _encode(_ramp_image(64, 64), min_size=4, max_size=16, shift=4)
-    data = mb.format_write(hdr, leaves)
+    hdr, leaves, res, _ = _encode(_ramp_image(64, 64), (1, 1, 1, 1), min_size=4, max_size=16,
+                                  shift=4, lam=30.0)
+    data = mb.format_write(hdr, leaves, res)
     rng = np.random.default_rng(0)
     outcomes = set()
     for _ in range(300):
@@ -141,7 +150,7 @@ def test_corrupted_payloads_never_crash():
         for _ in range(int(rng.integers(1, 4))):
             b[int(rng.integers(29, len(b)))] = int(rng.integers(0, 256))
         try:
-            _, _, l2 = mb.format_read(bytes(b))
+            _, l2, _ = mb.format_read(bytes(b))
             assert ((l2["row"] + l2["size"] <= 64) & (l2["col"] + l2["size"] <= 64)).all()
             outcomes.add("ok")
         except mb.MarsError as e:
@@ -156,18 +165,41 @@ def test_corrupted_payloads_never_crash():
 
 
 def test_writer_rejects_bad_leaf_sets():
-    hdr, leaves, _ = _encode(_ramp_image(32, 32), min_size=4, max_size=16, shift=4)
+    hdr, leaves, _, _ = _encode(_ramp_image(32, 32), min_size=4, max_size=16, shift=4)
     with pytest.raises(mb.MarsError, match="same position"):
         mb.format_write(hdr, np.concatenate([leaves, leaves[:1]]))
     with pytest.raises(mb.MarsError, match="missing"):
         mb.format_write(hdr, leaves[1:])
+    bad = _mb_header(hdr)
+    bad.residual_qstep = 0.25
     with pytest.raises(mb.MarsError, match="qstep"):
-        mb.format_write(hdr, leaves, 0.25)
+        mb.format_write(bad, leaves)
     m3 = leaves.copy()
-    m3["mode"][0] = 3
-    with pytest.raises(mb.MarsError) as e:
+    k = int(np.flatnonzero(m3["mode"] == 2)[0])
+    m3["mode"][k] = 3  # a mode-3 leaf needs size*size residual levels
+    with pytest.raises(mb.MarsError, match="residual pool"):
         mb.format_write(hdr, m3)
-    assert e.value.code == -8
+    n = int(m3["size"][k]) ** 2
+    levels = np.arange(n) % 7 - 3
+    assert mb.format_read(mb.format_write(hdr, m3, levels))[2].tolist() == levels.tolist()
+
+
+def test_dct_and_dead_zone_restatements():
+    # dct.rs:97-151 and quant.rs:118-152 restated: round trip within 1e-9, DC-only energy
+    # for a constant block, requantising a dequantised level is the identity.
+    rng = np.random.default_rng(1)
+    for size in (2, 4, 8, 16):
+        block = rng.random((size, size)) * 255.0
+        back = orc.inverse_dct2d(orc.forward_dct2d(block))
+        assert np.abs(back - block).max() < 1e-9
+    c = orc.forward_dct2d(np.full((8, 8), 100.0))
+    assert abs(c[0, 0] - 800.0) < 1e-9 and np.abs(c.ravel()[1:]).max() < 1e-9
+    assert orc.dead_zone_quantize(0.0, 4.0, 0.5) == 0
+    for _ in range(2000):
+        step = max(rng.random() * 25.0, 0.05)
+        dz = min(rng.random() / 2.0, 0.49)
+        level = int(rng.integers(-63, 64))
+        assert orc.dead_zone_quantize(orc.dead_zone_dequantize(level, step, dz), step, dz) == level
 
 
 # crates/mars-entropy/src/lib.rs:366-465

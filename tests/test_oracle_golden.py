@@ -75,14 +75,15 @@ def test_provider_pattern_pinned_evals():
     # 1184 RD lambda 50 with modes {0, 2}).  RD evals do not depend on which modes compete.
     img = provider_pattern_16()
     p = dict(min_size=4, max_size=8, shift=4, t_rms=8.0)
-    _, _, sev, wev = orc.encode(img, orc.make_params(**p))
+    _, _, _, sev, wev = orc.encode(img, orc.make_params(**p))
     assert (sev, wev) == (608, 0)
-    _, _, sev, wev = orc.encode(img, orc.make_params(lam=2.0, **p), allowed_modes=(1, 1, 1, 0))
+    _, _, _, sev, wev = orc.encode(img, orc.make_params(lam=2.0, **p), allowed_modes=(1, 1, 1, 1))
     assert (sev, wev) == (1184, 608)
-    _, _, sev, wev = orc.encode(img, orc.make_params(lam=2.0, **p), allowed_modes=(1, 1, 1, 0),
-                                adaptive_density=True)
+    _, _, _, sev, wev = orc.encode(img, orc.make_params(lam=2.0, **p), allowed_modes=(1, 1, 1, 1),
+                                   adaptive_density=True, residual_adaptive=True)
     assert (sev, wev) == (864, 608)
-    _, _, sev, wev = orc.encode(img, orc.make_params(lam=50.0, **p), allowed_modes=(1, 0, 1, 0))
+    _, _, _, sev, wev = orc.encode(img, orc.make_params(lam=50.0, **p), allowed_modes=(1, 0, 1, 0),
+                                   residual_qstep=17.123456789)
     assert (sev, wev) == (1184, 608)
 
 
@@ -90,8 +91,8 @@ def test_provider_pattern_recorded_requests():
     # crates/mars-codec/tests/search_provider.rs:114-177: the final RD walk makes 20 searches
     # (4 size-8 parents + 16 size-4 children); every leaf then tiles the 16x16 plane.
     img = provider_pattern_16()
-    hdr, leaves, sev, _ = orc.encode(img, orc.make_params(min_size=4, max_size=8, shift=4,
-                                                          lam=2.0))
+    hdr, leaves, _, sev, _ = orc.encode(img, orc.make_params(min_size=4, max_size=8, shift=4,
+                                                             lam=2.0))
     assert sev == 4 * 8 + 16 * 72
     cover = np.zeros((16, 16), dtype=np.int32)
     for l in leaves:
@@ -160,7 +161,7 @@ def test_thread_count_identity():
     base = orc.encode(img, p, nthreads=1)
     for nt in (2, 4):
         again = orc.encode(img, p, nthreads=nt)
-        assert again[2] == base[2]
+        assert again[3] == base[3]
         assert again[1].tobytes() == base[1].tobytes()
 
 

@@ -38,7 +38,8 @@ def test_oracle_encode_decodes_identically_in_reference_decoder(seed, lam):
     # Our threshold-walk encode, written as .ifs, decoded by the 1998 C decoder and by the
     # oracle's decode_iterative restatement: identical PGM bytes.
     img = synthetic.gray(128, 96, seed)
-    hdr, leaves, _, _ = orc.encode(img, orc.make_params(min_size=4, max_size=16, shift=4, lam=lam))
+    hdr, leaves, _, _, _ = orc.encode(img, orc.make_params(min_size=4, max_size=16, shift=4,
+                                                           lam=lam))
     data = orc.ifs_write(hdr, leaves)
     ref = decmars(data)
     ours = orc.pgm_bytes(orc.decode(hdr, leaves, 10))
