@@ -67,7 +67,13 @@ typedef struct mars_options {
     int32_t adaptive_density;
     int32_t residual_adaptive;
     float residual_qstep;
+    int32_t method; /* MARS_METHOD_*: the search provider of the final walk */
 } mars_options;
+
+/* Search methods (MethodName, crates/mars-search/src/lib.rs): the exhaustive search
+ * (ExhaustiveSearch, encode.rs:582-602) and Fisher's classified search
+ * (IndexedSearchProvider with Fisher, lib.rs:471-552, fisher.rs). */
+enum { MARS_METHOD_EXHAUSTIVE = 0, MARS_METHOD_FISHER = 1 };
 
 /* RawMoments, encode.rs:225-232. */
 typedef struct mars_moments {
@@ -141,6 +147,15 @@ uint64_t mars_search_table_evals(const mars_table* table);
  * (instrumentation). */
 uint64_t mars_search_table_exact_fits(const mars_table* table);
 void mars_search_table_free(mars_table* table);
+
+/* IndexedSearchProvider::build (crates/mars-search/src/lib.rs:480-513) for `method`: the
+ * per-size domain indexes (plus the doubled-stride ones when adaptive_density and a
+ * lambda are set) and the searches of every node an encode can request, answered through
+ * mars_search_table_lookup.  MARS_METHOD_EXHAUSTIVE builds what mars_search_table_build
+ * builds. */
+int mars_indexed_table_build(mars_ctx* ctx, const uint8_t* plane, uint32_t width,
+                             uint32_t height, const mars_params* params, int32_t adaptive_density,
+                             int32_t method, mars_table** out);
 
 /* search_block over an explicit list of block origins at one size and shift (host
  * buffers).  out[i] / evals[i] belong to (rows[i], cols[i]). */

@@ -46,7 +46,12 @@ class Options(C.Structure):
     """EncodeOptions (encode.rs:78-109): allowed modes, adaptive density, residual
     quantisation (LambdaAdaptive when residual_adaptive, else Fixed(residual_qstep), 0 = 8)."""
     _fields_ = [("allowed_modes", C.c_uint8 * 4), ("adaptive_density", C.c_int32),
-                ("residual_adaptive", C.c_int32), ("residual_qstep", C.c_float)]
+                ("residual_adaptive", C.c_int32), ("residual_qstep", C.c_float),
+                ("method", C.c_int32)]
+
+
+# MethodName (crates/mars-search/src/lib.rs): the search provider of the final walk.
+METHODS = {"exhaustive": 0, "fisher": 1}
 
 
 class Header(C.Structure):
@@ -79,7 +84,7 @@ EXPORTS = (
     "mars_ifs_parse", "mars_ifs_write", "mars_bytes_free", "mars_search_blocks_noalloc",
     "mars_decode_plan_create", "mars_decode_plan_run", "mars_decode_plan_free",
     "mars_format_write", "mars_format_read", "mars_entropy_encode", "mars_entropy_decode",
-    "mars_residuals_free",
+    "mars_residuals_free", "mars_indexed_table_build",
 )
 
 _lib = None
@@ -108,6 +113,8 @@ def lib():
     L.mars_ctx_launch_count.restype = u64
     L.mars_ctx_set_search_path.argtypes = [vp, C.c_int32]
     L.mars_search_table_build.argtypes = [vp, vp, u32, u32, P(Params), C.c_int32, P(vp)]
+    L.mars_indexed_table_build.argtypes = [vp, vp, u32, u32, P(Params), C.c_int32, C.c_int32,
+                                           P(vp)]
     L.mars_search_table_lookup.argtypes = [vp, u32, u32, u32, u32, vp, P(u64)]
     L.mars_search_table_evals.argtypes = [vp]
     L.mars_search_table_evals.restype = u64
@@ -188,6 +195,17 @@ class GpuSearch:
         self._h = C.c_void_p(handle)
         self.width, self.height = width, height
 
+    def search_many(self, rows, cols, size: int, shift: int):
+        """SearchProvider::search for many nodes of one size: (candidates, evals) arrays."""
+        out = np.zeros(len(rows), dtype=CANDIDATE_DTYPE)
+        evals = np.zeros(len(rows), dtype=np.uint64)
+        ev = C.c_uint64()
+        for i, (r, c) in enumerate(zip(rows, cols)):
+            check(lib().mars_search_table_lookup(self._h, int(r), int(c), size, shift,
+                                                 out[i:i + 1].ctypes.data, C.byref(ev)))
+            evals[i] = ev.value
+        return out, evals
+
     def search(self, row: int, col: int, size: int, shift: int) -> SearchOutcome:
         out = np.zeros(1, dtype=CANDIDATE_DTYPE)
         ev = C.c_uint64()
@@ -263,12 +281,20 @@ class Context:
     def launches(self) -> int:
         return lib().mars_ctx_launch_count(self._h)
 
-    def search_provider(self, img, params: Params, adaptive_density: bool = False) -> GpuSearch:
+    def search_provider(self, img, params: Params, adaptive_density: bool = False,
+                        method: str = "exhaustive") -> GpuSearch:
+        """The provider factory: ExhaustiveSearch, or IndexedSearchProvider::build for a
+        classified method ("fisher")."""
         a = _plane(img)
         h, w = a.shape
         t = C.c_void_p()
-        check(lib().mars_search_table_build(self._h, a.ctypes.data, w, h, C.byref(params),
-                                            int(adaptive_density), C.byref(t)))
+        if method == "exhaustive":
+            check(lib().mars_search_table_build(self._h, a.ctypes.data, w, h, C.byref(params),
+                                                int(adaptive_density), C.byref(t)))
+        else:
+            check(lib().mars_indexed_table_build(self._h, a.ctypes.data, w, h, C.byref(params),
+                                                 int(adaptive_density), METHODS[method],
+                                                 C.byref(t)))
         return GpuSearch(self, t.value, w, h)
 
     def search_blocks(self, img, size: int, shift: int, params: Params, rows, cols):
@@ -291,14 +317,14 @@ class Context:
         return self.search_blocks(a, size, shift, params, rr.ravel(), cc.ravel())
 
     def encode(self, img, params: Params, allowed_modes=(1, 0, 1, 0), adaptive_density=False,
-               residual_adaptive=False, residual_qstep=0.0):
+               residual_adaptive=False, residual_qstep=0.0, method="exhaustive"):
         """encode_image_with_search with the GPU provider: (header, leaves, residuals,
         counters); `residuals` holds the levels of the mode-3 leaves, size*size each, in
         leaf order."""
         a = _plane(img)
         h, w = a.shape
         opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density),
-                       int(residual_adaptive), float(residual_qstep))
+                       int(residual_adaptive), float(residual_qstep), METHODS[method])
         hdr, cnt = Header(), Counters()
         ptr, n = C.c_void_p(), C.c_size_t()
         rptr, rn = C.c_void_p(), C.c_size_t()

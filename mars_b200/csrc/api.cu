@@ -396,10 +396,65 @@ int run_jobs(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uin
     return MARS_OK;
 }
 
+// Fisher's classified search for every job: per (size, shift) the domain index
+// (Fisher::index) and the searches of the job's nodes (Fisher::candidates +
+// search_block_fitted); per-node eval counts come back from the device.
+int run_jobs_fisher(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uint32_t h,
+                    const mars::FitParams& fp, const std::vector<Job>& jobs,
+                    mars::CandidateOut* d_out, uint64_t* d_evals) {
+    const cudaStream_t st = ctx->stream;
+    int32_t* d_D = nullptr;
+    const int dw = (int)(w / 2);
+    MARS_CUDA(sc.get(&d_D, std::max<size_t>(1, (size_t)(w / 2) * (h / 2))));
+    MARS_CUDA(mars::launch_contract(d_plane, (int)w, (int)h, d_D, st));
+    ctx->launches += 1;
+    size_t total = 0, max_pos = 0;
+    for (const Job& j : jobs) {
+        total += j.rows.size();
+        const mars::LevelGeom g = level_geom(w, h, j.size, j.shift);
+        if (g.nrow_d > 0 && g.ncol_d > 0) max_pos = std::max(max_pos, (size_t)g.nrow_d * g.ncol_d);
+    }
+    std::vector<uint32_t> rc(2 * total);
+    size_t off = 0;
+    for (const Job& j : jobs) {
+        std::copy(j.rows.begin(), j.rows.end(), rc.begin() + (long)off);
+        std::copy(j.cols.begin(), j.cols.end(), rc.begin() + (long)(total + off));
+        off += j.rows.size();
+    }
+    uint32_t* d_rc = nullptr;
+    MARS_CUDA(sc.get(&d_rc, std::max<size_t>(1, rc.size())));
+    MARS_CUDA(cudaMemcpyAsync(d_rc, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice, st));
+    mars::FisherIndex ix;
+    MARS_CUDA(sc.get(&ix.key, std::max<size_t>(1, max_pos)));
+    MARS_CUDA(sc.get(&ix.diso, std::max<size_t>(1, max_pos)));
+    MARS_CUDA(sc.get(&ix.list, std::max<size_t>(1, max_pos)));
+    MARS_CUDA(sc.get(&ix.counts, 72));
+    MARS_CUDA(sc.get(&ix.offsets, 72));
+    MARS_CUDA(sc.get(&ix.ref, 72));
+    off = 0;
+    for (const Job& j : jobs) {
+        const mars::LevelGeom g = level_geom(w, h, j.size, j.shift);
+        const int nrow = std::max(g.nrow_d, 0), ncol = std::max(g.ncol_d, 0);
+        MARS_CUDA(mars::launch_fisher_index(d_D, dw, (int)j.size, (int)j.shift, nrow, ncol, ix, st));
+        MARS_CUDA(mars::launch_fisher_search(d_plane, (int)w, (int)h, d_D, dw, (int)j.size,
+                                             (int)j.shift, std::max(ncol, 1), d_rc + off,
+                                             d_rc + total + off, (int)j.rows.size(), ix, fp,
+                                             d_out + off, d_evals + off, st));
+        ctx->launches += nrow * ncol > 0 ? 5 : 3;
+        off += j.rows.size();
+    }
+    return MARS_OK;
+}
+
 int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, uint32_t w,
-                uint32_t h, const mars_params* params, bool adaptive, mars_table** out) {
+                uint32_t h, const mars_params* params, bool adaptive, mars_table** out,
+                int method = MARS_METHOD_EXHAUSTIVE) {
     if (!ctx || !out) return fail(MARS_EINVAL, "NULL argument");
     if (int e = check_params(params)) return e;
+    if (method != MARS_METHOD_EXHAUSTIVE && method != MARS_METHOD_FISHER)
+        return fail(MARS_EUNSUPPORTED, "unknown search method " + std::to_string(method));
+    if (method == MARS_METHOD_FISHER && params->max_size > 64)
+        return fail(MARS_EUNSUPPORTED, "the classified search supports block sizes up to 64");
     if (w == 0 || h == 0 || w > 65535 || h > 65535)
         return fail(MARS_EINVAL, "plane dimensions must be in 1..65535");
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -436,7 +491,15 @@ int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, 
         mars::CandidateOut* d_out = nullptr;
         MARS_CUDA(sc.get(&d_out, total));
         MARS_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), ctx->stream));
-        if (int e = run_jobs(ctx, sc, d_plane, w, h, fp, jobs, d_out)) return e;
+        if (method == MARS_METHOD_FISHER) {
+            uint64_t* d_evals = nullptr;
+            MARS_CUDA(sc.get(&d_evals, total));
+            if (int e = run_jobs_fisher(ctx, sc, d_plane, w, h, fp, jobs, d_out, d_evals)) return e;
+            MARS_CUDA(cudaMemcpyAsync(t->evals.data(), d_evals, total * sizeof(uint64_t),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        } else {
+            if (int e = run_jobs(ctx, sc, d_plane, w, h, fp, jobs, d_out)) return e;
+        }
         MARS_CUDA(cudaMemcpyAsync(t->cands.data(), d_out, total * sizeof(mars_candidate),
                                   cudaMemcpyDeviceToHost, ctx->stream));
         unsigned long long exact = 0;
@@ -451,8 +514,8 @@ int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, 
         const uint64_t ev = level_evals(w, h, j.size, j.shift);
         for (size_t i = 0; i < j.rows.size(); ++i) {
             t->index[node_key(j.rows[i], j.cols[i], j.size, j.shift)] = (uint32_t)(off + i);
-            t->evals[off + i] = ev;
-            t->total_evals += ev;
+            if (method == MARS_METHOD_EXHAUSTIVE) t->evals[off + i] = ev;
+            t->total_evals += t->evals[off + i];
         }
         off += j.rows.size();
     }
@@ -545,6 +608,14 @@ int mars_search_table_build(mars_ctx* ctx, const uint8_t* plane, uint32_t width,
                             mars_table** out) {
     if (!plane) return fail(MARS_EINVAL, "plane is NULL");
     return build_table(ctx, plane, nullptr, width, height, params, adaptive_density != 0, out);
+}
+
+int mars_indexed_table_build(mars_ctx* ctx, const uint8_t* plane, uint32_t width,
+                             uint32_t height, const mars_params* params, int32_t adaptive_density,
+                             int32_t method, mars_table** out) {
+    if (!plane) return fail(MARS_EINVAL, "plane is NULL");
+    return build_table(ctx, plane, nullptr, width, height, params, adaptive_density != 0, out,
+                       method);
 }
 
 int mars_search_table_lookup(const mars_table* t, uint32_t row, uint32_t col, uint32_t size,
@@ -659,18 +730,33 @@ int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t he
         !(std::isfinite(options->residual_qstep) && options->residual_qstep >= 1.0f &&
           options->residual_qstep <= 65535.0f))
         return fail(MARS_EINVAL, "residual qstep must be finite and in [1, 65535]");
-    mars_table* table = nullptr;
     const bool adaptive = params->has_lambda && options->adaptive_density;
-    if (int e = build_table(ctx, plane, nullptr, width, height, params, adaptive, &table)) return e;
+    // The final walk's provider (the options' method) and, for an RD encode, the
+    // exhaustive table the warm-up walk reads (the warm-up is exhaustive for every method).
+    mars_table* table = nullptr;
+    mars_table* warm = nullptr;
+    if (int e = build_table(ctx, plane, nullptr, width, height, params, adaptive, &table,
+                            options->method))
+        return e;
     std::unique_ptr<mars_table, void (*)(mars_table*)> guard(table, mars_search_table_free);
-    const mars::codec::Provider provider = [table](uint32_t row, uint32_t col, uint32_t size,
-                                                   uint32_t shift, mars::codec::SearchAnswer* ans) {
-        return mars_search_table_lookup(table, row, col, size, shift, &ans->cand, &ans->evals);
+    if (params->has_lambda && options->method != MARS_METHOD_EXHAUSTIVE) {
+        mars_params wp = *params;
+        wp.has_lambda = 0;
+        if (int e = build_table(ctx, plane, nullptr, width, height, &wp, false, &warm)) return e;
+    }
+    std::unique_ptr<mars_table, void (*)(mars_table*)> wguard(warm, mars_search_table_free);
+    auto lookup = [](mars_table* t) {
+        return [t](uint32_t row, uint32_t col, uint32_t size, uint32_t shift,
+                   mars::codec::SearchAnswer* ans) {
+            return mars_search_table_lookup(t, row, col, size, shift, &ans->cand, &ans->evals);
+        };
     };
+    const mars::codec::Provider provider = lookup(table);
+    const mars::codec::Provider warmup = lookup(warm ? warm : table);
     std::vector<mars_leaf> out;
     std::vector<int32_t> res;
     const mars::codec::Image im{plane, width, height};
-    if (int e = mars::codec::encode(im, *params, *options, provider, provider, header, &out, &res,
+    if (int e = mars::codec::encode(im, *params, *options, provider, warmup, header, &out, &res,
                                     counters))
         return e;
     *nleaves = out.size();

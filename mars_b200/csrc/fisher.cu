@@ -1,0 +1,354 @@
+// Fisher classified search (crates/mars-search/src/{fisher,classify,tables}.rs and the
+// shared fit loop search_block_fitted, lib.rs:211-297), on the device.
+//
+// Indexing (Fisher::index, fisher.rs:30-56): every domain position of a level is classified
+// from its s x s window of the contracted plane D.  newclass (classify.rs:94-101) sorts the
+// four quadrant sums with the reference's 3-pass descending bubble sort, carrying the index
+// permutation, and reads (isometry, class) off the ORDERING row that permutation matches;
+// variance_class (classify.rs:106-118) does the same with the quadrant variances
+// sum2/n - (sum/n)^2 of the block after `flips` by that isometry.  All quadrant sums and
+// sums of squares are exact integers (D <= 1020, pixels <= 255), so the f64 sums the
+// reference accumulates are those integers whatever their order: the sums are taken here in
+// integer arithmetic, the flip becomes a permutation of the four quadrants, and only the
+// variance formula is evaluated in f64, with the reference's operations.  Positions are
+// then grouped into the 3 x 24 buckets in raster order (stable), and an empty bucket reads
+// the first non-empty one in (class, variance class) order.
+//
+// Search (Fisher::candidates + search_block_fitted): one warp per range block.  The range
+// is classified the same way (on its pixels), its bucket's candidates are fitted lane by
+// lane with the exact integer moments and fit_f64, each under the isometry
+// MAPPING[range isometry][domain isometry], and the winner is the first minimum rms in
+// bucket order (strict `<`); evals = the bucket's length, duplicates included.
+#include <cuda_runtime.h>
+
+#include "fit.cuh"
+#include "kernels.cuh"
+
+namespace mars {
+namespace {
+
+// ORDERING (tables.rs:13-38): the 24 descending-order permutations of the quadrants, each
+// with the isometry and class newclass assigns to it.  The table is data shared with the
+// reference so that class numbers and bucket order agree.
+__constant__ int8_t kOrdering[24][6] = {
+    {3, 2, 1, 0, 3, 0}, {2, 3, 1, 0, 5, 1}, {2, 1, 3, 0, 5, 2}, {3, 1, 2, 0, 7, 0},
+    {1, 3, 2, 0, 1, 1}, {1, 2, 3, 0, 1, 2}, {3, 2, 0, 1, 3, 1}, {2, 3, 0, 1, 5, 0},
+    {2, 1, 0, 3, 2, 2}, {3, 1, 0, 2, 7, 1}, {1, 3, 0, 2, 1, 0}, {1, 2, 0, 3, 4, 2},
+    {3, 0, 2, 1, 3, 2}, {2, 0, 3, 1, 2, 0}, {2, 0, 1, 3, 2, 1}, {3, 0, 1, 2, 7, 2},
+    {1, 0, 2, 3, 4, 1}, {1, 0, 3, 2, 4, 0}, {0, 3, 2, 1, 6, 2}, {0, 2, 3, 1, 6, 1},
+    {0, 2, 1, 3, 6, 0}, {0, 3, 1, 2, 0, 2}, {0, 1, 3, 2, 0, 1}, {0, 1, 2, 3, 0, 0},
+};
+// MAPPING (tables.rs:42-51): isometry composition, [range isometry][domain isometry].
+__constant__ uint8_t kMapping[8][8] = {
+    {0, 1, 2, 3, 4, 5, 6, 7}, {2, 0, 3, 1, 7, 6, 4, 5}, {1, 3, 0, 2, 6, 7, 5, 4},
+    {3, 2, 1, 0, 5, 4, 7, 6}, {4, 7, 6, 5, 0, 3, 2, 1}, {5, 6, 7, 4, 3, 0, 1, 2},
+    {6, 4, 5, 7, 1, 2, 0, 3}, {7, 5, 4, 6, 2, 1, 3, 0},
+};
+
+// flips(b, iso) reads out[i][j] = b[src(i, j)] (classify.rs:139-164); quadrant q of the
+// flipped block (TL, TR, BL, BR) is quadrant kFlipQuad[iso][q] of the original.
+__constant__ uint8_t kFlipQuad[8][4] = {
+    {0, 1, 2, 3},  // identity
+    {1, 3, 0, 2},  // src (j, s-1-i)
+    {2, 0, 3, 1},  // src (s-1-j, i)
+    {3, 2, 1, 0},  // src (s-1-i, s-1-j)
+    {1, 0, 3, 2},  // src (i, s-1-j)
+    {2, 3, 0, 1},  // src (s-1-i, j)
+    {0, 2, 1, 3},  // src (j, i)
+    {3, 1, 2, 0},  // src (s-1-j, s-1-i)
+};
+
+// The 3-pass descending bubble sort of index_func.c (classify.rs:62-73) and match().
+template <class T>
+__device__ __forceinline__ int sorted_row(T a0, T a1, T a2, T a3) {
+    T a[4] = {a0, a1, a2, a3};
+    int o[4] = {0, 1, 2, 3};
+#pragma unroll
+    for (int i = 2; i >= 0; --i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j)
+            if (a[j] < a[j + 1]) {
+                const T t = a[j];
+                a[j] = a[j + 1];
+                a[j + 1] = t;
+                const int u = o[j];
+                o[j] = o[j + 1];
+                o[j + 1] = u;
+            }
+    for (int r = 0; r < 24; ++r)
+        if (kOrdering[r][0] == o[0] && kOrdering[r][1] == o[1] && kOrdering[r][2] == o[2] &&
+            kOrdering[r][3] == o[3])
+            return r;
+    return 23;  // unreachable: o is a permutation of 0..3
+}
+
+// variance_2 (classify.rs:77-89) from exact quadrant sums: sum2/n - (sum/n)^2.
+__device__ __forceinline__ double quad_variance(int64_t sum, int64_t sum2, double n) {
+    const double m = __ddiv_rn((double)sum, n);
+    return __dsub_rn(__ddiv_rn((double)sum2, n), __dmul_rn(m, m));
+}
+
+// (isometry, class * 24 + variance class) from the four quadrant sums and sums of squares.
+__device__ __forceinline__ void classify(const int64_t q[4], const int64_t q2[4], int h,
+                                         int* iso, int* bucket) {
+    const int r = sorted_row<int64_t>(q[0], q[1], q[2], q[3]);
+    const int is = kOrdering[r][4], clas = kOrdering[r][5];
+    const double n = (double)(h * h);
+    double v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int src = kFlipQuad[is][k];
+        v[k] = quad_variance(q[src], q2[src], n);
+    }
+    const int var_class = sorted_row<double>(v[0], v[1], v[2], v[3]);
+    *iso = is;
+    *bucket = clas * 24 + var_class;
+}
+
+__global__ void fisher_classify_domains_kernel(const int32_t* __restrict__ D, int dw, int size,
+                                               int shift, int nrow_d, int ncol_d,
+                                               uint8_t* __restrict__ key,
+                                               uint8_t* __restrict__ diso) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nrow_d * ncol_d) return;
+    const int r0 = (p / ncol_d) * shift / 2, c0 = (p % ncol_d) * shift / 2;
+    const int h = size / 2;
+    int64_t q[4] = {0, 0, 0, 0}, q2[4] = {0, 0, 0, 0};
+    for (int u = 0; u < size; ++u) {
+        const int32_t* row = D + (size_t)(r0 + u) * dw + c0;
+        for (int v = 0; v < size; ++v) {
+            const int64_t d = row[v];
+            const int k = (u >= h ? 2 : 0) + (v >= h ? 1 : 0);
+            q[k] += d;
+            q2[k] += d * d;
+        }
+    }
+    int iso, bucket;
+    classify(q, q2, h, &iso, &bucket);
+    key[p] = (uint8_t)bucket;
+    diso[p] = (uint8_t)iso;
+}
+
+// Bucket sizes: block b counts the positions of bucket b.
+__global__ void fisher_count_kernel(const uint8_t* __restrict__ key, int n,
+                                    uint32_t* __restrict__ counts) {
+    __shared__ uint32_t total;
+    if (threadIdx.x == 0) total = 0;
+    __syncthreads();
+    uint32_t c = 0;
+    for (int p = threadIdx.x; p < n; p += blockDim.x) c += key[p] == blockIdx.x;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&total, c);
+    __syncthreads();
+    if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+// Offsets, and the bucket each class reads (itself, or the first non-empty one).
+__global__ void fisher_offsets_kernel(const uint32_t* __restrict__ counts,
+                                      uint32_t* __restrict__ offsets,
+                                      uint32_t* __restrict__ ref) {
+    if (threadIdx.x != 0) return;
+    uint32_t off = 0;
+    int first = -1;
+    for (int b = 0; b < 72; ++b) {
+        offsets[b] = off;
+        off += counts[b];
+        if (first < 0 && counts[b] > 0) first = b;
+    }
+    for (int b = 0; b < 72; ++b) ref[b] = counts[b] > 0 ? b : (first < 0 ? b : first);
+}
+
+// Stable compaction: block b writes the positions of bucket b in raster order.
+__global__ void fisher_fill_kernel(const uint8_t* __restrict__ key, int n,
+                                   const uint32_t* __restrict__ offsets,
+                                   uint32_t* __restrict__ list) {
+    __shared__ uint32_t warp_sum[32];
+    __shared__ uint32_t base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) base = offsets[blockIdx.x];
+    __syncthreads();
+    for (int start = 0; start < n; start += blockDim.x) {
+        const int p = start + threadIdx.x;
+        const bool hit = p < n && key[p] == blockIdx.x;
+        const uint32_t ballot = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) warp_sum[warp] = __popc(ballot);
+        __syncthreads();
+        uint32_t before = 0, all = 0;
+        for (int k = 0; k < nw; ++k) {
+            before += k < warp ? warp_sum[k] : 0;
+            all += warp_sum[k];
+        }
+        if (hit) list[base + before + __popc(ballot & ((1u << lane) - 1))] = (uint32_t)p;
+        __syncthreads();
+        if (threadIdx.x == 0) base += all;
+        __syncthreads();
+    }
+}
+
+// One warp per range block.  Shared memory per warp: the 8 permuted copies of the range
+// (permute_range, encode.rs:833-842: range_k[u*s + v] = range[map(k, u, v)]).
+constexpr int kFisherWarps = 4;
+
+__global__ void __launch_bounds__(32 * kFisherWarps) fisher_search_kernel(
+    const uint8_t* __restrict__ plane, int w, int h, const int32_t* __restrict__ D, int dw,
+    int size, int shift, int ncol_d, const uint32_t* __restrict__ rows,
+    const uint32_t* __restrict__ cols, int nranges, const uint32_t* __restrict__ counts,
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ ref,
+    const uint32_t* __restrict__ list, const uint8_t* __restrict__ diso, FitParams fp,
+    CandidateOut* __restrict__ out, uint64_t* __restrict__ evals_out) {
+    extern __shared__ uint8_t smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ri = blockIdx.x * kFisherWarps + warp;
+    if (ri >= nranges) return;
+    const int n = size * size, hq = size / 2;
+    uint8_t* perm = smem + (size_t)warp * 8 * n;
+    const uint32_t row = rows[ri], col = cols[ri];
+    CandidateOut res;
+    res.dom_row = res.dom_col = res.isometry = res.qalfa = res.qbeta = res.valid = 0;
+    res.rms = 0.0;
+    res.s0 = res.s1_x4 = res.s2_x16 = res.t0 = res.t1_x4 = res.t2 = 0;
+    if (row + size > (uint32_t)h || col + size > (uint32_t)w) {
+        // Blocks outside the plane are reported as no candidate and no evals.
+        if (lane == 0) {
+            out[ri] = res;
+            evals_out[ri] = 0;
+        }
+        return;
+    }
+    // Range pixels -> quadrant sums and sums of squares, then the 8 permuted copies.
+    int64_t q[4] = {0, 0, 0, 0}, q2[4] = {0, 0, 0, 0}, t0 = 0, t2 = 0;
+    for (int k = lane; k < n; k += 32) {
+        const int i = k / size, j = k % size;
+        const int64_t p = plane[(size_t)(row + i) * w + col + j];
+        const int qk = (i >= hq ? 2 : 0) + (j >= hq ? 1 : 0);
+        q[qk] += p;
+        q2[qk] += p * p;
+        t0 += p;
+        t2 += p * p;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            q[k] += __shfl_xor_sync(0xffffffffu, q[k], o);
+            q2[k] += __shfl_xor_sync(0xffffffffu, q2[k], o);
+        }
+        t0 += __shfl_xor_sync(0xffffffffu, t0, o);
+        t2 += __shfl_xor_sync(0xffffffffu, t2, o);
+    }
+    for (int e = lane; e < 8 * n; e += 32) {
+        const int k = e / n, uv = e % n, u = uv / size, v = uv % size;
+        int i, j;
+        switch (k) {  // isometry::map (isometry.rs:7-19)
+            case 0: i = u; j = v; break;
+            case 1: i = size - 1 - v; j = u; break;
+            case 2: i = v; j = size - 1 - u; break;
+            case 3: i = size - 1 - u; j = size - 1 - v; break;
+            case 4: i = u; j = size - 1 - v; break;
+            case 5: i = size - 1 - u; j = v; break;
+            case 6: i = v; j = u; break;
+            default: i = size - 1 - v; j = size - 1 - u; break;
+        }
+        perm[e] = plane[(size_t)(row + i) * w + col + j];
+    }
+    __syncwarp();
+    int isom, key;
+    classify(q, q2, hq, &isom, &key);
+    const uint32_t b = ref[key];
+    const uint32_t len = counts[b], off = offsets[b];
+
+    double best_rms = 0.0;
+    uint32_t best_e = 0xffffffffu;
+    FitResult best_fit{};
+    int64_t best_s1 = 0, best_s2 = 0, best_t1 = 0;
+    for (uint32_t e = lane; e < len; e += 32) {
+        const uint32_t p = list[off + e];
+        const int iso = kMapping[isom][diso[p]];
+        const int dr = (int)((p / ncol_d) * shift / 2), dc = (int)((p % ncol_d) * shift / 2);
+        const uint8_t* rp = perm + iso * n;
+        int64_t s1 = 0, s2 = 0, t1 = 0;
+        for (int u = 0; u < size; ++u) {
+            const int32_t* drow = D + (size_t)(dr + u) * dw + dc;
+            for (int v = 0; v < size; ++v) {
+                const int64_t d = drow[v];
+                s1 += d;
+                s2 += d * d;
+                t1 += d * rp[u * size + v];
+            }
+        }
+        const FitResult f = fit_exact(n, s1, s2, t0, t1, t2, fp);
+        if (best_e == 0xffffffffu || f.rms < best_rms) {
+            best_rms = f.rms;
+            best_e = e;
+            best_fit = f;
+            best_s1 = s1;
+            best_s2 = s2;
+            best_t1 = t1;
+        }
+    }
+    // First minimum in bucket order: lexicographic (rms, index) over the lanes.
+    double r = best_e == 0xffffffffu ? __longlong_as_double(0x7ff0000000000000ll) : best_rms;
+    uint32_t ie = best_e;
+    for (int o = 16; o > 0; o >>= 1) {
+        const double r2 = __shfl_xor_sync(0xffffffffu, r, o);
+        const uint32_t e2 = __shfl_xor_sync(0xffffffffu, ie, o);
+        if (r2 < r || (r2 == r && e2 < ie)) {
+            r = r2;
+            ie = e2;
+        }
+    }
+    if (ie != 0xffffffffu && ie == best_e) {
+        const uint32_t p = list[off + ie];
+        res.dom_row = (p / ncol_d) * shift;
+        res.dom_col = (p % ncol_d) * shift;
+        res.isometry = kMapping[isom][diso[p]];
+        res.qalfa = best_fit.qalfa;
+        res.qbeta = best_fit.qbeta;
+        res.valid = 1;
+        res.rms = best_fit.rms;
+        res.s0 = n;
+        res.s1_x4 = best_s1;
+        res.s2_x16 = best_s2;
+        res.t0 = t0;
+        res.t1_x4 = best_t1;
+        res.t2 = t2;
+        out[ri] = res;
+        evals_out[ri] = len;
+    } else if (ie == 0xffffffffu && lane == 0) {
+        out[ri] = res;
+        evals_out[ri] = 0;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_fisher_index(const int32_t* D, int dw, int size, int shift, int nrow_d,
+                                int ncol_d, FisherIndex ix, cudaStream_t st) {
+    const int npos = nrow_d * ncol_d;
+    if (npos > 0)
+        fisher_classify_domains_kernel<<<(npos + 255) / 256, 256, 0, st>>>(
+            D, dw, size, shift, nrow_d, ncol_d, ix.key, ix.diso);
+    fisher_count_kernel<<<72, 256, 0, st>>>(ix.key, npos, ix.counts);
+    fisher_offsets_kernel<<<1, 32, 0, st>>>(ix.counts, ix.offsets, ix.ref);
+    if (npos > 0) fisher_fill_kernel<<<72, 1024, 0, st>>>(ix.key, npos, ix.offsets, ix.list);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fisher_search(const uint8_t* plane, int w, int h, const int32_t* D, int dw,
+                                 int size, int shift, int ncol_d, const uint32_t* rows,
+                                 const uint32_t* cols, int nranges, FisherIndex ix,
+                                 const FitParams& fp, CandidateOut* out, uint64_t* evals,
+                                 cudaStream_t st) {
+    if (nranges <= 0) return cudaSuccess;
+    const size_t smem = (size_t)kFisherWarps * 8 * size * size;
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(
+            fisher_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    fisher_search_kernel<<<(nranges + kFisherWarps - 1) / kFisherWarps, 32 * kFisherWarps, smem,
+                           st>>>(plane, w, h, D, dw, size, shift, ncol_d, rows, cols, nranges,
+                                 ix.counts, ix.offsets, ix.ref, ix.list, ix.diso, fp, out, evals);
+    return cudaGetLastError();
+}
+
+}  // namespace mars

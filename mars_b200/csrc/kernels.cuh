@@ -74,6 +74,28 @@ int search_simt_splits(const LevelGeom& g, int nranges, int num_sms);
 cudaError_t launch_reduce(const Partial* partials, int ntiles, int nranges, const LevelGeom& g,
                           RangeStats rs, DomainStats ds, CandidateOut* out, cudaStream_t st);
 
+// ---- Fisher classified search (fisher.cu) ----
+// The index of one (size, shift) level: per domain position (raster order) its bucket
+// (class * 24 + variance class) and canonicalising isometry; per bucket its length, offset
+// into `list` (positions grouped by bucket, raster order within a bucket) and the bucket a
+// class reads (itself, or the first non-empty bucket when it is empty).
+struct FisherIndex {
+    uint8_t* key;       // [npos]
+    uint8_t* diso;      // [npos]
+    uint32_t* counts;   // [72]
+    uint32_t* offsets;  // [72]
+    uint32_t* ref;      // [72]
+    uint32_t* list;     // [npos]
+};
+cudaError_t launch_fisher_index(const int32_t* D, int dw, int size, int shift, int nrow_d,
+                                int ncol_d, FisherIndex ix, cudaStream_t st);
+// One warp per range block; writes the winner (valid = 0 for none) and the eval count.
+cudaError_t launch_fisher_search(const uint8_t* plane, int w, int h, const int32_t* D, int dw,
+                                 int size, int shift, int ncol_d, const uint32_t* rows,
+                                 const uint32_t* cols, int nranges, FisherIndex ix,
+                                 const FitParams& fp, CandidateOut* out, uint64_t* evals,
+                                 cudaStream_t st);
+
 // ---- decode (decode.cu) ----
 // One leaf of the decode map in 16 bytes, dequantised on the device:
 //   x: row | col << 16

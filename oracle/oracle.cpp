@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -225,6 +226,213 @@ uint64_t search_top_k(const Image& im, const Contracted& c, uint32_t row, uint32
     return evals;
 }
 
+// ------------------------------------------------------------------ Fisher (classified)
+
+// ORDERING and MAPPING (crates/mars-search/src/tables.rs:13-51), data from Mars 1's
+// globals.h.
+const int FISHER_ORDERING[24][6] = {
+    {3, 2, 1, 0, 3, 0}, {2, 3, 1, 0, 5, 1}, {2, 1, 3, 0, 5, 2}, {3, 1, 2, 0, 7, 0},
+    {1, 3, 2, 0, 1, 1}, {1, 2, 3, 0, 1, 2}, {3, 2, 0, 1, 3, 1}, {2, 3, 0, 1, 5, 0},
+    {2, 1, 0, 3, 2, 2}, {3, 1, 0, 2, 7, 1}, {1, 3, 0, 2, 1, 0}, {1, 2, 0, 3, 4, 2},
+    {3, 0, 2, 1, 3, 2}, {2, 0, 3, 1, 2, 0}, {2, 0, 1, 3, 2, 1}, {3, 0, 1, 2, 7, 2},
+    {1, 0, 2, 3, 4, 1}, {1, 0, 3, 2, 4, 0}, {0, 3, 2, 1, 6, 2}, {0, 2, 3, 1, 6, 1},
+    {0, 2, 1, 3, 6, 0}, {0, 3, 1, 2, 0, 2}, {0, 1, 3, 2, 0, 1}, {0, 1, 2, 3, 0, 0},
+};
+const uint8_t FISHER_MAPPING[8][8] = {
+    {0, 1, 2, 3, 4, 5, 6, 7}, {2, 0, 3, 1, 7, 6, 4, 5}, {1, 3, 0, 2, 6, 7, 5, 4},
+    {3, 2, 1, 0, 5, 4, 7, 6}, {4, 7, 6, 5, 0, 3, 2, 1}, {5, 6, 7, 4, 3, 0, 1, 2},
+    {6, 4, 5, 7, 1, 2, 0, 3}, {7, 5, 4, 6, 2, 1, 3, 0},
+};
+
+// classify::Block (classify.rs:21-37).
+struct FBlock {
+    std::vector<double> data;
+    size_t size;
+    double at(size_t i, size_t j) const { return data[i * size + j]; }
+};
+
+// match_order (tables.rs:57-62).
+size_t match_order(const int order[4]) {
+    for (size_t r = 0; r < 24; ++r)
+        if (FISHER_ORDERING[r][0] == order[0] && FISHER_ORDERING[r][1] == order[1] &&
+            FISHER_ORDERING[r][2] == order[2] && FISHER_ORDERING[r][3] == order[3])
+            return r;
+    std::abort();  // order is always a permutation of 0..3
+}
+
+// bubble_sort_desc_with_order (classify.rs:62-73).
+void bubble_sort_desc(double a[4], int order[4]) {
+    for (int k = 0; k < 4; ++k) order[k] = k;
+    for (int i = 2; i >= 0; --i)
+        for (int j = 0; j <= i; ++j)
+            if (a[j] < a[j + 1]) {
+                std::swap(a[j], a[j + 1]);
+                std::swap(order[j], order[j + 1]);
+            }
+}
+
+// newclass (classify.rs:42-55, 94-101).
+void newclass(const FBlock& b, uint8_t* iso, uint8_t* clas) {
+    const size_t h = b.size / 2;
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (size_t i = 0; i < h; ++i)
+        for (size_t j = 0; j < h; ++j) {
+            a[0] += b.at(i, j);
+            a[1] += b.at(i, j + h);
+            a[2] += b.at(i + h, j);
+            a[3] += b.at(i + h, j + h);
+        }
+    int order[4];
+    bubble_sort_desc(a, order);
+    const size_t r = match_order(order);
+    *iso = (uint8_t)FISHER_ORDERING[r][4];
+    *clas = (uint8_t)FISHER_ORDERING[r][5];
+}
+
+// variance_2 (classify.rs:77-89).
+double variance_2(const FBlock& b, size_t atx, size_t aty, size_t size) {
+    double sum = 0.0, sum2 = 0.0;
+    for (size_t i = atx; i < atx + size; ++i)
+        for (size_t j = aty; j < aty + size; ++j) {
+            const double v = b.at(i, j);
+            sum += v;
+            sum2 += v * v;
+        }
+    const double n = (double)(size * size);
+    return sum2 / n - (sum / n) * (sum / n);
+}
+
+// variance_class (classify.rs:106-118).
+uint8_t variance_class(const FBlock& b) {
+    const size_t h = b.size / 2;
+    double a[4] = {variance_2(b, 0, 0, h), variance_2(b, 0, h, h), variance_2(b, h, 0, h),
+                   variance_2(b, h, h, h)};
+    int order[4];
+    bubble_sort_desc(a, order);
+    return (uint8_t)match_order(order);
+}
+
+// flips (classify.rs:139-164): out[i][j] = b[src(i, j)].
+FBlock flips(const FBlock& b, uint8_t iso) {
+    const size_t s = b.size;
+    FBlock out{std::vector<double>(s * s), s};
+    for (size_t i = 0; i < s; ++i)
+        for (size_t j = 0; j < s; ++j) {
+            size_t si, sj;
+            switch (iso) {
+                case 0: si = i; sj = j; break;
+                case 1: si = j; sj = s - i - 1; break;
+                case 2: si = s - j - 1; sj = i; break;
+                case 3: si = s - i - 1; sj = s - j - 1; break;
+                case 4: si = i; sj = s - j - 1; break;
+                case 5: si = s - i - 1; sj = j; break;
+                case 6: si = j; sj = i; break;
+                default: si = s - j - 1; sj = s - i - 1; break;
+            }
+            out.data[i * s + j] = b.at(si, sj);
+        }
+    return out;
+}
+
+// Fisher::index for one (size, shift) (fisher.rs:30-56): [clas][var_class] buckets of
+// (dom_row, dom_col, dom_iso) in raster order; empty buckets copy the first non-empty one.
+struct FisherLevel {
+    std::vector<std::tuple<uint32_t, uint32_t, uint8_t>> bucket[3][24];
+};
+
+FisherLevel fisher_index(const Image& im, const Contracted& c, uint32_t size, uint32_t shift) {
+    FisherLevel L;
+    if (im.h >= 2 * size && im.w >= 2 * size) {
+        const uint32_t step = std::max<uint32_t>(shift, 1);
+        for (uint32_t r = 0; r <= im.h - 2 * size; r += step)
+            for (uint32_t cc = 0; cc <= im.w - 2 * size; cc += step) {
+                FBlock b{std::vector<double>((size_t)size * size), size};
+                for (uint32_t u = 0; u < size; ++u)
+                    for (uint32_t v = 0; v < size; ++v)
+                        b.data[u * size + v] = (double)c.data[(r / 2 + u) * c.stride + cc / 2 + v];
+                uint8_t iso, clas;
+                newclass(b, &iso, &clas);
+                const uint8_t var = variance_class(flips(b, iso));
+                L.bucket[clas][var].emplace_back(r, cc, iso);
+            }
+    }
+    const std::vector<std::tuple<uint32_t, uint32_t, uint8_t>>* fb = nullptr;
+    for (auto& row : L.bucket)
+        for (auto& b : row)
+            if (!fb && !b.empty()) fb = &b;
+    if (fb) {
+        const auto copy = *fb;
+        for (auto& row : L.bucket)
+            for (auto& b : row)
+                if (b.empty()) b = copy;
+    }
+    return L;
+}
+
+// Fisher::candidates + search_block_fitted (fisher.rs:58-78, lib.rs:211-297): the range's
+// bucket in order, isometry MAPPING[range iso][domain iso], strict `<` on rms.
+uint64_t fisher_search(const Image& im, const Contracted& c, const FisherLevel& L, uint32_t row,
+                       uint32_t col, uint32_t size, const orc_params& p, orc_candidate* best) {
+    const size_t su = size;
+    std::vector<uint8_t> range(su * su);
+    int64_t t0 = 0, t2 = 0;
+    FBlock rb{std::vector<double>(su * su), su};
+    for (size_t i = 0; i < su; ++i)
+        for (size_t j = 0; j < su; ++j) {
+            const uint8_t r = im.px[(row + i) * (size_t)im.w + col + j];
+            range[i * su + j] = r;
+            rb.data[i * su + j] = (double)r;
+            t0 += r;
+            t2 += (int64_t)r * r;
+        }
+    std::vector<uint8_t> by_iso(8 * su * su);
+    for (uint32_t k = 0; k < 8; ++k) permute_range(range.data(), k, size, &by_iso[k * su * su]);
+    uint8_t isom, clas;
+    newclass(rb, &isom, &clas);
+    const uint8_t var = variance_class(flips(rb, isom));
+    const auto& bucket = L.bucket[clas][var];
+    std::memset(best, 0, sizeof *best);
+    uint64_t evals = 0;
+    const int64_t s0 = (int64_t)size * size;
+    for (const auto& e : bucket) {
+        const uint32_t dr = std::get<0>(e), dc = std::get<1>(e);
+        const uint8_t iso = FISHER_MAPPING[isom][std::get<2>(e)];
+        int64_t s1_x4, s2_x16;
+        domain_sums(c, dr / 2, dc / 2, su, &s1_x4, &s2_x16);
+        const int64_t t1_x4 = cross_term_permuted(c, dr / 2, dc / 2, su, &by_iso[iso * su * su]);
+        orc_candidate cand;
+        cand.dom_row = dr;
+        cand.dom_col = dc;
+        cand.isometry = iso;
+        cand.valid = 1;
+        cand.m = orc_moments{s0, s1_x4, s2_x16, t0, t1_x4, t2};
+        fit_f64(cand.m, p.max_alfa, p.bits_alfa, p.bits_beta, &cand.qalfa, &cand.qbeta, &cand.rms);
+        evals += 1;
+        if (!best->valid || cand.rms < best->rms) *best = cand;
+    }
+    return evals;
+}
+
+// IndexedSearchProvider with Fisher (lib.rs:426-513): indexes per power-of-two size from
+// min_size (from 2 when the borders are not min_size-aligned) to max_size, at the base
+// stride and, for adaptive-density RD encodes, at the doubled stride.
+struct FisherIndexes {
+    std::map<std::pair<uint32_t, uint32_t>, FisherLevel> levels;  // (size, shift)
+    static FisherIndexes build(const Image& im, const Contracted& c, const orc_params& p,
+                               bool adaptive) {
+        FisherIndexes F;
+        std::vector<uint32_t> shifts{p.shift};
+        if (p.has_lambda && adaptive) shifts.push_back(p.shift * 2);
+        for (uint32_t sh : shifts) {
+            uint32_t size = (im.w % p.min_size != 0 || im.h % p.min_size != 0)
+                                ? 2
+                                : std::max<uint32_t>(p.min_size, 2);
+            for (; size <= p.max_size; size *= 2) F.levels[{size, sh}] = fisher_index(im, c, size, sh);
+        }
+        return F;
+    }
+};
+
 // ------------------------------------------------------------------ rate snapshot
 
 // AdaptiveModel (crates/mars-entropy/src/lib.rs:36-121).
@@ -414,7 +622,21 @@ struct Ctx {
     const RateModels* rate;
     uint8_t allowed[4];
     bool adaptive_density;
+    const FisherIndexes* fisher = nullptr;  // the final walk's provider when classified
 };
+
+// SearchProvider::search of the walk: ExhaustiveSearch, or the Fisher provider.
+uint64_t provider_search(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
+                         uint32_t shift, std::vector<orc_candidate>& top) {
+    if (!ctx.fisher)
+        return search_top_k(ctx.im, *ctx.contracted, row, col, size, shift, ctx.params, 1, top);
+    top.clear();
+    orc_candidate best;
+    const uint64_t ev = fisher_search(ctx.im, *ctx.contracted, ctx.fisher->levels.at({size, shift}),
+                                      row, col, size, ctx.params, &best);
+    if (best.valid) top.push_back(best);
+    return ev;
+}
 
 orc_leaf make_leaf(uint32_t row, uint32_t col, uint32_t size) {
     orc_leaf l;
@@ -481,8 +703,7 @@ WalkResult walk(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size) {
         return r;
     }
     std::vector<orc_candidate> top;
-    const uint64_t block_evals =
-        search_top_k(ctx.im, *ctx.contracted, row, col, size, ctx.params.shift, ctx.params, 1, top);
+    const uint64_t block_evals = provider_search(ctx, row, col, size, ctx.params.shift, top);
     const double best_rms = top.empty() ? INFINITY : top[0].rms;
     if (best_rms > ctx.params.t_rms && size > hdr.min_size) {
         WalkResult r = split(ctx, row, col, size / 2);
@@ -876,8 +1097,7 @@ RdResult walk_rd(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, doub
                                ? adaptive_shift(ctx.params.shift, block_rms(ctx.im, row, col, size))
                                : ctx.params.shift;
     std::vector<orc_candidate> top;
-    const uint64_t block_evals =
-        search_top_k(ctx.im, *ctx.contracted, row, col, size, shift, ctx.params, 1, top);
+    const uint64_t block_evals = provider_search(ctx, row, col, size, shift, top);
     Priced leaf = best_mode_leaf(ctx, row, col, size, top, node_lambda, sc);
     if (size <= hdr.min_size) {
         RdResult r;
@@ -1195,6 +1415,11 @@ int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
     std::vector<int32_t> res;
     uint64_t sev = 0, wev = 0;
     int status = 0;
+    if (o->method != 0 && o->method != 1) return -1;
+    // IndexedSearchProvider::build before the walks (lib.rs:480-513).
+    std::unique_ptr<FisherIndexes> fisher;
+    if (o->method == 1)
+        fisher.reset(new FisherIndexes(FisherIndexes::build(im, c, *p, o->adaptive_density != 0)));
     run_parallel(nthreads, [&]() {
         if (p->has_lambda) {
             // build_rate_snapshot (encode.rs:1139-1169): exhaustive threshold walk at t_rms 8.
@@ -1210,13 +1435,13 @@ int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
             wev = wr.evals;
             Ctx ctx{im, &c, hdr, *p, &rate, {o->allowed_modes[0], o->allowed_modes[1],
                                              o->allowed_modes[2], o->allowed_modes[3]},
-                    o->adaptive_density != 0};
+                    o->adaptive_density != 0, fisher.get()};
             RdResult rr = walk_rd(ctx, 0, 0, virtual_size(hdr), p->lambda);
             out = std::move(rr.leaves);
             res = std::move(rr.resid);
             sev = rr.evals;
         } else {
-            Ctx ctx{im, &c, hdr, *p, nullptr, {1, 1, 1, 1}, false};
+            Ctx ctx{im, &c, hdr, *p, nullptr, {1, 1, 1, 1}, false, fisher.get()};
             WalkResult wr = walk(ctx, 0, 0, virtual_size(hdr));
             out = std::move(wr.leaves);
             sev = wr.evals;
@@ -1236,6 +1461,42 @@ int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
 }
 
 void orc_free(void* ptr) { std::free(ptr); }
+
+int orc_fisher_search_blocks(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size,
+                             uint32_t shift, const orc_params* p, const uint32_t* rows,
+                             const uint32_t* cols, size_t n, orc_candidate* out,
+                             uint64_t* evals_per_block, int nthreads) {
+    if (!px || !p || size < 2 || shift == 0) return -1;
+    Image im{px, w, h};
+    Contracted c = Contracted::build(im);
+    const FisherLevel L = fisher_index(im, c, size, shift);
+    run_parallel(nthreads, [&]() {
+#pragma omp taskloop grainsize(16)
+        for (size_t i = 0; i < n; ++i)
+            evals_per_block[i] = fisher_search(im, c, L, rows[i], cols[i], size, *p, &out[i]);
+    });
+    return 0;
+}
+
+int orc_fisher_classify_domains(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size,
+                                uint32_t shift, uint8_t* bucket, uint8_t* iso) {
+    if (!px || size < 2 || shift == 0 || h < 2 * size || w < 2 * size) return -1;
+    Image im{px, w, h};
+    Contracted c = Contracted::build(im);
+    size_t k = 0;
+    for (uint32_t r = 0; r <= h - 2 * size; r += shift)
+        for (uint32_t cc = 0; cc <= w - 2 * size; cc += shift, ++k) {
+            FBlock b{std::vector<double>((size_t)size * size), size};
+            for (uint32_t u = 0; u < size; ++u)
+                for (uint32_t v = 0; v < size; ++v)
+                    b.data[u * size + v] = (double)c.data[(r / 2 + u) * c.stride + cc / 2 + v];
+            uint8_t is, clas;
+            newclass(b, &is, &clas);
+            bucket[k] = (uint8_t)(clas * 24 + variance_class(flips(b, is)));
+            iso[k] = is;
+        }
+    return 0;
+}
 
 void orc_forward_dct2d(const double* block, uint32_t size, double* out) {
     const auto r = forward_dct2d(std::vector<double>(block, block + (size_t)size * size), size);

@@ -80,6 +80,16 @@ int orc_search_grid(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size, ui
                     int nthreads);
 
 /* Same, over an explicit list of block origins (rows[i], cols[i]). */
+/* Fisher::index at (size, shift) + Fisher::candidates / search_block_fitted for each block. */
+int orc_fisher_search_blocks(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size,
+                             uint32_t shift, const orc_params* p, const uint32_t* rows,
+                             const uint32_t* cols, size_t n, orc_candidate* out,
+                             uint64_t* evals_per_block, int nthreads);
+/* The bucket (class * 24 + variance class) and canonicalising isometry of every domain
+ * position at (size, shift), raster order (classify.rs newclass / variance_class). */
+int orc_fisher_classify_domains(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size,
+                                uint32_t shift, uint8_t* bucket, uint8_t* iso);
+
 int orc_search_blocks(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size, uint32_t shift,
                       const orc_params* p, const uint32_t* rows, const uint32_t* cols,
                       size_t n, orc_candidate* out, uint64_t* evals_per_block, int nthreads);

@@ -95,6 +95,11 @@ def lib():
         L.orc_search_blocks.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_uint32, P(Params), C.c_void_p, C.c_void_p, C.c_size_t,
                                         C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_fisher_search_blocks.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                               C.c_uint32, P(Params), C.c_void_p, C.c_void_p,
+                                               C.c_size_t, C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_fisher_classify_domains.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                                  C.c_uint32, C.c_void_p, C.c_void_p]
         L.orc_encode.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, P(Params), P(Options),
                                  P(Header), P(C.c_void_p), P(C.c_size_t), P(C.c_void_p),
                                  P(C.c_size_t), P(C.c_uint64), P(C.c_uint64), C.c_int]
@@ -189,6 +194,37 @@ def search_blocks(img, size, shift, params: Params, rows, cols, nthreads=0):
     if rc:
         raise ValueError(f"orc_search_blocks failed: {rc}")
     return out, ev
+
+
+def fisher_search_blocks(img, size, shift, params: Params, rows, cols, nthreads=0):
+    """Fisher::index at (size, shift), then Fisher::candidates + search_block_fitted per block:
+    (candidates, evals per block)."""
+    a = _u8(img)
+    h, w = a.shape
+    rows = np.ascontiguousarray(rows, dtype=np.uint32)
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    out = np.zeros(len(rows), dtype=CANDIDATE_DTYPE)
+    ev = np.zeros(len(rows), dtype=np.uint64)
+    rc = lib().orc_fisher_search_blocks(a.ctypes.data, w, h, size, shift, C.byref(params),
+                                        rows.ctypes.data, cols.ctypes.data, len(rows),
+                                        out.ctypes.data, ev.ctypes.data, nthreads)
+    if rc:
+        raise ValueError(f"orc_fisher_search_blocks failed: {rc}")
+    return out, ev
+
+
+def fisher_classify_domains(img, size, shift):
+    """(bucket, isometry) of every domain position at (size, shift), raster order."""
+    a = _u8(img)
+    h, w = a.shape
+    n = ((h - 2 * size) // shift + 1) * ((w - 2 * size) // shift + 1)
+    bucket = np.zeros(n, np.uint8)
+    iso = np.zeros(n, np.uint8)
+    rc = lib().orc_fisher_classify_domains(a.ctypes.data, w, h, size, shift, bucket.ctypes.data,
+                                           iso.ctypes.data)
+    if rc:
+        raise ValueError(f"orc_fisher_classify_domains failed: {rc}")
+    return bucket, iso
 
 
 def encode(img, params: Params, allowed_modes=(1, 0, 1, 0), adaptive_density=False, nthreads=0,

@@ -1,0 +1,108 @@
+"""Fisher's classified search on the GPU (IndexedSearchProvider with Fisher,
+crates/mars-search/src/{lib,fisher,classify,tables}.rs) against the oracle's restatement,
+bit-exact: every node's candidate (domain, isometry, qalfa, qbeta, rms bits, moments) and
+eval count, and whole encodes through the Fisher provider.
+
+The device classifies from exact integer quadrant sums and a permutation of the quadrants;
+the oracle follows the reference literally (f64 blocks, flips, variance_2 loops), so
+agreement checks the two formulations against each other."""
+import numpy as np
+import pytest
+
+import mars_b200 as mb
+from mars_b200 import synthetic
+from oracle import oracle as orc
+from tests.golden_data import fixture_images
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = mb.Context(0)
+    yield c
+    c.close()
+
+
+def _grid(w, h, size):
+    r, c = np.meshgrid(np.arange(0, h - size + 1, size), np.arange(0, w - size + 1, size),
+                       indexing="ij")
+    return r.ravel().astype(np.uint32), c.ravel().astype(np.uint32)
+
+
+def _table_parity(ctx, img, min_size, max_size, shift, sizes):
+    h, w = img.shape
+    prov = ctx.search_provider(img, mb.make_params(min_size=min_size, max_size=max_size,
+                                                   shift=shift), method="fisher")
+    p = orc.make_params(min_size=min_size, max_size=max_size, shift=shift)
+    checked = 0
+    for size in sizes:
+        rows, cols = _grid(w, h, size)
+        if len(rows) == 0:
+            continue
+        g, gev = prov.search_many(rows, cols, size, shift)
+        o, oev = orc.fisher_search_blocks(img, size, shift, p, rows, cols)
+        assert np.array_equal(gev, oev), f"size {size}: eval counts differ"
+        assert g.tobytes() == o.tobytes(), f"size {size}: candidates differ"
+        checked += len(rows)
+    prov.close()
+    return checked
+
+
+@pytest.mark.parametrize("shift", [2, 4])
+def test_synthetic_plane_every_node(ctx, shift):
+    img = synthetic.gray(128, 96, 3)
+    assert _table_parity(ctx, img, 4, 32, shift, (4, 8, 16, 32)) > 0
+
+
+@pytest.mark.parametrize("name", ["mixed_129x127", "flat128", "checker8", "noise_u8", "zoneplate",
+                                  "ramp_h"])
+def test_fixture_images_every_node(ctx, name):
+    imgs, _ = fixture_images()
+    img = imgs[name]
+    h, w = img.shape
+    # Unaligned borders index sizes down to 2 (lib.rs:426-458); flat planes leave all but one
+    # bucket empty, exercising the first-non-empty fallback (fisher.rs:42-54).
+    sizes = (2, 4, 8, 16) if (w % 4 or h % 4) else (4, 8, 16)
+    assert _table_parity(ctx, img, 4, 16, 2, sizes) > 0
+
+
+def test_plane_without_domains(ctx):
+    img = synthetic.gray(12, 12, 1)
+    prov = ctx.search_provider(img, mb.make_params(min_size=4, max_size=8, shift=2),
+                               method="fisher")
+    out = prov.search(0, 0, 8, 2)
+    assert out.candidate is None and out.evals == 0
+    prov.close()
+
+
+def _encode_parity(ctx, img, params_kw, modes, adaptive=False):
+    gh, gl, gr, gc = ctx.encode(img, mb.make_params(**params_kw), allowed_modes=modes,
+                                adaptive_density=adaptive, method="fisher")
+    oh, ol, orr, osev, owev = orc.encode(img, orc.make_params(**params_kw), allowed_modes=modes,
+                                         adaptive_density=adaptive, method="fisher")
+    assert bytes(gh) == bytes(oh)
+    assert (gc.search_evals, gc.warmup_evals) == (osev, owev)
+    assert gl.tobytes() == ol.tobytes()
+    assert gr.tobytes() == orr.tobytes()
+    return gc
+
+
+@pytest.mark.parametrize("lam", [None, 50.0, 200.0])
+def test_fisher_encodes(ctx, lam):
+    # encmars --method fisher (IndexedSearchProvider::build with Fisher): the final walk
+    # searches the Fisher index, the RD warm-up stays exhaustive.
+    img = synthetic.gray(128, 128, 7)
+    gc = _encode_parity(ctx, img, dict(min_size=4, max_size=16, shift=2, lam=lam), (1, 1, 1, 1))
+    ex = ctx.encode(img, mb.make_params(min_size=4, max_size=16, shift=2, lam=lam),
+                    allowed_modes=(1, 1, 1, 1))[3]
+    assert gc.search_evals < ex.search_evals / 50
+    assert gc.warmup_evals == ex.warmup_evals
+
+
+def test_fisher_encode_adaptive_density_and_borders(ctx):
+    imgs, _ = fixture_images()
+    _encode_parity(ctx, imgs["mixed_129x127"], dict(min_size=4, max_size=16, shift=2, lam=200.0),
+                   (1, 1, 1, 0), adaptive=True)
+    _encode_parity(ctx, imgs["mixed_250x250"], dict(min_size=4, max_size=32, shift=4, t_rms=8.0),
+                   (1, 0, 1, 0))
