@@ -48,8 +48,9 @@ WORKLOAD = ("exhaustive search of every RD quadtree node of a 512x512 synthetic 
 # DRAM bytes (read + write) per launch of the dominant search kernel, from one ncu capture
 # of this workload's s=4 level (profiles/corr_tc_s4_512x512_ncu.md).
 NCU_TRAFFIC = {4: 21_066_496 + 12_032}
-# The same for one decode iteration, by plane side (profiles/decode_cell_*_ncu.md).
-NCU_DECODE_TRAFFIC = {4096: 34_837_248 + 706_816}
+# The same for one decode iteration, by plane side (profiles/decode_cell_*_ncu.md; the
+# 16384^2 figure is dram__bytes.sum.per_second x gpu__time_duration.sum of its capture).
+NCU_DECODE_TRAFFIC = {4096: 34_831_104 + 748_800, 16384: 4_797_900_000}
 
 
 def rank_info():
