@@ -227,6 +227,25 @@ int mars_decode_plan_create(mars_ctx* ctx, const mars_header* header, const mars
 int mars_decode_plan_run(mars_decode_plan* plan, uint32_t iterations, uint8_t* d_out);
 void mars_decode_plan_free(mars_decode_plan* plan);
 
+/* Colour input of the codec and its metric, on device planes, asynchronous on the context's
+ * stream except mars_mse_device:
+ *   ycbcr / rgb_from_ycbcr (crates/mars-core/src/metrics.rs:377-460): BT.601 full range,
+ *     n pixels of three planes each way;
+ *   downsample_box (crates/mars-codec/src/color.rs:60-83): w x h -> ceil(w/2) x ceil(h/2);
+ *   upsample_nearest (color.rs:85-101): sw x sh -> w x h;
+ *   mse (metrics.rs:29-48): exact sum of squared differences / n, returned on the host. */
+int mars_ycbcr_device(mars_ctx* ctx, const uint8_t* d_r, const uint8_t* d_g, const uint8_t* d_b,
+                      size_t n, uint8_t* d_y, uint8_t* d_cb, uint8_t* d_cr);
+int mars_rgb_from_ycbcr_device(mars_ctx* ctx, const uint8_t* d_y, const uint8_t* d_cb,
+                               const uint8_t* d_cr, size_t n, uint8_t* d_r, uint8_t* d_g,
+                               uint8_t* d_b);
+int mars_downsample_box_device(mars_ctx* ctx, const uint8_t* d_src, uint32_t width,
+                               uint32_t height, uint8_t* d_dst);
+int mars_upsample_nearest_device(mars_ctx* ctx, const uint8_t* d_src, uint32_t src_width,
+                                 uint32_t src_height, uint8_t* d_dst, uint32_t width,
+                                 uint32_t height);
+int mars_mse_device(mars_ctx* ctx, const uint8_t* d_a, const uint8_t* d_b, size_t n, double* mse);
+
 /* .ifs bitstream.  Buffers returned here are freed with mars_bytes_free / mars_leaves_free. */
 int mars_ifs_parse(const uint8_t* data, size_t len, mars_header* header, mars_leaf** leaves,
                    size_t* nleaves);

@@ -84,7 +84,9 @@ EXPORTS = (
     "mars_ifs_parse", "mars_ifs_write", "mars_bytes_free", "mars_search_blocks_noalloc",
     "mars_decode_plan_create", "mars_decode_plan_run", "mars_decode_plan_free",
     "mars_format_write", "mars_format_read", "mars_entropy_encode", "mars_entropy_decode",
-    "mars_residuals_free", "mars_indexed_table_build",
+    "mars_residuals_free", "mars_indexed_table_build", "mars_ycbcr_device",
+    "mars_rgb_from_ycbcr_device", "mars_downsample_box_device", "mars_upsample_nearest_device",
+    "mars_mse_device",
 )
 
 _lib = None
@@ -143,6 +145,11 @@ def lib():
     L.mars_format_read.argtypes = [vp, sz, P(Header), P(vp), P(sz), P(vp), P(sz)]
     L.mars_residuals_free.argtypes = [vp]
     L.mars_residuals_free.restype = None
+    L.mars_ycbcr_device.argtypes = [vp, vp, vp, vp, sz, vp, vp, vp]
+    L.mars_rgb_from_ycbcr_device.argtypes = [vp, vp, vp, vp, sz, vp, vp, vp]
+    L.mars_downsample_box_device.argtypes = [vp, vp, u32, u32, vp]
+    L.mars_upsample_nearest_device.argtypes = [vp, vp, u32, u32, vp, u32, u32]
+    L.mars_mse_device.argtypes = [vp, vp, vp, sz, P(C.c_double)]
     L.mars_entropy_encode.argtypes = [vp, sz, P(vp), P(sz)]
     L.mars_entropy_decode.argtypes = [vp, sz, vp, sz, vp]
     _lib = L
@@ -246,6 +253,7 @@ class Context:
         h = C.c_void_p()
         check(lib().mars_ctx_create(C.byref(h), device))
         self._h = h
+        self.device = device
 
     @property
     def handle(self) -> int:
@@ -337,6 +345,64 @@ class Context:
         lib().mars_leaves_free(ptr)
         lib().mars_residuals_free(rptr)
         return hdr, leaves, resid, cnt
+
+    # ---- colour input and metric (device kernels; host arrays staged through torch) ----
+
+    def _dev(self, arr):
+        import torch
+        return torch.from_numpy(np.ascontiguousarray(arr, dtype=np.uint8).ravel()).to(
+            f"cuda:{self.device}")
+
+    def _convert(self, planes, inverse: bool):
+        import torch
+        a, b, c = (self._dev(p) for p in planes)
+        outs = [torch.empty_like(a) for _ in range(3)]
+        fn = lib().mars_rgb_from_ycbcr_device if inverse else lib().mars_ycbcr_device
+        check(fn(self._h, a.data_ptr(), b.data_ptr(), c.data_ptr(), a.numel(),
+                 outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr()))
+        torch.cuda.synchronize()
+        shape = np.asarray(planes[0]).shape
+        return tuple(o.cpu().numpy().reshape(shape) for o in outs)
+
+    def ycbcr(self, r, g, b):
+        """metrics::ycbcr (crates/mars-core/src/metrics.rs:377-430): BT.601 full-range Y, Cb,
+        Cr planes of three RGB planes."""
+        return self._convert((r, g, b), False)
+
+    def rgb_from_ycbcr(self, y, cb, cr):
+        """metrics::rgb_from_ycbcr (metrics.rs:432-460)."""
+        return self._convert((y, cb, cr), True)
+
+    def downsample_box(self, plane):
+        """color::downsample_box (crates/mars-codec/src/color.rs:60-83)."""
+        import torch
+        h, w = np.asarray(plane).shape
+        src = self._dev(plane)
+        dst = torch.empty(((h + 1) // 2) * ((w + 1) // 2), dtype=torch.uint8, device=src.device)
+        check(lib().mars_downsample_box_device(self._h, src.data_ptr(), w, h, dst.data_ptr()))
+        torch.cuda.synchronize()
+        return dst.cpu().numpy().reshape((h + 1) // 2, (w + 1) // 2)
+
+    def upsample_nearest(self, plane, width: int, height: int):
+        """color::upsample_nearest (color.rs:85-101)."""
+        import torch
+        sh, sw = np.asarray(plane).shape
+        src = self._dev(plane)
+        dst = torch.empty(width * height, dtype=torch.uint8, device=src.device)
+        check(lib().mars_upsample_nearest_device(self._h, src.data_ptr(), sw, sh, dst.data_ptr(),
+                                                 width, height))
+        torch.cuda.synchronize()
+        return dst.cpu().numpy().reshape(height, width)
+
+    def mse(self, a, b) -> float:
+        """metrics::mse (metrics.rs:29-48): exact integer SSE / pixel count."""
+        if np.asarray(a).shape != np.asarray(b).shape:
+            raise ValueError("MSE requires identical dimensions")
+        da, db = self._dev(a), self._dev(b)
+        out = C.c_double()
+        check(lib().mars_mse_device(self._h, da.data_ptr(), db.data_ptr(), da.numel(),
+                                    C.byref(out)))
+        return out.value
 
     def decode_plan(self, hdr: Header, leaves: np.ndarray, residuals=None) -> "DecodePlan":
         leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
@@ -454,6 +520,12 @@ def entropy_decode(data: bytes, shape) -> list:
     check(lib().mars_entropy_decode(buf.ctypes.data, len(data), ev.ctypes.data, len(ev),
                                     out.ctypes.data))
     return [int(x) for x in out]
+
+
+def psnr_from_mse(mse: float) -> Optional[float]:
+    """metrics::psnr_from_mse (metrics.rs:57-59): 10 log10(255^2 / mse); None when the planes
+    are identical."""
+    return 10.0 * math.log10(255.0 * 255.0 / mse) if mse > 0.0 else None
 
 
 def ifs_write(hdr: Header, leaves: np.ndarray) -> bytes:

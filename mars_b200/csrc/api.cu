@@ -1022,6 +1022,71 @@ void mars_decode_plan_free(mars_decode_plan* p) {
     delete p;
 }
 
+int mars_ycbcr_device(mars_ctx* ctx, const uint8_t* d_r, const uint8_t* d_g, const uint8_t* d_b,
+                      size_t n, uint8_t* d_y, uint8_t* d_cb, uint8_t* d_cr) {
+    if (!ctx || (n && (!d_r || !d_g || !d_b || !d_y || !d_cb || !d_cr)))
+        return fail(MARS_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    MARS_CUDA(mars::launch_ycbcr(d_r, d_g, d_b, n, d_y, d_cb, d_cr, false, ctx->stream));
+    ctx->launches += n ? 1 : 0;
+    return MARS_OK;
+}
+
+int mars_rgb_from_ycbcr_device(mars_ctx* ctx, const uint8_t* d_y, const uint8_t* d_cb,
+                               const uint8_t* d_cr, size_t n, uint8_t* d_r, uint8_t* d_g,
+                               uint8_t* d_b) {
+    if (!ctx || (n && (!d_r || !d_g || !d_b || !d_y || !d_cb || !d_cr)))
+        return fail(MARS_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    MARS_CUDA(mars::launch_ycbcr(d_y, d_cb, d_cr, n, d_r, d_g, d_b, true, ctx->stream));
+    ctx->launches += n ? 1 : 0;
+    return MARS_OK;
+}
+
+int mars_downsample_box_device(mars_ctx* ctx, const uint8_t* d_src, uint32_t width,
+                               uint32_t height, uint8_t* d_dst) {
+    if (!ctx || !d_src || !d_dst) return fail(MARS_EINVAL, "NULL argument");
+    if (width == 0 || height == 0 || width > 65535 || height > 65535)
+        return fail(MARS_EINVAL, "plane dimensions must be in 1..65535");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    MARS_CUDA(mars::launch_downsample_box(d_src, (int)width, (int)height, d_dst, ctx->stream));
+    ctx->launches += 1;
+    return MARS_OK;
+}
+
+int mars_upsample_nearest_device(mars_ctx* ctx, const uint8_t* d_src, uint32_t src_width,
+                                 uint32_t src_height, uint8_t* d_dst, uint32_t width,
+                                 uint32_t height) {
+    if (!ctx || !d_src || !d_dst) return fail(MARS_EINVAL, "NULL argument");
+    if (src_width == 0 || src_height == 0 || width > 65535 || height > 65535)
+        return fail(MARS_EINVAL, "plane dimensions out of range");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    MARS_CUDA(mars::launch_upsample_nearest(d_src, (int)src_width, (int)src_height, d_dst,
+                                            (int)width, (int)height, ctx->stream));
+    ctx->launches += 1;
+    return MARS_OK;
+}
+
+int mars_mse_device(mars_ctx* ctx, const uint8_t* d_a, const uint8_t* d_b, size_t n, double* mse) {
+    if (!ctx || !mse || (n && (!d_a || !d_b))) return fail(MARS_EINVAL, "NULL argument");
+    if (n == 0) return fail(MARS_EINVAL, "MSE of an empty plane is undefined");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    MARS_CUDA(mars::launch_sse(d_a, d_b, n, ctx->num_sms, ctx->d_counter, ctx->stream));
+    ctx->launches += 1;
+    unsigned long long sum = 0;
+    MARS_CUDA(cudaMemcpyAsync(&sum, ctx->d_counter, sizeof sum, cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    if (int e = sync_bounded(ctx)) return e;
+    // Exact numerator, one rounding in the division, as the reference.
+    *mse = (double)sum / (double)n;
+    return MARS_OK;
+}
+
 int mars_ifs_parse(const uint8_t* data, size_t len, mars_header* header, mars_leaf** leaves,
                    size_t* nleaves) {
     if (!data || !header || !leaves || !nleaves) return fail(MARS_EINVAL, "NULL argument");

@@ -96,6 +96,21 @@ cudaError_t launch_fisher_search(const uint8_t* plane, int w, int h, const int32
                                  const FitParams& fp, CandidateOut* out, uint64_t* evals,
                                  cudaStream_t st);
 
+// ---- colour and metrics (color.cu) ----
+// ycbcr (inverse = false: r, g, b -> y, cb, cr) or rgb_from_ycbcr (inverse = true: y, cb, cr
+// -> r, g, b) over n pixels of three planes.
+cudaError_t launch_ycbcr(const uint8_t* p0, const uint8_t* p1, const uint8_t* p2, size_t n,
+                         uint8_t* q0, uint8_t* q1, uint8_t* q2, bool inverse, cudaStream_t st);
+// w x h -> ceil(w/2) x ceil(h/2).
+cudaError_t launch_downsample_box(const uint8_t* src, int w, int h, uint8_t* dst,
+                                  cudaStream_t st);
+// sw x sh -> w x h.
+cudaError_t launch_upsample_nearest(const uint8_t* src, int sw, int sh, uint8_t* dst, int w,
+                                    int h, cudaStream_t st);
+// Sum of squared differences of two planes of n bytes into *out (zeroed first).
+cudaError_t launch_sse(const uint8_t* a, const uint8_t* b, size_t n, int num_sms,
+                       unsigned long long* out, cudaStream_t st);
+
 // ---- decode (decode.cu) ----
 // One leaf of the decode map in 16 bytes, dequantised on the device:
 //   x: row | col << 16

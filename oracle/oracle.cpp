@@ -1498,6 +1498,61 @@ int orc_fisher_classify_domains(const uint8_t* px, uint32_t w, uint32_t h, uint3
     return 0;
 }
 
+// metrics.rs:377-430; f64::round is half away from zero, as std::round.
+void orc_ycbcr(const uint8_t* r, const uint8_t* g, const uint8_t* b, size_t n, uint8_t* y,
+               uint8_t* cb, uint8_t* cr) {
+    auto to_u8 = [](double v) { return (uint8_t)std::min(255.0, std::max(0.0, std::round(v))); };
+    for (size_t i = 0; i < n; ++i) {
+        const double R = r[i], G = g[i], B = b[i];
+        y[i] = to_u8(0.299 * R + 0.587 * G + 0.114 * B);
+        cb[i] = to_u8(128.0 - 0.168736 * R - 0.331264 * G + 0.5 * B);
+        cr[i] = to_u8(128.0 + 0.5 * R - 0.418688 * G - 0.081312 * B);
+    }
+}
+
+// metrics.rs:432-460.
+void orc_rgb_from_ycbcr(const uint8_t* y, const uint8_t* cb, const uint8_t* cr, size_t n,
+                        uint8_t* r, uint8_t* g, uint8_t* b) {
+    auto to_u8 = [](double v) { return (uint8_t)std::min(255.0, std::max(0.0, std::round(v))); };
+    for (size_t i = 0; i < n; ++i) {
+        const double Y = y[i], Cb = (double)cb[i] - 128.0, Cr = (double)cr[i] - 128.0;
+        r[i] = to_u8(Y + 1.402 * Cr);
+        g[i] = to_u8(Y - 0.344136 * Cb - 0.714136 * Cr);
+        b[i] = to_u8(Y + 1.772 * Cb);
+    }
+}
+
+// color.rs:60-83.
+void orc_downsample_box(const uint8_t* src, uint32_t w, uint32_t h, uint8_t* dst) {
+    const uint32_t ow = (w + 1) / 2, oh = (h + 1) / 2;
+    for (uint32_t oy = 0; oy < oh; ++oy)
+        for (uint32_t ox = 0; ox < ow; ++ox) {
+            const uint32_t x0 = 2 * ox, y0 = 2 * oy;
+            const uint32_t x1 = std::min(x0 + 1, w - 1), y1 = std::min(y0 + 1, h - 1);
+            const uint32_t sum = (uint32_t)src[y0 * w + x0] + src[y0 * w + x1] + src[y1 * w + x0] +
+                                 src[y1 * w + x1];
+            dst[oy * ow + ox] = (uint8_t)((sum + 2) / 4);
+        }
+}
+
+// color.rs:85-101.
+void orc_upsample_nearest(const uint8_t* src, uint32_t sw, uint32_t sh, uint8_t* dst, uint32_t w,
+                          uint32_t h) {
+    for (uint32_t y = 0; y < h; ++y)
+        for (uint32_t x = 0; x < w; ++x)
+            dst[(size_t)y * w + x] = src[(size_t)std::min(y / 2, sh - 1) * sw + std::min(x / 2, sw - 1)];
+}
+
+// metrics.rs:29-48: exact u64 sum, one division.
+double orc_mse(const uint8_t* a, const uint8_t* b, size_t n) {
+    uint64_t sum = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const int32_t d = (int32_t)a[i] - (int32_t)b[i];
+        sum += (uint64_t)(d * d);
+    }
+    return (double)sum / (double)n;
+}
+
 void orc_forward_dct2d(const double* block, uint32_t size, double* out) {
     const auto r = forward_dct2d(std::vector<double>(block, block + (size_t)size * size), size);
     std::copy(r.begin(), r.end(), out);

@@ -106,6 +106,18 @@ void orc_free(void* ptr);
 int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, const int32_t* residuals,
                size_t nresiduals, uint32_t iterations, uint8_t* out);
 
+/* metrics::ycbcr / rgb_from_ycbcr (crates/mars-core/src/metrics.rs:377-460),
+ * color::downsample_box / upsample_nearest (crates/mars-codec/src/color.rs:60-101) and
+ * metrics::mse (metrics.rs:29-48). */
+void orc_ycbcr(const uint8_t* r, const uint8_t* g, const uint8_t* b, size_t n, uint8_t* y,
+               uint8_t* cb, uint8_t* cr);
+void orc_rgb_from_ycbcr(const uint8_t* y, const uint8_t* cb, const uint8_t* cr, size_t n,
+                        uint8_t* r, uint8_t* g, uint8_t* b);
+void orc_downsample_box(const uint8_t* src, uint32_t w, uint32_t h, uint8_t* dst);
+void orc_upsample_nearest(const uint8_t* src, uint32_t sw, uint32_t sh, uint8_t* dst, uint32_t w,
+                          uint32_t h);
+double orc_mse(const uint8_t* a, const uint8_t* b, size_t n);
+
 /* dct.rs forward_dct2d / inverse_dct2d and quant.rs dead-zone quantiser, for tests. */
 void orc_forward_dct2d(const double* block, uint32_t size, double* out);
 void orc_inverse_dct2d(const double* coeffs, uint32_t size, double* out);

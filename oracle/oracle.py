@@ -106,6 +106,13 @@ def lib():
         L.orc_free.argtypes = [C.c_void_p]
         L.orc_decode.argtypes = [P(Header), C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
                                  C.c_uint32, C.c_void_p]
+        L.orc_ycbcr.argtypes = [C.c_void_p] * 3 + [C.c_size_t] + [C.c_void_p] * 3
+        L.orc_rgb_from_ycbcr.argtypes = [C.c_void_p] * 3 + [C.c_size_t] + [C.c_void_p] * 3
+        L.orc_downsample_box.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
+        L.orc_upsample_nearest.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                           C.c_uint32, C.c_uint32]
+        L.orc_mse.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+        L.orc_mse.restype = C.c_double
         L.orc_forward_dct2d.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
         L.orc_inverse_dct2d.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
         L.orc_dead_zone_quantize.argtypes = [C.c_double, C.c_double, C.c_double]
@@ -261,6 +268,43 @@ def decode(hdr: Header, leaves: np.ndarray, iterations: int = 10, residuals=None
     if rc:
         raise ValueError(f"orc_decode failed: {rc}")
     return out
+
+
+def _convert(fn, planes):
+    a, b, c = (np.ascontiguousarray(p, dtype=np.uint8) for p in planes)
+    outs = [np.empty_like(a) for _ in range(3)]
+    fn(a.ctypes.data, b.ctypes.data, c.ctypes.data, a.size, *[o.ctypes.data for o in outs])
+    return tuple(outs)
+
+
+def ycbcr(r, g, b):
+    return _convert(lib().orc_ycbcr, (r, g, b))
+
+
+def rgb_from_ycbcr(y, cb, cr):
+    return _convert(lib().orc_rgb_from_ycbcr, (y, cb, cr))
+
+
+def downsample_box(plane):
+    a = _u8(plane)
+    h, w = a.shape
+    out = np.empty(((h + 1) // 2, (w + 1) // 2), np.uint8)
+    lib().orc_downsample_box(a.ctypes.data, w, h, out.ctypes.data)
+    return out
+
+
+def upsample_nearest(plane, width, height):
+    a = _u8(plane)
+    sh, sw = a.shape
+    out = np.empty((height, width), np.uint8)
+    lib().orc_upsample_nearest(a.ctypes.data, sw, sh, out.ctypes.data, width, height)
+    return out
+
+
+def mse(a, b) -> float:
+    x, y = _u8(a), _u8(b)
+    assert x.shape == y.shape
+    return float(lib().orc_mse(x.ctypes.data, y.ctypes.data, x.size))
 
 
 def forward_dct2d(block: np.ndarray) -> np.ndarray:

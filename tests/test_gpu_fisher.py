@@ -30,6 +30,22 @@ def _grid(w, h, size):
     return r.ravel().astype(np.uint32), c.ravel().astype(np.uint32)
 
 
+def _border_twos(w, h):
+    """Size-2 nodes a walk reaches: in-plane children of size-4 nodes that cross the border
+    (forced splits, encode.rs:1330-1468)."""
+    rows, cols = [], []
+    for pr in range(0, h, 4):
+        for pc in range(0, w, 4):
+            if pr + 4 <= h and pc + 4 <= w:
+                continue
+            for r in (pr, pr + 2):
+                for c in (pc, pc + 2):
+                    if r + 2 <= h and c + 2 <= w:
+                        rows.append(r)
+                        cols.append(c)
+    return np.array(rows, np.uint32), np.array(cols, np.uint32)
+
+
 def _table_parity(ctx, img, min_size, max_size, shift, sizes):
     h, w = img.shape
     prov = ctx.search_provider(img, mb.make_params(min_size=min_size, max_size=max_size,
@@ -37,7 +53,9 @@ def _table_parity(ctx, img, min_size, max_size, shift, sizes):
     p = orc.make_params(min_size=min_size, max_size=max_size, shift=shift)
     checked = 0
     for size in sizes:
-        rows, cols = _grid(w, h, size)
+        # Every in-plane aligned node of size >= min_size is requested by some walk; below
+        # min_size only the border nodes that forced splits reach.
+        rows, cols = _grid(w, h, size) if size >= min_size else _border_twos(w, h)
         if len(rows) == 0:
             continue
         g, gev = prov.search_many(rows, cols, size, shift)
