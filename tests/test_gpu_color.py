@@ -55,11 +55,11 @@ def test_downsample_and_upsample(ctx, shape):
 @pytest.mark.parametrize("n", [1, 15, 16, 17, 4096, 1 << 20, (1 << 20) + 3])
 def test_mse(ctx, n):
     rng = np.random.default_rng(n)
-    a = rng.integers(0, 256, n, dtype=np.uint8)
-    b = rng.integers(0, 256, n, dtype=np.uint8)
+    a = rng.integers(0, 256, (1, n), dtype=np.uint8)
+    b = rng.integers(0, 256, (1, n), dtype=np.uint8)
     assert ctx.mse(a, b) == orc.mse(a, b)
     assert ctx.mse(a, a) == 0.0
-    assert ctx.mse(np.zeros(n, np.uint8), np.full(n, 255, np.uint8)) == 65025.0
+    assert ctx.mse(np.zeros((1, n), np.uint8), np.full((1, n), 255, np.uint8)) == 65025.0
 
 
 def test_color_pipeline_matches_the_oracle_pipeline(ctx):
