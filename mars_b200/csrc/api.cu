@@ -18,6 +18,7 @@
 
 #include "../../include/mars_b200.h"
 #include "codec.hpp"
+#include "context.hpp"
 #include "residual.hpp"
 #include "kernels.cuh"
 #include "tc.cuh"
@@ -48,20 +49,6 @@ namespace mars {
 // The message mars_last_error() reports, for entry points defined in other files.
 int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
 }  // namespace mars
-
-struct mars_ctx {
-    int device = 0;
-    int num_sms = 148;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    std::atomic<uint64_t> launches{0};
-    std::mutex mu;
-    unsigned long long* d_counter = nullptr;  // survivors that took the exact f64 fit
-    int* d_err = nullptr;                     // kernel-side error bits (bounded waits)
-    int search_path = 0;                      // 0 auto, 1 CUDA cores only, 2 tensor cores
-    bool tma_16_boxes = false;                // load A stages as 16 2-D boxes (A/B checks)
-    PFN_cuTensorMapEncodeTiled_v12000 encode_tiled = nullptr;
-};
 
 struct mars_table {
     uint32_t width = 0, height = 0;
@@ -1115,3 +1102,7 @@ int mars_ifs_write(const mars_header* header, const mars_leaf* leaves, size_t n,
 }
 
 }  // extern "C"
+
+namespace mars {
+int ctx_sync(mars_ctx* ctx) { return sync_bounded(ctx); }
+}  // namespace mars

@@ -1,0 +1,35 @@
+// The library context (mars_ctx) and the host helpers shared by the files that implement
+// the C ABI.  Internal: not part of include/mars_b200.h.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <atomic>
+#include <mutex>
+#include <string>
+
+#include "../../include/mars_b200.h"
+
+struct mars_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::atomic<uint64_t> launches{0};
+    std::mutex mu;
+    unsigned long long* d_counter = nullptr;  // survivors that took the exact f64 fit
+    int* d_err = nullptr;                     // kernel-side error bits (bounded waits)
+    int search_path = 0;                      // 0 auto, 1 CUDA cores only, 2 tensor cores
+    bool tma_16_boxes = false;                // load A stages as 16 2-D boxes (A/B checks)
+    PFN_cuTensorMapEncodeTiled_v12000 encode_tiled = nullptr;
+};
+
+namespace mars {
+// Records the message mars_last_error() reports and returns `code`.
+int set_last_error(int code, const std::string& msg);
+// Waits for the context's stream with the library's deadline (MARS_SYNC_TIMEOUT_S) and
+// turns kernel-reported errors into a status.  The caller holds ctx->mu.
+int ctx_sync(mars_ctx* ctx);
+}  // namespace mars

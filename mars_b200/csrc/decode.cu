@@ -115,20 +115,22 @@ __global__ void decode_expand_kernel(const DecodeLeaf* __restrict__ leaves,
     m.rc = (uint32_t)L.row | ((uint32_t)L.col << 16);
     m.dom = (uint32_t)L.dom_row | ((uint32_t)L.dom_col << 16);
     m.roff = -1;
-    uint32_t kind, cbyte = 0;
+    uint32_t kind, cbyte = 0, flags = 0;
     if (L.mode == 1) {
         kind = kLeafAffine;
+    } else if (L.mode == 3 && resid_off && resid_off[k] >= 0) {
+        // A zero-alpha residual leaf still adds its residual (ifs.rs:459-479).
+        kind = kLeafResidual;
+        m.roff = resid_off[k];
+        if (!L.domain) flags = kLeafNoDomain;
     } else if (!L.domain) {
         // d = 0: (0.5 + 0*alfa) + beta, the same for every pixel of the leaf.
         kind = kLeafConst;
         cbyte = clamp_u8(__dadd_rn(__dadd_rn(0.5, __dmul_rn(0.0, L.alfa)), L.beta));
-    } else if (L.mode == 3 && resid_off && resid_off[k] >= 0) {
-        kind = kLeafResidual;
-        m.roff = resid_off[k];
     } else {
         kind = kLeafDomain;
     }
-    m.info = (uint32_t)L.size | (kind << 12) | ((uint32_t)L.iso << 14) | (cbyte << 24);
+    m.info = (uint32_t)L.size | (kind << 12) | ((uint32_t)L.iso << 14) | flags | (cbyte << 24);
     maps[k] = m;
 }
 
@@ -168,8 +170,11 @@ __global__ void decode_pixel_kernel(const uint8_t* __restrict__ src, uint8_t* __
             const int S = (int)(m.info & 0xFFFu);
             const IsoInv t = iso_inverse((int)((m.info >> 14) & 7u), S - 1);
             const int u = t.cu + t.ai * i + t.aj * j, v = t.cv + t.bi * i + t.bj * j;
-            const size_t p = ((size_t)(m.dom & 0xFFFFu) + 2 * u) * w + (m.dom >> 16) + 2 * v;
-            const int sum = (int)src[p] + (int)src[p + w] + (int)src[p + 1] + (int)src[p + w + 1];
+            int sum = 0;
+            if (!(m.info & kLeafNoDomain)) {
+                const size_t p = ((size_t)(m.dom & 0xFFFFu) + 2 * u) * w + (m.dom >> 16) + 2 * v;
+                sum = (int)src[p] + (int)src[p + w] + (int)src[p + 1] + (int)src[p + w + 1];
+            }
             double value = domain_value(sum, m);
             if (kind == kLeafResidual) value = __dadd_rn(value, resid[m.roff + u * S + v]);
             out = to_u8(value);
@@ -231,17 +236,16 @@ __global__ void __launch_bounds__(128) decode_cell_kernel(
             const int vmin = v00 - 3 * ((t.bi < 0) | (t.bj < 0));
             const size_t total = (size_t)w * h;
             size_t off = ((size_t)(m.dom & 0xFFFFu) + 2 * umin) * w + (m.dom >> 16) + 2 * vmin;
-            uint32_t sums[4][2];  // 2x2 sums of sample (umin + p, vmin + q), 16-bit lanes
+            // 2x2 sums of sample (umin + p, vmin + q) in 16-bit lanes; zero without a domain.
+            uint32_t sums[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+            if (!(m.info & kLeafNoDomain)) {
 #pragma unroll
-            for (int r = 0; r < 8; ++r, off += w) {
-                const uint64_t row = load8(src, off, total);
-                const uint32_t s0 = pair_sums((uint32_t)row), s1 = pair_sums((uint32_t)(row >> 32));
-                if (r & 1) {
+                for (int r = 0; r < 8; ++r, off += w) {
+                    const uint64_t row = load8(src, off, total);
+                    const uint32_t s0 = pair_sums((uint32_t)row);
+                    const uint32_t s1 = pair_sums((uint32_t)(row >> 32));
                     sums[r >> 1][0] += s0;
                     sums[r >> 1][1] += s1;
-                } else {
-                    sums[r >> 1][0] = s0;
-                    sums[r >> 1][1] = s1;
                 }
             }
             // Values in sample order: byte q of word p is sample (umin + p, vmin + q).

@@ -128,16 +128,20 @@ struct DecodeConsts {
 };
 // Kinds of expanded leaf.
 enum : uint32_t { kLeafConst = 0, kLeafAffine = 1, kLeafDomain = 2, kLeafResidual = 3 };
+// info bit 17 of a residual leaf with qalfa == 0: no domain read, d = 0.
+constexpr uint32_t kLeafNoDomain = 1u << 17;
 // A leaf expanded for the gather (built once per leaf list by launch_decode_expand):
 //   const:    qalfa == 0 (modes 0/2): every pixel is the byte in info bits 24-31;
 //   affine:   mode 1: round((a + gx*i) + gy*j), (i, j) = (y - row, x - col);
 //   domain:   qalfa != 0 (modes 0/2): (0.5 + sum*a) + b, sum the 2x2 sum at
 //             (dom_row + 2u, dom_col + 2v), (u, v) the inverse isometry of (i, j), a = alfa/4;
-//   residual: mode 3: the domain value + res[roff + u*size + v], res the residual pool.
+//   residual: mode 3: the domain value + res[roff + u*size + v], res the residual pool;
+//             with qalfa == 0 (kLeafNoDomain) the domain is not read and sum = 0, so the
+//             value is (0.5 + 0*a) + b + res as in the reference.
 struct __align__(16) DecodeMap {
     double a, b, gx, gy;
     uint32_t rc;    // row | col << 16
-    uint32_t info;  // size (bits 0-11) | kind (12-13) | isometry (14-16) | const byte (24-31)
+    uint32_t info;  // size (0-11) | kind (12-13) | isometry (14-16) | no-domain (17) | const byte (24-31)
     uint32_t dom;   // dom_row | dom_col << 16
     int32_t roff;   // residual pool offset (kind residual), else -1
 };

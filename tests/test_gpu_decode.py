@@ -63,6 +63,46 @@ def test_unaligned_leaves_one_pixel_cells(ctx):
         assert np.array_equal(ctx.decode(hdr, leaves, iters), orc.decode(_ohdr(hdr), leaves, iters))
 
 
+def _mode3(leaves, rng, p_zero=0.5):
+    """Turn the domain leaves into mode-3 leaves, half of them with qalfa = 0 (no domain
+    read, the residual still added: ifs.rs:459-479), with random residual levels."""
+    out = leaves.copy()
+    pool = []
+    for k in range(len(out)):
+        if out["mode"][k] != 2:
+            continue
+        out["mode"][k] = 3
+        if rng.random() < p_zero:
+            out["qalfa"][k] = 0
+        n = int(out["size"][k]) ** 2
+        lv = np.zeros(n, np.int32)
+        nz = rng.choice(n, size=min(n, 6), replace=False)
+        lv[nz] = rng.integers(-20, 21, size=len(nz))
+        pool.append(lv)
+    return out, (np.concatenate(pool) if pool else np.zeros(0, np.int32))
+
+
+@pytest.mark.parametrize("w,h,seed", [(128, 96, 11), (30, 30, 12)])
+def test_zero_alpha_residual_leaves(ctx, w, h, seed):
+    rng = np.random.default_rng(seed)
+    if w == 30:  # size-5 leaves: the one-pixel-cell kernel
+        rows = []
+        for r in range(0, h, 5):
+            for c in range(0, w, 5):
+                dr, dc = int(rng.integers(0, h - 9)), int(rng.integers(0, w - 9))
+                rows.append((r, c, 5, 2, int(rng.integers(1, 17)), int(rng.integers(0, 128)),
+                             int(rng.integers(0, 8)), dr, dc, 0, 0))
+        base = np.array(rows, dtype=mb.LEAF_DTYPE)
+    else:
+        base = synthetic.quadtree_leaves(w, h, seed)
+    leaves, pool = _mode3(base, rng)
+    assert (leaves["mode"] == 3).any() and ((leaves["mode"] == 3) & (leaves["qalfa"] == 0)).any()
+    hdr = _hdr(w, h)
+    for iters in (1, 5):
+        assert np.array_equal(ctx.decode(hdr, leaves, iters, pool),
+                              orc.decode(_ohdr(hdr), leaves, iters, pool))
+
+
 def test_later_leaves_overwrite_earlier(ctx):
     # decode_step writes leaves in order, so a later leaf wins where two overlap.
     w = h = 64
