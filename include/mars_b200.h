@@ -227,6 +227,51 @@ int mars_decode_plan_create(mars_ctx* ctx, const mars_header* header, const mars
 int mars_decode_plan_run(mars_decode_plan* plan, uint32_t iterations, uint8_t* d_out);
 void mars_decode_plan_free(mars_decode_plan* plan);
 
+/* Attractor refinement (no reference counterpart: the reference fits each leaf to the
+ * collage error only).  The decode map of decode_leaf (crates/mars-codec/src/ifs.rs:406-484)
+ * is read as a continuous map of the plane, x_p = s_L * d_p(x) + o_L (+ the mode-3 residual),
+ * d_p the 2x2 domain mean at the inverse isometry of p, flat leaves x_p = o_L and mode-1
+ * leaves fixed; its fixed point x* is differentiated against the target t by the adjoint
+ * lambda = 2(x* - t) + D^T(S lambda), so dL/ds_L = sum_L lambda*d and dL/do_L = sum_L lambda
+ * for L = sum (x* - t)^2.
+ *
+ *   mars_refine_plan_create: validates and uploads the leaf list, its residual levels and the
+ *     w*h target plane, and builds the transposed-map gather lists;
+ *   mars_refine_params: the leaves' dequantised (s, o), n floats each (s = 0 for leaves
+ *     without a domain; o = 0 for mode 1);
+ *   mars_refine_forward: iterates from the flat-128 seed until max |x' - x| < tol or
+ *     max_iters; returns the loss, the iterations run and, when x_out is non-NULL, x*
+ *     (w*h floats, host);
+ *   mars_refine_backward: the adjoint at the last forward's x*, until the relative step
+ *     |lambda' - lambda| / |lambda'| < tol or max_iters, then the per-leaf gradients;
+ *   mars_refine_run: `steps` damped per-leaf Newton updates of (s, o) (initial damping `lr`,
+ *     halved on every step that does not lower the loss), re-quantised to the header's grid
+ *     (qalfa >= 1 kept on domain leaves), decoded exactly with `decode_iterations` steps;
+ *     out_leaves gets the best-decoding of the refined list and the refined list with the
+ *     leaves that decode worse put back, when it beats the input list, else the input list.
+ *     Geometry, modes, isometries, domains and residual levels are unchanged. */
+typedef struct mars_refine_plan mars_refine_plan;
+typedef struct mars_refine_report {
+    double loss_start, loss_end;     /* continuous-model loss before and after the updates */
+    double psnr_plain, psnr_refined; /* exact decodes of the input and refined lists, dB */
+    uint32_t steps;                  /* gradient steps taken */
+    uint32_t improving_steps;        /* of which lowered the loss (the others halve the step) */
+    uint32_t changed_leaves;         /* leaves of out_leaves whose qalfa/qbeta changed */
+    uint32_t accepted;               /* 1 when out_leaves is the refined list */
+} mars_refine_report;
+int mars_refine_plan_create(mars_ctx* ctx, const mars_header* header, const mars_leaf* leaves,
+                            size_t n, const int32_t* residuals, size_t nresiduals,
+                            const uint8_t* target, mars_refine_plan** out);
+int mars_refine_params(mars_refine_plan* plan, float* s, float* o);
+int mars_refine_forward(mars_refine_plan* plan, const float* s, const float* o,
+                        uint32_t max_iters, double tol, float* x_out, double* loss,
+                        uint32_t* iters);
+int mars_refine_backward(mars_refine_plan* plan, uint32_t max_iters, double tol, float* grad_s,
+                         float* grad_o, uint32_t* iters, double* residual);
+int mars_refine_run(mars_refine_plan* plan, uint32_t steps, float lr, uint32_t decode_iterations,
+                    mars_leaf* out_leaves, mars_refine_report* report);
+void mars_refine_plan_free(mars_refine_plan* plan);
+
 /* Colour input of the codec and its metric, on device planes, asynchronous on the context's
  * stream except mars_mse_device:
  *   ycbcr / rgb_from_ycbcr (crates/mars-core/src/metrics.rs:377-460): BT.601 full range,

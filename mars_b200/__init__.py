@@ -65,6 +65,12 @@ class Counters(C.Structure):
     _fields_ = [("search_evals", C.c_uint64), ("warmup_evals", C.c_uint64)]
 
 
+class RefineReport(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("loss_start", "loss_end", "psnr_plain",
+                                          "psnr_refined")] + [
+        (n, C.c_uint32) for n in ("steps", "improving_steps", "changed_leaves", "accepted")]
+
+
 CANDIDATE_DTYPE = np.dtype([
     ("dom_row", "<u4"), ("dom_col", "<u4"), ("isometry", "<u4"), ("qalfa", "<u4"),
     ("qbeta", "<u4"), ("valid", "<u4"), ("rms", "<f8"), ("s0", "<i8"), ("s1_x4", "<i8"),
@@ -86,7 +92,8 @@ EXPORTS = (
     "mars_format_write", "mars_format_read", "mars_entropy_encode", "mars_entropy_decode",
     "mars_residuals_free", "mars_indexed_table_build", "mars_ycbcr_device",
     "mars_rgb_from_ycbcr_device", "mars_downsample_box_device", "mars_upsample_nearest_device",
-    "mars_mse_device",
+    "mars_mse_device", "mars_refine_plan_create", "mars_refine_params", "mars_refine_forward",
+    "mars_refine_backward", "mars_refine_run", "mars_refine_plan_free",
 )
 
 _lib = None
@@ -150,6 +157,14 @@ def lib():
     L.mars_downsample_box_device.argtypes = [vp, vp, u32, u32, vp]
     L.mars_upsample_nearest_device.argtypes = [vp, vp, u32, u32, vp, u32, u32]
     L.mars_mse_device.argtypes = [vp, vp, vp, sz, P(C.c_double)]
+    fp, dp = P(C.c_float), P(C.c_double)
+    L.mars_refine_plan_create.argtypes = [vp, P(Header), vp, sz, vp, sz, vp, P(vp)]
+    L.mars_refine_params.argtypes = [vp, vp, vp]
+    L.mars_refine_forward.argtypes = [vp, vp, vp, u32, C.c_double, vp, dp, P(u32)]
+    L.mars_refine_backward.argtypes = [vp, u32, C.c_double, vp, vp, P(u32), dp]
+    L.mars_refine_run.argtypes = [vp, u32, C.c_float, u32, vp, P(RefineReport)]
+    L.mars_refine_plan_free.argtypes = [vp]
+    L.mars_refine_plan_free.restype = None
     L.mars_entropy_encode.argtypes = [vp, sz, P(vp), P(sz)]
     L.mars_entropy_decode.argtypes = [vp, sz, vp, sz, vp]
     _lib = L
@@ -412,6 +427,19 @@ class Context:
                                             len(leaves), res.ctypes.data, len(res), C.byref(h)))
         return DecodePlan(h.value)
 
+    def refine_plan(self, hdr: Header, leaves: np.ndarray, target, residuals=None) -> "RefinePlan":
+        """The attractor-refinement plan of a leaf list against its target plane."""
+        leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+        res = _residuals(residuals)
+        t = np.ascontiguousarray(target, dtype=np.uint8)
+        if t.shape != (hdr.height, hdr.width):
+            raise ValueError("the target must be a (height, width) plane")
+        h = C.c_void_p()
+        check(lib().mars_refine_plan_create(self._h, C.byref(hdr), leaves.ctypes.data,
+                                            len(leaves), res.ctypes.data, len(res),
+                                            t.ctypes.data, C.byref(h)))
+        return RefinePlan(h.value, leaves, hdr)
+
     def decode(self, hdr: Header, leaves: np.ndarray, iterations: int = 10,
                residuals=None) -> np.ndarray:
         leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
@@ -439,6 +467,61 @@ class DecodePlan:
     def close(self) -> None:
         if self._h:
             lib().mars_decode_plan_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RefinePlan:
+    """mars_refine_*: the decode map's fixed point and its adjoint gradient on the device."""
+
+    def __init__(self, handle: int, leaves: np.ndarray, hdr: Header):
+        self._h = C.c_void_p(handle)
+        self.n = len(leaves)
+        self.shape = (hdr.height, hdr.width)
+
+    def params(self):
+        """The leaves' dequantised (s, o) as float32 arrays."""
+        s, o = np.zeros(self.n, np.float32), np.zeros(self.n, np.float32)
+        check(lib().mars_refine_params(self._h, s.ctypes.data, o.ctypes.data))
+        return s, o
+
+    def forward(self, s, o, max_iters: int = 400, tol: float = 1e-4, want_x: bool = False):
+        """-> (loss, iterations, x* or None)."""
+        s = np.ascontiguousarray(s, np.float32)
+        o = np.ascontiguousarray(o, np.float32)
+        if len(s) != self.n or len(o) != self.n:
+            raise ValueError("s and o need one value per leaf")
+        x = np.zeros(self.shape, np.float32) if want_x else None
+        loss, it = C.c_double(), C.c_uint32()
+        check(lib().mars_refine_forward(self._h, s.ctypes.data, o.ctypes.data, max_iters, tol,
+                                        x.ctypes.data if want_x else None, C.byref(loss),
+                                        C.byref(it)))
+        return loss.value, it.value, x
+
+    def backward(self, max_iters: int = 400, tol: float = 1e-6):
+        """-> (dL/ds, dL/do, iterations, relative residual) at the last forward's x*."""
+        gs, go = np.zeros(self.n, np.float32), np.zeros(self.n, np.float32)
+        it, res = C.c_uint32(), C.c_double()
+        check(lib().mars_refine_backward(self._h, max_iters, tol, gs.ctypes.data, go.ctypes.data,
+                                         C.byref(it), C.byref(res)))
+        return gs, go, it.value, res.value
+
+    def run(self, steps: int = 20, lr: float = 0.5, decode_iterations: int = 10):
+        """-> (leaves, RefineReport): the refined list if it decodes better, else the input."""
+        out = np.zeros(self.n, LEAF_DTYPE)
+        rep = RefineReport()
+        check(lib().mars_refine_run(self._h, steps, lr, decode_iterations, out.ctypes.data,
+                                    C.byref(rep)))
+        return out, rep
+
+    def close(self) -> None:
+        if self._h:
+            lib().mars_refine_plan_free(self._h)
             self._h = C.c_void_p(None)
 
     def __del__(self):

@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmars_b200.so")
-SOURCES = ["api.cu", "search.cu", "search_tc.cu", "decode.cu", "fisher.cu", "color.cu", "noalloc.cu", "codec.cpp", "format.cpp"]
+SOURCES = ["api.cu", "search.cu", "search_tc.cu", "decode.cu", "fisher.cu", "color.cu", "refine.cu", "noalloc.cu", "codec.cpp", "format.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1643,4 +1643,128 @@ double orc_leaf_bits(const orc_header* warm_hdr, const orc_leaf* warm_leaves, si
     return leaf_bits(rate, *warm_hdr, *leaf, size_class_of(leaf->size));
 }
 
+
+// ------------------------------------------------------------------ attractor refinement
+//
+// The continuous decode map of the refinement mode in f64 (the reference has no such mode;
+// the map follows decode_leaf, ifs.rs:406-484, leaf by leaf with later leaves overwriting):
+// x_p = clamp(s_L d_p(x) + o_L + r_p, 0, 255) for modes 0/2/3, d_p the 2x2 domain mean at
+// sample (u, v) with (i, j) = isometry::map(u, v) (0 without a domain), mode-1 leaves at
+// their decoded value, uncovered pixels 0.  The adjoint is the explicit transposed scatter:
+// lambda = 2 (x* - t) + sum over live domain pixels p of (s_L / 4) lambda_p into the four
+// samples p reads.
+
+int orc_refine_params(const orc_header* hdr, const orc_leaf* leaves, size_t n, double* s,
+                      double* o) {
+    for (size_t k = 0; k < n; ++k) {
+        const orc_leaf& L = leaves[k];
+        s[k] = o[k] = 0.0;
+        if (L.mode == 1) continue;
+        const double alfa = (double)L.qalfa / (double)(1u << hdr->bits_alfa) * max_alfa_of(*hdr);
+        double beta = (double)L.qbeta / (double)((1u << hdr->bits_beta) - 1) *
+                      ((1.0 + std::fabs(alfa)) * 255.0);
+        if (alfa > 0.0) beta -= alfa * 255.0;
+        s[k] = L.qalfa != 0 ? alfa : 0.0;
+        o[k] = beta;
+    }
+    return 0;
+}
+
+int orc_refine_eval(const orc_header* hdr, const orc_leaf* leaves, size_t n,
+                    const int32_t* residuals, size_t nres, const uint8_t* target, const double* s,
+                    const double* o, uint32_t fwd_iters, uint32_t adj_iters, double* x_out,
+                    double* loss, double* gs, double* go) {
+    const size_t w = hdr->width, h = hdr->height, npx = w * h;
+    std::vector<std::vector<double>> res(n);
+    size_t used = 0;
+    for (size_t k = 0; k < n; ++k) {
+        if (leaves[k].mode != 3) continue;
+        const size_t m = (size_t)leaves[k].size * leaves[k].size;
+        if (used + m > nres) return -1;
+        std::vector<double> deq(m);
+        for (size_t i = 0; i < m; ++i)
+            deq[i] = dz_dequantize(residuals[used + i], qstep_get(*hdr), RESIDUAL_DEAD_ZONE);
+        res[k] = inverse_dct2d(deq, leaves[k].size);
+        used += m;
+    }
+    if (used != nres) return -1;
+    std::vector<double> x(npx, 128.0), next(npx), dmean(npx), raw(npx);
+    std::vector<int64_t> owner(npx, -1);
+    std::vector<size_t> src(npx);  // top-left domain pixel read by p
+    auto step = [&](const std::vector<double>& cur) {
+        std::fill(next.begin(), next.end(), 0.0);
+        for (size_t k = 0; k < n; ++k) {
+            const orc_leaf& L = leaves[k];
+            const uint32_t S = L.size;
+            for (uint32_t u = 0; u < S; ++u)
+                for (uint32_t v = 0; v < S; ++v) {
+                    uint32_t i, j;
+                    double value, d = 0.0;
+                    size_t q = 0;
+                    if (L.mode == 1) {
+                        i = u;
+                        j = v;
+                        const double b0 = (double)L.qbeta / (double)((1u << hdr->bits_beta) - 1) * 255.0;
+                        value = std::round(b0 + (double)L.qgx / AFFINE_GRAD_SCALE * (double)u +
+                                           (double)L.qgy / AFFINE_GRAD_SCALE * (double)v);
+                    } else {
+                        iso_map(L.isometry, u, v, S, &i, &j);
+                        if (L.qalfa != 0) {
+                            q = (L.dom_row + 2 * u) * w + L.dom_col + 2 * v;
+                            d = (cur[q] + cur[q + 1] + cur[q + w] + cur[q + w + 1]) / 4.0;
+                        }
+                        value = s[k] * d + o[k];
+                        if (!res[k].empty()) value += res[k][u * S + v];
+                    }
+                    const size_t pp = (L.row + i) * w + L.col + j;
+                    owner[pp] = (int64_t)k;
+                    dmean[pp] = d;
+                    raw[pp] = value;
+                    src[pp] = q;
+                    next[pp] = std::min(std::max(value, 0.0), 255.0);
+                }
+        }
+    };
+    for (uint32_t it = 0; it < fwd_iters; ++it) {
+        step(x);
+        x.swap(next);
+    }
+    step(x);  // the linearisation at x (next = F(x) is discarded)
+    double l = 0.0;
+    std::vector<double> g(npx), lam(npx, 0.0), acc(npx);
+    for (size_t p = 0; p < npx; ++p) {
+        const double r = x[p] - (double)target[p];
+        g[p] = 2.0 * r;
+        l += r * r;
+    }
+    *loss = l;
+    auto live = [&](size_t p) {
+        const int64_t k = owner[p];
+        return k >= 0 && leaves[k].mode != 1 && raw[p] >= 0.0 && raw[p] <= 255.0;
+    };
+    for (uint32_t it = 0; it < adj_iters; ++it) {
+        std::fill(acc.begin(), acc.end(), 0.0);
+        for (size_t p = 0; p < npx; ++p) {
+            const int64_t k = owner[p];
+            if (!live(p) || leaves[k].qalfa == 0) continue;
+            const double c = s[k] * lam[p] / 4.0;
+            const size_t q = src[p];
+            acc[q] += c;
+            acc[q + 1] += c;
+            acc[q + w] += c;
+            acc[q + w + 1] += c;
+        }
+        for (size_t p = 0; p < npx; ++p) lam[p] = g[p] + acc[p];
+    }
+    for (size_t k = 0; k < n; ++k) gs[k] = go[k] = 0.0;
+    for (size_t p = 0; p < npx; ++p) {
+        if (!live(p)) continue;
+        const int64_t k = owner[p];
+        gs[k] += leaves[k].qalfa != 0 ? lam[p] * dmean[p] : 0.0;
+        go[k] += lam[p];
+    }
+    if (x_out) std::copy(x.begin(), x.end(), x_out);
+    return 0;
+}
+
 }  // extern "C"

@@ -103,6 +103,14 @@ int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
 void orc_free(void* ptr);
 
 /* decode_iterative from the flat-128 seed, modes 0/1/2. */
+// Attractor refinement model (f64): the leaves' dequantised (s, o), and the loss, fixed
+// point x (after fwd_iters steps from 128), and adjoint gradients (adj_iters steps from 0).
+int orc_refine_params(const orc_header* hdr, const orc_leaf* leaves, size_t n, double* s,
+                      double* o);
+int orc_refine_eval(const orc_header* hdr, const orc_leaf* leaves, size_t n,
+                    const int32_t* residuals, size_t nres, const uint8_t* target, const double* s,
+                    const double* o, uint32_t fwd_iters, uint32_t adj_iters, double* x_out,
+                    double* loss, double* gs, double* go);
 int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, const int32_t* residuals,
                size_t nresiduals, uint32_t iterations, uint8_t* out);
 

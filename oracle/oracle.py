@@ -125,6 +125,12 @@ def lib():
                                     P(C.c_size_t)]
         L.orc_leaf_bits.argtypes = [P(Header), C.c_void_p, C.c_size_t, P(Leaf)]
         L.orc_leaf_bits.restype = C.c_double
+        L.orc_refine_params.argtypes = [P(Header), C.c_void_p, C.c_size_t, C.c_void_p,
+                                        C.c_void_p]
+        L.orc_refine_eval.argtypes = [P(Header), C.c_void_p, C.c_size_t, C.c_void_p,
+                                      C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_uint32, C.c_uint32, C.c_void_p, P(C.c_double),
+                                      C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -356,3 +362,33 @@ def ifs_write(hdr: Header, leaves: np.ndarray) -> bytes:
 def pgm_bytes(img: np.ndarray) -> bytes:
     h, w = img.shape
     return b"P5\n%d %d\n255\n" % (w, h) + np.ascontiguousarray(img, dtype=np.uint8).tobytes()
+
+
+def refine_params(hdr: Header, leaves: np.ndarray):
+    """The leaves' dequantised (s, o) in f64 (s = 0 without a domain, both 0 for mode 1)."""
+    leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    s, o = np.zeros(len(leaves)), np.zeros(len(leaves))
+    lib().orc_refine_params(C.byref(hdr), leaves.ctypes.data, len(leaves), s.ctypes.data,
+                            o.ctypes.data)
+    return s, o
+
+
+def refine_eval(hdr: Header, leaves: np.ndarray, target, s, o, residuals=None,
+                fwd_iters: int = 600, adj_iters: int = 600):
+    """The refinement model in f64: (loss, x*, dL/ds, dL/do) after fwd_iters forward steps
+    from the flat-128 seed and adj_iters adjoint steps from zero."""
+    leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    res = np.ascontiguousarray(residuals if residuals is not None else np.zeros(0), dtype=np.int32)
+    t = np.ascontiguousarray(target, dtype=np.uint8)
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    o = np.ascontiguousarray(o, dtype=np.float64)
+    x = np.zeros((hdr.height, hdr.width))
+    gs, go = np.zeros(len(leaves)), np.zeros(len(leaves))
+    loss = C.c_double()
+    rc = lib().orc_refine_eval(C.byref(hdr), leaves.ctypes.data, len(leaves), res.ctypes.data,
+                               len(res), t.ctypes.data, s.ctypes.data, o.ctypes.data, fwd_iters,
+                               adj_iters, x.ctypes.data, C.byref(loss), gs.ctypes.data,
+                               go.ctypes.data)
+    if rc:
+        raise ValueError(f"orc_refine_eval failed: {rc}")
+    return loss.value, x, gs, go
