@@ -5,8 +5,11 @@
 #include "residual.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <thread>
 
 namespace mars {
 namespace codec {
@@ -671,6 +674,103 @@ bool residual_offsets(const mars_leaf* leaves, size_t n, size_t npool, std::vect
     return at == npool;
 }
 
+// ------------------------------------------------------------- host parallelism
+//
+// Below the forced splits every node's subtree is independent of the others (the walks read
+// the plane, the provider and the frozen rate snapshot only), which is what lets the
+// reference run them as Rayon tasks (encode.rs:1442-1468, 2033-2071).  Here the roots of
+// those subtrees are collected in the order the sequential walk visits them, walked on a
+// pool of host threads, and their results concatenated in that order, so the leaf list,
+// the residual pool and the eval counts are the sequential walk's exactly.
+
+struct Root {
+    uint32_t row, col, size;
+};
+
+// The nodes the forced splits reach (split order TL, BL, TR, BR), skipping those outside.
+void collect_roots(const mars_header& hdr, uint32_t row, uint32_t col, uint32_t size,
+                   std::vector<Root>* out) {
+    if (row >= hdr.height || col >= hdr.width) return;
+    const bool forced = size > hdr.max_size || row + size > hdr.height || col + size > hdr.width;
+    if (!forced) {
+        out->push_back({row, col, size});
+        return;
+    }
+    const uint32_t half = size / 2;
+    collect_roots(hdr, row, col, half, out);
+    collect_roots(hdr, row + half, col, half, out);
+    collect_roots(hdr, row, col + half, half, out);
+    collect_roots(hdr, row + half, col + half, half, out);
+}
+
+// Host threads for the walks: MARS_HOST_THREADS when set (>= 1), else every core.
+unsigned host_threads() {
+    if (const char* e = std::getenv("MARS_HOST_THREADS")) {
+        const long v = std::strtol(e, nullptr, 10);
+        if (v >= 1) return (unsigned)std::min<long>(v, 1024);
+    }
+    const unsigned hc = std::thread::hardware_concurrency();
+    return hc ? hc : 1;
+}
+
+// Runs fn(i) for i in [0, n) on up to host_threads() threads (dynamic assignment).
+template <class F>
+void parallel_for(size_t n, F&& fn) {
+    const unsigned nt = (unsigned)std::min<size_t>(host_threads(), n);
+    if (nt <= 1) {
+        for (size_t i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    auto worker = [&] {
+        for (size_t i; (i = next.fetch_add(1)) < n;) fn(i);
+    };
+    std::vector<std::thread> pool;
+    pool.reserve(nt - 1);
+    for (unsigned t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+}
+
+// walk / walk_rd over the whole plane, root subtrees in parallel; the first failing root's
+// status (in walk order) is returned.
+int walk_all(const Ctx& base, WalkResult* out) {
+    std::vector<Root> roots;
+    collect_roots(base.hdr, 0, 0, virtual_size(base.hdr), &roots);
+    std::vector<WalkResult> res(roots.size());
+    std::vector<int> status(roots.size(), MARS_OK);
+    parallel_for(roots.size(), [&](size_t i) {
+        Ctx ctx = base;
+        res[i] = walk(ctx, roots[i].row, roots[i].col, roots[i].size);
+        status[i] = ctx.status;
+    });
+    for (size_t i = 0; i < roots.size(); ++i) {
+        if (status[i]) return status[i];
+        out->leaves.insert(out->leaves.end(), res[i].leaves.begin(), res[i].leaves.end());
+        out->evals += res[i].evals;
+    }
+    return MARS_OK;
+}
+
+int walk_rd_all(const Ctx& base, double lambda, RdResult* out) {
+    std::vector<Root> roots;
+    collect_roots(base.hdr, 0, 0, virtual_size(base.hdr), &roots);
+    std::vector<RdResult> res(roots.size());
+    std::vector<int> status(roots.size(), MARS_OK);
+    parallel_for(roots.size(), [&](size_t i) {
+        Ctx ctx = base;
+        res[i] = walk_rd(ctx, roots[i].row, roots[i].col, roots[i].size, lambda);
+        status[i] = ctx.status;
+    });
+    for (size_t i = 0; i < roots.size(); ++i) {
+        if (status[i]) return status[i];
+        out->leaves.insert(out->leaves.end(), res[i].leaves.begin(), res[i].leaves.end());
+        out->resid.insert(out->resid.end(), res[i].resid.begin(), res[i].resid.end());
+        out->evals += res[i].evals;
+    }
+    return MARS_OK;
+}
+
 int encode(const Image& im, const mars_params& p, const mars_options& o, const Provider& provider,
            const Provider& warmup, mars_header* hdr_out, std::vector<mars_leaf>* leaves,
            std::vector<int32_t>* residuals, mars_counters* counters) {
@@ -689,23 +789,23 @@ int encode(const Image& im, const mars_params& p, const mars_options& o, const P
         Ctx warm{im, hdr, p, &warmup, nullptr, {1, 1, 1, 1}, false};
         warm.params.t_rms = 8.0;
         warm.params.has_lambda = 0;
-        WalkResult wr = walk(warm, 0, 0, virtual_size(hdr));
-        if (warm.status) return warm.status;
+        WalkResult wr;
+        if (int st = walk_all(warm, &wr)) return st;
         RateModels rate;
         if (!rate.build(hdr, wr.leaves)) return MARS_EINVAL;
         Ctx ctx{im, hdr, p, &provider, &rate,
                 {o.allowed_modes[0], o.allowed_modes[1], o.allowed_modes[2], o.allowed_modes[3]},
                 o.adaptive_density != 0};
-        RdResult rr = walk_rd(ctx, 0, 0, virtual_size(hdr), p.lambda);
-        if (ctx.status) return ctx.status;
+        RdResult rr;
+        if (int st = walk_rd_all(ctx, p.lambda, &rr)) return st;
         *leaves = std::move(rr.leaves);
         *residuals = std::move(rr.resid);
         counters->search_evals = rr.evals;
         counters->warmup_evals = wr.evals;
     } else {
         Ctx ctx{im, hdr, p, &provider, nullptr, {1, 1, 1, 1}, false};
-        WalkResult wr = walk(ctx, 0, 0, virtual_size(hdr));
-        if (ctx.status) return ctx.status;
+        WalkResult wr;
+        if (int st = walk_all(ctx, &wr)) return st;
         *leaves = std::move(wr.leaves);
         counters->search_evals = wr.evals;
         counters->warmup_evals = 0;

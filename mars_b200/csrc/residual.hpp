@@ -25,13 +25,20 @@ constexpr int32_t kLevelClamp = 63;    // LEVEL_CLAMP, residual.rs
 constexpr uint32_t kBands = 4;         // BANDS, residual.rs
 constexpr uint8_t FIELD_RESID_NZ = 10, FIELD_RESID_MAG = 11;
 
-// basis(n, k, i) at [k * n + i] (dct.rs:13-20).
+// basis(n, k, i) at [k * n + i] (dct.rs:13-20).  Each table is built once; the map's
+// nodes never move, so a reference handed out stays valid while other threads insert.
 inline const std::vector<double>& basis(uint32_t n) {
     static std::mutex mu;
     static std::map<uint32_t, std::vector<double>> cache;
+    thread_local std::map<uint32_t, const std::vector<double>*> local;  // lock-free hits
+    auto hit = local.find(n);
+    if (hit != local.end()) return *hit->second;
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(n);
-    if (it != cache.end()) return it->second;
+    if (it != cache.end()) {
+        local.emplace(n, &it->second);
+        return it->second;
+    }
     std::vector<double> b((size_t)n * n);
     const double pi = 3.14159265358979323846264338327950288;
     const double frac_1_sqrt_2 = 0.707106781186547524400844362104849039;
@@ -41,7 +48,9 @@ inline const std::vector<double>& basis(uint32_t n) {
             b[(size_t)k * n + i] =
                 std::sqrt(2.0 / (double)n) * ck * std::cos(pi / (double)n * ((double)i + 0.5) * (double)k);
         }
-    return cache.emplace(n, std::move(b)).first->second;
+    const std::vector<double>& ref = cache.emplace(n, std::move(b)).first->second;
+    local.emplace(n, &ref);
+    return ref;
 }
 
 // dct1d / idct1d over a strided vector (dct.rs:22-36).

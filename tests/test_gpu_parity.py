@@ -272,3 +272,18 @@ def test_device_entry_rejects_blocks_outside_the_plane(ctx):
     assert rec[0]["valid"] == 1 and rec[1]["valid"] == 0 and rec[2]["valid"] == 0
     o, _ = orc.search(img, 0, 0, 8, 2, orc.make_params(shift=2))
     assert rec[0].tobytes() == o[0].tobytes()
+
+
+@pytest.mark.parametrize("threads", ["1", "3", "64"])
+def test_host_walk_threads_do_not_change_the_encode(ctx, monkeypatch, threads):
+    # The walks run their independent subtrees on a pool of host threads; any pool size
+    # gives the sequential walk's leaves, residuals and eval counts.
+    img = synthetic.gray(200, 168, 12)
+    p = mb.make_params(min_size=4, max_size=16, shift=2, lam=200.0)
+    monkeypatch.setenv("MARS_HOST_THREADS", "1")
+    ref = ctx.encode(img, p, allowed_modes=(1, 1, 1, 1))
+    monkeypatch.setenv("MARS_HOST_THREADS", threads)
+    got = ctx.encode(img, p, allowed_modes=(1, 1, 1, 1))
+    assert np.array_equal(got[1], ref[1]) and np.array_equal(got[2], ref[2])
+    assert (got[3].search_evals, got[3].warmup_evals) == (ref[3].search_evals, ref[3].warmup_evals)
+    _encode_parity(ctx, img, dict(min_size=4, max_size=16, shift=2, lam=200.0), modes=(1, 1, 1, 1))
