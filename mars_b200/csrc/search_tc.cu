@@ -27,7 +27,8 @@
 //
 // Warp roles (320 threads): warp 0 issues the loads, warp 1 owns TMEM and issues the MMAs
 // (one elected lane), warps 2-9 are the epilogue (TMEM lane quadrant = warp % 4, two warps
-// per quadrant splitting the 256 columns).  The accumulator is double-buffered in TMEM
+// per quadrant splitting the 256 columns, 16 ranges each).  (Sixteen epilogue warps of 8
+// ranges each measured slower: the per-tile barriers, not the issue slots, set the pace.)  The accumulator is double-buffered in TMEM
 // (2 x 256 columns).  The epilogue runs the pruning test of fit.cuh once per (domain
 // lane, range) -- shared by the 8 isometry columns -- and queues survivors in shared
 // memory; batches of survivors get the exact f64 fit and update the ranges' champions
@@ -46,8 +47,12 @@ namespace mars {
 namespace tc {
 namespace {
 
-constexpr int kThreads = 320;                   // 10 warps: load, MMA, 8 epilogue
-constexpr int kEpiThreads = 256;
+constexpr int kEpiWarps = 8;                    // 2 per TMEM lane quadrant
+constexpr int kThreads = 64 + 32 * kEpiWarps;   // 10 warps: load, MMA, 8 epilogue
+constexpr int kEpiThreads = 32 * kEpiWarps;
+constexpr int kColsPerWarp = 4 * 256 / kEpiWarps;  // accumulator columns per epilogue warp
+constexpr int kRangesPerWarp = kColsPerWarp / 8;
+constexpr int kChunks = kColsPerWarp / 32;         // 32-column TMEM loads per pass
 constexpr int kM = 128;
 constexpr int kN = 256;
 constexpr int kRangesPerTile = kN / 8;         // 32
@@ -200,19 +205,21 @@ __device__ __forceinline__ void tmem_wait(int32_t (&v)[32]) {
                  : "memory");
 }
 
-__device__ __forceinline__ void epi_barrier() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ void epi_barrier() {
+    asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
+}
 
-// Named barrier over the 8 epilogue warps that also ANDs a predicate across them, so the
+// Named barrier over the epilogue warps that also ANDs a predicate across them, so the
 // warps always agree on whether to go on.
 __device__ __forceinline__ bool epi_barrier_and(bool pred) {
     uint32_t out;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.and.pred q, 1, 256, p;\n\t"
+        "bar.red.and.pred q, 1, %2, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}"
         : "=r"(out)
-        : "r"((uint32_t)pred)
+        : "r"((uint32_t)pred), "n"(kEpiThreads)
         : "memory");
     return out != 0;
 }
@@ -297,7 +304,7 @@ __device__ __forceinline__ void publish_threshold(Smem& sm, int rl, const FitPar
 
 // Exact fits of every queued survivor, then the per-range winners of the batch (atomic
 // min on the f64 bit pattern of rms >= 0, then on the reference index) and the champion /
-// threshold update.  All 256 epilogue threads call this together.
+// threshold update.  All epilogue threads call this together.
 template <int N>
 __device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t tag, int et,
                                          const DomainStats& ds, const FitParams& fp,
@@ -534,11 +541,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         __syncwarp();
     } else {
         // ---------------------------------------------------------------- epilogue
-        // Warps 2..9: TMEM lane quadrant = warp % 4 (each quadrant twice), column half
-        // (ranges [16*half, 16*half + 16)) = which of the two warps of that quadrant.
-        const int et = threadIdx.x - 64;         // 0..255
+        // Warps 2..: TMEM lane quadrant = warp % 4; column part (kRangesPerWarp ranges from
+        // part * kRangesPerWarp) = which of the quadrant's warps.
+        const int et = threadIdx.x - 64;         // 0..kEpiThreads-1
         const int e = warp & 3;
-        const int half = (warp - 2) >> 2;
+        const int part = (warp - 2) >> 2;
         const int m = e * 32 + lane;             // this thread's domain lane
         const float four_inv_n = 4.0f / (float)N;
         unsigned long long exact = 0;
@@ -571,7 +578,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             // a_min * Ndd and a_min/2 * Ndd, pre-scaled by 4 / n like the range records.
             const float ad = __fmul_rd(fp.a_min, detf) * four_inv_n;
             const float ahd = __fmul_rd(fp.a_half, detf) * four_inv_n;
-            const uint32_t tcol = tmem + ((uint32_t)(e * 32) << 16) + (uint32_t)(b * kN + half * 128);
+            const uint32_t tcol =
+                tmem + ((uint32_t)(e * 32) << 16) + (uint32_t)(b * kN + part * kColsPerWarp);
             bool rescan = false;
 
             auto max8 = [](const int32_t (&v)[32], int o) {
@@ -579,28 +587,28 @@ __global__ void __launch_bounds__(kThreads, 1)
                            max(max(v[o + 4], v[o + 5]), max(v[o + 6], v[o + 7])));
             };
             const uint32_t tag = (uint32_t)(mt & 0xFFFF);
-            // Thresholds of this lane's domain against its 16 ranges (fit.cuh, branch-free
+            // Thresholds of this lane's domain against its ranges (fit.cuh, branch-free
             // form).  They do not depend on the accumulator; each stage below runs over all
-            // 16 ranges so the independent chains overlap.
-            int32_t thr[16];
+            // of them so the independent chains overlap.
+            int32_t thr[kRangesPerWarp];
             auto all_thresholds = [&]() {
-                float4 ra[16];
-                int4 rb[16];
+                float4 ra[kRangesPerWarp];
+                int4 rb[kRangesPerWarp];
                 const float4* rec = reinterpret_cast<const float4*>(sm.thr);
 #pragma unroll
-                for (int r = 0; r < 16; ++r) {
-                    ra[r] = rec[2 * (half * 16 + r)];
-                    rb[r] = reinterpret_cast<const int4*>(rec)[2 * (half * 16 + r) + 1];
+                for (int r = 0; r < kRangesPerWarp; ++r) {
+                    ra[r] = rec[2 * (part * kRangesPerWarp + r)];
+                    rb[r] = reinterpret_cast<const int4*>(rec)[2 * (part * kRangesPerWarp + r) + 1];
                 }
-                float tau[16];
+                float tau[kRangesPerWarp];
 #pragma unroll
-                for (int r = 0; r < 16; ++r) {
+                for (int r = 0; r < kRangesPerWarp; ++r) {
                     const float g1 = __fmul_rd(ra[r].x, sdetf);
                     const float tz = fminf(__fadd_rd(ra[r].y, ahd), fmaxf(g1, ad));
                     tau[r] = dom > rb[r].x ? tz : __fadd_rd(g1, ra[r].z);
                 }
 #pragma unroll
-                for (int r = 0; r < 16; ++r) {
+                for (int r = 0; r < kRangesPerWarp; ++r) {
                     const float num = __fadd_rd(__fmul_rd(s1f, ra[r].w), tau[r]);
                     thr[r] = dom < 0 ? INT32_MAX : __float2int_rd(num);
                 }
@@ -619,7 +627,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const int32_t tc = c < 8 ? t0 : (c < 16 ? t1 : (c < 24 ? t2 : t3));
                         mask |= (v[c] >= tc ? 1u : 0u) << c;
                     }
-                    const int col0 = half * 128 + ch * 32;
+                    const int col0 = part * kColsPerWarp + ch * 32;
                     if (rescan) mask &= ~sm.evaluated[(m * kN + col0) >> 5];
                     int slot = atomicAdd(&sm.qcount, __popc(mask));
                     while (mask) {
@@ -640,24 +648,24 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!epi_barrier_and(got)) break;
             tmem_fence_after();
             for (;;) {
-                // ---- scan: this thread's 128 accumulator columns, loads overlapped with tests
+                // ---- scan: this thread's accumulator columns in 32-column chunks, each
+                // chunk's load overlapped with the previous chunk's test
+                static_assert(kChunks % 2 == 0, "chunks are scanned in pairs");
                 int32_t va[32], vb[32];
                 __syncwarp();
                 tmem_ld32(tcol, va);
                 tmem_wait(va);
-                tmem_ld32(tcol + 32u, vb);
-                test_chunk(va, 0);
-                __syncwarp();
-                tmem_wait(vb);
-                tmem_ld32(tcol + 64u, va);
-                test_chunk(vb, 1);
-                __syncwarp();
-                tmem_wait(va);
-                tmem_ld32(tcol + 96u, vb);
-                test_chunk(va, 2);
-                __syncwarp();
-                tmem_wait(vb);
-                test_chunk(vb, 3);
+#pragma unroll
+                for (int ch = 0; ch < kChunks; ch += 2) {
+                    tmem_ld32(tcol + 32u * (ch + 1), vb);
+                    test_chunk(va, ch);
+                    __syncwarp();
+                    tmem_wait(vb);
+                    if (ch + 2 < kChunks) tmem_ld32(tcol + 32u * (ch + 2), va);
+                    test_chunk(vb, ch + 1);
+                    __syncwarp();
+                    if (ch + 2 < kChunks) tmem_wait(va);
+                }
 
                 epi_barrier();
                 const int queued = sm.qcount;
