@@ -375,6 +375,49 @@ def run_refine(mb, ctx, stream, dev, peaks):
     }
 
 
+UNEVEN_COUNT, UNEVEN_SEED, UNEVEN_LARGE = 64, 5, 4096
+
+
+def run_uneven(mb, ctx, dev, large=True):
+    """Uneven batch: 64 gray planes with sides drawn (seeded) from {128, 256, 384, 512, 768,
+    1024}, then one 4096x4096 plane; every RD-quadtree node of each (sizes 32..4, domain
+    stride 2, lambda 200 nodes) searched through the provider factory with host planes in
+    and host tables out, one plane after another on one context."""
+    import torch
+    sides = synthetic.batch_sides(UNEVEN_COUNT, UNEVEN_SEED)
+    imgs = [synthetic.gray(s, s, 100 + i) for i, s in enumerate(sides)]
+    params = mb.make_params(min_size=4, max_size=32, shift=SHIFT, lam=200.0)
+    ctx.search_provider(imgs[0], params).close()
+    torch.cuda.synchronize(dev)
+
+    def timed(planes):
+        ev = 0
+        t0 = time.perf_counter()
+        for im in planes:
+            prov = ctx.search_provider(im, params)
+            ev += int(mb.lib().mars_search_table_evals(prov._h))
+            prov.close()
+        return ev, time.perf_counter() - t0
+
+    launches0 = ctx.launches
+    ev_b, t_b = timed(imgs)
+    out = {
+        "workload": f"{UNEVEN_COUNT} synthetic gray planes, sides from "
+                    "{128,256,384,512,768,1024} (seed 5), exhaustive search of every RD "
+                    "quadtree node, sizes 32..4, domain stride 2",
+        "value": ev_b / t_b, "unit": "fits/s", "evals": ev_b, "seconds": t_b,
+        "images_per_s": len(imgs) / t_b, "gpu_launches": ctx.launches - launches0,
+        "timing": "host wall clock around the provider factory (host plane in, node table "
+                  "out), planes one after another",
+    }
+    if large:
+        big = synthetic.gray(UNEVEN_LARGE, UNEVEN_LARGE, 99)
+        ev_l, t_l = timed([big])
+        out["large"] = {"workload": f"one {UNEVEN_LARGE}x{UNEVEN_LARGE} plane, same search",
+                        "value": ev_l / t_l, "unit": "fits/s", "evals": ev_l, "seconds": t_l}
+    return out
+
+
 def run_reference(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -511,6 +554,10 @@ def run_gpu(args):
     if rank == 0 and not args.no_refine:
         refine = run_refine(mb, ctx, stream, dev, peaks)
 
+    uneven = None
+    if rank == 0 and not args.no_uneven:
+        uneven = run_uneven(mb, ctx, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, desc = cpu_baseline()
@@ -540,6 +587,7 @@ def run_gpu(args):
             "decode": decode,
             "decode_large": decode_large,
             "refine": refine,
+            "uneven": uneven,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -558,6 +606,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-decode", action="store_true", help="skip the decode leg")
     ap.add_argument("--no-refine", action="store_true", help="skip the refinement leg")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

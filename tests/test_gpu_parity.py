@@ -287,3 +287,30 @@ def test_host_walk_threads_do_not_change_the_encode(ctx, monkeypatch, threads):
     assert np.array_equal(got[1], ref[1]) and np.array_equal(got[2], ref[2])
     assert (got[3].search_evals, got[3].warmup_evals) == (ref[3].search_evals, ref[3].warmup_evals)
     _encode_parity(ctx, img, dict(min_size=4, max_size=16, shift=2, lam=200.0), modes=(1, 1, 1, 1))
+
+
+def test_uneven_batch_encodes(ctx):
+    # The uneven-batch workload in miniature: planes of the batch's side set, exhaustive
+    # search 32..4 at stride 2, lambda 200, encoded one after another on one context.
+    sides = [s for s in synthetic.batch_sides(64, 5) if s <= 256][:3]
+    assert len(set(sides)) >= 2
+    for i, s in enumerate(sides):
+        _encode_parity(ctx, synthetic.gray(s, s, 100 + i),
+                       dict(min_size=4, max_size=32, shift=2, lam=200.0))
+
+
+def test_large_plane_sampled_nodes(ctx):
+    # A 2048x2048 plane of the generator: a scattered sample of nodes of every size checked
+    # against the oracle's search of those nodes (its exhaustive search of one 32x32 node
+    # at this size takes seconds, so the sample thins out with the size).
+    img = synthetic.gray(2048, 2048, 99)
+    prov = ctx.search_provider(img, mb.make_params(min_size=4, max_size=32, shift=2))
+    p = orc.make_params(min_size=4, max_size=32, shift=2)
+    rng = np.random.default_rng(1)
+    for size, n in ((4, 64), (8, 16), (16, 4), (32, 2)):
+        rows = (rng.integers(0, 2048 // size, n) * size).astype(np.uint32)
+        cols = (rng.integers(0, 2048 // size, n) * size).astype(np.uint32)
+        g, gev = prov.search_many(rows, cols, size, 2)
+        o, oev = orc.search_blocks(img, size, 2, p, rows, cols)
+        assert np.array_equal(gev, oev) and g.tobytes() == o.tobytes(), size
+    prov.close()
