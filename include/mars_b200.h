@@ -9,6 +9,8 @@
  *     (make_search(&Contracted) -> Box<dyn SearchProvider>)   -> mars_search_table_build
  *   SearchProvider::search    encode.rs:558-560, ExhaustiveSearch encode.rs:582-596
  *                                                              -> mars_search_table_lookup
+ *   SearchProvider::search_candidates  encode.rs:561-578, 598-601 (search_top_k)
+ *                              -> mars_search_table_build_ranked / _lookup_ranked
  *   search_block              encode.rs:610-619 (the fixed-grid GPU differential of
  *                             crates/mars-bench/src/gpu_search.rs:124-193) -> mars_search_blocks
  *   encode_image_with_search  encode.rs:1054-1126 with build_rate_snapshot :1139-1169
@@ -59,15 +61,18 @@ typedef struct mars_params {
 } mars_params;
 
 /* The EncodeOptions fields supported (encode.rs:78-109): allowed_modes (modes 0-3),
- * adaptive_density and residual_quantisation: residual_adaptive != 0 is LambdaAdaptive
- * (the step from lambda, 8 without one), else Fixed(residual_qstep) with 0 meaning the
- * default step 8 (ResidualQstep::LEGACY). */
+ * adaptive_density, residual_quantisation (residual_adaptive != 0 is LambdaAdaptive: the
+ * step from lambda, 8 without one; else Fixed(residual_qstep) with 0 meaning the default
+ * step 8, ResidualQstep::LEGACY) and rd_candidates (0 or 1: the single winner; 2..8: the
+ * RD walk prices modes 2/3 for the best rd_candidates domains, which needs a lambda and the
+ * exhaustive method, as encmars.rs:553-566 requires). */
 typedef struct mars_options {
     uint8_t allowed_modes[4];
     int32_t adaptive_density;
     int32_t residual_adaptive;
     float residual_qstep;
     int32_t method; /* MARS_METHOD_*: the search provider of the final walk */
+    uint32_t rd_candidates;
 } mars_options;
 
 /* Search methods (MethodName, crates/mars-search/src/lib.rs): the exhaustive search
@@ -140,6 +145,19 @@ int mars_search_table_build(mars_ctx* ctx, const uint8_t* plane, uint32_t width,
  * no legal domain) and the eval count the reference reports for it. */
 int mars_search_table_lookup(const mars_table* table, uint32_t row, uint32_t col, uint32_t size,
                              uint32_t shift, mars_candidate* out, uint64_t* evals);
+/* The ranked provider factory (ExhaustiveSearch::search_candidates with max = k,
+ * encode.rs:598-601 over search_top_k, encode.rs:695-788): every node's best k <= 8
+ * candidates by (rms, reference order), as retain_top_k keeps them.  k = 1 is
+ * mars_search_table_build. */
+int mars_search_table_build_ranked(mars_ctx* ctx, const uint8_t* plane, uint32_t width,
+                                   uint32_t height, const mars_params* params,
+                                   int32_t adaptive_density, uint32_t k, mars_table** out);
+/* SearchProvider::search_candidates for one node: up to `max` ranked candidates into
+ * out[0..*count) and the node's evals.  A table built with k = 1 (or by the classified
+ * provider) returns its single winner, as the trait's default does (encode.rs:561-578). */
+int mars_search_table_lookup_ranked(const mars_table* table, uint32_t row, uint32_t col,
+                                    uint32_t size, uint32_t shift, uint32_t max,
+                                    mars_candidate* out, uint32_t* count, uint64_t* evals);
 /* Total evals the table's searches stand for (all nodes, all shifts, counted as the
  * reference counts them: domain positions x 8 per node). */
 uint64_t mars_search_table_evals(const mars_table* table);

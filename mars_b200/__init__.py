@@ -44,10 +44,11 @@ class Params(C.Structure):
 
 class Options(C.Structure):
     """EncodeOptions (encode.rs:78-109): allowed modes, adaptive density, residual
-    quantisation (LambdaAdaptive when residual_adaptive, else Fixed(residual_qstep), 0 = 8)."""
+    quantisation (LambdaAdaptive when residual_adaptive, else Fixed(residual_qstep), 0 = 8),
+    the final walk's search method and rd_candidates (0/1 = the single winner)."""
     _fields_ = [("allowed_modes", C.c_uint8 * 4), ("adaptive_density", C.c_int32),
                 ("residual_adaptive", C.c_int32), ("residual_qstep", C.c_float),
-                ("method", C.c_int32)]
+                ("method", C.c_int32), ("rd_candidates", C.c_uint32)]
 
 
 # MethodName (crates/mars-search/src/lib.rs): the search provider of the final walk.
@@ -92,7 +93,8 @@ EXPORTS = (
     "mars_format_write", "mars_format_read", "mars_entropy_encode", "mars_entropy_decode",
     "mars_residuals_free", "mars_indexed_table_build", "mars_ycbcr_device",
     "mars_rgb_from_ycbcr_device", "mars_downsample_box_device", "mars_upsample_nearest_device",
-    "mars_mse_device", "mars_refine_plan_create", "mars_refine_params", "mars_refine_forward",
+    "mars_mse_device", "mars_search_table_build_ranked", "mars_search_table_lookup_ranked",
+    "mars_refine_plan_create", "mars_refine_params", "mars_refine_forward",
     "mars_refine_backward", "mars_refine_run", "mars_refine_plan_free",
 )
 
@@ -125,6 +127,8 @@ def lib():
     L.mars_indexed_table_build.argtypes = [vp, vp, u32, u32, P(Params), C.c_int32, C.c_int32,
                                            P(vp)]
     L.mars_search_table_lookup.argtypes = [vp, u32, u32, u32, u32, vp, P(u64)]
+    L.mars_search_table_build_ranked.argtypes = [vp, vp, u32, u32, P(Params), C.c_int32, u32, P(vp)]
+    L.mars_search_table_lookup_ranked.argtypes = [vp, u32, u32, u32, u32, u32, vp, P(u32), P(u64)]
     L.mars_search_table_evals.argtypes = [vp]
     L.mars_search_table_evals.restype = u64
     L.mars_search_table_exact_fits.argtypes = [vp]
@@ -228,6 +232,15 @@ class GpuSearch:
             evals[i] = ev.value
         return out, evals
 
+    def search_candidates(self, row: int, col: int, size: int, shift: int, max_: int):
+        """SearchProvider::search_candidates: (structured array of up to max_ candidates
+        ascending by (rms, reference order), evals)."""
+        out = np.zeros(max(max_, 1), dtype=CANDIDATE_DTYPE)
+        n, ev = C.c_uint32(), C.c_uint64()
+        check(lib().mars_search_table_lookup_ranked(self._h, row, col, size, shift, max_,
+                                                    out.ctypes.data, C.byref(n), C.byref(ev)))
+        return out[: n.value], ev.value
+
     def search(self, row: int, col: int, size: int, shift: int) -> SearchOutcome:
         out = np.zeros(1, dtype=CANDIDATE_DTYPE)
         ev = C.c_uint64()
@@ -305,13 +318,19 @@ class Context:
         return lib().mars_ctx_launch_count(self._h)
 
     def search_provider(self, img, params: Params, adaptive_density: bool = False,
-                        method: str = "exhaustive") -> GpuSearch:
-        """The provider factory: ExhaustiveSearch, or IndexedSearchProvider::build for a
-        classified method ("fisher")."""
+                        method: str = "exhaustive", k: int = 1) -> GpuSearch:
+        """The provider factory: ExhaustiveSearch (ranking the best k of every node when
+        k > 1), or IndexedSearchProvider::build for a classified method ("fisher")."""
         a = _plane(img)
         h, w = a.shape
         t = C.c_void_p()
-        if method == "exhaustive":
+        if k != 1:
+            if method != "exhaustive":
+                raise ValueError("only the exhaustive search ranks candidates")
+            check(lib().mars_search_table_build_ranked(self._h, a.ctypes.data, w, h,
+                                                       C.byref(params), int(adaptive_density),
+                                                       int(k), C.byref(t)))
+        elif method == "exhaustive":
             check(lib().mars_search_table_build(self._h, a.ctypes.data, w, h, C.byref(params),
                                                 int(adaptive_density), C.byref(t)))
         else:
@@ -340,14 +359,16 @@ class Context:
         return self.search_blocks(a, size, shift, params, rr.ravel(), cc.ravel())
 
     def encode(self, img, params: Params, allowed_modes=(1, 0, 1, 0), adaptive_density=False,
-               residual_adaptive=False, residual_qstep=0.0, method="exhaustive"):
+               residual_adaptive=False, residual_qstep=0.0, method="exhaustive",
+               rd_candidates=1):
         """encode_image_with_search with the GPU provider: (header, leaves, residuals,
         counters); `residuals` holds the levels of the mode-3 leaves, size*size each, in
         leaf order."""
         a = _plane(img)
         h, w = a.shape
         opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density),
-                       int(residual_adaptive), float(residual_qstep), METHODS[method])
+                       int(residual_adaptive), float(residual_qstep), METHODS[method],
+                       int(rd_candidates))
         hdr, cnt = Header(), Counters()
         ptr, n = C.c_void_p(), C.c_size_t()
         rptr, rn = C.c_void_p(), C.c_size_t()

@@ -52,8 +52,10 @@ int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
 
 struct mars_table {
     uint32_t width = 0, height = 0;
+    uint32_t k = 1;  // ranked candidates per node (cands holds the first of each)
     std::unordered_map<uint64_t, uint32_t> index;
     std::vector<mars_candidate> cands;
+    std::vector<mars_candidate> ranked;  // k per node, when k > 1
     std::vector<uint64_t> evals;
     uint64_t total_evals = 0;
     uint64_t exact_fits = 0;
@@ -254,16 +256,17 @@ int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32
 }
 
 // Search every block of one (size, shift) level.  rows/cols/out are device pointers.
+// k > 1: the ranked search (n x k results); k == 1: the single winner.
 int run_level(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t* d_D,
               uint32_t w, uint32_t h, uint32_t size, uint32_t shift, const mars::FitParams& fp,
               const uint32_t* d_rows, const uint32_t* d_cols, size_t n,
-              mars::CandidateOut* d_out) {
+              mars::CandidateOut* d_out, uint32_t k = 1) {
     if (n == 0) return MARS_OK;
     const cudaStream_t st = ctx->stream;
     const mars::LevelGeom g = level_geom(w, h, size, shift);
     if (g.nrow_d <= 0 || g.ncol_d <= 0) {
         // No legal domain: every candidate is None (encode.rs:734-739).
-        MARS_CUDA(cudaMemsetAsync(d_out, 0, n * sizeof(mars::CandidateOut), st));
+        MARS_CUDA(cudaMemsetAsync(d_out, 0, n * k * sizeof(mars::CandidateOut), st));
         return MARS_OK;
     }
     const size_t ndom = (size_t)g.nrow_d * g.ncol_d;
@@ -282,6 +285,16 @@ int run_level(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t*
                                        (int)size, fp, rs, st));
     MARS_CUDA(mars::launch_domain_stats(d_D, g, ds, st));
     ctx->launches += 2;
+    if (k > 1) {
+        const int nsplit = mars::search_topk_splits(g, (int)n, ctx->num_sms);
+        mars::Partial* partials;
+        MARS_CUDA(sc.get(&partials, (size_t)nsplit * n * k));
+        MARS_CUDA(mars::launch_search_topk(d_D, d_plane, (int)w, d_rows, d_cols, (int)n, g, rs,
+                                           ds, fp, (int)k, partials, nsplit, ctx->d_counter, st));
+        MARS_CUDA(mars::launch_reduce_topk(partials, nsplit, (int)n, (int)k, g, rs, ds, d_out, st));
+        ctx->launches += 2;
+        return MARS_OK;
+    }
     if (use_tc(ctx, size, shift))
         return run_level_tc(ctx, sc, d_plane, d_D, w, h, g, fp, d_rows, d_cols, n, rs, ds, d_out);
     const int nsplit = mars::search_simt_splits(g, (int)n, ctx->num_sms);
@@ -355,7 +368,8 @@ uint64_t level_evals(uint32_t w, uint32_t h, uint32_t size, uint32_t shift) {
 
 // Runs all jobs on the device plane; results land in d_out (concatenated in job order).
 int run_jobs(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uint32_t h,
-             const mars::FitParams& fp, const std::vector<Job>& jobs, mars::CandidateOut* d_out) {
+             const mars::FitParams& fp, const std::vector<Job>& jobs, mars::CandidateOut* d_out,
+             uint32_t k = 1) {
     const cudaStream_t st = ctx->stream;
     int32_t* d_D = nullptr;
     MARS_CUDA(sc.get(&d_D, (size_t)(w / 2) * (h / 2)));
@@ -376,7 +390,7 @@ int run_jobs(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uin
     off = 0;
     for (const Job& j : jobs) {
         const int e = run_level(ctx, sc, d_plane, d_D, w, h, j.size, j.shift, fp, d_rc + off,
-                                d_rc + total + off, j.rows.size(), d_out + off);
+                                d_rc + total + off, j.rows.size(), d_out + off * k, k);
         if (e) return e;
         off += j.rows.size();
     }
@@ -435,9 +449,15 @@ int run_jobs_fisher(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t
 
 int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, uint32_t w,
                 uint32_t h, const mars_params* params, bool adaptive, mars_table** out,
-                int method = MARS_METHOD_EXHAUSTIVE) {
+                int method = MARS_METHOD_EXHAUSTIVE, uint32_t k = 1) {
     if (!ctx || !out) return fail(MARS_EINVAL, "NULL argument");
     if (int e = check_params(params)) return e;
+    if (k < 1 || k > (uint32_t)mars::kMaxTopK)
+        return fail(MARS_EUNSUPPORTED, "ranked searches keep 1.." + std::to_string(mars::kMaxTopK) +
+                                           " candidates per node");
+    if (k > 1 && method != MARS_METHOD_EXHAUSTIVE)
+        return fail(MARS_EINVAL, "a ranked search needs the exhaustive method; other methods "
+                                 "propose one candidate");
     if (method != MARS_METHOD_EXHAUSTIVE && method != MARS_METHOD_FISHER)
         return fail(MARS_EUNSUPPORTED, "unknown search method " + std::to_string(method));
     if (method == MARS_METHOD_FISHER && params->max_size > 64)
@@ -463,8 +483,10 @@ int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, 
     std::unique_ptr<mars_table> guard(t);
     t->width = w;
     t->height = h;
+    t->k = k;
     t->cands.resize(total);
     t->evals.resize(total);
+    if (k > 1) t->ranked.resize(total * k);
     {
         Scratch sc(ctx->stream);
         const uint8_t* d_plane = d_plane_in;
@@ -476,7 +498,7 @@ int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, 
             d_plane = dp;
         }
         mars::CandidateOut* d_out = nullptr;
-        MARS_CUDA(sc.get(&d_out, total));
+        MARS_CUDA(sc.get(&d_out, total * k));
         MARS_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), ctx->stream));
         if (method == MARS_METHOD_FISHER) {
             uint64_t* d_evals = nullptr;
@@ -485,15 +507,18 @@ int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, 
             MARS_CUDA(cudaMemcpyAsync(t->evals.data(), d_evals, total * sizeof(uint64_t),
                                       cudaMemcpyDeviceToHost, ctx->stream));
         } else {
-            if (int e = run_jobs(ctx, sc, d_plane, w, h, fp, jobs, d_out)) return e;
+            if (int e = run_jobs(ctx, sc, d_plane, w, h, fp, jobs, d_out, k)) return e;
         }
-        MARS_CUDA(cudaMemcpyAsync(t->cands.data(), d_out, total * sizeof(mars_candidate),
-                                  cudaMemcpyDeviceToHost, ctx->stream));
+        MARS_CUDA(cudaMemcpyAsync(k > 1 ? t->ranked.data() : t->cands.data(), d_out,
+                                  total * k * sizeof(mars_candidate), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
         unsigned long long exact = 0;
         MARS_CUDA(cudaMemcpyAsync(&exact, ctx->d_counter, sizeof exact, cudaMemcpyDeviceToHost,
                                   ctx->stream));
         if (int e = sync_bounded(ctx)) return e;
         t->exact_fits = exact;
+        if (k > 1)
+            for (size_t i = 0; i < total; ++i) t->cands[i] = t->ranked[i * k];
     }
     size_t off = 0;
     t->index.reserve(total * 2);
@@ -618,6 +643,34 @@ int mars_search_table_lookup(const mars_table* t, uint32_t row, uint32_t col, ui
     return MARS_OK;
 }
 
+int mars_search_table_build_ranked(mars_ctx* ctx, const uint8_t* plane, uint32_t width,
+                                   uint32_t height, const mars_params* params,
+                                   int32_t adaptive_density, uint32_t k, mars_table** out) {
+    if (!plane) return fail(MARS_EINVAL, "plane is NULL");
+    return build_table(ctx, plane, nullptr, width, height, params, adaptive_density != 0, out,
+                       MARS_METHOD_EXHAUSTIVE, k);
+}
+
+int mars_search_table_lookup_ranked(const mars_table* t, uint32_t row, uint32_t col,
+                                    uint32_t size, uint32_t shift, uint32_t max,
+                                    mars_candidate* out, uint32_t* count, uint64_t* evals) {
+    if (!t || !count || (max && !out)) return fail(MARS_EINVAL, "NULL argument");
+    auto it = t->index.find(node_key(row, col, size, shift));
+    if (it == t->index.end())
+        return fail(MARS_ENOTFOUND, "node (" + std::to_string(row) + "," + std::to_string(col) +
+                                        "," + std::to_string(size) + ") at shift " +
+                                        std::to_string(shift) + " is not in the table");
+    const size_t i = it->second;
+    const mars_candidate* src = t->k > 1 ? &t->ranked[i * t->k] : &t->cands[i];
+    uint32_t n = 0;
+    const uint32_t lim = std::min<uint32_t>(std::max<uint32_t>(max, 1), t->k);
+    for (uint32_t j = 0; j < lim && n < max; ++j)
+        if (src[j].valid) out[n++] = src[j];
+    *count = n;
+    if (evals) *evals = t->evals[i];
+    return MARS_OK;
+}
+
 uint64_t mars_search_table_evals(const mars_table* t) { return t ? t->total_evals : 0; }
 uint64_t mars_search_table_exact_fits(const mars_table* t) { return t ? t->exact_fits : 0; }
 
@@ -717,13 +770,19 @@ int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t he
         !(std::isfinite(options->residual_qstep) && options->residual_qstep >= 1.0f &&
           options->residual_qstep <= 65535.0f))
         return fail(MARS_EINVAL, "residual qstep must be finite and in [1, 65535]");
+    const uint32_t rd_k = std::max<uint32_t>(1, options->rd_candidates);
+    if (rd_k > 1 && !params->has_lambda)
+        return fail(MARS_EINVAL, "rd_candidates > 1 requires the RD path (a lambda)");
+    if (rd_k > 1 && options->method != MARS_METHOD_EXHAUSTIVE)
+        return fail(MARS_EINVAL, "rd_candidates > 1 requires the exhaustive search; other "
+                                 "methods propose one candidate");
     const bool adaptive = params->has_lambda && options->adaptive_density;
     // The final walk's provider (the options' method) and, for an RD encode, the
     // exhaustive table the warm-up walk reads (the warm-up is exhaustive for every method).
     mars_table* table = nullptr;
     mars_table* warm = nullptr;
     if (int e = build_table(ctx, plane, nullptr, width, height, params, adaptive, &table,
-                            options->method))
+                            options->method, rd_k))
         return e;
     std::unique_ptr<mars_table, void (*)(mars_table*)> guard(table, mars_search_table_free);
     if (params->has_lambda && options->method != MARS_METHOD_EXHAUSTIVE) {
@@ -740,11 +799,22 @@ int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t he
     };
     const mars::codec::Provider provider = lookup(table);
     const mars::codec::Provider warmup = lookup(warm ? warm : table);
+    const mars::codec::RankedProvider ranked = [table](uint32_t row, uint32_t col, uint32_t size,
+                                                       uint32_t shift, uint32_t max,
+                                                       std::vector<mars_candidate>* v,
+                                                       uint64_t* evals) {
+        v->resize(std::max<uint32_t>(max, 1));
+        uint32_t n = 0;
+        const int e = mars_search_table_lookup_ranked(table, row, col, size, shift, max, v->data(),
+                                                      &n, evals);
+        v->resize(e ? 0 : n);
+        return e;
+    };
     std::vector<mars_leaf> out;
     std::vector<int32_t> res;
     const mars::codec::Image im{plane, width, height};
     if (int e = mars::codec::encode(im, *params, *options, provider, warmup, header, &out, &res,
-                                    counters))
+                                    counters, rd_k > 1 ? &ranked : nullptr))
         return e;
     *nleaves = out.size();
     *leaves = (mars_leaf*)std::malloc(std::max<size_t>(1, out.size()) * sizeof(mars_leaf));

@@ -195,6 +195,8 @@ struct Ctx {
     uint8_t allowed[4];
     bool adaptive_density;
     int status = MARS_OK;
+    const RankedProvider* ranked = nullptr;  // search_candidates, when rd_candidates > 1
+    uint32_t rd_candidates = 1;
 };
 
 mars_leaf make_leaf(uint32_t row, uint32_t col, uint32_t size) {
@@ -403,9 +405,10 @@ std::vector<int32_t> residual_for_candidate(const Ctx& ctx, const std::vector<do
     return levels;
 }
 
-// best_mode_leaf (encode.rs:1536-1714), modes 0-3 with the single-winner list.
+// best_mode_leaf (encode.rs:1536-1714), modes 0-3 over the provider's ranked list (the
+// single winner unless rd_candidates > 1); candidates with qalfa < 1 are skipped.
 Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
-                      const SearchAnswer& ans, double lambda, uint32_t sc) {
+                      const mars_candidate* ranked, size_t nranked, double lambda, uint32_t sc) {
     const mars_header& hdr = ctx.hdr;
     std::vector<double> block((size_t)size * size);
     int64_t rsum = 0;
@@ -433,20 +436,21 @@ Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
         affine_fit(block, size, hdr.bits_beta, &l.qbeta, &l.qgx, &l.qgy, &sse);
         cands.push_back({l, sse, leaf_bits(*ctx.rate, hdr, l, sc), {}});
     }
-    if (ans.cand.valid && ans.cand.qalfa >= 1 && ctx.allowed[2]) {
-        const mars_candidate& c = ans.cand;
-        mars_leaf l = make_leaf(row, col, size);
-        l.mode = 2;
-        l.qalfa = c.qalfa;
-        l.qbeta = c.qbeta;
-        l.isometry = c.isometry;
-        l.dom_row = c.dom_row;
-        l.dom_col = c.dom_col;
-        const double sse2 = c.rms * c.rms * (double)size * (double)size;
-        cands.push_back({l, sse2, leaf_bits(*ctx.rate, hdr, l, sc), {}});
-    }
-    if (ans.cand.valid && ans.cand.qalfa >= 1 && ctx.allowed[3]) {
-        const mars_candidate& c = ans.cand;
+    for (size_t ci = 0; ci < nranked; ++ci) {
+        const mars_candidate& c = ranked[ci];
+        if (!c.valid || c.qalfa < 1) continue;
+        if (ctx.allowed[2]) {
+            mars_leaf l = make_leaf(row, col, size);
+            l.mode = 2;
+            l.qalfa = c.qalfa;
+            l.qbeta = c.qbeta;
+            l.isometry = c.isometry;
+            l.dom_row = c.dom_row;
+            l.dom_col = c.dom_col;
+            const double sse2 = c.rms * c.rms * (double)size * (double)size;
+            cands.push_back({l, sse2, leaf_bits(*ctx.rate, hdr, l, sc), {}});
+        }
+        if (!ctx.allowed[3]) continue;
         mars_leaf l = make_leaf(row, col, size);
         l.mode = 3;
         l.qalfa = c.qalfa;
@@ -520,13 +524,22 @@ RdResult walk_rd(Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, double lam
     const uint32_t shift = ctx.adaptive_density
                                ? adaptive_shift(ctx.params.shift, block_rms(ctx.im, row, col, size))
                                : ctx.params.shift;
+    // rd_candidates == 1 keeps the single-winner search(); above 1 the ranked list widens
+    // modes 2/3's competition (encode.rs:1946-1977).
     SearchAnswer ans;
-    const int st = (*ctx.provider)(row, col, size, shift, &ans);
+    std::vector<mars_candidate> ranked;
+    int st;
+    if (ctx.rd_candidates > 1 && ctx.ranked) {
+        st = (*ctx.ranked)(row, col, size, shift, ctx.rd_candidates, &ranked, &ans.evals);
+    } else {
+        st = (*ctx.provider)(row, col, size, shift, &ans);
+        if (!st && ans.cand.valid) ranked.push_back(ans.cand);
+    }
     if (st) {
         ctx.status = st;
         return {};
     }
-    Priced leaf = best_mode_leaf(ctx, row, col, size, ans, node_lambda, sc);
+    Priced leaf = best_mode_leaf(ctx, row, col, size, ranked.data(), ranked.size(), node_lambda, sc);
     if (size <= hdr.min_size) {
         RdResult r;
         r.leaves.push_back(leaf.leaf);
@@ -773,7 +786,8 @@ int walk_rd_all(const Ctx& base, double lambda, RdResult* out) {
 
 int encode(const Image& im, const mars_params& p, const mars_options& o, const Provider& provider,
            const Provider& warmup, mars_header* hdr_out, std::vector<mars_leaf>* leaves,
-           std::vector<int32_t>* residuals, mars_counters* counters) {
+           std::vector<int32_t>* residuals, mars_counters* counters,
+           const RankedProvider* ranked) {
     mars_header hdr = build_header(im.w, im.h, p);
     // encode.rs:1066-1071: LambdaAdaptive -> from_lambda (8 without lambda); Fixed(step).
     if (o.residual_adaptive)
@@ -796,6 +810,8 @@ int encode(const Image& im, const mars_params& p, const mars_options& o, const P
         Ctx ctx{im, hdr, p, &provider, &rate,
                 {o.allowed_modes[0], o.allowed_modes[1], o.allowed_modes[2], o.allowed_modes[3]},
                 o.adaptive_density != 0};
+        ctx.ranked = ranked;
+        ctx.rd_candidates = std::max<uint32_t>(1, o.rd_candidates);
         RdResult rr;
         if (int st = walk_rd_all(ctx, p.lambda, &rr)) return st;
         *leaves = std::move(rr.leaves);

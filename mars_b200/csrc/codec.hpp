@@ -27,6 +27,11 @@ struct SearchAnswer {
 // (encode.rs:532-540).  Must be callable from any thread.
 using Provider = std::function<int(uint32_t row, uint32_t col, uint32_t size, uint32_t shift,
                                    SearchAnswer* out)>;
+// SearchProvider::search_candidates (encode.rs:561-578): up to `max` candidates ascending by
+// (rms, encounter order) and the node's evals.
+using RankedProvider =
+    std::function<int(uint32_t row, uint32_t col, uint32_t size, uint32_t shift, uint32_t max,
+                      std::vector<mars_candidate>* out, uint64_t* evals)>;
 
 struct Image {
     const uint8_t* px;
@@ -45,9 +50,11 @@ uint32_t adaptive_shift(uint32_t base, double rms);
 // `warmup` answers the exhaustive t_rms = 8 warm-up walk of an RD encode
 // (build_rate_snapshot searches exhaustively whatever the provider is); `provider` answers
 // the final walk.
+// `ranked` answers the final walk's search_candidates when o.rd_candidates > 1.
 int encode(const Image& im, const mars_params& p, const mars_options& o, const Provider& provider,
            const Provider& warmup, mars_header* hdr, std::vector<mars_leaf>* leaves,
-           std::vector<int32_t>* residuals, mars_counters* counters);
+           std::vector<int32_t>* residuals, mars_counters* counters,
+           const RankedProvider* ranked = nullptr);
 
 // The residual step of a header as f64 (ResidualQstep::get, quant.rs:54-56); 0 in the
 // struct stands for the default step 8.

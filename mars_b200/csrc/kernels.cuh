@@ -73,6 +73,19 @@ int search_simt_tiles(const LevelGeom& g);
 int search_simt_splits(const LevelGeom& g, int nranges, int num_sms);
 cudaError_t launch_reduce(const Partial* partials, int ntiles, int nranges, const LevelGeom& g,
                           RangeStats rs, DomainStats ds, CandidateOut* out, cudaStream_t st);
+// Ranked search (search_top_k, encode.rs:695-788, k = 2..kMaxTopK): the CUDA-core kernel
+// keeping the best k by (rms, reference index); partials are nsplit x nranges x k, the
+// result nranges x k (valid = 0 past the ranked candidates).
+constexpr int kMaxTopK = 8;
+int search_topk_splits(const LevelGeom& g, int nranges, int num_sms);
+cudaError_t launch_search_topk(const int32_t* D, const uint8_t* plane, int w,
+                               const uint32_t* rows, const uint32_t* cols, int nranges,
+                               const LevelGeom& g, RangeStats rs, DomainStats ds,
+                               const FitParams& fp, int k, Partial* partials, int nsplit,
+                               unsigned long long* counter, cudaStream_t st);
+cudaError_t launch_reduce_topk(const Partial* partials, int nsplit, int nranges, int k,
+                               const LevelGeom& g, RangeStats rs, DomainStats ds,
+                               CandidateOut* out, cudaStream_t st);
 
 // ---- Fisher classified search (fisher.cu) ----
 // The index of one (size, shift) level: per domain position (raster order) its bucket

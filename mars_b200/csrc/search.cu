@@ -28,6 +28,7 @@ constexpr float kHugeSqrtDet = 1.0e15f;
 constexpr int kTileRowsMax = 16;  // domain positions per tile, vertically
 constexpr int kTileColsMax = 32;  // and horizontally
 constexpr size_t kSmemBudget = 200 * 1024;
+constexpr int kMaxTopKSplits = 64;  // domain-tile splits a ranked search may use
 
 // isometry::map (crates/mars-codec/src/isometry.rs:7-19) as a flat range index i*S + j.
 __host__ __device__ constexpr int iso_src(int k, int u, int v, int S) {
@@ -119,12 +120,16 @@ __global__ void range_stats_kernel(const uint8_t* __restrict__ plane, int w, int
 // domain statistics are staged in shared memory; every thread correlates its range block
 // with each domain of the tile under all 8 isometries, applies the exact-bound filter and
 // runs the exact f64 fit on survivors only.
-template <int S, int RPB>
+// KMAX = 1 keeps the single champion (search_with_shift); KMAX > 1 keeps the best k <= KMAX
+// candidates by (rms, reference index) -- search_top_k's retain_top_k list -- and prunes
+// against the k-th once the list is full.  Partials hold k entries per (split, range).
+template <int S, int RPB, int KMAX>
 __global__ void __launch_bounds__(RPB) search_simt_kernel(
     const int32_t* __restrict__ D, LevelGeom g, const uint8_t* __restrict__ plane, int w,
     const uint32_t* __restrict__ rows, const uint32_t* __restrict__ cols, int nranges,
     RangeStats rs, DomainStats ds, FitParams fp, Partial* __restrict__ partials, int tiles_c,
-    int ntiles, int tile_rows, int tile_cols, unsigned long long* __restrict__ exact_counter) {
+    int ntiles, int tile_rows, int tile_cols, unsigned long long* __restrict__ exact_counter,
+    int k) {
     constexpr int N = S * S;
     constexpr bool kRegs = S <= 8;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -168,11 +173,21 @@ __global__ void __launch_bounds__(RPB) search_simt_kernel(
     const float t0f = (float)t0;
     const float inv_n = 1.0f / (float)N;  // exact: N is a power of four
     const double inf = __longlong_as_double(0x7ff0000000000000ll);
-    double ch_rms = inf, ch_sum = inf;
-    uint32_t ch_idx = UINT32_MAX;
-    int32_t ch_t1 = 0;
-    uint32_t ch_qa = 0, ch_qb = 0;
-    Threshold th = make_threshold(ch_sum, ch_rms, UINT32_MAX, rms0, nrr, N, fp);
+    double ch_rms[KMAX], ch_sum[KMAX];
+    uint32_t ch_idx[KMAX];
+    int32_t ch_t1[KMAX];
+    uint32_t ch_qa[KMAX], ch_qb[KMAX];
+#pragma unroll
+    for (int j = 0; j < KMAX; ++j) {
+        ch_rms[j] = inf;
+        ch_sum[j] = inf;
+        ch_idx[j] = UINT32_MAX;
+        ch_t1[j] = 0;
+        ch_qa[j] = ch_qb[j] = 0;
+    }
+    const int kk = KMAX == 1 ? 1 : k;  // entries kept; the list is full once ch_idx[kk-1] is set
+    // Until the list is full nothing can be pruned: the infinite cut-off below does that.
+    Threshold th = make_threshold(inf, inf, UINT32_MAX, rms0, nrr, N, fp);
     unsigned long long exact = 0;
 
     for (int tile = blockIdx.y; tile < ntiles; tile += gridDim.y) {
@@ -235,29 +250,60 @@ __global__ void __launch_bounds__(RPB) search_simt_kernel(
                     ++exact;
                     const FitResult f = fit_exact(N, s1, s2, t0, acc[k], t2, fp);
                     const uint32_t idx = dom * 8u + (uint32_t)k;
-                    if (f.rms < ch_rms || (f.rms == ch_rms && idx < ch_idx)) {
-                        ch_rms = f.rms;
-                        ch_sum = f.sum;
-                        ch_idx = idx;
-                        ch_t1 = acc[k];
-                        ch_qa = f.qalfa;
-                        ch_qb = f.qbeta;
-                        th = make_threshold(ch_sum, ch_rms, dom, rms0, nrr, N, fp);
+                    if constexpr (KMAX == 1) {
+                        if (f.rms < ch_rms[0] || (f.rms == ch_rms[0] && idx < ch_idx[0])) {
+                            ch_rms[0] = f.rms;
+                            ch_sum[0] = f.sum;
+                            ch_idx[0] = idx;
+                            ch_t1[0] = acc[k];
+                            ch_qa[0] = f.qalfa;
+                            ch_qb[0] = f.qbeta;
+                            th = make_threshold(f.sum, f.rms, dom, rms0, nrr, N, fp);
+                        }
+                    } else {
+                        // Sorted insertion by (rms, index); an empty slot holds (inf, MAX).
+                        const int last = kk - 1;
+                        if (f.rms < ch_rms[last] || (f.rms == ch_rms[last] && idx < ch_idx[last])) {
+                            int pos = last;
+                            while (pos > 0 && (f.rms < ch_rms[pos - 1] ||
+                                               (f.rms == ch_rms[pos - 1] && idx < ch_idx[pos - 1]))) {
+                                ch_rms[pos] = ch_rms[pos - 1];
+                                ch_sum[pos] = ch_sum[pos - 1];
+                                ch_idx[pos] = ch_idx[pos - 1];
+                                ch_t1[pos] = ch_t1[pos - 1];
+                                ch_qa[pos] = ch_qa[pos - 1];
+                                ch_qb[pos] = ch_qb[pos - 1];
+                                --pos;
+                            }
+                            ch_rms[pos] = f.rms;
+                            ch_sum[pos] = f.sum;
+                            ch_idx[pos] = idx;
+                            ch_t1[pos] = acc[k];
+                            ch_qa[pos] = f.qalfa;
+                            ch_qb[pos] = f.qbeta;
+                            if (ch_idx[last] != UINT32_MAX)
+                                th = make_threshold(ch_sum[last], ch_rms[last], ch_idx[last] >> 3,
+                                                    rms0, nrr, N, fp);
+                        }
                     }
                 }
             }
         }
     }
     if (!in_grid) return;
-    Partial p;
-    p.rms = ch_rms;
-    p.sum = ch_sum;
-    p.idx = ch_idx;
-    p.t1x4 = ch_t1;
-    p.qalfa = (uint16_t)ch_qa;
-    p.qbeta = (uint16_t)ch_qb;
-    p.pad = 0;
-    partials[(size_t)blockIdx.y * nranges + r] = p;
+#pragma unroll
+    for (int j = 0; j < KMAX; ++j) {
+        if (j >= kk) break;
+        Partial p;
+        p.rms = ch_rms[j];
+        p.sum = ch_sum[j];
+        p.idx = ch_idx[j];
+        p.t1x4 = ch_t1[j];
+        p.qalfa = (uint16_t)ch_qa[j];
+        p.qbeta = (uint16_t)ch_qb[j];
+        p.pad = 0;
+        partials[((size_t)blockIdx.y * nranges + r) * kk + j] = p;
+    }
     if (exact_counter && exact) atomicAdd(exact_counter, exact);
 }
 
@@ -294,6 +340,55 @@ __global__ void reduce_kernel(const Partial* __restrict__ partials, int ntiles, 
     out[r] = c;
 }
 
+// The best k of each range over the splits' sorted k-lists, by (rms, reference index);
+// out holds k candidates per range (valid = 0 past the ranked ones).
+__global__ void reduce_topk_kernel(const Partial* __restrict__ partials, int nsplit, int nranges,
+                                   int k, LevelGeom g, RangeStats rs, DomainStats ds,
+                                   CandidateOut* __restrict__ out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nranges) return;
+    const int64_t n = (int64_t)g.size * g.size;
+    // Each split's list is sorted, so one cursor per split walks them in merge order.
+    uint8_t cursor[kMaxTopKSplits];
+    for (int t = 0; t < nsplit; ++t) cursor[t] = 0;
+    for (int j = 0; j < k; ++j) {
+        int bt = -1;
+        Partial best;
+        best.rms = __longlong_as_double(0x7ff0000000000000ll);
+        best.idx = UINT32_MAX;
+        for (int t = 0; t < nsplit; ++t) {
+            if (cursor[t] >= k) continue;
+            const Partial p = partials[((size_t)t * nranges + r) * k + cursor[t]];
+            if (p.idx == UINT32_MAX) continue;
+            if (bt < 0 || p.rms < best.rms || (p.rms == best.rms && p.idx < best.idx)) {
+                best = p;
+                bt = t;
+            }
+        }
+        CandidateOut c;
+        if (bt < 0) {
+            c = CandidateOut{0, 0, 0, 0, 0, 0, 0.0, 0, 0, 0, 0, 0, 0};
+        } else {
+            ++cursor[bt];
+            const uint32_t dom = best.idx >> 3;
+            c.dom_row = (dom / g.ncol_d) * g.shift;
+            c.dom_col = (dom % g.ncol_d) * g.shift;
+            c.isometry = best.idx & 7u;
+            c.qalfa = best.qalfa;
+            c.qbeta = best.qbeta;
+            c.valid = 1;
+            c.rms = best.rms;
+            c.s0 = n;
+            c.s1_x4 = ds.s1x4[dom];
+            c.s2_x16 = ds.s2x16[dom];
+            c.t0 = rs.t0[r];
+            c.t1_x4 = best.t1x4;
+            c.t2 = rs.t2[r];
+        }
+        out[(size_t)r * k + j] = c;
+    }
+}
+
 int rpb_for(int size) { return size <= 16 ? 64 : (size == 32 ? 32 : 16); }
 
 // Domain tile of the CUDA-core kernel: as large as 16 x 32 positions while the staged
@@ -310,11 +405,11 @@ void simt_tile(int S, int step, int rpb, int* tr, int* tcn) {
     *tcn = c;
 }
 
-template <int S, int RPB>
+template <int S, int RPB, int KMAX>
 cudaError_t launch_simt_t(const int32_t* D, const uint8_t* plane, int w, const uint32_t* rows,
                           const uint32_t* cols, int nranges, const LevelGeom& g, RangeStats rs,
                           DomainStats ds, const FitParams& fp, Partial* partials, int nsplit,
-                          unsigned long long* counter, cudaStream_t st) {
+                          unsigned long long* counter, cudaStream_t st, int k) {
     int tr, tcn;
     simt_tile(S, g.step_c, RPB, &tr, &tcn);
     const int tiles_c = (g.ncol_d + tcn - 1) / tcn;
@@ -323,14 +418,30 @@ cudaError_t launch_simt_t(const int32_t* D, const uint8_t* plane, int w, const u
     const int strip_rows = (tr - 1) * g.step_c + S;
     size_t smem = (size_t)strip_ld * strip_rows * 4 + 3 * (size_t)tr * tcn * 4;
     if (S > 8) smem += (size_t)S * S * RPB;
-    auto kern = search_simt_kernel<S, RPB>;
+    auto kern = search_simt_kernel<S, RPB, KMAX>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid((nranges + RPB - 1) / RPB, nsplit);
     kern<<<grid, RPB, smem, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, partials,
-                                  tiles_c, ntiles, tr, tcn, counter);
+                                  tiles_c, ntiles, tr, tcn, counter, k);
     return cudaGetLastError();
+}
+
+template <int KMAX>
+cudaError_t launch_simt_k(const int32_t* D, const uint8_t* plane, int w, const uint32_t* rows,
+                          const uint32_t* cols, int nranges, const LevelGeom& g, RangeStats rs,
+                          DomainStats ds, const FitParams& fp, Partial* partials, int nsplit,
+                          unsigned long long* counter, cudaStream_t st, int k) {
+    switch (g.size) {
+        case 2: return launch_simt_t<2, 64, KMAX>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st, k);
+        case 4: return launch_simt_t<4, 64, KMAX>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st, k);
+        case 8: return launch_simt_t<8, 64, KMAX>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st, k);
+        case 16: return launch_simt_t<16, 64, KMAX>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st, k);
+        case 32: return launch_simt_t<32, 32, KMAX>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st, k);
+        case 64: return launch_simt_t<64, 16, KMAX>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st, k);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace
@@ -378,15 +489,33 @@ cudaError_t launch_search_simt(const int32_t* D, const uint8_t* plane, int w,
                                const FitParams& fp, Partial* partials, int nsplit,
                                unsigned long long* counter, cudaStream_t st) {
     if (nranges == 0 || g.nrow_d <= 0 || g.ncol_d <= 0) return cudaSuccess;
-    switch (g.size) {
-        case 2: return launch_simt_t<2, 64>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
-        case 4: return launch_simt_t<4, 64>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
-        case 8: return launch_simt_t<8, 64>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
-        case 16: return launch_simt_t<16, 64>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
-        case 32: return launch_simt_t<32, 32>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
-        case 64: return launch_simt_t<64, 16>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit, counter, st);
-        default: return cudaErrorInvalidValue;
-    }
+    return launch_simt_k<1>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials, nsplit,
+                            counter, st, 1);
+}
+
+int search_topk_splits(const LevelGeom& g, int nranges, int num_sms) {
+    return std::min(search_simt_splits(g, nranges, num_sms), kMaxTopKSplits);
+}
+
+cudaError_t launch_search_topk(const int32_t* D, const uint8_t* plane, int w,
+                               const uint32_t* rows, const uint32_t* cols, int nranges,
+                               const LevelGeom& g, RangeStats rs, DomainStats ds,
+                               const FitParams& fp, int k, Partial* partials, int nsplit,
+                               unsigned long long* counter, cudaStream_t st) {
+    if (k < 1 || k > kMaxTopK || nsplit > kMaxTopKSplits) return cudaErrorInvalidValue;
+    if (nranges == 0 || g.nrow_d <= 0 || g.ncol_d <= 0) return cudaSuccess;
+    return launch_simt_k<kMaxTopK>(D, plane, w, rows, cols, nranges, g, rs, ds, fp, partials,
+                                   nsplit, counter, st, k);
+}
+
+cudaError_t launch_reduce_topk(const Partial* partials, int nsplit, int nranges, int k,
+                               const LevelGeom& g, RangeStats rs, DomainStats ds,
+                               CandidateOut* out, cudaStream_t st) {
+    if (nranges == 0) return cudaSuccess;
+    if (k < 1 || k > kMaxTopK || nsplit > kMaxTopKSplits) return cudaErrorInvalidValue;
+    reduce_topk_kernel<<<(nranges + 127) / 128, 128, 0, st>>>(partials, nsplit, nranges, k, g,
+                                                               rs, ds, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_reduce(const Partial* partials, int ntiles, int nranges, const LevelGeom& g,

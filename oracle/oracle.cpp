@@ -623,13 +623,15 @@ struct Ctx {
     uint8_t allowed[4];
     bool adaptive_density;
     const FisherIndexes* fisher = nullptr;  // the final walk's provider when classified
+    uint32_t rd_candidates = 1;             // search_candidates' max in walk_rd
 };
 
-// SearchProvider::search of the walk: ExhaustiveSearch, or the Fisher provider.
+// SearchProvider::search of the walk (k = 1), or search_candidates with max = k
+// (encode.rs:561-601): ExhaustiveSearch ranks, the Fisher provider proposes one.
 uint64_t provider_search(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
-                         uint32_t shift, std::vector<orc_candidate>& top) {
+                         uint32_t shift, std::vector<orc_candidate>& top, uint32_t k = 1) {
     if (!ctx.fisher)
-        return search_top_k(ctx.im, *ctx.contracted, row, col, size, shift, ctx.params, 1, top);
+        return search_top_k(ctx.im, *ctx.contracted, row, col, size, shift, ctx.params, k, top);
     top.clear();
     orc_candidate best;
     const uint64_t ev = fisher_search(ctx.im, *ctx.contracted, ctx.fisher->levels.at({size, shift}),
@@ -1096,8 +1098,10 @@ RdResult walk_rd(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, doub
     const uint32_t shift = ctx.adaptive_density
                                ? adaptive_shift(ctx.params.shift, block_rms(ctx.im, row, col, size))
                                : ctx.params.shift;
+    // walk_rd's search (encode.rs:1946-1977): search() unless rd_candidates > 1.
     std::vector<orc_candidate> top;
-    const uint64_t block_evals = provider_search(ctx, row, col, size, shift, top);
+    const uint64_t block_evals =
+        provider_search(ctx, row, col, size, shift, top, std::max<uint32_t>(1, ctx.rd_candidates));
     Priced leaf = best_mode_leaf(ctx, row, col, size, top, node_lambda, sc);
     if (size <= hdr.min_size) {
         RdResult r;
@@ -1416,6 +1420,8 @@ int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
     uint64_t sev = 0, wev = 0;
     int status = 0;
     if (o->method != 0 && o->method != 1) return -1;
+    // encmars.rs:553-566: more than one candidate needs the RD path and the exhaustive search.
+    if (o->rd_candidates > 1 && (!p->has_lambda || o->method != 0)) return -1;
     // IndexedSearchProvider::build before the walks (lib.rs:480-513).
     std::unique_ptr<FisherIndexes> fisher;
     if (o->method == 1)
@@ -1436,6 +1442,7 @@ int orc_encode(const uint8_t* px, uint32_t w, uint32_t h, const orc_params* p,
             Ctx ctx{im, &c, hdr, *p, &rate, {o->allowed_modes[0], o->allowed_modes[1],
                                              o->allowed_modes[2], o->allowed_modes[3]},
                     o->adaptive_density != 0, fisher.get()};
+            ctx.rd_candidates = o->rd_candidates;
             RdResult rr = walk_rd(ctx, 0, 0, virtual_size(hdr), p->lambda);
             out = std::move(rr.leaves);
             res = std::move(rr.resid);

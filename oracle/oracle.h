@@ -38,6 +38,7 @@ typedef struct orc_options {
     int32_t residual_adaptive; /* ResidualQuantisation::LambdaAdaptive */
     float residual_qstep;      /* Fixed(step); 0 = ResidualQstep::LEGACY (8) */
     int32_t method;            /* 0 ExhaustiveSearch, 1 Fisher (IndexedSearchProvider) */
+    uint32_t rd_candidates;    /* EncodeOptions::rd_candidates; 0 or 1 = the single winner */
 } orc_options;
 
 /* RawMoments (encode.rs:225-232). */

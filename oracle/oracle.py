@@ -27,7 +27,7 @@ class Params(C.Structure):
 class Options(C.Structure):
     _fields_ = [("allowed_modes", C.c_uint8 * 4), ("adaptive_density", C.c_int32),
                 ("residual_adaptive", C.c_int32), ("residual_qstep", C.c_float),
-                ("method", C.c_int32)]
+                ("method", C.c_int32), ("rd_candidates", C.c_uint32)]
 
 
 METHODS = {"exhaustive": 0, "fisher": 1}
@@ -241,14 +241,14 @@ def fisher_classify_domains(img, size, shift):
 
 
 def encode(img, params: Params, allowed_modes=(1, 0, 1, 0), adaptive_density=False, nthreads=0,
-           residual_adaptive=False, residual_qstep=0.0, method="exhaustive"):
+           residual_adaptive=False, residual_qstep=0.0, method="exhaustive", rd_candidates=1):
     """encode_image_with_search with ExhaustiveSearch (or the Fisher provider):
     (header, leaves, residuals, search_evals, warmup_evals); `residuals` holds the levels of
     the mode-3 leaves, size*size each, in leaf order."""
     a = _u8(img)
     h, w = a.shape
     opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density), int(residual_adaptive),
-                   float(residual_qstep), METHODS[method])
+                   float(residual_qstep), METHODS[method], int(rd_candidates))
     hdr = Header()
     ptr, n = C.c_void_p(), C.c_size_t()
     rptr, rn = C.c_void_p(), C.c_size_t()
