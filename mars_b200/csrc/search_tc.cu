@@ -799,71 +799,68 @@ __device__ __forceinline__ int iso_src_rt(int k, int u, int v, int S) {
 // good one makes the filter tight from the first tile).  One warp per range: the 32 lanes
 // share each candidate's correlation (S*S terms), then each lane fits the candidates it
 // owns.
-__global__ void seed_kernel(const int32_t* __restrict__ D, LevelGeom g, const uint8_t* __restrict__ plane,
-                            int w, const uint32_t* rows, const uint32_t* cols, int nranges,
-                            RangeStats rs, DomainStats ds, FitParams fp, SeedOut* __restrict__ out) {
-    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+// One CTA of 9 warps per range block: warp nb correlates the block with domain nb of the
+// 3 x 3 positions around the co-located one (clamped to the pool) under all 8 isometries,
+// each D sample loaded once for the 8 permuted range pixels (staged in shared memory);
+// lanes 0-7 fit their isometry exactly and the CTA keeps the best of the 72 by (rms,
+// reference index).  Exact int32 sums: |r * D| * N < 255 * 1020 * 4096 < 2^31.
+template <int S>
+__global__ void __launch_bounds__(288) seed_kernel(
+    const int32_t* __restrict__ D, LevelGeom g, const uint8_t* __restrict__ plane, int w,
+    const uint32_t* rows, const uint32_t* cols, int nranges, RangeStats rs, DomainStats ds,
+    FitParams fp, SeedOut* __restrict__ out) {
+    constexpr int N = S * S;
+    __shared__ uint8_t rsm[N];
+    __shared__ double c_rms[72], c_sum[72];
+    __shared__ uint32_t c_idx[72];
+    __shared__ int32_t c_t1[72];
+    const int r = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (r >= nranges) return;
-    const int S = g.size, N = S * S;
     if (rows[r] + (uint32_t)S > (uint32_t)g.h || cols[r] + (uint32_t)S > (uint32_t)g.w) {
-        if (lane == 0) out[r] = SeedOut{INFINITY, 0.0, UINT32_MAX, 0};
+        if (threadIdx.x == 0) out[r] = SeedOut{INFINITY, 0.0, UINT32_MAX, 0};
         return;
     }
+    const uint8_t* rb = plane + (size_t)rows[r] * w + cols[r];
+    for (int t = threadIdx.x; t < N; t += blockDim.x) rsm[t] = rb[(size_t)(t / S) * w + (t % S)];
+    __syncthreads();
     const int ac = min(max(((int)rows[r] - S / 2 + g.shift / 2) / g.shift, 0), g.nrow_d - 1);
     const int bc = min(max(((int)cols[r] - S / 2 + g.shift / 2) / g.shift, 0), g.ncol_d - 1);
-    const uint8_t* rb = plane + (size_t)rows[r] * w + cols[r];
-    double best_rms = INFINITY, best_sum = 0.0;
-    uint32_t best_idx = UINT32_MAX;
-    int32_t best_t1 = 0;
-    for (int base = 0; base < 72; base += 32) {
-        // Correlations of candidates base .. base+31; lane (cand - base) keeps its own.
-        int64_t mine = 0;
-        const int ncand = min(32, 72 - base);
-        for (int ci = 0; ci < ncand; ++ci) {
-            const int cand = base + ci, k = cand & 7, nb = cand >> 3;
-            const int a = min(max(ac + nb / 3 - 1, 0), g.nrow_d - 1);
-            const int bb = min(max(bc + nb % 3 - 1, 0), g.ncol_d - 1);
-            const int32_t* db = D + (size_t)(a * g.step_c) * g.dw + bb * g.step_c;
-            int64_t part = 0;
-            for (int t = lane; t < N; t += 32) {
-                const int u = t / S, v = t % S;
-                const int src = iso_src_rt(k, u, v, S);
-                part += (int64_t)rb[(size_t)(src / S) * w + (src % S)] * db[(size_t)u * g.dw + v];
-            }
+    const int nb = warp;
+    const int a = min(max(ac + nb / 3 - 1, 0), g.nrow_d - 1);
+    const int bb = min(max(bc + nb % 3 - 1, 0), g.ncol_d - 1);
+    const int32_t* db = D + (size_t)(a * g.step_c) * g.dw + bb * g.step_c;
+    int32_t acc[8];
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
-            if (lane == ci) mine = part;
-        }
-        if (lane < ncand) {
-            const int cand = base + lane, k = cand & 7, nb = cand >> 3;
-            const int a = min(max(ac + nb / 3 - 1, 0), g.nrow_d - 1);
-            const int bb = min(max(bc + nb % 3 - 1, 0), g.ncol_d - 1);
-            const uint32_t dom = (uint32_t)(a * g.ncol_d + bb);
-            const FitResult f = fit_exact(N, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], mine, rs.t2[r], fp);
-            const uint32_t idx = dom * 8u + (uint32_t)k;
-            if (f.rms < best_rms || (f.rms == best_rms && idx < best_idx)) {
-                best_rms = f.rms;
-                best_sum = f.sum;
-                best_idx = idx;
-                best_t1 = (int32_t)mine;
-            }
-        }
+    for (int k = 0; k < 8; ++k) acc[k] = 0;
+    for (int t = lane; t < N; t += 32) {
+        const int u = t / S, v = t % S;
+        const int32_t d = db[(size_t)u * g.dw + v];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] += (int32_t)rsm[iso_src_rt(k, u, v, S)] * d;
     }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        const double orms = __shfl_xor_sync(0xffffffffu, best_rms, off);
-        const double osum = __shfl_xor_sync(0xffffffffu, best_sum, off);
-        const uint32_t oidx = __shfl_xor_sync(0xffffffffu, best_idx, off);
-        const int32_t ot1 = __shfl_xor_sync(0xffffffffu, best_t1, off);
-        if (orms < best_rms || (orms == best_rms && oidx < best_idx)) {
-            best_rms = orms;
-            best_sum = osum;
-            best_idx = oidx;
-            best_t1 = ot1;
-        }
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], off);
+    if (lane < 8) {
+        int32_t t1 = acc[0];
+#pragma unroll
+        for (int k = 1; k < 8; ++k) t1 = lane == k ? acc[k] : t1;
+        const uint32_t dom = (uint32_t)(a * g.ncol_d + bb);
+        const FitResult f = fit_exact(N, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], t1, rs.t2[r], fp);
+        c_rms[nb * 8 + lane] = f.rms;
+        c_sum[nb * 8 + lane] = f.sum;
+        c_idx[nb * 8 + lane] = dom * 8u + (uint32_t)lane;
+        c_t1[nb * 8 + lane] = t1;
     }
-    if (lane == 0) out[r] = SeedOut{best_rms, best_sum, best_idx, best_t1};
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int b = 0;
+        for (int c = 1; c < 72; ++c)
+            if (c_rms[c] < c_rms[b] || (c_rms[c] == c_rms[b] && c_idx[c] < c_idx[b])) b = c;
+        out[r] = SeedOut{c_rms[b], c_sum[b], c_idx[b], c_t1[b]};
+    }
 }
 
 // Final champion over the M-splits; its exact correlation travels with it, so only the
@@ -991,9 +988,16 @@ cudaError_t launch_build_b(int size, const uint8_t* plane, int w, int h, const u
 cudaError_t launch_seed(const int32_t* D, const LevelGeom& g, const uint8_t* plane, int w,
                         const uint32_t* rows, const uint32_t* cols, int nranges, RangeStats rs,
                         DomainStats ds, const FitParams& fp, SeedOut* out, cudaStream_t st) {
-    const long long threads = (long long)nranges * 32;
-    seed_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(D, g, plane, w, rows, cols,
-                                                                   nranges, rs, ds, fp, out);
+    if (nranges == 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)nranges;
+    switch (g.size) {
+        case 4: seed_kernel<4><<<blocks, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
+        case 8: seed_kernel<8><<<blocks, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
+        case 16: seed_kernel<16><<<blocks, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
+        case 32: seed_kernel<32><<<blocks, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
+        case 64: seed_kernel<64><<<blocks, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
