@@ -6,11 +6,14 @@ work of one encode at the 512x512 exhaustive configuration (seeds 1-8, cycled). 
 is range x domain x isometry fits per second, with evals counted exactly as the reference
 counts them (domain positions x 8 per node).
 
-  value : device time of the search kernels with the planes already in HBM (CUDA events on
-          the launching stream; L2 flushed between steps by a 256 MiB write).
-  e2e   : the same work through the public provider-factory call
-          (mars_search_table_build): pinned host plane in, the full node table back on the
-          host, timed on the host around the synchronous call.
+  value : device time of one step with the planes already in HBM: a search plan's CUDA
+          graph (contraction + every level's statistics, seed, correlation and finish
+          kernels) launched once per step, CUDA events on the launching stream around it;
+          L2 flushed between steps by a 256 MiB write.
+  e2e   : the same work through the public call a caller makes per plane,
+          mars_search_plan_run: host plane in (through pinned staging), the full node
+          table back on the host, timed on the host around the synchronous call; the
+          one-shot factory mars_search_table_build is reported beside it.
   cpu_baseline : the CPU oracle (a C++ restatement of the reference's CPU search) on a
           bounded sample of the same nodes, all host threads.
 
@@ -488,33 +491,53 @@ def run_gpu(args):
             if timers is not None:
                 timers[size][1].record(stream)
 
+    # The timed step: every level of one plane as one CUDA-graph launch of a search plan
+    # (mars_search_plan_run_device: the plane is copied device to device into the plan's
+    # input buffer, then the captured contraction + 4 levels replay).
+    plan = ctx.search_plan(W, H, params)
+    plan_launches = plan.launches
+    ev_step = evals_per_step()
+    assert plan.evals == ev_step, (plan.evals, ev_step)
     for k in range(args.warmup):
+        plan.run_device(planes[k % len(planes)].data_ptr())
         step(k)
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
 
-    per_level = {s: 0.0 for s in SIZES}
+    t_graph = 0.0
     launches0 = ctx.launches
     with ClockSampler(local) as clocks:
         for k in range(args.steps):
             flush.fill_(k & 0xFF)  # evict L2 between timed steps (outside the events)
-            timers = {s: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                      for s in SIZES}
-            step(k, timers)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.run_device(planes[k % len(planes)].data_ptr())
+            e1.record(stream)
             torch.cuda.synchronize(dev)
-            for s in SIZES:
-                per_level[s] += timers[s][0].elapsed_time(timers[s][1]) / 1e3
+            t_graph += e0.elapsed_time(e1) / 1e3
     torch.cuda.synchronize(dev)
     launches = ctx.launches - launches0
-    t_total = reduce_max(sum(per_level.values()), dist, dev)
-    ev_step = evals_per_step()
+    t_total = reduce_max(t_graph, dist, dev)
     value = ev_step * args.steps * world / t_total
+
+    # Per-level breakdown (the levels launched one by one, CUDA events around each), which
+    # also gives the dominant kernel's launch time for the roofline.
+    lvl_steps = max(3, min(args.steps, 10))
+    per_level = {s: 0.0 for s in SIZES}
+    for k in range(lvl_steps):
+        flush.fill_(k & 0xFF)
+        timers = {s: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for s in SIZES}
+        step(k, timers)
+        torch.cuda.synchronize(dev)
+        for s in SIZES:
+            per_level[s] += timers[s][0].elapsed_time(timers[s][1]) / 1e3
 
     # Roofline of the dominant kernel: the level search whose launches take longest.
     dom = max(SIZES, key=lambda s: per_level[s])
-    t_launch = per_level[dom] / args.steps
+    t_launch = per_level[dom] / lvl_steps
     ops = 2.0 * macs_of_level(dom)  # int8-equivalent MAC ops of the correlation
     peaks = {}
     try:
@@ -526,23 +549,30 @@ def run_gpu(args):
         peak_src = "2 x fallback bf16 1.59 PFLOP/s"
     achieved = ops / t_launch / 1e12
 
-    # End to end through the provider factory: pinned host plane in, table out.
-    e2e_val = None
+    # End to end through the public calls, host plane in and the node table back on the
+    # host: the plan's run (what a caller encoding many planes of one size makes per plane)
+    # and, beside it, the one-shot provider factory (plan and buffers built per call).
+    e2e_val = e2e_factory = None
     h2d = d2h = 0
-    pinned = [torch.from_numpy(synthetic.gray(W, H, s)).pin_memory() for s in seeds]
+    host_planes = [synthetic.gray(W, H, s) for s in seeds]
     nodes = sum((H // s) * (W // s) for s in SIZES)
     if rank == 0 or world > 1:
-        e2e_steps = max(1, min(args.steps, 5))
+        e2e_steps = max(3, min(args.steps, 10))
         for k in range(min(2, args.warmup)):
-            ctx.search_provider(pinned[k % len(pinned)].numpy(), params).close()
+            plan.run(host_planes[k % len(host_planes)]).close()
+            ctx.search_provider(host_planes[k % len(host_planes)], params).close()
         t0 = time.perf_counter()
         for k in range(e2e_steps):
-            prov = ctx.search_provider(pinned[k % len(pinned)].numpy(), params)
-            prov.close()
+            plan.run(host_planes[k % len(host_planes)]).close()
         t_e2e = time.perf_counter() - t0
         e2e_val = ev_step * e2e_steps * world / t_e2e
-        h2d = W * H + nodes * 8
+        t0 = time.perf_counter()
+        for k in range(e2e_steps):
+            ctx.search_provider(host_planes[k % len(host_planes)], params).close()
+        e2e_factory = ev_step * e2e_steps * world / (time.perf_counter() - t0)
+        h2d = W * H
         d2h = nodes * 80 + 8
+    plan.close()
 
     decode = decode_large = None
     if not args.no_decode:
@@ -578,10 +608,14 @@ def run_gpu(args):
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum",
                          "peak_source": peak_src,
                          "ops_per_launch": ops, "launch_ms": 1e3 * t_launch},
-            "per_level_ms": {str(s): 1e3 * per_level[s] / args.steps for s in SIZES},
+            "per_level_ms": {str(s): 1e3 * per_level[s] / lvl_steps for s in SIZES},
+            "launch": "one CUDA-graph launch per step (search plan), "
+                      f"{plan_launches} kernel nodes",
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "call": "mars_search_plan_run",
+                    "factory_value": e2e_factory,
+                    "factory_call": "mars_search_table_build (node lists and scratch per call)"},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "decode": decode,

@@ -115,6 +115,7 @@ typedef struct mars_counters {
 typedef struct mars_ctx mars_ctx;
 typedef struct mars_table mars_table;
 typedef struct mars_decode_plan mars_decode_plan;
+typedef struct mars_search_plan mars_search_plan;
 
 const char* mars_last_error(void);
 const char* mars_version(void);
@@ -165,6 +166,25 @@ uint64_t mars_search_table_evals(const mars_table* table);
  * (instrumentation). */
 uint64_t mars_search_table_exact_fits(const mars_table* table);
 void mars_search_table_free(mars_table* table);
+
+/* Search plans: the provider factory for repeated planes of one geometry.  Creation plans
+ * every node an encode can request (as mars_search_table_build without adaptive density),
+ * uploads the node lists, keeps the device buffers and captures the whole search -- the
+ * contraction and every quadtree level's statistics, seed, correlation and finish
+ * kernels -- into one CUDA graph; each run is one graph launch.
+ *   mars_search_plan_run: host plane in (copied through pinned staging), table out;
+ *   mars_search_plan_run_device: device plane in, asynchronous on the context's stream,
+ *     results kept on the device until mars_search_plan_table fetches them.
+ * Tables from a plan answer mars_search_table_lookup like any other and may outlive it. */
+int mars_search_plan_create(mars_ctx* ctx, uint32_t width, uint32_t height,
+                            const mars_params* params, mars_search_plan** out);
+int mars_search_plan_run(mars_search_plan* plan, const uint8_t* plane, mars_table** out);
+int mars_search_plan_run_device(mars_search_plan* plan, const uint8_t* d_plane);
+int mars_search_plan_table(mars_search_plan* plan, mars_table** out);
+uint64_t mars_search_plan_evals(const mars_search_plan* plan);
+/* Kernel launches one run replays (the graph's kernel nodes). */
+uint64_t mars_search_plan_launches(const mars_search_plan* plan);
+void mars_search_plan_free(mars_search_plan* plan);
 
 /* IndexedSearchProvider::build (crates/mars-search/src/lib.rs:480-513) for `method`: the
  * per-size domain indexes (plus the doubled-stride ones when adaptive_density and a

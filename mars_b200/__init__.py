@@ -94,6 +94,9 @@ EXPORTS = (
     "mars_residuals_free", "mars_indexed_table_build", "mars_ycbcr_device",
     "mars_rgb_from_ycbcr_device", "mars_downsample_box_device", "mars_upsample_nearest_device",
     "mars_mse_device", "mars_search_table_build_ranked", "mars_search_table_lookup_ranked",
+    "mars_search_plan_create", "mars_search_plan_run", "mars_search_plan_run_device",
+    "mars_search_plan_table", "mars_search_plan_evals", "mars_search_plan_launches",
+    "mars_search_plan_free",
     "mars_refine_plan_create", "mars_refine_params", "mars_refine_forward",
     "mars_refine_backward", "mars_refine_run", "mars_refine_plan_free",
 )
@@ -127,6 +130,16 @@ def lib():
     L.mars_indexed_table_build.argtypes = [vp, vp, u32, u32, P(Params), C.c_int32, C.c_int32,
                                            P(vp)]
     L.mars_search_table_lookup.argtypes = [vp, u32, u32, u32, u32, vp, P(u64)]
+    L.mars_search_plan_create.argtypes = [vp, u32, u32, P(Params), P(vp)]
+    L.mars_search_plan_run.argtypes = [vp, vp, P(vp)]
+    L.mars_search_plan_run_device.argtypes = [vp, vp]
+    L.mars_search_plan_table.argtypes = [vp, P(vp)]
+    L.mars_search_plan_evals.argtypes = [vp]
+    L.mars_search_plan_evals.restype = u64
+    L.mars_search_plan_launches.argtypes = [vp]
+    L.mars_search_plan_launches.restype = u64
+    L.mars_search_plan_free.argtypes = [vp]
+    L.mars_search_plan_free.restype = None
     L.mars_search_table_build_ranked.argtypes = [vp, vp, u32, u32, P(Params), C.c_int32, u32, P(vp)]
     L.mars_search_table_lookup_ranked.argtypes = [vp, u32, u32, u32, u32, u32, vp, P(u32), P(u64)]
     L.mars_search_table_evals.argtypes = [vp]
@@ -339,6 +352,12 @@ class Context:
                                                  C.byref(t)))
         return GpuSearch(self, t.value, w, h)
 
+    def search_plan(self, width: int, height: int, params: Params) -> "SearchPlan":
+        """A graph-captured provider factory for repeated planes of one geometry."""
+        h = C.c_void_p()
+        check(lib().mars_search_plan_create(self._h, width, height, C.byref(params), C.byref(h)))
+        return SearchPlan(self, h.value, width, height)
+
     def search_blocks(self, img, size: int, shift: int, params: Params, rows, cols):
         """search_block for each (rows[i], cols[i]): (candidates, evals) arrays."""
         a = _plane(img)
@@ -488,6 +507,50 @@ class DecodePlan:
     def close(self) -> None:
         if self._h:
             lib().mars_decode_plan_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SearchPlan:
+    """mars_search_plan_*: every level of one plane's search as one CUDA-graph launch."""
+
+    def __init__(self, ctx: "Context", handle: int, width: int, height: int):
+        self._ctx = ctx
+        self._h = C.c_void_p(handle)
+        self.width, self.height = width, height
+
+    @property
+    def evals(self) -> int:
+        return lib().mars_search_plan_evals(self._h)
+
+    @property
+    def launches(self) -> int:
+        return lib().mars_search_plan_launches(self._h)
+
+    def run(self, img) -> GpuSearch:
+        a = _plane(img)
+        if a.shape != (self.height, self.width):
+            raise ValueError("plane shape differs from the plan's")
+        t = C.c_void_p()
+        check(lib().mars_search_plan_run(self._h, a.ctypes.data, C.byref(t)))
+        return GpuSearch(self._ctx, t.value, self.width, self.height)
+
+    def run_device(self, d_plane_ptr: int) -> None:
+        check(lib().mars_search_plan_run_device(self._h, C.c_void_p(d_plane_ptr)))
+
+    def table(self) -> GpuSearch:
+        t = C.c_void_p()
+        check(lib().mars_search_plan_table(self._h, C.byref(t)))
+        return GpuSearch(self._ctx, t.value, self.width, self.height)
+
+    def close(self) -> None:
+        if self._h:
+            lib().mars_search_plan_free(self._h)
             self._h = C.c_void_p(None)
 
     def __del__(self):

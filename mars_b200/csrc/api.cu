@@ -54,6 +54,11 @@ struct mars_table {
     uint32_t width = 0, height = 0;
     uint32_t k = 1;  // ranked candidates per node (cands holds the first of each)
     std::unordered_map<uint64_t, uint32_t> index;
+    // A search plan's tables share the plan's node index instead of owning one.
+    std::shared_ptr<const std::unordered_map<uint64_t, uint32_t>> shared_index;
+    const std::unordered_map<uint64_t, uint32_t>& nodes() const {
+        return shared_index ? *shared_index : index;
+    }
     std::vector<mars_candidate> cands;
     std::vector<mars_candidate> ranked;  // k per node, when k > 1
     std::vector<uint64_t> evals;
@@ -367,14 +372,8 @@ uint64_t level_evals(uint32_t w, uint32_t h, uint32_t size, uint32_t shift) {
 }
 
 // Runs all jobs on the device plane; results land in d_out (concatenated in job order).
-int run_jobs(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uint32_t h,
-             const mars::FitParams& fp, const std::vector<Job>& jobs, mars::CandidateOut* d_out,
-             uint32_t k = 1) {
-    const cudaStream_t st = ctx->stream;
-    int32_t* d_D = nullptr;
-    MARS_CUDA(sc.get(&d_D, (size_t)(w / 2) * (h / 2)));
-    MARS_CUDA(mars::launch_contract(d_plane, (int)w, (int)h, d_D, st));
-    ctx->launches += 1;
+// The jobs' node origins as one list: all rows, then all columns, in job order.
+std::vector<uint32_t> job_origins(const std::vector<Job>& jobs, size_t* total_out) {
     size_t total = 0;
     for (const Job& j : jobs) total += j.rows.size();
     std::vector<uint32_t> rc(2 * total);
@@ -384,10 +383,32 @@ int run_jobs(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uin
         std::copy(j.cols.begin(), j.cols.end(), rc.begin() + (long)(total + off));
         off += j.rows.size();
     }
-    uint32_t* d_rc = nullptr;
-    MARS_CUDA(sc.get(&d_rc, rc.size()));
-    MARS_CUDA(cudaMemcpyAsync(d_rc, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice, st));
-    off = 0;
+    *total_out = total;
+    return rc;
+}
+
+// `d_rc_in`: the job origins already on the device (job_origins layout), else uploaded here.
+int run_jobs(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uint32_t h,
+             const mars::FitParams& fp, const std::vector<Job>& jobs, mars::CandidateOut* d_out,
+             uint32_t k = 1, const uint32_t* d_rc_in = nullptr) {
+    const cudaStream_t st = ctx->stream;
+    int32_t* d_D = nullptr;
+    MARS_CUDA(sc.get(&d_D, std::max<size_t>(1, (size_t)(w / 2) * (h / 2))));
+    MARS_CUDA(mars::launch_contract(d_plane, (int)w, (int)h, d_D, st));
+    ctx->launches += 1;
+    size_t total = 0;
+    const uint32_t* d_rc = d_rc_in;
+    if (!d_rc) {
+        const std::vector<uint32_t> rc = job_origins(jobs, &total);
+        uint32_t* d = nullptr;
+        MARS_CUDA(sc.get(&d, rc.size()));
+        // A pageable source: the call returns once the bytes are staged, so `rc` may go.
+        MARS_CUDA(cudaMemcpyAsync(d, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice, st));
+        d_rc = d;
+    } else {
+        for (const Job& j : jobs) total += j.rows.size();
+    }
+    size_t off = 0;
     for (const Job& j : jobs) {
         const int e = run_level(ctx, sc, d_plane, d_D, w, h, j.size, j.shift, fp, d_rc + off,
                                 d_rc + total + off, j.rows.size(), d_out + off * k, k);
@@ -633,8 +654,8 @@ int mars_indexed_table_build(mars_ctx* ctx, const uint8_t* plane, uint32_t width
 int mars_search_table_lookup(const mars_table* t, uint32_t row, uint32_t col, uint32_t size,
                              uint32_t shift, mars_candidate* out, uint64_t* evals) {
     if (!t || !out) return fail(MARS_EINVAL, "NULL argument");
-    auto it = t->index.find(node_key(row, col, size, shift));
-    if (it == t->index.end())
+    auto it = t->nodes().find(node_key(row, col, size, shift));
+    if (it == t->nodes().end())
         return fail(MARS_ENOTFOUND, "node (" + std::to_string(row) + "," + std::to_string(col) +
                                         "," + std::to_string(size) + ") at shift " +
                                         std::to_string(shift) + " is not in the table");
@@ -655,8 +676,8 @@ int mars_search_table_lookup_ranked(const mars_table* t, uint32_t row, uint32_t 
                                     uint32_t size, uint32_t shift, uint32_t max,
                                     mars_candidate* out, uint32_t* count, uint64_t* evals) {
     if (!t || !count || (max && !out)) return fail(MARS_EINVAL, "NULL argument");
-    auto it = t->index.find(node_key(row, col, size, shift));
-    if (it == t->index.end())
+    auto it = t->nodes().find(node_key(row, col, size, shift));
+    if (it == t->nodes().end())
         return fail(MARS_ENOTFOUND, "node (" + std::to_string(row) + "," + std::to_string(col) +
                                         "," + std::to_string(size) + ") at shift " +
                                         std::to_string(shift) + " is not in the table");
@@ -829,6 +850,219 @@ int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t he
     }
     if (!res.empty()) std::memcpy(*residuals, res.data(), res.size() * sizeof(int32_t));
     return MARS_OK;
+}
+
+// ---------------------------------------------------------------- search plans
+//
+// A plan fixes one plane geometry and parameter set: the node lists are uploaded once, the
+// device buffers stay allocated, and the whole search -- contraction and every quadtree
+// level, each level's statistics, seed, correlation and finish kernels -- is captured once
+// into a CUDA graph (the levels' scratch as graph memory nodes, so their addresses and the
+// tensor maps built on them hold for every replay).  A run is one graph launch.
+
+}  // extern "C"
+
+struct mars_search_plan {
+    mars_ctx* ctx = nullptr;
+    uint32_t w = 0, h = 0;
+    mars_params params{};
+    std::vector<Job> jobs;
+    size_t total = 0;
+    uint32_t* d_rc = nullptr;
+    uint8_t* d_plane = nullptr;
+    mars::CandidateOut* d_out = nullptr;
+    uint8_t* h_plane = nullptr;        // pinned staging of the input plane
+    mars_candidate* h_out = nullptr;   // pinned staging of the node table
+    unsigned long long* h_exact = nullptr;
+    cudaGraph_t g_host = nullptr, g_dev = nullptr;
+    cudaGraphExec_t x_host = nullptr, x_dev = nullptr;
+    uint64_t launches_per_run = 0;
+    std::vector<uint64_t> evals;
+    uint64_t total_evals = 0;
+    std::shared_ptr<const std::unordered_map<uint64_t, uint32_t>> index;
+};
+
+namespace {
+
+void plan_release(mars_search_plan* p) {
+    if (!p) return;
+    if (p->x_host) cudaGraphExecDestroy(p->x_host);
+    if (p->x_dev) cudaGraphExecDestroy(p->x_dev);
+    if (p->g_host) cudaGraphDestroy(p->g_host);
+    if (p->g_dev) cudaGraphDestroy(p->g_dev);
+    cudaFree(p->d_rc);
+    cudaFree(p->d_plane);
+    cudaFree(p->d_out);
+    cudaFreeHost(p->h_plane);
+    cudaFreeHost(p->h_out);
+    cudaFreeHost(p->h_exact);
+    delete p;
+}
+
+// The plan's device work on the context's stream: with_copies adds the pinned input
+// upload and the table / counter downloads around it.
+int plan_enqueue(mars_search_plan* p, bool with_copies) {
+    mars_ctx* ctx = p->ctx;
+    const cudaStream_t st = ctx->stream;
+    Scratch sc(st);
+    if (with_copies)
+        MARS_CUDA(cudaMemcpyAsync(p->d_plane, p->h_plane, (size_t)p->w * p->h,
+                                  cudaMemcpyHostToDevice, st));
+    MARS_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), st));
+    const mars::FitParams fp = make_fit_params(p->params);
+    if (int e = run_jobs(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out, 1, p->d_rc))
+        return e;
+    if (with_copies) {
+        MARS_CUDA(cudaMemcpyAsync(p->h_out, p->d_out, p->total * sizeof(mars_candidate),
+                                  cudaMemcpyDeviceToHost, st));
+        MARS_CUDA(cudaMemcpyAsync(p->h_exact, ctx->d_counter, sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, st));
+    }
+    return MARS_OK;
+}
+
+int plan_capture(mars_search_plan* p, bool with_copies, cudaGraph_t* g, cudaGraphExec_t* x) {
+    const cudaStream_t st = p->ctx->stream;
+    MARS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const uint64_t l0 = p->ctx->launches.load();
+    const int err = plan_enqueue(p, with_copies);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (err || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return err ? err : fail(MARS_ECUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    }
+    p->launches_per_run = p->ctx->launches.load() - l0;
+    p->ctx->launches -= p->launches_per_run;  // captured, not launched
+    const cudaError_t ie = cudaGraphInstantiate(x, graph, 0);
+    if (ie != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(MARS_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    }
+    *g = graph;
+    return MARS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mars_search_plan_create(mars_ctx* ctx, uint32_t width, uint32_t height,
+                            const mars_params* params, mars_search_plan** out) {
+    if (!ctx || !params || !out) return fail(MARS_EINVAL, "NULL argument");
+    if (int e = check_params(params)) return e;
+    if (width == 0 || height == 0 || width > 65535 || height > 65535)
+        return fail(MARS_EINVAL, "plane dimensions must be in 1..65535");
+    std::unique_ptr<mars_search_plan, void (*)(mars_search_plan*)> p(new (std::nothrow)
+                                                                         mars_search_plan,
+                                                                     plan_release);
+    if (!p) return fail(MARS_ENOMEM, "plan allocation failed");
+    p->ctx = ctx;
+    p->w = width;
+    p->h = height;
+    p->params = *params;
+    p->jobs = plan_jobs(nullptr, width, height, *params, false);
+    const std::vector<uint32_t> rc = job_origins(p->jobs, &p->total);
+    if (p->total > 0xffffffffull) return fail(MARS_EINVAL, "too many quadtree nodes");
+    auto index = std::make_shared<std::unordered_map<uint64_t, uint32_t>>();
+    index->reserve(p->total * 2);
+    p->evals.resize(p->total);
+    size_t off = 0;
+    for (const Job& j : p->jobs) {
+        const uint64_t ev = level_evals(width, height, j.size, j.shift);
+        for (size_t i = 0; i < j.rows.size(); ++i) {
+            (*index)[node_key(j.rows[i], j.cols[i], j.size, j.shift)] = (uint32_t)(off + i);
+            p->evals[off + i] = ev;
+            p->total_evals += ev;
+        }
+        off += j.rows.size();
+    }
+    p->index = index;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    MARS_CUDA(cudaMalloc(&p->d_rc, std::max<size_t>(1, rc.size()) * 4));
+    MARS_CUDA(cudaMalloc(&p->d_plane, (size_t)width * height));
+    MARS_CUDA(cudaMalloc(&p->d_out, std::max<size_t>(1, p->total) * sizeof(mars::CandidateOut)));
+    MARS_CUDA(cudaMallocHost(&p->h_plane, (size_t)width * height));
+    MARS_CUDA(cudaMallocHost(&p->h_out, std::max<size_t>(1, p->total) * sizeof(mars_candidate)));
+    MARS_CUDA(cudaMallocHost(&p->h_exact, sizeof(unsigned long long)));
+    if (!rc.empty())
+        MARS_CUDA(cudaMemcpyAsync(p->d_rc, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    MARS_CUDA(cudaMemsetAsync(p->d_plane, 0, (size_t)width * height, ctx->stream));
+    // One ordinary run first: it sets every kernel's attributes outside the capture and
+    // checks the plan end to end.
+    if (int e = plan_enqueue(p.get(), false)) return e;
+    if (int e = sync_bounded(ctx)) return e;
+    if (int e = plan_capture(p.get(), true, &p->g_host, &p->x_host)) return e;
+    if (int e = plan_capture(p.get(), false, &p->g_dev, &p->x_dev)) return e;
+    *out = p.release();
+    return MARS_OK;
+}
+
+int mars_search_plan_run(mars_search_plan* p, const uint8_t* plane, mars_table** out) {
+    if (!p || !plane || !out) return fail(MARS_EINVAL, "NULL argument");
+    mars_ctx* ctx = p->ctx;
+    std::unique_ptr<mars_table> t(new (std::nothrow) mars_table);
+    if (!t) return fail(MARS_ENOMEM, "table allocation failed");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    std::memcpy(p->h_plane, plane, (size_t)p->w * p->h);
+    MARS_CUDA(cudaGraphLaunch(p->x_host, ctx->stream));
+    ctx->launches += p->launches_per_run;
+    if (int e = sync_bounded(ctx)) return e;
+    t->width = p->w;
+    t->height = p->h;
+    t->cands.assign(p->h_out, p->h_out + p->total);
+    t->evals = p->evals;
+    t->total_evals = p->total_evals;
+    t->exact_fits = *p->h_exact;
+    t->shared_index = p->index;
+    *out = t.release();
+    return MARS_OK;
+}
+
+int mars_search_plan_run_device(mars_search_plan* p, const uint8_t* d_plane) {
+    if (!p || !d_plane) return fail(MARS_EINVAL, "NULL argument");
+    mars_ctx* ctx = p->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    if (d_plane != p->d_plane)
+        MARS_CUDA(cudaMemcpyAsync(p->d_plane, d_plane, (size_t)p->w * p->h,
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
+    MARS_CUDA(cudaGraphLaunch(p->x_dev, ctx->stream));
+    ctx->launches += p->launches_per_run;
+    return MARS_OK;
+}
+
+int mars_search_plan_table(mars_search_plan* p, mars_table** out) {
+    if (!p || !out) return fail(MARS_EINVAL, "NULL argument");
+    mars_ctx* ctx = p->ctx;
+    std::unique_ptr<mars_table> t(new (std::nothrow) mars_table);
+    if (!t) return fail(MARS_ENOMEM, "table allocation failed");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    MARS_CUDA(cudaMemcpyAsync(p->h_out, p->d_out, p->total * sizeof(mars_candidate),
+                              cudaMemcpyDeviceToHost, ctx->stream));
+    if (int e = sync_bounded(ctx)) return e;
+    t->width = p->w;
+    t->height = p->h;
+    t->cands.assign(p->h_out, p->h_out + p->total);
+    t->evals = p->evals;
+    t->total_evals = p->total_evals;
+    t->shared_index = p->index;
+    *out = t.release();
+    return MARS_OK;
+}
+
+uint64_t mars_search_plan_evals(const mars_search_plan* p) { return p ? p->total_evals : 0; }
+uint64_t mars_search_plan_launches(const mars_search_plan* p) { return p ? p->launches_per_run : 0; }
+
+void mars_search_plan_free(mars_search_plan* p) {
+    if (!p) return;
+    cudaSetDevice(p->ctx->device);
+    cudaStreamSynchronize(p->ctx->stream);
+    plan_release(p);
 }
 
 void mars_leaves_free(mars_leaf* leaves) { std::free(leaves); }
