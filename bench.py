@@ -294,7 +294,7 @@ REFINE_STEPS = 20
 REFINE_DECODE_ITERS = 12
 
 
-def run_refine(mb, ctx, stream, dev, peaks):
+def run_refine(mb, ctx, stream, dev, peaks, seeds=REFINE_SEEDS, lambdas=REFINE_LAMBDAS):
     """Attractor refinement at 512x512: per seed 1-8 and lambda 50..800, the GPU RD encode
     (modes 0-3, block sizes 32..4, domain stride 2) and its refinement (20 steps); PSNR-Y of
     the exact 12-iteration decodes against the bytes of the .mars streams.  The gain is the
@@ -309,12 +309,12 @@ def run_refine(mb, ctx, stream, dev, peaks):
         mse = np.mean((a.astype(np.float64) - b.astype(np.float64)) ** 2)
         return 10.0 * np.log10(255.0 ** 2 / mse)
 
-    per_seed, gains, enc_t, ref_t, accepted = [], {l: [] for l in REFINE_LAMBDAS}, [], [], 0
+    per_seed, gains, enc_t, ref_t, accepted = [], {l: [] for l in lambdas}, [], [], 0
     bytes_ratio = []
-    for seed in REFINE_SEEDS:
+    for seed in seeds:
         img = synthetic.gray(W, H, seed)
         plain, refined = [], []
-        for lam in REFINE_LAMBDAS:
+        for lam in lambdas:
             params = mb.make_params(min_size=4, max_size=32, shift=SHIFT, lam=lam)
             t0 = time.perf_counter()
             hdr, leaves, res, _ = ctx.encode(img, params, allowed_modes=(1, 1, 1, 1))
@@ -333,11 +333,13 @@ def run_refine(mb, ctx, stream, dev, peaks):
             refined.append((rd.bpp(b1, W, H), p1))
             gains[lam].append(p1 - p0)
             bytes_ratio.append(b1 / b0)
-        r = rd.bd_metrics(plain, refined, ("plain", "refined"))
-        per_seed.append({"seed": seed, "bd_psnr_db": r.bd_psnr_db, "bd_rate_pct": r.bd_rate_pct,
-                         "bpp_interval": r.bd_psnr_bpp_interval,
-                         "plain": plain, "refined": refined})
-    bd = float(np.mean([p["bd_psnr_db"] for p in per_seed]))
+        if len(lambdas) >= rd.MIN_POINTS_PER_CURVE:
+            r = rd.bd_metrics(plain, refined, ("plain", "refined"))
+            per_seed.append({"seed": seed, "bd_psnr_db": r.bd_psnr_db,
+                             "bd_rate_pct": r.bd_rate_pct, "bpp_interval": r.bd_psnr_bpp_interval,
+                             "plain": plain, "refined": refined})
+    # BD metrics need at least 4 points per curve; shorter sweeps report per-lambda gains only.
+    bd = float(np.mean([p["bd_psnr_db"] for p in per_seed])) if per_seed else None
 
     # Per-iteration cost of the two solves on one plan (fixed iteration counts).
     img = synthetic.gray(W, H, 1)
@@ -364,7 +366,7 @@ def run_refine(mb, ctx, stream, dev, peaks):
         "value": bd, "unit": "dB", "higher_is_better": True,
         "per_lambda_gain_db": {str(int(l)): float(np.mean(g)) for l, g in gains.items()},
         "bytes_ratio_refined_over_plain": [float(min(bytes_ratio)), float(max(bytes_ratio))],
-        "accepted": f"{accepted}/{len(REFINE_SEEDS) * len(REFINE_LAMBDAS)}",
+        "accepted": f"{accepted}/{len(seeds) * len(lambdas)}",
         "per_seed": [{k: v for k, v in p.items() if k in ("seed", "bd_psnr_db", "bd_rate_pct")}
                      for p in per_seed],
         "ms_per_refine": 1e3 * float(np.median(ref_t)),
@@ -641,9 +643,29 @@ def main():
     ap.add_argument("--no-decode", action="store_true", help="skip the decode leg")
     ap.add_argument("--no-refine", action="store_true", help="skip the refinement leg")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
+    ap.add_argument("--refine-only", action="store_true",
+                    help="run only the refinement leg (for profiling), on --refine-seeds and "
+                         "--refine-lambdas, and print its JSON object")
+    ap.add_argument("--refine-seeds", default=",".join(map(str, REFINE_SEEDS)))
+    ap.add_argument("--refine-lambdas", default=",".join(str(int(l)) for l in REFINE_LAMBDAS))
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.refine_only:
+        import torch
+        import mars_b200 as mb
+        torch.cuda.set_device(0)
+        dev = torch.device("cuda", 0)
+        stream = torch.cuda.Stream(dev)
+        torch.cuda.set_stream(stream)
+        ctx = mb.Context(0)
+        ctx.set_stream(stream.cuda_stream)
+        out = run_refine(mb, ctx, stream, dev, {},
+                         tuple(int(x) for x in args.refine_seeds.split(",")),
+                         tuple(float(x) for x in args.refine_lambdas.split(",")))
+        print(json.dumps({"refine": out}), flush=True)
+        ctx.close()
+        return 0
     return run_gpu(args)
 
 
