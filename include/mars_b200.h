@@ -265,6 +265,25 @@ int mars_decode_plan_create(mars_ctx* ctx, const mars_header* header, const mars
 int mars_decode_plan_run(mars_decode_plan* plan, uint32_t iterations, uint8_t* d_out);
 void mars_decode_plan_free(mars_decode_plan* plan);
 
+/* decode_until_stable (crates/mars-codec/src/ifs.rs:321-353): steps from the flat-128
+ * seed until the largest per-pixel change of a step is <= threshold, at most
+ * max_iterations (>= 1) steps; *iterations_used is the number run.  The steps are queued
+ * ahead on the device (a step after convergence is a no-op), so the host waits once. */
+int mars_decode_until_stable(mars_ctx* ctx, const mars_header* header, const mars_leaf* leaves,
+                             size_t n, const int32_t* residuals, size_t nresiduals,
+                             uint8_t threshold, uint32_t max_iterations, uint8_t* out,
+                             uint32_t* iterations_used);
+int mars_decode_plan_run_until_stable(mars_decode_plan* plan, uint8_t threshold,
+                                      uint32_t max_iterations, uint8_t* d_out,
+                                      uint32_t* iterations_used);
+/* zoom_leaves (ifs.rs:356-392): the leaf list and canvas scaled by `factor` (positions,
+ * sizes (at least 1) and domain origins rounded half away from zero; affine gradients
+ * divided by it), so the same contractive map decodes at another resolution.  Residuals
+ * are dropped at any factor but 1: a mode-3 leaf comes back as mode 2, which decodes
+ * exactly as the reference's mode-3 leaf without a residual.  out_leaves holds n leaves. */
+int mars_zoom_leaves(const mars_header* header, const mars_leaf* leaves, size_t n,
+                     double factor, mars_header* out_header, mars_leaf* out_leaves);
+
 /* Attractor refinement (no reference counterpart: the reference fits each leaf to the
  * collage error only).  The decode map of decode_leaf (crates/mars-codec/src/ifs.rs:406-484)
  * is read as a continuous map of the plane, x_p = s_L * d_p(x) + o_L (+ the mode-3 residual),

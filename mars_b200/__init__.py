@@ -96,7 +96,8 @@ EXPORTS = (
     "mars_mse_device", "mars_search_table_build_ranked", "mars_search_table_lookup_ranked",
     "mars_search_plan_create", "mars_search_plan_run", "mars_search_plan_run_device",
     "mars_search_plan_table", "mars_search_plan_evals", "mars_search_plan_launches",
-    "mars_search_plan_free",
+    "mars_search_plan_free", "mars_decode_until_stable", "mars_decode_plan_run_until_stable",
+    "mars_zoom_leaves",
     "mars_refine_plan_create", "mars_refine_params", "mars_refine_forward",
     "mars_refine_backward", "mars_refine_run", "mars_refine_plan_free",
 )
@@ -130,6 +131,10 @@ def lib():
     L.mars_indexed_table_build.argtypes = [vp, vp, u32, u32, P(Params), C.c_int32, C.c_int32,
                                            P(vp)]
     L.mars_search_table_lookup.argtypes = [vp, u32, u32, u32, u32, vp, P(u64)]
+    L.mars_decode_until_stable.argtypes = [vp, P(Header), vp, sz, vp, sz, C.c_uint8, u32, vp,
+                                            P(u32)]
+    L.mars_decode_plan_run_until_stable.argtypes = [vp, C.c_uint8, u32, vp, P(u32)]
+    L.mars_zoom_leaves.argtypes = [P(Header), vp, sz, C.c_double, P(Header), vp]
     L.mars_search_plan_create.argtypes = [vp, u32, u32, P(Params), P(vp)]
     L.mars_search_plan_run.argtypes = [vp, vp, P(vp)]
     L.mars_search_plan_run_device.argtypes = [vp, vp]
@@ -480,6 +485,18 @@ class Context:
                                             t.ctypes.data, C.byref(h)))
         return RefinePlan(h.value, leaves, hdr)
 
+    def decode_until_stable(self, hdr: Header, leaves: np.ndarray, threshold: int,
+                            max_iterations: int, residuals=None):
+        """decode_until_stable (ifs.rs:321-353): (plane, iterations used)."""
+        leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+        res = _residuals(residuals)
+        out = np.zeros((hdr.height, hdr.width), dtype=np.uint8)
+        used = C.c_uint32()
+        check(lib().mars_decode_until_stable(self._h, C.byref(hdr), leaves.ctypes.data,
+                                             len(leaves), res.ctypes.data, len(res), threshold,
+                                             max_iterations, out.ctypes.data, C.byref(used)))
+        return out, used.value
+
     def decode(self, hdr: Header, leaves: np.ndarray, iterations: int = 10,
                residuals=None) -> np.ndarray:
         leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
@@ -613,6 +630,17 @@ class RefinePlan:
             self.close()
         except Exception:
             pass
+
+
+def zoom_leaves(hdr: Header, leaves: np.ndarray, factor: float):
+    """zoom_leaves (ifs.rs:356-392): (zoomed header, zoomed leaves); mode-3 leaves come back
+    as mode 2 at any factor but 1 (their residual is dropped)."""
+    leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    out = np.zeros(len(leaves), dtype=LEAF_DTYPE)
+    h2 = Header()
+    check(lib().mars_zoom_leaves(C.byref(hdr), leaves.ctypes.data, len(leaves), factor,
+                                 C.byref(h2), out.ctypes.data))
+    return h2, out
 
 
 def ifs_parse(data: bytes):

@@ -15,7 +15,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import (Context, Params, format_read, format_write)
+from . import (Context, Params, format_read, format_write, zoom_leaves)
 
 COLOR_MAGIC = b"MARC"
 COLOR_VERSION = 0
@@ -104,6 +104,52 @@ def encode_color(ctx: Context, image: np.ndarray, p: ColorEncodeParams):
     stats.y_bytes, stats.cb_bytes, stats.cr_bytes = len(yb), len(cbb), len(crb)
     stats.planes = {"y": y, "cb": cb, "cr": cr}
     return write_container(mode, [yb, cbb, crb]), stats
+
+
+def _decode_planes(ctx: Context, data: bytes, iterations: int, zoom: float, threshold):
+    mode, streams = read_container(data)
+    planes, used = [], 0
+    for s in streams:
+        hdr, leaves, res = format_read(s)
+        if zoom != 1.0:
+            hdr, leaves = zoom_leaves(hdr, leaves, zoom)
+            res = None  # zoom_leaves drops the residuals (its mode-3 leaves became mode 2)
+        if threshold is None:
+            planes.append(ctx.decode(hdr, leaves, iterations, res))
+            used = iterations
+        else:
+            plane, n = ctx.decode_until_stable(hdr, leaves, threshold, iterations, res)
+            planes.append(plane)
+            used = max(used, n)
+    return mode, planes, used
+
+
+def _assemble(ctx: Context, mode: int, planes):
+    if mode == MODE_GRAY:
+        return planes[0]
+    if mode not in (MODE_RGB_444, MODE_RGB_420) or len(planes) != 3:
+        raise ValueError(f"unknown mode {mode}")
+    y, cb, cr = planes
+    h, w = y.shape
+    if mode == MODE_RGB_420:
+        cb, cr = ctx.upsample_nearest(cb, w, h), ctx.upsample_nearest(cr, w, h)
+    r, g, b = ctx.rgb_from_ycbcr(y, cb, cr)
+    return np.stack([r, g, b], axis=-1)
+
+
+def decode_color_zoomed(ctx: Context, data: bytes, iterations: int, zoom: float) -> np.ndarray:
+    """decode_color_image_zoomed (color.rs:530-573): every plane's leaves zoomed
+    (zoom_leaves) before the decode."""
+    mode, planes, _ = _decode_planes(ctx, data, iterations, zoom, None)
+    return _assemble(ctx, mode, planes)
+
+
+def decode_color_auto(ctx: Context, data: bytes, threshold: int, max_iterations: int,
+                      zoom: float = 1.0):
+    """decode_color_image_auto (color.rs:575-629): each plane decoded until stable; returns
+    (image, the largest plane's iteration count)."""
+    mode, planes, used = _decode_planes(ctx, data, max_iterations, zoom, threshold)
+    return _assemble(ctx, mode, planes), used
 
 
 def decode_color(ctx: Context, data: bytes, iterations: int = 10) -> np.ndarray:

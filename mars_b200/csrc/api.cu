@@ -1302,6 +1302,111 @@ int mars_decode_plan_run(mars_decode_plan* p, uint32_t iterations, uint8_t* d_ou
     return MARS_OK;
 }
 
+int mars_decode_plan_run_until_stable(mars_decode_plan* p, uint8_t threshold,
+                                      uint32_t max_iterations, uint8_t* d_out,
+                                      uint32_t* iterations_used) {
+    if (!p || !d_out || !iterations_used) return fail(MARS_EINVAL, "NULL argument");
+    const uint32_t iters = std::max<uint32_t>(1, max_iterations);
+    if (iters > (1u << 20)) return fail(MARS_EINVAL, "max_iterations is above 2^20");
+    mars_ctx* ctx = p->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    const size_t px = (size_t)p->w * p->h;
+    Scratch sc(ctx->stream);
+    int* d_state = nullptr;  // [0] done, [1] used, [2 + i] step i's max delta
+    MARS_CUDA(sc.get(&d_state, 2 + (size_t)iters));
+    MARS_CUDA(cudaMemsetAsync(d_state, 0, (2 + (size_t)iters) * sizeof(int), ctx->stream));
+    // Step i reads buf[i % 2] and writes buf[(i + 1) % 2]; the decode that stopped after
+    // `used` steps ends in buf[used % 2].
+    uint8_t* buf[2] = {d_out, p->d_tmp};
+    MARS_CUDA(cudaMemsetAsync(buf[0], 128, px, ctx->stream));
+    for (uint32_t it = 0; it < iters; ++it) {
+        MARS_CUDA(mars::launch_decode_step_stable(buf[it & 1], buf[(it + 1) & 1], (int)p->w,
+                                                  (int)p->h, p->lg, p->d_owner, p->d_maps,
+                                                  p->d_rvals, d_state, d_state + 2 + it,
+                                                  (int)threshold, (int)it, d_state, d_state + 1,
+                                                  ctx->stream));
+        ctx->launches += 2;
+    }
+    int state[2] = {0, 0};
+    MARS_CUDA(cudaMemcpyAsync(state, d_state, sizeof state, cudaMemcpyDeviceToHost, ctx->stream));
+    if (int e = sync_bounded(ctx)) return e;
+    const uint32_t used = state[0] ? (uint32_t)state[1] : iters;
+    if (used & 1)
+        MARS_CUDA(cudaMemcpyAsync(d_out, p->d_tmp, px, cudaMemcpyDeviceToDevice, ctx->stream));
+    *iterations_used = used;
+    return MARS_OK;
+}
+
+int mars_decode_until_stable(mars_ctx* ctx, const mars_header* hdr, const mars_leaf* leaves,
+                             size_t n, const int32_t* residuals, size_t nresiduals,
+                             uint8_t threshold, uint32_t max_iterations, uint8_t* out,
+                             uint32_t* iterations_used) {
+    if (!ctx || !hdr || !out || !iterations_used) return fail(MARS_EINVAL, "NULL argument");
+    mars_decode_plan* plan = nullptr;
+    if (int e = mars_decode_plan_create(ctx, hdr, leaves, n, residuals, nresiduals, &plan))
+        return e;
+    std::unique_ptr<mars_decode_plan, void (*)(mars_decode_plan*)> guard(plan,
+                                                                         mars_decode_plan_free);
+    uint8_t* d_out = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        MARS_CUDA(cudaSetDevice(ctx->device));
+        MARS_CUDA(cudaMalloc(&d_out, std::max<size_t>(1, (size_t)hdr->width * hdr->height)));
+    }
+    std::unique_ptr<uint8_t, cudaError_t (*)(void*)> dguard(d_out, cudaFree);
+    if (int e = mars_decode_plan_run_until_stable(plan, threshold, max_iterations, d_out,
+                                                  iterations_used))
+        return e;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaMemcpyAsync(out, d_out, (size_t)hdr->width * hdr->height,
+                              cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_bounded(ctx);
+}
+
+// `(x * factor).round() as u32`: f64::round (half away from zero), then Rust's saturating
+// cast (NaN and negatives to 0).
+static uint32_t zoom_scale(uint32_t v, double factor) {
+    const double r = std::round((double)v * factor);
+    if (!(r > 0.0)) return 0;
+    if (r >= 4294967295.0) return 0xffffffffu;
+    return (uint32_t)r;
+}
+static int32_t zoom_grad(int32_t g, double factor) {
+    const double r = std::round((double)g / factor);
+    if (std::isnan(r)) return 0;
+    if (r >= 2147483647.0) return INT32_MAX;
+    if (r <= -2147483648.0) return INT32_MIN;
+    return (int32_t)r;
+}
+
+int mars_zoom_leaves(const mars_header* hdr, const mars_leaf* leaves, size_t n, double factor,
+                     mars_header* out_hdr, mars_leaf* out_leaves) {
+    if (!hdr || !out_hdr || (n && (!leaves || !out_leaves)))
+        return fail(MARS_EINVAL, "NULL argument");
+    if (!std::isfinite(factor) || factor <= 0.0)
+        return fail(MARS_EINVAL, "the zoom factor must be finite and positive");
+    for (size_t k = 0; k < n; ++k) {
+        mars_leaf L = leaves[k];
+        L.row = zoom_scale(L.row, factor);
+        L.col = zoom_scale(L.col, factor);
+        L.size = std::max<uint32_t>(zoom_scale(L.size, factor), 1);
+        L.dom_row = zoom_scale(L.dom_row, factor);
+        L.dom_col = zoom_scale(L.dom_col, factor);
+        L.qgx = zoom_grad(L.qgx, factor);
+        L.qgy = zoom_grad(L.qgy, factor);
+        // The residual is dropped at any factor but 1; a mode-3 leaf without one decodes by
+        // mode 2's formula (ifs.rs:441-456), and in this ABI every mode-3 leaf carries its
+        // levels in the residual pool, so the zoomed leaf comes back as mode 2.
+        if (factor != 1.0 && L.mode == 3) L.mode = 2;
+        out_leaves[k] = L;
+    }
+    *out_hdr = *hdr;
+    out_hdr->width = zoom_scale(hdr->width, factor);
+    out_hdr->height = zoom_scale(hdr->height, factor);
+    return MARS_OK;
+}
+
 void mars_decode_plan_free(mars_decode_plan* p) {
     if (!p) return;
     cudaSetDevice(p->ctx->device);

@@ -147,14 +147,33 @@ __device__ __forceinline__ uint32_t affine_pixel(const DecodeMap& m, int i, int 
                                     __dmul_rn(m.gy, (double)j))));
 }
 
+// Max-delta bookkeeping of the convergence-tested decode (decode_until_stable,
+// ifs.rs:321-353): a step that starts after convergence writes nothing, and every step
+// folds max |next - prev| of its pixels into its slot.
+struct StableState {
+    const int* done;  // set once an earlier step's delta met the threshold
+    int* delta;       // this step's max |next - prev|
+};
+
+__device__ __forceinline__ void fold_delta(uint32_t d, int* slot) {
+    for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_xor_sync(0xffffffffu, d, o));
+    if ((threadIdx.x & 31) == 0 && d) atomicMax(slot, (int)d);
+}
+
 // One pixel per thread (any owner-map granularity or width).
+template <bool kStable>
 __global__ void decode_pixel_kernel(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst,
                                     int w, int h, int lg, int mw,
                                     const int32_t* __restrict__ owner,
                                     const DecodeMap* __restrict__ maps,
-                                    const double* __restrict__ resid) {
+                                    const double* __restrict__ resid, StableState ss) {
+    if (kStable && *ss.done) return;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
+    if (kStable && (x >= w || y >= h)) {
+        fold_delta(0u, ss.delta);
+        return;
+    }
     if (x >= w || y >= h) return;
     const int32_t li = owner[(size_t)(y >> lg) * mw + (x >> lg)];
     uint32_t out = 0;
@@ -181,6 +200,10 @@ __global__ void decode_pixel_kernel(const uint8_t* __restrict__ src, uint8_t* __
         }
     }
     dst[(size_t)y * w + x] = (uint8_t)out;
+    if (kStable) {
+        const uint32_t prev = src[(size_t)y * w + x];
+        fold_delta(out > prev ? out - prev : prev - out, ss.delta);
+    }
 }
 
 // Eight bytes of the plane from byte offset `off` (off + 8 <= total), through aligned
@@ -203,12 +226,18 @@ __device__ __forceinline__ uint32_t pair_sums(uint32_t x) {
     return (x & 0x00FF00FFu) + ((x >> 8) & 0x00FF00FFu);
 }
 
+template <bool kStable>
 __global__ void __launch_bounds__(128) decode_cell_kernel(
     const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int w, int h, int lg, int mw,
     const int32_t* __restrict__ owner, const DecodeMap* __restrict__ maps,
-    const double* __restrict__ resid) {
+    const double* __restrict__ resid, StableState ss) {
+    if (kStable && *ss.done) return;
     const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int y0 = 4 * blockIdx.y;
+    if (kStable && (x0 >= w || y0 >= h)) {
+        fold_delta(0u, ss.delta);
+        return;
+    }
     if (x0 >= w || y0 >= h) return;
     const int32_t li = owner[(size_t)(y0 >> lg) * mw + (x0 >> lg)];
     uint64_t lo = 0, hi = 0;  // output rows 0-1 and 2-3, byte 4*a + b = pixel (y0 + a, x0 + b)
@@ -280,10 +309,32 @@ __global__ void __launch_bounds__(128) decode_cell_kernel(
         }
     }
     uint8_t* out = dst + (size_t)y0 * w + x0;
-    *reinterpret_cast<uint32_t*>(out) = (uint32_t)lo;
-    if (y0 + 1 < h) *reinterpret_cast<uint32_t*>(out + w) = (uint32_t)(lo >> 32);
-    if (y0 + 2 < h) *reinterpret_cast<uint32_t*>(out + 2 * (size_t)w) = (uint32_t)hi;
-    if (y0 + 3 < h) *reinterpret_cast<uint32_t*>(out + 3 * (size_t)w) = (uint32_t)(hi >> 32);
+    const uint32_t rows_out[4] = {(uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi,
+                                  (uint32_t)(hi >> 32)};
+    *reinterpret_cast<uint32_t*>(out) = rows_out[0];
+    if (y0 + 1 < h) *reinterpret_cast<uint32_t*>(out + w) = rows_out[1];
+    if (y0 + 2 < h) *reinterpret_cast<uint32_t*>(out + 2 * (size_t)w) = rows_out[2];
+    if (y0 + 3 < h) *reinterpret_cast<uint32_t*>(out + 3 * (size_t)w) = rows_out[3];
+    if (kStable) {
+        uint32_t m = 0;  // per-byte max |next - prev| over the cell's rows in the plane
+        const uint8_t* prev = src + (size_t)y0 * w + x0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+            if (y0 + a < h)
+                m = __vmaxu4(m, __vabsdiffu4(rows_out[a],
+                                             *reinterpret_cast<const uint32_t*>(prev + (size_t)a * w)));
+        m = max(max(m & 255u, (m >> 8) & 255u), max((m >> 16) & 255u, m >> 24));
+        fold_delta(m, ss.delta);
+    }
+}
+
+// After step `iter`: the first step whose delta met the threshold ends the decode.
+__global__ void decode_judge_kernel(const int* __restrict__ delta, int threshold, int iter,
+                                    int* __restrict__ done, int* __restrict__ used) {
+    if (!*done && *delta <= threshold) {
+        *done = 1;
+        *used = iter + 1;
+    }
 }
 
 }  // namespace
@@ -301,13 +352,38 @@ cudaError_t launch_decode_step(const uint8_t* src, uint8_t* dst, int w, int h, i
     const int mw = (w + (1 << lg) - 1) >> lg;
     const bool aligned =
         ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 7) == 0;
+    const StableState none{nullptr, nullptr};
     if (lg >= 2 && (w % 4) == 0 && aligned) {
         dim3 grid((w / 4 + 127) / 128, (h + 3) / 4);
-        decode_cell_kernel<<<grid, 128, 0, st>>>(src, dst, w, h, lg, mw, owner, maps, resid);
+        decode_cell_kernel<false><<<grid, 128, 0, st>>>(src, dst, w, h, lg, mw, owner, maps, resid,
+                                                        none);
     } else {
         dim3 grid((w + 255) / 256, h);
-        decode_pixel_kernel<<<grid, 256, 0, st>>>(src, dst, w, h, lg, mw, owner, maps, resid);
+        decode_pixel_kernel<false><<<grid, 256, 0, st>>>(src, dst, w, h, lg, mw, owner, maps,
+                                                         resid, none);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decode_step_stable(const uint8_t* src, uint8_t* dst, int w, int h, int lg,
+                                      const int32_t* owner, const DecodeMap* maps,
+                                      const double* resid, const int* done, int* delta,
+                                      int threshold, int iter, int* done_w, int* used,
+                                      cudaStream_t st) {
+    const int mw = (w + (1 << lg) - 1) >> lg;
+    const bool aligned =
+        ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 7) == 0;
+    const StableState ss{done, delta};
+    if (lg >= 2 && (w % 4) == 0 && aligned) {
+        dim3 grid((w / 4 + 127) / 128, (h + 3) / 4);
+        decode_cell_kernel<true><<<grid, 128, 0, st>>>(src, dst, w, h, lg, mw, owner, maps, resid,
+                                                       ss);
+    } else {
+        dim3 grid((w + 255) / 256, h);
+        decode_pixel_kernel<true><<<grid, 256, 0, st>>>(src, dst, w, h, lg, mw, owner, maps,
+                                                        resid, ss);
+    }
+    decode_judge_kernel<<<1, 1, 0, st>>>(delta, threshold, iter, done_w, used);
     return cudaGetLastError();
 }
 

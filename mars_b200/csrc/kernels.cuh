@@ -164,6 +164,14 @@ cudaError_t launch_decode_expand(const DecodeLeaf* leaves, const int32_t* resid_
                                  DecodeConsts c, DecodeMap* maps, cudaStream_t st);
 // owner: leaf index (or -1) per cell of 2^lg x 2^lg pixels, row-major, ceil(w/2^lg) wide.
 // resid: the residual pool (f64), or null.
+// One step of decode_until_stable (ifs.rs:321-353): a no-op once *done is set; otherwise
+// the step, its max |next - prev| into *delta, then *done / *used (= iter + 1) when that
+// delta is <= threshold.  done and done_w name the same flag.
+cudaError_t launch_decode_step_stable(const uint8_t* src, uint8_t* dst, int w, int h, int lg,
+                                      const int32_t* owner, const DecodeMap* maps,
+                                      const double* resid, const int* done, int* delta,
+                                      int threshold, int iter, int* done_w, int* used,
+                                      cudaStream_t st);
 cudaError_t launch_decode_step(const uint8_t* src, uint8_t* dst, int w, int h, int lg,
                                const int32_t* owner, const DecodeMap* maps, const double* resid,
                                cudaStream_t st);

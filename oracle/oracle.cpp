@@ -1584,6 +1584,14 @@ int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, const in
             at += (size_t)leaves[i].size * leaves[i].size;
         }
     if (at != nresiduals) return -1;
+    // Leaves whose range or domain leaves the plane make the reference index out of bounds
+    // (a panic); here they are an error.
+    for (size_t i = 0; i < n; ++i) {
+        const orc_leaf& L = leaves[i];
+        if (L.row + L.size > h || L.col + L.size > w) return -2;
+        if (L.mode != 1 && L.qalfa != 0 && (L.dom_row + 2 * L.size > h || L.dom_col + 2 * L.size > w))
+            return -2;
+    }
     std::vector<uint8_t> img(w * h, 128), next(w * h, 0);
     for (uint32_t it = 0; it < iterations; ++it) {
         std::fill(next.begin(), next.end(), 0);
@@ -1591,6 +1599,80 @@ int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, const in
         img.swap(next);
     }
     std::memcpy(out, img.data(), w * h);
+    return 0;
+}
+
+// decode_until_stable (ifs.rs:321-343) with max_pixel_delta (ifs.rs:347-353).
+int orc_decode_until_stable(const orc_header* hdr, const orc_leaf* leaves, size_t n,
+                            const int32_t* residuals, size_t nresiduals, uint8_t threshold,
+                            uint32_t max_iterations, uint8_t* out, uint32_t* used_out) {
+    const size_t w = hdr->width, h = hdr->height;
+    std::vector<const int32_t*> lv(n, nullptr);
+    size_t at = 0;
+    for (size_t i = 0; i < n; ++i)
+        if (leaves[i].mode == 3) {
+            lv[i] = residuals + at;
+            at += (size_t)leaves[i].size * leaves[i].size;
+        }
+    if (at != nresiduals) return -1;
+    for (size_t i = 0; i < n; ++i) {
+        const orc_leaf& L = leaves[i];
+        if (L.row + L.size > h || L.col + L.size > w) return -2;
+        if (L.mode != 1 && L.qalfa != 0 && (L.dom_row + 2 * L.size > h || L.dom_col + 2 * L.size > w))
+            return -2;
+    }
+    std::vector<uint8_t> img(w * h, 128), next(w * h, 0);
+    uint32_t used = 0;
+    for (uint32_t i = 0; i < std::max<uint32_t>(max_iterations, 1); ++i) {
+        std::fill(next.begin(), next.end(), 0);
+        for (size_t k = 0; k < n; ++k) decode_leaf(*hdr, leaves[k], lv[k], img.data(), w, next.data());
+        uint8_t delta = 0;
+        for (size_t p = 0; p < w * h; ++p) {
+            const uint8_t d = img[p] > next[p] ? img[p] - next[p] : next[p] - img[p];
+            delta = std::max(delta, d);
+        }
+        img.swap(next);
+        used = i + 1;
+        if (delta <= threshold) break;
+    }
+    std::memcpy(out, img.data(), w * h);
+    *used_out = used;
+    return 0;
+}
+
+// zoom_leaves (ifs.rs:370-392): `(v * factor).round() as u32` (half away from zero,
+// saturating), sizes at least 1, gradients `(g / factor).round() as i32`; residuals dropped
+// at any factor but 1 (a mode-3 leaf then decodes by mode 2's formula, so it is returned as
+// mode 2: this API keeps every mode-3 leaf's levels in the residual pool).
+int orc_zoom_leaves(const orc_header* hdr, const orc_leaf* leaves, size_t n, double factor,
+                    orc_header* out_hdr, orc_leaf* out) {
+    auto scale = [&](uint32_t v) -> uint32_t {
+        const double r = std::round((double)v * factor);
+        if (!(r > 0.0)) return 0;
+        return r >= 4294967295.0 ? 0xffffffffu : (uint32_t)r;
+    };
+    auto grad = [&](int32_t g) -> int32_t {
+        const double r = std::round((double)g / factor);
+        if (std::isnan(r)) return 0;
+        if (r >= 2147483647.0) return INT32_MAX;
+        if (r <= -2147483648.0) return INT32_MIN;
+        return (int32_t)r;
+    };
+    for (size_t k = 0; k < n; ++k) {
+        orc_leaf L = leaves[k];
+        L.row = scale(L.row);
+        L.col = scale(L.col);
+        L.size = std::max<uint32_t>(scale(L.size), 1);
+        L.dom_row = scale(L.dom_row);
+        L.dom_col = scale(L.dom_col);
+        L.qgx = grad(L.qgx);
+        L.qgy = grad(L.qgy);
+        if (factor != 1.0 && L.mode == 3) L.mode = 2;
+        out[k] = L;
+    }
+    *out_hdr = *hdr;
+    out_hdr->width = scale(hdr->width);
+    out_hdr->height = scale(hdr->height);
     return 0;
 }
 

@@ -114,6 +114,11 @@ int orc_refine_eval(const orc_header* hdr, const orc_leaf* leaves, size_t n,
                     double* loss, double* gs, double* go);
 int orc_decode(const orc_header* hdr, const orc_leaf* leaves, size_t n, const int32_t* residuals,
                size_t nresiduals, uint32_t iterations, uint8_t* out);
+int orc_decode_until_stable(const orc_header* hdr, const orc_leaf* leaves, size_t n,
+                            const int32_t* residuals, size_t nresiduals, uint8_t threshold,
+                            uint32_t max_iterations, uint8_t* out, uint32_t* used);
+int orc_zoom_leaves(const orc_header* hdr, const orc_leaf* leaves, size_t n, double factor,
+                    orc_header* out_hdr, orc_leaf* out);
 
 /* metrics::ycbcr / rgb_from_ycbcr (crates/mars-core/src/metrics.rs:377-460),
  * color::downsample_box / upsample_nearest (crates/mars-codec/src/color.rs:60-101) and

@@ -125,6 +125,11 @@ def lib():
                                     P(C.c_size_t)]
         L.orc_leaf_bits.argtypes = [P(Header), C.c_void_p, C.c_size_t, P(Leaf)]
         L.orc_leaf_bits.restype = C.c_double
+        L.orc_decode_until_stable.argtypes = [P(Header), C.c_void_p, C.c_size_t, C.c_void_p,
+                                              C.c_size_t, C.c_uint8, C.c_uint32, C.c_void_p,
+                                              P(C.c_uint32)]
+        L.orc_zoom_leaves.argtypes = [P(Header), C.c_void_p, C.c_size_t, C.c_double, P(Header),
+                                      C.c_void_p]
         L.orc_refine_params.argtypes = [P(Header), C.c_void_p, C.c_size_t, C.c_void_p,
                                         C.c_void_p]
         L.orc_refine_eval.argtypes = [P(Header), C.c_void_p, C.c_size_t, C.c_void_p,
@@ -392,3 +397,28 @@ def refine_eval(hdr: Header, leaves: np.ndarray, target, s, o, residuals=None,
     if rc:
         raise ValueError(f"orc_refine_eval failed: {rc}")
     return loss.value, x, gs, go
+
+
+def decode_until_stable(hdr: Header, leaves: np.ndarray, threshold: int, max_iterations: int,
+                        residuals=None):
+    """decode_until_stable (ifs.rs:321-343): (plane, iterations used)."""
+    leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    res = np.ascontiguousarray(residuals if residuals is not None else np.zeros(0), dtype=np.int32)
+    out = np.zeros((hdr.height, hdr.width), dtype=np.uint8)
+    used = C.c_uint32()
+    rc = lib().orc_decode_until_stable(C.byref(hdr), leaves.ctypes.data, len(leaves),
+                                       res.ctypes.data, len(res), threshold, max_iterations,
+                                       out.ctypes.data, C.byref(used))
+    if rc:
+        raise ValueError(f"orc_decode_until_stable failed: {rc}")
+    return out, used.value
+
+
+def zoom_leaves(hdr: Header, leaves: np.ndarray, factor: float):
+    """zoom_leaves (ifs.rs:370-392): (zoomed header, zoomed leaves)."""
+    leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+    out = np.zeros(len(leaves), dtype=LEAF_DTYPE)
+    h2 = Header()
+    lib().orc_zoom_leaves(C.byref(hdr), leaves.ctypes.data, len(leaves), factor, C.byref(h2),
+                          out.ctypes.data)
+    return h2, out

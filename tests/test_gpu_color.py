@@ -90,3 +90,34 @@ def test_color_pipeline_matches_the_oracle_pipeline(ctx):
                              orc.upsample_nearest(planes[2], W, H))
     assert np.array_equal(out, np.stack(ref, axis=-1))
     assert mb.psnr_from_mse(ctx.mse(out[..., 1], rgb[..., 1])) > 15.0
+
+
+def test_zoomed_and_auto_colour_decodes(ctx):
+    rgb = synthetic.rgb(96, 64, 5)
+    kw = dict(min_size=4, max_size=16, shift=2, lam=200.0)
+    params = color.ColorEncodeParams(mb.make_params(**kw), mb.make_params(**kw))
+    data, _ = color.encode_color(ctx, rgb, params)
+    mode, streams = color.read_container(data)
+    oplanes = []
+    for s in streams:
+        h, l, res = mb.format_read(s)
+        oh = orc.Header(*[getattr(h, f) for f, _ in h._fields_])
+        zh, zl = orc.zoom_leaves(oh, l, 2.0)
+        oplanes.append(orc.decode(zh, zl, 10))
+    H, W = oplanes[0].shape
+    ref = np.stack(orc.rgb_from_ycbcr(oplanes[0], orc.upsample_nearest(oplanes[1], W, H),
+                                      orc.upsample_nearest(oplanes[2], W, H)), axis=-1)
+    assert np.array_equal(color.decode_color_zoomed(ctx, data, 10, 2.0), ref)
+    out, used = color.decode_color_auto(ctx, data, 1, 40)
+    uses = []
+    oplanes = []
+    for s in streams:
+        h, l, res = mb.format_read(s)
+        oh = orc.Header(*[getattr(h, f) for f, _ in h._fields_])
+        p, n = orc.decode_until_stable(oh, l, 1, 40, res)
+        oplanes.append(p)
+        uses.append(n)
+    H, W = oplanes[0].shape
+    ref = np.stack(orc.rgb_from_ycbcr(oplanes[0], orc.upsample_nearest(oplanes[1], W, H),
+                                      orc.upsample_nearest(oplanes[2], W, H)), axis=-1)
+    assert used == max(uses) and np.array_equal(out, ref)

@@ -166,3 +166,54 @@ def test_decode_rejects_out_of_range_leaves(ctx):
     with pytest.raises(mb.MarsError) as e:
         ctx.decode_plan(_hdr(70000, 8), np.zeros(0, dtype=mb.LEAF_DTYPE))
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("threshold", [0, 1, 3, 255])
+def test_until_stable_matches_the_oracle(ctx, threshold):
+    # Aligned maps take the 4x4-cell kernel, the size-5 map the one-pixel kernel.
+    rng = np.random.default_rng(9)
+    maps = [(synthetic.quadtree_leaves(160, 96, 21), 160, 96, None)]
+    base = synthetic.quadtree_leaves(128, 96, 22)
+    leaves3, pool = _mode3(base, rng, p_zero=0.3)
+    maps.append((leaves3, 128, 96, pool))
+    rows = []
+    for r in range(0, 30, 5):
+        for c in range(0, 30, 5):
+            rows.append((r, c, 5, 2, int(rng.integers(1, 17)), int(rng.integers(0, 128)),
+                         int(rng.integers(0, 8)), int(rng.integers(0, 21)), int(rng.integers(0, 21)),
+                         0, 0))
+    maps.append((np.array(rows, dtype=mb.LEAF_DTYPE), 30, 30, None))
+    for leaves, w, h, res in maps:
+        hdr = _hdr(w, h)
+        got, used = ctx.decode_until_stable(hdr, leaves, threshold, 40, res)
+        want, oused = orc.decode_until_stable(_ohdr(hdr), leaves, threshold, 40, res)
+        assert used == oused and np.array_equal(got, want)
+
+
+def test_plan_until_stable_on_the_device(ctx):
+    import torch
+    leaves = synthetic.quadtree_leaves(256, 192, 23)
+    hdr = _hdr(256, 192)
+    plan = ctx.decode_plan(hdr, leaves)
+    out = torch.zeros(256 * 192, dtype=torch.uint8, device="cuda:0")
+    used = mb.C.c_uint32()
+    mb.check(mb.lib().mars_decode_plan_run_until_stable(plan._h, 2, 30, out.data_ptr(),
+                                                        mb.C.byref(used)))
+    torch.cuda.synchronize()
+    want, oused = orc.decode_until_stable(_ohdr(hdr), leaves, 2, 30)
+    assert used.value == oused
+    assert np.array_equal(out.cpu().numpy().reshape(192, 256), want)
+    plan.close()
+
+
+@pytest.mark.parametrize("factor", [2.0, 1.5, 0.5])
+def test_zoomed_decode_matches_the_oracle(ctx, factor):
+    img = synthetic.gray(128, 96, 24)
+    hdr, leaves, res, _ = ctx.encode(img, mb.make_params(min_size=4, max_size=16, shift=4, lam=200.0),
+                                     allowed_modes=(1, 1, 1, 1))
+    zh, zl = mb.zoom_leaves(hdr, leaves, factor)
+    ozh, ozl = orc.zoom_leaves(_ohdr(hdr), leaves, factor)
+    assert zl.tobytes() == ozl.tobytes()
+    got = ctx.decode(zh, zl, 10)
+    assert got.shape == (round(96 * factor), round(128 * factor))
+    assert np.array_equal(got, orc.decode(ozh, ozl, 10))
