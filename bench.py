@@ -380,6 +380,31 @@ def run_refine(mb, ctx, stream, dev, peaks, seeds=REFINE_SEEDS, lambdas=REFINE_L
     }
 
 
+def run_encode(mb, ctx, workers=3):
+    """Whole RD encodes of the 512x512 planes (seeds 1-8, lambda 200, sizes 32..4, stride 2):
+    the search on the GPU and the host walks, host plane in, leaves out.  `value`: images/s
+    through Context.encode_many (a search plan per size, `workers` planes in flight so one
+    plane's walks overlap the next one's search); `sequential`: one ctx.encode after
+    another.  Both for the default modes {0, 2} and for all four modes."""
+    imgs = [synthetic.gray(W, H, s) for s in range(1, 9)]
+    params = mb.make_params(min_size=4, max_size=32, shift=SHIFT, lam=200.0)
+    out = {"workload": "RD encode (search + walks + mode pricing) of 8 synthetic 512x512 gray "
+                       "planes, lambda 200, sizes 32..4, domain stride 2",
+           "unit": "images/s", "workers": workers}
+    for key, modes in (("modes_0_2", (1, 0, 1, 0)), ("modes_0_3", (1, 1, 1, 1))):
+        ctx.encode_many(imgs[:2], params, workers=workers, allowed_modes=modes)
+        t0 = time.perf_counter()
+        ctx.encode_many(imgs, params, workers=workers, allowed_modes=modes)
+        piped = len(imgs) / (time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        for im in imgs:
+            ctx.encode(im, params, allowed_modes=modes)
+        seq = len(imgs) / (time.perf_counter() - t0)
+        out[key] = {"value": piped, "sequential": seq}
+    out["value"] = out["modes_0_2"]["value"]
+    return out
+
+
 UNEVEN_COUNT, UNEVEN_SEED, UNEVEN_LARGE = 64, 5, 4096
 
 
@@ -582,6 +607,8 @@ def run_gpu(args):
         decode = run_decode(args, mb, ctx, stream, dev, peaks, DECODE_SIDE, with_cpu, flush)
         decode_large = run_decode(args, mb, ctx, stream, dev, peaks, DECODE_SIDE_LARGE, False)
 
+    encode = run_encode(mb, ctx) if rank == 0 else None
+
     refine = None
     if rank == 0 and not args.no_refine:
         refine = run_refine(mb, ctx, stream, dev, peaks)
@@ -622,6 +649,7 @@ def run_gpu(args):
             "clocks": clocks.summary(),
             "decode": decode,
             "decode_large": decode_large,
+            "encode": encode,
             "refine": refine,
             "uneven": uneven,
         }

@@ -185,6 +185,14 @@ uint64_t mars_search_plan_evals(const mars_search_plan* plan);
 /* Kernel launches one run replays (the graph's kernel nodes). */
 uint64_t mars_search_plan_launches(const mars_search_plan* plan);
 void mars_search_plan_free(mars_search_plan* plan);
+/* mars_encode through a plan (the plan's geometry and parameters): one graph launch for
+ * the search, then the walks.  Exhaustive, single-winner, no adaptive density; the
+ * outputs are mars_encode's.  Thread-safe per plan: concurrent calls overlap one plane's
+ * walks with another's search. */
+int mars_encode_planned(mars_search_plan* plan, const uint8_t* plane,
+                        const mars_options* options, mars_header* header, mars_leaf** leaves,
+                        size_t* nleaves, int32_t** residuals, size_t* nresiduals,
+                        mars_counters* counters);
 
 /* IndexedSearchProvider::build (crates/mars-search/src/lib.rs:480-513) for `method`: the
  * per-size domain indexes (plus the doubled-stride ones when adaptive_density and a

@@ -97,7 +97,7 @@ EXPORTS = (
     "mars_search_plan_create", "mars_search_plan_run", "mars_search_plan_run_device",
     "mars_search_plan_table", "mars_search_plan_evals", "mars_search_plan_launches",
     "mars_search_plan_free", "mars_decode_until_stable", "mars_decode_plan_run_until_stable",
-    "mars_zoom_leaves",
+    "mars_zoom_leaves", "mars_encode_planned",
     "mars_refine_plan_create", "mars_refine_params", "mars_refine_forward",
     "mars_refine_backward", "mars_refine_run", "mars_refine_plan_free",
 )
@@ -135,6 +135,8 @@ def lib():
                                             P(u32)]
     L.mars_decode_plan_run_until_stable.argtypes = [vp, C.c_uint8, u32, vp, P(u32)]
     L.mars_zoom_leaves.argtypes = [P(Header), vp, sz, C.c_double, P(Header), vp]
+    L.mars_encode_planned.argtypes = [vp, vp, P(Options), P(Header), P(vp), P(sz), P(vp), P(sz),
+                                      P(Counters)]
     L.mars_search_plan_create.argtypes = [vp, u32, u32, P(Params), P(vp)]
     L.mars_search_plan_run.argtypes = [vp, vp, P(vp)]
     L.mars_search_plan_run_device.argtypes = [vp, vp]
@@ -306,6 +308,9 @@ class Context:
         return self._h.value
 
     def close(self) -> None:
+        for plan in getattr(self, "_plans", {}).values():
+            plan.close()
+        self._plans = {}
         if self._h:
             lib().mars_ctx_destroy(self._h)
             self._h = C.c_void_p(None)
@@ -393,18 +398,44 @@ class Context:
         opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density),
                        int(residual_adaptive), float(residual_qstep), METHODS[method],
                        int(rd_candidates))
-        hdr, cnt = Header(), Counters()
-        ptr, n = C.c_void_p(), C.c_size_t()
-        rptr, rn = C.c_void_p(), C.c_size_t()
-        check(lib().mars_encode(self._h, a.ctypes.data, w, h, C.byref(params), C.byref(opts),
-                                C.byref(hdr), C.byref(ptr), C.byref(n), C.byref(rptr),
-                                C.byref(rn), C.byref(cnt)))
-        leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize),
-                               dtype=LEAF_DTYPE).copy()
-        resid = np.frombuffer(C.string_at(rptr, rn.value * 4), dtype=np.int32).copy()
-        lib().mars_leaves_free(ptr)
-        lib().mars_residuals_free(rptr)
-        return hdr, leaves, resid, cnt
+        return _encode_call(lambda *out: lib().mars_encode(
+            self._h, a.ctypes.data, w, h, C.byref(params), C.byref(opts), *out))
+
+    def encode_many(self, images, params: Params, workers: int = 3, **options):
+        """encode() over many planes, `workers` at a time: the C ABI is thread-safe, so one
+        plane's host walks overlap another's GPU search.  Exhaustive single-winner encodes
+        without adaptive density go through a search plan per plane size."""
+        from concurrent.futures import ThreadPoolExecutor
+        planned = (options.get("method", "exhaustive") == "exhaustive"
+                   and options.get("rd_candidates", 1) <= 1
+                   and not (params.has_lambda and options.get("adaptive_density", False)))
+        plans = {}
+        if planned:
+            for im in images:
+                shape = _plane(im).shape
+                if shape not in plans:
+                    plans[shape] = self.cached_plan(shape[1], shape[0], params)
+        modes = options.pop("allowed_modes", (1, 0, 1, 0))
+
+        def one(im):
+            if planned:
+                return plans[_plane(im).shape].encode(
+                    im, allowed_modes=modes,
+                    residual_adaptive=options.get("residual_adaptive", False),
+                    residual_qstep=options.get("residual_qstep", 0.0))
+            return self.encode(im, params, allowed_modes=modes, **options)
+
+        with ThreadPoolExecutor(max(1, workers)) as ex:
+            return list(ex.map(one, images))
+
+    def cached_plan(self, width: int, height: int, params: Params) -> "SearchPlan":
+        """A search plan kept by the context for its lifetime, one per (size, params)."""
+        key = (width, height, bytes(params))
+        if not hasattr(self, "_plans"):
+            self._plans = {}
+        if key not in self._plans:
+            self._plans[key] = self.search_plan(width, height, params)
+        return self._plans[key]
 
     # ---- colour input and metric (device kernels; host arrays staged through torch) ----
 
@@ -507,6 +538,21 @@ class Context:
         return out
 
 
+def _encode_call(call):
+    """Runs a mars_encode-shaped call and returns (header, leaves, residuals, counters)."""
+    hdr, cnt = Header(), Counters()
+    ptr, n = C.c_void_p(), C.c_size_t()
+    rptr, rn = C.c_void_p(), C.c_size_t()
+    check(call(C.byref(hdr), C.byref(ptr), C.byref(n), C.byref(rptr), C.byref(rn),
+               C.byref(cnt)))
+    leaves = np.frombuffer(C.string_at(ptr, n.value * LEAF_DTYPE.itemsize),
+                           dtype=LEAF_DTYPE).copy()
+    resid = np.frombuffer(C.string_at(rptr, rn.value * 4), dtype=np.int32).copy()
+    lib().mars_leaves_free(ptr)
+    lib().mars_residuals_free(rptr)
+    return hdr, leaves, resid, cnt
+
+
 def _residuals(residuals) -> np.ndarray:
     return np.ascontiguousarray(residuals if residuals is not None else np.zeros(0),
                                 dtype=np.int32)
@@ -559,6 +605,17 @@ class SearchPlan:
 
     def run_device(self, d_plane_ptr: int) -> None:
         check(lib().mars_search_plan_run_device(self._h, C.c_void_p(d_plane_ptr)))
+
+    def encode(self, img, allowed_modes=(1, 0, 1, 0), residual_adaptive=False,
+               residual_qstep=0.0):
+        """mars_encode_planned: (header, leaves, residuals, counters)."""
+        a = _plane(img)
+        if a.shape != (self.height, self.width):
+            raise ValueError("plane shape differs from the plan's")
+        opts = Options((C.c_uint8 * 4)(*allowed_modes), 0, int(residual_adaptive),
+                       float(residual_qstep), 0, 1)
+        return _encode_call(lambda *out: lib().mars_encode_planned(
+            self._h, a.ctypes.data, C.byref(opts), *out))
 
     def table(self) -> GpuSearch:
         t = C.c_void_p()

@@ -779,6 +779,61 @@ int mars_search_nodes_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t wid
                     (mars::CandidateOut*)d_out);
 }
 
+}  // extern "C"
+
+namespace {
+
+// The walks of encode_image_with_search over filled tables (`table` for the final walk,
+// `warm` for the RD warm-up), and the C-ABI outputs.
+int encode_on_tables(const uint8_t* plane, uint32_t width, uint32_t height,
+                     const mars_params* params, const mars_options* options, mars_table* table,
+                     mars_table* warm, uint32_t rd_k, mars_header* header, mars_leaf** leaves,
+                     size_t* nleaves, int32_t** residuals, size_t* nresiduals,
+                     mars_counters* counters) {
+    auto lookup = [](mars_table* t) {
+        return [t](uint32_t row, uint32_t col, uint32_t size, uint32_t shift,
+                   mars::codec::SearchAnswer* ans) {
+            return mars_search_table_lookup(t, row, col, size, shift, &ans->cand, &ans->evals);
+        };
+    };
+    const mars::codec::Provider provider = lookup(table);
+    const mars::codec::Provider warmup = lookup(warm);
+    const mars::codec::RankedProvider ranked = [table](uint32_t row, uint32_t col, uint32_t size,
+                                                       uint32_t shift, uint32_t max,
+                                                       std::vector<mars_candidate>* v,
+                                                       uint64_t* evals) {
+        v->resize(std::max<uint32_t>(max, 1));
+        uint32_t n = 0;
+        const int e = mars_search_table_lookup_ranked(table, row, col, size, shift, max, v->data(),
+                                                      &n, evals);
+        v->resize(e ? 0 : n);
+        return e;
+    };
+    std::vector<mars_leaf> out;
+    std::vector<int32_t> res;
+    const mars::codec::Image im{plane, width, height};
+    if (int e = mars::codec::encode(im, *params, *options, provider, warmup, header, &out, &res,
+                                    counters, rd_k > 1 ? &ranked : nullptr))
+        return e;
+    *nleaves = out.size();
+    *leaves = (mars_leaf*)std::malloc(std::max<size_t>(1, out.size()) * sizeof(mars_leaf));
+    if (!*leaves) return fail(MARS_ENOMEM, "leaf array allocation failed");
+    std::memcpy(*leaves, out.data(), out.size() * sizeof(mars_leaf));
+    *nresiduals = res.size();
+    *residuals = (int32_t*)std::malloc(std::max<size_t>(1, res.size()) * sizeof(int32_t));
+    if (!*residuals) {
+        std::free(*leaves);
+        *leaves = nullptr;
+        return fail(MARS_ENOMEM, "residual array allocation failed");
+    }
+    if (!res.empty()) std::memcpy(*residuals, res.data(), res.size() * sizeof(int32_t));
+    return MARS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
                 const mars_params* params, const mars_options* options, mars_header* header,
                 mars_leaf** leaves, size_t* nleaves, int32_t** residuals, size_t* nresiduals,
@@ -812,44 +867,8 @@ int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t he
         if (int e = build_table(ctx, plane, nullptr, width, height, &wp, false, &warm)) return e;
     }
     std::unique_ptr<mars_table, void (*)(mars_table*)> wguard(warm, mars_search_table_free);
-    auto lookup = [](mars_table* t) {
-        return [t](uint32_t row, uint32_t col, uint32_t size, uint32_t shift,
-                   mars::codec::SearchAnswer* ans) {
-            return mars_search_table_lookup(t, row, col, size, shift, &ans->cand, &ans->evals);
-        };
-    };
-    const mars::codec::Provider provider = lookup(table);
-    const mars::codec::Provider warmup = lookup(warm ? warm : table);
-    const mars::codec::RankedProvider ranked = [table](uint32_t row, uint32_t col, uint32_t size,
-                                                       uint32_t shift, uint32_t max,
-                                                       std::vector<mars_candidate>* v,
-                                                       uint64_t* evals) {
-        v->resize(std::max<uint32_t>(max, 1));
-        uint32_t n = 0;
-        const int e = mars_search_table_lookup_ranked(table, row, col, size, shift, max, v->data(),
-                                                      &n, evals);
-        v->resize(e ? 0 : n);
-        return e;
-    };
-    std::vector<mars_leaf> out;
-    std::vector<int32_t> res;
-    const mars::codec::Image im{plane, width, height};
-    if (int e = mars::codec::encode(im, *params, *options, provider, warmup, header, &out, &res,
-                                    counters, rd_k > 1 ? &ranked : nullptr))
-        return e;
-    *nleaves = out.size();
-    *leaves = (mars_leaf*)std::malloc(std::max<size_t>(1, out.size()) * sizeof(mars_leaf));
-    if (!*leaves) return fail(MARS_ENOMEM, "leaf array allocation failed");
-    std::memcpy(*leaves, out.data(), out.size() * sizeof(mars_leaf));
-    *nresiduals = res.size();
-    *residuals = (int32_t*)std::malloc(std::max<size_t>(1, res.size()) * sizeof(int32_t));
-    if (!*residuals) {
-        std::free(*leaves);
-        *leaves = nullptr;
-        return fail(MARS_ENOMEM, "residual array allocation failed");
-    }
-    if (!res.empty()) std::memcpy(*residuals, res.data(), res.size() * sizeof(int32_t));
-    return MARS_OK;
+    return encode_on_tables(plane, width, height, params, options, table, warm ? warm : table,
+                            rd_k, header, leaves, nleaves, residuals, nresiduals, counters);
 }
 
 // ---------------------------------------------------------------- search plans
@@ -1064,6 +1083,29 @@ void mars_search_plan_free(mars_search_plan* p) {
     cudaStreamSynchronize(p->ctx->stream);
     plan_release(p);
 }
+
+int mars_encode_planned(mars_search_plan* plan, const uint8_t* plane,
+                        const mars_options* options, mars_header* header, mars_leaf** leaves,
+                        size_t* nleaves, int32_t** residuals, size_t* nresiduals,
+                        mars_counters* counters) {
+    if (!plan || !plane || !options || !header || !leaves || !nleaves || !residuals ||
+        !nresiduals || !counters)
+        return fail(MARS_EINVAL, "NULL argument");
+    if (options->method != MARS_METHOD_EXHAUSTIVE || std::max<uint32_t>(1, options->rd_candidates) > 1 ||
+        (plan->params.has_lambda && options->adaptive_density))
+        return fail(MARS_EUNSUPPORTED, "a search plan serves exhaustive single-winner encodes "
+                                       "without adaptive density");
+    if (!options->residual_adaptive && options->residual_qstep != 0.0f &&
+        !(std::isfinite(options->residual_qstep) && options->residual_qstep >= 1.0f &&
+          options->residual_qstep <= 65535.0f))
+        return fail(MARS_EINVAL, "residual qstep must be finite and in [1, 65535]");
+    mars_table* table = nullptr;
+    if (int e = mars_search_plan_run(plan, plane, &table)) return e;
+    std::unique_ptr<mars_table, void (*)(mars_table*)> guard(table, mars_search_table_free);
+    return encode_on_tables(plane, plan->w, plan->h, &plan->params, options, table, table, 1,
+                            header, leaves, nleaves, residuals, nresiduals, counters);
+}
+
 
 void mars_leaves_free(mars_leaf* leaves) { std::free(leaves); }
 void mars_residuals_free(int32_t* residuals) { std::free(residuals); }

@@ -68,3 +68,30 @@ def test_plan_rejects_a_wrong_shape(ctx):
     with pytest.raises(ValueError):
         plan.run(np.zeros((32, 64), np.uint8))
     plan.close()
+
+
+@pytest.mark.parametrize("modes,lam", [((1, 0, 1, 0), 200.0), ((1, 1, 1, 1), 50.0), ((1, 0, 1, 0), None)])
+def test_planned_encodes_equal_the_one_shot_encode(ctx, modes, lam):
+    params = mb.make_params(min_size=4, max_size=16, shift=2, lam=lam)
+    imgs = [synthetic.gray(96, 80, s) for s in (3, 4, 5, 6)] + [synthetic.gray(64, 64, 7)]
+    many = ctx.encode_many(imgs, params, workers=3, allowed_modes=modes)
+    for im, got in zip(imgs, many):
+        want = ctx.encode(im, params, allowed_modes=modes)
+        assert bytes(got[0]) == bytes(want[0])
+        assert got[1].tobytes() == want[1].tobytes() and got[2].tobytes() == want[2].tobytes()
+        assert (got[3].search_evals, got[3].warmup_evals) == (want[3].search_evals,
+                                                              want[3].warmup_evals)
+
+
+def test_planned_encode_refuses_what_a_plan_cannot_serve(ctx):
+    params = mb.make_params(min_size=4, max_size=16, shift=2, lam=200.0)
+    plan = ctx.search_plan(64, 64, params)
+    img = synthetic.gray(64, 64, 8)
+    opts = mb.Options((mb.C.c_uint8 * 4)(1, 0, 1, 0), 0, 0, 0.0, 1, 1)  # Fisher
+    hdr, cnt = mb.Header(), mb.Counters()
+    ptr, n, rptr, rn = mb.C.c_void_p(), mb.C.c_size_t(), mb.C.c_void_p(), mb.C.c_size_t()
+    rc = mb.lib().mars_encode_planned(plan._h, img.ctypes.data, mb.C.byref(opts), mb.C.byref(hdr),
+                                      mb.C.byref(ptr), mb.C.byref(n), mb.C.byref(rptr),
+                                      mb.C.byref(rn), mb.C.byref(cnt))
+    assert rc == -8  # MARS_EUNSUPPORTED
+    plan.close()
