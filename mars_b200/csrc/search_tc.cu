@@ -550,18 +550,27 @@ __global__ void __launch_bounds__(kThreads, 1)
         const float four_inv_n = 4.0f / (float)N;
         unsigned long long exact = 0;
 
-        // This lane's domain statistics, prefetched one tile ahead.
+        // This lane's domain statistics, prefetched one tile ahead.  The lane's column
+        // offset within a tile is fixed (domain_of_lane is P * (q0 + 8h + r8) + p), and
+        // the tile's domain row and column step forward with mt, so no division runs per
+        // tile.
+        const int lane_col = domain_of_lane(m, P, 0);
+        const int tile_cols = kM;  // domain columns a tile spans: (kM / P) groups of P
+        int nx_a = m_begin / tiles_per_row, nx_t = m_begin % tiles_per_row;
         auto load_dom = [&](int mt, float& s1f, float& detf, float& sdetf, int& dom) {
             if (mt >= m_end) return;
-            const int a = mt / tiles_per_row;
-            const int c = domain_of_lane(m, P, (mt % tiles_per_row) * (kM / P));
+            const int c = nx_t * tile_cols + lane_col;
             if (c < g.ncol_d) {
-                dom = a * g.ncol_d + c;
+                dom = nx_a * g.ncol_d + c;
                 s1f = (float)ds.s1x4[dom];
                 detf = ds.detf[dom];
                 sdetf = ds.sdetf[dom];
             } else {
                 dom = -1;
+            }
+            if (++nx_t == tiles_per_row) {
+                nx_t = 0;
+                ++nx_a;
             }
         };
         float n_s1 = 0.f, n_det = 0.f, n_sdet = 0.f;
@@ -582,9 +591,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tmem + ((uint32_t)(e * 32) << 16) + (uint32_t)(b * kN + part * kColsPerWarp);
             bool rescan = false;
 
+            // Max of 8 accumulator columns with three-input integer max instructions.
             auto max8 = [](const int32_t (&v)[32], int o) {
-                return max(max(max(v[o], v[o + 1]), max(v[o + 2], v[o + 3])),
-                           max(max(v[o + 4], v[o + 5]), max(v[o + 6], v[o + 7])));
+                return __vimax3_s32(__vimax3_s32(v[o], v[o + 1], v[o + 2]),
+                                    __vimax3_s32(v[o + 3], v[o + 4], v[o + 5]),
+                                    max(v[o + 6], v[o + 7]));
             };
             const uint32_t tag = (uint32_t)(mt & 0xFFFF);
             // Thresholds of this lane's domain against its ranges (fit.cuh, branch-free
