@@ -284,8 +284,9 @@ __device__ __forceinline__ void publish_threshold(Smem& sm, int rl, const FitPar
     const Champ& C = sm.ch[rl];
     ThrRec t;
     if (!C.valid) {
-        // An invalid range never survives: c = +huge makes every threshold unreachable.
-        t = ThrRec{0.0f, 0.0f, 0.0f, 3.0e38f, INT32_MAX, 0, 0, 0};
+        // An invalid range never survives: in the Z-form (tie = -1) with sqrt_w = w2a =
+        // +inf, tau = +inf for every domain, flat all-zero ones (s1 = 0) included.
+        t = ThrRec{INFINITY, INFINITY, 0.0f, 3.0e38f, -1, 0, 0, 0};
         sm.thr[rl] = t;
         return;
     }
@@ -349,7 +350,7 @@ __device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t ta
         Champ& C = sm.ch[et];
         const double r2 = __longlong_as_double((long long)sm.key_rms[et]);
         const uint32_t i2 = sm.key_idx[et];
-        if (r2 < C.rms || (r2 == C.rms && i2 < C.idx)) {
+        if (C.valid && (r2 < C.rms || (r2 == C.rms && i2 < C.idx))) {
             C.rms = r2;
             C.idx = i2;
             C.sum = sm.key_sum[et];
@@ -611,6 +612,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                     ra[r] = rec[2 * (part * kRangesPerWarp + r)];
                     rb[r] = reinterpret_cast<const int4*>(rec)[2 * (part * kRangesPerWarp + r) + 1];
                 }
+                // s1 * c + tau with one rounding toward -inf (fma): still never above the
+                // exact threshold.  (Branching on an all-Z-form tile measured slower than
+                // these selects.)
                 float tau[kRangesPerWarp];
 #pragma unroll
                 for (int r = 0; r < kRangesPerWarp; ++r) {
@@ -619,10 +623,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                     tau[r] = dom > rb[r].x ? tz : __fadd_rd(g1, ra[r].z);
                 }
 #pragma unroll
-                for (int r = 0; r < kRangesPerWarp; ++r) {
-                    const float num = __fadd_rd(__fmul_rd(s1f, ra[r].w), tau[r]);
-                    thr[r] = dom < 0 ? INT32_MAX : __float2int_rd(num);
-                }
+                for (int r = 0; r < kRangesPerWarp; ++r)
+                    thr[r] = dom < 0 ? INT32_MAX : __float2int_rd(__fmaf_rd(s1f, ra[r].w, tau[r]));
             };
             auto test_chunk = [&](const int32_t (&v)[32], int ch) {
                 const int32_t t0 = thr[ch * 4], t1 = thr[ch * 4 + 1];

@@ -314,3 +314,33 @@ def test_large_plane_sampled_nodes(ctx):
         o, oev = orc.search_blocks(img, size, 2, p, rows, cols)
         assert np.array_equal(gev, oev) and g.tobytes() == o.tobytes(), size
     prov.close()
+
+
+@pytest.mark.parametrize("path", ["auto", "simt"])
+def test_out_of_plane_blocks_stay_invalid_next_to_black_domains(ctx, path):
+    # A black region gives domains with s1 = 0, whose pruning threshold does not depend on
+    # the range's brightness; an out-of-plane origin must still come back invalid.
+    import torch
+    img = synthetic.gray(128, 128, 4)
+    img[:48, :48] = 0
+    d_img = torch.from_numpy(img).cuda()
+    # Origins 1 and 2 leave the plane for both block sizes (126 + 4 > 128).
+    rows = torch.tensor([64, 126, 125, 0], dtype=torch.int32, device="cuda")
+    cols = torch.tensor([64, 0, 126, 0], dtype=torch.int32, device="cuda")
+    out = torch.zeros((4, 80), dtype=torch.uint8, device="cuda")
+    p = mb.make_params(shift=2)
+    ctx.set_search_path(path)
+    try:
+        for size in (4, 8):
+            torch.cuda.synchronize()
+            mb.check(mb.lib().mars_search_blocks_device(ctx.handle, d_img.data_ptr(), 128, 128,
+                                                        size, 2, mb.C.byref(p), rows.data_ptr(),
+                                                        cols.data_ptr(), 4, out.data_ptr()))
+            torch.cuda.synchronize()
+            rec = out.cpu().numpy().view(mb.CANDIDATE_DTYPE).ravel()
+            assert rec[1]["valid"] == 0 and rec[2]["valid"] == 0
+            for i in (0, 3):
+                o, _ = orc.search(img, int(rows[i]), int(cols[i]), size, 2, orc.make_params(shift=2))
+                assert rec[i].tobytes() == o[0].tobytes()
+    finally:
+        ctx.set_search_path("auto")
