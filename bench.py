@@ -607,14 +607,17 @@ def run_gpu(args):
         decode = run_decode(args, mb, ctx, stream, dev, peaks, DECODE_SIDE, with_cpu, flush)
         decode_large = run_decode(args, mb, ctx, stream, dev, peaks, DECODE_SIDE_LARGE, False)
 
-    encode = run_encode(mb, ctx) if rank == 0 else None
+    # The single-GPU legs run at N = 1 only: under torchrun the other ranks would sit in
+    # the final barrier for their whole duration.
+    single = rank == 0 and world == 1
+    encode = run_encode(mb, ctx) if single else None
 
     refine = None
-    if rank == 0 and not args.no_refine:
+    if single and not args.no_refine:
         refine = run_refine(mb, ctx, stream, dev, peaks)
 
     uneven = None
-    if rank == 0 and not args.no_uneven:
+    if single and not args.no_uneven:
         uneven = run_uneven(mb, ctx, dev)
 
     cpu = None
