@@ -50,7 +50,7 @@ WORKLOAD = ("exhaustive search of every RD quadtree node of a 512x512 synthetic 
 
 # DRAM bytes (read + write) per launch of the dominant search kernel, from one ncu capture
 # of this workload's s=4 level (profiles/corr_tc_s4_512x512_ncu.md).
-NCU_TRAFFIC = {4: 21_066_496 + 12_032}
+NCU_TRAFFIC = {4: 20_560_000}
 # The same for one decode iteration, by plane side (profiles/decode_cell_*_ncu.md; the
 # 16384^2 figure is dram__bytes.sum.per_second x gpu__time_duration.sum of its capture).
 NCU_DECODE_TRAFFIC = {4096: 34_831_104 + 748_800, 16384: 4_797_900_000}
