@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(128) decode_cell_kernel(
 }
 
 // After step `iter`: the first step whose delta met the threshold ends the decode.
-__global__ void decode_judge_kernel(const int* __restrict__ delta, int threshold, int iter,
+__global__ void decode_converged_kernel(const int* __restrict__ delta, int threshold, int iter,
                                     int* __restrict__ done, int* __restrict__ used) {
     if (!*done && *delta <= threshold) {
         *done = 1;
@@ -383,7 +383,7 @@ cudaError_t launch_decode_step_stable(const uint8_t* src, uint8_t* dst, int w, i
         decode_pixel_kernel<true><<<grid, 256, 0, st>>>(src, dst, w, h, lg, mw, owner, maps,
                                                         resid, ss);
     }
-    decode_judge_kernel<<<1, 1, 0, st>>>(delta, threshold, iter, done_w, used);
+    decode_converged_kernel<<<1, 1, 0, st>>>(delta, threshold, iter, done_w, used);
     return cudaGetLastError();
 }
 
