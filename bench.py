@@ -385,12 +385,16 @@ def run_encode(mb, ctx, workers=3):
     the search on the GPU and the host walks, host plane in, leaves out.  `value`: images/s
     through Context.encode_many (a search plan per size, `workers` planes in flight so one
     plane's walks overlap the next one's search); `sequential`: one ctx.encode after
-    another.  Both for the default modes {0, 2} and for all four modes."""
+    another.  Both for the default modes {0, 2} and for all four modes: the four-mode encode
+    prices every quadtree node (the residual mode's DCTs) on the device, the two-mode one on
+    the host walk."""
     imgs = [synthetic.gray(W, H, s) for s in range(1, 9)]
     params = mb.make_params(min_size=4, max_size=32, shift=SHIFT, lam=200.0)
     out = {"workload": "RD encode (search + walks + mode pricing) of 8 synthetic 512x512 gray "
                        "planes, lambda 200, sizes 32..4, domain stride 2",
-           "unit": "images/s", "workers": workers}
+           "unit": "images/s", "workers": workers,
+           "pricing": {"modes_0_2": "host walk", "modes_0_3": "device (rdprice.cu), one warp "
+                       "per quadtree node"}}
     for key, modes in (("modes_0_2", (1, 0, 1, 0)), ("modes_0_3", (1, 1, 1, 1))):
         ctx.encode_many(imgs[:2], params, workers=workers, allowed_modes=modes)
         t0 = time.perf_counter()

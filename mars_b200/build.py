@@ -8,11 +8,15 @@ import os
 import shutil
 import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmars_b200.so")
 SOURCES = ["api.cu", "search.cu", "search_tc.cu", "decode.cu", "fisher.cu", "color.cu", "refine.cu", "noalloc.cu", "codec.cpp", "format.cpp"]
+# Translation units whose f64 arithmetic must match the host's operation for operation: no
+# multiply-add contraction on the device (the host side is built with -ffp-contract=off).
+EXACT_F64_SOURCES = ["rdprice.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -40,17 +44,28 @@ def stale() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
         return LIB
-    cmd = [nvcc(), *host_compiler(), "-O3", "-std=c++17", "-shared", "-lineinfo", *ARCH,
-           "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", "-Xptxas", "-v" if verbose else "-O3",
-           "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
+    common = [nvcc(), *host_compiler(), "-O3", "-std=c++17", "-lineinfo", *ARCH,
+              "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
+              "-Xptxas", "-v" if verbose else "-O3"]
+    with tempfile.TemporaryDirectory() as tmp:
+        objects = []
+        for src in EXACT_F64_SOURCES:
+            obj = os.path.join(tmp, os.path.splitext(src)[0] + ".o")
+            _run([*common, "--fmad=false", "-c", "-o", obj, os.path.join(CSRC, src)], verbose)
+            objects.append(obj)
+        _run([*common, "-shared", "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES],
+              *objects], verbose)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+def _run(cmd: list[str], verbose: bool) -> None:
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
         raise RuntimeError("nvcc failed building libmars_b200.so")
     if verbose:
         sys.stderr.write(res.stderr)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
 
 
 if __name__ == "__main__":

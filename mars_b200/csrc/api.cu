@@ -75,15 +75,16 @@ uint64_t node_key(uint32_t row, uint32_t col, uint32_t size, uint32_t shift) {
            ((uint64_t)shift << 48);
 }
 
-// Device waits are bounded: poll an event until it completes or the deadline passes.
-int sync_bounded(mars_ctx* ctx) {
+// Device waits are bounded: poll an event until it completes or the deadline passes.  The
+// work waited for is the context's stream's, or `stream`'s when one is given.
+int sync_bounded(mars_ctx* ctx, cudaStream_t stream = nullptr) {
     static const double limit_s = [] {
         const char* e = std::getenv("MARS_SYNC_TIMEOUT_S");
         return e ? std::atof(e) : 300.0;
     }();
     cudaEvent_t ev;
     MARS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    MARS_CUDA(cudaEventRecord(ev, ctx->stream));
+    MARS_CUDA(cudaEventRecord(ev, stream ? stream : ctx->stream));
     const auto t0 = std::chrono::steady_clock::now();
     for (;;) {
         const cudaError_t q = cudaEventQuery(ev);
@@ -783,9 +784,116 @@ int mars_search_nodes_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t wid
 
 namespace {
 
+// The RD walk's node pricing on the device (rdprice.cu): the batch's plane, rate table,
+// bases, nodes and candidates up, one launch per node size, the winners and levels down.
+// Where it runs: on the device when the residual mode is allowed (a forward and an inverse
+// DCT per node and candidate) or candidates are ranked; otherwise the host walk's per-node
+// fits (O(size^2) each) cost less than the batch's round trip.  MARS_PRICING=host or
+// =device pins either (the same price_node code, the same doubles).
+bool price_on_device_for(const mars_options& o) {
+    static const int pinned = [] {
+        const char* e = std::getenv("MARS_PRICING");
+        if (!e) return 0;
+        if (std::string(e) == "host") return 1;
+        if (std::string(e) == "device") return 2;
+        return 0;
+    }();
+    if (pinned) return pinned == 2;
+    return o.allowed_modes[3] != 0 || o.rd_candidates > 1;
+}
+
+// A stream of its own for one call, so concurrent encodes on a context do not wait behind
+// each other's searches; destroyed (after its queued work) when the call returns.
+struct OwnStream {
+    cudaStream_t st = nullptr;
+    ~OwnStream() {
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+int price_on_device(mars_ctx* ctx, mars::codec::PriceBatch& b) {
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    OwnStream own;
+    MARS_CUDA(cudaStreamCreateWithFlags(&own.st, cudaStreamNonBlocking));
+    const cudaStream_t st = own.st;
+    Scratch sc(st);
+    const size_t nodes = b.row.size();
+    const bool residual = b.setup.allowed[3] != 0;
+    size_t nbasis = 0;
+    for (uint32_t s : b.sizes) nbasis += (size_t)s * s;
+    uint8_t* d_px;
+    double *d_bits, *d_basis;
+    int64_t* d_off;
+    uint32_t *d_rows, *d_cols;
+    mars::price::Cand* d_cands;
+    uint64_t* d_lat;
+    mars::price::Priced* d_out;
+    int8_t* d_lev;
+    const size_t noff = (size_t)mars::price::kFields * mars::price::kCtx;
+    MARS_CUDA(sc.get(&d_px, (size_t)b.im.w * b.im.h));
+    MARS_CUDA(sc.get(&d_bits, b.nbits));
+    MARS_CUDA(sc.get(&d_off, noff));
+    MARS_CUDA(sc.get(&d_basis, nbasis));
+    MARS_CUDA(sc.get(&d_rows, nodes));
+    MARS_CUDA(sc.get(&d_cols, nodes));
+    MARS_CUDA(sc.get(&d_cands, b.cands.size()));
+    MARS_CUDA(sc.get(&d_lat, nodes));
+    MARS_CUDA(sc.get(&d_out, nodes));
+    MARS_CUDA(sc.get(&d_lev, residual ? b.nlevels : 1));
+    MARS_CUDA(cudaMemcpyAsync(d_px, b.im.px, (size_t)b.im.w * b.im.h, cudaMemcpyHostToDevice, st));
+    MARS_CUDA(cudaMemcpyAsync(d_bits, b.bits, b.nbits * sizeof(double), cudaMemcpyHostToDevice, st));
+    MARS_CUDA(cudaMemcpyAsync(d_off, b.offset, noff * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    MARS_CUDA(cudaMemcpyAsync(d_rows, b.row.data(), nodes * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    MARS_CUDA(cudaMemcpyAsync(d_cols, b.col.data(), nodes * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    MARS_CUDA(cudaMemcpyAsync(d_cands, b.cands.data(), b.cands.size() * sizeof(mars::price::Cand),
+                              cudaMemcpyHostToDevice, st));
+    if (residual)
+        MARS_CUDA(cudaMemcpyAsync(d_lat, b.levels_at.data(), nodes * sizeof(uint64_t),
+                                  cudaMemcpyHostToDevice, st));
+    size_t at = 0;
+    for (size_t g = 0; g < b.sizes.size(); ++g) {
+        const size_t n = (size_t)b.sizes[g] * b.sizes[g];
+        MARS_CUDA(cudaMemcpyAsync(d_basis + at, b.basis[g], n * sizeof(double),
+                                  cudaMemcpyHostToDevice, st));
+        at += n;
+    }
+    at = 0;
+    for (size_t g = 0; g < b.sizes.size(); ++g) {
+        const uint32_t size = b.sizes[g], first = b.first[g], count = b.first[g + 1] - first;
+        mars::PriceLaunch a{};
+        a.px = d_px;
+        a.stride = b.im.w;
+        a.size = size;
+        a.count = count;
+        a.rows = d_rows + first;
+        a.cols = d_cols + first;
+        a.cands = d_cands + (size_t)first * b.k;
+        a.k = b.k;
+        a.setup = b.setup;
+        a.table = {d_bits, d_off};
+        a.basis = d_basis + at;
+        a.out = d_out + first;
+        a.levels = d_lev;
+        a.levels_at = d_lat + first;
+        const size_t gbytes = mars::price_scratch_bytes(size, count, &a.scratch_slots);
+        if (gbytes) MARS_CUDA(sc.get(&a.global_scratch, gbytes));
+        MARS_CUDA(mars::launch_price_nodes(a, st));
+        ctx->launches += 1;
+        at += (size_t)size * size;
+    }
+    b.priced.resize(nodes);
+    MARS_CUDA(cudaMemcpyAsync(b.priced.data(), d_out, nodes * sizeof(mars::price::Priced),
+                              cudaMemcpyDeviceToHost, st));
+    if (residual) {
+        b.levels.resize(b.nlevels);
+        MARS_CUDA(cudaMemcpyAsync(b.levels.data(), d_lev, b.nlevels, cudaMemcpyDeviceToHost, st));
+    }
+    return sync_bounded(ctx, st);
+}
+
 // The walks of encode_image_with_search over filled tables (`table` for the final walk,
 // `warm` for the RD warm-up), and the C-ABI outputs.
-int encode_on_tables(const uint8_t* plane, uint32_t width, uint32_t height,
+int encode_on_tables(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
                      const mars_params* params, const mars_options* options, mars_table* table,
                      mars_table* warm, uint32_t rd_k, mars_header* header, mars_leaf** leaves,
                      size_t* nleaves, int32_t** residuals, size_t* nresiduals,
@@ -812,8 +920,12 @@ int encode_on_tables(const uint8_t* plane, uint32_t width, uint32_t height,
     std::vector<mars_leaf> out;
     std::vector<int32_t> res;
     const mars::codec::Image im{plane, width, height};
+    const mars::codec::Pricer pricer = [ctx](mars::codec::PriceBatch& b) {
+        return price_on_device(ctx, b);
+    };
     if (int e = mars::codec::encode(im, *params, *options, provider, warmup, header, &out, &res,
-                                    counters, rd_k > 1 ? &ranked : nullptr))
+                                    counters, rd_k > 1 ? &ranked : nullptr,
+                                    price_on_device_for(*options) ? &pricer : nullptr))
         return e;
     *nleaves = out.size();
     *leaves = (mars_leaf*)std::malloc(std::max<size_t>(1, out.size()) * sizeof(mars_leaf));
@@ -867,7 +979,7 @@ int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t he
         if (int e = build_table(ctx, plane, nullptr, width, height, &wp, false, &warm)) return e;
     }
     std::unique_ptr<mars_table, void (*)(mars_table*)> wguard(warm, mars_search_table_free);
-    return encode_on_tables(plane, width, height, params, options, table, warm ? warm : table,
+    return encode_on_tables(ctx, plane, width, height, params, options, table, warm ? warm : table,
                             rd_k, header, leaves, nleaves, residuals, nresiduals, counters);
 }
 
@@ -1102,7 +1214,7 @@ int mars_encode_planned(mars_search_plan* plan, const uint8_t* plane,
     mars_table* table = nullptr;
     if (int e = mars_search_plan_run(plan, plane, &table)) return e;
     std::unique_ptr<mars_table, void (*)(mars_table*)> guard(table, mars_search_table_free);
-    return encode_on_tables(plane, plan->w, plan->h, &plan->params, options, table, table, 1,
+    return encode_on_tables(plan->ctx, plane, plan->w, plan->h, &plan->params, options, table, table, 1,
                             header, leaves, nleaves, residuals, nresiduals, counters);
 }
 

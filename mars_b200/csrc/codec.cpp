@@ -6,6 +6,10 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <functional>
+#include <mutex>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -197,6 +201,8 @@ struct Ctx {
     int status = MARS_OK;
     const RankedProvider* ranked = nullptr;  // search_candidates, when rd_candidates > 1
     uint32_t rd_candidates = 1;
+    const struct HostRates* table = nullptr;     // the snapshot as a bits table
+    const struct PricedNodes* priced = nullptr;  // the nodes priced in one batch, if any
 };
 
 mars_leaf make_leaf(uint32_t row, uint32_t col, uint32_t size) {
@@ -284,65 +290,78 @@ WalkResult walk(Ctx& ctx, uint32_t row, uint32_t col, uint32_t size) {
     return r;
 }
 
-// affine_fit (encode.rs:1724-1781).
-void affine_fit(const std::vector<double>& block, uint32_t size, uint32_t bits_beta,
-                uint32_t* qbeta_out, int32_t* qgx_out, int32_t* qgy_out, double* sse_out) {
-    const double n = (double)size * (double)size;
-    double t0 = 0.0, tu = 0.0, tv = 0.0;
-    for (uint32_t u = 0; u < size; ++u)
-        for (uint32_t v = 0; v < size; ++v) {
-            const double p = block[u * size + v];
-            t0 += p;
-            tu += p * (double)u;
-            tv += p * (double)v;
+// The pricing of one node runs price::price_node (price.hpp), the code the device pricing
+// kernel runs too.  HostRates holds the frozen snapshot as its bits table.
+struct HostRates {
+    std::vector<double> bits;
+    std::vector<int64_t> offset;
+    price::RateTable view() const { return {bits.data(), offset.data()}; }
+};
+
+// Every (field, context) best_mode_leaf can price for nodes up to max_size: the snapshot's
+// model where it has one, else a fresh model of the field's alphabet (RateModels::bits_for).
+HostRates build_rate_table(const RateModels& rate, const mars_header& hdr, uint32_t max_size) {
+    HostRates t;
+    t.offset.assign((size_t)price::kFields * price::kCtx, -1);
+    const uint32_t sc_max = std::min<uint32_t>(size_class_of(std::max<uint32_t>(max_size, 1)),
+                                               price::kSizeClasses - 1);
+    auto alphabet_of = [&](uint32_t field) -> uint32_t {
+        switch (field) {
+            case price::F_SPLIT: return 2;
+            case price::F_MODE: return MODE_ALPHABET;
+            case price::F_QALFA: return (1u << hdr.bits_alfa) - 1;
+            case price::F_QBETA:
+            case price::F_QBETA_DC: return 1u << hdr.bits_beta;
+            case price::F_ISOMETRY: return 8;
+            case price::F_DOM_ROW: return (uint32_t)(2 * (1ll << bits_coord_row(hdr)));
+            case price::F_DOM_COL: return (uint32_t)(2 * (1ll << bits_coord_col(hdr)));
+            case price::F_GX:
+            case price::F_GY: return (uint32_t)(2 * (int64_t)AFFINE_GRAD_CLAMP + 1);
+            case price::F_RESID_NZ: return 2;
+            default: return (uint32_t)(2 * price::kLevelClamp + 1);
         }
-    double su = -0.0, suu = -0.0;
-    for (uint32_t u = 0; u < size; ++u) su += (double)u;
-    for (uint32_t u = 0; u < size; ++u) suu += (double)u * (double)u;
-    const double s0 = n, s_u = (double)size * su, s_v = s_u, s_uu = (double)size * suu,
-                 s_vv = s_uu, s_uv = su * su;
-    auto det3 = [](const double m[3][3]) {
-        return m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
-               m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
-               m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
     };
-    const double a[3][3] = {{s0, s_u, s_v}, {s_u, s_uu, s_uv}, {s_v, s_uv, s_vv}};
-    const double det_a = det3(a);
-    double b0, gx, gy;
-    if (std::fabs(det_a) < 1e-9) {
-        b0 = t0 / s0;
-        gx = 0.0;
-        gy = 0.0;
-    } else {
-        const double a_b0[3][3] = {{t0, s_u, s_v}, {tu, s_uu, s_uv}, {tv, s_uv, s_vv}};
-        const double a_gx[3][3] = {{s0, t0, s_v}, {s_u, tu, s_uv}, {s_v, tv, s_vv}};
-        const double a_gy[3][3] = {{s0, s_u, t0}, {s_u, s_uu, tu}, {s_v, s_uv, tv}};
-        b0 = det3(a_b0) / det_a;
-        gx = det3(a_gx) / det_a;
-        gy = det3(a_gy) / det_a;
+    std::map<uint32_t, int64_t> fresh;  // alphabet -> where its fresh model's bits start
+    auto add = [&](uint32_t field, uint32_t ctx) {
+        int64_t& at = t.offset[(size_t)field * price::kCtx + ctx];
+        auto it = rate.models.find({(uint8_t)field, ctx});
+        if (it != rate.models.end()) {
+            at = (int64_t)t.bits.size();
+            t.bits.resize(t.bits.size() + it->second.counts.size());
+            it->second.all_bits(t.bits.data() + at);
+            return;
+        }
+        // Contexts without a model share one table per alphabet.
+        const uint32_t a = std::max<uint32_t>(alphabet_of(field), 2);
+        auto f = fresh.find(a);
+        if (f == fresh.end()) {
+            f = fresh.emplace(a, (int64_t)t.bits.size()).first;
+            t.bits.resize(t.bits.size() + a);
+            AdaptiveModel(a).all_bits(t.bits.data() + f->second);
+        }
+        at = f->second;
+    };
+    for (uint32_t sc = 0; sc <= sc_max; ++sc) {
+        for (uint32_t field = 0; field < price::F_RESID_NZ; ++field) add(field, sc);
+        for (uint32_t band = 0; band < price::kBands; ++band) {
+            add(price::F_RESID_NZ, sc * price::kBands + band);
+            add(price::F_RESID_MAG, sc * price::kBands + band);
+        }
     }
-    const uint32_t max_qbeta = (1u << bits_beta) - 1;
-    const uint32_t qbeta = quantise_f64(std::max(b0 / 255.0 * (double)max_qbeta, 0.0), max_qbeta);
-    auto qgrad = [](double g) {
-        double r = std::round(g * AFFINE_GRAD_SCALE);
-        if (r < -(double)AFFINE_GRAD_CLAMP) r = -(double)AFFINE_GRAD_CLAMP;
-        if (r > (double)AFFINE_GRAD_CLAMP) r = (double)AFFINE_GRAD_CLAMP;
-        return (int32_t)r;
-    };
-    const int32_t qgx = qgrad(gx), qgy = qgrad(gy);
-    const double b0q = (double)qbeta / (double)max_qbeta * 255.0;
-    const double gxq = (double)qgx / AFFINE_GRAD_SCALE, gyq = (double)qgy / AFFINE_GRAD_SCALE;
-    double sse = 0.0;
-    for (uint32_t u = 0; u < size; ++u)
-        for (uint32_t v = 0; v < size; ++v) {
-            const double pred = b0q + gxq * (double)u + gyq * (double)v;
-            const double diff = block[u * size + v] - pred;
-            sse += diff * diff;
-        }
-    *qbeta_out = qbeta;
-    *qgx_out = qgx;
-    *qgy_out = qgy;
-    *sse_out = sse;
+    return t;
+}
+
+price::Setup make_setup(const mars_header& hdr, const mars_params& p, const uint8_t allowed[4],
+                        double lambda) {
+    price::Setup s;
+    s.bits_alfa = p.bits_alfa;
+    s.max_alfa = p.max_alfa;
+    s.bits_beta = hdr.bits_beta;
+    s.shift = hdr.shift;
+    s.qstep = qstep_of(hdr);
+    s.lambda = lambda;
+    for (int m = 0; m < 4; ++m) s.allowed[m] = allowed[m];
+    return s;
 }
 
 struct Priced {
@@ -351,127 +370,91 @@ struct Priced {
     std::vector<int32_t> levels;  // mode 3
 };
 
-// residual_for_candidate (encode.rs:1783-1851): the mode-2 prediction's error in
-// domain-local (u, v) order, forward DCT, dead-zone quantised and clamped, then priced by
-// the SSE of the pixels the decoder will produce.
-std::vector<int32_t> residual_for_candidate(const Ctx& ctx, const std::vector<double>& block,
-                                            uint32_t size, const mars_candidate& c,
-                                            double* sse_out) {
-    const mars_header& hdr = ctx.hdr;
-    const double alfa = (double)c.qalfa / (double)(1u << ctx.params.bits_alfa) * ctx.params.max_alfa;
-    double beta = (double)c.qbeta / (double)((1u << hdr.bits_beta) - 1) *
-                  ((1.0 + std::fabs(alfa)) * 255.0);
-    if (alfa > 0.0) beta -= alfa * 255.0;
-    const size_t n = (size_t)size * size;
-    std::vector<double> resid(n), prediction(n);
-    for (uint32_t u = 0; u < size; ++u)
-        for (uint32_t v = 0; v < size; ++v) {
-            const uint32_t dr = c.dom_row + 2 * u, dc = c.dom_col + 2 * v;
-            const double d = ((double)pixel_at(ctx.im, dr, dc) + (double)pixel_at(ctx.im, dr + 1, dc) +
-                              (double)pixel_at(ctx.im, dr, dc + 1) +
-                              (double)pixel_at(ctx.im, dr + 1, dc + 1)) /
-                             4.0;
-            uint32_t i, j;
-            iso_map(c.isometry, u, v, size, &i, &j);
-            const double pred = 0.5 + d * alfa + beta;
-            prediction[u * size + v] = pred;
-            resid[u * size + v] = block[i * size + j] - pred;
-        }
-    const std::vector<double> coeffs = residual::forward_dct2d(resid, size);
-    const double step = qstep_of(hdr);
-    std::vector<int32_t> levels(n);
-    std::vector<double> deq(n);
-    for (size_t k = 0; k < n; ++k) {
-        int32_t l = residual::dead_zone_quantize(coeffs[k], step, residual::kDeadZone);
-        if (l < -residual::kLevelClamp) l = -residual::kLevelClamp;
-        if (l > residual::kLevelClamp) l = residual::kLevelClamp;
-        levels[k] = l;
-        deq[k] = residual::dead_zone_dequantize(l, step, residual::kDeadZone);
+// The transposed basis (bt[i * n + k] = basis(n, k, i)) the forward transform's row pass
+// reads; cached per thread.
+const double* basis_t(uint32_t n) {
+    thread_local std::map<uint32_t, std::vector<double>> cache;
+    auto it = cache.find(n);
+    if (it == cache.end()) {
+        const std::vector<double>& b = residual::basis(n);
+        std::vector<double> t((size_t)n * n);
+        for (uint32_t k = 0; k < n; ++k)
+            for (uint32_t i = 0; i < n; ++i) t[(size_t)i * n + k] = b[(size_t)k * n + i];
+        it = cache.emplace(n, std::move(t)).first;
     }
-    const std::vector<double> recon = residual::inverse_dct2d(deq, size);
-    double sse = 0.0;
-    for (uint32_t u = 0; u < size; ++u)
-        for (uint32_t v = 0; v < size; ++v) {
-            const size_t k = u * size + v;
-            uint32_t i, j;
-            iso_map(c.isometry, u, v, size, &i, &j);
-            double pv = prediction[k] + recon[k];
-            if (pv < 0.0) pv = 0.0;
-            if (pv > 255.0) pv = 255.0;
-            const double diff = block[i * size + j] - (double)(uint8_t)pv;
-            sse += diff * diff;
-        }
-    *sse_out = sse;
-    return levels;
+    return it->second.data();
 }
 
-// best_mode_leaf (encode.rs:1536-1714), modes 0-3 over the provider's ranked list (the
-// single winner unless rd_candidates > 1); candidates with qalfa < 1 are skipped.
+price::Cand to_cand(const mars_candidate& c) {
+    return {c.dom_row, c.dom_col, c.isometry, c.qalfa, c.qbeta, c.valid, c.rms};
+}
+
+// best_mode_leaf (encode.rs:1536-1714) on the host: price::price_node as a team of one
+// lane with thread-local scratch.
 Priced best_mode_leaf(const Ctx& ctx, uint32_t row, uint32_t col, uint32_t size,
                       const mars_candidate* ranked, size_t nranked, double lambda, uint32_t sc) {
-    const mars_header& hdr = ctx.hdr;
-    std::vector<double> block((size_t)size * size);
-    int64_t rsum = 0;
-    for (uint32_t i = 0; i < size; ++i)
-        for (uint32_t j = 0; j < size; ++j) {
-            const uint32_t v = pixel_at(ctx.im, row + i, col + j);
-            block[i * size + j] = (double)v;
-            rsum += v;
-        }
-    const int64_t s0 = (int64_t)size * size;
-    std::vector<Priced> cands;
-    auto mode0 = [&]() {
-        mars_leaf l = make_leaf(row, col, size);
-        l.qbeta = best_beta(rsum, s0, hdr.bits_beta);
-        const double beta2 = (double)l.qbeta / (double)((1u << hdr.bits_beta) - 1) * 255.0;
-        double sse = -0.0;
-        for (double p : block) sse += (p - beta2) * (p - beta2);
-        cands.push_back({l, sse, leaf_bits(*ctx.rate, hdr, l, sc), {}});
-    };
-    if (ctx.allowed[0]) mode0();
-    if (ctx.allowed[1]) {
-        mars_leaf l = make_leaf(row, col, size);
-        l.mode = 1;
-        double sse;
-        affine_fit(block, size, hdr.bits_beta, &l.qbeta, &l.qgx, &l.qgy, &sse);
-        cands.push_back({l, sse, leaf_bits(*ctx.rate, hdr, l, sc), {}});
-    }
-    for (size_t ci = 0; ci < nranked; ++ci) {
-        const mars_candidate& c = ranked[ci];
-        if (!c.valid || c.qalfa < 1) continue;
-        if (ctx.allowed[2]) {
-            mars_leaf l = make_leaf(row, col, size);
-            l.mode = 2;
-            l.qalfa = c.qalfa;
-            l.qbeta = c.qbeta;
-            l.isometry = c.isometry;
-            l.dom_row = c.dom_row;
-            l.dom_col = c.dom_col;
-            const double sse2 = c.rms * c.rms * (double)size * (double)size;
-            cands.push_back({l, sse2, leaf_bits(*ctx.rate, hdr, l, sc), {}});
-        }
-        if (!ctx.allowed[3]) continue;
-        mars_leaf l = make_leaf(row, col, size);
-        l.mode = 3;
-        l.qalfa = c.qalfa;
-        l.qbeta = c.qbeta;
-        l.isometry = c.isometry;
-        l.dom_row = c.dom_row;
-        l.dom_col = c.dom_col;
-        double sse3;
-        std::vector<int32_t> levels = residual_for_candidate(ctx, block, size, c, &sse3);
-        const double r3 = leaf_bits(*ctx.rate, hdr, l, sc, levels.data());
-        cands.push_back({l, sse3, r3, std::move(levels)});
-    }
-    if (cands.empty()) mode0();
-    size_t best = 0;
-    for (size_t i = 1; i < cands.size(); ++i) {
-        const double jb = cands[best].d + lambda * cands[best].r;
-        const double ji = cands[i].d + lambda * cands[i].r;
-        if (ji < jb) best = i;
-    }
-    return std::move(cands[best]);
+    thread_local std::vector<double> dscr;
+    thread_local std::vector<int32_t> iscr;
+    const size_t n = (size_t)size * size;
+    if (dscr.size() < 5 * n) dscr.resize(5 * n);
+    if (iscr.size() < 2 * n) iscr.resize(2 * n);
+    price::Scratch s{dscr.data(), dscr.data() + n, dscr.data() + 2 * n, dscr.data() + 3 * n,
+                     dscr.data() + 4 * n, iscr.data(), iscr.data() + n};
+    thread_local std::vector<price::Cand> cands;
+    cands.resize(nranked);
+    for (size_t i = 0; i < nranked; ++i) cands[i] = to_cand(ranked[i]);
+    const price::Setup setup = make_setup(ctx.hdr, ctx.params, ctx.allowed, lambda);
+    const price::RateTable view = ctx.table->view();
+    const price::Priced p =
+        price::price_node(ctx.im.px, ctx.im.w, row, col, size, cands.data(), (uint32_t)nranked,
+                          setup, view, residual::basis(size).data(), basis_t(size), sc, s, {0, 1});
+    Priced out{p.leaf, p.d, p.r, {}};
+    if (p.has_levels) out.levels.assign(s.best_levels, s.best_levels + n);
+    return out;
 }
+
+// A pricer's answers for the RD walk: node (row, col, size) -> its entry in the batch,
+// through one dense grid per node size.
+struct PricedNodes {
+    const PriceBatch* batch = nullptr;
+    std::vector<uint32_t> sizes, cols;
+    std::vector<size_t> base;
+    std::vector<int64_t> at;  // grid cell -> batch index, -1 when absent
+    void build(const PriceBatch& b) {
+        batch = &b;
+        size_t total = 0;
+        for (uint32_t s : b.sizes) {
+            const uint32_t c = (b.im.w + s - 1) / s, r = (b.im.h + s - 1) / s;
+            sizes.push_back(s);
+            cols.push_back(c);
+            base.push_back(total);
+            total += (size_t)c * r;
+        }
+        at.assign(total, -1);
+        for (size_t g = 0; g < b.sizes.size(); ++g)
+            for (uint32_t i = b.first[g]; i < b.first[g + 1]; ++i)
+                at[base[g] + (size_t)(b.row[i] / sizes[g]) * cols[g] + b.col[i] / sizes[g]] = i;
+    }
+    bool get(uint32_t row, uint32_t col, uint32_t size, Priced* out, uint64_t* evals) const {
+        for (size_t g = 0; g < sizes.size(); ++g) {
+            if (sizes[g] != size) continue;
+            const int64_t i = at[base[g] + (size_t)(row / size) * cols[g] + col / size];
+            if (i < 0 || batch->row[i] != row || batch->col[i] != col) return false;
+            const price::Priced& p = batch->priced[i];
+            *evals = batch->evals[i];
+            out->leaf = p.leaf;
+            out->d = p.d;
+            out->r = p.r;
+            out->levels.clear();
+            if (p.has_levels) {
+                const int8_t* l = batch->levels.data() + batch->levels_at[i];
+                out->levels.assign(l, l + (size_t)size * size);
+            }
+            return true;
+        }
+        return false;
+    }
+};
 
 struct RdResult {
     std::vector<mars_leaf> leaves;
@@ -521,25 +504,34 @@ RdResult walk_rd(Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, double lam
         return r;
     }
     const double node_lambda = lambda * 1.0;
-    const uint32_t shift = ctx.adaptive_density
-                               ? adaptive_shift(ctx.params.shift, block_rms(ctx.im, row, col, size))
-                               : ctx.params.shift;
-    // rd_candidates == 1 keeps the single-winner search(); above 1 the ranked list widens
-    // modes 2/3's competition (encode.rs:1946-1977).
     SearchAnswer ans;
-    std::vector<mars_candidate> ranked;
-    int st;
-    if (ctx.rd_candidates > 1 && ctx.ranked) {
-        st = (*ctx.ranked)(row, col, size, shift, ctx.rd_candidates, &ranked, &ans.evals);
+    Priced leaf;
+    if (ctx.priced) {
+        // Priced in one batch beforehand, with the provider's answer for this node.
+        if (!ctx.priced->get(row, col, size, &leaf, &ans.evals)) {
+            ctx.status = MARS_ENOTFOUND;
+            return {};
+        }
     } else {
-        st = (*ctx.provider)(row, col, size, shift, &ans);
-        if (!st && ans.cand.valid) ranked.push_back(ans.cand);
+        const uint32_t shift =
+            ctx.adaptive_density ? adaptive_shift(ctx.params.shift, block_rms(ctx.im, row, col, size))
+                                 : ctx.params.shift;
+        // rd_candidates == 1 keeps the single-winner search(); above 1 the ranked list widens
+        // modes 2/3's competition (encode.rs:1946-1977).
+        std::vector<mars_candidate> ranked;
+        int st;
+        if (ctx.rd_candidates > 1 && ctx.ranked) {
+            st = (*ctx.ranked)(row, col, size, shift, ctx.rd_candidates, &ranked, &ans.evals);
+        } else {
+            st = (*ctx.provider)(row, col, size, shift, &ans);
+            if (!st && ans.cand.valid) ranked.push_back(ans.cand);
+        }
+        if (st) {
+            ctx.status = st;
+            return {};
+        }
+        leaf = best_mode_leaf(ctx, row, col, size, ranked.data(), ranked.size(), node_lambda, sc);
     }
-    if (st) {
-        ctx.status = st;
-        return {};
-    }
-    Priced leaf = best_mode_leaf(ctx, row, col, size, ranked.data(), ranked.size(), node_lambda, sc);
     if (size <= hdr.min_size) {
         RdResult r;
         r.leaves.push_back(leaf.leaf);
@@ -727,6 +719,70 @@ unsigned host_threads() {
 }
 
 // Runs fn(i) for i in [0, n) on up to host_threads() threads (dynamic assignment).
+// A process-wide pool of host workers that parallel_for calls share (threads are started
+// once, not per walk).  The calling thread works on its own call's items too, so every call
+// finishes even while all workers serve other calls; a call takes at most `max_helpers`
+// workers.
+class HostPool {
+public:
+    static HostPool& get() {
+        static HostPool* pool = new HostPool();  // never destroyed: workers outlive main()
+        return *pool;
+    }
+    void run(size_t n, unsigned max_helpers, const std::function<void(size_t)>& fn) {
+        Job job{&fn, n, max_helpers};
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            jobs_.push_back(&job);
+        }
+        cv_.notify_all();
+        work(job);
+        std::unique_lock<std::mutex> lk(mu_);
+        auto it = std::find(jobs_.begin(), jobs_.end(), &job);
+        if (it != jobs_.end()) jobs_.erase(it);
+        done_.wait(lk, [&] { return job.helpers == 0; });
+    }
+
+private:
+    struct Job {
+        const std::function<void(size_t)>* fn;
+        size_t n;
+        unsigned max_helpers;
+        std::atomic<size_t> next{0};
+        unsigned helpers = 0;  // guarded by mu_
+    };
+    static void work(Job& j) {
+        for (size_t i; (i = j.next.fetch_add(1)) < j.n;) (*j.fn)(i);
+    }
+    HostPool() {
+        const unsigned hc = std::max(1u, std::thread::hardware_concurrency());
+        for (unsigned t = 1; t < hc; ++t) std::thread([this] { loop(); }).detach();
+    }
+    // The first queued job with items left and room for a helper; exhausted jobs leave the
+    // queue (their callers wait for the helpers still on them).
+    Job* eligible() {
+        while (!jobs_.empty() && jobs_.front()->next.load() >= jobs_.front()->n) jobs_.pop_front();
+        for (Job* j : jobs_)
+            if (j->next.load() < j->n && j->helpers < j->max_helpers) return j;
+        return nullptr;
+    }
+    void loop() {
+        std::unique_lock<std::mutex> lk(mu_);
+        for (;;) {
+            Job* j;
+            cv_.wait(lk, [&] { return (j = eligible()) != nullptr; });
+            ++j->helpers;
+            lk.unlock();
+            work(*j);
+            lk.lock();
+            if (--j->helpers == 0) done_.notify_all();
+        }
+    }
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    std::deque<Job*> jobs_;
+};
+
 template <class F>
 void parallel_for(size_t n, F&& fn) {
     const unsigned nt = (unsigned)std::min<size_t>(host_threads(), n);
@@ -734,15 +790,8 @@ void parallel_for(size_t n, F&& fn) {
         for (size_t i = 0; i < n; ++i) fn(i);
         return;
     }
-    std::atomic<size_t> next{0};
-    auto worker = [&] {
-        for (size_t i; (i = next.fetch_add(1)) < n;) fn(i);
-    };
-    std::vector<std::thread> pool;
-    pool.reserve(nt - 1);
-    for (unsigned t = 1; t < nt; ++t) pool.emplace_back(worker);
-    worker();
-    for (auto& t : pool) t.join();
+    const std::function<void(size_t)> f = [&fn](size_t i) { fn(i); };
+    HostPool::get().run(n, nt - 1, f);
 }
 
 // walk / walk_rd over the whole plane, root subtrees in parallel; the first failing root's
@@ -784,10 +833,102 @@ int walk_rd_all(const Ctx& base, double lambda, RdResult* out) {
     return MARS_OK;
 }
 
+// The nodes walk_rd prices (every in-plane, unforced node of more than one pixel down to
+// min_size) below one root, with the candidates walk_rd asks its provider for.
+struct NodeList {
+    std::vector<uint32_t> row, col, size;
+    std::vector<price::Cand> cands;  // k per node
+    std::vector<uint64_t> evals;
+};
+void collect_priced(Ctx& ctx, uint32_t row, uint32_t col, uint32_t size, uint32_t k,
+                    NodeList& out) {
+    const mars_header& hdr = ctx.hdr;
+    if (ctx.status || row >= hdr.height || col >= hdr.width || size < 2) return;
+    const bool forced = size > hdr.max_size || row + size > hdr.height || col + size > hdr.width;
+    if (!forced) {
+        const uint32_t shift = ctx.adaptive_density
+                                   ? adaptive_shift(ctx.params.shift, block_rms(ctx.im, row, col, size))
+                                   : ctx.params.shift;
+        thread_local std::vector<mars_candidate> ranked;
+        ranked.clear();
+        uint64_t evals = 0;
+        int st;
+        if (ctx.rd_candidates > 1 && ctx.ranked) {
+            st = (*ctx.ranked)(row, col, size, shift, ctx.rd_candidates, &ranked, &evals);
+        } else {
+            SearchAnswer ans;
+            st = (*ctx.provider)(row, col, size, shift, &ans);
+            if (!st && ans.cand.valid) ranked.push_back(ans.cand);
+            evals = ans.evals;
+        }
+        if (st) {
+            ctx.status = st;
+            return;
+        }
+        const price::Cand none{0, 0, 0, 0, 0, 0, 0.0};
+        for (uint32_t i = 0; i < k; ++i)
+            out.cands.push_back(i < ranked.size() ? to_cand(ranked[i]) : none);
+        out.row.push_back(row);
+        out.col.push_back(col);
+        out.size.push_back(size);
+        out.evals.push_back(evals);
+        if (size <= hdr.min_size) return;
+    }
+    const uint32_t half = size / 2;
+    collect_priced(ctx, row, col, half, k, out);
+    collect_priced(ctx, row + half, col, half, k, out);
+    collect_priced(ctx, row, col + half, half, k, out);
+    collect_priced(ctx, row + half, col + half, half, k, out);
+}
+
+// Fills a PriceBatch with every node of the RD walk (grouped by size, largest first; roots
+// in walk order within a group) and runs the pricer on it.
+int price_all(const Ctx& base, double lambda, const Pricer& pricer, PriceBatch* batch) {
+    const uint32_t k = base.rd_candidates > 1 && base.ranked ? base.rd_candidates : 1;
+    std::vector<Root> roots;
+    collect_roots(base.hdr, 0, 0, virtual_size(base.hdr), &roots);
+    std::vector<NodeList> lists(roots.size());
+    std::vector<int> status(roots.size(), MARS_OK);
+    parallel_for(roots.size(), [&](size_t i) {
+        Ctx ctx = base;
+        collect_priced(ctx, roots[i].row, roots[i].col, roots[i].size, k, lists[i]);
+        status[i] = ctx.status;
+    });
+    for (int st : status)
+        if (st) return st;
+    PriceBatch& b = *batch;
+    b.im = base.im;
+    b.setup = make_setup(base.hdr, base.params, base.allowed, lambda * 1.0);
+    b.bits = base.table->bits.data();
+    b.nbits = base.table->bits.size();
+    b.offset = base.table->offset.data();
+    b.k = k;
+    for (uint32_t size = virtual_size(base.hdr); size >= 2; size /= 2) {
+        const uint32_t start = (uint32_t)b.row.size();
+        for (const NodeList& l : lists)
+            for (size_t i = 0; i < l.row.size(); ++i) {
+                if (l.size[i] != size) continue;
+                b.row.push_back(l.row[i]);
+                b.col.push_back(l.col[i]);
+                b.cands.insert(b.cands.end(), l.cands.begin() + i * k, l.cands.begin() + (i + 1) * k);
+                b.evals.push_back(l.evals[i]);
+                b.levels_at.push_back(b.nlevels);
+                b.nlevels += (uint64_t)size * size;
+            }
+        if (b.row.size() == start) continue;
+        b.sizes.push_back(size);
+        b.first.push_back(start);
+        b.basis.push_back(residual::basis(size).data());
+    }
+    b.first.push_back((uint32_t)b.row.size());
+    if (b.row.empty()) return MARS_OK;
+    return pricer(b);
+}
+
 int encode(const Image& im, const mars_params& p, const mars_options& o, const Provider& provider,
            const Provider& warmup, mars_header* hdr_out, std::vector<mars_leaf>* leaves,
            std::vector<int32_t>* residuals, mars_counters* counters,
-           const RankedProvider* ranked) {
+           const RankedProvider* ranked, const Pricer* pricer) {
     mars_header hdr = build_header(im.w, im.h, p);
     // encode.rs:1066-1071: LambdaAdaptive -> from_lambda (8 without lambda); Fixed(step).
     if (o.residual_adaptive)
@@ -812,6 +953,15 @@ int encode(const Image& im, const mars_params& p, const mars_options& o, const P
                 o.adaptive_density != 0};
         ctx.ranked = ranked;
         ctx.rd_candidates = std::max<uint32_t>(1, o.rd_candidates);
+        const HostRates rates = build_rate_table(rate, hdr, p.max_size);
+        ctx.table = &rates;
+        PriceBatch batch;
+        PricedNodes priced;
+        if (pricer) {
+            if (int st = price_all(ctx, p.lambda, *pricer, &batch)) return st;
+            priced.build(batch);
+            ctx.priced = &priced;
+        }
         RdResult rr;
         if (int st = walk_rd_all(ctx, p.lambda, &rr)) return st;
         *leaves = std::move(rr.leaves);

@@ -13,6 +13,7 @@
 
 #include "../../include/mars_b200.h"
 #include "entropy.hpp"
+#include "price.hpp"
 
 namespace mars {
 namespace codec {
@@ -38,6 +39,32 @@ struct Image {
     uint32_t w, h;
 };
 
+// Every node the RD walk prices (best_mode_leaf, encode.rs:1536-1714), handed in one batch
+// to a pricer that runs price::price_node elsewhere (the device) before the walk reads the
+// answers.  Nodes are grouped by size, largest first (group g is [first[g], first[g+1]) of
+// size sizes[g], DCT basis basis[g]); each node has k candidates (invalid ones pad a short
+// list).  The pricer fills `priced` (one per node) and, when mode 3 is allowed, `levels`
+// (size*size per node at levels_at[i], written for nodes whose winner is mode 3; the levels
+// fit int8).
+struct PriceBatch {
+    Image im;
+    price::Setup setup;
+    const double* bits;
+    size_t nbits;
+    const int64_t* offset;  // price::kFields * price::kCtx entries
+    uint32_t k;
+    std::vector<uint32_t> sizes, first;
+    std::vector<const double*> basis;
+    std::vector<uint32_t> row, col;
+    std::vector<price::Cand> cands;
+    std::vector<uint64_t> evals;  // the provider's evals for the node
+    std::vector<uint64_t> levels_at;
+    uint64_t nlevels = 0;
+    std::vector<price::Priced> priced;
+    std::vector<int8_t> levels;
+};
+using Pricer = std::function<int(PriceBatch& batch)>;
+
 uint32_t quantise_f64(double x, uint32_t max);
 uint32_t best_beta(int64_t range_sum, int64_t pixel_count, uint32_t bits_beta);
 mars_header build_header(uint32_t w, uint32_t h, const mars_params& p);
@@ -51,10 +78,12 @@ uint32_t adaptive_shift(uint32_t base, double rms);
 // (build_rate_snapshot searches exhaustively whatever the provider is); `provider` answers
 // the final walk.
 // `ranked` answers the final walk's search_candidates when o.rd_candidates > 1.
+// `pricer`, when given, prices the RD walk's nodes in one batch; without it the walk prices
+// each node on the host as it reaches it (the same price::price_node, the same doubles).
 int encode(const Image& im, const mars_params& p, const mars_options& o, const Provider& provider,
            const Provider& warmup, mars_header* hdr, std::vector<mars_leaf>* leaves,
            std::vector<int32_t>* residuals, mars_counters* counters,
-           const RankedProvider* ranked = nullptr);
+           const RankedProvider* ranked = nullptr, const Pricer* pricer = nullptr);
 
 // The residual step of a header as f64 (ResidualQstep::get, quant.rs:54-56); 0 in the
 // struct stands for the default step 8.

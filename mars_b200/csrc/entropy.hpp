@@ -66,6 +66,17 @@ struct AdaptiveModel {
         left_and_prob(s, &left, &prob);
         return -std::log2((double)prob / (double)kPrecisionTotal);
     }
+    // bits_for of every symbol, with one running prefix: the same (left, prob) pairs and
+    // the same doubles as calling bits_for symbol by symbol.
+    void all_bits(double* out) const {
+        uint64_t before = 0;
+        for (uint32_t s = 0; s < (uint32_t)counts.size(); ++s) {
+            const uint32_t l = scaled(before) + s;
+            const uint32_t r = scaled(before + counts[s]) + s + 1;
+            out[s] = -std::log2((double)(r - l) / (double)kPrecisionTotal);
+            before += counts[s];
+        }
+    }
     // The symbol whose interval holds `quantile` (lib.rs:102-121).
     uint32_t symbol_for_quantile(uint32_t quantile, uint32_t* left, uint32_t* prob) const {
         uint64_t cum = 0;

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "fit.cuh"
+#include "price.hpp"
 
 namespace mars {
 
@@ -175,5 +176,28 @@ cudaError_t launch_decode_step_stable(const uint8_t* src, uint8_t* dst, int w, i
 cudaError_t launch_decode_step(const uint8_t* src, uint8_t* dst, int w, int h, int lg,
                                const int32_t* owner, const DecodeMap* maps, const double* resid,
                                cudaStream_t st);
+
+// RD pricing of one node size (rdprice.cu): count nodes of size x size at (rows, cols), k
+// candidates each; out[i] the node's priced winner, levels[levels_at[i]..] its mode-3 levels.
+// basis: basis(size, k, i) at [k * size + i], computed on the host.  Sizes 2..64; size 64
+// needs global_scratch of price_scratch_bytes() for scratch_slots warp slots.
+struct PriceLaunch {
+    const uint8_t* px;
+    uint32_t stride, size, count;
+    const uint32_t* rows;
+    const uint32_t* cols;
+    const price::Cand* cands;
+    uint32_t k;
+    price::Setup setup;
+    price::RateTable table;
+    const double* basis;
+    price::Priced* out;
+    int8_t* levels;
+    const uint64_t* levels_at;
+    unsigned char* global_scratch;
+    uint32_t scratch_slots;
+};
+size_t price_scratch_bytes(uint32_t size, uint32_t count, uint32_t* slots);
+cudaError_t launch_price_nodes(const PriceLaunch& a, cudaStream_t st);
 
 }  // namespace mars
