@@ -140,43 +140,73 @@ struct Team {
     }
 };
 
-// The 2-D transforms of dct.rs:22-80 with every 1-D output a left-to-right sum seeded with
-// -0.0; b[k * n + i] = basis(n, k, i) and bt its transpose (bt[i * n + k]), which only
-// changes which lane reads which address.  Forward (dct.rs:38-58): rows, then columns.
-MARS_HD inline void forward_dct2d(const double* in, uint32_t n, const double* b, const double* bt,
-                                  double* tmp, double* out, const Team& T) {
-    for (uint32_t idx = T.lane; idx < n * n; idx += T.lanes) {
-        const uint32_t r = idx / n, k = idx % n;
-        double s = -0.0;
-        for (uint32_t i = 0; i < n; ++i) s += in[r * n + i] * bt[i * n + k];
-        tmp[r * n + k] = s;
+// s += term(k) for k = 0..n-1, left to right: the terms of a group of eight are formed
+// (loads, products) before the group's additions, so the dependent chain is additions only.
+// The same values are added in the same order as a plain loop.
+template <class F>
+MARS_HD inline double chain(double s, uint32_t n, F term) {
+    uint32_t k = 0;
+    for (; k + 8 <= n; k += 8) {
+        double x[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = term(k + j);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s += x[j];
     }
-    T.sync();
-    for (uint32_t idx = T.lane; idx < n * n; idx += T.lanes) {
-        const uint32_t k = idx / n, c = idx % n;
-        double s = -0.0;
-        for (uint32_t i = 0; i < n; ++i) s += tmp[i * n + c] * b[k * n + i];
-        out[k * n + c] = s;
+    for (; k < n; ++k) s += term(k);
+    return s;
+}
+
+// One pass of the 2-D transforms of dct.rs:22-80: for every output idx < n*n (the team's
+// share, four interleaved per lane), out[idx] = the left-to-right sum from -0.0 over
+// i < n of a[abase(idx) + i * sa] * b[bbase(idx) + i * sb].  A base is (idx / n) * n
+// ("row"), idx % n ("col") or idx / n ("div").
+enum Base : uint32_t { ROW, COL, DIV };
+MARS_HD inline uint32_t base_of(Base m, uint32_t idx, uint32_t n) {
+    return m == ROW ? (idx / n) * n : m == COL ? idx % n : idx / n;
+}
+MARS_HD inline void dct_pass(const double* a, Base am, uint32_t sa, const double* b, Base bm,
+                             uint32_t sb, double* out, uint32_t n, const Team& T) {
+    const uint32_t nn = n * n;
+    for (uint32_t first = T.lane; first < nn; first += 4 * T.lanes) {
+        uint32_t ia[4], ib[4];
+        double acc[4];
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            uint32_t idx = first + g * T.lanes;
+            if (idx >= nn) idx = nn - 1;  // computed, not stored
+            ia[g] = base_of(am, idx, n);
+            ib[g] = base_of(bm, idx, n);
+            acc[g] = -0.0;
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+            double x[4];
+#pragma unroll
+            for (int g = 0; g < 4; ++g) x[g] = a[ia[g] + i * sa] * b[ib[g] + i * sb];
+#pragma unroll
+            for (int g = 0; g < 4; ++g) acc[g] += x[g];
+        }
+#pragma unroll
+        for (int g = 0; g < 4; ++g)
+            if (first + g * T.lanes < nn) out[first + g * T.lanes] = acc[g];
     }
     T.sync();
 }
-// Inverse (dct.rs:60-80): columns, then rows.
+
+// b[k * n + i] = basis(n, k, i); bt its transpose (bt[i * n + k]), which only changes which
+// lane reads which address.  Forward (dct.rs:38-58): rows (tmp[r][k] = sum_i in[r][i] *
+// basis(k, i)), then columns (out[k][c] = sum_i tmp[i][c] * basis(k, i)).
+MARS_HD inline void forward_dct2d(const double* in, uint32_t n, const double* b, const double* bt,
+                                  double* tmp, double* out, const Team& T) {
+    dct_pass(in, ROW, 1, bt, COL, n, tmp, n, T);
+    dct_pass(tmp, COL, n, b, ROW, 1, out, n, T);
+}
+// Inverse (dct.rs:60-80): columns (tmp[i][c] = sum_k in[k][c] * basis(k, i)), then rows
+// (out[r][i] = sum_k tmp[r][k] * basis(k, i)).
 MARS_HD inline void inverse_dct2d(const double* in, uint32_t n, const double* b, double* tmp,
                                   double* out, const Team& T) {
-    for (uint32_t idx = T.lane; idx < n * n; idx += T.lanes) {
-        const uint32_t i = idx / n, c = idx % n;
-        double s = -0.0;
-        for (uint32_t k = 0; k < n; ++k) s += in[k * n + c] * b[k * n + i];
-        tmp[i * n + c] = s;
-    }
-    T.sync();
-    for (uint32_t idx = T.lane; idx < n * n; idx += T.lanes) {
-        const uint32_t r = idx / n, i = idx % n;
-        double s = -0.0;
-        for (uint32_t k = 0; k < n; ++k) s += tmp[r * n + k] * b[k * n + i];
-        out[r * n + i] = s;
-    }
-    T.sync();
+    dct_pass(in, COL, n, b, DIV, n, tmp, n, T);
+    dct_pass(tmp, ROW, 1, b, COL, n, out, n, T);
 }
 
 MARS_HD inline mars_leaf make_leaf(uint32_t row, uint32_t col, uint32_t size) {
@@ -189,10 +219,30 @@ MARS_HD inline mars_leaf make_leaf(uint32_t row, uint32_t col, uint32_t size) {
     return l;
 }
 
+// The residual's event bits per coefficient (residual.rs): nzb[i] the nonzero flag's, magb[i]
+// the magnitude's (+0.0 for a zero level, which adds nothing to a positive total), looked up
+// by the team in parallel.
+MARS_HD inline void residual_event_bits(const RateTable& t, uint32_t sc, const int32_t* levels,
+                                        uint32_t n, double* nzb, double* magb, const Team& T) {
+    for (uint32_t i = T.lane; i < n; i += T.lanes) {
+        const uint32_t band = band_of(i, n);
+        int32_t l = levels[i];
+        if (l < -kLevelClamp) l = -kLevelClamp;
+        if (l > kLevelClamp) l = kLevelClamp;
+        nzb[i] = rbits(t, F_RESID_NZ, sc * kBands + band, l != 0 ? 1u : 0u);
+        magb[i] = l != 0 ? rbits(t, F_RESID_MAG, sc * kBands + band,
+                                 ((uint32_t)l << 1) ^ (uint32_t)(l >> 31))
+                         : 0.0;
+    }
+    T.sync();
+}
+
 // The leaf's event bits with a fresh domain predictor (emit_leaf, mars_format.rs:515-595;
-// the residual's events for mode 3, residual.rs), summed left to right from -0.0.
+// the residual's events for mode 3, residual.rs), summed left to right from -0.0.  Mode 3
+// reads its events' bits from residual_event_bits.
 MARS_HD inline double leaf_bits(const RateTable& t, const Setup& s, const mars_leaf& leaf,
-                                uint32_t sc, const int32_t* levels) {
+                                uint32_t sc, const double* nzb = nullptr,
+                                const double* magb = nullptr) {
     double r = -0.0;
     r += rbits(t, F_MODE, sc, leaf.mode);
     if (leaf.mode == 0) {
@@ -208,16 +258,22 @@ MARS_HD inline double leaf_bits(const RateTable& t, const Setup& s, const mars_l
         r += rbits(t, F_DOM_ROW, sc, zigzag((int64_t)(leaf.dom_row / s.shift)));
         r += rbits(t, F_DOM_COL, sc, zigzag((int64_t)(leaf.dom_col / s.shift)));
         if (leaf.mode == 3) {
+            // r > 0 here (every event costs bits), so adding a zero level's +0.0 is exact.
             const uint32_t n = leaf.size * leaf.size;
-            for (uint32_t i = 0; i < n; ++i) {
-                const uint32_t band = band_of(i, n);
-                int32_t l = levels[i];
-                if (l < -kLevelClamp) l = -kLevelClamp;
-                if (l > kLevelClamp) l = kLevelClamp;
-                r += rbits(t, F_RESID_NZ, sc * kBands + band, l != 0 ? 1u : 0u);
-                if (l != 0)
-                    r += rbits(t, F_RESID_MAG, sc * kBands + band,
-                               ((uint32_t)l << 1) ^ (uint32_t)(l >> 31));
+            uint32_t i = 0;
+            for (; i + 4 <= n; i += 4) {
+                double x[8];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    x[2 * j] = nzb[i + j];
+                    x[2 * j + 1] = magb[i + j];
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j) r += x[j];
+            }
+            for (; i < n; ++i) {
+                r += nzb[i];
+                r += magb[i];
             }
         }
     }
@@ -229,14 +285,10 @@ MARS_HD inline void affine_fit(const double* block, uint32_t size, uint32_t bits
                                uint32_t* qbeta_out, int32_t* qgx_out, int32_t* qgy_out,
                                double* sse_out) {
     const double n = (double)size * (double)size;
-    double t0 = 0.0, tu = 0.0, tv = 0.0;
-    for (uint32_t u = 0; u < size; ++u)
-        for (uint32_t v = 0; v < size; ++v) {
-            const double p = block[u * size + v];
-            t0 += p;
-            tu += p * (double)u;
-            tv += p * (double)v;
-        }
+    const uint32_t nn = size * size;
+    const double t0 = chain(0.0, nn, [&](uint32_t k) { return block[k]; });
+    const double tu = chain(0.0, nn, [&](uint32_t k) { return block[k] * (double)(k / size); });
+    const double tv = chain(0.0, nn, [&](uint32_t k) { return block[k] * (double)(k % size); });
     double su = -0.0, suu = -0.0;
     for (uint32_t u = 0; u < size; ++u) su += (double)u;
     for (uint32_t u = 0; u < size; ++u) suu += (double)u * (double)u;
@@ -277,13 +329,11 @@ MARS_HD inline void affine_fit(const double* block, uint32_t size, uint32_t bits
     const int32_t qgx = qgrad(gx), qgy = qgrad(gy);
     const double b0q = (double)qbeta / (double)max_qbeta * 255.0;
     const double gxq = (double)qgx / kGradScale, gyq = (double)qgy / kGradScale;
-    double sse = 0.0;
-    for (uint32_t u = 0; u < size; ++u)
-        for (uint32_t v = 0; v < size; ++v) {
-            const double pred = b0q + gxq * (double)u + gyq * (double)v;
-            const double diff = block[u * size + v] - pred;
-            sse += diff * diff;
-        }
+    const double sse = chain(0.0, nn, [&](uint32_t k) {
+        const double pred = b0q + gxq * (double)(k / size) + gyq * (double)(k % size);
+        const double diff = block[k] - pred;
+        return diff * diff;
+    });
     *qbeta_out = qbeta;
     *qgx_out = qgx;
     *qgy_out = qgy;
@@ -341,19 +391,15 @@ MARS_HD inline double residual_for_candidate(const uint8_t* px, uint32_t stride,
     }
     T.sync();
     inverse_dct2d(sc.resid, size, b, sc.tmp, sc.coef, T);  // coef <- the reconstruction
-    double sse = 0.0;
-    for (uint32_t u = 0; u < size; ++u)
-        for (uint32_t v = 0; v < size; ++v) {
-            const uint32_t k = u * size + v;
-            uint32_t i, j;
-            iso_map(c.isometry, u, v, size, &i, &j);
-            double pv = sc.pred[k] + sc.coef[k];
-            if (pv < 0.0) pv = 0.0;
-            if (pv > 255.0) pv = 255.0;
-            const double diff = sc.block[i * size + j] - (double)(uint8_t)pv;
-            sse += diff * diff;
-        }
-    return sse;
+    return chain(0.0, n, [&](uint32_t k) {
+        uint32_t i, j;
+        iso_map(c.isometry, k / size, k % size, size, &i, &j);
+        double pv = sc.pred[k] + sc.coef[k];
+        if (pv < 0.0) pv = 0.0;
+        if (pv > 255.0) pv = 255.0;
+        const double diff = sc.block[i * size + j] - (double)(uint8_t)pv;
+        return diff * diff;
+    });
 }
 
 // The priced winner of one node.
@@ -403,9 +449,10 @@ MARS_HD inline Priced price_node(const uint8_t* px, uint32_t stride, uint32_t ro
         mars_leaf l = make_leaf(row, col, size);
         l.qbeta = best_beta(rsum, s0, s.bits_beta);
         const double beta2 = (double)l.qbeta / (double)((1u << s.bits_beta) - 1) * 255.0;
-        double sse = -0.0;
-        for (uint32_t k = 0; k < n; ++k) sse += (sc.block[k] - beta2) * (sc.block[k] - beta2);
-        offer(l, sse, leaf_bits(t, s, l, sc_class, nullptr), false);
+        const double sse = chain(-0.0, n, [&](uint32_t k) {
+            return (sc.block[k] - beta2) * (sc.block[k] - beta2);
+        });
+        offer(l, sse, leaf_bits(t, s, l, sc_class), false);
     };
     if (s.allowed[0]) mode0();
     if (s.allowed[1]) {
@@ -413,7 +460,7 @@ MARS_HD inline Priced price_node(const uint8_t* px, uint32_t stride, uint32_t ro
         l.mode = 1;
         double sse;
         affine_fit(sc.block, size, s.bits_beta, &l.qbeta, &l.qgx, &l.qgy, &sse);
-        offer(l, sse, leaf_bits(t, s, l, sc_class, nullptr), false);
+        offer(l, sse, leaf_bits(t, s, l, sc_class), false);
     }
     for (uint32_t ci = 0; ci < nranked; ++ci) {
         const Cand& c = ranked[ci];
@@ -427,12 +474,14 @@ MARS_HD inline Priced price_node(const uint8_t* px, uint32_t stride, uint32_t ro
         if (s.allowed[2]) {
             l.mode = 2;
             const double sse2 = c.rms * c.rms * (double)size * (double)size;
-            offer(l, sse2, leaf_bits(t, s, l, sc_class, nullptr), false);
+            offer(l, sse2, leaf_bits(t, s, l, sc_class), false);
         }
         if (s.allowed[3]) {
             l.mode = 3;
             const double sse3 = residual_for_candidate(px, stride, size, c, s, b, bt, sc, T);
-            offer(l, sse3, leaf_bits(t, s, l, sc_class, sc.levels), true);
+            // resid and tmp are free once the reconstruction's SSE is taken.
+            residual_event_bits(t, sc_class, sc.levels, n, sc.tmp, sc.resid, T);
+            offer(l, sse3, leaf_bits(t, s, l, sc_class, sc.tmp, sc.resid), true);
         }
     }
     if (!have) mode0();
