@@ -385,7 +385,9 @@ def run_encode(mb, ctx, workers=3):
     the search on the GPU and the host walks, host plane in, leaves out.  `value`: images/s
     through Context.encode_many (a search plan per size, `workers` planes in flight so one
     plane's walks overlap the next one's search); `sequential`: one ctx.encode after
-    another.  Both for the default modes {0, 2} and for all four modes: the four-mode encode
+    another; `planned_sequential`: one planned encode after another (search, warm-up walk,
+    pricing and RD walk on the device; the host builds the rate snapshot and receives the
+    leaves).  Both for the default modes {0, 2} and for all four modes: the four-mode encode
     prices every quadtree node (the residual mode's DCTs) on the device, the two-mode one on
     the host walk."""
     imgs = [synthetic.gray(W, H, s) for s in range(1, 9)]
@@ -404,7 +406,13 @@ def run_encode(mb, ctx, workers=3):
         for im in imgs:
             ctx.encode(im, params, allowed_modes=modes)
         seq = len(imgs) / (time.perf_counter() - t0)
-        out[key] = {"value": piped, "sequential": seq}
+        plan = ctx.cached_plan(W, H, params)
+        plan.encode(imgs[0], allowed_modes=modes)
+        t0 = time.perf_counter()
+        for im in imgs:
+            plan.encode(im, allowed_modes=modes)
+        planned = len(imgs) / (time.perf_counter() - t0)
+        out[key] = {"value": piped, "sequential": seq, "planned_sequential": planned}
     out["value"] = out["modes_0_2"]["value"]
     return out
 

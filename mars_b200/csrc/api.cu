@@ -1011,6 +1011,16 @@ struct mars_search_plan {
     std::vector<uint64_t> evals;
     uint64_t total_evals = 0;
     std::shared_ptr<const std::unordered_map<uint64_t, uint32_t>> index;
+    // The walks on the device (built on the first encode that uses them).
+    std::mutex walk_mu;
+    int walk_state = 0;  // 0 not built, 1 built, -1 this plan's tree needs the host walk
+    mars::WalkPlan walk{};
+    uint32_t *d_wrows = nullptr, *d_wcols = nullptr;
+    int32_t *d_child = nullptr, *d_roots = nullptr;
+    uint64_t *d_wevals = nullptr, *d_levels_at = nullptr;
+    double* d_basis = nullptr;
+    std::vector<size_t> basis_at;  // per level, into d_basis
+    uint64_t nlevels_total = 0;    // sum of size^2 over the nodes
 };
 
 namespace {
@@ -1027,6 +1037,13 @@ void plan_release(mars_search_plan* p) {
     cudaFreeHost(p->h_plane);
     cudaFreeHost(p->h_out);
     cudaFreeHost(p->h_exact);
+    cudaFree(p->d_wrows);
+    cudaFree(p->d_wcols);
+    cudaFree(p->d_child);
+    cudaFree(p->d_roots);
+    cudaFree(p->d_wevals);
+    cudaFree(p->d_levels_at);
+    cudaFree(p->d_basis);
     delete p;
 }
 
@@ -1196,6 +1213,287 @@ void mars_search_plan_free(mars_search_plan* p) {
     plan_release(p);
 }
 
+}  // extern "C"
+
+namespace {
+
+// The static tables of the walks on the device for one plan: its nodes with their children
+// (TL, BL, TR, BR), the roots, evals, level offsets and DCT bases.  Returns false (and
+// marks the plan) when the tree has nodes the plan does not search (pixel leaves at
+// min_size 1 or at the edges of thin planes): those encodes keep the host walk.
+int plan_walk_setup(mars_search_plan* p, bool* usable) {
+    std::lock_guard<std::mutex> lock(p->walk_mu);
+    if (p->walk_state) {
+        *usable = p->walk_state > 0;
+        return MARS_OK;
+    }
+    *usable = false;
+    p->walk_state = -1;
+    const mars_params& prm = p->params;
+    if (prm.min_size < 2 || p->jobs.size() > 32 || p->total == 0) return MARS_OK;
+    const mars_header hdr = mars::codec::build_header(p->w, p->h, prm);
+    const auto& index = *p->index;
+    mars::WalkPlan w{};
+    std::vector<uint32_t> rows, cols;
+    std::vector<uint64_t> levels_at;
+    std::vector<double> basis;
+    uint64_t lev = 0;
+    for (const Job& j : p->jobs) {
+        if (j.shift != prm.shift) return MARS_OK;
+        w.first[w.nlevels] = (uint32_t)rows.size();
+        w.count[w.nlevels] = (uint32_t)j.rows.size();
+        w.size[w.nlevels] = j.size;
+        ++w.nlevels;
+        p->basis_at.push_back(basis.size());
+        const std::vector<double>& b = mars::residual::basis(j.size);
+        basis.insert(basis.end(), b.begin(), b.end());
+        for (size_t i = 0; i < j.rows.size(); ++i) {
+            rows.push_back(j.rows[i]);
+            cols.push_back(j.cols[i]);
+            levels_at.push_back(lev);
+            lev += (uint64_t)j.size * j.size;
+        }
+    }
+    for (uint32_t L = 1; L < w.nlevels; ++L)
+        if (w.size[L] <= w.size[L - 1]) return MARS_OK;  // one level per size, ascending
+    auto find = [&](uint32_t r, uint32_t c, uint32_t size) -> int64_t {
+        auto it = index.find(node_key(r, c, size, prm.shift));
+        return it == index.end() ? -1 : (int64_t)it->second;
+    };
+    std::vector<int32_t> child(4 * rows.size(), -1);
+    for (uint32_t L = 0; L < w.nlevels; ++L) {
+        const uint32_t size = w.size[L], half = size / 2;
+        if (size <= prm.min_size) continue;
+        for (uint32_t i = w.first[L]; i < w.first[L] + w.count[L]; ++i) {
+            const uint32_t rs[4] = {rows[i], rows[i] + half, rows[i], rows[i] + half};
+            const uint32_t cs[4] = {cols[i], cols[i], cols[i] + half, cols[i] + half};
+            for (int q = 0; q < 4; ++q) {
+                const int64_t c = find(rs[q], cs[q], half);
+                if (c < 0) return MARS_OK;
+                child[4 * (size_t)i + q] = (int32_t)c;
+            }
+        }
+    }
+    std::vector<int32_t> roots;
+    for (const auto& r : mars::codec::quadtree_roots(hdr)) {
+        const int64_t c = r[2] >= 2 ? find(r[0], r[1], r[2]) : -1;
+        if (c < 0) return MARS_OK;
+        roots.push_back((int32_t)c);
+    }
+    mars_ctx* ctx = p->ctx;
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    auto up = [&](auto** dst, const auto& v) -> cudaError_t {
+        using T = typename std::decay_t<decltype(v)>::value_type;
+        cudaError_t e = cudaMalloc((void**)dst, std::max<size_t>(1, v.size()) * sizeof(T));
+        if (e == cudaSuccess && !v.empty())
+            e = cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+        return e;
+    };
+    MARS_CUDA(up(&p->d_wrows, rows));
+    MARS_CUDA(up(&p->d_wcols, cols));
+    MARS_CUDA(up(&p->d_child, child));
+    MARS_CUDA(up(&p->d_roots, roots));
+    MARS_CUDA(up(&p->d_wevals, p->evals));
+    MARS_CUDA(up(&p->d_levels_at, levels_at));
+    MARS_CUDA(up(&p->d_basis, basis));
+    w.nodes = (uint32_t)rows.size();
+    w.nroots = (uint32_t)roots.size();
+    w.rows = p->d_wrows;
+    w.cols = p->d_wcols;
+    w.child = p->d_child;
+    w.roots = p->d_roots;
+    w.evals = p->d_wevals;
+    w.levels_at = p->d_levels_at;
+    w.stride = p->w;
+    p->walk = w;
+    p->nlevels_total = lev;
+    p->walk_state = 1;
+    *usable = true;
+    return MARS_OK;
+}
+
+// MARS_PLAN_WALK=host keeps planned encodes on the host walk over a downloaded table.
+bool plan_walk_on_host() {
+    static const bool on = [] {
+        const char* e = std::getenv("MARS_PLAN_WALK");
+        return e && std::string(e) == "host";
+    }();
+    return on;
+}
+
+template <class T>
+int copy_out_array(const std::vector<T>& v, T** out, size_t* n) {
+    *n = v.size();
+    *out = (T*)std::malloc(std::max<size_t>(1, v.size()) * sizeof(T));
+    if (!*out) return fail(MARS_ENOMEM, "output allocation failed");
+    if (!v.empty()) std::memcpy(*out, v.data(), v.size() * sizeof(T));
+    return MARS_OK;
+}
+
+// A planned encode with both walks on the device: the plan's search, then the warm-up walk
+// over its candidates, the rate snapshot on the host from the warm-up leaves, the pricing of
+// every node and the RD walk's decisions -- the host receives only leaves.
+int plan_encode_device(mars_search_plan* plan, const uint8_t* plane, const mars_options* o,
+                       mars_header* header, mars_leaf** leaves, size_t* nleaves,
+                       int32_t** residuals, size_t* nresiduals, mars_counters* counters) {
+    mars_ctx* ctx = plan->ctx;
+    const mars_params& prm = plan->params;
+    mars_header hdr;
+    if (mars::codec::encode_header(plan->w, plan->h, prm, *o, &hdr))
+        return fail(MARS_EINVAL, "residual qstep out of range");
+    const mars::WalkPlan& w = plan->walk;
+    const size_t nodes = w.nodes;
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    OwnStream own;
+    MARS_CUDA(cudaStreamCreateWithFlags(&own.st, cudaStreamNonBlocking));
+    const cudaStream_t st = own.st;
+    Scratch sc(st);
+    unsigned char* d_cands;
+    uint8_t* d_px;
+    mars::WalkScratch ws{};
+    mars_leaf *d_warm, *d_leaves;
+    MARS_CUDA(sc.get(&d_cands, nodes * sizeof(mars_candidate)));
+    MARS_CUDA(sc.get(&d_px, (size_t)plan->w * plan->h));
+    MARS_CUDA(sc.get(&ws.split, nodes));
+    MARS_CUDA(sc.get(&ws.cnt, nodes));
+    MARS_CUDA(sc.get(&ws.ev, nodes));
+    MARS_CUDA(sc.get(&ws.ofs, nodes));
+    MARS_CUDA(sc.get(&ws.rofs, nodes));
+    MARS_CUDA(sc.get(&ws.rd, nodes));
+    MARS_CUDA(sc.get(&ws.rr, nodes));
+    MARS_CUDA(sc.get(&ws.totals, 2));
+    MARS_CUDA(sc.get(&d_warm, nodes));
+    MARS_CUDA(sc.get(&d_leaves, nodes));
+    cudaEvent_t ev_alloc, ev_search;
+    MARS_CUDA(cudaEventCreateWithFlags(&ev_alloc, cudaEventDisableTiming));
+    MARS_CUDA(cudaEventCreateWithFlags(&ev_search, cudaEventDisableTiming));
+    struct Events {
+        cudaEvent_t a, b;
+        ~Events() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } evs{ev_alloc, ev_search};
+    MARS_CUDA(cudaEventRecord(ev_alloc, st));
+    {
+        // The search on the plan's buffers, then this call's copies of its candidates and
+        // plane, in the context's stream order (the next run of the plan queues behind them).
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        MARS_CUDA(cudaStreamWaitEvent(ctx->stream, ev_alloc, 0));
+        MARS_CUDA(cudaMemcpyAsync(plan->d_plane, plane, (size_t)plan->w * plan->h,
+                                  cudaMemcpyHostToDevice, ctx->stream));
+        MARS_CUDA(cudaGraphLaunch(plan->x_dev, ctx->stream));
+        ctx->launches += plan->launches_per_run;
+        MARS_CUDA(cudaMemcpyAsync(d_cands, plan->d_out, nodes * sizeof(mars_candidate),
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
+        MARS_CUDA(cudaMemcpyAsync(d_px, plan->d_plane, (size_t)plan->w * plan->h,
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
+        MARS_CUDA(cudaEventRecord(ev_search, ctx->stream));
+    }
+    MARS_CUDA(cudaStreamWaitEvent(st, ev_search, 0));
+    mars::WalkPlan wp = w;
+    wp.px = d_px;
+    // The warm-up walk (t_rms = 8 for the rate snapshot; the plain walk itself without RD).
+    const double t_rms = prm.has_lambda ? 8.0 : prm.t_rms;
+    MARS_CUDA(mars::launch_warm_walk(wp, d_cands, sizeof(mars_candidate), t_rms, prm.min_size,
+                                     prm.zero_threshold, hdr.bits_beta, ws, d_warm, st));
+    ctx->launches += 2 * w.nlevels + 1;
+    unsigned long long tot[2];
+    MARS_CUDA(cudaMemcpyAsync(tot, ws.totals, sizeof tot, cudaMemcpyDeviceToHost, st));
+    if (int e = sync_bounded(ctx, st)) return e;
+    std::vector<mars_leaf> warm(tot[0]);
+    MARS_CUDA(cudaMemcpyAsync(warm.data(), d_warm, warm.size() * sizeof(mars_leaf),
+                              cudaMemcpyDeviceToHost, st));
+    if (int e = sync_bounded(ctx, st)) return e;
+    const uint64_t warm_evals = tot[1];
+    *header = hdr;
+    if (!prm.has_lambda) {
+        counters->search_evals = warm_evals;
+        counters->warmup_evals = 0;
+        if (int e = copy_out_array(warm, leaves, nleaves)) return e;
+        return copy_out_array(std::vector<int32_t>(), residuals, nresiduals);
+    }
+    // The rate snapshot from the warm-up leaves, then every node priced and the RD walk.
+    std::vector<double> bits;
+    std::vector<int64_t> off;
+    if (mars::codec::rate_table_from_warmup(hdr, warm, prm.max_size, &bits, &off))
+        return fail(MARS_EINVAL, "rate snapshot of the warm-up leaves failed");
+    double split0[32] = {0}, split1[32] = {0};
+    for (uint32_t L = 0; L < w.nlevels; ++L) {
+        const uint32_t c = (uint32_t)__builtin_ctz(w.size[L]);
+        const int64_t at = off[(size_t)mars::price::F_SPLIT * mars::price::kCtx + c];
+        if (at < 0) return fail(MARS_EINVAL, "rate table misses a split context");
+        split0[c] = bits[at];
+        split1[c] = bits[at + 1];
+    }
+    const uint8_t allowed[4] = {o->allowed_modes[0], o->allowed_modes[1], o->allowed_modes[2],
+                                o->allowed_modes[3]};
+    const mars::price::Setup setup = mars::codec::price_setup(hdr, prm, allowed, prm.lambda);
+    double* d_bits;
+    int64_t* d_off;
+    mars::price::Priced* d_priced;
+    int8_t* d_lev;
+    int32_t* d_res;
+    const bool residual = allowed[3] != 0;
+    MARS_CUDA(sc.get(&d_bits, bits.size()));
+    MARS_CUDA(sc.get(&d_off, off.size()));
+    MARS_CUDA(sc.get(&d_priced, nodes));
+    MARS_CUDA(sc.get(&d_lev, residual ? plan->nlevels_total : 1));
+    MARS_CUDA(sc.get(&d_res, residual ? plan->nlevels_total : 1));
+    MARS_CUDA(cudaMemcpyAsync(d_bits, bits.data(), bits.size() * sizeof(double),
+                              cudaMemcpyHostToDevice, st));
+    MARS_CUDA(cudaMemcpyAsync(d_off, off.data(), off.size() * sizeof(int64_t),
+                              cudaMemcpyHostToDevice, st));
+    for (uint32_t L = w.nlevels; L-- > 0;) {  // largest nodes first
+        mars::PriceLaunch a{};
+        a.px = d_px;
+        a.stride = plan->w;
+        a.size = w.size[L];
+        a.count = w.count[L];
+        a.rows = plan->d_wrows + w.first[L];
+        a.cols = plan->d_wcols + w.first[L];
+        a.cands = d_cands + (size_t)w.first[L] * sizeof(mars_candidate);
+        a.cand_stride = sizeof(mars_candidate);
+        a.k = 1;
+        a.setup = setup;
+        a.table = {d_bits, d_off};
+        a.basis = plan->d_basis + plan->basis_at[L];
+        a.out = d_priced + w.first[L];
+        a.levels = d_lev;
+        a.levels_at = plan->d_levels_at + w.first[L];
+        const size_t gbytes = mars::price_scratch_bytes(a.size, a.count, &a.scratch_slots);
+        if (gbytes) MARS_CUDA(sc.get(&a.global_scratch, gbytes));
+        MARS_CUDA(mars::launch_price_nodes(a, st));
+        ctx->launches += 1;
+    }
+    MARS_CUDA(mars::launch_rd_walk(wp, d_priced, d_lev, prm.lambda * 1.0, split0, split1,
+                                   prm.min_size, ws, d_leaves, d_res, st));
+    ctx->launches += 2 * w.nlevels + 1;
+    MARS_CUDA(cudaMemcpyAsync(tot, ws.totals, sizeof tot, cudaMemcpyDeviceToHost, st));
+    if (int e = sync_bounded(ctx, st)) return e;
+    std::vector<mars_leaf> out(tot[0]);
+    std::vector<int32_t> res(tot[1]);
+    MARS_CUDA(cudaMemcpyAsync(out.data(), d_leaves, out.size() * sizeof(mars_leaf),
+                              cudaMemcpyDeviceToHost, st));
+    if (!res.empty())
+        MARS_CUDA(cudaMemcpyAsync(res.data(), d_res, res.size() * sizeof(int32_t),
+                                  cudaMemcpyDeviceToHost, st));
+    if (int e = sync_bounded(ctx, st)) return e;
+    counters->search_evals = plan->total_evals;
+    counters->warmup_evals = warm_evals;
+    if (int e = copy_out_array(out, leaves, nleaves)) return e;
+    if (int e = copy_out_array(res, residuals, nresiduals)) {
+        std::free(*leaves);
+        *leaves = nullptr;
+        return e;
+    }
+    return MARS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int mars_encode_planned(mars_search_plan* plan, const uint8_t* plane,
                         const mars_options* options, mars_header* header, mars_leaf** leaves,
                         size_t* nleaves, int32_t** residuals, size_t* nresiduals,
@@ -1211,6 +1509,12 @@ int mars_encode_planned(mars_search_plan* plan, const uint8_t* plane,
         !(std::isfinite(options->residual_qstep) && options->residual_qstep >= 1.0f &&
           options->residual_qstep <= 65535.0f))
         return fail(MARS_EINVAL, "residual qstep must be finite and in [1, 65535]");
+    bool device_walk = false;
+    if (!plan_walk_on_host())
+        if (int e = plan_walk_setup(plan, &device_walk)) return e;
+    if (device_walk)
+        return plan_encode_device(plan, plane, options, header, leaves, nleaves, residuals,
+                                  nresiduals, counters);
     mars_table* table = nullptr;
     if (int e = mars_search_plan_run(plan, plane, &table)) return e;
     std::unique_ptr<mars_table, void (*)(mars_table*)> guard(table, mars_search_table_free);

@@ -925,11 +925,9 @@ int price_all(const Ctx& base, double lambda, const Pricer& pricer, PriceBatch* 
     return pricer(b);
 }
 
-int encode(const Image& im, const mars_params& p, const mars_options& o, const Provider& provider,
-           const Provider& warmup, mars_header* hdr_out, std::vector<mars_leaf>* leaves,
-           std::vector<int32_t>* residuals, mars_counters* counters,
-           const RankedProvider* ranked, const Pricer* pricer) {
-    mars_header hdr = build_header(im.w, im.h, p);
+int encode_header(uint32_t w, uint32_t h, const mars_params& p, const mars_options& o,
+                  mars_header* out) {
+    mars_header hdr = build_header(w, h, p);
     // encode.rs:1066-1071: LambdaAdaptive -> from_lambda (8 without lambda); Fixed(step).
     if (o.residual_adaptive)
         hdr.residual_qstep = p.has_lambda ? qstep_from_lambda(p.lambda) : 8.0f;
@@ -937,6 +935,41 @@ int encode(const Image& im, const mars_params& p, const mars_options& o, const P
         hdr.residual_qstep = 8.0f;
     else if (!qstep_new((double)o.residual_qstep, &hdr.residual_qstep))
         return MARS_EINVAL;
+    *out = hdr;
+    return MARS_OK;
+}
+
+int rate_table_from_warmup(const mars_header& hdr, const std::vector<mars_leaf>& warm,
+                           uint32_t max_size, std::vector<double>* bits,
+                           std::vector<int64_t>* offset) {
+    RateModels rate;
+    if (!rate.build(hdr, warm)) return MARS_EINVAL;
+    HostRates t = build_rate_table(rate, hdr, max_size);
+    *bits = std::move(t.bits);
+    *offset = std::move(t.offset);
+    return MARS_OK;
+}
+
+price::Setup price_setup(const mars_header& hdr, const mars_params& p, const uint8_t allowed[4],
+                         double lambda) {
+    return make_setup(hdr, p, allowed, lambda * 1.0);
+}
+
+std::vector<std::array<uint32_t, 3>> quadtree_roots(const mars_header& hdr) {
+    std::vector<Root> roots;
+    collect_roots(hdr, 0, 0, virtual_size(hdr), &roots);
+    std::vector<std::array<uint32_t, 3>> out;
+    out.reserve(roots.size());
+    for (const Root& r : roots) out.push_back({r.row, r.col, r.size});
+    return out;
+}
+
+int encode(const Image& im, const mars_params& p, const mars_options& o, const Provider& provider,
+           const Provider& warmup, mars_header* hdr_out, std::vector<mars_leaf>* leaves,
+           std::vector<int32_t>* residuals, mars_counters* counters,
+           const RankedProvider* ranked, const Pricer* pricer) {
+    mars_header hdr;
+    if (int st = encode_header(im.w, im.h, p, o, &hdr)) return st;
     residuals->clear();
     if (p.has_lambda) {
         // build_rate_snapshot (encode.rs:1139-1169): the t_rms = 8 threshold walk with the

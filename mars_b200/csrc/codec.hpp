@@ -4,6 +4,7 @@
 // f64 operation order (this translation unit is built with -ffp-contract=off).
 #pragma once
 
+#include <array>
 #include <cstdint>
 #include <functional>
 #include <map>
@@ -84,6 +85,21 @@ int encode(const Image& im, const mars_params& p, const mars_options& o, const P
            const Provider& warmup, mars_header* hdr, std::vector<mars_leaf>* leaves,
            std::vector<int32_t>* residuals, mars_counters* counters,
            const RankedProvider* ranked = nullptr, const Pricer* pricer = nullptr);
+
+// The header an encode writes: build_header plus the residual step the options choose
+// (encode.rs:1066-1071); MARS_EINVAL for a step outside the format's range.
+int encode_header(uint32_t w, uint32_t h, const mars_params& p, const mars_options& o,
+                  mars_header* out);
+// The RD pricing's bits table from the warm-up walk's leaves (build_rate_snapshot,
+// encode.rs:1139-1169, then RateModels as price::RateTable): bits and offsets.
+int rate_table_from_warmup(const mars_header& hdr, const std::vector<mars_leaf>& warm,
+                           uint32_t max_size, std::vector<double>* bits,
+                           std::vector<int64_t>* offset);
+// The constants best_mode_leaf reads for one encode (walk_rd's node lambda = lambda * 1.0).
+price::Setup price_setup(const mars_header& hdr, const mars_params& p, const uint8_t allowed[4],
+                         double lambda);
+// The unforced quadtree nodes directly below the forced splits, in walk order.
+std::vector<std::array<uint32_t, 3>> quadtree_roots(const mars_header& hdr);
 
 // The residual step of a header as f64 (ResidualQstep::get, quant.rs:54-56); 0 in the
 // struct stands for the default step 8.

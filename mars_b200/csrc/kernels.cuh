@@ -186,7 +186,8 @@ struct PriceLaunch {
     uint32_t stride, size, count;
     const uint32_t* rows;
     const uint32_t* cols;
-    const price::Cand* cands;
+    const void* cands;     // k per node, cand_stride bytes apart (0: packed price::Cand)
+    uint32_t cand_stride;  // sizeof(mars_candidate) to read a search table in place
     uint32_t k;
     price::Setup setup;
     price::RateTable table;
@@ -199,5 +200,45 @@ struct PriceLaunch {
 };
 size_t price_scratch_bytes(uint32_t size, uint32_t count, uint32_t* slots);
 cudaError_t launch_price_nodes(const PriceLaunch& a, cudaStream_t st);
+
+// The warm-up and RD walks over a search plan's nodes (rdprice.cu).  Nodes in plan order:
+// level L holds count[L] nodes of size[L] from first[L], levels by ascending size, each in
+// walk order.  child: 4 per node (TL, BL, TR, BR; -1 at min_size); roots: the unforced nodes
+// below the forced splits, in walk order; levels_at: each node's offset in the pricing's
+// level buffer; px/stride: the plane.
+struct WalkPlan {
+    uint32_t nodes, nlevels, nroots;
+    uint32_t first[32], count[32], size[32];
+    const uint32_t* rows;
+    const uint32_t* cols;
+    const int32_t* child;
+    const int32_t* roots;
+    const uint64_t* evals;
+    const uint64_t* levels_at;
+    const uint8_t* px;
+    uint32_t stride;
+};
+// Per-call device scratch of the walks, `nodes` entries each (totals: 2).
+struct WalkScratch {
+    uint8_t* split;
+    uint32_t* cnt;
+    uint64_t* ev;  // warm-up: subtree evals; RD: subtree residual levels
+    uint32_t* ofs;
+    uint64_t* rofs;
+    double* rd;
+    double* rr;
+    unsigned long long* totals;
+};
+// Warm-up walk with threshold t_rms: leaves (totals[0] of them, in walk order) into out;
+// totals[1] = the evals of the visited nodes.
+cudaError_t launch_warm_walk(const WalkPlan& w, const void* cands, uint32_t cand_stride,
+                             double t_rms, uint32_t min_size, uint32_t zero_threshold,
+                             uint32_t bits_beta, WalkScratch& s, mars_leaf* out, cudaStream_t st);
+// RD walk over priced nodes: leaves (totals[0]) into out and their mode-3 levels (totals[1]
+// values) into out_res, in walk order.  split0/split1: the split flag's bits per size class.
+cudaError_t launch_rd_walk(const WalkPlan& w, const price::Priced* priced, const int8_t* levels,
+                           double lambda, const double* split0, const double* split1,
+                           uint32_t min_size, WalkScratch& s, mars_leaf* out, int32_t* out_res,
+                           cudaStream_t st);
 
 }  // namespace mars

@@ -12,6 +12,7 @@
 #pragma once
 
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
 
 #include "../../include/mars_b200.h"
@@ -51,6 +52,10 @@ struct Cand {
     uint32_t dom_row, dom_col, isometry, qalfa, qbeta, valid;
     double rms;
 };
+static_assert(offsetof(Cand, valid) == offsetof(mars_candidate, valid) &&
+                  offsetof(Cand, rms) == offsetof(mars_candidate, rms) &&
+                  alignof(mars_candidate) >= alignof(Cand),
+              "a mars_candidate begins with a Cand");
 
 // The constants one encode's pricing reads.
 struct Setup {
@@ -413,11 +418,14 @@ struct Priced {
 // best_mode_leaf (encode.rs:1536-1714) for the node's block over the ranked candidates
 // (the single winner unless rd_candidates > 1; invalid or qalfa < 1 ones are skipped);
 // candidates are compared in the reference's order by J = d + lambda * r, first minimum.
-// Every lane returns the same Priced; sc.best_levels is complete when it returns.
+// Every lane returns the same Priced; sc.best_levels is complete when it returns.  The
+// candidates sit `cand_bytes` apart (a mars_candidate array, whose leading fields are a Cand,
+// is read in place).
 MARS_HD inline Priced price_node(const uint8_t* px, uint32_t stride, uint32_t row, uint32_t col,
                                  uint32_t size, const Cand* ranked, uint32_t nranked,
                                  const Setup& s, const RateTable& t, const double* b,
-                                 const double* bt, uint32_t sc_class, Scratch& sc, const Team& T) {
+                                 const double* bt, uint32_t sc_class, Scratch& sc, const Team& T,
+                                 uint32_t cand_bytes = sizeof(Cand)) {
     const uint32_t n = size * size;
     int64_t part = 0;
     for (uint32_t k = T.lane; k < n; k += T.lanes) {
@@ -463,7 +471,8 @@ MARS_HD inline Priced price_node(const uint8_t* px, uint32_t stride, uint32_t ro
         offer(l, sse, leaf_bits(t, s, l, sc_class), false);
     }
     for (uint32_t ci = 0; ci < nranked; ++ci) {
-        const Cand& c = ranked[ci];
+        const Cand& c = *reinterpret_cast<const Cand*>(
+            reinterpret_cast<const unsigned char*>(ranked) + (size_t)ci * cand_bytes);
         if (!c.valid || c.qalfa < 1) continue;
         mars_leaf l = make_leaf(row, col, size);
         l.qalfa = c.qalfa;
