@@ -417,6 +417,66 @@ def run_encode(mb, ctx, workers=3):
     return out
 
 
+CLASSIFIED_SEEDS = (1, 2, 3, 4)
+
+
+def run_classified(mb, ctx):
+    """Classified search on 768x512 colour: synthetic RGB (the generator per channel, random
+    3x3 channel mix), BT.601 YCbCr with Cb/Cr box-downsampled to 4:2:0 on the device, then
+    the Fisher-classified search (domains bucketed by the reference's block classification)
+    of every RD-quadtree node of the three planes, ranges 16..4, domain stride 2.  `value`:
+    classified fits/s over the planes of seeds 1-4 (host planes in, node tables out, the
+    colour conversion included); `exhaustive` the same planes through the exhaustive search;
+    `encode` whole colour RD encodes (lambda 200, all modes, Fisher) into MARC bytes."""
+    from mars_b200 import color
+    rgbs = [synthetic.rgb(768, 512, s) for s in CLASSIFIED_SEEDS]
+    params = mb.make_params(min_size=4, max_size=16, shift=SHIFT, lam=200.0)
+
+    def planes(rgb):
+        y, cb, cr = ctx.ycbcr(rgb[..., 0], rgb[..., 1], rgb[..., 2])
+        return [y, ctx.downsample_box(cb), ctx.downsample_box(cr)]
+
+    def searched(method):
+        ev = 0
+        t0 = time.perf_counter()
+        for rgb in rgbs:
+            for pl in planes(rgb):
+                prov = ctx.search_provider(pl, params, method=method)
+                ev += int(mb.lib().mars_search_table_evals(prov._h))
+                prov.close()
+        return ev, time.perf_counter() - t0
+
+    for method in ("fisher", "exhaustive"):  # warm-up
+        for pl in planes(rgbs[0]):
+            ctx.search_provider(pl, params, method=method).close()
+    launches0 = ctx.launches
+    ev_f, t_f = searched("fisher")
+    launches = ctx.launches - launches0
+    ev_x, t_x = searched("exhaustive")
+    cparams = color.ColorEncodeParams(params, params, method="fisher")
+    color.encode_color(ctx, rgbs[0], cparams)
+    nbytes = 0
+    t0 = time.perf_counter()
+    for rgb in rgbs:
+        data, _ = color.encode_color(ctx, rgb, cparams)
+        nbytes += len(data)
+    t_e = time.perf_counter() - t0
+    return {
+        "workload": "768x512 synthetic RGB (seeds 1-4, random channel mix) -> YCbCr 4:2:0 "
+                    "on the device, Fisher-classified search of every RD quadtree node of Y, "
+                    "Cb, Cr (ranges 16..4, domain stride 2)",
+        "value": ev_f / t_f, "unit": "fits/s", "evals": ev_f, "seconds": t_f,
+        "images_per_s": len(rgbs) / t_f, "gpu_launches": launches,
+        "exhaustive": {"value": ev_x / t_x, "unit": "fits/s", "evals": ev_x, "seconds": t_x,
+                       "images_per_s": len(rgbs) / t_x},
+        "encode": {"value": len(rgbs) / t_e, "unit": "colour images/s",
+                   "bytes_per_image": nbytes / len(rgbs),
+                   "call": "color.encode_color (Fisher, lambda 200, modes 0-3, MARC bytes)"},
+        "timing": "host wall clock, host planes in and host tables / bytes out, one image "
+                  "after another",
+    }
+
+
 UNEVEN_COUNT, UNEVEN_SEED, UNEVEN_LARGE = 64, 5, 4096
 
 
@@ -632,6 +692,10 @@ def run_gpu(args):
     if single and not args.no_uneven:
         uneven = run_uneven(mb, ctx, dev)
 
+    classified = None
+    if single and not args.no_classified:
+        classified = run_classified(mb, ctx)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, desc = cpu_baseline()
@@ -667,6 +731,7 @@ def run_gpu(args):
             "encode": encode,
             "refine": refine,
             "uneven": uneven,
+            "classified": classified,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -686,6 +751,8 @@ def main():
     ap.add_argument("--no-decode", action="store_true", help="skip the decode leg")
     ap.add_argument("--no-refine", action="store_true", help="skip the refinement leg")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
+    ap.add_argument("--no-classified", action="store_true",
+                    help="skip the classified colour leg")
     ap.add_argument("--refine-only", action="store_true",
                     help="run only the refinement leg (for profiling), on --refine-seeds and "
                          "--refine-lambdas, and print its JSON object")

@@ -98,9 +98,13 @@ def encode_color(ctx: Context, image: np.ndarray, p: ColorEncodeParams):
         mode = MODE_RGB_444
     else:
         raise ValueError("subsampling is '420' or '444'")
-    yb, stats.y_evals = _encode_plane(ctx, y, p.y, p)
-    cbb, stats.cb_evals = _encode_plane(ctx, cb, p.chroma, p)
-    crb, stats.cr_evals = _encode_plane(ctx, cr, p.chroma, p)
+    # The planes are independent encodes; the C ABI is thread-safe, so one plane's host
+    # walks overlap another's search on the device.
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(3) as pool:
+        jobs = [pool.submit(_encode_plane, ctx, pl, prm, p)
+                for pl, prm in ((y, p.y), (cb, p.chroma), (cr, p.chroma))]
+        (yb, stats.y_evals), (cbb, stats.cb_evals), (crb, stats.cr_evals) = [j.result() for j in jobs]
     stats.y_bytes, stats.cb_bytes, stats.cr_bytes = len(yb), len(cbb), len(crb)
     stats.planes = {"y": y, "cb": cb, "cr": cr}
     return write_container(mode, [yb, cbb, crb]), stats
