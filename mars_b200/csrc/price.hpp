@@ -162,6 +162,33 @@ MARS_HD inline double chain(double s, uint32_t n, F term) {
     return s;
 }
 
+// Independent serial sums run side by side: sum j (j < nc <= 32) is
+// init[j] + x_j[0] (+ y_j[0]) + x_j[1] (+ y_j[1]) + ..., n terms of x (and, when `pairs`,
+// n terms of y read at y_j[k * ys_j]), left to right.  On the device lane j evaluates sum
+// j -- the lanes run one instruction stream over different arrays -- and every lane
+// receives all nc results; the host evaluates them one after another.  Each sum's order and
+// values are those of a plain loop.
+MARS_HD inline double one_sum(const double* x, const double* y, uint32_t ys, double init,
+                              uint32_t n, bool pairs) {
+    if (!pairs) return chain(init, n, [&](uint32_t k) { return x[k]; });
+    return chain(init, 2 * n,
+                 [&](uint32_t k) { return (k & 1) ? y[(size_t)(k >> 1) * ys] : x[k >> 1]; });
+}
+MARS_HD inline void team_sums(const double* const* x, const double* const* y, const uint32_t* ys,
+                              const double* init, uint32_t nc, uint32_t n, bool pairs,
+                              double* out, const Team& T) {
+#ifdef __CUDA_ARCH__
+    if (T.lanes > 1) {
+        const uint32_t j = T.lane < nc ? T.lane : 0;
+        const double v = one_sum(x[j], pairs ? y[j] : nullptr, pairs ? ys[j] : 0, init[j], n, pairs);
+        for (uint32_t c = 0; c < nc; ++c) out[c] = __shfl_sync(0xffffffffu, v, c);
+        return;
+    }
+#endif
+    for (uint32_t j = 0; j < nc; ++j)
+        out[j] = one_sum(x[j], pairs ? y[j] : nullptr, pairs ? ys[j] : 0, init[j], n, pairs);
+}
+
 // One pass of the 2-D transforms of dct.rs:22-80: for every output idx < n*n (the team's
 // share, four interleaved per lane), out[idx] = the left-to-right sum from -0.0 over
 // i < n of a[abase(idx) + i * sa] * b[bbase(idx) + i * sb].  A base is (idx / n) * n
@@ -244,7 +271,8 @@ MARS_HD inline void residual_event_bits(const RateTable& t, uint32_t sc, const i
 
 // The leaf's event bits with a fresh domain predictor (emit_leaf, mars_format.rs:515-595;
 // the residual's events for mode 3, residual.rs), summed left to right from -0.0.  Mode 3
-// reads its events' bits from residual_event_bits.
+// reads its events' bits from residual_event_bits; without them (nzb null) the result is
+// the sum up to the first residual event, which the residual's events then continue.
 MARS_HD inline double leaf_bits(const RateTable& t, const Setup& s, const mars_leaf& leaf,
                                 uint32_t sc, const double* nzb = nullptr,
                                 const double* magb = nullptr) {
@@ -262,38 +290,25 @@ MARS_HD inline double leaf_bits(const RateTable& t, const Setup& s, const mars_l
         r += rbits(t, F_ISOMETRY, sc, leaf.isometry);
         r += rbits(t, F_DOM_ROW, sc, zigzag((int64_t)(leaf.dom_row / s.shift)));
         r += rbits(t, F_DOM_COL, sc, zigzag((int64_t)(leaf.dom_col / s.shift)));
-        if (leaf.mode == 3) {
+        if (leaf.mode == 3 && nzb) {
             // r > 0 here (every event costs bits), so adding a zero level's +0.0 is exact.
             const uint32_t n = leaf.size * leaf.size;
-            uint32_t i = 0;
-            for (; i + 4 <= n; i += 4) {
-                double x[8];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    x[2 * j] = nzb[i + j];
-                    x[2 * j + 1] = magb[i + j];
-                }
-#pragma unroll
-                for (int j = 0; j < 8; ++j) r += x[j];
-            }
-            for (; i < n; ++i) {
-                r += nzb[i];
-                r += magb[i];
-            }
+            r = chain(r, 2 * n, [&](uint32_t k) { return (k & 1) ? magb[k >> 1] : nzb[k >> 1]; });
         }
     }
     return r;
 }
 
-// affine_fit (encode.rs:1724-1781) on the block's doubles in range raster order.
-MARS_HD inline void affine_fit(const double* block, uint32_t size, uint32_t bits_beta,
-                               uint32_t* qbeta_out, int32_t* qgx_out, int32_t* qgy_out,
-                               double* sse_out) {
+// affine_fit (encode.rs:1724-1781) from the block's sums t0 = sum p, tu = sum p*u,
+// tv = sum p*v (each from 0.0, raster order): the quantised plane and its coefficients.
+struct Affine {
+    uint32_t qbeta;
+    int32_t qgx, qgy;
+    double b0q, gxq, gyq;
+};
+MARS_HD inline Affine affine_from_sums(double t0, double tu, double tv, uint32_t size,
+                                       uint32_t bits_beta) {
     const double n = (double)size * (double)size;
-    const uint32_t nn = size * size;
-    const double t0 = chain(0.0, nn, [&](uint32_t k) { return block[k]; });
-    const double tu = chain(0.0, nn, [&](uint32_t k) { return block[k] * (double)(k / size); });
-    const double tv = chain(0.0, nn, [&](uint32_t k) { return block[k] * (double)(k % size); });
     double su = -0.0, suu = -0.0;
     for (uint32_t u = 0; u < size; ++u) su += (double)u;
     for (uint32_t u = 0; u < size; ++u) suu += (double)u * (double)u;
@@ -324,25 +339,26 @@ MARS_HD inline void affine_fit(const double* block, uint32_t size, uint32_t bits
         gy = det3(a_gy) / det_a;
     }
     const uint32_t max_qbeta = (1u << bits_beta) - 1;
-    const uint32_t qbeta = quantise(dmax(b0 / 255.0 * (double)max_qbeta, 0.0), max_qbeta);
+    Affine f;
+    f.qbeta = quantise(dmax(b0 / 255.0 * (double)max_qbeta, 0.0), max_qbeta);
     auto qgrad = [](double g) {
         double r = round(g * kGradScale);
         if (r < -(double)kGradClamp) r = -(double)kGradClamp;
         if (r > (double)kGradClamp) r = (double)kGradClamp;
         return (int32_t)r;
     };
-    const int32_t qgx = qgrad(gx), qgy = qgrad(gy);
-    const double b0q = (double)qbeta / (double)max_qbeta * 255.0;
-    const double gxq = (double)qgx / kGradScale, gyq = (double)qgy / kGradScale;
-    const double sse = chain(0.0, nn, [&](uint32_t k) {
-        const double pred = b0q + gxq * (double)(k / size) + gyq * (double)(k % size);
-        const double diff = block[k] - pred;
-        return diff * diff;
-    });
-    *qbeta_out = qbeta;
-    *qgx_out = qgx;
-    *qgy_out = qgy;
-    *sse_out = sse;
+    f.qgx = qgrad(gx);
+    f.qgy = qgrad(gy);
+    f.b0q = (double)f.qbeta / (double)max_qbeta * 255.0;
+    f.gxq = (double)f.qgx / kGradScale;
+    f.gyq = (double)f.qgy / kGradScale;
+    return f;
+}
+// The squared error of pixel k against the quantised plane (affine_fit's SSE term).
+MARS_HD inline double affine_term(const Affine& f, double p, uint32_t k, uint32_t size) {
+    const double pred = f.b0q + f.gxq * (double)(k / size) + f.gyq * (double)(k % size);
+    const double diff = p - pred;
+    return diff * diff;
 }
 
 // Scratch of one node's pricing: five double and two int32 arrays of size*size each.
@@ -362,9 +378,10 @@ MARS_HD inline int64_t team_sum(int64_t v, const Team& T) {
     return v;
 }
 
-// residual_for_candidate (encode.rs:1783-1851): levels into sc.levels, returns the SSE of
-// the clamped, truncated reconstruction.
-MARS_HD inline double residual_for_candidate(const uint8_t* px, uint32_t stride, uint32_t size,
+// residual_for_candidate (encode.rs:1783-1851): levels into sc.levels and, in sc.pred, the
+// squared error of every pixel of the clamped, truncated reconstruction (their sum, from 0.0
+// in raster order, is the candidate's SSE).
+MARS_HD inline void residual_for_candidate(const uint8_t* px, uint32_t stride, uint32_t size,
                                              const Cand& c, const Setup& s, const double* b,
                                              const double* bt, Scratch& sc, const Team& T) {
     const double alfa = (double)c.qalfa / (double)(1u << s.bits_alfa) * s.max_alfa;
@@ -396,15 +413,17 @@ MARS_HD inline double residual_for_candidate(const uint8_t* px, uint32_t stride,
     }
     T.sync();
     inverse_dct2d(sc.resid, size, b, sc.tmp, sc.coef, T);  // coef <- the reconstruction
-    return chain(0.0, n, [&](uint32_t k) {
+    // The decoded pixels' squared errors replace the prediction, element by element.
+    for (uint32_t k = T.lane; k < n; k += T.lanes) {
         uint32_t i, j;
         iso_map(c.isometry, k / size, k % size, size, &i, &j);
         double pv = sc.pred[k] + sc.coef[k];
         if (pv < 0.0) pv = 0.0;
         if (pv > 255.0) pv = 255.0;
         const double diff = sc.block[i * size + j] - (double)(uint8_t)pv;
-        return diff * diff;
-    });
+        sc.pred[k] = diff * diff;
+    }
+    T.sync();
 }
 
 // The priced winner of one node.
@@ -436,6 +455,34 @@ MARS_HD inline Priced price_node(const uint8_t* px, uint32_t stride, uint32_t ro
     const int64_t rsum = team_sum(part, T);
     T.sync();
     const int64_t s0 = (int64_t)size * size;
+    // Mode 0's SSE and mode 1's moments t0, tu, tv: four independent sums side by side.
+    const uint32_t qbeta0 = best_beta(rsum, s0, s.bits_beta);
+    const double beta2 = (double)qbeta0 / (double)((1u << s.bits_beta) - 1) * 255.0;
+    for (uint32_t k = T.lane; k < n; k += T.lanes) {
+        const double p = sc.block[k];
+        sc.pred[k] = (p - beta2) * (p - beta2);
+        sc.resid[k] = p * (double)(k / size);
+        sc.tmp[k] = p * (double)(k % size);
+    }
+    T.sync();
+    double sums[4];
+    {
+        const double* xs[4] = {sc.pred, sc.block, sc.resid, sc.tmp};
+        const double init[4] = {-0.0, 0.0, 0.0, 0.0};
+        team_sums(xs, nullptr, nullptr, init, 4, n, false, sums, T);
+    }
+    T.sync();
+    Affine aff{};
+    double sse1 = 0.0;
+    if (s.allowed[1]) {
+        aff = affine_from_sums(sums[1], sums[2], sums[3], size, s.bits_beta);
+        for (uint32_t k = T.lane; k < n; k += T.lanes) sc.pred[k] = affine_term(aff, sc.block[k], k, size);
+        T.sync();
+        const double* xs[1] = {sc.pred};
+        const double init[1] = {0.0};
+        team_sums(xs, nullptr, nullptr, init, 1, n, false, &sse1, T);
+        T.sync();
+    }
     Priced best;
     best.leaf = make_leaf(row, col, size);
     best.d = best.r = 0.0;
@@ -455,21 +502,19 @@ MARS_HD inline Priced price_node(const uint8_t* px, uint32_t stride, uint32_t ro
     };
     auto mode0 = [&]() {
         mars_leaf l = make_leaf(row, col, size);
-        l.qbeta = best_beta(rsum, s0, s.bits_beta);
-        const double beta2 = (double)l.qbeta / (double)((1u << s.bits_beta) - 1) * 255.0;
-        const double sse = chain(-0.0, n, [&](uint32_t k) {
-            return (sc.block[k] - beta2) * (sc.block[k] - beta2);
-        });
-        offer(l, sse, leaf_bits(t, s, l, sc_class), false);
+        l.qbeta = qbeta0;
+        offer(l, sums[0], leaf_bits(t, s, l, sc_class), false);
     };
     if (s.allowed[0]) mode0();
     if (s.allowed[1]) {
         mars_leaf l = make_leaf(row, col, size);
         l.mode = 1;
-        double sse;
-        affine_fit(sc.block, size, s.bits_beta, &l.qbeta, &l.qgx, &l.qgy, &sse);
-        offer(l, sse, leaf_bits(t, s, l, sc_class), false);
+        l.qbeta = aff.qbeta;
+        l.qgx = aff.qgx;
+        l.qgy = aff.qgy;
+        offer(l, sse1, leaf_bits(t, s, l, sc_class), false);
     }
+    const double zero = 0.0;
     for (uint32_t ci = 0; ci < nranked; ++ci) {
         const Cand& c = *reinterpret_cast<const Cand*>(
             reinterpret_cast<const unsigned char*>(ranked) + (size_t)ci * cand_bytes);
@@ -487,10 +532,19 @@ MARS_HD inline Priced price_node(const uint8_t* px, uint32_t stride, uint32_t ro
         }
         if (s.allowed[3]) {
             l.mode = 3;
-            const double sse3 = residual_for_candidate(px, stride, size, c, s, b, bt, sc, T);
-            // resid and tmp are free once the reconstruction's SSE is taken.
+            residual_for_candidate(px, stride, size, c, s, b, bt, sc, T);
+            // resid and tmp are free once the reconstruction's squared errors are in pred.
             residual_event_bits(t, sc_class, sc.levels, n, sc.tmp, sc.resid, T);
-            offer(l, sse3, leaf_bits(t, s, l, sc_class, sc.tmp, sc.resid), true);
+            // The SSE (each term paired with +0.0: the sum is >= 0, so nothing changes) and
+            // the bits (the leaf's events up to the residual, then every coefficient's nonzero
+            // flag and magnitude) side by side.
+            double v[2];
+            const double* xs[2] = {sc.pred, sc.tmp};
+            const double* ys[2] = {&zero, sc.resid};
+            const uint32_t ystride[2] = {0, 1};
+            const double init[2] = {0.0, leaf_bits(t, s, l, sc_class)};
+            team_sums(xs, ys, ystride, init, 2, n, true, v, T);
+            offer(l, v[0], v[1], true);
         }
     }
     if (!have) mode0();
