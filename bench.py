@@ -51,6 +51,9 @@ WORKLOAD = ("exhaustive search of every RD quadtree node of a 512x512 synthetic 
 # DRAM bytes (read + write) per launch of the dominant search kernel, from one ncu capture
 # of this workload's s=4 level (profiles/corr_tc_s4_512x512_ncu.md).
 NCU_TRAFFIC = {4: 20_560_000}
+# Thread instructions per candidate fit of the correlation kernel's level (warp
+# instructions x 32 / fits, same capture): the issue cost behind the epilogue roofline.
+NCU_INSTR_PER_FIT = {4: 1.14e9 * 32 / 8.52e9, 8: 0.42e9 * 32 / 2.0e9}
 # The same for one decode iteration, by plane side (profiles/decode_cell_*_ncu.md; the
 # 16384^2 figure is dram__bytes.sum.per_second x gpu__time_duration.sum of its capture).
 NCU_DECODE_TRAFFIC = {4096: 34_831_104 + 748_800, 16384: 4_797_900_000}
@@ -192,10 +195,17 @@ def cpu_baseline(budget_s=12.0, seed=1):
         total_time += level_evals(size) * len(rows) / rate
         sampled[size] = m
     value = evals_per_step() / total_time
+    # One host thread on the s=8 level's first nodes, for the per-eval cost of one core.
+    rows, cols = level_nodes(8)
+    n1 = 8
+    t0 = time.perf_counter()
+    orc.search_blocks(img, 8, SHIFT, p, rows[:n1], cols[:n1], nthreads=1)
+    ns_per_eval = (time.perf_counter() - t0) / (n1 * level_evals(8)) * 1e9
     desc = ("oracle search_blocks on a random sample of the 512x512 seed-1 step's nodes per "
             f"level ({', '.join(f's{s}: {n} blocks' for s, n in sampled.items())}); per-level "
-            "fits/s combined over the full step's eval mix")
-    return value, cores, desc
+            "fits/s combined over the full step's eval mix; single_core_ns_per_eval: one "
+            f"thread on {n1} s=8 blocks")
+    return value, cores, desc, ns_per_eval
 
 
 DECODE_SIDE = 4096         # the decode GB/s figure: both planes (2 x 16.8 MB) fit in L2
@@ -402,6 +412,8 @@ def run_encode(mb, ctx, workers=3):
         t0 = time.perf_counter()
         ctx.encode_many(imgs, params, workers=workers, allowed_modes=modes)
         piped = len(imgs) / (time.perf_counter() - t0)
+        for _ in range(2):  # a geometry's second encode makes the context's plan for it
+            ctx.encode(imgs[0], params, allowed_modes=modes)
         t0 = time.perf_counter()
         for im in imgs:
             ctx.encode(im, params, allowed_modes=modes)
@@ -529,7 +541,7 @@ def run_reference(args):
     for _ in range(args.warmup):
         cpu_baseline(budget_s=2.0)
     for _ in range(args.steps):
-        v, cores, desc = cpu_baseline(budget_s=max(4.0, 40.0 / max(1, args.steps)))
+        v, cores, desc, _ = cpu_baseline(budget_s=max(4.0, 40.0 / max(1, args.steps)))
         vals.append(v)
     value = float(np.median(vals))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
@@ -647,6 +659,20 @@ def run_gpu(args):
         peak_tops = 2.0 * 1590.0
         peak_src = "2 x fallback bf16 1.59 PFLOP/s"
     achieved = ops / t_launch / 1e12
+    # The fused epilogue's bound at small s: every candidate costs NCU_INSTR_PER_FIT thread
+    # instructions, issued at most one warp instruction per scheduler (4 per SM) per clock.
+    epilogue = None
+    if dom in NCU_INSTR_PER_FIT:
+        props = torch.cuda.get_device_properties(dev)
+        clk_hz = 1965e6
+        fits_dom = level_evals(dom) * len(level_nodes(dom)[0])
+        peak_fits = props.multi_processor_count * 4 * clk_hz * 32 / NCU_INSTR_PER_FIT[dom]
+        epilogue = {"bound": "issue", "kernel": f"search level s={dom}",
+                    "achieved": fits_dom / t_launch, "peak": peak_fits, "unit": "fits/s",
+                    "frac": fits_dom / t_launch / peak_fits,
+                    "instr_per_fit": NCU_INSTR_PER_FIT[dom],
+                    "peak_source": f"{props.multi_processor_count} SMs x 4 issue slots x "
+                                   "1965 MHz x 32 threads / thread instructions per fit (ncu)"}
 
     # End to end through the public calls, host plane in and the node table back on the
     # host: the plan's run (what a caller encoding many planes of one size makes per plane)
@@ -698,8 +724,9 @@ def run_gpu(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, cores, desc = cpu_baseline()
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+        v, cores, desc, ns1 = cpu_baseline()
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc,
+               "single_core_ns_per_eval": ns1}
 
     if rank == 0:
         line = {
@@ -715,7 +742,8 @@ def run_gpu(args):
                          "frac": achieved / peak_tops, "traffic": NCU_TRAFFIC.get(dom),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum",
                          "peak_source": peak_src,
-                         "ops_per_launch": ops, "launch_ms": 1e3 * t_launch},
+                         "ops_per_launch": ops, "launch_ms": 1e3 * t_launch,
+                         "epilogue": epilogue},
             "per_level_ms": {str(s): 1e3 * per_level[s] / lvl_steps for s in SIZES},
             "launch": "one CUDA-graph launch per step (search plan), "
                       f"{plan_launches} kernel nodes",

@@ -395,48 +395,11 @@ class Context:
         leaf order."""
         a = _plane(img)
         h, w = a.shape
-        if (method == "exhaustive" and rd_candidates <= 1
-                and not (params.has_lambda and adaptive_density)):
-            plan = self._repeat_plan(w, h, params)
-            if plan is not None:
-                return plan.encode(a, allowed_modes=allowed_modes,
-                                   residual_adaptive=residual_adaptive,
-                                   residual_qstep=residual_qstep)
         opts = Options((C.c_uint8 * 4)(*allowed_modes), int(adaptive_density),
                        int(residual_adaptive), float(residual_qstep), METHODS[method],
                        int(rd_candidates))
         return _encode_call(lambda *out: lib().mars_encode(
             self._h, a.ctypes.data, w, h, C.byref(params), C.byref(opts), *out))
-
-    # Repeated encodes of one plane geometry go through a cached search plan (the search as
-    # one graph launch, both walks on the device); the first encode of a geometry takes the
-    # one-shot path, which builds no plan.  Plans are kept for planes of at most
-    # _REPEAT_PLAN_PIXELS pixels and for at most _REPEAT_PLANS geometries per context.
-    _REPEAT_PLANS = 8
-    _REPEAT_PLAN_PIXELS = 2048 * 2048
-
-    def _repeat_plan(self, width: int, height: int, params: Params):
-        import threading
-        lock = self.__dict__.setdefault("_repeat_lock", threading.Lock())
-        with lock:
-            if width * height > self._REPEAT_PLAN_PIXELS:
-                return None
-            key = (width, height, bytes(params))
-            plans = self.__dict__.setdefault("_plans", {})
-            if key in plans:
-                return plans[key]
-            seen = self.__dict__.setdefault("_seen", set())
-            made = self.__dict__.setdefault("_repeat_made", [0])
-            if key not in seen or made[0] >= self._REPEAT_PLANS:
-                seen.add(key)
-                return None
-            made[0] += 1
-            try:
-                plans[key] = self.search_plan(width, height, params)
-            except MarsError:
-                self._REPEAT_PLAN_PIXELS = 0  # this context keeps the one-shot path
-                return None
-            return plans[key]
 
     def encode_many(self, images, params: Params, workers: int = 3, **options):
         """encode() over many planes, `workers` at a time: the C ABI is thread-safe, so one

@@ -612,6 +612,8 @@ int mars_ctx_create(mars_ctx** out, int device) {
 
 void mars_ctx_destroy(mars_ctx* ctx) {
     if (!ctx) return;
+    for (auto& kp : ctx->plan_cache) mars_search_plan_free(kp.second);
+    ctx->plan_cache.clear();
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
@@ -946,6 +948,49 @@ int encode_on_tables(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32
 
 extern "C" {
 
+}  // extern "C"
+
+namespace {
+
+// The plan mars_encode uses for a plane geometry it has encoded before: one search plan
+// per (width, height, params), made on the second encode of that geometry (the first takes
+// the one-shot path), for planes up to kPlanCachePixels and at most kPlanCacheSize
+// geometries per context.  Null when the geometry should take the one-shot path.
+// MARS_PLAN_CACHE=0 turns the cache off.
+constexpr uint64_t kPlanCachePixels = 2048ull * 2048ull;
+constexpr size_t kPlanCacheSize = 8, kPlansSeen = 64;
+
+mars_search_plan* cached_encode_plan(mars_ctx* ctx, uint32_t w, uint32_t h,
+                                     const mars_params* p) {
+    static const bool off = [] {
+        const char* e = std::getenv("MARS_PLAN_CACHE");
+        return e && std::string(e) == "0";
+    }();
+    if (off || (uint64_t)w * h > kPlanCachePixels) return nullptr;
+    std::string key(reinterpret_cast<const char*>(&w), sizeof w);
+    key.append(reinterpret_cast<const char*>(&h), sizeof h);
+    key.append(reinterpret_cast<const char*>(p), sizeof *p);
+    std::lock_guard<std::mutex> lock(ctx->plan_cache_mu);
+    for (auto& kp : ctx->plan_cache)
+        if (kp.first == key) return kp.second;
+    auto seen = std::find(ctx->plans_seen.begin(), ctx->plans_seen.end(), key);
+    if (seen == ctx->plans_seen.end() || ctx->plan_cache.size() >= kPlanCacheSize) {
+        if (seen == ctx->plans_seen.end()) {
+            if (ctx->plans_seen.size() >= kPlansSeen) ctx->plans_seen.erase(ctx->plans_seen.begin());
+            ctx->plans_seen.push_back(key);
+        }
+        return nullptr;
+    }
+    mars_search_plan* plan = nullptr;
+    if (mars_search_plan_create(ctx, w, h, p, &plan) != MARS_OK) return nullptr;
+    ctx->plan_cache.emplace_back(key, plan);
+    return plan;
+}
+
+}  // namespace
+
+extern "C" {
+
 int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t height,
                 const mars_params* params, const mars_options* options, mars_header* header,
                 mars_leaf** leaves, size_t* nleaves, int32_t** residuals, size_t* nresiduals,
@@ -965,6 +1010,11 @@ int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t he
         return fail(MARS_EINVAL, "rd_candidates > 1 requires the exhaustive search; other "
                                  "methods propose one candidate");
     const bool adaptive = params->has_lambda && options->adaptive_density;
+    // A geometry met before: its search plan (one graph launch, both walks on the device).
+    if (options->method == MARS_METHOD_EXHAUSTIVE && rd_k == 1 && !adaptive)
+        if (mars_search_plan* plan = cached_encode_plan(ctx, width, height, params))
+            return mars_encode_planned(plan, plane, options, header, leaves, nleaves, residuals,
+                                       nresiduals, counters);
     // The final walk's provider (the options' method) and, for an RD encode, the
     // exhaustive table the warm-up walk reads (the warm-up is exhaustive for every method).
     mars_table* table = nullptr;

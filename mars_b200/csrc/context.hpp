@@ -9,6 +9,8 @@
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "../../include/mars_b200.h"
 
@@ -24,6 +26,10 @@ struct mars_ctx {
     int search_path = 0;                      // 0 auto, 1 CUDA cores only, 2 tensor cores
     bool tma_16_boxes = false;                // load A stages as 16 2-D boxes (A/B checks)
     PFN_cuTensorMapEncodeTiled_v12000 encode_tiled = nullptr;
+    // Search plans mars_encode keeps for plane geometries it has met before (api.cu).
+    std::mutex plan_cache_mu;
+    std::vector<std::pair<std::string, mars_search_plan*>> plan_cache;
+    std::vector<std::string> plans_seen;
 };
 
 namespace mars {
