@@ -381,7 +381,8 @@ def run_refine(mb, ctx, stream, dev, peaks, seeds=REFINE_SEEDS, lambdas=REFINE_L
                      for p in per_seed],
         "ms_per_refine": 1e3 * float(np.median(ref_t)),
         "encode": {"value": 1.0 / float(np.median(enc_t)), "unit": "images/s",
-                   "note": "ctx.encode (search table + host RD walks + mode-3 pricing) of one "
+                   "note": "ctx.encode (search, walks and mode pricing; from a geometry's "
+                           "second encode on through the context's search plan) of one "
                            "512x512 plane, host buffers in and leaves out, median over the "
                            f"{len(enc_t)} encodes above"},
         "us_per_forward_iter": 1e6 * t_fwd, "us_per_adjoint_iter": 1e6 * t_adj,
