@@ -454,6 +454,13 @@ int run_jobs_fisher(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t
     MARS_CUDA(sc.get(&ix.counts, 72));
     MARS_CUDA(sc.get(&ix.offsets, 72));
     MARS_CUDA(sc.get(&ix.ref, 72));
+    size_t max_part = 1;
+    for (const Job& j : jobs)
+        max_part = std::max(max_part, j.rows.size() * (size_t)mars::fisher_warps_per_range((int)j.size));
+    mars::CandidateOut* part = nullptr;
+    uint32_t* part_e = nullptr;
+    MARS_CUDA(sc.get(&part, max_part));
+    MARS_CUDA(sc.get(&part_e, max_part));
     off = 0;
     for (const Job& j : jobs) {
         const mars::LevelGeom g = level_geom(w, h, j.size, j.shift);
@@ -462,8 +469,8 @@ int run_jobs_fisher(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t
         MARS_CUDA(mars::launch_fisher_search(d_plane, (int)w, (int)h, d_D, dw, (int)j.size,
                                              (int)j.shift, std::max(ncol, 1), d_rc + off,
                                              d_rc + total + off, (int)j.rows.size(), ix, fp,
-                                             d_out + off, d_evals + off, st));
-        ctx->launches += nrow * ncol > 0 ? 5 : 3;
+                                             d_out + off, d_evals + off, part, part_e, st));
+        ctx->launches += (nrow * ncol > 0 ? 5 : 3) + (mars::fisher_warps_per_range((int)j.size) > 1);
         off += j.rows.size();
     }
     return MARS_OK;

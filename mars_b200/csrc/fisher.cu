@@ -185,21 +185,30 @@ __global__ void fisher_fill_kernel(const uint8_t* __restrict__ key, int n,
     }
 }
 
-// One warp per range block.  Shared memory per warp: the 8 permuted copies of the range
-// (permute_range, encode.rs:833-842: range_k[u*s + v] = range[map(k, u, v)]).
+// `wpr` warps per range block (1, or 2 / 4 for the large sizes, whose levels have few
+// ranges): warp `sub` of a range takes the bucket candidates e = 32 sub + lane,
+// 32 sub + lane + 32 wpr, ...; with wpr > 1 each warp leaves its first minimum in `part`
+// and fisher_merge_kernel picks the range's (rms, bucket index) minimum.  Shared memory per
+// warp: the 8 permuted copies of the range (permute_range, encode.rs:833-842:
+// range_k[u*s + v] = range[map(k, u, v)]).
 constexpr int kFisherWarps = 4;
+constexpr uint32_t kNoCandidate = 0xffffffffu;
 
 __global__ void __launch_bounds__(32 * kFisherWarps) fisher_search_kernel(
     const uint8_t* __restrict__ plane, int w, int h, const int32_t* __restrict__ D, int dw,
     int size, int shift, int ncol_d, const uint32_t* __restrict__ rows,
     const uint32_t* __restrict__ cols, int nranges, const uint32_t* __restrict__ counts,
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ ref,
-    const uint32_t* __restrict__ list, const uint8_t* __restrict__ diso, FitParams fp,
-    CandidateOut* __restrict__ out, uint64_t* __restrict__ evals_out) {
+    const uint32_t* __restrict__ list, const uint8_t* __restrict__ diso, FitParams fp, int wpr,
+    CandidateOut* __restrict__ out, uint64_t* __restrict__ evals_out,
+    CandidateOut* __restrict__ part, uint32_t* __restrict__ part_e) {
     extern __shared__ uint8_t smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ri = blockIdx.x * kFisherWarps + warp;
+    const int gw = blockIdx.x * kFisherWarps + warp;
+    const int ri = gw / wpr, sub = gw % wpr;
     if (ri >= nranges) return;
+    // Where this warp's answer goes: the range's output, or its slot among the partials.
+    CandidateOut* const dst = wpr == 1 ? out + ri : part + (size_t)ri * wpr + sub;
     const int n = size * size, hq = size / 2;
     uint8_t* perm = smem + (size_t)warp * 8 * n;
     const uint32_t row = rows[ri], col = cols[ri];
@@ -210,8 +219,9 @@ __global__ void __launch_bounds__(32 * kFisherWarps) fisher_search_kernel(
     if (row + size > (uint32_t)h || col + size > (uint32_t)w) {
         // Blocks outside the plane are reported as no candidate and no evals.
         if (lane == 0) {
-            out[ri] = res;
-            evals_out[ri] = 0;
+            *dst = res;
+            if (wpr > 1) part_e[(size_t)ri * wpr + sub] = kNoCandidate;
+            if (sub == 0) evals_out[ri] = 0;
         }
         return;
     }
@@ -260,7 +270,7 @@ __global__ void __launch_bounds__(32 * kFisherWarps) fisher_search_kernel(
     uint32_t best_e = 0xffffffffu;
     FitResult best_fit{};
     int64_t best_s1 = 0, best_s2 = 0, best_t1 = 0;
-    for (uint32_t e = lane; e < len; e += 32) {
+    for (uint32_t e = 32u * sub + lane; e < len; e += 32u * wpr) {
         const uint32_t p = list[off + e];
         const int iso = kMapping[isom][diso[p]];
         const int dr = (int)((p / ncol_d) * shift / 2), dc = (int)((p % ncol_d) * shift / 2);
@@ -311,12 +321,34 @@ __global__ void __launch_bounds__(32 * kFisherWarps) fisher_search_kernel(
         res.t0 = t0;
         res.t1_x4 = best_t1;
         res.t2 = t2;
-        out[ri] = res;
-        evals_out[ri] = len;
+        *dst = res;
+        if (wpr > 1) part_e[(size_t)ri * wpr + sub] = ie;
     } else if (ie == 0xffffffffu && lane == 0) {
-        out[ri] = res;
-        evals_out[ri] = 0;
+        *dst = res;
+        if (wpr > 1) part_e[(size_t)ri * wpr + sub] = kNoCandidate;
     }
+    if (sub == 0 && lane == 0) evals_out[ri] = len;
+}
+
+// The range's answer from its warps' first minima: the smallest rms, then the smallest
+// bucket index (the first minimum in bucket order).
+__global__ void fisher_merge_kernel(const CandidateOut* __restrict__ part,
+                                    const uint32_t* __restrict__ part_e, int wpr, int nranges,
+                                    CandidateOut* __restrict__ out) {
+    const int ri = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ri >= nranges) return;
+    int best = -1;
+    for (int s = 0; s < wpr; ++s) {
+        const uint32_t e = part_e[(size_t)ri * wpr + s];
+        if (e == kNoCandidate) continue;
+        if (best < 0) {
+            best = s;
+            continue;
+        }
+        const double r = part[(size_t)ri * wpr + s].rms, rb = part[(size_t)ri * wpr + best].rms;
+        if (r < rb || (r == rb && e < part_e[(size_t)ri * wpr + best])) best = s;
+    }
+    out[ri] = part[(size_t)ri * wpr + (best < 0 ? 0 : best)];
 }
 
 }  // namespace
@@ -337,18 +369,26 @@ cudaError_t launch_fisher_search(const uint8_t* plane, int w, int h, const int32
                                  int size, int shift, int ncol_d, const uint32_t* rows,
                                  const uint32_t* cols, int nranges, FisherIndex ix,
                                  const FitParams& fp, CandidateOut* out, uint64_t* evals,
-                                 cudaStream_t st) {
+                                 CandidateOut* part, uint32_t* part_e, cudaStream_t st) {
     if (nranges <= 0) return cudaSuccess;
+    const int wpr = fisher_warps_per_range(size);
     const size_t smem = (size_t)kFisherWarps * 8 * size * size;
     if (smem > 48 * 1024) {
         const cudaError_t e = cudaFuncSetAttribute(
             fisher_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    fisher_search_kernel<<<(nranges + kFisherWarps - 1) / kFisherWarps, 32 * kFisherWarps, smem,
-                           st>>>(plane, w, h, D, dw, size, shift, ncol_d, rows, cols, nranges,
-                                 ix.counts, ix.offsets, ix.ref, ix.list, ix.diso, fp, out, evals);
+    const long long warps = (long long)nranges * wpr;
+    fisher_search_kernel<<<(unsigned)((warps + kFisherWarps - 1) / kFisherWarps),
+                           32 * kFisherWarps, smem, st>>>(
+        plane, w, h, D, dw, size, shift, ncol_d, rows, cols, nranges, ix.counts, ix.offsets,
+        ix.ref, ix.list, ix.diso, fp, wpr, out, evals, part, part_e);
+    if (wpr > 1)
+        fisher_merge_kernel<<<(nranges + 127) / 128, 128, 0, st>>>(part, part_e, wpr, nranges,
+                                                                   out);
     return cudaGetLastError();
 }
+
+int fisher_warps_per_range(int size) { return size >= 16 ? 4 : (size == 8 ? 2 : 1); }
 
 }  // namespace mars

@@ -108,7 +108,10 @@ cudaError_t launch_fisher_search(const uint8_t* plane, int w, int h, const int32
                                  int size, int shift, int ncol_d, const uint32_t* rows,
                                  const uint32_t* cols, int nranges, FisherIndex ix,
                                  const FitParams& fp, CandidateOut* out, uint64_t* evals,
-                                 cudaStream_t st);
+                                 CandidateOut* part, uint32_t* part_e, cudaStream_t st);
+// Warps per range block of the Fisher search at a size; part / part_e need
+// nranges * fisher_warps_per_range(size) entries when that is above 1.
+int fisher_warps_per_range(int size);
 
 // ---- colour and metrics (color.cu) ----
 // ycbcr (inverse = false: r, g, b -> y, cb, cr) or rgb_from_ycbcr (inverse = true: y, cb, cr
