@@ -48,14 +48,17 @@ WORKLOAD = ("exhaustive search of every RD quadtree node of a 512x512 synthetic 
             "block sizes 32..4, domain stride 2, 8 isometries, seeds 1-8")
 
 
-# DRAM bytes (read + write) per launch of the dominant search kernel, from one ncu capture
-# of this workload's s=4 level (profiles/corr_tc_s4_512x512_ncu.md).
+# Figures that only ncu measures (bench.py cannot run under a profiler), copied from the
+# committed captures named beside them; re-captured whenever the kernel changes.
+# DRAM bytes (read + write) per launch of the dominant search kernel, s=4 level.
+NCU_SOURCE = "profiles/corr_tc_s4_512x512_ncu.md"
 NCU_TRAFFIC = {4: 20_560_000}
 # Thread instructions per candidate fit of the correlation kernel's level (warp
 # instructions x 32 / fits, same capture): the issue cost behind the epilogue roofline.
 NCU_INSTR_PER_FIT = {4: 1.14e9 * 32 / 8.52e9, 8: 0.42e9 * 32 / 2.0e9}
-# The same for one decode iteration, by plane side (profiles/decode_cell_*_ncu.md; the
-# 16384^2 figure is dram__bytes.sum.per_second x gpu__time_duration.sum of its capture).
+# DRAM bytes of one decode iteration, by plane side (profiles/decode_cell_4096x4096_ncu.md,
+# profiles/decode_cell_16384x16384_ncu.md; the 16384^2 figure is
+# dram__bytes.sum.per_second x gpu__time_duration.sum of its capture).
 NCU_DECODE_TRAFFIC = {4096: 34_831_104 + 748_800, 16384: 4_797_900_000}
 
 
@@ -168,44 +171,45 @@ class ClockSampler:
                 "source": "nvml" if self._nvml else "nvidia-smi"}
 
 
-def cpu_baseline(budget_s=12.0, seed=1):
-    """The oracle (reference CPU search restated in C++) on a bounded sample of the step's
-    nodes, all host threads.  Returns (fits/s, description)."""
+def cpu_sample_blocks(cores):
+    """Blocks per level of the CPU sample: 8 per host thread (every thread busy through the
+    oracle's one-block dynamic schedule), capped at the level's node count.  The GPU line's
+    cpu_baseline and the reference arm use this same sample."""
+    return {s: min(len(level_nodes(s)[0]), 8 * cores) for s in SIZES}
+
+
+def cpu_baseline(seed=1, single_core=True):
+    """The oracle (reference CPU search restated in C++) on a fixed random sample of the
+    step's nodes per level, all host threads.  Returns (fits/s over the full step's eval
+    mix, cores, description, single-core ns per eval or None, measured sample seconds)."""
     from oracle import oracle as orc
     img = synthetic.gray(W, H, seed)
     p = orc.make_params(min_size=4, max_size=32, shift=SHIFT)
     cores = os.cpu_count() or 1
-    per_level = budget_s / len(SIZES)
-    total_time = 0.0
-    sampled = {}
+    counts = cpu_sample_blocks(cores)
+    total_time = sample_s = 0.0
     for size in SIZES:
         rows, cols = level_nodes(size)
-        rng = np.random.default_rng(size)
-        order = rng.permutation(len(rows))
-        m, el = max(1, cores // 2), 0.0
-        while True:
-            pick = order[:m]
-            t0 = time.perf_counter()
-            orc.search_blocks(img, size, SHIFT, p, rows[pick], cols[pick], nthreads=0)
-            el = time.perf_counter() - t0
-            if el >= per_level / 4 or m >= len(rows):
-                break
-            m = min(len(rows), m * 2)
-        rate = m * level_evals(size) / el
+        pick = np.random.default_rng(size).permutation(len(rows))[:counts[size]]
+        t0 = time.perf_counter()
+        orc.search_blocks(img, size, SHIFT, p, rows[pick], cols[pick], nthreads=0)
+        el = time.perf_counter() - t0
+        sample_s += el
+        rate = len(pick) * level_evals(size) / el
         total_time += level_evals(size) * len(rows) / rate
-        sampled[size] = m
     value = evals_per_step() / total_time
-    # One host thread on the s=8 level's first nodes, for the per-eval cost of one core.
-    rows, cols = level_nodes(8)
-    n1 = 8
-    t0 = time.perf_counter()
-    orc.search_blocks(img, 8, SHIFT, p, rows[:n1], cols[:n1], nthreads=1)
-    ns_per_eval = (time.perf_counter() - t0) / (n1 * level_evals(8)) * 1e9
-    desc = ("oracle search_blocks on a random sample of the 512x512 seed-1 step's nodes per "
-            f"level ({', '.join(f's{s}: {n} blocks' for s, n in sampled.items())}); per-level "
-            "fits/s combined over the full step's eval mix; single_core_ns_per_eval: one "
-            f"thread on {n1} s=8 blocks")
-    return value, cores, desc, ns_per_eval
+    ns_per_eval = None
+    if single_core:
+        # One host thread on the s=8 level's first nodes, for the per-eval cost of one core.
+        rows, cols = level_nodes(8)
+        t0 = time.perf_counter()
+        orc.search_blocks(img, 8, SHIFT, p, rows[:8], cols[:8], nthreads=1)
+        ns_per_eval = (time.perf_counter() - t0) / (8 * level_evals(8)) * 1e9
+    desc = ("oracle search_blocks (one block per OpenMP work item) on a fixed random sample of "
+            "the 512x512 seed-1 step's nodes per level "
+            f"({', '.join(f's{s}: {n} blocks' for s, n in counts.items())}), {cores} threads; "
+            "per-level fits/s combined over the full step's eval mix")
+    return value, cores, desc, ns_per_eval, sample_s
 
 
 DECODE_SIDE = 4096         # the decode GB/s figure: both planes (2 x 16.8 MB) fit in L2
@@ -537,22 +541,28 @@ def run_reference(args):
     rank, world, _ = rank_info()
     if rank != 0:
         return 0
-    vals = []
+    vals, secs = [], []
     desc, cores = "", os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_baseline(budget_s=2.0)
+    # One warm-up sample at most: every sample is the same few seconds of CPU work.
+    for _ in range(min(args.warmup, 1)):
+        cpu_baseline(single_core=False)
     for _ in range(args.steps):
-        v, cores, desc, _ = cpu_baseline(budget_s=max(4.0, 40.0 / max(1, args.steps)))
+        v, cores, desc, _, s = cpu_baseline(single_core=False)
         vals.append(v)
+        secs.append(s)
     value = float(np.median(vals))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * evals_per_step() / value, "higher_is_better": True,
+            # A step here is one bounded sample of the workload (its measured seconds); the
+            # full 512x512 step's time is extrapolated from the sample's per-level rates.
+            "ms_per_step": 1e3 * float(np.mean(secs)),
+            "extrapolated_ms_per_full_step": 1e3 * evals_per_step() / value,
+            "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "i64/f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "image": "512x512", "sizes": list(SIZES),
                        "shift": SHIFT, "evals_per_step": evals_per_step()},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": desc},
+                             "sample": desc, "sample_seconds": float(np.median(secs))},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "note": "the reference's Rust (cargo) is not installed in this image; its CPU "
@@ -665,15 +675,16 @@ def run_gpu(args):
     epilogue = None
     if dom in NCU_INSTR_PER_FIT:
         props = torch.cuda.get_device_properties(dev)
-        clk_hz = 1965e6
+        clk_mhz = clocks.summary()["sm_mhz"] or 1965.0  # median SM clock of the timed region
         fits_dom = level_evals(dom) * len(level_nodes(dom)[0])
-        peak_fits = props.multi_processor_count * 4 * clk_hz * 32 / NCU_INSTR_PER_FIT[dom]
+        peak_fits = props.multi_processor_count * 4 * clk_mhz * 1e6 * 32 / NCU_INSTR_PER_FIT[dom]
         epilogue = {"bound": "issue", "kernel": f"search level s={dom}",
                     "achieved": fits_dom / t_launch, "peak": peak_fits, "unit": "fits/s",
                     "frac": fits_dom / t_launch / peak_fits,
                     "instr_per_fit": NCU_INSTR_PER_FIT[dom],
                     "peak_source": f"{props.multi_processor_count} SMs x 4 issue slots x "
-                                   "1965 MHz x 32 threads / thread instructions per fit (ncu)"}
+                                   f"{clk_mhz:.0f} MHz (sampled median) x 32 threads / thread "
+                                   f"instructions per fit ({NCU_SOURCE})"}
 
     # End to end through the public calls, host plane in and the node table back on the
     # host: the plan's run (what a caller encoding many planes of one size makes per plane)
@@ -725,9 +736,9 @@ def run_gpu(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, cores, desc, ns1 = cpu_baseline()
+        v, cores, desc, ns1, secs = cpu_baseline()
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc,
-               "single_core_ns_per_eval": ns1}
+               "sample_seconds": secs, "single_core_ns_per_eval": ns1}
 
     if rank == 0:
         line = {
@@ -741,7 +752,8 @@ def run_gpu(args):
             "roofline": {"bound": "tensor", "kernel": f"search level s={dom}",
                          "achieved": achieved, "peak": peak_tops, "unit": "TOP/s",
                          "frac": achieved / peak_tops, "traffic": NCU_TRAFFIC.get(dom),
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                           f"({NCU_SOURCE})",
                          "peak_source": peak_src,
                          "ops_per_launch": ops, "launch_ms": 1e3 * t_launch,
                          "epilogue": epilogue},

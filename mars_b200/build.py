@@ -9,6 +9,7 @@ import shutil
 import subprocess
 import sys
 import tempfile
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -48,13 +49,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
               "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
               "-Xptxas", "-v" if verbose else "-O3"]
     with tempfile.TemporaryDirectory() as tmp:
-        objects = []
-        for src in EXACT_F64_SOURCES:
-            obj = os.path.join(tmp, os.path.splitext(src)[0] + ".o")
-            _run([*common, "--fmad=false", "-c", "-o", obj, os.path.join(CSRC, src)], verbose)
-            objects.append(obj)
-        _run([*common, "-shared", "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES],
-              *objects], verbose)
+        # One object per translation unit, compiled in parallel, then one link.
+        jobs = [(src, []) for src in SOURCES] + [(src, ["--fmad=false"]) for src in EXACT_F64_SOURCES]
+        objects = [os.path.join(tmp, os.path.splitext(src)[0] + ".o") for src, _ in jobs]
+
+        def compile_one(i):
+            src, extra = jobs[i]
+            _run([*common, *extra, "-c", "-o", objects[i], os.path.join(CSRC, src)], verbose)
+
+        with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as pool:
+            list(pool.map(compile_one, range(len(jobs))))
+        _run([*common, "-shared", "-o", LIB + ".tmp", *objects], verbose)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -48,6 +48,43 @@ bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
 namespace mars {
 // The message mars_last_error() reports, for entry points defined in other files.
 int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+
+int check_fit_params(const mars_params& p) {
+    if (p.bits_alfa < 1 || p.bits_alfa > 16 || p.bits_beta < 1 || p.bits_beta > 16)
+        return set_last_error(MARS_EINVAL, "bits_alfa/bits_beta must be in 1..16");
+    if (!(p.max_alfa > 0.0) || !std::isfinite(p.max_alfa))
+        return set_last_error(MARS_EINVAL, "max_alfa must be finite and positive");
+    return MARS_OK;
+}
+
+FitParams make_fit_params(const mars_params& p) {
+    FitParams fp;
+    fp.max_alfa = p.max_alfa;
+    fp.bits_alfa = p.bits_alfa;
+    fp.bits_beta = p.bits_beta;
+    const double a = p.max_alfa / (double)(1u << p.bits_alfa);  // exact (power-of-two scale)
+    float af = (float)a;
+    if ((double)af > a) af = std::nextafter(af, 0.0f);
+    fp.a_min = af;
+    fp.two_a = 2.0f * af;
+    fp.a_half = 0.5f * af;
+    fp.eta_per_n = 1e-6 * (1.0 + p.max_alfa) * (1.0 + p.max_alfa);
+    return fp;
+}
+
+LevelGeom level_geom(uint32_t w, uint32_t h, uint32_t size, uint32_t shift) {
+    LevelGeom g;
+    g.size = (int)size;
+    g.shift = (int)shift;
+    g.step_c = (int)(shift / 2);
+    g.dw = (int)(w / 2);
+    g.dh = (int)(h / 2);
+    g.w = (int)w;
+    g.h = (int)h;
+    g.nrow_d = h >= 2 * size ? (int)((h - 2 * size) / shift + 1) : 0;
+    g.ncol_d = w >= 2 * size ? (int)((w - 2 * size) / shift + 1) : 0;
+    return g;
+}
 }  // namespace mars
 
 struct mars_table {
@@ -114,10 +151,7 @@ int sync_bounded(mars_ctx* ctx, cudaStream_t stream = nullptr) {
 
 int check_params(const mars_params* p) {
     if (!p) return fail(MARS_EINVAL, "params is NULL");
-    if (p->bits_alfa < 1 || p->bits_alfa > 16 || p->bits_beta < 1 || p->bits_beta > 16)
-        return fail(MARS_EINVAL, "bits_alfa/bits_beta must be in 1..16");
-    if (!(p->max_alfa > 0.0) || !std::isfinite(p->max_alfa))
-        return fail(MARS_EINVAL, "max_alfa must be finite and positive");
+    if (int e = mars::check_fit_params(*p)) return e;
     if (p->shift == 0 || (p->shift & 1))
         return fail(MARS_EUNSUPPORTED, "the domain stride must be even (the reference CLI "
                                        "enforces an even shift in 2..=254)");
@@ -130,34 +164,9 @@ int check_params(const mars_params* p) {
     return MARS_OK;
 }
 
-mars::FitParams make_fit_params(const mars_params& p) {
-    mars::FitParams fp;
-    fp.max_alfa = p.max_alfa;
-    fp.bits_alfa = p.bits_alfa;
-    fp.bits_beta = p.bits_beta;
-    const double a = p.max_alfa / (double)(1u << p.bits_alfa);  // exact (power-of-two scale)
-    float af = (float)a;
-    if ((double)af > a) af = std::nextafter(af, 0.0f);
-    fp.a_min = af;
-    fp.two_a = 2.0f * af;
-    fp.a_half = 0.5f * af;
-    fp.eta_per_n = 1e-6 * (1.0 + p.max_alfa) * (1.0 + p.max_alfa);
-    return fp;
-}
+using mars::level_geom;
+using mars::make_fit_params;
 
-mars::LevelGeom level_geom(uint32_t w, uint32_t h, uint32_t size, uint32_t shift) {
-    mars::LevelGeom g;
-    g.size = (int)size;
-    g.shift = (int)shift;
-    g.step_c = (int)(shift / 2);
-    g.dw = (int)(w / 2);
-    g.dh = (int)(h / 2);
-    g.w = (int)w;
-    g.h = (int)h;
-    g.nrow_d = h >= 2 * size ? (int)((h - 2 * size) / shift + 1) : 0;
-    g.ncol_d = w >= 2 * size ? (int)((w - 2 * size) / shift + 1) : 0;
-    return g;
-}
 
 // Grow-nothing scratch: every buffer is taken from the stream-ordered pool and returned
 // to it at the end of the call (the pool keeps the memory cached between calls).

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/mars_b200.h"
+#include "kernels.cuh"
 
 struct mars_ctx {
     int device = 0;
@@ -38,4 +39,11 @@ int set_last_error(int code, const std::string& msg);
 // Waits for the context's stream with the library's deadline (MARS_SYNC_TIMEOUT_S) and
 // turns kernel-reported errors into a status.  The caller holds ctx->mu.
 int ctx_sync(mars_ctx* ctx);
+// The bits_alfa / bits_beta / max_alfa checks every search entry point makes (MARS_EINVAL
+// with a message on failure).
+int check_fit_params(const mars_params& p);
+// The device-side fit constants of a parameter set (fit.cuh).
+FitParams make_fit_params(const mars_params& p);
+// The domain pool geometry of one (size, shift) level of a w x h plane.
+LevelGeom level_geom(uint32_t w, uint32_t h, uint32_t size, uint32_t shift);
 }  // namespace mars

@@ -13,6 +13,7 @@
 #include <string>
 
 #include "../../include/mars_b200.h"
+#include "context.hpp"
 #include "kernels.cuh"
 
 namespace {
@@ -26,10 +27,6 @@ std::mutex g_mu;
 void* g_scratch_addr[kMaxDevices] = {};
 
 }  // namespace
-
-namespace mars {
-int set_last_error(int code, const std::string& msg);  // api.cu
-}  // namespace mars
 
 namespace {
 
@@ -63,9 +60,7 @@ extern "C" int mars_search_blocks_noalloc(const uint8_t* d_plane, uint32_t width
     if (size < 2 || size > 64 || (size & (size - 1)))
         return fail(MARS_EINVAL, "size must be a power of two in 2..64");
     if (shift == 0 || (shift & 1)) return fail(MARS_EUNSUPPORTED, "shift must be even");
-    if (params->bits_alfa < 1 || params->bits_alfa > 16 || params->bits_beta < 1 ||
-        params->bits_beta > 16 || !(params->max_alfa > 0.0) || !std::isfinite(params->max_alfa))
-        return fail(MARS_EINVAL, "bits_alfa/bits_beta must be in 1..16 and max_alfa positive");
+    if (int e = mars::check_fit_params(*params)) return e;
     if (width == 0 || height == 0 || width > 65535 || height > 65535)
         return fail(MARS_EINVAL, "plane dimensions must be in 1..65535");
     if (n == 0) return MARS_OK;
@@ -76,16 +71,7 @@ extern "C" int mars_search_blocks_noalloc(const uint8_t* d_plane, uint32_t width
     if (cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
         return fail(MARS_ENODEV, "cannot query the current device");
 
-    mars::LevelGeom g;
-    g.size = (int)size;
-    g.shift = (int)shift;
-    g.step_c = (int)(shift / 2);
-    g.dw = (int)(width / 2);
-    g.dh = (int)(height / 2);
-    g.w = (int)width;
-    g.h = (int)height;
-    g.nrow_d = height >= 2 * size ? (int)((height - 2 * size) / shift + 1) : 0;
-    g.ncol_d = width >= 2 * size ? (int)((width - 2 * size) / shift + 1) : 0;
+    const mars::LevelGeom g = mars::level_geom(width, height, size, shift);
     const cudaStream_t st = (cudaStream_t)stream;
     if (g.nrow_d <= 0 || g.ncol_d <= 0) {
         const cudaError_t e = cudaMemsetAsync(d_out, 0, n * sizeof(mars_candidate), st);
@@ -124,17 +110,7 @@ extern "C" int mars_search_blocks_noalloc(const uint8_t* d_plane, uint32_t width
     ds.sdetf = reinterpret_cast<float*>(base + off[9]);
     mars::Partial* partials = reinterpret_cast<mars::Partial*>(base + off[10]);
 
-    mars::FitParams fp;
-    fp.max_alfa = params->max_alfa;
-    fp.bits_alfa = params->bits_alfa;
-    fp.bits_beta = params->bits_beta;
-    const double a = params->max_alfa / (double)(1u << params->bits_alfa);
-    float af = (float)a;
-    if ((double)af > a) af = std::nextafter(af, 0.0f);
-    fp.a_min = af;
-    fp.two_a = 2.0f * af;
-    fp.a_half = 0.5f * af;
-    fp.eta_per_n = 1e-6 * (1.0 + params->max_alfa) * (1.0 + params->max_alfa);
+    const mars::FitParams fp = mars::make_fit_params(*params);
 
     cudaError_t e = mars::launch_contract(d_plane, (int)width, (int)height, d_D, st);
     if (e == cudaSuccess)

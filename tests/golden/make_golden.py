@@ -1,7 +1,8 @@
 """Regenerates the committed golden fixtures from the reference checkout.
 
-Run once in a container that has the reference at REFERENCE (default /root/reference);
-the outputs are committed, so the tests never read the reference at run time.
+Run once in a container that has the reference checkout, named by --reference or the
+MARS_REFERENCE environment variable; the outputs are committed, so the tests never read the
+reference at run time.
 
   * mars1/<stem>.ifs + mars1_manifest.json -- the reference's 142 Mars 1 golden .ifs
     streams (fixtures/mars1/) with the pinned transform counts, stream SHA-256 and
@@ -29,9 +30,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("MARS_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("MARS_REFERENCE"))
     args = ap.parse_args()
     ref = args.reference
+    if not ref:
+        ap.error("name the reference checkout with --reference or MARS_REFERENCE")
 
     # --- Mars 1 .ifs streams and their pinned decode hashes
     with open(os.path.join(ref, "fixtures/mars1/manifest.toml"), "rb") as f:
