@@ -1361,7 +1361,7 @@ int orc_search_blocks(const uint8_t* px, uint32_t w, uint32_t h, uint32_t size, 
     Contracted c = Contracted::build(im);
 #ifdef _OPENMP
     const int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
 #else
     (void)nthreads;
 #endif
