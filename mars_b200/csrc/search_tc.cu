@@ -59,7 +59,11 @@ constexpr int kRangesPerTile = kN / 8;         // 32
 constexpr int kStageA = 16 * 1024;             // 16 row groups x 8 K-groups x 128 B
 constexpr int kStageB = 32 * 1024;             // 32 row groups x 8 K-groups x 128 B
 constexpr int kQueueCap = 2048;                // survivors the queue can hold
-constexpr int kFlush = 256;                    // drain the queue once it holds this many
+// Each epilogue warp owns kWarpCap consecutive queue entries and its own count, so no warp
+// reads a count another warp may still be adding to; the queue is drained when any warp's
+// region holds kWarpFlush entries.
+constexpr int kWarpCap = kQueueCap / kEpiWarps;  // 256
+constexpr int kWarpFlush = 48;
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 1.965 GHz
 
 // Pipeline depth: as many A stages as fit beside the resident B tile (S <= 8), otherwise
@@ -238,13 +242,21 @@ struct Champ {
 //   g1 = sqrt_w * sqrt(Ndd);  tau_z = min(w2a + a_half*Ndd, max(g1, a_min*Ndd));
 //   tau = (dom > tie) ? tau_z : g1 + neg;   prune  <=>  t1' < s1_x4 * c + 4 tau / n.
 // tie = -1 puts every domain in the Z-form, INT32_MAX none; neg = 0 or -inf (W <= 0).
+// Since tau_z >= g1 whenever W > 0 (W/(2a) + a*Ndd/2 >= sqrt(W*Ndd) by the AM-GM
+// inequality, and max(g1, .) >= g1), the short form  t1' < s1_x4 * c + (g1 + neg) * 4/n
+// is a valid threshold for every range with W > 0, whatever its tie mode; it is also the
+// exact threshold outside the Z-form.  It differs from the full one only when
+// a_min^2 * Ndd > W, which the best candidates of a range almost never meet, so it prunes
+// the same candidates at a third of the instructions.  `full` marks the ranges that need
+// the full form: a Z-form range with W <= 0, for which the short form prunes nothing.
 struct __align__(16) ThrRec {
     float sqrt_w, w2a, neg, c;  // sqrt_w, w2a, neg pre-scaled by 4 / n (exact: n = 4^k)
-    int32_t tie, pad0, pad1, pad2;
+    int32_t tie, full, pad1, pad2;
 };
 
 // A survivor waiting for its exact fit.  Survivors of several tiles are batched: the
-// queue is drained when it holds kFlush entries, when a tile overflows it, and at the end.
+// queue is drained when a warp's region holds kWarpFlush entries, when a tile overflows a
+// region, and at the end.
 struct __align__(8) QEntry {
     int32_t t1;     // t1' = t1_x4 - 128 * s1_x4
     uint32_t dom;   // domain position index (row-major)
@@ -261,8 +273,8 @@ struct Smem {
     uint64_t bres;
     uint32_t tmem_base;
     int abort_flag;
-    int qcount;
-    int overflow_seen;
+    int wcount[kEpiWarps];  // entries each epilogue warp queued (may exceed kWarpCap)
+    uint32_t full_bits;     // bit r: range r of the tile needs the full threshold form
     unsigned long long key_rms[kRangesPerTile];  // per-pass winner: f64 bits (rms >= 0)
     uint32_t key_idx[kRangesPerTile];
     double key_sum[kRangesPerTile];
@@ -285,9 +297,11 @@ __device__ __forceinline__ void publish_threshold(Smem& sm, int rl, const FitPar
     ThrRec t;
     if (!C.valid) {
         // An invalid range never survives: in the Z-form (tie = -1) with sqrt_w = w2a =
-        // +inf, tau = +inf for every domain, flat all-zero ones (s1 = 0) included.
+        // +inf, tau = +inf for every domain, flat all-zero ones (s1 = 0) included; in the
+        // short form g1 = +inf (sqrt(Ndd) > 0 always: +huge for a flat domain).
         t = ThrRec{INFINITY, INFINITY, 0.0f, 3.0e38f, -1, 0, 0, 0};
         sm.thr[rl] = t;
+        atomicAnd(&sm.full_bits, ~(1u << rl));
         return;
     }
     const Threshold th = make_threshold(C.sum, C.rms, C.idx >> 3, C.rms0, C.nrr, n, fp);
@@ -299,18 +313,29 @@ __device__ __forceinline__ void publish_threshold(Smem& sm, int rl, const FitPar
     t.neg = th.wpos ? 0.0f : -INFINITY;
     t.c = (float)C.t0 / (float)n - 128.0f;  // exact: t0 < 2^24, n a power of four
     t.tie = th.mode == 2 ? -1 : (th.mode == 1 ? (int32_t)th.tie_dom : INT32_MAX);
-    t.pad0 = t.pad1 = t.pad2 = 0;
+    t.full = th.mode != 0 && !th.wpos;
+    t.pad1 = t.pad2 = 0;
     sm.thr[rl] = t;
+    if (t.full)
+        atomicOr(&sm.full_bits, 1u << rl);
+    else
+        atomicAnd(&sm.full_bits, ~(1u << rl));
 }
 
 // Exact fits of every queued survivor, then the per-range winners of the batch (atomic
 // min on the f64 bit pattern of rms >= 0, then on the reference index) and the champion /
-// threshold update.  All epilogue threads call this together.
+// threshold update.  All epilogue threads call this together, after a barrier, so every
+// warp's count is final.  Entry qi is live when it lies inside its warp's filled part.
+__device__ __forceinline__ bool queued_entry(const Smem& sm, int qi) {
+    return (qi % kWarpCap) < sm.wcount[qi / kWarpCap];
+}
+
 template <int N>
-__device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t tag, int et,
+__device__ __noinline__ void drain_queue(Smem& sm, bool mark, uint32_t tag, int et,
                                          const DomainStats& ds, const FitParams& fp,
                                          unsigned long long& exact) {
-    for (int qi = et; qi < n; qi += kEpiThreads) {
+    for (int qi = et; qi < kQueueCap; qi += kEpiThreads) {
+        if (!queued_entry(sm, qi)) continue;
         QEntry& q = sm.queue[qi];
         const int rl = (int)(q.code & 255u) >> 3;
         const Champ& C = sm.ch[rl];
@@ -323,14 +348,16 @@ __device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t ta
         atomicMin(&sm.key_rms[rl], (unsigned long long)__double_as_longlong(f.rms));
     }
     epi_barrier();
-    for (int qi = et; qi < n; qi += kEpiThreads) {
+    for (int qi = et; qi < kQueueCap; qi += kEpiThreads) {
+        if (!queued_entry(sm, qi)) continue;
         const QEntry& q = sm.queue[qi];
         const int col = (int)(q.code & 255u), rl = col >> 3;
         if ((unsigned long long)__double_as_longlong(q.rms) == sm.key_rms[rl])
             atomicMin(&sm.key_idx[rl], q.dom * 8u + (uint32_t)(col & 7));
     }
     epi_barrier();
-    for (int qi = et; qi < n; qi += kEpiThreads) {
+    for (int qi = et; qi < kQueueCap; qi += kEpiThreads) {
+        if (!queued_entry(sm, qi)) continue;
         const QEntry& q = sm.queue[qi];
         const int col = (int)(q.code & 255u), rl = col >> 3;
         if ((unsigned long long)__double_as_longlong(q.rms) == sm.key_rms[rl] &&
@@ -339,7 +366,7 @@ __device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t ta
             sm.key_t1[rl] = q.t1 + 128 * ds.s1x4[q.dom];  // t1_x4, exact in int32 (S <= 64)
         }
         if (mark && (q.code >> 16) == tag) {
-            // The tile overflowed the queue: remember what was fitted so the next pass
+            // A region overflowed in this tile: remember what was fitted so the next pass
             // over the same accumulator only queues candidates not yet seen.
             const int qm = (int)(q.code >> 8) & 127;
             atomicOr(&sm.evaluated[(qm * kN + col) >> 5], 1u << (col & 31));
@@ -360,7 +387,8 @@ __device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t ta
         sm.key_rms[et] = ~0ull;
         sm.key_idx[et] = UINT32_MAX;
     }
-    if (et == 0) sm.qcount = 0;
+    epi_barrier();
+    if (et < kEpiWarps) sm.wcount[et] = 0;
     epi_barrier();
 }
 
@@ -405,8 +433,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         mbar_init(&sm.bres, 1);
         sm.abort_flag = 0;
-        sm.qcount = 0;
-        sm.overflow_seen = 0;
+        for (int w = 0; w < kEpiWarps; ++w) sm.wcount[w] = 0;
+        sm.full_bits = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = threadIdx.x; i < kM * kN / 32; i += kThreads) sm.evaluated[i] = 0u;
@@ -433,8 +461,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         sm.key_rms[threadIdx.x] = ~0ull;
         sm.key_idx[threadIdx.x] = UINT32_MAX;
-        publish_threshold(sm, threadIdx.x, fp, N);
     }
+    __syncthreads();  // full_bits and the champions are set before the records
+    if (threadIdx.x < kRangesPerTile) publish_threshold(sm, threadIdx.x, fp, N);
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&sm.tmem_base)),
@@ -545,6 +574,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // Warps 2..: TMEM lane quadrant = warp % 4; column part (kRangesPerWarp ranges from
         // part * kRangesPerWarp) = which of the quadrant's warps.
         const int et = threadIdx.x - 64;         // 0..kEpiThreads-1
+        const int ew = et >> 5;                  // epilogue warp 0..kEpiWarps-1
         const int e = warp & 3;
         const int part = (warp - 2) >> 2;
         const int m = e * 32 + lane;             // this thread's domain lane
@@ -604,17 +634,30 @@ __global__ void __launch_bounds__(kThreads, 1)
             // of them so the independent chains overlap.
             int32_t thr[kRangesPerWarp];
             auto all_thresholds = [&]() {
+                const float4* rec = reinterpret_cast<const float4*>(sm.thr);
+                const uint32_t fullw = (sm.full_bits >> (part * kRangesPerWarp)) &
+                                       ((1u << kRangesPerWarp) - 1u);
+                if (fullw == 0u) {
+                    // Short form for every range: s1 * c + (g1 + neg), each step rounded
+                    // toward -inf (the inner fma is exactly fmul_rd(sqrt_w, sqrt(Ndd))
+                    // plus 0 or -inf).
+#pragma unroll
+                    for (int r = 0; r < kRangesPerWarp; ++r) {
+                        const float4 ra = rec[2 * (part * kRangesPerWarp + r)];
+                        const float g = __fmaf_rd(ra.x, sdetf, ra.z);
+                        thr[r] = dom < 0 ? INT32_MAX : __float2int_rd(__fmaf_rd(s1f, ra.w, g));
+                    }
+                    return;
+                }
                 float4 ra[kRangesPerWarp];
                 int4 rb[kRangesPerWarp];
-                const float4* rec = reinterpret_cast<const float4*>(sm.thr);
 #pragma unroll
                 for (int r = 0; r < kRangesPerWarp; ++r) {
                     ra[r] = rec[2 * (part * kRangesPerWarp + r)];
                     rb[r] = reinterpret_cast<const int4*>(rec)[2 * (part * kRangesPerWarp + r) + 1];
                 }
                 // s1 * c + tau with one rounding toward -inf (fma): still never above the
-                // exact threshold.  (Branching on an all-Z-form tile measured slower than
-                // these selects.)
+                // exact threshold.
                 float tau[kRangesPerWarp];
 #pragma unroll
                 for (int r = 0; r < kRangesPerWarp; ++r) {
@@ -642,57 +685,74 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     const int col0 = part * kColsPerWarp + ch * 32;
                     if (rescan) mask &= ~sm.evaluated[(m * kN + col0) >> 5];
-                    int slot = atomicAdd(&sm.qcount, __popc(mask));
+                    int slot = atomicAdd(&sm.wcount[ew], __popc(mask));
                     while (mask) {
                         const int c = __ffs(mask) - 1;
                         mask &= mask - 1;
                         int32_t val = v[0];
 #pragma unroll
                         for (int q = 1; q < 32; ++q) val = c == q ? v[q] : val;
-                        if (slot < kQueueCap)
-                            sm.queue[slot] = QEntry{val, (uint32_t)dom,
-                                                    (uint32_t)(tag << 16 | m << 8 | (col0 + c)), 0u, 0.0, 0.0};
+                        if (slot < kWarpCap)
+                            sm.queue[ew * kWarpCap + slot] =
+                                QEntry{val, (uint32_t)dom, (uint32_t)(tag << 16 | m << 8 | (col0 + c)),
+                                       0u, 0.0, 0.0};
                         ++slot;
                     }
                 }
             };
             all_thresholds();  // overlaps the MMAs of this tile
-            const bool got = mbar_wait(&sm.tfull[b], bph, abort_flag, err, 16);
-            if (!epi_barrier_and(got)) break;
-            tmem_fence_after();
+            // Every warp waits for the accumulator on its own and scans it; one barrier per
+            // pass makes the warps agree to go on (a warp whose bounded wait gave up scans
+            // nothing and votes to stop) and tells them whether a drain is due.  The result
+            // of the wait is made warp-uniform, so the scan's aligned TMEM loads run with
+            // every lane.
+            bool got = __all_sync(0xffffffffu, mbar_wait(&sm.tfull[b], bph, abort_flag, err, 16));
+            bool first = true;
             for (;;) {
-                // ---- scan: this thread's accumulator columns in 32-column chunks, each
-                // chunk's load overlapped with the previous chunk's test
-                static_assert(kChunks % 2 == 0, "chunks are scanned in pairs");
-                int32_t va[32], vb[32];
-                __syncwarp();
-                tmem_ld32(tcol, va);
-                tmem_wait(va);
+                if (got) {
+                    if (first) tmem_fence_after();
+                    // ---- scan: this thread's accumulator columns in 32-column chunks, each
+                    // chunk's load overlapped with the previous chunk's test
+                    static_assert(kChunks % 2 == 0, "chunks are scanned in pairs");
+                    int32_t va[32], vb[32];
+                    __syncwarp();
+                    tmem_ld32(tcol, va);
+                    tmem_wait(va);
 #pragma unroll
-                for (int ch = 0; ch < kChunks; ch += 2) {
-                    tmem_ld32(tcol + 32u * (ch + 1), vb);
-                    test_chunk(va, ch);
-                    __syncwarp();
-                    tmem_wait(vb);
-                    if (ch + 2 < kChunks) tmem_ld32(tcol + 32u * (ch + 2), va);
-                    test_chunk(vb, ch + 1);
-                    __syncwarp();
-                    if (ch + 2 < kChunks) tmem_wait(va);
+                    for (int ch = 0; ch < kChunks; ch += 2) {
+                        tmem_ld32(tcol + 32u * (ch + 1), vb);
+                        test_chunk(va, ch);
+                        __syncwarp();
+                        tmem_wait(vb);
+                        if (ch + 2 < kChunks) tmem_ld32(tcol + 32u * (ch + 2), va);
+                        test_chunk(vb, ch + 1);
+                        __syncwarp();
+                        if (ch + 2 < kChunks) tmem_wait(va);
+                    }
                 }
-
-                epi_barrier();
-                const int queued = sm.qcount;
+                first = false;
+                // Common case: every warp got its accumulator and no region needs draining.
+                // This warp's count is final here (its lanes' atomics are done).
+                __syncwarp();
                 const bool last = mt + 1 == m_end;
-                if (queued > kQueueCap) {
-                    drain_queue<N>(sm, kQueueCap, true, tag, et, ds, fp, exact);
+                if (epi_barrier_and(got && !last && sm.wcount[ew] < kWarpFlush)) break;
+                // Rare: some warp gave up waiting (stop), or a drain is due.
+                if (!epi_barrier_and(got)) {
+                    got = false;
+                    break;
+                }
+                bool over = false;
+#pragma unroll
+                for (int w2 = 0; w2 < kEpiWarps; ++w2) over |= sm.wcount[w2] > kWarpCap;
+                drain_queue<N>(sm, over, tag, et, ds, fp, exact);
+                if (over) {
                     rescan = true;
                     all_thresholds();
                     continue;  // pass again over the same accumulator
                 }
-                if (queued >= kFlush || (last && queued > 0))
-                    drain_queue<N>(sm, queued, false, tag, et, ds, fp, exact);
                 break;
             }
+            if (!got) break;
             if (rescan) {
                 for (int w2 = et; w2 < kM * kN / 32; w2 += kEpiThreads) sm.evaluated[w2] = 0u;
                 epi_barrier();
