@@ -537,6 +537,64 @@ def run_uneven(mb, ctx, dev, large=True):
     return out
 
 
+LARGE_BLOCKS = 1024  # range blocks per level of the large-plane profile case
+
+
+def run_large_profile(args):
+    """The large-plane case of the uneven batch, sized for a profiler: one side x side
+    synthetic plane (seed 99), and per level (sizes 32..4, stride 2) the search of its first
+    LARGE_BLOCKS aligned range blocks against every domain of the plane through
+    mars_search_blocks_device (contraction, domain statistics, operand planes, B operand,
+    seeds, correlation, finish; one call per level, CUDA events around the calls).  Prints
+    one JSON object: per level the milliseconds per call, the correlation's algorithmic int8
+    TOP/s (evals x s^2 MACs x 2) and the algorithmic bytes of its decimation (u8 plane in,
+    contracted plane and the level's domain statistics out)."""
+    import torch
+    import mars_b200 as mb
+    side = args.profile_large
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx = mb.Context(0)
+    ctx.set_stream(stream.cuda_stream)
+    plane = torch.from_numpy(synthetic.gray(side, side, 99)).to(dev)
+    params = mb.make_params(min_size=4, max_size=32, shift=SHIFT)
+    out = {"workload": f"{side}x{side} synthetic gray plane (seed 99): the first {LARGE_BLOCKS} "
+                       "aligned range blocks of each level against every domain, stride 2",
+           "levels": {}}
+    for size in SIZES:
+        nb = min(LARGE_BLOCKS, (side // size) ** 2)
+        k = np.arange(nb)
+        rows = torch.from_numpy(((k // (side // size)) * size).astype(np.int32)).to(dev)
+        cols = torch.from_numpy(((k % (side // size)) * size).astype(np.int32)).to(dev)
+        res = torch.empty((nb, 80), dtype=torch.uint8, device=dev)
+
+        def call():
+            mb.check(mb.lib().mars_search_blocks_device(
+                ctx.handle, plane.data_ptr(), side, side, size, SHIFT, mb.C.byref(params),
+                rows.data_ptr(), cols.data_ptr(), nb, res.data_ptr()))
+        for _ in range(args.warmup):
+            call()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / args.steps
+        nd = ((side - 2 * size) // SHIFT + 1) ** 2
+        macs = nb * nd * 8 * size * size
+        out["levels"][str(size)] = {
+            "blocks": nb, "domains": nd, "ms_per_call": ms,
+            "int8_tops_algorithmic": 2 * macs / (ms * 1e-3) / 1e12,
+            "decimation_bytes": side * side + (side // 2) ** 2 * 4 + nd * 20}
+    print(json.dumps({"large_profile": out}), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_reference(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -799,9 +857,14 @@ def main():
                          "--refine-lambdas, and print its JSON object")
     ap.add_argument("--refine-seeds", default=",".join(map(str, REFINE_SEEDS)))
     ap.add_argument("--refine-lambdas", default=",".join(str(int(l)) for l in REFINE_LAMBDAS))
+    ap.add_argument("--profile-large", type=int, default=0, metavar="SIDE",
+                    help="run only the large-plane profile case (a SIDE x SIDE plane, the "
+                         "first blocks of every level) and print its JSON object")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_large:
+        return run_large_profile(args)
     if args.refine_only:
         import torch
         import mars_b200 as mb

@@ -131,7 +131,9 @@ uint64_t mars_ctx_launch_count(const mars_ctx* ctx);
 /* Correlation kernel selection for A/B checks: 0 = automatic (tensor cores wherever the
  * level allows, CUDA cores otherwise), 1 = CUDA cores only, 2 = automatic as well (the
  * tensor-core path never serves a level it does not support), 3 = automatic with the
- * tensor-core operand loads split into per-phase boxes.  Results are identical. */
+ * tensor-core operand loads split into per-phase boxes and the 2x2 box folded into K at
+ * every block size, 4 = automatic with the fold at every block size (no split-digit
+ * contracted operand at sizes 16..64).  Results are identical. */
 int mars_ctx_set_search_path(mars_ctx* ctx, int32_t path);
 
 /* The provider factory (encode.rs:1076): search every quadtree node an encode of this

@@ -331,10 +331,12 @@ class Context:
         check(lib().mars_ctx_set_stream(self._h, C.c_void_p(stream_ptr)))
 
     def set_search_path(self, path: str) -> None:
-        """'auto' (tensor cores wherever a level allows), 'simt' (CUDA cores only) or
-        'boxes' (tensor cores, operand stages loaded as per-phase boxes)."""
+        """'auto' (tensor cores wherever a level allows), 'simt' (CUDA cores only), 'boxes'
+        (tensor cores, operand stages loaded as per-phase boxes, the 2x2 box folded into K
+        at every size) or 'fold' (tensor cores, the fold at every size instead of the
+        split-digit contracted operand at sizes 16..64)."""
         check(lib().mars_ctx_set_search_path(self._h, {"auto": 0, "simt": 1, "tc": 2,
-                                                       "boxes": 3}[path]))
+                                                       "boxes": 3, "fold": 4}[path]))
 
     @property
     def launches(self) -> int:

@@ -14,7 +14,7 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmars_b200.so")
-SOURCES = ["api.cu", "search.cu", "search_tc.cu", "decode.cu", "fisher.cu", "color.cu", "refine.cu", "noalloc.cu", "codec.cpp", "format.cpp"]
+SOURCES = ["api.cu", "search.cu", "search_tc.cu", "decode.cu", "fisher.cu", "fisher_tc.cu", "color.cu", "refine.cu", "noalloc.cu", "codec.cpp", "format.cpp"]
 # Translation units whose f64 arithmetic must match the host's operation for operation: no
 # multiply-add contraction on the device (the host side is built with -ffp-contract=off).
 EXACT_F64_SOURCES = ["rdprice.cu"]

@@ -19,6 +19,7 @@
 #include "../../include/mars_b200.h"
 #include "codec.hpp"
 #include "context.hpp"
+#include "fisher_tc.cuh"
 #include "residual.hpp"
 #include "kernels.cuh"
 #include "tc.cuh"
@@ -239,32 +240,72 @@ int make_maps(mars_ctx* ctx, const uint8_t* d_phases, uint32_t w, uint32_t h, ui
     return MARS_OK;
 }
 
-// The tcgen05 path for one level: phase copies of the plane, the B operand, seed
-// champions, the correlation + exact-bound kernel, and the final champion per block.
+// The two 4-D views of the split-digit path over the digit phase copies (hi digit's P
+// phase planes, then lo's), the same box shape as the pixel view.  False when the driver
+// rejects them; the level then takes the fold path.
+bool make_digit_maps(mars_ctx* ctx, const uint8_t* d_digits, uint32_t w, uint32_t h,
+                     uint32_t shift, mars::tc::TcMaps* maps) {
+    if (!ctx->encode_tiled) return false;
+    std::memset(maps, 0, sizeof(*maps));
+    const uint32_t P = (uint32_t)mars::tc::digit_phase_count((int)shift);
+    const uint64_t dh = h / 2;
+    const uint64_t wp = (uint64_t)mars::tc::row_pitch((int)(w / 2));
+    const uint32_t per_phase = 16u / P;
+    const cuuint64_t dims4[4] = {wp, dh, per_phase, (cuuint64_t)P};
+    const cuuint64_t strides4[3] = {wp, 128, dh * wp};
+    const cuuint32_t box4[4] = {128, 8, per_phase, P};
+    const cuuint32_t estr4[4] = {1, 1, 1, 1};
+    for (int digit = 0; digit < 2; ++digit) {
+        void* addr = (void*)(d_digits + (size_t)digit * P * dh * wp);
+        const CUresult r = ctx->encode_tiled(digit ? &maps->all_lo : &maps->all,
+                                             CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, addr, dims4,
+                                             strides4, box4, estr4, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                             CU_TENSOR_MAP_SWIZZLE_NONE,
+                                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return false;
+    }
+    maps->use_all = 1;
+    return true;
+}
+
+// The tcgen05 path for one level: phase copies of the plane (or, for block sizes 16..64,
+// digit phase copies of the contracted plane), the B operand, seed champions, the
+// correlation + exact-bound kernel, and the final champion per block.
 int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t* d_D,
                  uint32_t w, uint32_t h, const mars::LevelGeom& g, const mars::FitParams& fp,
                  const uint32_t* d_rows, const uint32_t* d_cols, size_t n, mars::RangeStats rs,
                  mars::DomainStats ds, mars::CandidateOut* d_out) {
     const cudaStream_t st = ctx->stream;
-    const int P = mars::tc::phase_count(g.shift);
     uint8_t* d_phases = nullptr;
     uint8_t* d_b = nullptr;
     mars::tc::SeedOut* d_seed = nullptr;
-    MARS_CUDA(sc.get(&d_phases, mars::tc::phase_bytes((int)w, (int)h, g.shift)));
-    MARS_CUDA(sc.get(&d_b, mars::tc::b_bytes(g.size, (int)n)));
+    mars::tc::TcMaps maps;
+    bool digits = mars::tc::digits_supported(g.size, g.shift) && !ctx->tma_16_boxes &&
+                  !ctx->fold_only;
+    if (digits) {
+        MARS_CUDA(sc.get(&d_phases, mars::tc::digit_plane_bytes((int)w, (int)h, g.shift)));
+        digits = make_digit_maps(ctx, d_phases, w, h, (uint32_t)g.shift, &maps);
+    }
+    if (!digits) {
+        MARS_CUDA(sc.get(&d_phases, mars::tc::phase_bytes((int)w, (int)h, g.shift)));
+        if (int e = make_maps(ctx, d_phases, w, h, (uint32_t)g.shift, &maps)) return e;
+    }
+    MARS_CUDA(sc.get(&d_b, mars::tc::b_bytes(g.size, (int)n, digits)));
     MARS_CUDA(sc.get(&d_seed, n));
-    const int msplit = mars::tc::msplit_for(g, (int)n, ctx->num_sms);
+    const int msplit = mars::tc::msplit_for(g, (int)n, ctx->num_sms, digits);
     mars::Partial* partials = nullptr;
     MARS_CUDA(sc.get(&partials, (size_t)msplit * n));
-    mars::tc::TcMaps maps;
-    if (int e = make_maps(ctx, d_phases, w, h, (uint32_t)g.shift, &maps)) return e;
-    MARS_CUDA(mars::tc::launch_phase_planes(d_plane, (int)w, (int)h, g.shift, d_phases, st));
+    if (digits)
+        MARS_CUDA(mars::tc::launch_digit_planes(d_D, (int)w, (int)h, g.shift, d_phases, st));
+    else
+        MARS_CUDA(mars::tc::launch_phase_planes(d_plane, (int)w, (int)h, g.shift, d_phases, st));
     MARS_CUDA(mars::tc::launch_build_b(g.size, d_plane, (int)w, (int)h, d_rows, d_cols, (int)n,
-                                       d_b, st));
+                                       d_b, digits, st));
     MARS_CUDA(mars::tc::launch_seed(d_D, g, d_plane, (int)w, d_rows, d_cols, (int)n, rs, ds, fp,
                                     d_seed, st));
     MARS_CUDA(mars::tc::launch_corr(maps, d_b, g, (int)n, rs, ds, fp, d_seed, partials, msplit,
-                                    ctx->d_err, ctx->d_counter, st));
+                                    digits, ctx->d_err, ctx->d_counter, st));
     MARS_CUDA(mars::tc::launch_finish(partials, msplit, (int)n, g, rs, ds, fp, d_out, st));
     ctx->launches += 5;
     return MARS_OK;
@@ -428,6 +469,91 @@ int run_jobs(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uin
     return MARS_OK;
 }
 
+// Whether the classified search of a level runs as the tensor-core bucketed batch
+// (fisher_tc.cu): block sizes 4, 8, 16 at an even stride, unless the CUDA-core path is
+// pinned (mars_ctx_set_search_path 1 or MARS_SEARCH_PATH=simt).
+bool use_fisher_tc(const mars_ctx* ctx, uint32_t size, uint32_t shift) {
+    if (!use_tc(ctx, 4, 2)) return false;  // the CUDA-core path is pinned
+    return mars::ftc::supported((int)size, (int)shift);
+}
+
+// One level of the classified search on tensor cores: statistics, each range's bucket,
+// the ranges grouped by bucket, then the batch (fisher_tc.cu).
+int run_fisher_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t* d_D,
+                  uint32_t w, uint32_t h, const mars::LevelGeom& g, const mars::FitParams& fp,
+                  const uint32_t* d_rows, const uint32_t* d_cols, int n,
+                  const mars::FisherIndex& ix, mars::CandidateOut* d_out, uint64_t* d_evals) {
+    const cudaStream_t st = ctx->stream;
+    const size_t npos = (size_t)g.nrow_d * g.ncol_d;
+    mars::RangeStats rs;
+    mars::DomainStats ds;
+    MARS_CUDA(sc.get(&rs.t0, n));
+    MARS_CUDA(sc.get(&rs.t2, n));
+    MARS_CUDA(sc.get(&rs.nrr, n));
+    MARS_CUDA(sc.get(&rs.sum0, n));
+    MARS_CUDA(sc.get(&rs.rms0, n));
+    MARS_CUDA(sc.get(&ds.s1x4, npos));
+    MARS_CUDA(sc.get(&ds.s2x16, npos));
+    MARS_CUDA(sc.get(&ds.detf, npos));
+    MARS_CUDA(sc.get(&ds.sdetf, npos));
+    MARS_CUDA(mars::launch_range_stats(d_plane, (int)w, (int)h, d_rows, d_cols, n, g.size, fp, rs,
+                                       st));
+    MARS_CUDA(mars::launch_domain_stats(d_D, g, ds, st));
+    mars::ftc::FisherTcArgs a{};
+    uint8_t *rbucket = nullptr, *riso = nullptr;
+    uint32_t *rlist = nullptr, *plan = nullptr, *ref_scratch = nullptr;
+    MARS_CUDA(sc.get(&rbucket, n));
+    MARS_CUDA(sc.get(&riso, n));
+    MARS_CUDA(sc.get(&rlist, n));
+    MARS_CUDA(sc.get(&a.rrank, n));
+    MARS_CUDA(sc.get(&plan, mars::ftc::kPlanWords));
+    MARS_CUDA(sc.get(&ref_scratch, 72));
+    a.plan.rcounts = plan;
+    a.plan.roffsets = plan + 72;
+    a.plan.p_base = plan + 144;
+    a.plan.chunks = plan + 216;
+    a.plan.ntiles = plan + 288;
+    a.plan.a_tile_base = plan + 360;
+    a.plan.b_tile_base = plan + 433;
+    a.plan.item_base = plan + 506;
+    MARS_CUDA(mars::ftc::launch_range_classes(d_plane, (int)w, (int)h, g.size, d_rows, d_cols, n,
+                                              ix.ref, rbucket, riso, st));
+    MARS_CUDA(mars::launch_fisher_group(rbucket, n, a.plan.rcounts, a.plan.roffsets, ref_scratch,
+                                        rlist, st));
+    a.a_rows_max = mars::ftc::a_rows_max(npos);
+    a.b_rows_max = mars::ftc::b_rows_max((size_t)n);
+    a.items_max = mars::ftc::items_max((size_t)n);
+    MARS_CUDA(sc.get(&a.aglob, mars::ftc::a_bytes(g.size, npos)));
+    MARS_CUDA(sc.get(&a.bglob, mars::ftc::b_bytes(g.size, (size_t)n)));
+    MARS_CUDA(sc.get(&a.seeds, n));
+    MARS_CUDA(sc.get(&a.partials, mars::ftc::partials_max((size_t)n)));
+    a.plane = d_plane;
+    a.w = (int)w;
+    a.h = (int)h;
+    a.D = d_D;
+    a.dw = g.dw;
+    a.size = g.size;
+    a.shift = g.shift;
+    a.ncol_d = g.ncol_d;
+    a.rows = d_rows;
+    a.cols = d_cols;
+    a.nranges = n;
+    a.ix = ix;
+    a.rbucket = rbucket;
+    a.riso = riso;
+    a.rlist = rlist;
+    a.rs = rs;
+    a.ds = ds;
+    a.fp = fp;
+    a.out = d_out;
+    a.evals = d_evals;
+    a.err = ctx->d_err;
+    a.counter = ctx->d_counter;
+    MARS_CUDA(mars::ftc::launch_search(a, st));
+    ctx->launches += 13;
+    return MARS_OK;
+}
+
 // Fisher's classified search for every job: per (size, shift) the domain index
 // (Fisher::index) and the searches of the job's nodes (Fisher::candidates +
 // search_block_fitted); per-node eval counts come back from the device.
@@ -474,12 +600,20 @@ int run_jobs_fisher(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t
     for (const Job& j : jobs) {
         const mars::LevelGeom g = level_geom(w, h, j.size, j.shift);
         const int nrow = std::max(g.nrow_d, 0), ncol = std::max(g.ncol_d, 0);
+        const int n = (int)j.rows.size();
         MARS_CUDA(mars::launch_fisher_index(d_D, dw, (int)j.size, (int)j.shift, nrow, ncol, ix, st));
-        MARS_CUDA(mars::launch_fisher_search(d_plane, (int)w, (int)h, d_D, dw, (int)j.size,
-                                             (int)j.shift, std::max(ncol, 1), d_rc + off,
-                                             d_rc + total + off, (int)j.rows.size(), ix, fp,
-                                             d_out + off, d_evals + off, part, part_e, st));
-        ctx->launches += (nrow * ncol > 0 ? 5 : 3) + (mars::fisher_warps_per_range((int)j.size) > 1);
+        ctx->launches += nrow * ncol > 0 ? 4 : 2;
+        if (use_fisher_tc(ctx, j.size, j.shift) && nrow * ncol > 0 && n > 0) {
+            if (int e = run_fisher_tc(ctx, sc, d_plane, d_D, w, h, g, fp, d_rc + off,
+                                      d_rc + total + off, n, ix, d_out + off, d_evals + off))
+                return e;
+        } else {
+            MARS_CUDA(mars::launch_fisher_search(d_plane, (int)w, (int)h, d_D, dw, (int)j.size,
+                                                 (int)j.shift, std::max(ncol, 1), d_rc + off,
+                                                 d_rc + total + off, n, ix, fp, d_out + off,
+                                                 d_evals + off, part, part_e, st));
+            ctx->launches += 1 + (mars::fisher_warps_per_range((int)j.size) > 1);
+        }
         off += j.rows.size();
     }
     return MARS_OK;
@@ -648,10 +782,11 @@ int mars_ctx_set_stream(mars_ctx* ctx, void* stream) {
 uint64_t mars_ctx_launch_count(const mars_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
 
 int mars_ctx_set_search_path(mars_ctx* ctx, int32_t path) {
-    if (!ctx || path < 0 || path > 3) return fail(MARS_EINVAL, "path must be 0, 1, 2 or 3");
+    if (!ctx || path < 0 || path > 4) return fail(MARS_EINVAL, "path must be 0 .. 4");
     std::lock_guard<std::mutex> lock(ctx->mu);
-    ctx->search_path = path == 3 ? 0 : path;
+    ctx->search_path = path >= 3 ? 0 : path;
     ctx->tma_16_boxes = path == 3;
+    ctx->fold_only = path == 4;
     return MARS_OK;
 }
 

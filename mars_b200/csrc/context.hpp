@@ -26,6 +26,7 @@ struct mars_ctx {
     int* d_err = nullptr;                     // kernel-side error bits (bounded waits)
     int search_path = 0;                      // 0 auto, 1 CUDA cores only, 2 tensor cores
     bool tma_16_boxes = false;                // load A stages as 16 2-D boxes (A/B checks)
+    bool fold_only = false;                   // no split-digit operand at sizes 16..64 (A/B)
     PFN_cuTensorMapEncodeTiled_v12000 encode_tiled = nullptr;
     // Search plans mars_encode keeps for plane geometries it has met before (api.cu).
     std::mutex plan_cache_mu;

@@ -42,191 +42,48 @@
 
 #include "kernels.cuh"
 #include "tc.cuh"
+#include "tc_ptx.cuh"
 
 namespace mars {
 namespace tc {
 namespace {
 
-constexpr int kEpiWarps = 8;                    // 2 per TMEM lane quadrant
-constexpr int kThreads = 64 + 32 * kEpiWarps;   // 10 warps: load, MMA, 8 epilogue
-constexpr int kEpiThreads = 32 * kEpiWarps;
-constexpr int kColsPerWarp = 4 * 256 / kEpiWarps;  // accumulator columns per epilogue warp
-constexpr int kRangesPerWarp = kColsPerWarp / 8;
-constexpr int kChunks = kColsPerWarp / 32;         // 32-column TMEM loads per pass
-constexpr int kM = 128;
-constexpr int kN = 256;
-constexpr int kRangesPerTile = kN / 8;         // 32
+constexpr int kN = 256;                        // accumulator columns of a TMEM buffer
+constexpr int kRangesPerTile = kN / 8;         // 32: the most ranges a tile holds
 constexpr int kStageA = 16 * 1024;             // 16 row groups x 8 K-groups x 128 B
-constexpr int kStageB = 32 * 1024;             // 32 row groups x 8 K-groups x 128 B
 constexpr int kQueueCap = 2048;                // survivors the queue can hold
-// Each epilogue warp owns kWarpCap consecutive queue entries and its own count, so no warp
-// reads a count another warp may still be adding to; the queue is drained when any warp's
-// region holds kWarpFlush entries.
-constexpr int kWarpCap = kQueueCap / kEpiWarps;  // 256
-constexpr int kWarpFlush = 48;
-constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 1.965 GHz
+constexpr int kFlush = 256;                    // drain the queue once it holds this many
 
-// Pipeline depth: as many A stages as fit beside the resident B tile (S <= 8), otherwise
-// three stages of A + B.
+// Pipeline depth of the fold path: as many A stages as fit beside the resident B tile
+// (S <= 8), otherwise three stages of A + B.
 __host__ __device__ constexpr int stages_for(int S) { return S == 4 ? 6 : (S == 8 ? 4 : 3); }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// One bounded poll of an mbarrier phase.  The suspend-time hint lets the hardware park
-// the waiting thread until the phase completes (or ~20 us pass) instead of spinning, so
-// waiting warps leave the issue slots to the epilogue warps sharing their scheduler.
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait: false when the deadline passed or another warp already gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                          int* err_global, int code) {
-    const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity)) {
-        if (*abort_flag) return false;
-        if (clock64() - t0 > kWaitCycles) {
-            *abort_flag = 1;
-            atomicOr(err_global, code);
-            return false;
-        }
-    }
-    return true;
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
-                                            uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-        "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y,
-                                            uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
-        "l"((uint64_t)map), "r"(x), "r"(y), "r"(0), "r"(0), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-            "r"(smem_u32(dst)),
-        "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// SWIZZLE_NONE K-major shared-memory matrix descriptor: core matrices of 8 rows x 16 B,
-// LBO = 128 B between K-adjacent core matrices, SBO = 1024 B between 8-row groups.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
-    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)(128u >> 4) << 16;
-    d |= (uint64_t)(1024u >> 4) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
-    return d;                // base offset 0, layout type 0 (no swizzle)
-}
-
-// Instruction descriptor, kind::i8: D = s32, A = u8, B = s8, both K-major, M = 128, N = 256.
-constexpr uint32_t kIdesc = (2u << 4) | (0u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) |
-                            ((uint32_t)(kM >> 4) << 24);
-
-__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                       uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_fence_before() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_fence_after() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-// TMEM -> registers, 32 columns of this warp's 32 lanes.  The load completes
-// asynchronously: tmem_wait() names the destination registers as read-write operands so
-// no consumer can be scheduled ahead of it.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int32_t (&v)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-          "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
-          "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
-          "=r"(v[31])
-        : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_wait(int32_t (&v)[32]) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]),
-                   "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]),
-                   "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15]), "+r"(v[16]), "+r"(v[17]),
-                   "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]), "+r"(v[22]), "+r"(v[23]),
-                   "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]), "+r"(v[29]),
-                   "+r"(v[30]), "+r"(v[31])
-                 :
-                 : "memory");
-}
-
-__device__ __forceinline__ void epi_barrier() {
-    asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
-}
-
-// Named barrier over the epilogue warps that also ANDs a predicate across them, so the
-// warps always agree on whether to go on.
-__device__ __forceinline__ bool epi_barrier_and(bool pred) {
-    uint32_t out;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.and.pred q, 1, %2, p;\n\t"
-        "selp.u32 %0, 1, 0, q;\n\t}"
-        : "=r"(out)
-        : "r"((uint32_t)pred), "n"(kEpiThreads)
-        : "memory");
-    return out != 0;
-}
+// Tile shape of a level.
+//   Fold path (DIG = false): A is u8 pixels of the 2S x 2S domain block (K = 4 S^2, the
+//     2x2 box sum folded into K); N = 256 columns = 32 ranges x 8 isometries.
+//   Digit path (DIG = true, S >= 16): A is the contracted plane D = 4d of the reference
+//     (Contracted::build, encode.rs:478-502; 0..1020) split into two u8 digits,
+//     D = 128 hi + lo (hi 0..7, lo 0..127), K = S^2 per digit, half the fold's MACs; N = 128
+//     columns per digit = 16 ranges x 8 isometries, the two digits' accumulators side by
+//     side in a 256-column TMEM buffer (hi at +0, lo at +128), t1' = 128 hi + lo exactly.
+//   Either way a TMEM buffer is 256 columns and two of them double-buffer the 512.
+template <int S, bool DIG>
+struct Cfg {
+    static constexpr int kNt = DIG ? 128 : 256;         // accumulator columns per digit
+    static constexpr int kRt = kNt / 8;                 // ranges per tile
+    static constexpr int kCols = 4 * kNt / kEpiWarps;   // columns per epilogue warp and digit
+    static constexpr int kRw = kCols / 8;               // ranges per epilogue warp
+    static constexpr int kCh = kCols / 32;              // 32-column chunks per warp and digit
+    static constexpr int kStageBt = kNt * 128;          // B bytes per 128-byte K stage
+    static constexpr int kDigits = DIG ? 2 : 1;
+    static constexpr int ROWS = DIG ? S : 2 * S;        // rows of a domain's K window
+    static constexpr int J = DIG ? S / 16 : (S >= 8 ? S / 8 : 1);  // 16-byte groups a row
+    static constexpr int KST = J * ROWS / 8;            // 128-byte K stages per tile
+    static constexpr bool kBRes = KST * kStageBt <= 64 * 1024;  // B stays resident
+    static constexpr int kStages = DIG ? 3 : stages_for(S);
+    static constexpr uint32_t kTx = kDigits * kStageA + (kBRes ? 0 : kStageBt);
+    static_assert(!DIG || S >= 16, "the digit path needs whole 16-byte digit rows");
+};
 
 // Champion of one range block (reference order: smaller rms, then smaller index).
 struct Champ {
@@ -242,21 +99,13 @@ struct Champ {
 //   g1 = sqrt_w * sqrt(Ndd);  tau_z = min(w2a + a_half*Ndd, max(g1, a_min*Ndd));
 //   tau = (dom > tie) ? tau_z : g1 + neg;   prune  <=>  t1' < s1_x4 * c + 4 tau / n.
 // tie = -1 puts every domain in the Z-form, INT32_MAX none; neg = 0 or -inf (W <= 0).
-// Since tau_z >= g1 whenever W > 0 (W/(2a) + a*Ndd/2 >= sqrt(W*Ndd) by the AM-GM
-// inequality, and max(g1, .) >= g1), the short form  t1' < s1_x4 * c + (g1 + neg) * 4/n
-// is a valid threshold for every range with W > 0, whatever its tie mode; it is also the
-// exact threshold outside the Z-form.  It differs from the full one only when
-// a_min^2 * Ndd > W, which the best candidates of a range almost never meet, so it prunes
-// the same candidates at a third of the instructions.  `full` marks the ranges that need
-// the full form: a Z-form range with W <= 0, for which the short form prunes nothing.
 struct __align__(16) ThrRec {
     float sqrt_w, w2a, neg, c;  // sqrt_w, w2a, neg pre-scaled by 4 / n (exact: n = 4^k)
-    int32_t tie, full, pad1, pad2;
+    int32_t tie, pad0, pad1, pad2;
 };
 
 // A survivor waiting for its exact fit.  Survivors of several tiles are batched: the
-// queue is drained when a warp's region holds kWarpFlush entries, when a tile overflows a
-// region, and at the end.
+// queue is drained when it holds kFlush entries, when a tile overflows it, and at the end.
 struct __align__(8) QEntry {
     int32_t t1;     // t1' = t1_x4 - 128 * s1_x4
     uint32_t dom;   // domain position index (row-major)
@@ -273,8 +122,8 @@ struct Smem {
     uint64_t bres;
     uint32_t tmem_base;
     int abort_flag;
-    int wcount[kEpiWarps];  // entries each epilogue warp queued (may exceed kWarpCap)
-    uint32_t full_bits;     // bit r: range r of the tile needs the full threshold form
+    int qcount;
+    int overflow_seen;
     unsigned long long key_rms[kRangesPerTile];  // per-pass winner: f64 bits (rms >= 0)
     uint32_t key_idx[kRangesPerTile];
     double key_sum[kRangesPerTile];
@@ -297,11 +146,9 @@ __device__ __forceinline__ void publish_threshold(Smem& sm, int rl, const FitPar
     ThrRec t;
     if (!C.valid) {
         // An invalid range never survives: in the Z-form (tie = -1) with sqrt_w = w2a =
-        // +inf, tau = +inf for every domain, flat all-zero ones (s1 = 0) included; in the
-        // short form g1 = +inf (sqrt(Ndd) > 0 always: +huge for a flat domain).
+        // +inf, tau = +inf for every domain, flat all-zero ones (s1 = 0) included.
         t = ThrRec{INFINITY, INFINITY, 0.0f, 3.0e38f, -1, 0, 0, 0};
         sm.thr[rl] = t;
-        atomicAnd(&sm.full_bits, ~(1u << rl));
         return;
     }
     const Threshold th = make_threshold(C.sum, C.rms, C.idx >> 3, C.rms0, C.nrr, n, fp);
@@ -313,29 +160,18 @@ __device__ __forceinline__ void publish_threshold(Smem& sm, int rl, const FitPar
     t.neg = th.wpos ? 0.0f : -INFINITY;
     t.c = (float)C.t0 / (float)n - 128.0f;  // exact: t0 < 2^24, n a power of four
     t.tie = th.mode == 2 ? -1 : (th.mode == 1 ? (int32_t)th.tie_dom : INT32_MAX);
-    t.full = th.mode != 0 && !th.wpos;
-    t.pad1 = t.pad2 = 0;
+    t.pad0 = t.pad1 = t.pad2 = 0;
     sm.thr[rl] = t;
-    if (t.full)
-        atomicOr(&sm.full_bits, 1u << rl);
-    else
-        atomicAnd(&sm.full_bits, ~(1u << rl));
 }
 
 // Exact fits of every queued survivor, then the per-range winners of the batch (atomic
 // min on the f64 bit pattern of rms >= 0, then on the reference index) and the champion /
-// threshold update.  All epilogue threads call this together, after a barrier, so every
-// warp's count is final.  Entry qi is live when it lies inside its warp's filled part.
-__device__ __forceinline__ bool queued_entry(const Smem& sm, int qi) {
-    return (qi % kWarpCap) < sm.wcount[qi / kWarpCap];
-}
-
-template <int N>
-__device__ __noinline__ void drain_queue(Smem& sm, bool mark, uint32_t tag, int et,
+// threshold update.  All epilogue threads call this together.
+template <int N, int NT>
+__device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t tag, int et,
                                          const DomainStats& ds, const FitParams& fp,
                                          unsigned long long& exact) {
-    for (int qi = et; qi < kQueueCap; qi += kEpiThreads) {
-        if (!queued_entry(sm, qi)) continue;
+    for (int qi = et; qi < n; qi += kEpiThreads) {
         QEntry& q = sm.queue[qi];
         const int rl = (int)(q.code & 255u) >> 3;
         const Champ& C = sm.ch[rl];
@@ -348,16 +184,14 @@ __device__ __noinline__ void drain_queue(Smem& sm, bool mark, uint32_t tag, int 
         atomicMin(&sm.key_rms[rl], (unsigned long long)__double_as_longlong(f.rms));
     }
     epi_barrier();
-    for (int qi = et; qi < kQueueCap; qi += kEpiThreads) {
-        if (!queued_entry(sm, qi)) continue;
+    for (int qi = et; qi < n; qi += kEpiThreads) {
         const QEntry& q = sm.queue[qi];
         const int col = (int)(q.code & 255u), rl = col >> 3;
         if ((unsigned long long)__double_as_longlong(q.rms) == sm.key_rms[rl])
             atomicMin(&sm.key_idx[rl], q.dom * 8u + (uint32_t)(col & 7));
     }
     epi_barrier();
-    for (int qi = et; qi < kQueueCap; qi += kEpiThreads) {
-        if (!queued_entry(sm, qi)) continue;
+    for (int qi = et; qi < n; qi += kEpiThreads) {
         const QEntry& q = sm.queue[qi];
         const int col = (int)(q.code & 255u), rl = col >> 3;
         if ((unsigned long long)__double_as_longlong(q.rms) == sm.key_rms[rl] &&
@@ -366,10 +200,10 @@ __device__ __noinline__ void drain_queue(Smem& sm, bool mark, uint32_t tag, int 
             sm.key_t1[rl] = q.t1 + 128 * ds.s1x4[q.dom];  // t1_x4, exact in int32 (S <= 64)
         }
         if (mark && (q.code >> 16) == tag) {
-            // A region overflowed in this tile: remember what was fitted so the next pass
+            // The tile overflowed the queue: remember what was fitted so the next pass
             // over the same accumulator only queues candidates not yet seen.
             const int qm = (int)(q.code >> 8) & 127;
-            atomicOr(&sm.evaluated[(qm * kN + col) >> 5], 1u << (col & 31));
+            atomicOr(&sm.evaluated[(qm * NT + col) >> 5], 1u << (col & 31));
         }
     }
     epi_barrier();
@@ -387,30 +221,35 @@ __device__ __noinline__ void drain_queue(Smem& sm, bool mark, uint32_t tag, int 
         sm.key_rms[et] = ~0ull;
         sm.key_idx[et] = UINT32_MAX;
     }
-    epi_barrier();
-    if (et < kEpiWarps) sm.wcount[et] = 0;
+    if (et == 0) sm.qcount = 0;
     epi_barrier();
 }
 
-template <int S>
+template <int S, bool DIG>
 __global__ void __launch_bounds__(kThreads, 1)
     corr_tc_kernel(const __grid_constant__ TcMaps maps, const uint8_t* __restrict__ bglob,
                    LevelGeom g, int nranges, RangeStats rs, DomainStats ds, FitParams fp,
                    const SeedOut* __restrict__ seeds, int m_tiles, int m_per_cta,
                    Partial* __restrict__ partials, int* __restrict__ err,
                    unsigned long long* __restrict__ exact_counter) {
+    using C_ = Cfg<S, DIG>;
     constexpr int N = S * S;
-    constexpr int J = S >= 8 ? S / 8 : 1;  // 16-byte column groups per pixel row
-    constexpr int ROWS = 2 * S;            // pixel rows of a domain block
-    constexpr int KST = J * ROWS / 8;      // 128-byte K stages per tile
-    constexpr bool kBRes = KST <= 2;       // B tile stays resident in shared memory
-    constexpr int kStages = stages_for(S);
-    constexpr uint32_t kTxStage = kBRes ? kStageA : kStageA + kStageB;
+    constexpr int NT = C_::kNt;
+    constexpr int RT = C_::kRt;
+    constexpr int ROWS = C_::ROWS;
+    constexpr int KST = C_::KST;
+    constexpr bool kBRes = C_::kBRes;
+    constexpr int kStages = C_::kStages;
+    constexpr int kStageB = C_::kStageBt;
+    constexpr int kStageAll = C_::kDigits * kStageA;  // A bytes of one stage (both digits)
+    constexpr int kColsPerWarp = C_::kCols;
+    constexpr int kRangesPerWarp = C_::kRw;
+    constexpr int kChunks = C_::kCh;
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    unsigned char* stA = base;                                  // kStages x 16 KB
-    unsigned char* stB = stA + kStages * kStageA;               // kStages x 32 KB or resident
+    unsigned char* stA = base;                                  // kStages x (1 or 2) x 16 KB
+    unsigned char* stB = stA + kStages * kStageAll;             // kStages B stages or resident
     unsigned char* after_b = stB + (kBRes ? KST * kStageB : kStages * kStageB);
     Smem& sm = *reinterpret_cast<Smem*>(after_b);
 
@@ -418,7 +257,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int ntile = blockIdx.x;
     const int m_begin = blockIdx.y * m_per_cta;
     const int m_end = min(m_tiles, m_begin + m_per_cta);
-    const int P = 16 / g.shift;
+    // Phase copies: domains lie shift pixels (fold) or shift / 2 contracted samples
+    // (digits) apart; P same-phase copies put each group of 16 / P domains' starts on
+    // 16-byte boundaries.
+    const int P = DIG ? 32 / g.shift : 16 / g.shift;
     const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
     const uint8_t* btile = bglob + (size_t)ntile * KST * kStageB;
 
@@ -433,14 +275,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         mbar_init(&sm.bres, 1);
         sm.abort_flag = 0;
-        for (int w = 0; w < kEpiWarps; ++w) sm.wcount[w] = 0;
-        sm.full_bits = 0u;
+        sm.qcount = 0;
+        sm.overflow_seen = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = threadIdx.x; i < kM * kN / 32; i += kThreads) sm.evaluated[i] = 0u;
-    if (threadIdx.x < kRangesPerTile) {
+    for (int i = threadIdx.x; i < kM * NT / 32; i += kThreads) sm.evaluated[i] = 0u;
+    if (threadIdx.x < RT) {
         Champ& C = sm.ch[threadIdx.x];
-        const int r = ntile * kRangesPerTile + threadIdx.x;
+        const int r = ntile * RT + threadIdx.x;
         C.valid = r < nranges && seeds[r].idx != UINT32_MAX;
         if (C.valid) {
             C.t0 = rs.t0[r];
@@ -461,9 +303,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         sm.key_rms[threadIdx.x] = ~0ull;
         sm.key_idx[threadIdx.x] = UINT32_MAX;
+        publish_threshold(sm, threadIdx.x, fp, N);
     }
-    __syncthreads();  // full_bits and the champions are set before the records
-    if (threadIdx.x < kRangesPerTile) publish_threshold(sm, threadIdx.x, fp, N);
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&sm.tmem_base)),
@@ -490,14 +331,20 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int mt = m_begin; mt < m_end && !*abort_flag; ++mt) {
                 const int a = mt / tiles_per_row;
                 const int q0 = (mt % tiles_per_row) * (kM / P);
-                const int dom_row = a * g.shift;
+                // First row of the domain row's window: a pixel row (fold) or a
+                // contracted-plane row (digits).
+                const int dom_row = DIG ? a * (g.shift / 2) : a * g.shift;
                 for (int t = 0; t < KST; ++t) {
                     if (issued >= kStages && !mbar_wait(&sm.empty[s], ph ^ 1, abort_flag, err, 1)) break;
-                    mbar_expect_tx(&sm.full[s], kTxStage);
+                    mbar_expect_tx(&sm.full[s], C_::kTx);
                     const int kg0 = t * 8;
                     const int j = kg0 / ROWS, y0 = kg0 % ROWS;
-                    unsigned char* dstA = stA + s * kStageA;
-                    if (maps.use_all) {
+                    unsigned char* dstA = stA + s * kStageAll;
+                    if (DIG) {
+                        tma_load_4d(dstA, &maps.all, 16 * (q0 + j), dom_row + y0, &sm.full[s]);
+                        tma_load_4d(dstA + kStageA, &maps.all_lo, 16 * (q0 + j), dom_row + y0,
+                                    &sm.full[s]);
+                    } else if (maps.use_all) {
                         tma_load_4d(dstA, &maps.all, 16 * (q0 + j), dom_row + y0, &sm.full[s]);
                     } else {
                         const int per_phase = 16 / P;
@@ -552,12 +399,16 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     tmem_fence_after();
-                    const uint32_t a_addr = smem_u32(stA + s * kStageA);
+                    const uint32_t a_addr = smem_u32(stA + s * kStageAll);
                     const uint32_t b_addr = smem_u32(kBRes ? stB + t * kStageB : stB + s * kStageB);
 #pragma unroll
-                    for (int kk = 0; kk < 4; ++kk)
-                        mma_i8(dcol, smem_desc(a_addr + kk * 256), smem_desc(b_addr + kk * 256),
-                               (t > 0 || kk > 0) ? 1u : 0u);
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const uint64_t bd = smem_desc(b_addr + kk * 256);
+                        const uint32_t acc = (t > 0 || kk > 0) ? 1u : 0u;
+                        mma_i8<NT>(dcol, smem_desc(a_addr + kk * 256), bd, acc);
+                        if (DIG)  // low digit into the buffer's second half
+                            mma_i8<NT>(dcol + NT, smem_desc(a_addr + kStageA + kk * 256), bd, acc);
+                    }
                     mma_commit(&sm.empty[s]);
                     if (++s == kStages) {
                         s = 0;
@@ -574,7 +425,6 @@ __global__ void __launch_bounds__(kThreads, 1)
         // Warps 2..: TMEM lane quadrant = warp % 4; column part (kRangesPerWarp ranges from
         // part * kRangesPerWarp) = which of the quadrant's warps.
         const int et = threadIdx.x - 64;         // 0..kEpiThreads-1
-        const int ew = et >> 5;                  // epilogue warp 0..kEpiWarps-1
         const int e = warp & 3;
         const int part = (warp - 2) >> 2;
         const int m = e * 32 + lane;             // this thread's domain lane
@@ -634,30 +484,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             // of them so the independent chains overlap.
             int32_t thr[kRangesPerWarp];
             auto all_thresholds = [&]() {
-                const float4* rec = reinterpret_cast<const float4*>(sm.thr);
-                const uint32_t fullw = (sm.full_bits >> (part * kRangesPerWarp)) &
-                                       ((1u << kRangesPerWarp) - 1u);
-                if (fullw == 0u) {
-                    // Short form for every range: s1 * c + (g1 + neg), each step rounded
-                    // toward -inf (the inner fma is exactly fmul_rd(sqrt_w, sqrt(Ndd))
-                    // plus 0 or -inf).
-#pragma unroll
-                    for (int r = 0; r < kRangesPerWarp; ++r) {
-                        const float4 ra = rec[2 * (part * kRangesPerWarp + r)];
-                        const float g = __fmaf_rd(ra.x, sdetf, ra.z);
-                        thr[r] = dom < 0 ? INT32_MAX : __float2int_rd(__fmaf_rd(s1f, ra.w, g));
-                    }
-                    return;
-                }
                 float4 ra[kRangesPerWarp];
                 int4 rb[kRangesPerWarp];
+                const float4* rec = reinterpret_cast<const float4*>(sm.thr);
 #pragma unroll
                 for (int r = 0; r < kRangesPerWarp; ++r) {
                     ra[r] = rec[2 * (part * kRangesPerWarp + r)];
                     rb[r] = reinterpret_cast<const int4*>(rec)[2 * (part * kRangesPerWarp + r) + 1];
                 }
                 // s1 * c + tau with one rounding toward -inf (fma): still never above the
-                // exact threshold.
+                // exact threshold.  (Branching on an all-Z-form tile measured slower than
+                // these selects.)
                 float tau[kRangesPerWarp];
 #pragma unroll
                 for (int r = 0; r < kRangesPerWarp; ++r) {
@@ -684,38 +521,46 @@ __global__ void __launch_bounds__(kThreads, 1)
                         mask |= (v[c] >= tc ? 1u : 0u) << c;
                     }
                     const int col0 = part * kColsPerWarp + ch * 32;
-                    if (rescan) mask &= ~sm.evaluated[(m * kN + col0) >> 5];
-                    int slot = atomicAdd(&sm.wcount[ew], __popc(mask));
+                    if (rescan) mask &= ~sm.evaluated[(m * NT + col0) >> 5];
+                    int slot = atomicAdd(&sm.qcount, __popc(mask));
                     while (mask) {
                         const int c = __ffs(mask) - 1;
                         mask &= mask - 1;
                         int32_t val = v[0];
 #pragma unroll
                         for (int q = 1; q < 32; ++q) val = c == q ? v[q] : val;
-                        if (slot < kWarpCap)
-                            sm.queue[ew * kWarpCap + slot] =
-                                QEntry{val, (uint32_t)dom, (uint32_t)(tag << 16 | m << 8 | (col0 + c)),
-                                       0u, 0.0, 0.0};
+                        if (slot < kQueueCap)
+                            sm.queue[slot] = QEntry{val, (uint32_t)dom,
+                                                    (uint32_t)(tag << 16 | m << 8 | (col0 + c)), 0u, 0.0, 0.0};
                         ++slot;
                     }
                 }
             };
             all_thresholds();  // overlaps the MMAs of this tile
-            // Every warp waits for the accumulator on its own and scans it; one barrier per
-            // pass makes the warps agree to go on (a warp whose bounded wait gave up scans
-            // nothing and votes to stop) and tells them whether a drain is due.  The result
-            // of the wait is made warp-uniform, so the scan's aligned TMEM loads run with
-            // every lane.
-            bool got = __all_sync(0xffffffffu, mbar_wait(&sm.tfull[b], bph, abort_flag, err, 16));
-            bool first = true;
+            const bool got = mbar_wait(&sm.tfull[b], bph, abort_flag, err, 16);
+            if (!epi_barrier_and(got)) break;
+            tmem_fence_after();
             for (;;) {
-                if (got) {
-                    if (first) tmem_fence_after();
-                    // ---- scan: this thread's accumulator columns in 32-column chunks, each
-                    // chunk's load overlapped with the previous chunk's test
-                    static_assert(kChunks % 2 == 0, "chunks are scanned in pairs");
-                    int32_t va[32], vb[32];
-                    __syncwarp();
+                // ---- scan: this thread's accumulator columns in 32-column chunks, each
+                // chunk's load overlapped with the previous chunk's test
+                static_assert(kChunks % 2 == 0, "chunks are scanned in pairs");
+                int32_t va[32], vb[32];
+                __syncwarp();
+                if (DIG) {
+                    // t1' = 128 hi + lo per column, both digits' accumulators loaded together
+                    // (exact: |t1'| < 2^31).
+#pragma unroll
+                    for (int ch = 0; ch < kChunks; ++ch) {
+                        tmem_ld32(tcol + 32u * ch, va);
+                        tmem_ld32(tcol + (uint32_t)NT + 32u * ch, vb);
+                        tmem_wait(va);
+                        tmem_wait(vb);
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) va[c] = va[c] * 128 + vb[c];
+                        test_chunk(va, ch);
+                        __syncwarp();
+                    }
+                } else {
                     tmem_ld32(tcol, va);
                     tmem_wait(va);
 #pragma unroll
@@ -730,31 +575,22 @@ __global__ void __launch_bounds__(kThreads, 1)
                         if (ch + 2 < kChunks) tmem_wait(va);
                     }
                 }
-                first = false;
-                // Common case: every warp got its accumulator and no region needs draining.
-                // This warp's count is final here (its lanes' atomics are done).
-                __syncwarp();
+
+                epi_barrier();
+                const int queued = sm.qcount;
                 const bool last = mt + 1 == m_end;
-                if (epi_barrier_and(got && !last && sm.wcount[ew] < kWarpFlush)) break;
-                // Rare: some warp gave up waiting (stop), or a drain is due.
-                if (!epi_barrier_and(got)) {
-                    got = false;
-                    break;
-                }
-                bool over = false;
-#pragma unroll
-                for (int w2 = 0; w2 < kEpiWarps; ++w2) over |= sm.wcount[w2] > kWarpCap;
-                drain_queue<N>(sm, over, tag, et, ds, fp, exact);
-                if (over) {
+                if (queued > kQueueCap) {
+                    drain_queue<N, NT>(sm, kQueueCap, true, tag, et, ds, fp, exact);
                     rescan = true;
                     all_thresholds();
                     continue;  // pass again over the same accumulator
                 }
+                if (queued >= kFlush || (last && queued > 0))
+                    drain_queue<N, NT>(sm, queued, false, tag, et, ds, fp, exact);
                 break;
             }
-            if (!got) break;
             if (rescan) {
-                for (int w2 = et; w2 < kM * kN / 32; w2 += kEpiThreads) sm.evaluated[w2] = 0u;
+                for (int w2 = et; w2 < kM * NT / 32; w2 += kEpiThreads) sm.evaluated[w2] = 0u;
                 epi_barrier();
             }
             // The accumulator has been read completely: hand it back to the MMA warp.
@@ -770,9 +606,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         tmem_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
     }
-    if (threadIdx.x < kRangesPerTile) {
+    if (threadIdx.x < RT) {
         const Champ& C = sm.ch[threadIdx.x];
-        const int r = ntile * kRangesPerTile + threadIdx.x;
+        const int r = ntile * RT + threadIdx.x;
         if (r < nranges) {
             Partial p;
             p.rms = C.rms;
@@ -787,24 +623,28 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-// B operand of one level: rows n = range * 8 + isometry; for each 256-row N tile and each
-// 128-byte K stage, 32 row groups x 8 K-groups x (8 rows x 16 B).
-template <int S>
+// B operand of one level: rows n = range * 8 + isometry; for each N tile (NT rows) and each
+// 128-byte K stage, NT / 8 row groups x 8 K-groups x (8 rows x 16 B).  Fold path: the range
+// sample r[map_k(u, v)] - 128 upsampled 2x2 onto the domain's 2S x 2S pixel positions;
+// digit path: the S x S samples themselves (the positions of the contracted window).
+template <int S, bool DIG>
 __global__ void build_b_kernel(const uint8_t* __restrict__ plane, int w, int h,
                                const uint32_t* rows, const uint32_t* cols, int nranges,
                                int ntiles, uint8_t* __restrict__ out) {
-    constexpr int J = S >= 8 ? S / 8 : 1;
-    constexpr int ROWS = 2 * S;
-    constexpr int KG = J * ROWS;
+    using C_ = Cfg<S, DIG>;
+    constexpr int NT = C_::kNt;
+    constexpr int ROWS = C_::ROWS;
+    constexpr int KG = C_::J * ROWS;
     constexpr int KST = KG / 8;
+    constexpr int XMAX = DIG ? S : 2 * S;  // K positions per row that carry a sample
     // one thread per (n, kg): writes one 16-byte K-group of one B row
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long total = (long long)ntiles * kN * KG;
+    const long long total = (long long)ntiles * NT * KG;
     if (tid >= total) return;
     const int kg = (int)(tid % KG);
     const long long nglob = tid / KG;
-    const int nt = (int)(nglob / kN), n = (int)(nglob % kN);
-    const int r = nt * kRangesPerTile + n / 8, k = n % 8;
+    const int nt = (int)(nglob / NT), n = (int)(nglob % NT);
+    const int r = nt * C_::kRt + n / 8, k = n % 8;
     const int j = kg / ROWS, y = kg % ROWS;
     const int t = kg / 8, kgl = kg % 8;
     const bool inside = r < nranges && rows[r] + (uint32_t)S <= (uint32_t)h &&
@@ -814,8 +654,8 @@ __global__ void build_b_kernel(const uint8_t* __restrict__ plane, int w, int h,
     for (int e = 0; e < 16; ++e) {
         const int x = 16 * j + e;
         int8_t val = 0;
-        if (inside && x < 2 * S) {
-            const int u = y >> 1, vv = x >> 1;
+        if (inside && x < XMAX) {
+            const int u = DIG ? y : y >> 1, vv = DIG ? x : x >> 1;
             int i, jj;
             switch (k) {
                 case 0: i = u; jj = vv; break;
@@ -831,7 +671,7 @@ __global__ void build_b_kernel(const uint8_t* __restrict__ plane, int w, int h,
         }
         bytes[e] = (uint8_t)val;
     }
-    const size_t off = (((size_t)nt * KST + t) * 32 + (n >> 3)) * 1024 + (size_t)kgl * 128 +
+    const size_t off = (((size_t)nt * KST + t) * (NT / 8) + (n >> 3)) * 1024 + (size_t)kgl * 128 +
                        (size_t)(n & 7) * 16;
     uint4 pk;
     pk.x = bytes[0] | bytes[1] << 8 | bytes[2] << 16 | (uint32_t)bytes[3] << 24;
@@ -839,6 +679,21 @@ __global__ void build_b_kernel(const uint8_t* __restrict__ plane, int w, int h,
     pk.z = bytes[8] | bytes[9] << 8 | bytes[10] << 16 | (uint32_t)bytes[11] << 24;
     pk.w = bytes[12] | bytes[13] << 8 | bytes[14] << 16 | (uint32_t)bytes[15] << 24;
     *reinterpret_cast<uint4*>(out + off) = pk;
+}
+
+// Digit phase copies of the contracted plane D (dw x dh, i32, 0..1020): plane
+// z = digit * P + p (digit 0 = hi = D >> 7, 1 = lo = D & 127) is that digit shifted left by
+// step_c * p samples, zero past the right edge; row pitch wp (a multiple of 16).
+__global__ void digit_planes_kernel(const int32_t* __restrict__ D, int dw, int dh, int wp,
+                                    int step_c, int P, uint8_t* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= wp || y >= dh || z >= 2 * P) return;
+    const int digit = z / P, p = z % P;
+    const int sx = x + step_c * p;
+    const int v = sx < dw ? D[(size_t)y * dw + sx] : 0;
+    out[((size_t)z * dh + y) * wp + x] = (uint8_t)(digit == 0 ? v >> 7 : v & 127);
 }
 
 // Phase copies of the plane: copy p (of P = 16 / shift) is the plane shifted left by
@@ -974,18 +829,21 @@ __global__ void finish_kernel(const Partial* __restrict__ partials, int nsplit, 
     out[r] = c;
 }
 
-template <int S>
-size_t smem_bytes() {
-    constexpr int J = S >= 8 ? S / 8 : 1;
-    constexpr int KST = J * 2 * S / 8;
-    constexpr bool kBRes = KST <= 2;
-    constexpr int kStages = stages_for(S);
-    static_assert(kStages <= kMaxStages, "pipeline depth");
-    return 1024 + (size_t)kStages * kStageA + (kBRes ? (size_t)KST * kStageB : (size_t)kStages * kStageB) +
+template <int S, bool DIG>
+constexpr size_t smem_bytes() {
+    using C_ = Cfg<S, DIG>;
+    static_assert(C_::kStages <= kMaxStages, "pipeline depth");
+    return 1024 + (size_t)C_::kStages * C_::kDigits * kStageA +
+           (C_::kBRes ? (size_t)C_::KST * C_::kStageBt : (size_t)C_::kStages * C_::kStageBt) +
            sizeof(Smem);
 }
+static_assert(smem_bytes<4, false>() <= 232448 && smem_bytes<8, false>() <= 232448 &&
+                  smem_bytes<16, false>() <= 232448 && smem_bytes<32, false>() <= 232448 &&
+                  smem_bytes<16, true>() <= 232448 && smem_bytes<32, true>() <= 232448 &&
+                  smem_bytes<64, true>() <= 232448,
+              "shared memory per CTA (227 KB)");
 
-template <int S>
+template <int S, bool DIG>
 cudaError_t launch_t(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
                      RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
                      Partial* partials, int msplit, int* err, unsigned long long* counter,
@@ -993,9 +851,9 @@ cudaError_t launch_t(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& 
     const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
     const int m_tiles = g.nrow_d * tiles_per_row;
     const int m_per_cta = (m_tiles + msplit - 1) / msplit;
-    const int ntiles = (nranges + kRangesPerTile - 1) / kRangesPerTile;
-    const size_t smem = smem_bytes<S>();
-    auto kern = corr_tc_kernel<S>;
+    const int ntiles = (nranges + Cfg<S, DIG>::kRt - 1) / Cfg<S, DIG>::kRt;
+    const size_t smem = smem_bytes<S, DIG>();
+    auto kern = corr_tc_kernel<S, DIG>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(ntiles, msplit);
@@ -1004,15 +862,15 @@ cudaError_t launch_t(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& 
     return cudaGetLastError();
 }
 
-template <int S>
+template <int S, bool DIG>
 cudaError_t build_b_t(const uint8_t* plane, int w, int h, const uint32_t* rows,
                       const uint32_t* cols, int nranges, uint8_t* out, cudaStream_t st) {
-    constexpr int J = S >= 8 ? S / 8 : 1;
-    constexpr int KG = J * 2 * S;
-    const int ntiles = (nranges + kRangesPerTile - 1) / kRangesPerTile;
-    const long long total = (long long)ntiles * kN * KG;
-    build_b_kernel<S><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(plane, w, h, rows, cols,
-                                                                       nranges, ntiles, out);
+    using C_ = Cfg<S, DIG>;
+    constexpr int KG = C_::J * C_::ROWS;
+    const int ntiles = (nranges + C_::kRt - 1) / C_::kRt;
+    const long long total = (long long)ntiles * C_::kNt * KG;
+    build_b_kernel<S, DIG><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+        plane, w, h, rows, cols, nranges, ntiles, out);
     return cudaGetLastError();
 }
 
@@ -1023,11 +881,19 @@ bool supported(int size, int shift) {
            (shift == 2 || shift == 4 || shift == 8 || shift == 16);
 }
 
-size_t b_bytes(int size, int nranges) {
-    const int J = size >= 8 ? size / 8 : 1;
-    const int KG = J * 2 * size;
-    const size_t ntiles = (size_t)(nranges + kRangesPerTile - 1) / kRangesPerTile;
-    return ntiles * (size_t)kN * (size_t)KG * 16;
+bool digits_supported(int size, int shift) {
+    return (size == 16 || size == 32 || size == 64) &&
+           (shift == 2 || shift == 4 || shift == 8 || shift == 16);
+}
+
+int ranges_per_tile(bool digits) { return digits ? 16 : 32; }
+
+size_t b_bytes(int size, int nranges, bool digits) {
+    // K-groups of 16 bytes per B row: fold J * 2S with J = max(1, S / 8); digits S * S / 16.
+    const int KG = digits ? size * size / 16 : (size >= 8 ? size / 8 : 1) * 2 * size;
+    const int rt = ranges_per_tile(digits);
+    const size_t ntiles = (size_t)(nranges + rt - 1) / rt;
+    return ntiles * (size_t)(rt * 8) * (size_t)KG * 16;
 }
 
 int phase_count(int shift) { return 16 / shift; }
@@ -1036,6 +902,19 @@ int row_pitch(int w) { return ((w + 15) / 16) * 16 + 16; }
 // domain uses); the allocation carries that much slack after the last phase copy.
 size_t phase_bytes(int w, int h, int shift) {
     return (size_t)phase_count(shift) * h * row_pitch(w) + 2048;
+}
+int digit_phase_count(int shift) { return 32 / shift; }
+size_t digit_plane_bytes(int w, int h, int shift) {
+    return 2 * (size_t)digit_phase_count(shift) * (h / 2) * row_pitch(w / 2) + 2048;
+}
+
+cudaError_t launch_digit_planes(const int32_t* D, int w, int h, int shift, uint8_t* out,
+                                cudaStream_t st) {
+    const int P = digit_phase_count(shift), dw = w / 2, dh = h / 2, wp = row_pitch(dw);
+    if (dh == 0) return cudaSuccess;
+    dim3 grid((wp + 255) / 256, dh, 2 * P);
+    digit_planes_kernel<<<grid, 256, 0, st>>>(D, dw, dh, wp, shift / 2, P, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_phase_planes(const uint8_t* plane, int w, int h, int shift, uint8_t* out,
@@ -1047,13 +926,22 @@ cudaError_t launch_phase_planes(const uint8_t* plane, int w, int h, int shift, u
 }
 
 cudaError_t launch_build_b(int size, const uint8_t* plane, int w, int h, const uint32_t* rows,
-                           const uint32_t* cols, int nranges, uint8_t* out, cudaStream_t st) {
+                           const uint32_t* cols, int nranges, uint8_t* out, bool digits,
+                           cudaStream_t st) {
+    if (digits) {
+        switch (size) {
+            case 16: return build_b_t<16, true>(plane, w, h, rows, cols, nranges, out, st);
+            case 32: return build_b_t<32, true>(plane, w, h, rows, cols, nranges, out, st);
+            case 64: return build_b_t<64, true>(plane, w, h, rows, cols, nranges, out, st);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (size) {
-        case 4: return build_b_t<4>(plane, w, h, rows, cols, nranges, out, st);
-        case 8: return build_b_t<8>(plane, w, h, rows, cols, nranges, out, st);
-        case 16: return build_b_t<16>(plane, w, h, rows, cols, nranges, out, st);
-        case 32: return build_b_t<32>(plane, w, h, rows, cols, nranges, out, st);
-        case 64: return build_b_t<64>(plane, w, h, rows, cols, nranges, out, st);
+        case 4: return build_b_t<4, false>(plane, w, h, rows, cols, nranges, out, st);
+        case 8: return build_b_t<8, false>(plane, w, h, rows, cols, nranges, out, st);
+        case 16: return build_b_t<16, false>(plane, w, h, rows, cols, nranges, out, st);
+        case 32: return build_b_t<32, false>(plane, w, h, rows, cols, nranges, out, st);
+        case 64: return build_b_t<64, false>(plane, w, h, rows, cols, nranges, out, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1078,11 +966,12 @@ cudaError_t launch_seed(const int32_t* D, const LevelGeom& g, const uint8_t* pla
 // CTA sweeping ceil(m_tiles / msplit) domain tiles after a fixed set-up (B load, range
 // records, pipeline fill) worth about kSetupTiles tiles.  Pick the split with the fewest
 // tile-times over all waves.
-int msplit_for(const LevelGeom& g, int nranges, int num_sms) {
+int msplit_for(const LevelGeom& g, int nranges, int num_sms, bool digits) {
     constexpr long long kSetupTiles = 4;
     const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
     const int m_tiles = g.nrow_d * tiles_per_row;
-    const int ntiles = (nranges + kRangesPerTile - 1) / kRangesPerTile;
+    const int rt = ranges_per_tile(digits);
+    const int ntiles = (nranges + rt - 1) / rt;
     int best = 1;
     long long best_cost = -1;
     for (int ms = 1; ms <= m_tiles; ++ms) {
@@ -1099,16 +988,27 @@ int msplit_for(const LevelGeom& g, int nranges, int num_sms) {
 
 cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
                         RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
-                        Partial* partials, int msplit, int* err, unsigned long long* counter,
-                        cudaStream_t st) {
+                        Partial* partials, int msplit, bool digits, int* err,
+                        unsigned long long* counter, cudaStream_t st) {
+#define MARS_CORR(S_, D_) \
+    launch_t<S_, D_>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st)
+    if (digits) {
+        switch (g.size) {
+            case 16: return MARS_CORR(16, true);
+            case 32: return MARS_CORR(32, true);
+            case 64: return MARS_CORR(64, true);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (g.size) {
-        case 4: return launch_t<4>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st);
-        case 8: return launch_t<8>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st);
-        case 16: return launch_t<16>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st);
-        case 32: return launch_t<32>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st);
-        case 64: return launch_t<64>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st);
+        case 4: return MARS_CORR(4, false);
+        case 8: return MARS_CORR(8, false);
+        case 16: return MARS_CORR(16, false);
+        case 32: return MARS_CORR(32, false);
+        case 64: return MARS_CORR(64, false);
         default: return cudaErrorInvalidValue;
     }
+#undef MARS_CORR
 }
 
 cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,

@@ -17,8 +17,11 @@ constexpr int kMaxPhases = 8;  // 16 / shift for shift = 2
 // same-phase 128-byte column groups x phases -- whose 128 x 8 x (16/P) x P box is a whole
 // 16 KB A stage in core-matrix order; when the driver rejects that view (`use_all` = 0)
 // the stage is loaded as 16 boxes of 128 B x 8 rows through the per-phase 2-D maps.
+// The digit path (S >= 16) reads the hi digit's phase copies through `all` and the lo
+// digit's through `all_lo`, both 4-D views of the same shape (it has no 2-D fallback).
 struct alignas(64) TcMaps {
     CUtensorMap all;
+    CUtensorMap all_lo;
     CUtensorMap m[kMaxPhases];
     int32_t use_all;
 };
@@ -30,23 +33,32 @@ struct SeedOut {
 };
 
 bool supported(int size, int shift);
+// Levels the split-digit contracted operand serves (block sizes 16..64).
+bool digits_supported(int size, int shift);
 int phase_count(int shift);
 int row_pitch(int w);
 size_t phase_bytes(int w, int h, int shift);
-size_t b_bytes(int size, int nranges);
-int msplit_for(const LevelGeom& g, int nranges, int num_sms);
+// Digit phase copies of the contracted plane: 2 digits x (32 / shift) phases x (h / 2) rows
+// of row_pitch(w / 2) bytes (plus slack).
+int digit_phase_count(int shift);
+size_t digit_plane_bytes(int w, int h, int shift);
+size_t b_bytes(int size, int nranges, bool digits);
+int msplit_for(const LevelGeom& g, int nranges, int num_sms, bool digits);
 
 cudaError_t launch_phase_planes(const uint8_t* plane, int w, int h, int shift, uint8_t* out,
                                 cudaStream_t st);
+cudaError_t launch_digit_planes(const int32_t* D, int w, int h, int shift, uint8_t* out,
+                                cudaStream_t st);
 cudaError_t launch_build_b(int size, const uint8_t* plane, int w, int h, const uint32_t* rows,
-                           const uint32_t* cols, int nranges, uint8_t* out, cudaStream_t st);
+                           const uint32_t* cols, int nranges, uint8_t* out, bool digits,
+                           cudaStream_t st);
 cudaError_t launch_seed(const int32_t* D, const LevelGeom& g, const uint8_t* plane, int w,
                         const uint32_t* rows, const uint32_t* cols, int nranges, RangeStats rs,
                         DomainStats ds, const FitParams& fp, SeedOut* out, cudaStream_t st);
 cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
                         RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
-                        Partial* partials, int msplit, int* err, unsigned long long* counter,
-                        cudaStream_t st);
+                        Partial* partials, int msplit, bool digits, int* err,
+                        unsigned long long* counter, cudaStream_t st);
 cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,
                           RangeStats rs, DomainStats ds, const FitParams& fp, CandidateOut* out,
                           cudaStream_t st);

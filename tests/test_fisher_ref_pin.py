@@ -126,3 +126,38 @@ def test_range_reads_the_bucket_the_reference_c_code_assigns(name, img, size, sh
     assert out["valid"].all()
     assert np.array_equal(bucket[pos], eff), f"{name}: a winner lies outside its C bucket"
     assert np.array_equal(out["isometry"], MAPPING[risos, diso[pos]])
+
+
+def _iso_permute(block, k):
+    """permute_range (crates/mars-codec/src/encode.rs:833-842) with isometry::map
+    (crates/mars-codec/src/isometry.rs:7-19): out[u, v] = block[map_k(u, v)]."""
+    s = block.shape[0]
+    u, v = np.meshgrid(np.arange(s), np.arange(s), indexing="ij")
+    i, j = [(u, v), (s - 1 - v, u), (v, s - 1 - u), (s - 1 - u, s - 1 - v), (u, s - 1 - v),
+            (s - 1 - u, v), (v, u), (s - 1 - v, s - 1 - u)][k]
+    return block[i, j]
+
+
+def _flips(block, iso):
+    """flips (crates/mars-search/src/classify.rs; Mars 1 coding_func.c:1200-1247):
+    out[i, j] = block[source of (i, j) under iso]."""
+    s = block.shape[0]
+    i, j = np.meshgrid(np.arange(s), np.arange(s), indexing="ij")
+    si, sj = [(i, j), (j, s - i - 1), (s - j - 1, i), (s - i - 1, s - j - 1), (i, s - j - 1),
+              (s - i - 1, j), (j, i), (s - j - 1, s - i - 1)][iso]
+    return block[si, sj]
+
+
+@pytest.mark.parametrize("size", [2, 4, 8, 16])
+def test_canonical_orientation_turns_every_bucket_into_one_product(size):
+    """For every (range isometry, domain isometry) pair the classified search's cross term
+    sum R[MAPPING[ri][di](u, v)] * D[u, v] equals sum flips(R, ri) * flips(D, di): with both
+    operands brought to their canonical orientation, the pairs of one bucket are one plain
+    matrix product (no per-pair isometry)."""
+    rng = np.random.default_rng(size)
+    for ri in range(8):
+        for di in range(8):
+            r = rng.integers(0, 256, (size, size))
+            d = rng.integers(0, 1021, (size, size))
+            want = int((_iso_permute(r, MAPPING[ri, di]) * d).sum())
+            assert int((_flips(r, ri) * _flips(d, di)).sum()) == want, (ri, di)

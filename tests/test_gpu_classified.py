@@ -58,3 +58,27 @@ def test_reduced_colour_encode_through_fisher(ctx):
     assert (stats.y_bytes, stats.cb_bytes, stats.cr_bytes) == tuple(len(s) for s in streams)
     out = color.decode_color(ctx, data, 10)
     assert out.shape == rgb.shape
+
+
+@pytest.mark.parametrize("side,seed", [(256, 1), (384, 6)])
+def test_device_buckets_equal_the_reference_c_classifier(ctx, side, seed):
+    """The device's classified search reads, for every range block, the bucket the
+    reference's own 1998 C classifier assigns (oracle/_ref/libmars1_fisher.so): its eval
+    count is that bucket's length and its winner lies in that bucket with isometry
+    MAPPING[range iso][domain iso].  Square planes: the C contraction is the intended one."""
+    from tests.test_fisher_ref_pin import MAPPING, expected_reads
+    img = synthetic.gray(side, side, seed)
+    prov = ctx.search_provider(img, mb.make_params(min_size=4, max_size=16, shift=2),
+                               method="fisher")
+    try:
+        for size in (4, 8, 16):
+            rows, cols, eff, length, risos, bucket, diso = expected_reads(img, size, 2)
+            cands, evals = prov.search_many(rows, cols, size, 2)
+            assert np.array_equal(evals, length), size
+            ncol = (side - 2 * size) // 2 + 1
+            pos = (cands["dom_row"] // 2) * ncol + cands["dom_col"] // 2
+            assert cands["valid"].all()
+            assert np.array_equal(bucket[pos], eff), size
+            assert np.array_equal(cands["isometry"], MAPPING[risos, diso[pos]]), size
+    finally:
+        prov.close()

@@ -124,3 +124,32 @@ def test_fisher_encode_adaptive_density_and_borders(ctx):
                    (1, 1, 1, 0), adaptive=True)
     _encode_parity(ctx, imgs["mixed_250x250"], dict(min_size=4, max_size=32, shift=4, t_rms=8.0),
                    (1, 0, 1, 0))
+
+
+@pytest.mark.parametrize("name,side,seed", [("synthetic", 256, 11), ("synthetic", 384, 12),
+                                            ("flat128", 0, 0), ("checker8", 0, 0)])
+def test_tensor_core_batch_equals_cuda_core_kernel(ctx, name, side, seed):
+    """The class-bucketed tcgen05 batch (sizes 4, 8, 16) and the CUDA-core Fisher kernel give
+    the same node table bit for bit: same winners, rms bits, moments and eval counts; flat128
+    sends every range to one bucket (the first-non-empty fallback) and checker8 to few."""
+    if name == "synthetic":
+        img = synthetic.gray(side, side, seed)
+    else:
+        img = fixture_images()[0][name]
+    h, w = img.shape
+    params = mb.make_params(min_size=4, max_size=16, shift=2)
+    simt = mb.Context(0)
+    simt.set_search_path("simt")
+    try:
+        a = ctx.search_provider(img, params, method="fisher")
+        b = simt.search_provider(img, params, method="fisher")
+        for size in (4, 8, 16):
+            rows, cols = _grid(w, h, size)
+            x, xe = a.search_many(rows, cols, size, 2)
+            y, ye = b.search_many(rows, cols, size, 2)
+            assert np.array_equal(xe, ye), size
+            assert x.tobytes() == y.tobytes(), size
+        a.close()
+        b.close()
+    finally:
+        simt.close()

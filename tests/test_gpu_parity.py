@@ -234,20 +234,25 @@ def test_tensor_core_path_equals_cuda_core_path(ctx, shift):
     simt.set_search_path("simt")
     boxes = mb.Context(0)
     boxes.set_search_path("boxes")  # tensor cores, A stages loaded as per-phase 2-D boxes
+    fold = mb.Context(0)
+    fold.set_search_path("fold")  # tensor cores, pixels with the 2x2 box folded into K
     try:
         for size in (4, 8, 16, 32, 64):
             if 2 * size > 224:
                 continue
             p = mb.make_params(shift=shift)
-            a, aev = ctx.search_grid(img, size, shift, p)
+            a, aev = ctx.search_grid(img, size, shift, p)  # split digits at sizes 16..64
             b, bev = simt.search_grid(img, size, shift, p)
             c, _ = boxes.search_grid(img, size, shift, p)
+            d, _ = fold.search_grid(img, size, shift, p)
             assert np.array_equal(aev, bev)
             assert a.tobytes() == b.tobytes(), (size, shift)
             assert c.tobytes() == a.tobytes(), (size, shift)
+            assert d.tobytes() == a.tobytes(), (size, shift)
     finally:
         simt.close()
         boxes.close()
+        fold.close()
     o, _ = orc.search_grid(img, 8, shift, orc.make_params(shift=shift))
     a, _ = ctx.search_grid(img, 8, shift, mb.make_params(shift=shift))
     assert a.tobytes() == o.tobytes()
@@ -324,14 +329,14 @@ def test_out_of_plane_blocks_stay_invalid_next_to_black_domains(ctx, path):
     img = synthetic.gray(128, 128, 4)
     img[:48, :48] = 0
     d_img = torch.from_numpy(img).cuda()
-    # Origins 1 and 2 leave the plane for both block sizes (126 + 4 > 128).
+    # Origins 1 and 2 leave the plane for every block size (126 + 4 > 128).
     rows = torch.tensor([64, 126, 125, 0], dtype=torch.int32, device="cuda")
     cols = torch.tensor([64, 0, 126, 0], dtype=torch.int32, device="cuda")
     out = torch.zeros((4, 80), dtype=torch.uint8, device="cuda")
     p = mb.make_params(shift=2)
     ctx.set_search_path(path)
     try:
-        for size in (4, 8):
+        for size in (4, 8, 16):
             torch.cuda.synchronize()
             mb.check(mb.lib().mars_search_blocks_device(ctx.handle, d_img.data_ptr(), 128, 128,
                                                         size, 2, mb.C.byref(p), rows.data_ptr(),
