@@ -857,6 +857,9 @@ def main():
                          "--refine-lambdas, and print its JSON object")
     ap.add_argument("--refine-seeds", default=",".join(map(str, REFINE_SEEDS)))
     ap.add_argument("--refine-lambdas", default=",".join(str(int(l)) for l in REFINE_LAMBDAS))
+    ap.add_argument("--classified-only", action="store_true",
+                    help="run only the classified colour leg (for profiling) and print its "
+                         "JSON object")
     ap.add_argument("--profile-large", type=int, default=0, metavar="SIDE",
                     help="run only the large-plane profile case (a SIDE x SIDE plane, the "
                          "first blocks of every level) and print its JSON object")
@@ -865,6 +868,14 @@ def main():
         return run_reference(args)
     if args.profile_large:
         return run_large_profile(args)
+    if args.classified_only:
+        import torch
+        import mars_b200 as mb
+        torch.cuda.set_device(0)
+        ctx = mb.Context(0)
+        print(json.dumps({"classified": run_classified(mb, ctx)}), flush=True)
+        ctx.close()
+        return 0
     if args.refine_only:
         import torch
         import mars_b200 as mb

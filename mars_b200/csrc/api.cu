@@ -769,6 +769,11 @@ void mars_ctx_destroy(mars_ctx* ctx) {
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->d_err) cudaFree(ctx->d_err);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    for (int b = 0; b < mars_ctx::kBranches; ++b) {
+        if (ctx->branch[b]) cudaStreamDestroy(ctx->branch[b]);
+        if (ctx->join_ev[b]) cudaEventDestroy(ctx->join_ev[b]);
+    }
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     delete ctx;
 }
 
@@ -1250,6 +1255,53 @@ void plan_release(mars_search_plan* p) {
 
 // The plan's device work on the context's stream: with_copies adds the pinned input
 // upload and the table / counter downloads around it.
+// run_jobs with the levels as parallel branches: the contraction on the context's stream,
+// then each level on one of the context's branch streams (its own scratch, allocated and
+// freed on that branch), joined back before the results are read.  Inside a capture the
+// branches become parallel paths of the graph, so one level's set-up kernels and tail
+// overlap another level's correlation.  The caller holds ctx->mu.
+int run_jobs_branched(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uint32_t h,
+                      const mars::FitParams& fp, const std::vector<Job>& jobs,
+                      mars::CandidateOut* d_out, const uint32_t* d_rc) {
+    const cudaStream_t main = ctx->stream;
+    if (!ctx->fork_ev) {
+        MARS_CUDA(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+        for (int b = 0; b < mars_ctx::kBranches; ++b) {
+            MARS_CUDA(cudaStreamCreateWithFlags(&ctx->branch[b], cudaStreamNonBlocking));
+            MARS_CUDA(cudaEventCreateWithFlags(&ctx->join_ev[b], cudaEventDisableTiming));
+        }
+    }
+    int32_t* d_D = nullptr;
+    MARS_CUDA(sc.get(&d_D, std::max<size_t>(1, (size_t)(w / 2) * (h / 2))));
+    MARS_CUDA(mars::launch_contract(d_plane, (int)w, (int)h, d_D, main));
+    ctx->launches += 1;
+    size_t total = 0;
+    for (const Job& j : jobs) total += j.rows.size();
+    MARS_CUDA(cudaEventRecord(ctx->fork_ev, main));
+    const int nb = (int)std::min<size_t>(jobs.size(), mars_ctx::kBranches);
+    for (int b = 0; b < nb; ++b) MARS_CUDA(cudaStreamWaitEvent(ctx->branch[b], ctx->fork_ev, 0));
+    size_t off = 0;
+    int err = MARS_OK;
+    for (size_t i = 0; i < jobs.size() && !err; ++i) {
+        const Job& j = jobs[i];
+        const int b = (int)(i % mars_ctx::kBranches);
+        ctx->stream = ctx->branch[b];
+        {
+            Scratch sb(ctx->branch[b]);
+            err = run_level(ctx, sb, d_plane, d_D, w, h, j.size, j.shift, fp, d_rc + off,
+                            d_rc + total + off, j.rows.size(), d_out + off, 1);
+        }
+        ctx->stream = main;
+        off += j.rows.size();
+    }
+    // Join every branch that was forked, also after an error (a capture must end joined).
+    for (int b = 0; b < nb; ++b) {
+        MARS_CUDA(cudaEventRecord(ctx->join_ev[b], ctx->branch[b]));
+        MARS_CUDA(cudaStreamWaitEvent(main, ctx->join_ev[b], 0));
+    }
+    return err;
+}
+
 int plan_enqueue(mars_search_plan* p, bool with_copies) {
     mars_ctx* ctx = p->ctx;
     const cudaStream_t st = ctx->stream;
@@ -1259,7 +1311,7 @@ int plan_enqueue(mars_search_plan* p, bool with_copies) {
                                   cudaMemcpyHostToDevice, st));
     MARS_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), st));
     const mars::FitParams fp = make_fit_params(p->params);
-    if (int e = run_jobs(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out, 1, p->d_rc))
+    if (int e = run_jobs_branched(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out, p->d_rc))
         return e;
     if (with_copies) {
         MARS_CUDA(cudaMemcpyAsync(p->h_out, p->d_out, p->total * sizeof(mars_candidate),

@@ -28,6 +28,12 @@ struct mars_ctx {
     bool tma_16_boxes = false;                // load A stages as 16 2-D boxes (A/B checks)
     bool fold_only = false;                   // no split-digit operand at sizes 16..64 (A/B)
     PFN_cuTensorMapEncodeTiled_v12000 encode_tiled = nullptr;
+    // Streams and events a search plan's capture forks its levels onto (created on first use;
+    // the levels of a plane run as parallel branches of the plan's graph).
+    static constexpr int kBranches = 4;
+    cudaStream_t branch[kBranches] = {};
+    cudaEvent_t fork_ev = nullptr;
+    cudaEvent_t join_ev[kBranches] = {};
     // Search plans mars_encode keeps for plane geometries it has met before (api.cu).
     std::mutex plan_cache_mu;
     std::vector<std::pair<std::string, mars_search_plan*>> plan_cache;

@@ -639,6 +639,12 @@ int mars_refine_run(mars_refine_plan* p, uint32_t steps, float lr, uint32_t deco
     const int kTries = 8;          // step halvings per gradient step
     const double kMaxDs = 0.25, kMaxShift = 16.0;  // per-leaf trust region of a step
     const int kPasses = 6;         // discrete descent passes on the format grid
+    // Progressive re-quantisation: the fractions of the live leaves fixed to the grid in
+    // turn (those whose rounding the model prices cheapest first), each followed by
+    // kRefixSteps continuous steps of the leaves still free, which absorb the fixed
+    // leaves' rounding through the attractor's coupling.
+    const double kFixFractions[] = {0.5, 0.75, 0.9};
+    const uint32_t kRefixSteps = 3;
     std::memset(report, 0, sizeof *report);
 
     // decode_leaf's dequantisation (ifs.rs:434-439) of a grid point.
@@ -678,75 +684,86 @@ int mars_refine_run(mars_refine_plan* p, uint32_t steps, float lr, uint32_t deco
 
         // 1. Continuous steps from the plain search's dequantised parameters.
         std::vector<float> s = p->s0, o = p->o0, ts(n), to(n);
+        std::vector<char> fixed(n, 0);  // leaves already put on the grid (phase 1b)
         double loss = 0.0;
         if (int e = evaluate(s, o, true, &loss)) return e;
         if (int e = gradients(true)) return e;
         report->loss_start = loss;
         double step = lr;
-        for (uint32_t it = 0; it < steps; ++it) {
-            report->steps = it + 1;
-            bool moved = false;
-            for (int tr = 0; tr < kTries && !moved; ++tr, step *= 0.5) {
-                // Per leaf, the damped Newton step of the 2x2 model H = 2 [[sum d^2, sum d],
-                // [sum d, n]] (the curvature without the feedback through the domains) on the
-                // exact gradient.  When s hits its bounds, o takes the model's optimum for the
-                // clamped s, so near-flat domains cannot trade a clamped s for a runaway o.
-                for (size_t k = 0; k < n; ++k) {
-                    ts[k] = s[k];
-                    to[k] = o[k];
-                    const double* c = &st[k * kGradStats];
-                    const double gs = c[0], go = c[1], A = c[2], B = c[3], C = c[4];
-                    if (p->kind[k] == kRAffine || C <= 0.0) continue;
-                    double ds = 0.0;
-                    if (p->kind[k] == kRDomain) {
-                        const double det = A * C - B * B;
-                        if (det > 1e-9 * A * C) {
-                            double sn = (double)s[k] - step * (C * gs - B * go) / (2.0 * det);
-                            sn = std::min(std::max(sn, s_lo), s_hi);
-                            ds = sn - (double)s[k];
+        // `count` damped Newton steps of the free leaves; false when a step found no descent.
+        auto newton_steps = [&](uint32_t count, uint32_t* taken, int* err) -> bool {
+            for (uint32_t it = 0; it < count; ++it) {
+                ++*taken;
+                bool moved = false;
+                for (int tr = 0; tr < kTries && !moved; ++tr, step *= 0.5) {
+                    // Per leaf, the damped Newton step of the 2x2 model H = 2 [[sum d^2,
+                    // sum d], [sum d, n]] (the curvature without the feedback through the
+                    // domains) on the exact gradient.  When s hits its bounds, o takes the
+                    // model's optimum for the clamped s, so near-flat domains cannot trade a
+                    // clamped s for a runaway o.
+                    for (size_t k = 0; k < n; ++k) {
+                        ts[k] = s[k];
+                        to[k] = o[k];
+                        const double* c = &st[k * kGradStats];
+                        const double gs = c[0], go = c[1], A = c[2], B = c[3], C = c[4];
+                        if (fixed[k] || p->kind[k] == kRAffine || C <= 0.0) continue;
+                        double ds = 0.0;
+                        if (p->kind[k] == kRDomain) {
+                            const double det = A * C - B * B;
+                            if (det > 1e-9 * A * C) {
+                                double sn = (double)s[k] - step * (C * gs - B * go) / (2.0 * det);
+                                sn = std::min(std::max(sn, s_lo), s_hi);
+                                ds = sn - (double)s[k];
+                            }
                         }
+                        // A trust region per leaf: |ds| <= kMaxDs and the leaf's mean value
+                        // moves by at most kMaxShift grey levels, so one ill-conditioned leaf
+                        // cannot spoil the step of all the others.
+                        ds = std::min(std::max(ds, -kMaxDs), kMaxDs);
+                        const double sn = (double)s[k] + ds;
+                        double dov = -step * go / (2.0 * C) - B / C * ds;
+                        const double shift = ds * B / C + dov;
+                        dov -= shift - std::min(std::max(shift, -kMaxShift), kMaxShift);
+                        const double on = (double)o[k] + dov;
+                        // The offsets the header's beta grid can express for this contrast.
+                        const double a = p->kind[k] == kRDomain ? sn : 0.0;
+                        ts[k] = (float)sn;
+                        to[k] = (float)std::min(std::max(on, -a * 255.0), 255.0);
                     }
-                    // A trust region per leaf: |ds| <= kMaxDs and the leaf's mean value moves
-                    // by at most kMaxShift grey levels, so one ill-conditioned leaf cannot
-                    // spoil the step of all the others.
-                    ds = std::min(std::max(ds, -kMaxDs), kMaxDs);
-                    const double sn = (double)s[k] + ds;
-                    double dov = -step * go / (2.0 * C) - B / C * ds;
-                    const double shift = ds * B / C + dov;
-                    dov -= shift - std::min(std::max(shift, -kMaxShift), kMaxShift);
-                    const double on = (double)o[k] + dov;
-                    // The offsets the header's beta grid can express for this contrast.
-                    const double a = p->kind[k] == kRDomain ? sn : 0.0;
-                    ts[k] = (float)sn;
-                    to[k] = (float)std::min(std::max(on, -a * 255.0), 255.0);
+                    double tl = 0.0;
+                    if ((*err = evaluate(ts, to, false, &tl))) return false;
+                    if (tl < loss) {
+                        loss = tl;
+                        s.swap(ts);
+                        o.swap(to);
+                        moved = true;
+                        report->improving_steps += 1;
+                    }
                 }
-                double tl = 0.0;
-                if (int e = evaluate(ts, to, false, &tl)) return e;
-                if (tl < loss) {
-                    loss = tl;
-                    s.swap(ts);
-                    o.swap(to);
-                    moved = true;
-                    report->improving_steps += 1;
-                }
+                if (!moved) return false;  // no descent along this direction at any damping
+                step = std::min((double)lr, step * 4.0);  // undo the last halving, then grow
+                // The accepted trial was the last solve: the linearisation is at (s, o).
+                if ((*err = gradients(false))) return false;
             }
-            if (!moved) break;  // no descent along this direction at any tried damping
-            step = std::min((double)lr, step * 4.0);  // undo the last halving, then grow
-            // The accepted trial was the last solve: the linearisation is at (s, o).
-            if (int e = gradients(false)) return e;
+            return true;
+        };
+        {
+            int err = 0;
+            uint32_t taken = 0;
+            newton_steps(steps, &taken, &err);
+            if (err) return err;
+            report->steps = taken;
         }
         report->loss_end = loss;
 
-        // 2. Re-quantisation, aware of the (s, o) coupling: per leaf the grid points around
-        // the continuous optimum (qalfa rounded down and up, each with the offset moved to
-        // the model's optimum for that alfa, qbeta rounded down and up) are scored with the
-        // quadratic model of the last statistics and the cheapest kept.  Domain leaves keep
-        // qalfa >= 1.
-        for (size_t k = 0; k < n; ++k) {
-            mars_leaf& L = grid[k];
+        // The grid point of leaf k nearest its continuous (s, o) under the quadratic model of
+        // the last statistics: qalfa rounded down and up, each with the offset moved to the
+        // model's optimum for that alfa, qbeta rounded down and up; domain leaves keep
+        // qalfa >= 1.  Returns the model cost of the move (or -1 for a leaf left as it is).
+        auto nearest_grid = [&](size_t k, mars_leaf* L) -> double {
             const double* c = &st[k * kGradStats];
             const double A = c[2], B = c[3], C = c[4];
-            if (p->kind[k] == kRAffine || C <= 0.0) continue;  // no live pixel: keep it as it was
+            if (p->kind[k] == kRAffine || C <= 0.0) return -1.0;  // no live pixel
             const bool domain = p->kind[k] == kRDomain;
             const double qs = domain ? (double)s[k] / alfa_unit : 0.0;
             const uint32_t qa_lo = domain ? (uint32_t)std::max(1.0, std::min((double)max_qalfa, std::floor(qs))) : 0;
@@ -761,12 +778,57 @@ int mars_refine_run(mars_refine_plan* p, uint32_t steps, float lr, uint32_t deco
                     const double cost = A * dsv * dsv + 2.0 * B * dsv * dov + C * dov * dov;
                     if (cost < best) {
                         best = cost;
-                        if (domain) L.qalfa = qa;
-                        L.qbeta = qb;
+                        if (domain) L->qalfa = qa;
+                        L->qbeta = qb;
                     }
                 }
             }
+            return best;
+        };
+
+        // 1b. Progressive re-quantisation: fix the cheapest-to-round leaves to their grid
+        // points, let the free ones absorb the change, and fix more.
+        {
+            size_t live = 0;
+            for (size_t k = 0; k < n; ++k) live += nearest_grid(k, &grid[k]) >= 0.0 ? 1u : 0u;
+            std::vector<std::pair<double, size_t>> order;
+            for (double frac : kFixFractions) {
+                order.clear();
+                size_t nfixed = 0;
+                for (size_t k = 0; k < n; ++k) {
+                    if (fixed[k]) {
+                        ++nfixed;
+                        continue;
+                    }
+                    mars_leaf L = grid[k];
+                    const double cost = nearest_grid(k, &L);
+                    if (cost >= 0.0) order.push_back({cost, k});
+                }
+                const size_t want = (size_t)(frac * (double)live);
+                if (want <= nfixed || order.empty()) continue;
+                std::sort(order.begin(), order.end());
+                const size_t add = std::min(order.size(), want - nfixed);
+                for (size_t i = 0; i < add; ++i) {
+                    const size_t k = order[i].second;
+                    nearest_grid(k, &grid[k]);
+                    fixed[k] = 1;
+                    s[k] = p->kind[k] == kRDomain ? (float)alfa_of(grid[k].qalfa) : 0.0f;
+                    o[k] = (float)beta_of(p->kind[k] == kRDomain ? grid[k].qalfa : 0, grid[k].qbeta);
+                }
+                if (int e = evaluate(s, o, false, &loss)) return e;
+                if (int e = gradients(false)) return e;
+                int err = 0;
+                uint32_t taken = 0;
+                step = lr;
+                newton_steps(kRefixSteps, &taken, &err);
+                if (err) return err;
+            }
         }
+
+        // 2. Re-quantisation of the leaves still free, aware of the (s, o) coupling (the
+        // model-cheapest grid point around each continuous optimum).
+        for (size_t k = 0; k < n; ++k)
+            if (!fixed[k]) nearest_grid(k, &grid[k]);
 
         // 3. Discrete descent on the grid: at the current grid point, the exact gradient and
         // the 2x2 model rank each leaf's neighbouring grid points (qalfa +-1 with the model's
