@@ -56,10 +56,13 @@ NCU_TRAFFIC = {4: 20_560_000}
 # Thread instructions per candidate fit of the correlation kernel's level (warp
 # instructions x 32 / fits, same capture): the issue cost behind the epilogue roofline.
 NCU_INSTR_PER_FIT = {4: 1.14e9 * 32 / 8.52e9, 8: 0.42e9 * 32 / 2.0e9}
-# DRAM bytes of one decode iteration, by plane side (profiles/decode_cell_4096x4096_ncu.md,
-# profiles/decode_cell_16384x16384_ncu.md; the 16384^2 figure is
-# dram__bytes.sum.per_second x gpu__time_duration.sum of its capture).
-NCU_DECODE_TRAFFIC = {4096: 34_831_104 + 748_800, 16384: 4_797_900_000}
+# DRAM bytes of one decode iteration, by plane side (profiles/decode_cell_4096x4096_ncu.md;
+# profiles/decode_sorted_16384x16384_ncu.md: dram__bytes.sum.per_second x
+# gpu__time_duration.sum of the gather and the place launch of one iteration).
+NCU_DECODE_TRAFFIC = {4096: 34_831_104 + 748_800, 16384: 651_660_000 + 802_090_000}
+# The kernels of one decode iteration: the cell kernel while the two planes total at most
+# 96 MiB, the source-ordered gather and place beyond (api.cu, want_sorted_decode).
+DECODE_SORTED_BYTES = 96 << 20
 
 
 def rank_info():
@@ -291,7 +294,10 @@ def run_decode(args, mb, ctx, stream, dev, peaks, side, with_cpu, flush=None):
                "timed decodes (256 MiB write)") if resident else
               "not flushed: both planes exceed L2",
         "clocks": clocks.summary(),
-        "roofline": {"bound": "hbm", "kernel": "decode_cell_kernel", "achieved": achieved,
+        "roofline": {"bound": "hbm",
+                     "kernel": ("sorted_gather_kernel + sorted_place_kernel"
+                                if 2 * px > DECODE_SORTED_BYTES else "decode_cell_kernel"),
+                     "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": NCU_DECODE_TRAFFIC.get(side), "peak_source": src,
                      "bytes_per_launch": algo / DECODE_ITERS,
@@ -857,6 +863,9 @@ def main():
                          "--refine-lambdas, and print its JSON object")
     ap.add_argument("--refine-seeds", default=",".join(map(str, REFINE_SEEDS)))
     ap.add_argument("--refine-lambdas", default=",".join(str(int(l)) for l in REFINE_LAMBDAS))
+    ap.add_argument("--decode-only", type=int, default=0, metavar="SIDE",
+                    help="run only the decode leg on a SIDE x SIDE synthetic map (for "
+                         "profiling) and print its JSON object")
     ap.add_argument("--classified-only", action="store_true",
                     help="run only the classified colour leg (for profiling) and print its "
                          "JSON object")
@@ -868,6 +877,24 @@ def main():
         return run_reference(args)
     if args.profile_large:
         return run_large_profile(args)
+    if args.decode_only:
+        import torch
+        import mars_b200 as mb
+        torch.cuda.set_device(0)
+        dev = torch.device("cuda", 0)
+        stream = torch.cuda.Stream(dev)
+        torch.cuda.set_stream(stream)
+        ctx = mb.Context(0)
+        ctx.set_stream(stream.cuda_stream)
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        print(json.dumps({"decode": run_decode(args, mb, ctx, stream, dev, peaks, args.decode_only,
+                                               False)}), flush=True)
+        ctx.close()
+        return 0
     if args.classified_only:
         import torch
         import mars_b200 as mb

@@ -1876,7 +1876,25 @@ struct mars_decode_plan {
     mars::DecodeMap* d_maps = nullptr;
     double* d_rvals = nullptr;  // mode-3 residual values, or null
     uint8_t* d_tmp = nullptr;   // ping-pong partner of the caller's output buffer
+    // Source-ordered steps (planes larger than L2; decode.cu): the domain cells' jobs in
+    // source-row order, each 4x4 cell's job slot, and the per-cell output buffer.
+    mars::DecodeConsts consts{};
+    uint4* d_jobs = nullptr;
+    uint32_t* d_inv = nullptr;
+    uint4* d_cellbuf = nullptr;
+    uint32_t njobs = 0;
 };
+
+namespace {
+// Whether a decode plan of a w x h plane takes the source-ordered steps: by default when
+// the two ping-pong planes exceed 96 MB (they no longer stay in L2 between steps);
+// MARS_DECODE_SORTED=1 / 0 forces it on (where eligible) / off.
+bool want_sorted_decode(uint32_t w, uint32_t h) {
+    const char* e = std::getenv("MARS_DECODE_SORTED");
+    if (e && *e) return std::string(e) != "0";
+    return 2ull * w * h > (96ull << 20);
+}
+}  // namespace
 
 extern "C" {
 
@@ -1980,14 +1998,39 @@ int mars_decode_plan_create(mars_ctx* ctx, const mars_header* hdr, const mars_le
         e = mars::launch_decode_expand(d_leaves, d_roff, (int)n, consts, p->d_maps, ctx->stream);
         ctx->launches += 1;
     }
+    p->consts = consts;
+    uint32_t *d_key = nullptr, *d_rows = nullptr, *d_cursor = nullptr;
+    if (e == cudaSuccess && n && want_sorted_decode(p->w, p->h) &&
+        mars::decode_sorted_eligible((int)p->w, (int)p->h, lg, !rvals.empty())) {
+        const size_t cells = mars::decode_sorted_cells((int)p->w, (int)p->h);
+        e = cudaMalloc(&d_key, cells * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&d_rows, (size_t)p->h * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&d_cursor, ((size_t)p->h + 1) * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_jobs, cells * sizeof(uint4));
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_inv, cells * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_cellbuf, cells * sizeof(uint4));
+        if (e == cudaSuccess)
+            e = mars::launch_decode_sorted_build((int)p->w, (int)p->h, lg, p->d_owner, p->d_maps,
+                                                 d_leaves, d_key, d_rows, d_cursor, p->d_jobs,
+                                                 p->d_inv, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&p->njobs, d_cursor + p->h, 4, cudaMemcpyDeviceToHost, ctx->stream);
+        ctx->launches += 3;
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     cudaFree(d_leaves);
     cudaFree(d_roff);
+    cudaFree(d_key);
+    cudaFree(d_rows);
+    cudaFree(d_cursor);
     if (e != cudaSuccess) {
         cudaFree(p->d_owner);
         cudaFree(p->d_maps);
         cudaFree(p->d_rvals);
         cudaFree(p->d_tmp);
+        cudaFree(p->d_jobs);
+        cudaFree(p->d_inv);
+        cudaFree(p->d_cellbuf);
         delete p;
         return fail(MARS_ECUDA, std::string("decode plan: ") + cudaGetErrorString(e));
     }
@@ -2005,9 +2048,16 @@ int mars_decode_plan_run(mars_decode_plan* p, uint32_t iterations, uint8_t* d_ou
     uint8_t* b = (iterations & 1) ? d_out : p->d_tmp;
     MARS_CUDA(cudaMemsetAsync(a, 128, (size_t)p->w * p->h, ctx->stream));
     for (uint32_t it = 0; it < iterations; ++it) {
-        MARS_CUDA(mars::launch_decode_step(a, b, (int)p->w, (int)p->h, p->lg, p->d_owner,
-                                           p->d_maps, p->d_rvals, ctx->stream));
-        ctx->launches += 1;
+        if (p->d_jobs) {
+            MARS_CUDA(mars::launch_decode_sorted_step(a, b, (int)p->w, (int)p->h, p->lg, p->d_owner,
+                                                      p->d_maps, p->d_jobs, p->njobs, p->d_inv,
+                                                      p->consts, p->d_cellbuf, ctx->stream));
+            ctx->launches += 2;
+        } else {
+            MARS_CUDA(mars::launch_decode_step(a, b, (int)p->w, (int)p->h, p->lg, p->d_owner,
+                                               p->d_maps, p->d_rvals, ctx->stream));
+            ctx->launches += 1;
+        }
         std::swap(a, b);
     }
     return MARS_OK;
@@ -2126,6 +2176,9 @@ void mars_decode_plan_free(mars_decode_plan* p) {
     cudaFree(p->d_maps);
     cudaFree(p->d_rvals);
     cudaFree(p->d_tmp);
+    cudaFree(p->d_jobs);
+    cudaFree(p->d_inv);
+    cudaFree(p->d_cellbuf);
     delete p;
 }
 

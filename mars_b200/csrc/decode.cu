@@ -337,6 +337,204 @@ __global__ void decode_converged_kernel(const int* __restrict__ delta, int thres
     }
 }
 
+// ---- source-ordered decode of planes larger than L2 (decode_sorted_*) ----
+//
+// Gathering cell by cell in output order reads each cell's 8x8 domain window from a random
+// place of the previous iterate; once the plane no longer fits in L2, every 8-byte row read
+// costs whole DRAM sectors.  The source-ordered form splits a step in two:
+//   gather : the domain cells in the order of their windows' source rows (a list built once
+//            per leaf list), each computing its 16 output bytes into a cell buffer; the
+//            windows of cells running together lie in a narrow band of source rows, which
+//            L2 keeps, so the plane is read about once;
+//   place  : every output cell in output order, copying its 16 bytes from the cell buffer
+//            (domain cells) or computing them (constant and affine cells), four coalesced
+//            4-byte row stores.
+// The values are the cell kernel's, operation for operation.  Maps with mode-3 residuals keep
+// the cell kernel.
+
+// The window of a domain cell: the byte offset of its top-left sample pixel and the source
+// row it starts at.
+__device__ __forceinline__ void cell_window(const DecodeMap& m, int x0, int y0, int w,
+                                            size_t* off, int* row) {
+    const int S = (int)(m.info & 0xFFFu);
+    const int k = (int)((m.info >> 14) & 7u);
+    const IsoInv t = iso_inverse(k, S - 1);
+    const int i0 = y0 - (int)(m.rc & 0xFFFFu), j0 = x0 - (int)(m.rc >> 16);
+    const int u00 = t.cu + t.ai * i0 + t.aj * j0, v00 = t.cv + t.bi * i0 + t.bj * j0;
+    const int umin = u00 - 3 * ((t.ai < 0) | (t.aj < 0));
+    const int vmin = v00 - 3 * ((t.bi < 0) | (t.bj < 0));
+    *row = (int)(m.dom & 0xFFFFu) + 2 * umin;
+    *off = (size_t)(*row) * w + (m.dom >> 16) + 2 * vmin;
+}
+
+__device__ __forceinline__ bool is_domain_cell(const DecodeMap& m) {
+    return ((m.info >> 12) & 3u) == kLeafDomain;
+}
+
+// Pass 1 of the list build: per 4x4 cell its window's source row (or ~0 for a cell without
+// a domain window) and the rows' cell counts.
+__global__ void sorted_key_kernel(int w, int h, int lg, int mw, const int32_t* __restrict__ owner,
+                                  const DecodeMap* __restrict__ maps, uint32_t* __restrict__ key,
+                                  uint32_t* __restrict__ row_count) {
+    const int cw = w / 4, chh = (h + 3) / 4;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (long long)cw * chh) return;
+    const int x0 = 4 * (int)(c % cw), y0 = 4 * (int)(c / cw);
+    const int32_t li = owner[(size_t)(y0 >> lg) * mw + (x0 >> lg)];
+    uint32_t k = 0xFFFFFFFFu;
+    if (li >= 0) {
+        const DecodeMap m = maps[li];
+        if (is_domain_cell(m)) {
+            size_t off;
+            int row;
+            cell_window(m, x0, y0, w, &off, &row);
+            k = (uint32_t)row;
+            atomicAdd(&row_count[row], 1u);
+        }
+    }
+    key[c] = k;
+}
+
+// Exclusive scan of the row counts (one block): the first list slot of each source row, and
+// in cursor[h] the total.
+__global__ void sorted_scan_kernel(const uint32_t* __restrict__ row_count, int h,
+                                   uint32_t* __restrict__ cursor) {
+    __shared__ uint32_t carry;
+    __shared__ uint32_t warp_tot[32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int base = 0; base < h; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const uint32_t v = i < h ? row_count[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[warp] = x;
+        __syncthreads();
+        uint32_t before = carry;
+        for (int k = 0; k < warp; ++k) before += warp_tot[k];
+        if (i < h) cursor[i] = before + x - v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t all = 0;
+            for (int k = 0; k < nw; ++k) all += warp_tot[k];
+            carry += all;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) cursor[h] = carry;  // the number of domain cells
+}
+
+// Pass 2: each domain cell takes the next slot of its source row and writes its job
+// (window offset, qalfa | isometry << 24, beta) there and the slot into inv.
+__global__ void sorted_scatter_kernel(int w, int h, int lg, int mw,
+                                      const int32_t* __restrict__ owner,
+                                      const DecodeMap* __restrict__ maps,
+                                      const DecodeLeaf* __restrict__ leaves,
+                                      const uint32_t* __restrict__ key, uint32_t* __restrict__ cursor,
+                                      uint4* __restrict__ jobs, uint32_t* __restrict__ inv) {
+    const int cw = w / 4, chh = (h + 3) / 4;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (long long)cw * chh) return;
+    const uint32_t row = key[c];
+    if (row == 0xFFFFFFFFu) return;
+    const int x0 = 4 * (int)(c % cw), y0 = 4 * (int)(c / cw);
+    const int32_t li = owner[(size_t)(y0 >> lg) * mw + (x0 >> lg)];
+    const DecodeMap m = maps[li];
+    size_t off;
+    int r;
+    cell_window(m, x0, y0, w, &off, &r);
+    const uint32_t pos = atomicAdd(&cursor[row], 1u);
+    const uint32_t qalfa = leaves[li].w & 0x1FFFFu;
+    const uint32_t k = (m.info >> 14) & 7u;
+    jobs[pos] = make_uint4((uint32_t)off, qalfa | (k << 24),
+                           (uint32_t)__double2loint(m.b), (uint32_t)__double2hiint(m.b));
+    inv[c] = pos;
+}
+
+// Gather pass: job -> the cell's 16 output bytes (row-major 4x4) in the cell buffer.
+__global__ void __launch_bounds__(128) sorted_gather_kernel(
+    const uint8_t* __restrict__ src, size_t total, int w, const uint4* __restrict__ jobs,
+    uint32_t n, DecodeConsts cst, uint4* __restrict__ cellbuf) {
+    const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const uint4 jb = jobs[pos];
+    size_t off = jb.x;
+    const int k = (int)(jb.y >> 24);
+    DecodeMap m;
+    // decode_expand's a = alfa / 4, alfa = (qalfa / 2^bits_alfa) * max_alfa (ifs.rs:434-439).
+    m.a = __dmul_rn(__dmul_rn(__ddiv_rn((double)(jb.y & 0x1FFFFu), cst.alfa_den), cst.max_alfa), 0.25);
+    m.b = __hiloint2double((int)jb.w, (int)jb.z);
+    uint32_t sums[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+#pragma unroll
+    for (int r = 0; r < 8; ++r, off += w) {
+        const uint64_t row = load8(src, off, total);
+        sums[r >> 1][0] += pair_sums((uint32_t)row);
+        sums[r >> 1][1] += pair_sums((uint32_t)(row >> 32));
+    }
+    uint32_t rw[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int sum = (int)((sums[p][q >> 1] >> (16 * (q & 1))) & 0xFFFFu);
+            rw[p] |= to_u8(domain_value(sum, m)) << (8 * q);
+        }
+    const bool tr = (0xC6u >> k) & 1u, uneg = (0xACu >> k) & 1u, vneg = (0x9Au >> k) & 1u;
+    if (vneg) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) rw[p] = __byte_perm(rw[p], 0, 0x0123);
+    }
+    if (uneg) {
+        const uint32_t t0 = rw[0], t1 = rw[1];
+        rw[0] = rw[3];
+        rw[1] = rw[2];
+        rw[2] = t1;
+        rw[3] = t0;
+    }
+    if (tr) transpose4x4(rw[0], rw[1], rw[2], rw[3]);
+    cellbuf[pos] = make_uint4(rw[0], rw[1], rw[2], rw[3]);
+}
+
+// Place pass: every 4x4 output cell in output order.
+__global__ void __launch_bounds__(128) sorted_place_kernel(
+    uint8_t* __restrict__ dst, int w, int h, int lg, int mw, const int32_t* __restrict__ owner,
+    const DecodeMap* __restrict__ maps, const uint32_t* __restrict__ inv,
+    const uint4* __restrict__ cellbuf) {
+    const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int y0 = 4 * blockIdx.y;
+    if (x0 >= w || y0 >= h) return;
+    const int32_t li = owner[(size_t)(y0 >> lg) * mw + (x0 >> lg)];
+    uint32_t rw[4] = {0, 0, 0, 0};
+    if (li >= 0) {
+        const DecodeMap m = maps[li];
+        const uint32_t kind = (m.info >> 12) & 3u;
+        if (kind == kLeafDomain) {
+            const uint4 v = cellbuf[inv[(size_t)(y0 / 4) * (w / 4) + x0 / 4]];
+            rw[0] = v.x;
+            rw[1] = v.y;
+            rw[2] = v.z;
+            rw[3] = v.w;
+        } else if (kind == kLeafConst) {
+            rw[0] = rw[1] = rw[2] = rw[3] = 0x01010101u * (m.info >> 24);
+        } else {
+            const int i0 = y0 - (int)(m.rc & 0xFFFFu), j0 = x0 - (int)(m.rc >> 16);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) rw[a] |= affine_pixel(m, i0 + a, j0 + b) << (8 * b);
+        }
+    }
+    uint8_t* out = dst + (size_t)y0 * w + x0;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+        if (y0 + a < h) *reinterpret_cast<uint32_t*>(out + (size_t)a * w) = rw[a];
+}
+
 }  // namespace
 
 cudaError_t launch_decode_expand(const DecodeLeaf* leaves, const int32_t* resid_off, int n,
@@ -384,6 +582,42 @@ cudaError_t launch_decode_step_stable(const uint8_t* src, uint8_t* dst, int w, i
                                                         resid, ss);
     }
     decode_converged_kernel<<<1, 1, 0, st>>>(delta, threshold, iter, done_w, used);
+    return cudaGetLastError();
+}
+
+
+size_t decode_sorted_cells(int w, int h) { return (size_t)(w / 4) * ((h + 3) / 4); }
+
+bool decode_sorted_eligible(int w, int h, int lg, bool residuals) {
+    return lg >= 2 && (w % 4) == 0 && !residuals && w > 0 && h > 0;
+}
+
+cudaError_t launch_decode_sorted_build(int w, int h, int lg, const int32_t* owner,
+                                       const DecodeMap* maps, const DecodeLeaf* leaves,
+                                       uint32_t* key, uint32_t* row_count, uint32_t* cursor,
+                                       uint4* jobs, uint32_t* inv, cudaStream_t st) {
+    const int mw = (w + (1 << lg) - 1) >> lg;
+    const size_t cells = decode_sorted_cells(w, h);
+    cudaError_t e = cudaMemsetAsync(row_count, 0, (size_t)h * 4, st);
+    if (e != cudaSuccess) return e;
+    const unsigned blocks = (unsigned)((cells + 255) / 256);
+    sorted_key_kernel<<<blocks, 256, 0, st>>>(w, h, lg, mw, owner, maps, key, row_count);
+    sorted_scan_kernel<<<1, 1024, 0, st>>>(row_count, h, cursor);
+    sorted_scatter_kernel<<<blocks, 256, 0, st>>>(w, h, lg, mw, owner, maps, leaves, key, cursor,
+                                                   jobs, inv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decode_sorted_step(const uint8_t* src, uint8_t* dst, int w, int h, int lg,
+                                      const int32_t* owner, const DecodeMap* maps,
+                                      const uint4* jobs, uint32_t njobs, const uint32_t* inv,
+                                      DecodeConsts c, uint4* cellbuf, cudaStream_t st) {
+    const int mw = (w + (1 << lg) - 1) >> lg;
+    if (njobs)
+        sorted_gather_kernel<<<(njobs + 127) / 128, 128, 0, st>>>(src, (size_t)w * h, w, jobs,
+                                                                 njobs, c, cellbuf);
+    dim3 grid((w / 4 + 127) / 128, (h + 3) / 4);
+    sorted_place_kernel<<<grid, 128, 0, st>>>(dst, w, h, lg, mw, owner, maps, inv, cellbuf);
     return cudaGetLastError();
 }
 

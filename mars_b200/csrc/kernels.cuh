@@ -184,6 +184,23 @@ cudaError_t launch_decode_step(const uint8_t* src, uint8_t* dst, int w, int h, i
                                const int32_t* owner, const DecodeMap* maps, const double* resid,
                                cudaStream_t st);
 
+// Source-ordered decode of large planes (decode.cu): the domain cells' jobs sorted by the
+// source row of their windows (built once per leaf list), then per step a gather into a
+// 16-byte-per-cell buffer and a placement in output order.  Eligible: cells of 4 x 4 pixels
+// or more (lg >= 2), width % 4 == 0, no mode-3 residuals.  key / inv hold one word per 4x4
+// cell, jobs and the cell buffer 16 bytes per domain cell (at most one per cell), row_count
+// h words and cursor h + 1 (cursor[h]: the number of domain cells after the build).
+size_t decode_sorted_cells(int w, int h);
+bool decode_sorted_eligible(int w, int h, int lg, bool residuals);
+cudaError_t launch_decode_sorted_build(int w, int h, int lg, const int32_t* owner,
+                                       const DecodeMap* maps, const DecodeLeaf* leaves,
+                                       uint32_t* key, uint32_t* row_count, uint32_t* cursor,
+                                       uint4* jobs, uint32_t* inv, cudaStream_t st);
+cudaError_t launch_decode_sorted_step(const uint8_t* src, uint8_t* dst, int w, int h, int lg,
+                                      const int32_t* owner, const DecodeMap* maps,
+                                      const uint4* jobs, uint32_t njobs, const uint32_t* inv,
+                                      DecodeConsts c, uint4* cellbuf, cudaStream_t st);
+
 // RD pricing of one node size (rdprice.cu): count nodes of size x size at (rows, cols), k
 // candidates each; out[i] the node's priced winner, levels[levels_at[i]..] its mode-3 levels.
 // basis: basis(size, k, i) at [k * size + i], computed on the host.  Sizes 2..64; size 64

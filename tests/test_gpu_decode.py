@@ -217,3 +217,25 @@ def test_zoomed_decode_matches_the_oracle(ctx, factor):
     got = ctx.decode(zh, zl, 10)
     assert got.shape == (round(96 * factor), round(128 * factor))
     assert np.array_equal(got, orc.decode(ozh, ozl, 10))
+
+
+@pytest.mark.parametrize("w,h,seed", [(320, 256, 11), (1024, 768, 13), (516, 302, 14)])
+def test_source_ordered_plan_steps_match_the_oracle(ctx, monkeypatch, w, h, seed):
+    """The source-ordered steps large planes take (domain cells gathered in the order of their
+    windows' source rows into a cell buffer, then placed in output order) give the cell
+    kernel's bytes: forced on here for planes small enough for the oracle; (516, 302) leaves a
+    border no leaf covers and a last cell row cut by the plane's edge."""
+    import torch
+    monkeypatch.setenv("MARS_DECODE_SORTED", "1")
+    leaves = synthetic.quadtree_leaves(w, h, seed)
+    hdr = _hdr(w, h)
+    plan = ctx.decode_plan(hdr, leaves)
+    dev = torch.empty(w * h, dtype=torch.uint8, device="cuda:0")
+    for iters in (1, 3, 10):
+        dev.fill_(7)
+        torch.cuda.synchronize()
+        plan.run(iters, dev.data_ptr())
+        torch.cuda.synchronize()
+        got = dev.cpu().numpy().reshape(h, w)
+        assert np.array_equal(got, orc.decode(_ohdr(hdr), leaves, iters)), iters
+    plan.close()
