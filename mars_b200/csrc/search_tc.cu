@@ -683,29 +683,66 @@ __global__ void build_b_kernel(const uint8_t* __restrict__ plane, int w, int h,
 
 // Digit phase copies of the contracted plane D (dw x dh, i32, 0..1020): plane
 // z = digit * P + p (digit 0 = hi = D >> 7, 1 = lo = D & 127) is that digit shifted left by
-// step_c * p samples, zero past the right edge; row pitch wp (a multiple of 16).
+// STEP * p samples, zero past the right edge; row pitch wp (a multiple of 16).  One thread
+// per 16 output columns of a row: it loads the 32 - STEP samples every phase of those
+// columns reads once and writes 16 bytes to each of the 2 P planes.
+template <int STEP>
 __global__ void digit_planes_kernel(const int32_t* __restrict__ D, int dw, int dh, int wp,
-                                    int step_c, int P, uint8_t* __restrict__ out) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+                                    uint8_t* __restrict__ out) {
+    constexpr int P = 16 / STEP, SPAN = 16 + STEP * (P - 1);
+    const int x = 16 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int y = blockIdx.y;
-    const int z = blockIdx.z;
-    if (x >= wp || y >= dh || z >= 2 * P) return;
-    const int digit = z / P, p = z % P;
-    const int sx = x + step_c * p;
-    const int v = sx < dw ? D[(size_t)y * dw + sx] : 0;
-    out[((size_t)z * dh + y) * wp + x] = (uint8_t)(digit == 0 ? v >> 7 : v & 127);
+    if (x >= wp || y >= dh) return;
+    const int32_t* row = D + (size_t)y * dw;
+    uint8_t hi[SPAN], lo[SPAN];
+#pragma unroll
+    for (int i = 0; i < SPAN; ++i) {
+        const int v = x + i < dw ? __ldg(row + x + i) : 0;
+        hi[i] = (uint8_t)(v >> 7);
+        lo[i] = (uint8_t)(v & 127);
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        uint32_t wh[4], wl[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int b = STEP * p + 4 * k;
+            wh[k] = hi[b] | hi[b + 1] << 8 | hi[b + 2] << 16 | (uint32_t)hi[b + 3] << 24;
+            wl[k] = lo[b] | lo[b + 1] << 8 | lo[b + 2] << 16 | (uint32_t)lo[b + 3] << 24;
+        }
+        *reinterpret_cast<uint4*>(out + ((size_t)p * dh + y) * wp + x) =
+            make_uint4(wh[0], wh[1], wh[2], wh[3]);
+        *reinterpret_cast<uint4*>(out + ((size_t)(P + p) * dh + y) * wp + x) =
+            make_uint4(wl[0], wl[1], wl[2], wl[3]);
+    }
 }
 
-// Phase copies of the plane: copy p (of P = 16 / shift) is the plane shifted left by
-// shift * p pixels, zero past the right edge; row pitch wp (a multiple of 16).
+// Phase copies of the plane: copy p (of P = 16 / SHIFT) is the plane shifted left by
+// SHIFT * p pixels, zero past the right edge; row pitch wp (a multiple of 16).  One thread
+// per 16 output columns of a row: the 32 - SHIFT source bytes all phases read, loaded once,
+// and one 16-byte store per phase.
+template <int SHIFT>
 __global__ void phase_planes_kernel(const uint8_t* __restrict__ plane, int w, int h, int wp,
-                                    int shift, int P, uint8_t* __restrict__ out) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+                                    uint8_t* __restrict__ out) {
+    constexpr int P = 16 / SHIFT, SPAN = 16 + SHIFT * (P - 1);
+    const int x = 16 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int y = blockIdx.y;
-    const int p = blockIdx.z;
-    if (x >= wp || y >= h || p >= P) return;
-    const int sx = x + shift * p;
-    out[((size_t)p * h + y) * wp + x] = sx < w ? plane[(size_t)y * w + sx] : 0;
+    if (x >= wp || y >= h) return;
+    const uint8_t* row = plane + (size_t)y * w;
+    uint8_t v[SPAN];
+#pragma unroll
+    for (int i = 0; i < SPAN; ++i) v[i] = x + i < w ? __ldg(row + x + i) : (uint8_t)0;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        uint32_t wd[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int b = SHIFT * p + 4 * k;
+            wd[k] = v[b] | v[b + 1] << 8 | v[b + 2] << 16 | (uint32_t)v[b + 3] << 24;
+        }
+        *reinterpret_cast<uint4*>(out + ((size_t)p * h + y) * wp + x) =
+            make_uint4(wd[0], wd[1], wd[2], wd[3]);
+    }
 }
 
 // isometry::map (crates/mars-codec/src/isometry.rs:7-19) as a flat range index i*S + j.
@@ -910,18 +947,30 @@ size_t digit_plane_bytes(int w, int h, int shift) {
 
 cudaError_t launch_digit_planes(const int32_t* D, int w, int h, int shift, uint8_t* out,
                                 cudaStream_t st) {
-    const int P = digit_phase_count(shift), dw = w / 2, dh = h / 2, wp = row_pitch(dw);
+    const int dw = w / 2, dh = h / 2, wp = row_pitch(dw);
     if (dh == 0) return cudaSuccess;
-    dim3 grid((wp + 255) / 256, dh, 2 * P);
-    digit_planes_kernel<<<grid, 256, 0, st>>>(D, dw, dh, wp, shift / 2, P, out);
+    dim3 grid((wp / 16 + 127) / 128, dh);
+    switch (shift) {
+        case 2: digit_planes_kernel<1><<<grid, 128, 0, st>>>(D, dw, dh, wp, out); break;
+        case 4: digit_planes_kernel<2><<<grid, 128, 0, st>>>(D, dw, dh, wp, out); break;
+        case 8: digit_planes_kernel<4><<<grid, 128, 0, st>>>(D, dw, dh, wp, out); break;
+        case 16: digit_planes_kernel<8><<<grid, 128, 0, st>>>(D, dw, dh, wp, out); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_phase_planes(const uint8_t* plane, int w, int h, int shift, uint8_t* out,
                                 cudaStream_t st) {
-    const int P = phase_count(shift), wp = row_pitch(w);
-    dim3 grid((wp + 255) / 256, h, P);
-    phase_planes_kernel<<<grid, 256, 0, st>>>(plane, w, h, wp, shift, P, out);
+    const int wp = row_pitch(w);
+    dim3 grid((wp / 16 + 127) / 128, h);
+    switch (shift) {
+        case 2: phase_planes_kernel<2><<<grid, 128, 0, st>>>(plane, w, h, wp, out); break;
+        case 4: phase_planes_kernel<4><<<grid, 128, 0, st>>>(plane, w, h, wp, out); break;
+        case 8: phase_planes_kernel<8><<<grid, 128, 0, st>>>(plane, w, h, wp, out); break;
+        case 16: phase_planes_kernel<16><<<grid, 128, 0, st>>>(plane, w, h, wp, out); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
