@@ -312,12 +312,16 @@ REFINE_SEEDS = tuple(range(1, 9))
 REFINE_LAMBDAS = (50.0, 100.0, 200.0, 400.0, 800.0)
 REFINE_STEPS = 20
 REFINE_DECODE_ITERS = 12
+REFINE_DOMAIN_PASSES = 5
 
 
-def run_refine(mb, ctx, stream, dev, peaks, seeds=REFINE_SEEDS, lambdas=REFINE_LAMBDAS):
+def run_refine(mb, ctx, stream, dev, peaks, seeds=REFINE_SEEDS, lambdas=REFINE_LAMBDAS,
+               domain_passes=REFINE_DOMAIN_PASSES):
     """Attractor refinement at 512x512: per seed 1-8 and lambda 50..800, the GPU RD encode
-    (modes 0-3, block sizes 32..4, domain stride 2) and its refinement (20 steps); PSNR-Y of
-    the exact 12-iteration decodes against the bytes of the .mars streams.  The gain is the
+    (modes 0-3, block sizes 32..4, domain stride 2), the domain re-search against the
+    attractor (`domain_passes` passes of mars_refine_domains) and the (s, o) refinement of the
+    result (20 steps); PSNR-Y of the exact 12-iteration decodes against the bytes of the
+    .mars streams.  `domain_only_bd_psnr_db` is the gain of the re-search alone.  The gain is the
     BD-PSNR of the refined curve over the plain one per seed (PCHIP in log bpp over the
     overlap, the reference's mars-bench BD contract: 5 points per curve), averaged over
     seeds; the per-lambda gains at the same lambda are listed beside it (the byte counts of
@@ -329,11 +333,11 @@ def run_refine(mb, ctx, stream, dev, peaks, seeds=REFINE_SEEDS, lambdas=REFINE_L
         mse = np.mean((a.astype(np.float64) - b.astype(np.float64)) ** 2)
         return 10.0 * np.log10(255.0 ** 2 / mse)
 
-    per_seed, gains, enc_t, ref_t, accepted = [], {l: [] for l in lambdas}, [], [], 0
-    bytes_ratio = []
+    per_seed, gains, enc_t, ref_t, dom_t, accepted = [], {l: [] for l in lambdas}, [], [], [], 0
+    bytes_ratio, dom_bd = [], []
     for seed in seeds:
         img = synthetic.gray(W, H, seed)
-        plain, refined = [], []
+        plain, refined, domain_only = [], [], []
         for lam in lambdas:
             params = mb.make_params(min_size=4, max_size=32, shift=SHIFT, lam=lam)
             t0 = time.perf_counter()
@@ -341,16 +345,25 @@ def run_refine(mb, ctx, stream, dev, peaks, seeds=REFINE_SEEDS, lambdas=REFINE_L
             enc_t.append(time.perf_counter() - t0)
             b0 = len(mb.format_write(hdr, leaves, res))
             t0 = time.perf_counter()
-            plan = ctx.refine_plan(hdr, leaves, img, res)
+            start = leaves
+            if domain_passes:
+                start, _ = ctx.refine_domains(params, hdr, leaves, img, res,
+                                              passes=domain_passes,
+                                              decode_iterations=REFINE_DECODE_ITERS)
+            dom_t.append(time.perf_counter() - t0)
+            plan = ctx.refine_plan(hdr, start, img, res)
             out, rep = plan.run(steps=REFINE_STEPS, lr=1.0, decode_iterations=REFINE_DECODE_ITERS)
             ref_t.append(time.perf_counter() - t0)
             plan.close()
-            accepted += rep.accepted
+            accepted += int(rep.accepted or any(start != leaves))
             b1 = len(mb.format_write(hdr, out, res))
+            bd_ = len(mb.format_write(hdr, start, res))
             p0 = psnr(ctx.decode(hdr, leaves, REFINE_DECODE_ITERS, res), img)
             p1 = psnr(ctx.decode(hdr, out, REFINE_DECODE_ITERS, res), img)
+            pd = psnr(ctx.decode(hdr, start, REFINE_DECODE_ITERS, res), img)
             plain.append((rd.bpp(b0, W, H), p0))
             refined.append((rd.bpp(b1, W, H), p1))
+            domain_only.append((rd.bpp(bd_, W, H), pd))
             gains[lam].append(p1 - p0)
             bytes_ratio.append(b1 / b0)
         if len(lambdas) >= rd.MIN_POINTS_PER_CURVE:
@@ -358,6 +371,8 @@ def run_refine(mb, ctx, stream, dev, peaks, seeds=REFINE_SEEDS, lambdas=REFINE_L
             per_seed.append({"seed": seed, "bd_psnr_db": r.bd_psnr_db,
                              "bd_rate_pct": r.bd_rate_pct, "bpp_interval": r.bd_psnr_bpp_interval,
                              "plain": plain, "refined": refined})
+            if domain_passes:
+                dom_bd.append(rd.bd_metrics(plain, domain_only, ("plain", "domains")).bd_psnr_db)
     # BD metrics need at least 4 points per curve; shorter sweeps report per-lambda gains only.
     bd = float(np.mean([p["bd_psnr_db"] for p in per_seed])) if per_seed else None
 
@@ -381,9 +396,13 @@ def run_refine(mb, ctx, stream, dev, peaks, seeds=REFINE_SEEDS, lambdas=REFINE_L
     return {
         "workload": "attractor refinement of the GPU RD encode, 512x512 synthetic gray, seeds "
                     "1-8, lambda 50/100/200/400/800, modes 0-3, sizes 32..4, domain stride 2; "
-                    f"{REFINE_STEPS} steps, exact decodes of {REFINE_DECODE_ITERS} iterations",
+                    f"{domain_passes} domain re-search passes, then {REFINE_STEPS} (s, o) steps; "
+                    f"exact decodes of {REFINE_DECODE_ITERS} iterations",
         "metric": "PSNR-Y gain at equal bytes (BD-PSNR, refined vs plain GPU search)",
         "value": bd, "unit": "dB", "higher_is_better": True,
+        "domain_passes": domain_passes,
+        "domain_only_bd_psnr_db": float(np.mean(dom_bd)) if dom_bd else None,
+        "ms_per_domain_refine": 1e3 * float(np.median(dom_t)),
         "per_lambda_gain_db": {str(int(l)): float(np.mean(g)) for l, g in gains.items()},
         "bytes_ratio_refined_over_plain": [float(min(bytes_ratio)), float(max(bytes_ratio))],
         "accepted": f"{accepted}/{len(seeds) * len(lambdas)}",
@@ -863,6 +882,8 @@ def main():
                          "--refine-lambdas, and print its JSON object")
     ap.add_argument("--refine-seeds", default=",".join(map(str, REFINE_SEEDS)))
     ap.add_argument("--refine-lambdas", default=",".join(str(int(l)) for l in REFINE_LAMBDAS))
+    ap.add_argument("--refine-domain-passes", type=int, default=REFINE_DOMAIN_PASSES,
+                    help="passes of the domain re-search before the (s, o) refinement")
     ap.add_argument("--decode-only", type=int, default=0, metavar="SIDE",
                     help="run only the decode leg on a SIDE x SIDE synthetic map (for "
                          "profiling) and print its JSON object")
@@ -914,7 +935,8 @@ def main():
         ctx.set_stream(stream.cuda_stream)
         out = run_refine(mb, ctx, stream, dev, {},
                          tuple(int(x) for x in args.refine_seeds.split(",")),
-                         tuple(float(x) for x in args.refine_lambdas.split(",")))
+                         tuple(float(x) for x in args.refine_lambdas.split(",")),
+                         args.refine_domain_passes)
         print(json.dumps({"refine": out}), flush=True)
         ctx.close()
         return 0

@@ -229,6 +229,17 @@ int mars_search_nodes_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t wid
                              uint32_t height, const mars_params* params, mars_candidate* d_out,
                              size_t capacity, size_t* n_nodes, uint64_t* total_evals);
 
+/* mars_search_blocks_device with the range blocks read from one device plane and the domain
+ * pool from another of the same size (both width*height u8): the attractor re-search of
+ * mars_refine_domains, whose domain plane is a decode of the code being refined.  No
+ * reference counterpart (the reference searches one plane); the per-range result is
+ * mars_search_blocks_device's over the domain plane's pool, the same on identical planes. */
+int mars_search_blocks_cross_device(mars_ctx* ctx, const uint8_t* d_range_plane,
+                                    const uint8_t* d_domain_plane, uint32_t width,
+                                    uint32_t height, uint32_t size, uint32_t shift,
+                                    const mars_params* params, const uint32_t* d_rows,
+                                    const uint32_t* d_cols, size_t n, mars_candidate* d_out);
+
 /* The level search of mars_search_blocks_device for callers that cannot allocate device
  * memory -- real-time pipelines that forbid allocation once they are running, plug-ins
  * whose host application owns every device allocation, hosts with a fixed device-memory
@@ -338,6 +349,23 @@ int mars_refine_backward(mars_refine_plan* plan, uint32_t max_iters, double tol,
 int mars_refine_run(mars_refine_plan* plan, uint32_t steps, float lr, uint32_t decode_iterations,
                     mars_leaf* out_leaves, mars_refine_report* report);
 void mars_refine_plan_free(mars_refine_plan* plan);
+
+/* Domain re-search against the attractor (local iterative improvement of the domain choices):
+ * `passes` rounds, each decoding the current list exactly (`decode_iterations` steps) and
+ * searching every mode-2 leaf again (mars_search_blocks_cross_device: range block from
+ * `target`, domain pool from the decoded plane, stride header->shift, the fit of `params`).
+ * A round's new (domain, isometry, qalfa, qbeta) replace the old where the candidate is
+ * valid with qalfa >= 1; the round is kept when the exact decode's squared error falls,
+ * else with only the leaves whose own pixels decode better, if that lowers it; otherwise
+ * the rounds stop.  Geometry, modes and the mode-3 residuals are unchanged.  out_leaves
+ * holds n leaves; report: loss_start / loss_end = the decodes' squared error, psnr_plain /
+ * psnr_refined their PSNR, steps = rounds run, improving_steps = rounds kept,
+ * changed_leaves = leaves that differ from the input, accepted = any round kept. */
+int mars_refine_domains(mars_ctx* ctx, const mars_params* params, const mars_header* header,
+                        const mars_leaf* leaves, size_t n, const int32_t* residuals,
+                        size_t nresiduals, const uint8_t* target, uint32_t passes,
+                        uint32_t decode_iterations, mars_leaf* out_leaves,
+                        mars_refine_report* report);
 
 /* Colour input of the codec and its metric, on device planes, asynchronous on the context's
  * stream except mars_mse_device:

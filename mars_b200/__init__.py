@@ -100,6 +100,7 @@ EXPORTS = (
     "mars_zoom_leaves", "mars_encode_planned",
     "mars_refine_plan_create", "mars_refine_params", "mars_refine_forward",
     "mars_refine_backward", "mars_refine_run", "mars_refine_plan_free",
+    "mars_search_blocks_cross_device", "mars_refine_domains",
 )
 
 _lib = None
@@ -187,6 +188,10 @@ def lib():
     L.mars_refine_forward.argtypes = [vp, vp, vp, u32, C.c_double, vp, dp, P(u32)]
     L.mars_refine_backward.argtypes = [vp, u32, C.c_double, vp, vp, P(u32), dp]
     L.mars_refine_run.argtypes = [vp, u32, C.c_float, u32, vp, P(RefineReport)]
+    L.mars_search_blocks_cross_device.argtypes = [vp, vp, vp, u32, u32, u32, u32, P(Params),
+                                                  vp, vp, sz, vp]
+    L.mars_refine_domains.argtypes = [vp, P(Params), P(Header), vp, sz, vp, sz, vp, u32, u32,
+                                      vp, P(RefineReport)]
     L.mars_refine_plan_free.argtypes = [vp]
     L.mars_refine_plan_free.restype = None
     L.mars_entropy_encode.argtypes = [vp, sz, P(vp), P(sz)]
@@ -517,6 +522,24 @@ class Context:
                                             len(leaves), res.ctypes.data, len(res),
                                             t.ctypes.data, C.byref(h)))
         return RefinePlan(h.value, leaves, hdr)
+
+    def refine_domains(self, params: Params, hdr: Header, leaves: np.ndarray, target,
+                       residuals=None, passes: int = 3, decode_iterations: int = 12):
+        """mars_refine_domains: -> (leaves, RefineReport).  Every mode-2 leaf is searched
+        again with its range block from `target` and the domain pool from the decode of the
+        current list; a pass is kept only when the exact decode improves."""
+        leaves = np.ascontiguousarray(leaves, dtype=LEAF_DTYPE)
+        res = _residuals(residuals)
+        t = np.ascontiguousarray(target, dtype=np.uint8)
+        if t.shape != (hdr.height, hdr.width):
+            raise ValueError("the target must be a (height, width) plane")
+        out = np.zeros(len(leaves), LEAF_DTYPE)
+        rep = RefineReport()
+        check(lib().mars_refine_domains(self._h, C.byref(params), C.byref(hdr),
+                                        leaves.ctypes.data, len(leaves), res.ctypes.data,
+                                        len(res), t.ctypes.data, passes, decode_iterations,
+                                        out.ctypes.data, C.byref(rep)))
+        return out, rep
 
     def decode_until_stable(self, hdr: Header, leaves: np.ndarray, threshold: int,
                             max_iterations: int, residuals=None):

@@ -275,7 +275,7 @@ bool make_digit_maps(mars_ctx* ctx, const uint8_t* d_digits, uint32_t w, uint32_
 int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t* d_D,
                  uint32_t w, uint32_t h, const mars::LevelGeom& g, const mars::FitParams& fp,
                  const uint32_t* d_rows, const uint32_t* d_cols, size_t n, mars::RangeStats rs,
-                 mars::DomainStats ds, mars::CandidateOut* d_out) {
+                 mars::DomainStats ds, mars::CandidateOut* d_out, const uint8_t* d_dplane) {
     const cudaStream_t st = ctx->stream;
     uint8_t* d_phases = nullptr;
     uint8_t* d_b = nullptr;
@@ -299,7 +299,7 @@ int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32
     if (digits)
         MARS_CUDA(mars::tc::launch_digit_planes(d_D, (int)w, (int)h, g.shift, d_phases, st));
     else
-        MARS_CUDA(mars::tc::launch_phase_planes(d_plane, (int)w, (int)h, g.shift, d_phases, st));
+        MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, g.shift, d_phases, st));
     MARS_CUDA(mars::tc::launch_build_b(g.size, d_plane, (int)w, (int)h, d_rows, d_cols, (int)n,
                                        d_b, digits, st));
     MARS_CUDA(mars::tc::launch_seed(d_D, g, d_plane, (int)w, d_rows, d_cols, (int)n, rs, ds, fp,
@@ -313,10 +313,13 @@ int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32
 
 // Search every block of one (size, shift) level.  rows/cols/out are device pointers.
 // k > 1: the ranked search (n x k results); k == 1: the single winner.
+// One level of the search: ranges are read from d_plane; domains from d_D (the contracted
+// domain plane) and, on the tensor-core path, from the pixel plane d_dplane (d_plane when
+// null).  The two planes differ only for the attractor re-search of mars_refine_domains.
 int run_level(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t* d_D,
               uint32_t w, uint32_t h, uint32_t size, uint32_t shift, const mars::FitParams& fp,
               const uint32_t* d_rows, const uint32_t* d_cols, size_t n,
-              mars::CandidateOut* d_out, uint32_t k = 1) {
+              mars::CandidateOut* d_out, uint32_t k = 1, const uint8_t* d_dplane = nullptr) {
     if (n == 0) return MARS_OK;
     const cudaStream_t st = ctx->stream;
     const mars::LevelGeom g = level_geom(w, h, size, shift);
@@ -352,7 +355,8 @@ int run_level(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t*
         return MARS_OK;
     }
     if (use_tc(ctx, size, shift))
-        return run_level_tc(ctx, sc, d_plane, d_D, w, h, g, fp, d_rows, d_cols, n, rs, ds, d_out);
+        return run_level_tc(ctx, sc, d_plane, d_D, w, h, g, fp, d_rows, d_cols, n, rs, ds, d_out,
+                            d_dplane ? d_dplane : d_plane);
     const int nsplit = mars::search_simt_splits(g, (int)n, ctx->num_sms);
     mars::Partial* partials;
     MARS_CUDA(sc.get(&partials, (size_t)nsplit * n));
@@ -911,6 +915,29 @@ int mars_search_blocks_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t wi
     ctx->launches += 1;
     return run_level(ctx, sc, d_plane, d_D, width, height, size, shift, fp, d_rows, d_cols, n,
                      (mars::CandidateOut*)d_out);
+}
+
+int mars_search_blocks_cross_device(mars_ctx* ctx, const uint8_t* d_range_plane,
+                                    const uint8_t* d_domain_plane, uint32_t width,
+                                    uint32_t height, uint32_t size, uint32_t shift,
+                                    const mars_params* params, const uint32_t* d_rows,
+                                    const uint32_t* d_cols, size_t n, mars_candidate* d_out) {
+    if (!ctx || !d_range_plane || !d_domain_plane || (n && (!d_rows || !d_cols || !d_out)))
+        return fail(MARS_EINVAL, "NULL argument");
+    if (int e = check_params(params)) return e;
+    if (!is_pow2(size) || size < 2 || size > 64)
+        return fail(size > 64 ? MARS_EUNSUPPORTED : MARS_EINVAL, "size must be a power of two in 2..64");
+    if (shift == 0 || (shift & 1)) return fail(MARS_EUNSUPPORTED, "shift must be even");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    MARS_CUDA(cudaSetDevice(ctx->device));
+    const mars::FitParams fp = make_fit_params(*params);
+    Scratch sc(ctx->stream);
+    int32_t* d_D = nullptr;
+    MARS_CUDA(sc.get(&d_D, (size_t)(width / 2) * (height / 2)));
+    MARS_CUDA(mars::launch_contract(d_domain_plane, (int)width, (int)height, d_D, ctx->stream));
+    ctx->launches += 1;
+    return run_level(ctx, sc, d_range_plane, d_D, width, height, size, shift, fp, d_rows, d_cols,
+                     n, (mars::CandidateOut*)d_out, 1, d_domain_plane);
 }
 
 int mars_search_nodes_device(mars_ctx* ctx, const uint8_t* d_plane, uint32_t width,
@@ -2279,3 +2306,160 @@ int mars_ifs_write(const mars_header* header, const mars_leaf* leaves, size_t n,
 namespace mars {
 int ctx_sync(mars_ctx* ctx) { return sync_bounded(ctx); }
 }  // namespace mars
+
+extern "C" {
+
+// Local iterative improvement of the domain choices (the decoder-side re-search of
+// Hamzaoui, Hartenstein and Saupe's local iterative improvement of fractal codes): each pass
+// decodes the current list, searches every mode-2 leaf again with its range block taken
+// from the target and the domain pool from the decoded plane, and keeps the pass when the
+// exact decode improves (else the leaves whose own pixels improved, if that improves it).
+int mars_refine_domains(mars_ctx* ctx, const mars_params* params, const mars_header* hdr,
+                        const mars_leaf* leaves, size_t n, const int32_t* residuals,
+                        size_t nresiduals, const uint8_t* target, uint32_t passes,
+                        uint32_t decode_iterations, mars_leaf* out_leaves,
+                        mars_refine_report* report) {
+    if (!ctx || !params || !hdr || !target || !report || (n && (!leaves || !out_leaves)))
+        return fail(MARS_EINVAL, "NULL argument");
+    if (int e = check_params(params)) return e;
+    const uint32_t w = hdr->width, h = hdr->height;
+    if (w == 0 || h == 0 || w > 65535 || h > 65535)
+        return fail(MARS_EINVAL, "plane dimensions must be in 1..65535");
+    if (hdr->shift == 0 || (hdr->shift & 1)) return fail(MARS_EUNSUPPORTED, "shift must be even");
+    for (size_t k = 0; k < n; ++k) {
+        const mars_leaf& L = leaves[k];
+        if (L.size == 0 || L.row + L.size > h || L.col + L.size > w)
+            return fail(MARS_EINVAL, "leaf " + std::to_string(k) + " is outside the plane");
+    }
+    std::memset(report, 0, sizeof *report);
+    const size_t npx = (size_t)w * h;
+    std::vector<mars_leaf> cur(leaves, leaves + n), trial;
+    std::vector<uint8_t> x(npx), y(npx);
+    auto decode = [&](const std::vector<mars_leaf>& ls, std::vector<uint8_t>* img) {
+        return mars_decode(ctx, hdr, ls.data(), n, residuals, nresiduals, decode_iterations,
+                           img->data());
+    };
+    auto sse_of = [&](const std::vector<uint8_t>& img) {
+        double acc = 0.0;
+        for (size_t q = 0; q < npx; ++q) {
+            const double d = (double)img[q] - (double)target[q];
+            acc += d * d;
+        }
+        return acc;
+    };
+    auto psnr_of = [&](double sse) {
+        return sse > 0.0 ? 10.0 * std::log10(255.0 * 255.0 * (double)npx / sse) : INFINITY;
+    };
+    if (int e = decode(cur, &x)) return e;
+    double sse = sse_of(x);
+    report->loss_start = sse;
+    report->psnr_plain = psnr_of(sse);
+
+    // The mode-2 leaves by size, the order their candidates come back in.
+    std::vector<size_t> order;
+    std::vector<std::pair<uint32_t, size_t>> levels;  // (size, count)
+    for (uint32_t size = 64; size >= 2; size /= 2) {
+        const size_t before = order.size();
+        for (size_t k = 0; k < n; ++k) {
+            const mars_leaf& L = cur[k];
+            if (L.mode == 2 && L.size == size && 2 * size <= w && 2 * size <= h) order.push_back(k);
+        }
+        if (order.size() > before) levels.push_back({size, order.size() - before});
+    }
+    std::vector<int32_t> owner(npx, -1);
+    for (size_t k = 0; k < n; ++k)
+        for (uint32_t r = 0; r < cur[k].size; ++r)
+            std::fill_n(owner.begin() + (long)((size_t)(cur[k].row + r) * w + cur[k].col),
+                        cur[k].size, (int32_t)k);
+    std::vector<uint32_t> rc(2 * order.size());
+    for (size_t i = 0; i < order.size(); ++i) {
+        rc[i] = cur[order[i]].row;
+        rc[order.size() + i] = cur[order[i]].col;
+    }
+    std::vector<mars::CandidateOut> cand(order.size());
+    const mars::FitParams fp = make_fit_params(*params);
+
+    for (uint32_t pass = 0; pass < passes && !order.empty(); ++pass) {
+        report->steps += 1;
+        {
+            std::lock_guard<std::mutex> lock(ctx->mu);
+            MARS_CUDA(cudaSetDevice(ctx->device));
+            const cudaStream_t st = ctx->stream;
+            Scratch sc(st);
+            uint8_t *d_t = nullptr, *d_x = nullptr;
+            int32_t* d_D = nullptr;
+            uint32_t* d_rc = nullptr;
+            mars::CandidateOut* d_out = nullptr;
+            MARS_CUDA(sc.get(&d_t, npx));
+            MARS_CUDA(sc.get(&d_x, npx));
+            MARS_CUDA(sc.get(&d_D, std::max<size_t>(1, (size_t)(w / 2) * (h / 2))));
+            MARS_CUDA(sc.get(&d_rc, rc.size()));
+            MARS_CUDA(sc.get(&d_out, cand.size()));
+            MARS_CUDA(cudaMemcpyAsync(d_t, target, npx, cudaMemcpyHostToDevice, st));
+            MARS_CUDA(cudaMemcpyAsync(d_x, x.data(), npx, cudaMemcpyHostToDevice, st));
+            MARS_CUDA(cudaMemcpyAsync(d_rc, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice, st));
+            MARS_CUDA(mars::launch_contract(d_x, (int)w, (int)h, d_D, st));
+            ctx->launches += 1;
+            size_t off = 0;
+            for (const auto& lv : levels) {
+                const int e = run_level(ctx, sc, d_t, d_D, w, h, lv.first, hdr->shift, fp,
+                                        d_rc + off, d_rc + order.size() + off, lv.second,
+                                        d_out + off, 1, d_x);
+                if (e) return e;
+                off += lv.second;
+            }
+            MARS_CUDA(cudaMemcpyAsync(cand.data(), d_out, cand.size() * sizeof(mars::CandidateOut),
+                                      cudaMemcpyDeviceToHost, st));
+            if (int e = sync_bounded(ctx)) return e;
+        }
+        trial = cur;
+        size_t changed = 0;
+        for (size_t i = 0; i < order.size(); ++i) {
+            const mars::CandidateOut& c = cand[i];
+            mars_leaf& L = trial[order[i]];
+            if (!c.valid || c.qalfa < 1) continue;
+            if (c.dom_row == L.dom_row && c.dom_col == L.dom_col && c.isometry == L.isometry &&
+                c.qalfa == L.qalfa && c.qbeta == L.qbeta)
+                continue;
+            L.dom_row = c.dom_row;
+            L.dom_col = c.dom_col;
+            L.isometry = c.isometry;
+            L.qalfa = c.qalfa;
+            L.qbeta = c.qbeta;
+            ++changed;
+        }
+        if (!changed) break;
+        if (int e = decode(trial, &y)) return e;
+        double sse_y = sse_of(y);
+        if (!(sse_y < sse)) {
+            // Keep the re-searched leaves whose own pixels decode better.
+            std::vector<double> before(n, 0.0), after(n, 0.0);
+            for (size_t q = 0; q < npx; ++q) {
+                if (owner[q] < 0) continue;
+                const double t = target[q];
+                before[owner[q]] += ((double)x[q] - t) * ((double)x[q] - t);
+                after[owner[q]] += ((double)y[q] - t) * ((double)y[q] - t);
+            }
+            for (size_t k = 0; k < n; ++k)
+                if (after[k] >= before[k]) trial[k] = cur[k];
+            if (int e = decode(trial, &y)) return e;
+            sse_y = sse_of(y);
+            if (!(sse_y < sse)) break;
+        }
+        cur.swap(trial);
+        x.swap(y);
+        sse = sse_y;
+        report->improving_steps += 1;
+    }
+    report->loss_end = sse;
+    report->psnr_refined = psnr_of(sse);
+    report->accepted = report->improving_steps > 0 ? 1u : 0u;
+    uint32_t changed = 0;
+    for (size_t k = 0; k < n; ++k)
+        changed += std::memcmp(&cur[k], &leaves[k], sizeof(mars_leaf)) != 0 ? 1u : 0u;
+    report->changed_leaves = changed;
+    std::copy(cur.begin(), cur.end(), out_leaves);
+    return MARS_OK;
+}
+
+}  // extern "C"

@@ -172,14 +172,22 @@ def best_beta(range_sum: int, pixel_count: int, bits_beta: int = 7) -> int:
     return lib().orc_best_beta(range_sum, pixel_count, bits_beta)
 
 
-def search(img, row, col, size, shift, params: Params, k=1):
-    """search_top_k for one block: (candidates structured array, evals)."""
+def search(img, row, col, size, shift, params: Params, k=1, contracted=None):
+    """search_top_k for one block: (candidates structured array, evals).  `contracted` (the
+    (h/2, w/2) int32 contraction of another plane of the same size) replaces the domain pool
+    of `img`'s own contraction: ranges from `img`, domains from that plane."""
     a = _u8(img)
     h, w = a.shape
+    cd = None
+    if contracted is not None:
+        cd = np.ascontiguousarray(contracted, dtype=np.int32)
+        if cd.shape != (h // 2, w // 2):
+            raise ValueError("the contracted plane must be (h/2, w/2)")
     out = np.zeros(k, dtype=CANDIDATE_DTYPE)
     n, ev = C.c_uint32(), C.c_uint64()
-    rc = lib().orc_search(a.ctypes.data, w, h, None, row, col, size, shift, C.byref(params), k,
-                          out.ctypes.data, C.byref(n), C.byref(ev))
+    rc = lib().orc_search(a.ctypes.data, w, h, None if cd is None else cd.ctypes.data, row, col,
+                          size, shift, C.byref(params), k, out.ctypes.data, C.byref(n),
+                          C.byref(ev))
     if rc:
         raise ValueError(f"orc_search failed: {rc}")
     return out[: n.value], ev.value

@@ -116,3 +116,112 @@ def test_refinement_loop_end_to_end(ctx, side, seed):
     h2, l2, r2 = mb.format_read(mb.format_write(hdr, out, res))
     assert np.array_equal(l2, out) and np.array_equal(r2, res)
     plan.close()
+
+
+# ---- the domain re-search against the attractor (mars_refine_domains) and the two-plane
+# search under it (mars_search_blocks_cross_device)
+
+def _cross_planes(w, h, seed):
+    """A target plane and a second plane of the same size standing in for its decode: the
+    target with seeded noise and a small shift, so the two pools differ everywhere."""
+    t = synthetic.gray(w, h, seed)
+    rng = np.random.default_rng(seed)
+    x = np.roll(t.astype(np.int32), 1, axis=1) + rng.integers(-9, 10, size=t.shape)
+    return t, np.clip(x, 0, 255).astype(np.uint8)
+
+
+def _cross_device(ctx, t, x, size, shift, p, rows, cols):
+    import torch
+    h, w = t.shape
+    d_t = torch.from_numpy(t).cuda()
+    d_x = torch.from_numpy(x).cuda()
+    d_r = torch.from_numpy(np.asarray(rows, np.int32)).cuda()
+    d_c = torch.from_numpy(np.asarray(cols, np.int32)).cuda()
+    out = torch.zeros((len(rows), mb.CANDIDATE_DTYPE.itemsize), dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    mb.check(mb.lib().mars_search_blocks_cross_device(ctx.handle, d_t.data_ptr(), d_x.data_ptr(),
+                                                      w, h, size, shift, mb.C.byref(p),
+                                                      d_r.data_ptr(), d_c.data_ptr(), len(rows),
+                                                      out.data_ptr()))
+    torch.cuda.synchronize()
+    return out.cpu().numpy().view(mb.CANDIDATE_DTYPE).ravel()
+
+
+@pytest.mark.parametrize("path", ["auto", "simt"])
+@pytest.mark.parametrize("size,shift", [(4, 2), (8, 4), (16, 2), (32, 4)])
+def test_cross_search_matches_the_oracle(ctx, path, size, shift):
+    # Ranges from one plane, domains from another: every aligned block against the oracle's
+    # search_top_k over the second plane's contraction, record for record (moments included).
+    w, h = 96, 80
+    t, x = _cross_planes(w, h, 7 + size)
+    rows, cols = np.meshgrid(np.arange(h // size) * size, np.arange(w // size) * size,
+                             indexing="ij")
+    rows, cols = rows.ravel(), cols.ravel()
+    ctx.set_search_path(path)
+    try:
+        got = _cross_device(ctx, t, x, size, shift, mb.make_params(shift=shift), rows, cols)
+    finally:
+        ctx.set_search_path("auto")
+    cx = orc.contract(x)
+    op = orc.make_params(shift=shift)
+    for i, (r, c) in enumerate(zip(rows, cols)):
+        o, _ = orc.search(t, int(r), int(c), size, shift, op, contracted=cx)
+        assert got[i].tobytes() == o[0].tobytes(), (i, r, c)
+
+
+def test_cross_search_on_one_plane_is_the_search(ctx):
+    import torch
+    img = synthetic.gray(128, 128, 4)
+    rows = np.array([0, 8, 64, 120], np.int32)
+    cols = np.array([0, 16, 40, 120], np.int32)
+    p = mb.make_params(shift=2)
+    got = _cross_device(ctx, img, img, 8, 2, p, rows, cols)
+    d_img = torch.from_numpy(img).cuda()
+    d_r, d_c = torch.from_numpy(rows).cuda(), torch.from_numpy(cols).cuda()
+    out = torch.zeros((4, mb.CANDIDATE_DTYPE.itemsize), dtype=torch.uint8, device="cuda")
+    mb.check(mb.lib().mars_search_blocks_device(ctx.handle, d_img.data_ptr(), 128, 128, 8, 2,
+                                                mb.C.byref(p), d_r.data_ptr(), d_c.data_ptr(),
+                                                4, out.data_ptr()))
+    torch.cuda.synchronize()
+    assert got.tobytes() == out.cpu().numpy().tobytes()
+
+
+@pytest.mark.parametrize("seed,lam", [(1, 100.0), (3, 400.0)])
+def test_domain_refinement_end_to_end(ctx, seed, lam):
+    # Only mode-2 leaves move, to valid domains of the header's grid with qalfa >= 1; the
+    # result decodes to the reported PSNR, never below the input's, and stays a valid stream.
+    side = 128
+    img = synthetic.gray(side, side, seed)
+    p = mb.make_params(min_size=4, max_size=32, shift=2, lam=lam)
+    hdr, leaves, res, _ = ctx.encode(img, p, allowed_modes=(1, 1, 1, 1))
+    out, rep = ctx.refine_domains(p, hdr, leaves, img, res, passes=3, decode_iterations=12)
+    for f in ("row", "col", "size", "mode", "qgx", "qgy"):
+        assert np.array_equal(out[f], leaves[f]), f
+    fixed = leaves["mode"] != 2
+    assert out[fixed].tobytes() == leaves[fixed].tobytes()
+    moved = out[~fixed]
+    assert np.all(moved["qalfa"] >= 1) and np.all(moved["isometry"] < 8)
+    assert np.all(moved["dom_row"] % hdr.shift == 0) and np.all(moved["dom_col"] % hdr.shift == 0)
+    assert np.all(moved["dom_row"] + 2 * moved["size"] <= side)
+    assert np.all(moved["dom_col"] + 2 * moved["size"] <= side)
+    p0 = _psnr(ctx.decode(hdr, leaves, 12, res), img)
+    p1 = _psnr(ctx.decode(hdr, out, 12, res), img)
+    assert rep.psnr_plain == pytest.approx(p0, abs=1e-9)
+    assert rep.psnr_refined == pytest.approx(p1, abs=1e-9)
+    assert p1 >= p0
+    assert rep.changed_leaves == int(np.sum(np.any(
+        out.view(np.uint8).reshape(len(out), -1) != leaves.view(np.uint8).reshape(len(out), -1),
+        axis=1)))
+    assert bool(rep.accepted) == (rep.changed_leaves > 0)
+    data = mb.format_write(hdr, out, res)
+    h2, l2, r2 = mb.format_read(data)
+    assert l2.tobytes() == out.tobytes() and np.array_equal(r2, res)
+
+
+def test_domain_refinement_with_no_pass_returns_the_input(ctx):
+    img = synthetic.gray(64, 64, 2)
+    p = mb.make_params(min_size=4, max_size=16, shift=2, lam=200.0)
+    hdr, leaves, res, _ = ctx.encode(img, p, allowed_modes=(1, 0, 1, 0))
+    out, rep = ctx.refine_domains(p, hdr, leaves, img, res, passes=0)
+    assert out.tobytes() == leaves.tobytes()
+    assert rep.steps == 0 and rep.accepted == 0 and rep.changed_leaves == 0

@@ -93,3 +93,20 @@ def test_adjoint_without_domains_is_the_plain_residual():
         blk = img[L["row"]:L["row"] + 8, L["col"]:L["col"] + 8].astype(np.float64)
         assert go[k] == pytest.approx(np.sum(2 * (o[k] - blk)), rel=1e-12)
     assert np.all(gs == 0)
+
+
+def test_oracle_search_takes_a_foreign_domain_pool():
+    # The cross-plane oracle of the attractor re-search: the plane's own contraction passed
+    # in gives the plain search; another plane's contraction gives that plane's domains.
+    import numpy as np
+    from mars_b200 import synthetic
+    from oracle import oracle as orc
+    t = synthetic.gray(48, 48, 5)
+    x = synthetic.gray(48, 48, 6)
+    p = orc.make_params(shift=2)
+    for r, c in [(0, 0), (8, 24), (40, 40)]:
+        a, ea = orc.search(t, r, c, 8, 2, p)
+        b, eb = orc.search(t, r, c, 8, 2, p, contracted=orc.contract(t))
+        assert a.tobytes() == b.tobytes() and ea == eb
+        d, _ = orc.search(t, r, c, 8, 2, p, contracted=orc.contract(x))
+        assert d[0]["t0"] == a[0]["t0"] and d[0]["t2"] == a[0]["t2"]  # the same range block
