@@ -112,8 +112,9 @@ __global__ void fisher_fill_kernel(const uint8_t* __restrict__ key, int n,
 // ranges): warp `sub` of a range takes the bucket candidates e = 32 sub + lane,
 // 32 sub + lane + 32 wpr, ...; with wpr > 1 each warp leaves its first minimum in `part`
 // and fisher_merge_kernel picks the range's (rms, bucket index) minimum.  Shared memory per
-// warp: the 8 permuted copies of the range (permute_range, encode.rs:833-842:
-// range_k[u*s + v] = range[map(k, u, v)]).
+// range: the 8 permuted copies of the range (permute_range, encode.rs:833-842:
+// range_k[u*s + v] = range[map(k, u, v)]), built by the range's wpr warps together (wpr
+// divides kFisherWarps, so they share a CTA; named barrier 1 + warp / wpr).
 constexpr int kFisherWarps = 4;
 constexpr uint32_t kNoCandidate = 0xffffffffu;
 
@@ -133,7 +134,7 @@ __global__ void __launch_bounds__(32 * kFisherWarps) fisher_search_kernel(
     // Where this warp's answer goes: the range's output, or its slot among the partials.
     CandidateOut* const dst = wpr == 1 ? out + ri : part + (size_t)ri * wpr + sub;
     const int n = size * size, hq = size / 2;
-    uint8_t* perm = smem + (size_t)warp * 8 * n;
+    uint8_t* perm = smem + (size_t)(warp / wpr) * 8 * n;
     const uint32_t row = rows[ri], col = cols[ri];
     CandidateOut res;
     res.dom_row = res.dom_col = res.isometry = res.qalfa = res.qbeta = res.valid = 0;
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(32 * kFisherWarps) fisher_search_kernel(
         t0 += __shfl_xor_sync(0xffffffffu, t0, o);
         t2 += __shfl_xor_sync(0xffffffffu, t2, o);
     }
-    for (int e = lane; e < 8 * n; e += 32) {
+    for (int e = 32 * sub + lane; e < 8 * n; e += 32 * wpr) {
         const int k = e / n, uv = e % n, u = uv / size, v = uv % size;
         int i, j;
         switch (k) {  // isometry::map (isometry.rs:7-19)
@@ -183,7 +184,12 @@ __global__ void __launch_bounds__(32 * kFisherWarps) fisher_search_kernel(
         }
         perm[e] = plane[(size_t)(row + i) * w + col + j];
     }
-    __syncwarp();
+    // The range's warps returned above together or not at all (same ri), so the group
+    // barrier sees all 32 * wpr threads.
+    if (wpr > 1)
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + warp / wpr), "r"(32 * wpr) : "memory");
+    else
+        __syncwarp();
     int isom, key;
     fisher_classify(q, q2, hq, &isom, &key);
     const uint32_t b = ref[key];
@@ -303,7 +309,7 @@ cudaError_t launch_fisher_search(const uint8_t* plane, int w, int h, const int32
                                  CandidateOut* part, uint32_t* part_e, cudaStream_t st) {
     if (nranges <= 0) return cudaSuccess;
     const int wpr = fisher_warps_per_range(size);
-    const size_t smem = (size_t)kFisherWarps * 8 * size * size;
+    const size_t smem = (size_t)(kFisherWarps / wpr) * 8 * size * size;
     if (smem > 48 * 1024) {
         const cudaError_t e = cudaFuncSetAttribute(
             fisher_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

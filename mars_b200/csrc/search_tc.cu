@@ -97,11 +97,13 @@ struct Champ {
 // The per-range pruning record the epilogue reads for every (domain lane, range) pair,
 // branch-free form of prune_below (fit.cuh):
 //   g1 = sqrt_w * sqrt(Ndd);  tau_z = min(w2a + a_half*Ndd, max(g1, a_min*Ndd));
-//   tau = (dom > tie) ? tau_z : g1 + neg;   prune  <=>  t1' < s1_x4 * c + 4 tau / n.
-// tie = -1 puts every domain in the Z-form, INT32_MAX none; neg = 0 or -inf (W <= 0).
+//   tau = (dom > tie) ? tau_z : g1;   prune  <=>  t1' < s1_x4 * c + 4 tau / n.
+// tie = -1 puts every domain in the Z-form, INT32_MAX none.  W <= 0 is sqrt_w = -inf:
+// g1 = -inf (sqrt(Ndd) > 0), nothing pruned in the plain form, and tau_z unchanged
+// (max(-inf, a_min Ndd) = max(0, a_min Ndd)).
 struct __align__(16) ThrRec {
-    float sqrt_w, w2a, neg, c;  // sqrt_w, w2a, neg pre-scaled by 4 / n (exact: n = 4^k)
-    int32_t tie, pad0, pad1, pad2;
+    float sqrt_w, w2a, c;  // sqrt_w, w2a pre-scaled by 4 / n (exact: n = 4^k)
+    int32_t tie;
 };
 
 // A survivor waiting for its exact fit.  Survivors of several tiles are batched: the
@@ -147,20 +149,17 @@ __device__ __forceinline__ void publish_threshold(Smem& sm, int rl, const FitPar
     if (!C.valid) {
         // An invalid range never survives: in the Z-form (tie = -1) with sqrt_w = w2a =
         // +inf, tau = +inf for every domain, flat all-zero ones (s1 = 0) included.
-        t = ThrRec{INFINITY, INFINITY, 0.0f, 3.0e38f, -1, 0, 0, 0};
-        sm.thr[rl] = t;
+        sm.thr[rl] = ThrRec{INFINITY, INFINITY, 3.0e38f, -1};
         return;
     }
     const Threshold th = make_threshold(C.sum, C.rms, C.idx >> 3, C.rms0, C.nrr, n, fp);
     // Scaling by 4 / n (a power of two) is exact, so folding it in keeps every bound
     // rounded toward -inf.
     const float four_inv_n = 4.0f / (float)n;
-    t.sqrt_w = th.sqrt_w * four_inv_n;
+    t.sqrt_w = th.wpos ? th.sqrt_w * four_inv_n : -INFINITY;
     t.w2a = th.w2a * four_inv_n;
-    t.neg = th.wpos ? 0.0f : -INFINITY;
     t.c = (float)C.t0 / (float)n - 128.0f;  // exact: t0 < 2^24, n a power of four
     t.tie = th.mode == 2 ? -1 : (th.mode == 1 ? (int32_t)th.tie_dom : INT32_MAX);
-    t.pad0 = t.pad1 = t.pad2 = 0;
     sm.thr[rl] = t;
 }
 
@@ -480,31 +479,25 @@ __global__ void __launch_bounds__(kThreads, 1)
             };
             const uint32_t tag = (uint32_t)(mt & 0xFFFF);
             // Thresholds of this lane's domain against its ranges (fit.cuh, branch-free
-            // form).  They do not depend on the accumulator; each stage below runs over all
-            // of them so the independent chains overlap.
+            // form).  They do not depend on the accumulator: the 4 of 32-column chunk ch are
+            // computed while that chunk's accumulator load and the previous chunk's test are
+            // in flight, so the independent chains interleave (all 16 up front, before the
+            // scan, measured 10 % slower at s = 4 with the 32-byte record).
             int32_t thr[kRangesPerWarp];
-            auto all_thresholds = [&]() {
-                float4 ra[kRangesPerWarp];
-                int4 rb[kRangesPerWarp];
+            auto chunk_thresholds = [&](int ch) {
                 const float4* rec = reinterpret_cast<const float4*>(sm.thr);
 #pragma unroll
-                for (int r = 0; r < kRangesPerWarp; ++r) {
-                    ra[r] = rec[2 * (part * kRangesPerWarp + r)];
-                    rb[r] = reinterpret_cast<const int4*>(rec)[2 * (part * kRangesPerWarp + r) + 1];
+                for (int q = 0; q < 4; ++q) {
+                    const int r = 4 * ch + q;
+                    const float4 ra = rec[part * kRangesPerWarp + r];
+                    const int tie = __float_as_int(ra.w);
+                    // s1 * c + tau with one rounding toward -inf (fma): still never above
+                    // the exact threshold.
+                    const float g1 = __fmul_rd(ra.x, sdetf);
+                    const float tz = fminf(__fadd_rd(ra.y, ahd), fmaxf(g1, ad));
+                    const float tau = dom > tie ? tz : g1;
+                    thr[r] = dom < 0 ? INT32_MAX : __float2int_rd(__fmaf_rd(s1f, ra.z, tau));
                 }
-                // s1 * c + tau with one rounding toward -inf (fma): still never above the
-                // exact threshold.  (Branching on an all-Z-form tile measured slower than
-                // these selects.)
-                float tau[kRangesPerWarp];
-#pragma unroll
-                for (int r = 0; r < kRangesPerWarp; ++r) {
-                    const float g1 = __fmul_rd(ra[r].x, sdetf);
-                    const float tz = fminf(__fadd_rd(ra[r].y, ahd), fmaxf(g1, ad));
-                    tau[r] = dom > rb[r].x ? tz : __fadd_rd(g1, ra[r].z);
-                }
-#pragma unroll
-                for (int r = 0; r < kRangesPerWarp; ++r)
-                    thr[r] = dom < 0 ? INT32_MAX : __float2int_rd(__fmaf_rd(s1f, ra[r].w, tau[r]));
             };
             auto test_chunk = [&](const int32_t (&v)[32], int ch) {
                 const int32_t t0 = thr[ch * 4], t1 = thr[ch * 4 + 1];
@@ -536,7 +529,6 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                 }
             };
-            all_thresholds();  // overlaps the MMAs of this tile
             const bool got = mbar_wait(&sm.tfull[b], bph, abort_flag, err, 16);
             if (!epi_barrier_and(got)) break;
             tmem_fence_after();
@@ -553,6 +545,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     for (int ch = 0; ch < kChunks; ++ch) {
                         tmem_ld32(tcol + 32u * ch, va);
                         tmem_ld32(tcol + (uint32_t)NT + 32u * ch, vb);
+                        chunk_thresholds(ch);
                         tmem_wait(va);
                         tmem_wait(vb);
 #pragma unroll
@@ -562,14 +555,19 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                 } else {
                     tmem_ld32(tcol, va);
+                    chunk_thresholds(0);
                     tmem_wait(va);
 #pragma unroll
                     for (int ch = 0; ch < kChunks; ch += 2) {
                         tmem_ld32(tcol + 32u * (ch + 1), vb);
+                        chunk_thresholds(ch + 1);
                         test_chunk(va, ch);
                         __syncwarp();
                         tmem_wait(vb);
-                        if (ch + 2 < kChunks) tmem_ld32(tcol + 32u * (ch + 2), va);
+                        if (ch + 2 < kChunks) {
+                            tmem_ld32(tcol + 32u * (ch + 2), va);
+                            chunk_thresholds(ch + 2);
+                        }
                         test_chunk(vb, ch + 1);
                         __syncwarp();
                         if (ch + 2 < kChunks) tmem_wait(va);
@@ -582,8 +580,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (queued > kQueueCap) {
                     drain_queue<N, NT>(sm, kQueueCap, true, tag, et, ds, fp, exact);
                     rescan = true;
-                    all_thresholds();
-                    continue;  // pass again over the same accumulator
+                    continue;  // pass again over the same accumulator (fresh thresholds)
                 }
                 if (queued >= kFlush || (last && queued > 0))
                     drain_queue<N, NT>(sm, queued, false, tag, et, ds, fp, exact);

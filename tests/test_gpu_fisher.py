@@ -67,10 +67,16 @@ def _table_parity(ctx, img, min_size, max_size, shift, sizes):
     return checked
 
 
+@pytest.mark.parametrize("path", ["auto", "simt"])
 @pytest.mark.parametrize("shift", [2, 4])
-def test_synthetic_plane_every_node(ctx, shift):
+def test_synthetic_plane_every_node(ctx, shift, path):
+    # "simt" runs every size on the CUDA-core kernel: 1, 2 and 4 warps per range block.
     img = synthetic.gray(128, 96, 3)
-    assert _table_parity(ctx, img, 4, 32, shift, (4, 8, 16, 32)) > 0
+    ctx.set_search_path(path)
+    try:
+        assert _table_parity(ctx, img, 4, 32, shift, (4, 8, 16, 32)) > 0
+    finally:
+        ctx.set_search_path("auto")
 
 
 @pytest.mark.parametrize("name", ["mixed_129x127", "flat128", "checker8", "noise_u8", "zoneplate",
