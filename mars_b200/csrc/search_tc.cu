@@ -51,8 +51,10 @@ namespace {
 constexpr int kN = 256;                        // accumulator columns of a TMEM buffer
 constexpr int kRangesPerTile = kN / 8;         // 32: the most ranges a tile holds
 constexpr int kStageA = 16 * 1024;             // 16 row groups x 8 K-groups x 128 B
-constexpr int kQueueCap = 2048;                // survivors the queue can hold
-constexpr int kFlush = 256;                    // drain the queue once it holds this many
+constexpr int kGroups = 2;                     // independent epilogue groups of 4 warps
+constexpr int kGroupThreads = kEpiThreads / kGroups;
+constexpr int kQueueCap = 1024;                // survivors a group's queue can hold
+constexpr int kFlush = 128;                    // drain a group's queue once it holds this many
 
 // Pipeline depth of the fold path: as many A stages as fit beside the resident B tile
 // (S <= 8), otherwise three stages of A + B.
@@ -124,8 +126,7 @@ struct Smem {
     uint64_t bres;
     uint32_t tmem_base;
     int abort_flag;
-    int qcount;
-    int overflow_seen;
+    int qcount[kGroups];
     unsigned long long key_rms[kRangesPerTile];  // per-pass winner: f64 bits (rms >= 0)
     uint32_t key_idx[kRangesPerTile];
     double key_sum[kRangesPerTile];
@@ -133,8 +134,26 @@ struct Smem {
     ThrRec thr[kRangesPerTile];
     Champ ch[kRangesPerTile];
     uint32_t evaluated[kM * kN / 32];           // candidates already fitted in this tile
-    QEntry queue[kQueueCap];
+    QEntry queue[kGroups][kQueueCap];
 };
+
+// Barriers of one epilogue group (its 4 warps, one per TMEM lane quadrant): named barrier
+// 1 + group over kGroupThreads threads.
+__device__ __forceinline__ void group_barrier(int grp) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "n"(kGroupThreads) : "memory");
+}
+__device__ __forceinline__ bool group_barrier_and(int grp, bool pred) {
+    uint32_t out;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(out)
+        : "r"((uint32_t)pred), "r"(1 + grp), "n"(kGroupThreads)
+        : "memory");
+    return out != 0;
+}
 
 __device__ __forceinline__ int domain_of_lane(int m, int P, int tile_q0) {
     const int g = m >> 3, r8 = m & 7;
@@ -166,12 +185,13 @@ __device__ __forceinline__ void publish_threshold(Smem& sm, int rl, const FitPar
 // Exact fits of every queued survivor, then the per-range winners of the batch (atomic
 // min on the f64 bit pattern of rms >= 0, then on the reference index) and the champion /
 // threshold update.  All epilogue threads call this together.
-template <int N, int NT>
-__device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t tag, int et,
-                                         const DomainStats& ds, const FitParams& fp,
+template <int N, int NT, int RG>
+__device__ __noinline__ void drain_queue(Smem& sm, int grp, int n, bool mark, uint32_t tag,
+                                         int gt, const DomainStats& ds, const FitParams& fp,
                                          unsigned long long& exact) {
-    for (int qi = et; qi < n; qi += kEpiThreads) {
-        QEntry& q = sm.queue[qi];
+    QEntry* const queue = sm.queue[grp];
+    for (int qi = gt; qi < n; qi += kGroupThreads) {
+        QEntry& q = queue[qi];
         const int rl = (int)(q.code & 255u) >> 3;
         const Champ& C = sm.ch[rl];
         const int32_t s1 = ds.s1x4[q.dom];
@@ -182,16 +202,16 @@ __device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t ta
         ++exact;
         atomicMin(&sm.key_rms[rl], (unsigned long long)__double_as_longlong(f.rms));
     }
-    epi_barrier();
-    for (int qi = et; qi < n; qi += kEpiThreads) {
-        const QEntry& q = sm.queue[qi];
+    group_barrier(grp);
+    for (int qi = gt; qi < n; qi += kGroupThreads) {
+        const QEntry& q = queue[qi];
         const int col = (int)(q.code & 255u), rl = col >> 3;
         if ((unsigned long long)__double_as_longlong(q.rms) == sm.key_rms[rl])
             atomicMin(&sm.key_idx[rl], q.dom * 8u + (uint32_t)(col & 7));
     }
-    epi_barrier();
-    for (int qi = et; qi < n; qi += kEpiThreads) {
-        const QEntry& q = sm.queue[qi];
+    group_barrier(grp);
+    for (int qi = gt; qi < n; qi += kGroupThreads) {
+        const QEntry& q = queue[qi];
         const int col = (int)(q.code & 255u), rl = col >> 3;
         if ((unsigned long long)__double_as_longlong(q.rms) == sm.key_rms[rl] &&
             q.dom * 8u + (uint32_t)(col & 7) == sm.key_idx[rl]) {
@@ -205,23 +225,25 @@ __device__ __noinline__ void drain_queue(Smem& sm, int n, bool mark, uint32_t ta
             atomicOr(&sm.evaluated[(qm * NT + col) >> 5], 1u << (col & 31));
         }
     }
-    epi_barrier();
-    if (et < kRangesPerTile && sm.key_rms[et] != ~0ull) {
-        Champ& C = sm.ch[et];
-        const double r2 = __longlong_as_double((long long)sm.key_rms[et]);
-        const uint32_t i2 = sm.key_idx[et];
+    group_barrier(grp);
+    // The group's ranges: RG of them from grp * RG.
+    const int rl = grp * RG + gt;
+    if (gt < RG && sm.key_rms[rl] != ~0ull) {
+        Champ& C = sm.ch[rl];
+        const double r2 = __longlong_as_double((long long)sm.key_rms[rl]);
+        const uint32_t i2 = sm.key_idx[rl];
         if (C.valid && (r2 < C.rms || (r2 == C.rms && i2 < C.idx))) {
             C.rms = r2;
             C.idx = i2;
-            C.sum = sm.key_sum[et];
-            C.t1x4 = sm.key_t1[et];
-            publish_threshold(sm, et, fp, N);
+            C.sum = sm.key_sum[rl];
+            C.t1x4 = sm.key_t1[rl];
+            publish_threshold(sm, rl, fp, N);
         }
-        sm.key_rms[et] = ~0ull;
-        sm.key_idx[et] = UINT32_MAX;
+        sm.key_rms[rl] = ~0ull;
+        sm.key_idx[rl] = UINT32_MAX;
     }
-    if (et == 0) sm.qcount = 0;
-    epi_barrier();
+    if (gt == 0) sm.qcount[grp] = 0;
+    group_barrier(grp);
 }
 
 template <int S, bool DIG>
@@ -274,8 +296,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         mbar_init(&sm.bres, 1);
         sm.abort_flag = 0;
-        sm.qcount = 0;
-        sm.overflow_seen = 0;
+        for (int q = 0; q < kGroups; ++q) sm.qcount[q] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = threadIdx.x; i < kM * NT / 32; i += kThreads) sm.evaluated[i] = 0u;
@@ -423,9 +444,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ---------------------------------------------------------------- epilogue
         // Warps 2..: TMEM lane quadrant = warp % 4; column part (kRangesPerWarp ranges from
         // part * kRangesPerWarp) = which of the quadrant's warps.
-        const int et = threadIdx.x - 64;         // 0..kEpiThreads-1
         const int e = warp & 3;
-        const int part = (warp - 2) >> 2;
+        const int part = (warp - 2) >> 2;        // = the epilogue group
+        const int gt = threadIdx.x - 64 - part * kGroupThreads;  // 0..kGroupThreads-1
         const int m = e * 32 + lane;             // this thread's domain lane
         const float four_inv_n = 4.0f / (float)N;
         unsigned long long exact = 0;
@@ -515,7 +536,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     const int col0 = part * kColsPerWarp + ch * 32;
                     if (rescan) mask &= ~sm.evaluated[(m * NT + col0) >> 5];
-                    int slot = atomicAdd(&sm.qcount, __popc(mask));
+                    int slot = atomicAdd(&sm.qcount[part], __popc(mask));
                     while (mask) {
                         const int c = __ffs(mask) - 1;
                         mask &= mask - 1;
@@ -523,14 +544,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                         for (int q = 1; q < 32; ++q) val = c == q ? v[q] : val;
                         if (slot < kQueueCap)
-                            sm.queue[slot] = QEntry{val, (uint32_t)dom,
+                            sm.queue[part][slot] = QEntry{val, (uint32_t)dom,
                                                     (uint32_t)(tag << 16 | m << 8 | (col0 + c)), 0u, 0.0, 0.0};
                         ++slot;
                     }
                 }
             };
             const bool got = mbar_wait(&sm.tfull[b], bph, abort_flag, err, 16);
-            if (!epi_barrier_and(got)) break;
+            if (!group_barrier_and(part, got)) break;
             tmem_fence_after();
             for (;;) {
                 // ---- scan: this thread's accumulator columns in 32-column chunks, each
@@ -574,21 +595,26 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                 }
 
-                epi_barrier();
-                const int queued = sm.qcount;
+                group_barrier(part);
+                const int queued = sm.qcount[part];
                 const bool last = mt + 1 == m_end;
                 if (queued > kQueueCap) {
-                    drain_queue<N, NT>(sm, kQueueCap, true, tag, et, ds, fp, exact);
+                    drain_queue<N, NT, kRangesPerWarp>(sm, part, kQueueCap, true, tag, gt, ds,
+                                                       fp, exact);
                     rescan = true;
                     continue;  // pass again over the same accumulator (fresh thresholds)
                 }
                 if (queued >= kFlush || (last && queued > 0))
-                    drain_queue<N, NT>(sm, queued, false, tag, et, ds, fp, exact);
+                    drain_queue<N, NT, kRangesPerWarp>(sm, part, queued, false, tag, gt, ds,
+                                                       fp, exact);
                 break;
             }
             if (rescan) {
-                for (int w2 = et; w2 < kM * NT / 32; w2 += kEpiThreads) sm.evaluated[w2] = 0u;
-                epi_barrier();
+                // This group's words of the bitmask: NT / 64 of each lane's NT / 32.
+                constexpr int kWg = NT / 64;
+                for (int w2 = gt; w2 < kM * kWg; w2 += kGroupThreads)
+                    sm.evaluated[(w2 / kWg) * (NT / 32) + part * kWg + w2 % kWg] = 0u;
+                group_barrier(part);
             }
             // The accumulator has been read completely: hand it back to the MMA warp.
             tmem_fence_before();
