@@ -851,6 +851,37 @@ __global__ void __launch_bounds__(288) seed_kernel(
     }
 }
 
+// The coarse pre-pass's champion of each range (the best of its M-splits over every
+// `ratio`-th domain position of each axis) as a seed on the full grid: its domain index is
+// mapped to the fine grid, and it replaces the seed when it is better by (rms, index).
+// Any real candidate is a valid seed; a better one prunes more from the first tile.
+__global__ void seed_merge_kernel(const Partial* __restrict__ partials, int nsplit, int nranges,
+                                  int coarse_ncol, int fine_ncol, int ratio,
+                                  SeedOut* __restrict__ seeds) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nranges) return;
+    const SeedOut s = seeds[r];
+    if (s.idx == UINT32_MAX) return;  // no range block here
+    // The pre-pass started from this seed, whose index is on the fine grid.  A split's
+    // champion only ever changes to a strictly better (rms, index) pair, so a partial equal
+    // to the seed's pair is the seed itself; every other one is a coarse-grid candidate.
+    bool have = false;
+    Partial best{};
+    for (int t = 0; t < nsplit; ++t) {
+        const Partial p = partials[(size_t)t * nranges + r];
+        if (p.idx == UINT32_MAX || (p.rms == s.rms && p.idx == s.idx)) continue;
+        if (!have || p.rms < best.rms || (p.rms == best.rms && p.idx < best.idx)) best = p;
+        have = true;
+    }
+    if (!have) return;
+    const uint32_t dom1 = best.idx >> 3;
+    const uint32_t a1 = dom1 / (uint32_t)coarse_ncol, b1 = dom1 % (uint32_t)coarse_ncol;
+    const uint32_t idx =
+        ((a1 * (uint32_t)ratio) * (uint32_t)fine_ncol + b1 * (uint32_t)ratio) * 8u + (best.idx & 7u);
+    if (best.rms < s.rms || (best.rms == s.rms && idx < s.idx))
+        seeds[r] = SeedOut{best.rms, best.sum, idx, best.t1x4};
+}
+
 // Final champion over the M-splits; its exact correlation travels with it, so only the
 // (cheap) exact fit is redone here to fill in qalfa / qbeta.
 __global__ void finish_kernel(const Partial* __restrict__ partials, int nsplit, int nranges,
@@ -1081,6 +1112,14 @@ cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeo
         default: return cudaErrorInvalidValue;
     }
 #undef MARS_CORR
+}
+
+cudaError_t launch_seed_merge(const Partial* partials, int nsplit, int nranges, int coarse_ncol,
+                              int fine_ncol, int ratio, SeedOut* seeds, cudaStream_t st) {
+    if (nranges == 0) return cudaSuccess;
+    seed_merge_kernel<<<(nranges + 127) / 128, 128, 0, st>>>(partials, nsplit, nranges,
+                                                             coarse_ncol, fine_ncol, ratio, seeds);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,

@@ -59,6 +59,8 @@ cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeo
                         RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
                         Partial* partials, int msplit, bool digits, int* err,
                         unsigned long long* counter, cudaStream_t st);
+cudaError_t launch_seed_merge(const Partial* partials, int nsplit, int nranges, int coarse_ncol,
+                              int fine_ncol, int ratio, SeedOut* seeds, cudaStream_t st);
 cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,
                           RangeStats rs, DomainStats ds, const FitParams& fp, CandidateOut* out,
                           cudaStream_t st);
