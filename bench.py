@@ -620,6 +620,54 @@ def run_large_profile(args):
     return 0
 
 
+def run_large_full(args):
+    """One whole exhaustive search of a side x side synthetic plane (seed 99): every
+    RD-quadtree node, sizes 32..4, stride 2, through mars_search_nodes_device (the levels
+    one after another on one stream; plane in HBM, node table left in HBM).  `warmup`
+    untimed searches, then one timed with CUDA events.  Prints one JSON object: evals, nodes,
+    seconds and fits/s.  At 4096x4096 this is the uneven batch's large plane (4.65e13
+    evals, ~17 s per search on one B200), so it is not part of the default run."""
+    import torch
+    import mars_b200 as mb
+    side = args.large_full
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx = mb.Context(0)
+    ctx.set_stream(stream.cuda_stream)
+    plane = torch.from_numpy(synthetic.gray(side, side, 99)).to(dev)
+    params = mb.make_params(min_size=4, max_size=32, shift=SHIFT)
+    n, ev = mb.C.c_size_t(), mb.C.c_uint64()
+    mb.check(mb.lib().mars_search_nodes_device(ctx.handle, plane.data_ptr(), side, side,
+                                               mb.C.byref(params), None, 0, mb.C.byref(n),
+                                               mb.C.byref(ev)))
+    out = torch.empty((n.value, 80), dtype=torch.uint8, device=dev)
+
+    def call():
+        mb.check(mb.lib().mars_search_nodes_device(ctx.handle, plane.data_ptr(), side, side,
+                                                   mb.C.byref(params), out.data_ptr(), n.value,
+                                                   mb.C.byref(n), mb.C.byref(ev)))
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(dev.index) as clocks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        call()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    sec = e0.elapsed_time(e1) / 1e3
+    print(json.dumps({"large_full": {
+        "workload": f"exhaustive search of every RD quadtree node of a {side}x{side} synthetic "
+                    "gray plane (seed 99), block sizes 32..4, domain stride 2",
+        "nodes": n.value, "evals": ev.value, "seconds": sec, "value": ev.value / sec,
+        "unit": "fits/s", "warmup": args.warmup, "clocks": clocks.summary(),
+        "call": "mars_search_nodes_device (levels in sequence, no graph)"}}), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_reference(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -893,7 +941,12 @@ def main():
     ap.add_argument("--profile-large", type=int, default=0, metavar="SIDE",
                     help="run only the large-plane profile case (a SIDE x SIDE plane, the "
                          "first blocks of every level) and print its JSON object")
+    ap.add_argument("--large-full", type=int, default=0, metavar="SIDE",
+                    help="time one whole exhaustive search of a SIDE x SIDE plane (every RD "
+                         "node) and print its JSON object")
     args = ap.parse_args()
+    if args.large_full:
+        return run_large_full(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.profile_large:

@@ -107,3 +107,49 @@ def test_rd_encode_bytes_match_oracle(ctx, plan, golden, lam):
     data2 = mb.format_write(hdr2, leaves2, res2)
     assert hashlib.sha256(data2).hexdigest() == want["sha256"]
     assert (cnt2.search_evals, cnt2.warmup_evals) == (want["search_evals"], want["warmup_evals"])
+
+
+# ---- the 4096x4096 plane of the uneven batch: a seeded sample of nodes (corners and border
+# blocks included) searched over every domain of the plane, against the oracle's records
+# (tests/golden/make_sample_4096.py).  At this size one block sweeps 4.1 M domain positions:
+# thousands of domain tiles per CTA, 32-bit domain indices near 2^25, and, at 32 and 16, the
+# split-digit operand over a 2048x2048 contracted plane.
+
+SAMPLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sample_4096.json")
+
+
+@pytest.fixture(scope="module")
+def sample():
+    with open(SAMPLE) as f:
+        s = json.load(f)
+    import torch
+    s["plane"] = torch.from_numpy(synthetic.gray(s["side"], s["side"], s["seed"])).cuda()
+    return s
+
+
+@pytest.mark.parametrize("path", ["auto", "simt"])
+@pytest.mark.parametrize("size", [32, 16, 8, 4])
+def test_4096_sample_matches_oracle_records(ctx, sample, size, path):
+    import torch
+    side, shift = sample["side"], sample["shift"]
+    lv = sample["levels"][str(size)]
+    n = len(lv["rows"])
+    ndom = ((side - 2 * size) // shift + 1) ** 2
+    assert lv["evals"] == [8 * ndom] * n  # the exhaustive count, positions x 8
+    rows = torch.tensor(lv["rows"], dtype=torch.int32, device="cuda")
+    cols = torch.tensor(lv["cols"], dtype=torch.int32, device="cuda")
+    out = torch.zeros((n, mb.CANDIDATE_DTYPE.itemsize), dtype=torch.uint8, device="cuda")
+    p = mb.make_params(min_size=4, max_size=32, shift=shift)
+    ctx.set_search_path(path)
+    try:
+        torch.cuda.synchronize()
+        mb.check(mb.lib().mars_search_blocks_device(ctx.handle, sample["plane"].data_ptr(), side,
+                                                    side, size, shift, mb.C.byref(p),
+                                                    rows.data_ptr(), cols.data_ptr(), n,
+                                                    out.data_ptr()))
+        torch.cuda.synchronize()
+    finally:
+        ctx.set_search_path("auto")
+    got = out.cpu().numpy()
+    for i in range(n):
+        assert got[i].tobytes().hex() == lv["records"][i], (size, lv["rows"][i], lv["cols"][i])
