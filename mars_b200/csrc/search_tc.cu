@@ -517,15 +517,21 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const float g1 = __fmul_rd(ra.x, sdetf);
                     const float tz = fminf(__fadd_rd(ra.y, ahd), fmaxf(g1, ad));
                     const float tau = dom > tie ? tz : g1;
-                    thr[r] = dom < 0 ? INT32_MAX : __float2int_rd(__fmaf_rd(s1f, ra.z, tau));
+                    thr[r] = __float2int_rd(__fmaf_rd(s1f, ra.z, tau));
                 }
             };
-            auto test_chunk = [&](const int32_t (&v)[32], int ch) {
+            // Whether any column of chunk ch can survive.  A lane past the domain row's end
+            // (dom < 0) never passes; its thresholds, from stale or zero statistics, are
+            // never read.
+            auto chunk_pass = [&](const int32_t (&v)[32], int ch) {
+                return (dom >= 0) & ((max8(v, 0) >= thr[ch * 4]) | (max8(v, 8) >= thr[ch * 4 + 1]) |
+                                     (max8(v, 16) >= thr[ch * 4 + 2]) |
+                                     (max8(v, 24) >= thr[ch * 4 + 3]));
+            };
+            auto chunk_rare = [&](const int32_t (&v)[32], int ch) {
                 const int32_t t0 = thr[ch * 4], t1 = thr[ch * 4 + 1];
                 const int32_t t2 = thr[ch * 4 + 2], t3 = thr[ch * 4 + 3];
-                const bool any = (max8(v, 0) >= t0) | (max8(v, 8) >= t1) | (max8(v, 16) >= t2) |
-                                 (max8(v, 24) >= t3);
-                if (any) {
+                {
                     // Rare: bit c of `mask` = column c of this chunk survives (and was not
                     // fitted by an earlier pass over this accumulator).
                     uint32_t mask = 0u;
@@ -549,6 +555,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                         ++slot;
                     }
                 }
+            };
+            auto test_chunk = [&](const int32_t (&v)[32], int ch) {
+                if (chunk_pass(v, ch)) chunk_rare(v, ch);
             };
             const bool got = mbar_wait(&sm.tfull[b], bph, abort_flag, err, 16);
             if (!group_barrier_and(part, got)) break;
@@ -575,23 +584,22 @@ __global__ void __launch_bounds__(kThreads, 1)
                         __syncwarp();
                     }
                 } else {
-                    tmem_ld32(tcol, va);
-                    chunk_thresholds(0);
-                    tmem_wait(va);
 #pragma unroll
                     for (int ch = 0; ch < kChunks; ch += 2) {
+                        // Two chunks per round: both loads in flight while their 8
+                        // thresholds are computed, one branch for the pair.
+                        tmem_ld32(tcol + 32u * ch, va);
                         tmem_ld32(tcol + 32u * (ch + 1), vb);
+                        chunk_thresholds(ch);
                         chunk_thresholds(ch + 1);
-                        test_chunk(va, ch);
-                        __syncwarp();
+                        tmem_wait(va);
                         tmem_wait(vb);
-                        if (ch + 2 < kChunks) {
-                            tmem_ld32(tcol + 32u * (ch + 2), va);
-                            chunk_thresholds(ch + 2);
+                        const bool pa = chunk_pass(va, ch), pb = chunk_pass(vb, ch + 1);
+                        if (pa | pb) {
+                            if (pa) chunk_rare(va, ch);
+                            if (pb) chunk_rare(vb, ch + 1);
                         }
-                        test_chunk(vb, ch + 1);
                         __syncwarp();
-                        if (ch + 2 < kChunks) tmem_wait(va);
                     }
                 }
 
@@ -843,11 +851,25 @@ __global__ void __launch_bounds__(288) seed_kernel(
         c_t1[nb * 8 + lane] = t1;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int b = 0;
-        for (int c = 1; c < 72; ++c)
+    if (warp == 0) {
+        // The best of the 72 by (rms, reference index): each lane takes candidates lane,
+        // lane + 32, lane + 64, then a shuffle reduction.
+        int b = lane;
+        for (int c = lane + 32; c < 72; c += 32)
             if (c_rms[c] < c_rms[b] || (c_rms[c] == c_rms[b] && c_idx[c] < c_idx[b])) b = c;
-        out[r] = SeedOut{c_rms[b], c_sum[b], c_idx[b], c_t1[b]};
+        double br = c_rms[b];
+        uint32_t bi = c_idx[b];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double r2 = __shfl_xor_sync(0xffffffffu, br, o);
+            const uint32_t i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+            const int b2 = __shfl_xor_sync(0xffffffffu, b, o);
+            if (r2 < br || (r2 == br && i2 < bi)) {
+                br = r2;
+                bi = i2;
+                b = b2;
+            }
+        }
+        if (lane == 0) out[r] = SeedOut{c_rms[b], c_sum[b], c_idx[b], c_t1[b]};
     }
 }
 
