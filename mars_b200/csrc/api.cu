@@ -88,15 +88,76 @@ LevelGeom level_geom(uint32_t w, uint32_t h, uint32_t size, uint32_t shift) {
 }
 }  // namespace mars
 
+namespace mars {
+// The node index of a search table: (row, col, size, shift) -> position in the node table.
+// Every node of one (size, shift) job sits on the size-aligned grid, so a job's nodes are a
+// dense grid of ceil(w/size) x ceil(h/size) cells; a job with few nodes in a large grid (the
+// border blocks below min_size) keeps a sorted list instead, so memory stays bounded by the
+// node count.  A node added twice keeps the last position.
+class NodeIndex {
+  public:
+    void add_job(uint32_t size, uint32_t shift, uint32_t w, uint32_t h, const uint32_t* rows,
+                 const uint32_t* cols, size_t n, uint32_t first) {
+        Level* L = level(size, shift);
+        if (!L) {
+            levels_.push_back(Level{size, shift, (w + size - 1) / size, (h + size - 1) / size, {}, {}});
+            L = &levels_.back();
+            const uint64_t cells = (uint64_t)L->gw * L->gh;
+            if ((uint64_t)n * 8 >= cells) L->dense.assign((size_t)cells, UINT32_MAX);
+        }
+        for (size_t i = 0; i < n; ++i) {
+            const uint32_t r = rows[i], c = cols[i], at = first + (uint32_t)i;
+            if (!L->dense.empty() && r % size == 0 && c % size == 0 && r / size < L->gh &&
+                c / size < L->gw)
+                L->dense[(size_t)(r / size) * L->gw + c / size] = at;
+            else
+                L->sparse.push_back({key(r, c), at});
+        }
+        // Stable: for a repeated node the later entry stays last and wins below.
+        std::stable_sort(L->sparse.begin(), L->sparse.end(),
+                         [](const auto& x, const auto& y) { return x.first < y.first; });
+    }
+    // The node's position, or -1 when the table does not hold it.
+    int64_t find(uint32_t row, uint32_t col, uint32_t size, uint32_t shift) const {
+        for (const Level& L : levels_) {
+            if (L.size != size || L.shift != shift) continue;
+            if (!L.dense.empty() && row % size == 0 && col % size == 0 && row / size < L.gh &&
+                col / size < L.gw) {
+                const uint32_t v = L.dense[(size_t)(row / size) * L.gw + col / size];
+                if (v != UINT32_MAX) return v;
+            }
+            const uint64_t k = key(row, col);
+            auto it = std::upper_bound(L.sparse.begin(), L.sparse.end(), k,
+                                       [](uint64_t x, const auto& e) { return x < e.first; });
+            if (it != L.sparse.begin() && (it - 1)->first == k) return (it - 1)->second;
+            return -1;
+        }
+        return -1;
+    }
+
+  private:
+    struct Level {
+        uint32_t size, shift, gw, gh;
+        std::vector<uint32_t> dense;
+        std::vector<std::pair<uint64_t, uint32_t>> sparse;
+    };
+    static uint64_t key(uint32_t r, uint32_t c) { return (uint64_t)r << 32 | c; }
+    Level* level(uint32_t size, uint32_t shift) {
+        for (Level& L : levels_)
+            if (L.size == size && L.shift == shift) return &L;
+        return nullptr;
+    }
+    std::vector<Level> levels_;
+};
+}  // namespace mars
+
 struct mars_table {
     uint32_t width = 0, height = 0;
     uint32_t k = 1;  // ranked candidates per node (cands holds the first of each)
-    std::unordered_map<uint64_t, uint32_t> index;
+    mars::NodeIndex index;
     // A search plan's tables share the plan's node index instead of owning one.
-    std::shared_ptr<const std::unordered_map<uint64_t, uint32_t>> shared_index;
-    const std::unordered_map<uint64_t, uint32_t>& nodes() const {
-        return shared_index ? *shared_index : index;
-    }
+    std::shared_ptr<const mars::NodeIndex> shared_index;
+    const mars::NodeIndex& nodes() const { return shared_index ? *shared_index : index; }
     std::vector<mars_candidate> cands;
     std::vector<mars_candidate> ranked;  // k per node, when k > 1
     std::vector<uint64_t> evals;
@@ -107,11 +168,6 @@ struct mars_table {
 namespace {
 
 static_assert(sizeof(mars_candidate) == sizeof(mars::CandidateOut), "candidate layout");
-
-uint64_t node_key(uint32_t row, uint32_t col, uint32_t size, uint32_t shift) {
-    return (uint64_t)row | ((uint64_t)col << 16) | ((uint64_t)size << 32) |
-           ((uint64_t)shift << 48);
-}
 
 // Device waits are bounded: poll an event until it completes or the deadline passes.  The
 // work waited for is the context's stream's, or `stream`'s when one is given.
@@ -727,11 +783,11 @@ int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, 
             for (size_t i = 0; i < total; ++i) t->cands[i] = t->ranked[i * k];
     }
     size_t off = 0;
-    t->index.reserve(total * 2);
     for (const Job& j : jobs) {
         const uint64_t ev = level_evals(w, h, j.size, j.shift);
+        t->index.add_job(j.size, j.shift, w, h, j.rows.data(), j.cols.data(), j.rows.size(),
+                         (uint32_t)off);
         for (size_t i = 0; i < j.rows.size(); ++i) {
-            t->index[node_key(j.rows[i], j.cols[i], j.size, j.shift)] = (uint32_t)(off + i);
             if (method == MARS_METHOD_EXHAUSTIVE) t->evals[off + i] = ev;
             t->total_evals += t->evals[off + i];
         }
@@ -847,13 +903,13 @@ int mars_indexed_table_build(mars_ctx* ctx, const uint8_t* plane, uint32_t width
 int mars_search_table_lookup(const mars_table* t, uint32_t row, uint32_t col, uint32_t size,
                              uint32_t shift, mars_candidate* out, uint64_t* evals) {
     if (!t || !out) return fail(MARS_EINVAL, "NULL argument");
-    auto it = t->nodes().find(node_key(row, col, size, shift));
-    if (it == t->nodes().end())
+    const int64_t at = t->nodes().find(row, col, size, shift);
+    if (at < 0)
         return fail(MARS_ENOTFOUND, "node (" + std::to_string(row) + "," + std::to_string(col) +
                                         "," + std::to_string(size) + ") at shift " +
                                         std::to_string(shift) + " is not in the table");
-    *out = t->cands[it->second];
-    if (evals) *evals = t->evals[it->second];
+    *out = t->cands[(size_t)at];
+    if (evals) *evals = t->evals[(size_t)at];
     return MARS_OK;
 }
 
@@ -869,12 +925,12 @@ int mars_search_table_lookup_ranked(const mars_table* t, uint32_t row, uint32_t 
                                     uint32_t size, uint32_t shift, uint32_t max,
                                     mars_candidate* out, uint32_t* count, uint64_t* evals) {
     if (!t || !count || (max && !out)) return fail(MARS_EINVAL, "NULL argument");
-    auto it = t->nodes().find(node_key(row, col, size, shift));
-    if (it == t->nodes().end())
+    const int64_t at = t->nodes().find(row, col, size, shift);
+    if (at < 0)
         return fail(MARS_ENOTFOUND, "node (" + std::to_string(row) + "," + std::to_string(col) +
                                         "," + std::to_string(size) + ") at shift " +
                                         std::to_string(shift) + " is not in the table");
-    const size_t i = it->second;
+    const size_t i = (size_t)at;
     const mars_candidate* src = t->k > 1 ? &t->ranked[i * t->k] : &t->cands[i];
     uint32_t n = 0;
     const uint32_t lim = std::min<uint32_t>(std::max<uint32_t>(max, 1), t->k);
@@ -1273,7 +1329,7 @@ struct mars_search_plan {
     uint64_t launches_per_run = 0;
     std::vector<uint64_t> evals;
     uint64_t total_evals = 0;
-    std::shared_ptr<const std::unordered_map<uint64_t, uint32_t>> index;
+    std::shared_ptr<const mars::NodeIndex> index;
     // The walks on the device (built on the first encode that uses them).
     std::mutex walk_mu;
     int walk_state = 0;  // 0 not built, 1 built, -1 this plan's tree needs the host walk
@@ -1422,14 +1478,14 @@ int mars_search_plan_create(mars_ctx* ctx, uint32_t width, uint32_t height,
     p->jobs = plan_jobs(nullptr, width, height, *params, false);
     const std::vector<uint32_t> rc = job_origins(p->jobs, &p->total);
     if (p->total > 0xffffffffull) return fail(MARS_EINVAL, "too many quadtree nodes");
-    auto index = std::make_shared<std::unordered_map<uint64_t, uint32_t>>();
-    index->reserve(p->total * 2);
+    auto index = std::make_shared<mars::NodeIndex>();
     p->evals.resize(p->total);
     size_t off = 0;
     for (const Job& j : p->jobs) {
         const uint64_t ev = level_evals(width, height, j.size, j.shift);
+        index->add_job(j.size, j.shift, width, height, j.rows.data(), j.cols.data(), j.rows.size(),
+                       (uint32_t)off);
         for (size_t i = 0; i < j.rows.size(); ++i) {
-            (*index)[node_key(j.rows[i], j.cols[i], j.size, j.shift)] = (uint32_t)(off + i);
             p->evals[off + i] = ev;
             p->total_evals += ev;
         }
@@ -1567,8 +1623,7 @@ int plan_walk_setup(mars_search_plan* p, bool* usable) {
     for (uint32_t L = 1; L < w.nlevels; ++L)
         if (w.size[L] <= w.size[L - 1]) return MARS_OK;  // one level per size, ascending
     auto find = [&](uint32_t r, uint32_t c, uint32_t size) -> int64_t {
-        auto it = index.find(node_key(r, c, size, prm.shift));
-        return it == index.end() ? -1 : (int64_t)it->second;
+        return index.find(r, c, size, prm.shift);
     };
     std::vector<int32_t> child(4 * rows.size(), -1);
     for (uint32_t L = 0; L < w.nlevels; ++L) {
