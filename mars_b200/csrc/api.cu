@@ -598,6 +598,8 @@ int run_fisher_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int3
     MARS_CUDA(sc.get(&a.rrank, n));
     MARS_CUDA(sc.get(&plan, mars::ftc::kPlanWords));
     MARS_CUDA(sc.get(&ref_scratch, 72));
+    uint32_t* group_work = nullptr;
+    MARS_CUDA(sc.get(&group_work, mars::fisher_group_work_words((size_t)n)));
     a.plan.rcounts = plan;
     a.plan.roffsets = plan + 72;
     a.plan.p_base = plan + 144;
@@ -609,7 +611,7 @@ int run_fisher_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int3
     MARS_CUDA(mars::ftc::launch_range_classes(d_plane, (int)w, (int)h, g.size, d_rows, d_cols, n,
                                               ix.ref, rbucket, riso, st));
     MARS_CUDA(mars::launch_fisher_group(rbucket, n, a.plan.rcounts, a.plan.roffsets, ref_scratch,
-                                        rlist, st));
+                                        rlist, group_work, st));
     a.a_rows_max = mars::ftc::a_rows_max(npos);
     a.b_rows_max = mars::ftc::b_rows_max((size_t)n);
     a.items_max = mars::ftc::items_max((size_t)n);
@@ -679,6 +681,7 @@ int run_jobs_fisher(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t
     MARS_CUDA(sc.get(&ix.counts, 72));
     MARS_CUDA(sc.get(&ix.offsets, 72));
     MARS_CUDA(sc.get(&ix.ref, 72));
+    MARS_CUDA(sc.get(&ix.work, mars::fisher_group_work_words(max_pos)));
     size_t max_part = 1;
     for (const Job& j : jobs)
         max_part = std::max(max_part, j.rows.size() * (size_t)mars::fisher_warps_per_range((int)j.size));

@@ -53,59 +53,116 @@ __global__ void fisher_classify_domains_kernel(const int32_t* __restrict__ D, in
 }
 
 // Bucket sizes: block b counts the positions of bucket b.
-__global__ void fisher_count_kernel(const uint8_t* __restrict__ key, int n,
-                                    uint32_t* __restrict__ counts) {
-    __shared__ uint32_t total;
-    if (threadIdx.x == 0) total = 0;
-    __syncthreads();
-    uint32_t c = 0;
-    for (int p = threadIdx.x; p < n; p += blockDim.x) c += key[p] == blockIdx.x;
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&total, c);
-    __syncthreads();
-    if (threadIdx.x == 0) counts[blockIdx.x] = total;
-}
+// Grouping by bucket, a stable counting sort in three kernels.  Keys are bucket numbers
+// 0..71; other values are left out.  The keys are cut into chunks of kGroupChunk, each chunk
+// taken by one block of 8 warps, each warp a run of kGroupWarpKeys consecutive keys.
+constexpr int kGroupChunk = 4096;
+constexpr int kGroupWarps = 8;
+constexpr int kGroupWarpKeys = kGroupChunk / kGroupWarps;
 
-// Offsets, and the bucket each class reads (itself, or the first non-empty one).
-__global__ void fisher_offsets_kernel(const uint32_t* __restrict__ counts,
-                                      uint32_t* __restrict__ offsets,
-                                      uint32_t* __restrict__ ref) {
-    if (threadIdx.x != 0) return;
-    uint32_t off = 0;
-    int first = -1;
-    for (int b = 0; b < 72; ++b) {
-        offsets[b] = off;
-        off += counts[b];
-        if (first < 0 && counts[b] > 0) first = b;
+// Per chunk, the count of each bucket (hist[chunk * 72 + bucket]).  Equal keys of a warp step
+// are added once by their lowest lane.
+__global__ void __launch_bounds__(32 * kGroupWarps)
+    fisher_hist_kernel(const uint8_t* __restrict__ key, int n, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[72];
+    const int lane = threadIdx.x & 31;
+    for (int b = threadIdx.x; b < 72; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kGroupChunk;
+    for (int i = threadIdx.x; i < kGroupChunk; i += blockDim.x) {
+        const int p = base + i;
+        const unsigned k = p < n ? key[p] : 255u;
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        if (k < 72 && lane == __ffs(peers) - 1) atomicAdd(&h[k], (uint32_t)__popc(peers));
     }
-    for (int b = 0; b < 72; ++b) ref[b] = counts[b] > 0 ? b : (first < 0 ? b : first);
+    __syncthreads();
+    for (int b = threadIdx.x; b < 72; b += blockDim.x) hist[(size_t)blockIdx.x * 72 + b] = h[b];
 }
 
-// Stable compaction: block b writes the positions of bucket b in raster order.
-__global__ void fisher_fill_kernel(const uint8_t* __restrict__ key, int n,
-                                   const uint32_t* __restrict__ offsets,
-                                   uint32_t* __restrict__ list) {
-    __shared__ uint32_t warp_sum[32];
-    __shared__ uint32_t base;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (threadIdx.x == 0) base = offsets[blockIdx.x];
+// Bucket totals and offsets, the bucket each class reads (itself, or the first non-empty
+// one when it is empty), and every chunk's first slot in each bucket (cbase).
+__global__ void fisher_scan_kernel(const uint32_t* __restrict__ hist, int nchunks,
+                                   uint32_t* __restrict__ counts, uint32_t* __restrict__ offsets,
+                                   uint32_t* __restrict__ ref, uint32_t* __restrict__ cbase) {
+    __shared__ uint32_t tot[72], offs[72];
+    const int b = threadIdx.x;
+    if (b < 72) {
+        uint32_t t = 0;
+        for (int c = 0; c < nchunks; ++c) t += hist[(size_t)c * 72 + b];
+        tot[b] = t;
+        counts[b] = t;
+    }
     __syncthreads();
-    for (int start = 0; start < n; start += blockDim.x) {
-        const int p = start + threadIdx.x;
-        const bool hit = p < n && key[p] == blockIdx.x;
-        const uint32_t ballot = __ballot_sync(0xffffffffu, hit);
-        if (lane == 0) warp_sum[warp] = __popc(ballot);
-        __syncthreads();
-        uint32_t before = 0, all = 0;
-        for (int k = 0; k < nw; ++k) {
-            before += k < warp ? warp_sum[k] : 0;
-            all += warp_sum[k];
+    if (b == 0) {
+        uint32_t off = 0;
+        int first = -1;
+        for (int bb = 0; bb < 72; ++bb) {
+            offs[bb] = off;
+            offsets[bb] = off;
+            off += tot[bb];
+            if (first < 0 && tot[bb] > 0) first = bb;
         }
-        if (hit) list[base + before + __popc(ballot & ((1u << lane) - 1))] = (uint32_t)p;
-        __syncthreads();
-        if (threadIdx.x == 0) base += all;
-        __syncthreads();
+        for (int bb = 0; bb < 72; ++bb) ref[bb] = tot[bb] > 0 ? bb : (first < 0 ? bb : first);
     }
+    __syncthreads();
+    if (b < 72) {
+        uint32_t run = offs[b];
+        for (int c = 0; c < nchunks; ++c) {
+            cbase[(size_t)c * 72 + b] = run;
+            run += hist[(size_t)c * 72 + b];
+        }
+    }
+}
+
+// Stable scatter: each warp counts its run per bucket, the block turns the counts into
+// per-warp first slots, then each warp writes its run's positions in order (the rank among
+// equal keys of a step from __match_any_sync).  The result is raster order within a bucket.
+__global__ void __launch_bounds__(32 * kGroupWarps)
+    fisher_scatter_kernel(const uint8_t* __restrict__ key, int n,
+                          const uint32_t* __restrict__ cbase, uint32_t* __restrict__ list) {
+    __shared__ uint32_t wh[kGroupWarps][72];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < kGroupWarps * 72; i += blockDim.x) (&wh[0][0])[i] = 0;
+    __syncthreads();
+    const int w0 = blockIdx.x * kGroupChunk + warp * kGroupWarpKeys;
+    for (int s = 0; s < kGroupWarpKeys; s += 32) {
+        const int p = w0 + s + lane;
+        const unsigned k = p < n ? key[p] : 255u;
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        if (k < 72 && lane == __ffs(peers) - 1) wh[warp][k] += (uint32_t)__popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    if (threadIdx.x < 72) {
+        const int bk = threadIdx.x;
+        uint32_t run = cbase[(size_t)blockIdx.x * 72 + bk];
+        for (int w = 0; w < kGroupWarps; ++w) {
+            const uint32_t c = wh[w][bk];
+            wh[w][bk] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    for (int s = 0; s < kGroupWarpKeys; s += 32) {
+        const int p = w0 + s + lane;
+        const unsigned k = p < n ? key[p] : 255u;
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        if (k < 72) list[wh[warp][k] + (uint32_t)__popc(peers & ((1u << lane) - 1))] = (uint32_t)p;
+        __syncwarp();
+        if (k < 72 && lane == __ffs(peers) - 1) wh[warp][k] += (uint32_t)__popc(peers);
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_group(const uint8_t* key, int n, uint32_t* counts, uint32_t* offsets,
+                         uint32_t* ref, uint32_t* list, uint32_t* work, cudaStream_t st) {
+    const int nchunks = n > 0 ? (n + kGroupChunk - 1) / kGroupChunk : 1;
+    uint32_t* hist = work;
+    uint32_t* cbase = work + (size_t)nchunks * 72;
+    fisher_hist_kernel<<<nchunks, 32 * kGroupWarps, 0, st>>>(key, n, hist);
+    fisher_scan_kernel<<<1, 96, 0, st>>>(hist, nchunks, counts, offsets, ref, cbase);
+    if (n > 0) fisher_scatter_kernel<<<nchunks, 32 * kGroupWarps, 0, st>>>(key, n, cbase, list);
+    return cudaGetLastError();
 }
 
 // `wpr` warps per range block (1, or 2 / 4 for the large sizes, whose levels have few
@@ -288,18 +345,17 @@ cudaError_t launch_fisher_index(const int32_t* D, int dw, int size, int shift, i
     if (npos > 0)
         fisher_classify_domains_kernel<<<(npos + 255) / 256, 256, 0, st>>>(
             D, dw, size, shift, nrow_d, ncol_d, ix.key, ix.diso);
-    fisher_count_kernel<<<72, 256, 0, st>>>(ix.key, npos, ix.counts);
-    fisher_offsets_kernel<<<1, 32, 0, st>>>(ix.counts, ix.offsets, ix.ref);
-    if (npos > 0) fisher_fill_kernel<<<72, 1024, 0, st>>>(ix.key, npos, ix.offsets, ix.list);
-    return cudaGetLastError();
+    return launch_group(ix.key, npos, ix.counts, ix.offsets, ix.ref, ix.list, ix.work, st);
+}
+
+size_t fisher_group_work_words(size_t n) {
+    const size_t nchunks = n > 0 ? (n + kGroupChunk - 1) / kGroupChunk : 1;
+    return 2 * nchunks * 72;
 }
 
 cudaError_t launch_fisher_group(const uint8_t* key, int n, uint32_t* counts, uint32_t* offsets,
-                                uint32_t* ref, uint32_t* list, cudaStream_t st) {
-    fisher_count_kernel<<<72, 256, 0, st>>>(key, n, counts);
-    fisher_offsets_kernel<<<1, 32, 0, st>>>(counts, offsets, ref);
-    if (n > 0) fisher_fill_kernel<<<72, 1024, 0, st>>>(key, n, offsets, list);
-    return cudaGetLastError();
+                                uint32_t* ref, uint32_t* list, uint32_t* work, cudaStream_t st) {
+    return launch_group(key, n, counts, offsets, ref, list, work, st);
 }
 
 cudaError_t launch_fisher_search(const uint8_t* plane, int w, int h, const int32_t* D, int dw,

@@ -737,22 +737,22 @@ __device__ __forceinline__ int32_t canon_t1(const int32_t* D, int dw, int dr, in
     return t1;
 }
 
-// Seed champion of each range: the exact best of the first 32 entries of its bucket (warp
-// per range, lane e % 32 fits entry e, first minimum by (rms, bucket index)).
+// Seed champion of each range: the exact best of the first 32 entries of its bucket, first
+// minimum by (rms, bucket index).  One warp per range: the range's canonical samples are
+// staged once in shared memory, then lane e correlates entry e whole.  The domain's flip
+// (flip_src) is affine in the canonical (i, j), so each lane walks its domain with two
+// strides chosen once, and the warp reduces once.
 template <int S>
-__global__ void fisher_seed_kernel(const uint8_t* __restrict__ plane, int w,
-                                   const int32_t* __restrict__ D, int dw, int shift, int ncol_d,
-                                   const uint32_t* __restrict__ rows,
-                                   const uint32_t* __restrict__ cols, int nranges,
-                                   const uint8_t* __restrict__ rbucket,
-                                   const uint8_t* __restrict__ riso,
-                                   const uint32_t* __restrict__ counts,
-                                   const uint32_t* __restrict__ offsets,
-                                   const uint32_t* __restrict__ list,
-                                   const uint8_t* __restrict__ diso, RangeStats rs, DomainStats ds,
-                                   FitParams fp, tc::SeedOut* __restrict__ out) {
+__global__ void __launch_bounds__(256) fisher_seed_kernel(
+    const uint8_t* __restrict__ plane, int w, const int32_t* __restrict__ D, int dw, int shift,
+    int ncol_d, const uint32_t* __restrict__ rows, const uint32_t* __restrict__ cols,
+    int nranges, const uint8_t* __restrict__ rbucket, const uint8_t* __restrict__ riso,
+    const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+    const uint32_t* __restrict__ list, const uint8_t* __restrict__ diso, RangeStats rs,
+    DomainStats ds, FitParams fp, tc::SeedOut* __restrict__ out) {
+    __shared__ uint8_t canon[8][S * S];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
     if (gw >= nranges) return;
     const int b = rbucket[gw];
     if (b == 255 || counts[b] == 0) {
@@ -761,26 +761,47 @@ __global__ void fisher_seed_kernel(const uint8_t* __restrict__ plane, int w,
     }
     const uint8_t* rb = plane + (size_t)rows[gw] * w + cols[gw];
     const int ri = riso[gw];
+    for (int f = lane; f < S * S; f += 32) {
+        const int sr = flip_src(ri, f / S, f % S, S);
+        canon[warp][f] = rb[(size_t)(sr / S) * w + sr % S];
+    }
+    __syncwarp();
     const uint32_t n = counts[b] < 32u ? counts[b] : 32u;
     double best = INFINITY, best_sum = 0.0;
     uint32_t best_e = kNone;
     int32_t best_t1 = 0;
-    for (uint32_t e = 0; e < n; ++e) {
+    if ((uint32_t)lane < n) {
+        const uint32_t e = (uint32_t)lane;
         const uint32_t p = list[offsets[b] + e];
         const int dr = (int)(p / (uint32_t)ncol_d) * (shift / 2);
         const int dc = (int)(p % (uint32_t)ncol_d) * (shift / 2);
-        int32_t t1 = canon_t1<S>(D, dw, dr, dc, diso[p], rb, w, ri, lane);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t1 += __shfl_xor_sync(0xffffffffu, t1, o);
-        if ((uint32_t)lane == (e & 31u)) {
-            const FitResult f = fit_exact(S * S, ds.s1x4[p], ds.s2x16[p], rs.t0[gw], t1, rs.t2[gw], fp);
-            if (f.rms < best) {
-                best = f.rms;
-                best_sum = f.sum;
-                best_e = e;
-                best_t1 = t1;
-            }
+        // flip_src(iso, i, j) = (row, col) of the domain sample, affine in (i, j): the
+        // sample's offset in D is o0 + i * oi + j * oj.
+        int r0, c0, ri_i, ri_j, ci_i, ci_j;  // row = r0 + i ri_i + j ri_j, col likewise
+        switch (diso[p]) {
+            case 0: r0 = 0; ri_i = 1; ri_j = 0; c0 = 0; ci_i = 0; ci_j = 1; break;
+            case 1: r0 = 0; ri_i = 0; ri_j = 1; c0 = S - 1; ci_i = -1; ci_j = 0; break;
+            case 2: r0 = S - 1; ri_i = 0; ri_j = -1; c0 = 0; ci_i = 1; ci_j = 0; break;
+            case 3: r0 = S - 1; ri_i = -1; ri_j = 0; c0 = S - 1; ci_i = 0; ci_j = -1; break;
+            case 4: r0 = 0; ri_i = 1; ri_j = 0; c0 = S - 1; ci_i = 0; ci_j = -1; break;
+            case 5: r0 = S - 1; ri_i = -1; ri_j = 0; c0 = 0; ci_i = 0; ci_j = 1; break;
+            case 6: r0 = 0; ri_i = 0; ri_j = 1; c0 = 0; ci_i = 1; ci_j = 0; break;
+            default: r0 = S - 1; ri_i = 0; ri_j = -1; c0 = S - 1; ci_i = -1; ci_j = 0; break;
         }
+        const int32_t* d0 = D + (size_t)(dr + r0) * dw + dc + c0;
+        const long long oi = (long long)ri_i * dw + ci_i, oj = (long long)ri_j * dw + ci_j;
+        const uint8_t* rc = canon[warp];
+        int32_t t1 = 0;
+        for (int i = 0; i < S; ++i) {
+            const int32_t* di = d0 + i * oi;
+#pragma unroll
+            for (int j = 0; j < S; ++j) t1 += di[j * oj] * (int32_t)rc[i * S + j];
+        }
+        const FitResult f = fit_exact(S * S, ds.s1x4[p], ds.s2x16[p], rs.t0[gw], t1, rs.t2[gw], fp);
+        best = f.rms;
+        best_sum = f.sum;
+        best_e = e;
+        best_t1 = t1;
     }
     double r = best;
     uint32_t ie = best_e;

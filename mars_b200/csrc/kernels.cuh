@@ -100,13 +100,16 @@ struct FisherIndex {
     uint32_t* offsets;  // [72]
     uint32_t* ref;      // [72]
     uint32_t* list;     // [npos]
+    uint32_t* work;     // [fisher_group_work_words(npos)], the grouping's scratch
 };
+// Scratch words the grouping of n keys needs (per-chunk bucket counts and first slots).
+size_t fisher_group_work_words(size_t n);
 cudaError_t launch_fisher_index(const int32_t* D, int dw, int size, int shift, int nrow_d,
                                 int ncol_d, FisherIndex ix, cudaStream_t st);
 // Groups the n entries of `key` (bucket numbers 0..71; others are left out) by bucket:
 // counts, offsets, the bucket each reads (ref) and the grouped indices in `list`, stable.
 cudaError_t launch_fisher_group(const uint8_t* key, int n, uint32_t* counts, uint32_t* offsets,
-                                uint32_t* ref, uint32_t* list, cudaStream_t st);
+                                uint32_t* ref, uint32_t* list, uint32_t* work, cudaStream_t st);
 // One warp per range block; writes the winner (valid = 0 for none) and the eval count.
 cudaError_t launch_fisher_search(const uint8_t* plane, int w, int h, const int32_t* D, int dw,
                                  int size, int shift, int ncol_d, const uint32_t* rows,
