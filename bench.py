@@ -55,7 +55,7 @@ NCU_SOURCE = "profiles/corr_tc_s4_512x512_ncu.md"
 NCU_TRAFFIC = {4: 20_560_000}
 # Thread instructions per candidate fit of the correlation kernel's level (warp
 # instructions x 32 / fits, same capture): the issue cost behind the epilogue roofline.
-NCU_INSTR_PER_FIT = {4: 1.0435e9 * 32 / 8.52e9, 8: 0.3886e9 * 32 / 2.0e9}
+NCU_INSTR_PER_FIT = {4: 0.9722e9 * 32 / 8.52e9, 8: 0.3886e9 * 32 / 2.0e9}
 # DRAM bytes of one decode iteration, by plane side (profiles/decode_cell_4096x4096_ncu.md;
 # profiles/decode_sorted_16384x16384_ncu.md: dram__bytes.sum.per_second x
 # gpu__time_duration.sum of the gather and the place launch of one iteration).
