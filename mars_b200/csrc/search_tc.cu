@@ -873,6 +873,87 @@ __global__ void __launch_bounds__(288) seed_kernel(
     }
 }
 
+constexpr int kSeedSide = 3;                       // seed domains: a 3 x 3 patch
+constexpr int kSeedCands = 8 * kSeedSide * kSeedSide;  // x 8 isometries
+
+// seed_kernel for the small blocks (S = 4, 8): the same 72 candidates, one warp per range
+// block (8 per CTA).  Lane l correlates candidates l, l + 32, l + 64 whole (S^2 terms) from the
+// range staged in shared memory; isometry::map is affine in (u, v), so a candidate walks the
+// staged range with a base and two strides and lanes of different isometries do not
+// diverge.  One (rms, reference index) reduction picks the winner.
+template <int S>
+__global__ void __launch_bounds__(256) seed_small_kernel(
+    const int32_t* __restrict__ D, LevelGeom g, const uint8_t* __restrict__ plane, int w,
+    const uint32_t* rows, const uint32_t* cols, int nranges, RangeStats rs, DomainStats ds,
+    FitParams fp, SeedOut* __restrict__ out) {
+    constexpr int N = S * S;
+    __shared__ uint8_t rsm[8][N];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = blockIdx.x * 8 + warp;
+    if (r >= nranges) return;
+    if (rows[r] + (uint32_t)S > (uint32_t)g.h || cols[r] + (uint32_t)S > (uint32_t)g.w) {
+        if (lane == 0) out[r] = SeedOut{INFINITY, 0.0, UINT32_MAX, 0};
+        return;
+    }
+    const uint8_t* rb = plane + (size_t)rows[r] * w + cols[r];
+    for (int t = lane; t < N; t += 32) rsm[warp][t] = rb[(size_t)(t / S) * w + (t % S)];
+    __syncwarp();
+    const int ac = min(max(((int)rows[r] - S / 2 + g.shift / 2) / g.shift, 0), g.nrow_d - 1);
+    const int bc = min(max(((int)cols[r] - S / 2 + g.shift / 2) / g.shift, 0), g.ncol_d - 1);
+    double best = INFINITY, best_sum = 0.0;
+    uint32_t best_idx = UINT32_MAX;
+    int32_t best_t1 = 0;
+    for (int c = lane; c < kSeedCands; c += 32) {
+        const int nb = c >> 3, k = c & 7;
+        const int a = min(max(ac + nb / kSeedSide - kSeedSide / 2, 0), g.nrow_d - 1);
+        const int bb = min(max(bc + nb % kSeedSide - kSeedSide / 2, 0), g.ncol_d - 1);
+        const int32_t* db = D + (size_t)(a * g.step_c) * g.dw + bb * g.step_c;
+        // iso_src_rt(k, u, v, S) = base + u * du + v * dv
+        int base, du, dv;
+        switch (k) {
+            case 0: base = 0; du = S; dv = 1; break;
+            case 1: base = (S - 1) * S; du = 1; dv = -S; break;
+            case 2: base = S - 1; du = -1; dv = S; break;
+            case 3: base = (S - 1) * S + S - 1; du = -S; dv = -1; break;
+            case 4: base = S - 1; du = S; dv = -1; break;
+            case 5: base = (S - 1) * S; du = -S; dv = 1; break;
+            case 6: base = 0; du = 1; dv = S; break;
+            default: base = (S - 1) * S + S - 1; du = -1; dv = -S; break;
+        }
+        const uint8_t* rr = rsm[warp];
+        int32_t t1 = 0;
+#pragma unroll
+        for (int u = 0; u < S; ++u)
+#pragma unroll
+            for (int v = 0; v < S; ++v)
+                t1 += (int32_t)rr[base + u * du + v * dv] * db[(size_t)u * g.dw + v];
+        const uint32_t dom = (uint32_t)(a * g.ncol_d + bb);
+        const FitResult f = fit_exact(N, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], t1, rs.t2[r], fp);
+        const uint32_t idx = dom * 8u + (uint32_t)k;
+        if (f.rms < best || (f.rms == best && idx < best_idx)) {
+            best = f.rms;
+            best_sum = f.sum;
+            best_idx = idx;
+            best_t1 = t1;
+        }
+    }
+    double br = best;
+    uint32_t bi = best_idx;
+    int bl = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double r2 = __shfl_xor_sync(0xffffffffu, br, o);
+        const uint32_t i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        const int l2 = __shfl_xor_sync(0xffffffffu, bl, o);
+        if (r2 < br || (r2 == br && i2 < bi)) {
+            br = r2;
+            bi = i2;
+            bl = l2;
+        }
+    }
+    if (lane == bl) out[r] = SeedOut{best, best_sum, best_idx, best_t1};
+}
+
 // The coarse pre-pass's champion of each range (the best of its M-splits over every
 // `ratio`-th domain position of each axis) as a seed on the full grid: its domain index is
 // mapped to the fine grid, and it replaces the seed when it is better by (rms, index).
@@ -1077,8 +1158,8 @@ cudaError_t launch_seed(const int32_t* D, const LevelGeom& g, const uint8_t* pla
     if (nranges == 0) return cudaSuccess;
     const unsigned blocks = (unsigned)nranges;
     switch (g.size) {
-        case 4: seed_kernel<4><<<blocks, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
-        case 8: seed_kernel<8><<<blocks, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
+        case 4: seed_small_kernel<4><<<(blocks + 7) / 8, 256, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
+        case 8: seed_small_kernel<8><<<(blocks + 7) / 8, 256, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
         case 16: seed_kernel<16><<<blocks, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
         case 32: seed_kernel<32><<<blocks, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
         case 64: seed_kernel<64><<<blocks, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, fp, out); break;
