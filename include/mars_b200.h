@@ -204,6 +204,14 @@ int mars_encode_planned(mars_search_plan* plan, const uint8_t* plane,
 int mars_indexed_table_build(mars_ctx* ctx, const uint8_t* plane, uint32_t width,
                              uint32_t height, const mars_params* params, int32_t adaptive_density,
                              int32_t method, mars_table** out);
+/* A search plan for `method` (MARS_METHOD_EXHAUSTIVE is mars_search_plan_create): the same
+ * nodes as mars_indexed_table_build without adaptive density, the whole search of a plane
+ * -- for Fisher the per-size domain indexes, range classification and bucketed searches --
+ * captured once as a CUDA graph.  The run / run_device / table calls are the plan calls
+ * above; a Fisher table's eval counts are the bucket lengths of that run's plane.  Planned
+ * encodes (mars_encode_planned) take exhaustive plans only. */
+int mars_indexed_plan_create(mars_ctx* ctx, uint32_t width, uint32_t height,
+                             const mars_params* params, int32_t method, mars_search_plan** out);
 
 /* search_block over an explicit list of block origins at one size and shift (host
  * buffers).  out[i] / evals[i] belong to (rows[i], cols[i]). */

@@ -95,6 +95,7 @@ EXPORTS = (
     "mars_rgb_from_ycbcr_device", "mars_downsample_box_device", "mars_upsample_nearest_device",
     "mars_mse_device", "mars_search_table_build_ranked", "mars_search_table_lookup_ranked",
     "mars_search_plan_create", "mars_search_plan_run", "mars_search_plan_run_device",
+    "mars_indexed_plan_create",
     "mars_search_plan_table", "mars_search_plan_evals", "mars_search_plan_launches",
     "mars_search_plan_free", "mars_decode_until_stable", "mars_decode_plan_run_until_stable",
     "mars_zoom_leaves", "mars_encode_planned",
@@ -139,6 +140,7 @@ def lib():
     L.mars_encode_planned.argtypes = [vp, vp, P(Options), P(Header), P(vp), P(sz), P(vp), P(sz),
                                       P(Counters)]
     L.mars_search_plan_create.argtypes = [vp, u32, u32, P(Params), P(vp)]
+    L.mars_indexed_plan_create.argtypes = [vp, u32, u32, P(Params), C.c_int32, P(vp)]
     L.mars_search_plan_run.argtypes = [vp, vp, P(vp)]
     L.mars_search_plan_run_device.argtypes = [vp, vp]
     L.mars_search_plan_table.argtypes = [vp, P(vp)]
@@ -369,10 +371,13 @@ class Context:
                                                  C.byref(t)))
         return GpuSearch(self, t.value, w, h)
 
-    def search_plan(self, width: int, height: int, params: Params) -> "SearchPlan":
-        """A graph-captured provider factory for repeated planes of one geometry."""
+    def search_plan(self, width: int, height: int, params: Params,
+                    method: str = "exhaustive") -> "SearchPlan":
+        """A graph-captured provider factory for repeated planes of one geometry
+        (mars_indexed_plan_create; "fisher" for the classified search)."""
         h = C.c_void_p()
-        check(lib().mars_search_plan_create(self._h, width, height, C.byref(params), C.byref(h)))
+        check(lib().mars_indexed_plan_create(self._h, width, height, C.byref(params),
+                                             METHODS[method], C.byref(h)))
         return SearchPlan(self, h.value, width, height)
 
     def search_blocks(self, img, size: int, shift: int, params: Params, rows, cols):

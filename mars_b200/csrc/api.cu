@@ -649,9 +649,11 @@ int run_fisher_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int3
 // Fisher's classified search for every job: per (size, shift) the domain index
 // (Fisher::index) and the searches of the job's nodes (Fisher::candidates +
 // search_block_fitted); per-node eval counts come back from the device.
+// `d_rc_in`: the job origins already on the device (job_origins layout), else uploaded here.
 int run_jobs_fisher(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uint32_t h,
                     const mars::FitParams& fp, const std::vector<Job>& jobs,
-                    mars::CandidateOut* d_out, uint64_t* d_evals) {
+                    mars::CandidateOut* d_out, uint64_t* d_evals,
+                    const uint32_t* d_rc_in = nullptr) {
     const cudaStream_t st = ctx->stream;
     int32_t* d_D = nullptr;
     const int dw = (int)(w / 2);
@@ -664,16 +666,21 @@ int run_jobs_fisher(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t
         const mars::LevelGeom g = level_geom(w, h, j.size, j.shift);
         if (g.nrow_d > 0 && g.ncol_d > 0) max_pos = std::max(max_pos, (size_t)g.nrow_d * g.ncol_d);
     }
-    std::vector<uint32_t> rc(2 * total);
+    const uint32_t* d_rc = d_rc_in;
     size_t off = 0;
-    for (const Job& j : jobs) {
-        std::copy(j.rows.begin(), j.rows.end(), rc.begin() + (long)off);
-        std::copy(j.cols.begin(), j.cols.end(), rc.begin() + (long)(total + off));
-        off += j.rows.size();
+    if (!d_rc) {
+        std::vector<uint32_t> rc(2 * total);
+        for (const Job& j : jobs) {
+            std::copy(j.rows.begin(), j.rows.end(), rc.begin() + (long)off);
+            std::copy(j.cols.begin(), j.cols.end(), rc.begin() + (long)(total + off));
+            off += j.rows.size();
+        }
+        uint32_t* d = nullptr;
+        MARS_CUDA(sc.get(&d, std::max<size_t>(1, rc.size())));
+        // A pageable source: the call returns once the bytes are staged, so `rc` may go.
+        MARS_CUDA(cudaMemcpyAsync(d, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice, st));
+        d_rc = d;
     }
-    uint32_t* d_rc = nullptr;
-    MARS_CUDA(sc.get(&d_rc, std::max<size_t>(1, rc.size())));
-    MARS_CUDA(cudaMemcpyAsync(d_rc, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice, st));
     mars::FisherIndex ix;
     MARS_CUDA(sc.get(&ix.key, std::max<size_t>(1, max_pos)));
     MARS_CUDA(sc.get(&ix.diso, std::max<size_t>(1, max_pos)));
@@ -1319,6 +1326,10 @@ struct mars_search_plan {
     mars_ctx* ctx = nullptr;
     uint32_t w = 0, h = 0;
     mars_params params{};
+    int method = MARS_METHOD_EXHAUSTIVE;
+    // Fisher plans: the eval counts are the bucket lengths, found on the device each run.
+    uint64_t* d_evals = nullptr;
+    uint64_t* h_evals = nullptr;  // pinned
     std::vector<Job> jobs;
     size_t total = 0;
     uint32_t* d_rc = nullptr;
@@ -1359,6 +1370,8 @@ void plan_release(mars_search_plan* p) {
     cudaFreeHost(p->h_plane);
     cudaFreeHost(p->h_out);
     cudaFreeHost(p->h_exact);
+    cudaFree(p->d_evals);
+    cudaFreeHost(p->h_evals);
     cudaFree(p->d_wrows);
     cudaFree(p->d_wcols);
     cudaFree(p->d_child);
@@ -1427,11 +1440,20 @@ int plan_enqueue(mars_search_plan* p, bool with_copies) {
                                   cudaMemcpyHostToDevice, st));
     MARS_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), st));
     const mars::FitParams fp = make_fit_params(p->params);
-    if (int e = run_jobs_branched(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out, p->d_rc))
+    if (p->method == MARS_METHOD_FISHER) {
+        if (int e = run_jobs_fisher(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out,
+                                    p->d_evals, p->d_rc))
+            return e;
+    } else if (int e = run_jobs_branched(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out,
+                                         p->d_rc)) {
         return e;
+    }
     if (with_copies) {
         MARS_CUDA(cudaMemcpyAsync(p->h_out, p->d_out, p->total * sizeof(mars_candidate),
                                   cudaMemcpyDeviceToHost, st));
+        if (p->method == MARS_METHOD_FISHER)
+            MARS_CUDA(cudaMemcpyAsync(p->h_evals, p->d_evals, p->total * sizeof(uint64_t),
+                                      cudaMemcpyDeviceToHost, st));
         MARS_CUDA(cudaMemcpyAsync(p->h_exact, ctx->d_counter, sizeof(unsigned long long),
                                   cudaMemcpyDeviceToHost, st));
     }
@@ -1466,8 +1488,17 @@ extern "C" {
 
 int mars_search_plan_create(mars_ctx* ctx, uint32_t width, uint32_t height,
                             const mars_params* params, mars_search_plan** out) {
+    return mars_indexed_plan_create(ctx, width, height, params, MARS_METHOD_EXHAUSTIVE, out);
+}
+
+int mars_indexed_plan_create(mars_ctx* ctx, uint32_t width, uint32_t height,
+                             const mars_params* params, int32_t method, mars_search_plan** out) {
     if (!ctx || !params || !out) return fail(MARS_EINVAL, "NULL argument");
     if (int e = check_params(params)) return e;
+    if (method != MARS_METHOD_EXHAUSTIVE && method != MARS_METHOD_FISHER)
+        return fail(MARS_EUNSUPPORTED, "unknown search method " + std::to_string(method));
+    if (method == MARS_METHOD_FISHER && params->max_size > 64)
+        return fail(MARS_EUNSUPPORTED, "the classified search supports block sizes up to 64");
     if (width == 0 || height == 0 || width > 65535 || height > 65535)
         return fail(MARS_EINVAL, "plane dimensions must be in 1..65535");
     std::unique_ptr<mars_search_plan, void (*)(mars_search_plan*)> p(new (std::nothrow)
@@ -1478,6 +1509,7 @@ int mars_search_plan_create(mars_ctx* ctx, uint32_t width, uint32_t height,
     p->w = width;
     p->h = height;
     p->params = *params;
+    p->method = method;
     p->jobs = plan_jobs(nullptr, width, height, *params, false);
     const std::vector<uint32_t> rc = job_origins(p->jobs, &p->total);
     if (p->total > 0xffffffffull) return fail(MARS_EINVAL, "too many quadtree nodes");
@@ -1488,10 +1520,11 @@ int mars_search_plan_create(mars_ctx* ctx, uint32_t width, uint32_t height,
         const uint64_t ev = level_evals(width, height, j.size, j.shift);
         index->add_job(j.size, j.shift, width, height, j.rows.data(), j.cols.data(), j.rows.size(),
                        (uint32_t)off);
-        for (size_t i = 0; i < j.rows.size(); ++i) {
-            p->evals[off + i] = ev;
-            p->total_evals += ev;
-        }
+        if (method == MARS_METHOD_EXHAUSTIVE)
+            for (size_t i = 0; i < j.rows.size(); ++i) {
+                p->evals[off + i] = ev;
+                p->total_evals += ev;
+            }
         off += j.rows.size();
     }
     p->index = index;
@@ -1503,6 +1536,10 @@ int mars_search_plan_create(mars_ctx* ctx, uint32_t width, uint32_t height,
     MARS_CUDA(cudaMallocHost(&p->h_plane, (size_t)width * height));
     MARS_CUDA(cudaMallocHost(&p->h_out, std::max<size_t>(1, p->total) * sizeof(mars_candidate)));
     MARS_CUDA(cudaMallocHost(&p->h_exact, sizeof(unsigned long long)));
+    if (method == MARS_METHOD_FISHER) {
+        MARS_CUDA(cudaMalloc(&p->d_evals, std::max<size_t>(1, p->total) * sizeof(uint64_t)));
+        MARS_CUDA(cudaMallocHost(&p->h_evals, std::max<size_t>(1, p->total) * sizeof(uint64_t)));
+    }
     if (!rc.empty())
         MARS_CUDA(cudaMemcpyAsync(p->d_rc, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice,
                                   ctx->stream));
@@ -1531,6 +1568,11 @@ int mars_search_plan_run(mars_search_plan* p, const uint8_t* plane, mars_table**
     t->width = p->w;
     t->height = p->h;
     t->cands.assign(p->h_out, p->h_out + p->total);
+    if (p->method == MARS_METHOD_FISHER) {
+        p->evals.assign(p->h_evals, p->h_evals + p->total);
+        p->total_evals = 0;
+        for (uint64_t e : p->evals) p->total_evals += e;
+    }
     t->evals = p->evals;
     t->total_evals = p->total_evals;
     t->exact_fits = *p->h_exact;
@@ -1561,10 +1603,18 @@ int mars_search_plan_table(mars_search_plan* p, mars_table** out) {
     MARS_CUDA(cudaSetDevice(ctx->device));
     MARS_CUDA(cudaMemcpyAsync(p->h_out, p->d_out, p->total * sizeof(mars_candidate),
                               cudaMemcpyDeviceToHost, ctx->stream));
+    if (p->method == MARS_METHOD_FISHER)
+        MARS_CUDA(cudaMemcpyAsync(p->h_evals, p->d_evals, p->total * sizeof(uint64_t),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
     if (int e = sync_bounded(ctx)) return e;
     t->width = p->w;
     t->height = p->h;
     t->cands.assign(p->h_out, p->h_out + p->total);
+    if (p->method == MARS_METHOD_FISHER) {
+        p->evals.assign(p->h_evals, p->h_evals + p->total);
+        p->total_evals = 0;
+        for (uint64_t e : p->evals) p->total_evals += e;
+    }
     t->evals = p->evals;
     t->total_evals = p->total_evals;
     t->shared_index = p->index;
@@ -1869,7 +1919,8 @@ int mars_encode_planned(mars_search_plan* plan, const uint8_t* plane,
     if (!plan || !plane || !options || !header || !leaves || !nleaves || !residuals ||
         !nresiduals || !counters)
         return fail(MARS_EINVAL, "NULL argument");
-    if (options->method != MARS_METHOD_EXHAUSTIVE || std::max<uint32_t>(1, options->rd_candidates) > 1 ||
+    if (plan->method != MARS_METHOD_EXHAUSTIVE || options->method != MARS_METHOD_EXHAUSTIVE ||
+        std::max<uint32_t>(1, options->rd_candidates) > 1 ||
         (plan->params.has_lambda && options->adaptive_density))
         return fail(MARS_EUNSUPPORTED, "a search plan serves exhaustive single-winner encodes "
                                        "without adaptive density");

@@ -159,3 +159,48 @@ def test_tensor_core_batch_equals_cuda_core_kernel(ctx, name, side, seed):
         b.close()
     finally:
         simt.close()
+
+
+@pytest.mark.parametrize("w,h", [(768, 512), (384, 256), (129, 127)])
+def test_fisher_plan_tables_equal_the_provider(ctx, w, h):
+    # mars_indexed_plan_create with Fisher: the graph-captured classified search, run on
+    # several planes of one geometry (host and device entry points), gives the one-shot
+    # provider's candidates and per-node eval counts (the bucket lengths of each plane).
+    import torch
+    p = mb.make_params(min_size=4, max_size=16, shift=2, lam=200.0)
+    plan = ctx.search_plan(w, h, p, method="fisher")
+    try:
+        for seed in (1, 2, 3):
+            img = synthetic.gray(w, h, seed)
+            want = ctx.search_provider(img, p, method="fisher")
+            if seed == 3:
+                d = torch.from_numpy(img).cuda()
+                torch.cuda.synchronize()
+                plan.run_device(d.data_ptr())
+                got = plan.table()
+            else:
+                got = plan.run(img)
+            sizes = (16, 8, 4) + ((2,) if (w % 4 or h % 4) else ())
+            for size in sizes:
+                rows, cols = _grid(w, h, size) if size >= 4 else _border_twos(w, h)
+                if len(rows) == 0:
+                    continue
+                a, ae = got.search_many(rows, cols, size, 2)
+                b, be = want.search_many(rows, cols, size, 2)
+                assert a.tobytes() == b.tobytes(), (seed, size)
+                assert np.array_equal(ae, be), (seed, size)
+            assert plan.evals == int(mb.lib().mars_search_table_evals(want._h))
+            got.close()
+            want.close()
+    finally:
+        plan.close()
+
+
+def test_fisher_plan_refuses_planned_encodes(ctx):
+    plan = ctx.search_plan(64, 64, mb.make_params(min_size=4, max_size=16, shift=2, lam=200.0),
+                           method="fisher")
+    try:
+        with pytest.raises(mb.MarsError):
+            plan.encode(synthetic.gray(64, 64, 1))
+    finally:
+        plan.close()
