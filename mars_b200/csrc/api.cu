@@ -1240,7 +1240,8 @@ constexpr uint64_t kPlanCachePixels = 2048ull * 2048ull;
 constexpr size_t kPlanCacheSize = 8, kPlansSeen = 64;
 
 mars_search_plan* cached_encode_plan(mars_ctx* ctx, uint32_t w, uint32_t h,
-                                     const mars_params* p) {
+                                     const mars_params* p,
+                                     int32_t method = MARS_METHOD_EXHAUSTIVE) {
     static const bool off = [] {
         const char* e = std::getenv("MARS_PLAN_CACHE");
         return e && std::string(e) == "0";
@@ -1249,6 +1250,7 @@ mars_search_plan* cached_encode_plan(mars_ctx* ctx, uint32_t w, uint32_t h,
     std::string key(reinterpret_cast<const char*>(&w), sizeof w);
     key.append(reinterpret_cast<const char*>(&h), sizeof h);
     key.append(reinterpret_cast<const char*>(p), sizeof *p);
+    key.append(reinterpret_cast<const char*>(&method), sizeof method);
     std::lock_guard<std::mutex> lock(ctx->plan_cache_mu);
     for (auto& kp : ctx->plan_cache)
         if (kp.first == key) return kp.second;
@@ -1261,7 +1263,7 @@ mars_search_plan* cached_encode_plan(mars_ctx* ctx, uint32_t w, uint32_t h,
         return nullptr;
     }
     mars_search_plan* plan = nullptr;
-    if (mars_search_plan_create(ctx, w, h, p, &plan) != MARS_OK) return nullptr;
+    if (mars_indexed_plan_create(ctx, w, h, p, method, &plan) != MARS_OK) return nullptr;
     ctx->plan_cache.emplace_back(key, plan);
     return plan;
 }
@@ -1294,6 +1296,28 @@ int mars_encode(mars_ctx* ctx, const uint8_t* plane, uint32_t width, uint32_t he
         if (mars_search_plan* plan = cached_encode_plan(ctx, width, height, params))
             return mars_encode_planned(plan, plane, options, header, leaves, nleaves, residuals,
                                        nresiduals, counters);
+    // A Fisher encode of a geometry met before: the final walk's table from the context's
+    // Fisher plan, the warm-up walk's exhaustive table from its exhaustive plan.
+    if (options->method == MARS_METHOD_FISHER && rd_k == 1 && !adaptive) {
+        mars_params wp = *params;
+        wp.has_lambda = 0;
+        // Both keys are looked up on every call, so both plans are made on the second encode.
+        mars_search_plan* fplan = cached_encode_plan(ctx, width, height, params, MARS_METHOD_FISHER);
+        mars_search_plan* wplan =
+            params->has_lambda ? cached_encode_plan(ctx, width, height, &wp) : nullptr;
+        if (fplan && (!params->has_lambda || wplan)) {
+            mars_table* ft = nullptr;
+            mars_table* wt = nullptr;
+            if (int e = mars_search_plan_run(fplan, plane, &ft)) return e;
+            std::unique_ptr<mars_table, void (*)(mars_table*)> fguard(ft, mars_search_table_free);
+            if (wplan)
+                if (int e = mars_search_plan_run(wplan, plane, &wt)) return e;
+            std::unique_ptr<mars_table, void (*)(mars_table*)> wguard(wt, mars_search_table_free);
+            return encode_on_tables(ctx, plane, width, height, params, options, ft, wt ? wt : ft,
+                                    rd_k, header, leaves, nleaves, residuals, nresiduals,
+                                    counters);
+        }
+    }
     // The final walk's provider (the options' method) and, for an RD encode, the
     // exhaustive table the warm-up walk reads (the warm-up is exhaustive for every method).
     mars_table* table = nullptr;

@@ -204,3 +204,13 @@ def test_fisher_plan_refuses_planned_encodes(ctx):
             plan.encode(synthetic.gray(64, 64, 1))
     finally:
         plan.close()
+
+
+@pytest.mark.parametrize("lam", [None, 200.0])
+def test_fisher_encodes_through_cached_plans(ctx, lam):
+    # From a geometry's second Fisher encode on, mars_encode serves the final walk from the
+    # context's Fisher search plan and the warm-up walk from its exhaustive plan: the
+    # results stay the oracle's, plane after plane.
+    kw = dict(min_size=4, max_size=16, shift=2, lam=lam)
+    for seed in (11, 12, 13):
+        _encode_parity(ctx, synthetic.gray(96, 64, seed), kw, (1, 1, 1, 1))
