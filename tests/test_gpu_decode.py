@@ -219,7 +219,8 @@ def test_zoomed_decode_matches_the_oracle(ctx, factor):
     assert np.array_equal(got, orc.decode(ozh, ozl, 10))
 
 
-@pytest.mark.parametrize("w,h,seed", [(320, 256, 11), (1024, 768, 13), (516, 302, 14)])
+@pytest.mark.parametrize("w,h,seed", [(320, 256, 11), (1024, 768, 13), (516, 302, 14),
+                                      (2500, 300, 15), (2052, 148, 16)])
 def test_source_ordered_plan_steps_match_the_oracle(ctx, monkeypatch, w, h, seed):
     """The source-ordered steps large planes take (domain cells gathered in the order of their
     windows' source rows into a cell buffer, then placed in output order) give the cell
