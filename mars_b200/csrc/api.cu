@@ -383,15 +383,20 @@ int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32
             const int ms1 = mars::tc::msplit_for(g1, (int)n, ctx->num_sms, false);
             mars::Partial* part1 = nullptr;
             MARS_CUDA(sc.get(&part1, (size_t)ms1 * n));
-            MARS_CUDA(mars::tc::launch_corr(maps1, d_b, g1, (int)n, rs, ds1, fp, d_seed, part1, ms1,
-                                            false, ctx->d_err, ctx->d_counter, st));
+            MARS_CUDA(mars::tc::launch_corr(maps1, d_b, g1, (int)n, rs, ds1, fp, d_seed, part1,
+                                            nullptr, ms1, false, ctx->d_err, ctx->d_counter, st));
             MARS_CUDA(mars::tc::launch_seed_merge(part1, ms1, (int)n, g1.ncol_d, g.ncol_d, kRatio,
                                                   d_seed, st));
             ctx->launches += 4;
         }
     }
-    MARS_CUDA(mars::tc::launch_corr(maps, d_b, g, (int)n, rs, ds, fp, d_seed, partials, msplit,
-                                    digits, ctx->d_err, ctx->d_counter, st));
+    // The M-splits' shared champion records (rms bits, index, t1_x4), worse than any real
+    // candidate to begin with.
+    unsigned long long* gch = nullptr;
+    MARS_CUDA(sc.get(&gch, 2 * n));
+    MARS_CUDA(cudaMemsetAsync(gch, 0xFF, 2 * n * sizeof(unsigned long long), st));
+    MARS_CUDA(mars::tc::launch_corr(maps, d_b, g, (int)n, rs, ds, fp, d_seed, partials, gch,
+                                    msplit, digits, ctx->d_err, ctx->d_counter, st));
     MARS_CUDA(mars::tc::launch_finish(partials, msplit, (int)n, g, rs, ds, fp, d_out, st));
     ctx->launches += 5;
     return MARS_OK;

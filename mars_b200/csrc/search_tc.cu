@@ -182,13 +182,31 @@ __device__ __forceinline__ void publish_threshold(Smem& sm, int rl, const FitPar
     sm.thr[rl] = t;
 }
 
+// 128-bit compare-and-swap on a global record (two 64-bit halves); returns the old value.
+// With cmp = val = 0 it is an atomic read.
+__device__ __forceinline__ void cas128(unsigned long long* addr, unsigned long long clo,
+                                       unsigned long long chi, unsigned long long vlo,
+                                       unsigned long long vhi, unsigned long long& olo,
+                                       unsigned long long& ohi) {
+    asm volatile(
+        "{\n\t.reg .b128 c, v, o;\n\t"
+        "mov.b128 c, {%2, %3};\n\t"
+        "mov.b128 v, {%4, %5};\n\t"
+        "atom.global.cas.b128 o, [%6], c, v;\n\t"
+        "mov.b128 {%0, %1}, o;\n\t}"
+        : "=l"(olo), "=l"(ohi)
+        : "l"(clo), "l"(chi), "l"(vlo), "l"(vhi), "l"(addr)
+        : "memory");
+}
+
 // Exact fits of every queued survivor, then the per-range winners of the batch (atomic
 // min on the f64 bit pattern of rms >= 0, then on the reference index) and the champion /
 // threshold update.  All epilogue threads call this together.
 template <int N, int NT, int RG>
 __device__ __noinline__ void drain_queue(Smem& sm, int grp, int n, bool mark, uint32_t tag,
                                          int gt, const DomainStats& ds, const FitParams& fp,
-                                         unsigned long long& exact) {
+                                         unsigned long long& exact, unsigned long long* gch,
+                                         int rbase) {
     QEntry* const queue = sm.queue[grp];
     for (int qi = gt; qi < n; qi += kGroupThreads) {
         QEntry& q = queue[qi];
@@ -242,6 +260,40 @@ __device__ __noinline__ void drain_queue(Smem& sm, int grp, int n, bool mark, ui
         sm.key_rms[rl] = ~0ull;
         sm.key_idx[rl] = UINT32_MAX;
     }
+    // The M-splits of a range share their champions through one global record per range
+    // (rms bits, reference index, t1_x4): publish ours when better, adopt the record when
+    // it is better.  An adopted champion is a real candidate of another split; its fit sum
+    // is recomputed exactly from its domain statistics.
+    if (gt < RG && gch && sm.ch[rl].valid) {
+        Champ& C = sm.ch[rl];
+        unsigned long long* rec = gch + 2 * (size_t)(rbase + rl);
+        unsigned long long clo, chi;
+        cas128(rec, 0ull, 0ull, 0ull, 0ull, clo, chi);
+        for (int tries = 0; tries < 64; ++tries) {
+            const unsigned long long mlo = (unsigned long long)__double_as_longlong(C.rms);
+            const uint32_t gidx = (uint32_t)chi;
+            if (mlo < clo || (mlo == clo && C.idx < gidx)) {
+                const unsigned long long vhi = (unsigned long long)C.idx |
+                                               (unsigned long long)(uint32_t)C.t1x4 << 32;
+                unsigned long long olo, ohi;
+                cas128(rec, clo, chi, mlo, vhi, olo, ohi);
+                if (olo == clo && ohi == chi) break;
+                clo = olo;
+                chi = ohi;
+            } else {
+                if (clo < mlo || (clo == mlo && gidx < C.idx)) {
+                    const uint32_t dom = gidx >> 3;
+                    C.rms = __longlong_as_double((long long)clo);
+                    C.idx = gidx;
+                    C.t1x4 = (int32_t)(uint32_t)(chi >> 32);
+                    C.sum = fit_exact(N, ds.s1x4[dom], ds.s2x16[dom], C.t0, (int64_t)C.t1x4,
+                                      C.t2, fp).sum;
+                    publish_threshold(sm, rl, fp, N);
+                }
+                break;
+            }
+        }
+    }
     if (gt == 0) sm.qcount[grp] = 0;
     group_barrier(grp);
 }
@@ -251,7 +303,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     corr_tc_kernel(const __grid_constant__ TcMaps maps, const uint8_t* __restrict__ bglob,
                    LevelGeom g, int nranges, RangeStats rs, DomainStats ds, FitParams fp,
                    const SeedOut* __restrict__ seeds, int m_tiles, int m_per_cta,
-                   Partial* __restrict__ partials, int* __restrict__ err,
+                   Partial* __restrict__ partials, unsigned long long* __restrict__ gch,
+                   int* __restrict__ err,
                    unsigned long long* __restrict__ exact_counter) {
     using C_ = Cfg<S, DIG>;
     constexpr int N = S * S;
@@ -608,13 +661,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const bool last = mt + 1 == m_end;
                 if (queued > kQueueCap) {
                     drain_queue<N, NT, kRangesPerWarp>(sm, part, kQueueCap, true, tag, gt, ds,
-                                                       fp, exact);
+                                                       fp, exact, gch, ntile * RT);
                     rescan = true;
                     continue;  // pass again over the same accumulator (fresh thresholds)
                 }
                 if (queued >= kFlush || (last && queued > 0))
                     drain_queue<N, NT, kRangesPerWarp>(sm, part, queued, false, tag, gt, ds,
-                                                       fp, exact);
+                                                       fp, exact, gch, ntile * RT);
                 break;
             }
             if (rescan) {
@@ -1040,8 +1093,8 @@ static_assert(smem_bytes<4, false>() <= 232448 && smem_bytes<8, false>() <= 2324
 template <int S, bool DIG>
 cudaError_t launch_t(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
                      RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
-                     Partial* partials, int msplit, int* err, unsigned long long* counter,
-                     cudaStream_t st) {
+                     Partial* partials, unsigned long long* gch, int msplit, int* err,
+                     unsigned long long* counter, cudaStream_t st) {
     const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
     const int m_tiles = g.nrow_d * tiles_per_row;
     const int m_per_cta = (m_tiles + msplit - 1) / msplit;
@@ -1052,7 +1105,7 @@ cudaError_t launch_t(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& 
     if (e != cudaSuccess) return e;
     dim3 grid(ntiles, msplit);
     kern<<<grid, kThreads, smem, st>>>(maps, bglob, g, nranges, rs, ds, fp, seeds, m_tiles,
-                                      m_per_cta, partials, err, counter);
+                                      m_per_cta, partials, gch, err, counter);
     return cudaGetLastError();
 }
 
@@ -1194,10 +1247,11 @@ int msplit_for(const LevelGeom& g, int nranges, int num_sms, bool digits) {
 
 cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
                         RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
-                        Partial* partials, int msplit, bool digits, int* err,
-                        unsigned long long* counter, cudaStream_t st) {
+                        Partial* partials, unsigned long long* gch, int msplit, bool digits,
+                        int* err, unsigned long long* counter, cudaStream_t st) {
 #define MARS_CORR(S_, D_) \
-    launch_t<S_, D_>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, msplit, err, counter, st)
+    launch_t<S_, D_>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, gch, msplit, err, \
+                     counter, st)
     if (digits) {
         switch (g.size) {
             case 16: return MARS_CORR(16, true);

@@ -57,8 +57,8 @@ cudaError_t launch_seed(const int32_t* D, const LevelGeom& g, const uint8_t* pla
                         DomainStats ds, const FitParams& fp, SeedOut* out, cudaStream_t st);
 cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
                         RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
-                        Partial* partials, int msplit, bool digits, int* err,
-                        unsigned long long* counter, cudaStream_t st);
+                        Partial* partials, unsigned long long* gch, int msplit, bool digits,
+                        int* err, unsigned long long* counter, cudaStream_t st);
 cudaError_t launch_seed_merge(const Partial* partials, int nsplit, int nranges, int coarse_ncol,
                               int fine_ncol, int ratio, SeedOut* seeds, cudaStream_t st);
 cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,
