@@ -133,7 +133,8 @@ uint64_t mars_ctx_launch_count(const mars_ctx* ctx);
  * tensor-core path never serves a level it does not support), 3 = automatic with the
  * tensor-core operand loads split into per-phase boxes and the 2x2 box folded into K at
  * every block size, 4 = automatic with the fold at every block size (no split-digit
- * contracted operand at sizes 16..64).  Results are identical. */
+ * contracted operand at sizes 16..64), 5 = automatic with one correlation launch per level
+ * (no all-levels persistent launch in search plans and tables).  Results are identical. */
 int mars_ctx_set_search_path(mars_ctx* ctx, int32_t path);
 
 /* The provider factory (encode.rs:1076): search every quadtree node an encode of this

@@ -340,10 +340,13 @@ class Context:
     def set_search_path(self, path: str) -> None:
         """'auto' (tensor cores wherever a level allows), 'simt' (CUDA cores only), 'boxes'
         (tensor cores, operand stages loaded as per-phase boxes, the 2x2 box folded into K
-        at every size) or 'fold' (tensor cores, the fold at every size instead of the
-        split-digit contracted operand at sizes 16..64)."""
+        at every size), 'fold' (tensor cores, the fold at every size instead of the
+        split-digit contracted operand at sizes 16..64) or 'per_level' (tensor cores, one
+        correlation launch per level instead of the all-levels persistent launch of search
+        plans and tables)."""
         check(lib().mars_ctx_set_search_path(self._h, {"auto": 0, "simt": 1, "tc": 2,
-                                                       "boxes": 3, "fold": 4}[path]))
+                                                       "boxes": 3, "fold": 4,
+                                                       "per_level": 5}[path]))
 
     @property
     def launches(self) -> int:

@@ -325,80 +325,144 @@ bool make_digit_maps(mars_ctx* ctx, const uint8_t* d_digits, uint32_t w, uint32_
     return true;
 }
 
-// The tcgen05 path for one level: phase copies of the plane (or, for block sizes 16..64,
-// digit phase copies of the contracted plane), the B operand, seed champions, the
-// correlation + exact-bound kernel, and the final champion per block.
+// A tensor-core level set up for its correlation: buffers taken from a Scratch, tensor
+// maps, split count, and the coarse pre-pass of block size 8.
+struct TcLevel {
+    mars::LevelGeom g{};
+    size_t n = 0;
+    bool digits = false;
+    int msplit = 1;
+    mars::RangeStats rs{};
+    mars::DomainStats ds{};
+    uint8_t* d_phases = nullptr;
+    uint8_t* d_b = nullptr;
+    mars::tc::SeedOut* d_seed = nullptr;
+    mars::tc::TcMaps maps{};
+    mars::Partial* partials = nullptr;
+    unsigned long long* gch = nullptr;
+    int* tickets = nullptr;  // all-levels launch only
+    int tail_tiles = 0, tail_msplit = 0;  // all-levels launch: the finer-split tail
+    bool coarse = false;
+    mars::LevelGeom g1{};
+    mars::DomainStats ds1{};
+    uint8_t* d_ph1 = nullptr;
+    mars::tc::TcMaps maps1{};
+    int ms1 = 1;
+    mars::Partial* part1 = nullptr;
+};
+
+// Whether a level takes the split-digit operand (block sizes 16..64 unless pinned off).
+bool tc_digits(const mars_ctx* ctx, const mars::LevelGeom& g) {
+    return mars::tc::digits_supported(g.size, g.shift) && !ctx->tma_16_boxes && !ctx->fold_only;
+}
+
+// Coarse pre-pass at block size 8: the same search over every 4th domain position of each
+// axis, whose champions seed the full sweep (tighter thresholds from the first tile: exact
+// fits of the 512x512 level 1.09 M -> 0.23 M, 0.98 -> 0.86 ms).  At size 4 its cost
+// outweighs the survivors it saves, and at 16..64 it is neutral or slower.
+constexpr int kCoarseRatio = 4;
+
+// Buffers and tensor maps of a level (g, rs and ds already set).  msplit 0 picks the
+// per-level launch's split count; tickets adds the all-levels launch's per-tile counters;
+// coarse_ok allows the coarse pre-pass (the all-levels launch leaves it out: the pre-pass
+// would sit on the path before the one launch, 0.16 ms at 512 x 512, more than the 0.12 ms
+// of correlation it saves).
+// A level whose digit views the driver rejects takes the fold path (L.digits false).
+int tc_level_setup(mars_ctx* ctx, Scratch& sc, uint32_t w, uint32_t h, size_t n, int msplit,
+                   bool tickets, bool coarse_ok, TcLevel& L) {
+    const mars::LevelGeom& g = L.g;
+    L.n = n;
+    L.digits = tc_digits(ctx, g);
+    if (L.digits) {
+        MARS_CUDA(sc.get(&L.d_phases, mars::tc::digit_plane_bytes((int)w, (int)h, g.shift)));
+        L.digits = make_digit_maps(ctx, L.d_phases, w, h, (uint32_t)g.shift, &L.maps);
+    }
+    if (!L.digits) {
+        MARS_CUDA(sc.get(&L.d_phases, mars::tc::phase_bytes((int)w, (int)h, g.shift)));
+        if (int e = make_maps(ctx, L.d_phases, w, h, (uint32_t)g.shift, &L.maps)) return e;
+    }
+    MARS_CUDA(sc.get(&L.d_b, mars::tc::b_bytes(g.size, (int)n, L.digits)));
+    MARS_CUDA(sc.get(&L.d_seed, n));
+    L.msplit = msplit > 0 ? msplit : mars::tc::msplit_for(g, (int)n, ctx->num_sms, L.digits);
+    MARS_CUDA(sc.get(&L.partials, (size_t)L.msplit * n));
+    // The M-splits' shared champion records (rms bits, index, t1_x4).
+    MARS_CUDA(sc.get(&L.gch, 2 * n));
+    if (tickets) {
+        const int rt = mars::tc::ranges_per_tile(L.digits);
+        MARS_CUDA(sc.get(&L.tickets, (n + rt - 1) / rt));
+    }
+    L.coarse = false;
+    if (coarse_ok && !L.digits && g.size == 8 && g.shift * kCoarseRatio <= 16 && n >= 256) {
+        L.g1 = level_geom(w, h, (uint32_t)g.size, (uint32_t)(g.shift * kCoarseRatio));
+        if (L.g1.nrow_d > 0 && L.g1.ncol_d > 0) {
+            L.coarse = true;
+            const size_t ndom1 = (size_t)L.g1.nrow_d * L.g1.ncol_d;
+            MARS_CUDA(sc.get(&L.ds1.s1x4, ndom1));
+            MARS_CUDA(sc.get(&L.ds1.s2x16, ndom1));
+            MARS_CUDA(sc.get(&L.ds1.detf, ndom1));
+            MARS_CUDA(sc.get(&L.ds1.sdetf, ndom1));
+            MARS_CUDA(sc.get(&L.d_ph1, mars::tc::phase_bytes((int)w, (int)h, L.g1.shift)));
+            if (int e = make_maps(ctx, L.d_ph1, w, h, (uint32_t)L.g1.shift, &L.maps1)) return e;
+            L.ms1 = mars::tc::msplit_for(L.g1, (int)n, ctx->num_sms, false);
+            MARS_CUDA(sc.get(&L.part1, (size_t)L.ms1 * n));
+        }
+    }
+    return MARS_OK;
+}
+
+// Everything of a level before its correlation, on stream st: phase (or digit phase)
+// copies, the B operand, seed champions, the coarse pre-pass, the shared champion records
+// and tickets.
+int tc_level_prep(mars_ctx* ctx, const TcLevel& L, const uint8_t* d_plane, const int32_t* d_D,
+                  const uint8_t* d_dplane, uint32_t w, uint32_t h, const mars::FitParams& fp,
+                  const uint32_t* d_rows, const uint32_t* d_cols, cudaStream_t st) {
+    const mars::LevelGeom& g = L.g;
+    const int n = (int)L.n;
+    if (L.digits)
+        MARS_CUDA(mars::tc::launch_digit_planes(d_D, (int)w, (int)h, g.shift, L.d_phases, st));
+    else
+        MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, g.shift, L.d_phases, st));
+    MARS_CUDA(mars::tc::launch_build_b(g.size, d_plane, (int)w, (int)h, d_rows, d_cols, n, L.d_b,
+                                       L.digits, st));
+    MARS_CUDA(mars::tc::launch_seed(d_D, g, d_plane, (int)w, d_rows, d_cols, n, L.rs, L.ds, fp,
+                                    L.d_seed, st));
+    ctx->launches += 3;
+    if (L.coarse) {
+        MARS_CUDA(mars::launch_domain_stats(d_D, L.g1, L.ds1, st));
+        MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, L.g1.shift, L.d_ph1, st));
+        MARS_CUDA(mars::tc::launch_corr(L.maps1, L.d_b, L.g1, n, L.rs, L.ds1, fp, L.d_seed,
+                                        L.part1, nullptr, L.ms1, false, ctx->d_err,
+                                        ctx->d_counter, st));
+        MARS_CUDA(mars::tc::launch_seed_merge(L.part1, L.ms1, n, L.g1.ncol_d, g.ncol_d,
+                                              kCoarseRatio, L.d_seed, st));
+        ctx->launches += 4;
+    }
+    MARS_CUDA(cudaMemsetAsync(L.gch, 0xFF, 2 * L.n * sizeof(unsigned long long), st));
+    if (L.tickets) {
+        const int rt = mars::tc::ranges_per_tile(L.digits);
+        MARS_CUDA(cudaMemsetAsync(L.tickets, 0, (L.n + rt - 1) / rt * sizeof(int), st));
+    }
+    return MARS_OK;
+}
+
+// The tcgen05 path for one level: set-up, the correlation + exact-bound kernel, and the
+// final champion per block.
 int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t* d_D,
                  uint32_t w, uint32_t h, const mars::LevelGeom& g, const mars::FitParams& fp,
                  const uint32_t* d_rows, const uint32_t* d_cols, size_t n, mars::RangeStats rs,
                  mars::DomainStats ds, mars::CandidateOut* d_out, const uint8_t* d_dplane) {
     const cudaStream_t st = ctx->stream;
-    uint8_t* d_phases = nullptr;
-    uint8_t* d_b = nullptr;
-    mars::tc::SeedOut* d_seed = nullptr;
-    mars::tc::TcMaps maps;
-    bool digits = mars::tc::digits_supported(g.size, g.shift) && !ctx->tma_16_boxes &&
-                  !ctx->fold_only;
-    if (digits) {
-        MARS_CUDA(sc.get(&d_phases, mars::tc::digit_plane_bytes((int)w, (int)h, g.shift)));
-        digits = make_digit_maps(ctx, d_phases, w, h, (uint32_t)g.shift, &maps);
-    }
-    if (!digits) {
-        MARS_CUDA(sc.get(&d_phases, mars::tc::phase_bytes((int)w, (int)h, g.shift)));
-        if (int e = make_maps(ctx, d_phases, w, h, (uint32_t)g.shift, &maps)) return e;
-    }
-    MARS_CUDA(sc.get(&d_b, mars::tc::b_bytes(g.size, (int)n, digits)));
-    MARS_CUDA(sc.get(&d_seed, n));
-    const int msplit = mars::tc::msplit_for(g, (int)n, ctx->num_sms, digits);
-    mars::Partial* partials = nullptr;
-    MARS_CUDA(sc.get(&partials, (size_t)msplit * n));
-    if (digits)
-        MARS_CUDA(mars::tc::launch_digit_planes(d_D, (int)w, (int)h, g.shift, d_phases, st));
-    else
-        MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, g.shift, d_phases, st));
-    MARS_CUDA(mars::tc::launch_build_b(g.size, d_plane, (int)w, (int)h, d_rows, d_cols, (int)n,
-                                       d_b, digits, st));
-    MARS_CUDA(mars::tc::launch_seed(d_D, g, d_plane, (int)w, d_rows, d_cols, (int)n, rs, ds, fp,
-                                    d_seed, st));
-    // Coarse pre-pass at block size 8: the same search over every 4th domain position of
-    // each axis, whose champions seed the full sweep (tighter thresholds from the first
-    // tile: exact fits of the 512x512 level 1.09 M -> 0.23 M, 0.98 -> 0.86 ms).  At size 4
-    // its cost outweighs the survivors it saves, and at 16..64 it is neutral or slower.
-    constexpr int kRatio = 4;
-    if (!digits && g.size == 8 && g.shift * kRatio <= 16 && n >= 256) {
-        const mars::LevelGeom g1 = level_geom(w, h, (uint32_t)g.size, (uint32_t)(g.shift * kRatio));
-        if (g1.nrow_d > 0 && g1.ncol_d > 0) {
-            const size_t ndom1 = (size_t)g1.nrow_d * g1.ncol_d;
-            mars::DomainStats ds1;
-            MARS_CUDA(sc.get(&ds1.s1x4, ndom1));
-            MARS_CUDA(sc.get(&ds1.s2x16, ndom1));
-            MARS_CUDA(sc.get(&ds1.detf, ndom1));
-            MARS_CUDA(sc.get(&ds1.sdetf, ndom1));
-            MARS_CUDA(mars::launch_domain_stats(d_D, g1, ds1, st));
-            uint8_t* d_ph1 = nullptr;
-            mars::tc::TcMaps maps1;
-            MARS_CUDA(sc.get(&d_ph1, mars::tc::phase_bytes((int)w, (int)h, g1.shift)));
-            if (int e = make_maps(ctx, d_ph1, w, h, (uint32_t)g1.shift, &maps1)) return e;
-            MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, g1.shift, d_ph1, st));
-            const int ms1 = mars::tc::msplit_for(g1, (int)n, ctx->num_sms, false);
-            mars::Partial* part1 = nullptr;
-            MARS_CUDA(sc.get(&part1, (size_t)ms1 * n));
-            MARS_CUDA(mars::tc::launch_corr(maps1, d_b, g1, (int)n, rs, ds1, fp, d_seed, part1,
-                                            nullptr, ms1, false, ctx->d_err, ctx->d_counter, st));
-            MARS_CUDA(mars::tc::launch_seed_merge(part1, ms1, (int)n, g1.ncol_d, g.ncol_d, kRatio,
-                                                  d_seed, st));
-            ctx->launches += 4;
-        }
-    }
-    // The M-splits' shared champion records (rms bits, index, t1_x4), worse than any real
-    // candidate to begin with.
-    unsigned long long* gch = nullptr;
-    MARS_CUDA(sc.get(&gch, 2 * n));
-    MARS_CUDA(cudaMemsetAsync(gch, 0xFF, 2 * n * sizeof(unsigned long long), st));
-    MARS_CUDA(mars::tc::launch_corr(maps, d_b, g, (int)n, rs, ds, fp, d_seed, partials, gch,
-                                    msplit, digits, ctx->d_err, ctx->d_counter, st));
-    MARS_CUDA(mars::tc::launch_finish(partials, msplit, (int)n, g, rs, ds, fp, d_out, st));
-    ctx->launches += 5;
+    TcLevel L;
+    L.g = g;
+    L.rs = rs;
+    L.ds = ds;
+    if (int e = tc_level_setup(ctx, sc, w, h, n, 0, false, true, L)) return e;
+    if (int e = tc_level_prep(ctx, L, d_plane, d_D, d_dplane, w, h, fp, d_rows, d_cols, st))
+        return e;
+    MARS_CUDA(mars::tc::launch_corr(L.maps, L.d_b, g, (int)n, rs, ds, fp, L.d_seed, L.partials,
+                                    L.gch, L.msplit, L.digits, ctx->d_err, ctx->d_counter, st));
+    MARS_CUDA(mars::tc::launch_finish(L.partials, L.msplit, (int)n, g, rs, ds, fp, d_out, st));
+    ctx->launches += 2;
     return MARS_OK;
 }
 
@@ -561,6 +625,192 @@ int run_jobs(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uin
         if (e) return e;
         off += j.rows.size();
     }
+    return MARS_OK;
+}
+
+// Whether the exhaustive single-candidate search of `jobs` runs its tensor-core levels as
+// one all-levels persistent launch: not pinned off (mars_ctx_set_search_path 5 or the
+// MARS_LEVEL_LAUNCH=per_level environment variable), every tensor-core level a kind the
+// kernel holds, at most kMaxLevelJobs of them.
+bool all_levels_eligible(const mars_ctx* ctx, uint32_t w, uint32_t h, const std::vector<Job>& jobs) {
+    static const bool env_per_level = [] {
+        const char* e = std::getenv("MARS_LEVEL_LAUNCH");
+        return e && std::string(e) == "per_level";
+    }();
+    if (ctx->per_level || env_per_level) return false;
+    int levels = 0;
+    for (const Job& j : jobs) {
+        if (j.rows.empty() || !use_tc(ctx, j.size, j.shift)) continue;
+        const mars::LevelGeom g = level_geom(w, h, j.size, j.shift);
+        if (g.nrow_d <= 0 || g.ncol_d <= 0) continue;
+        if (!mars::tc::all_levels_supported(g.size, tc_digits(ctx, g))) return false;
+        ++levels;
+    }
+    return levels > 0 && levels < mars::tc::kMaxLevelJobs;  // a level may add a tail job
+}
+
+// run_jobs for the exhaustive single-candidate search with the correlation of every
+// tensor-core level in one persistent launch (launch_corr_all, which also writes the
+// levels' final candidates).  Every buffer is taken on the context's stream before the
+// fork; each level's statistics, operands and seeds (and every other level, whole) then
+// run on one of the branch streams; the persistent launch follows the join.  The caller
+// holds ctx->mu and has checked all_levels_eligible.
+int run_jobs_all_levels(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w,
+                        uint32_t h, const mars::FitParams& fp, const std::vector<Job>& jobs,
+                        mars::CandidateOut* d_out, const uint32_t* d_rc_in) {
+    const cudaStream_t main = ctx->stream;
+    if (!ctx->fork_ev) {
+        MARS_CUDA(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+        for (int b = 0; b < mars_ctx::kBranches; ++b) {
+            MARS_CUDA(cudaStreamCreateWithFlags(&ctx->branch[b], cudaStreamNonBlocking));
+            MARS_CUDA(cudaEventCreateWithFlags(&ctx->join_ev[b], cudaEventDisableTiming));
+        }
+    }
+    int32_t* d_D = nullptr;
+    MARS_CUDA(sc.get(&d_D, std::max<size_t>(1, (size_t)(w / 2) * (h / 2))));
+    MARS_CUDA(mars::launch_contract(d_plane, (int)w, (int)h, d_D, main));
+    ctx->launches += 1;
+    size_t total = 0;
+    const uint32_t* d_rc = d_rc_in;
+    if (!d_rc) {
+        const std::vector<uint32_t> rc = job_origins(jobs, &total);
+        uint32_t* d = nullptr;
+        MARS_CUDA(sc.get(&d, rc.size()));
+        MARS_CUDA(cudaMemcpyAsync(d, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice, main));
+        d_rc = d;
+    } else {
+        for (const Job& j : jobs) total += j.rows.size();
+    }
+    // Which jobs are all-levels levels, and their split counts (chosen together).
+    std::vector<int> level_of(jobs.size(), -1);
+    std::vector<TcLevel> lv;
+    std::vector<size_t> lv_off;
+    {
+        size_t off = 0;
+        for (size_t i = 0; i < jobs.size(); ++i) {
+            const Job& j = jobs[i];
+            const mars::LevelGeom g = level_geom(w, h, j.size, j.shift);
+            if (!j.rows.empty() && use_tc(ctx, j.size, j.shift) && g.nrow_d > 0 && g.ncol_d > 0) {
+                level_of[i] = (int)lv.size();
+                TcLevel L;
+                L.g = g;
+                L.n = j.rows.size();
+                L.digits = tc_digits(ctx, g);
+                lv.push_back(L);
+                lv_off.push_back(off);
+            }
+            off += j.rows.size();
+        }
+    }
+    const int nl = (int)lv.size();
+    std::vector<mars::LevelGeom> gs(nl);
+    std::vector<int> ns(nl), ms(nl), tail_t(nl), tail_ms(nl);
+    std::unique_ptr<bool[]> dg(new bool[std::max(1, nl)]);
+    for (int l = 0; l < nl; ++l) {
+        gs[l] = lv[l].g;
+        ns[l] = (int)lv[l].n;
+        dg[l] = lv[l].digits;
+    }
+    mars::tc::all_levels_splits(gs.data(), ns.data(), dg.get(), nl, ctx->num_sms, ms.data(),
+                                tail_t.data(), tail_ms.data());
+    for (int l = 0; l < nl; ++l) {
+        TcLevel& L = lv[l];
+        const size_t n = L.n;
+        const size_t ndom = (size_t)L.g.nrow_d * L.g.ncol_d;
+        MARS_CUDA(sc.get(&L.rs.t0, n));
+        MARS_CUDA(sc.get(&L.rs.t2, n));
+        MARS_CUDA(sc.get(&L.rs.nrr, n));
+        MARS_CUDA(sc.get(&L.rs.sum0, n));
+        MARS_CUDA(sc.get(&L.rs.rms0, n));
+        MARS_CUDA(sc.get(&L.ds.s1x4, ndom));
+        MARS_CUDA(sc.get(&L.ds.s2x16, ndom));
+        MARS_CUDA(sc.get(&L.ds.detf, ndom));
+        MARS_CUDA(sc.get(&L.ds.sdetf, ndom));
+        const bool wanted = L.digits;
+        if (int e = tc_level_setup(ctx, sc, w, h, n, std::max(ms[l], tail_ms[l]), true, false, L))
+            return e;
+        if (L.digits != wanted)  // the driver rejected the digit views: no fold kernel here
+            return fail(MARS_ECUDA, "the split-digit tensor maps were rejected");
+        L.msplit = ms[l];
+        L.tail_tiles = tail_t[l];
+        L.tail_msplit = tail_ms[l];
+    }
+    int* d_work = nullptr;
+    MARS_CUDA(sc.get(&d_work, 1));
+    MARS_CUDA(cudaEventRecord(ctx->fork_ev, main));
+    const int nb = (int)std::min<size_t>(jobs.size(), mars_ctx::kBranches);
+    for (int b = 0; b < nb; ++b) MARS_CUDA(cudaStreamWaitEvent(ctx->branch[b], ctx->fork_ev, 0));
+    int err = MARS_OK;
+    size_t off = 0;
+    for (size_t i = 0; i < jobs.size() && !err; ++i) {
+        const Job& j = jobs[i];
+        const int b = (int)(i % mars_ctx::kBranches);
+        const cudaStream_t bs = ctx->branch[b];
+        const uint32_t* rows = d_rc + off;
+        const uint32_t* cols = d_rc + total + off;
+        const int l = level_of[i];
+        if (l >= 0) {
+            TcLevel& L = lv[l];
+            const mars::LevelGeom& g = L.g;
+            if (cudaError_t ce = mars::launch_range_stats(d_plane, (int)w, (int)h, rows, cols,
+                                                          (int)L.n, g.size, fp, L.rs, bs)) {
+                err = fail(MARS_ECUDA, cudaGetErrorString(ce));
+            } else if (cudaError_t ce2 = mars::launch_domain_stats(d_D, g, L.ds, bs)) {
+                err = fail(MARS_ECUDA, cudaGetErrorString(ce2));
+            } else {
+                ctx->launches += 2;
+                err = tc_level_prep(ctx, L, d_plane, d_D, d_plane, w, h, fp, rows, cols, bs);
+            }
+        } else {
+            ctx->stream = bs;
+            {
+                Scratch sb(bs);
+                err = run_level(ctx, sb, d_plane, d_D, w, h, j.size, j.shift, fp, rows, cols,
+                                j.rows.size(), d_out + off, 1);
+            }
+            ctx->stream = main;
+        }
+        off += j.rows.size();
+    }
+    // Join every branch that was forked, also after an error (a capture must end joined).
+    for (int b = 0; b < nb; ++b) {
+        MARS_CUDA(cudaEventRecord(ctx->join_ev[b], ctx->branch[b]));
+        MARS_CUDA(cudaStreamWaitEvent(main, ctx->join_ev[b], 0));
+    }
+    if (err) return err;
+    std::vector<mars::tc::LevelJob> lj;
+    for (int l = 0; l < nl; ++l) {
+        const TcLevel& L = lv[l];
+        mars::tc::LevelJob J;
+        J.maps = L.maps;
+        J.bglob = L.d_b;
+        J.g = L.g;
+        J.nranges = (int)L.n;
+        J.rs = L.rs;
+        J.ds = L.ds;
+        J.fp = fp;
+        J.seeds = L.d_seed;
+        J.partials = L.partials;
+        J.gch = L.gch;
+        J.tickets = L.tickets;
+        J.out = d_out + lv_off[l];
+        const int rt = mars::tc::ranges_per_tile(L.digits);
+        const int ntiles = (int)((L.n + rt - 1) / rt);
+        J.digits = L.digits ? 1 : 0;
+        J.tile_begin = 0;
+        J.tile_count = ntiles - L.tail_tiles;
+        J.msplit = L.msplit;
+        lj.push_back(J);
+        if (L.tail_tiles > 0) {
+            J.tile_begin = ntiles - L.tail_tiles;
+            J.tile_count = L.tail_tiles;
+            J.msplit = L.tail_msplit;
+            lj.push_back(J);
+        }
+    }
+    MARS_CUDA(mars::tc::launch_corr_all(lj.data(), (int)lj.size(), d_work, ctx->d_err,
+                                        ctx->d_counter, ctx->num_sms, main));
+    ctx->launches += 1;
     return MARS_OK;
 }
 
@@ -783,6 +1033,9 @@ int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, 
             if (int e = run_jobs_fisher(ctx, sc, d_plane, w, h, fp, jobs, d_out, d_evals)) return e;
             MARS_CUDA(cudaMemcpyAsync(t->evals.data(), d_evals, total * sizeof(uint64_t),
                                       cudaMemcpyDeviceToHost, ctx->stream));
+        } else if (k == 1 && all_levels_eligible(ctx, w, h, jobs)) {
+            if (int e = run_jobs_all_levels(ctx, sc, d_plane, w, h, fp, jobs, d_out, nullptr))
+                return e;
         } else {
             if (int e = run_jobs(ctx, sc, d_plane, w, h, fp, jobs, d_out, k)) return e;
         }
@@ -892,11 +1145,12 @@ int mars_ctx_set_stream(mars_ctx* ctx, void* stream) {
 uint64_t mars_ctx_launch_count(const mars_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
 
 int mars_ctx_set_search_path(mars_ctx* ctx, int32_t path) {
-    if (!ctx || path < 0 || path > 4) return fail(MARS_EINVAL, "path must be 0 .. 4");
+    if (!ctx || path < 0 || path > 5) return fail(MARS_EINVAL, "path must be 0 .. 5");
     std::lock_guard<std::mutex> lock(ctx->mu);
     ctx->search_path = path >= 3 ? 0 : path;
     ctx->tma_16_boxes = path == 3;
     ctx->fold_only = path == 4;
+    ctx->per_level = path == 5;
     return MARS_OK;
 }
 
@@ -1472,6 +1726,10 @@ int plan_enqueue(mars_search_plan* p, bool with_copies) {
     if (p->method == MARS_METHOD_FISHER) {
         if (int e = run_jobs_fisher(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out,
                                     p->d_evals, p->d_rc))
+            return e;
+    } else if (all_levels_eligible(ctx, p->w, p->h, p->jobs)) {
+        if (int e = run_jobs_all_levels(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out,
+                                        p->d_rc))
             return e;
     } else if (int e = run_jobs_branched(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out,
                                          p->d_rc)) {

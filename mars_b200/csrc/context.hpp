@@ -27,6 +27,7 @@ struct mars_ctx {
     int search_path = 0;                      // 0 auto, 1 CUDA cores only, 2 tensor cores
     bool tma_16_boxes = false;                // load A stages as 16 2-D boxes (A/B checks)
     bool fold_only = false;                   // no split-digit operand at sizes 16..64 (A/B)
+    bool per_level = false;                   // one correlation launch per level (A/B)
     PFN_cuTensorMapEncodeTiled_v12000 encode_tiled = nullptr;
     // Streams and events a search plan's capture forks its levels onto (created on first use;
     // the levels of a plane run as parallel branches of the plan's graph).

@@ -52,6 +52,21 @@ __global__ void contract_kernel(const uint8_t* __restrict__ plane, int w, int dw
     out[(size_t)r * dw + c] = (int32_t)p0[0] + (int32_t)p0[1] + (int32_t)p1[0] + (int32_t)p1[1];
 }
 
+__device__ __forceinline__ void store_domain_stats(DomainStats& ds, int idx, int64_t n,
+                                                   int64_t s1, int64_t s2) {
+    const int64_t det16 = n * s2 - s1 * s1;  // 16 * Ndd, exact
+    ds.s1x4[idx] = (int32_t)s1;
+    ds.s2x16[idx] = s2;
+    if (det16 == 0) {
+        ds.detf[idx] = kHugeDet;
+        ds.sdetf[idx] = kHugeSqrtDet;
+    } else {
+        const float df = __double2float_rd((double)det16 * 0.0625);
+        ds.detf[idx] = df;
+        ds.sdetf[idx] = __fsqrt_rd(df);
+    }
+}
+
 __global__ void domain_stats_kernel(const int32_t* __restrict__ D, LevelGeom g, DomainStats ds) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     const int ndom = g.nrow_d * g.ncol_d;
@@ -67,44 +82,11 @@ __global__ void domain_stats_kernel(const int32_t* __restrict__ D, LevelGeom g, 
             s2 += d * d;
         }
     }
-    const int64_t n = (int64_t)g.size * g.size;
-    const int64_t det16 = n * s2 - s1 * s1;  // 16 * Ndd, exact
-    ds.s1x4[idx] = (int32_t)s1;
-    ds.s2x16[idx] = s2;
-    if (det16 == 0) {
-        ds.detf[idx] = kHugeDet;
-        ds.sdetf[idx] = kHugeSqrtDet;
-    } else {
-        const float df = __double2float_rd((double)det16 * 0.0625);
-        ds.detf[idx] = df;
-        ds.sdetf[idx] = __fsqrt_rd(df);
-    }
+    store_domain_stats(ds, idx, (int64_t)g.size * g.size, s1, s2);
 }
 
-__global__ void range_stats_kernel(const uint8_t* __restrict__ plane, int w, int h,
-                                   const uint32_t* __restrict__ rows,
-                                   const uint32_t* __restrict__ cols, int nranges, int size,
-                                   FitParams fp, RangeStats rs) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nranges) return;
-    if (rows[r] + (uint32_t)size > (uint32_t)h || cols[r] + (uint32_t)size > (uint32_t)w) {
-        // A block outside the plane is never read; the search skips it (result invalid).
-        rs.t0[r] = 0;
-        rs.t2[r] = 0;
-        rs.nrr[r] = 0;
-        rs.sum0[r] = 0.0;
-        rs.rms0[r] = 0.0;
-        return;
-    }
-    const uint8_t* base = plane + (size_t)rows[r] * w + cols[r];
-    int32_t t0 = 0, t2 = 0;
-    for (int i = 0; i < size; ++i)
-        for (int j = 0; j < size; ++j) {
-            const int32_t p = base[(size_t)i * w + j];
-            t0 += p;
-            t2 += p * p;
-        }
-    const int64_t n = (int64_t)size * size;
+__device__ __forceinline__ void store_range_stats(RangeStats& rs, int r, int64_t n, int32_t t0,
+                                                  int32_t t2, const FitParams& fp) {
     rs.t0[r] = t0;
     rs.t2[r] = t2;
     rs.nrr[r] = n * (int64_t)t2 - (int64_t)t0 * t0;
@@ -113,6 +95,68 @@ __global__ void range_stats_kernel(const uint8_t* __restrict__ plane, int w, int
     const FitResult f0 = fit_exact(n, 0, 0, t0, 0, t2, fp);
     rs.sum0[r] = f0.sum;
     rs.rms0[r] = f0.rms;
+}
+
+__device__ __forceinline__ bool range_outside(const uint32_t* rows, const uint32_t* cols, int r,
+                                              int size, int w, int h, RangeStats& rs) {
+    if (rows[r] + (uint32_t)size > (uint32_t)h || cols[r] + (uint32_t)size > (uint32_t)w) {
+        // A block outside the plane is never read; the search skips it (result invalid).
+        rs.t0[r] = 0;
+        rs.t2[r] = 0;
+        rs.nrr[r] = 0;
+        rs.sum0[r] = 0.0;
+        rs.rms0[r] = 0.0;
+        return true;
+    }
+    return false;
+}
+
+__global__ void range_stats_kernel(const uint8_t* __restrict__ plane, int w, int h,
+                                   const uint32_t* __restrict__ rows,
+                                   const uint32_t* __restrict__ cols, int nranges, int size,
+                                   FitParams fp, RangeStats rs) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nranges) return;
+    if (range_outside(rows, cols, r, size, w, h, rs)) return;
+    const uint8_t* base = plane + (size_t)rows[r] * w + cols[r];
+    int32_t t0 = 0, t2 = 0;
+    for (int i = 0; i < size; ++i)
+        for (int j = 0; j < size; ++j) {
+            const int32_t p = base[(size_t)i * w + j];
+            t0 += p;
+            t2 += p * p;
+        }
+    store_range_stats(rs, r, (int64_t)size * size, t0, t2, fp);
+}
+
+// Warp-per-range form for block sizes >= 16, where a thread per range leaves the GPU nearly
+// idle (256 ranges of 32 x 32 in a 512 x 512 plane: 36 -> 7 us).  The sums are integers, so
+// splitting them over lanes changes nothing.  (The domain statistics keep a thread per
+// domain: neighbouring domains' windows overlap, so a warp's loads already coalesce.)
+__global__ void range_stats_warp_kernel(const uint8_t* __restrict__ plane, int w, int h,
+                                        const uint32_t* __restrict__ rows,
+                                        const uint32_t* __restrict__ cols, int nranges,
+                                        int size, FitParams fp, RangeStats rs) {
+    const int r = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= nranges) return;  // the whole warp
+    if (rows[r] + (uint32_t)size > (uint32_t)h || cols[r] + (uint32_t)size > (uint32_t)w) {
+        if (lane == 0) range_outside(rows, cols, r, size, w, h, rs);
+        return;
+    }
+    const uint8_t* base = plane + (size_t)rows[r] * w + cols[r];
+    const int n = size * size, lg = __ffs(size) - 1;
+    int32_t t0 = 0, t2 = 0;
+    for (int k = lane; k < n; k += 32) {
+        const int32_t p = base[(size_t)(k >> lg) * w + (k & (size - 1))];
+        t0 += p;
+        t2 += p * p;
+    }
+    for (int o = 16; o; o >>= 1) {
+        t0 += __shfl_xor_sync(0xffffffffu, t0, o);
+        t2 += __shfl_xor_sync(0xffffffffu, t2, o);
+    }
+    if (lane == 0) store_range_stats(rs, r, n, t0, t2, fp);
 }
 
 // One CTA = RPB range blocks (one per thread) x a strided subset of the domain tiles
@@ -466,8 +510,12 @@ cudaError_t launch_range_stats(const uint8_t* plane, int w, int h, const uint32_
                                const uint32_t* cols, int nranges, int size, const FitParams& fp,
                                RangeStats rs, cudaStream_t st) {
     if (nranges == 0) return cudaSuccess;
-    range_stats_kernel<<<(nranges + 127) / 128, 128, 0, st>>>(plane, w, h, rows, cols, nranges,
-                                                               size, fp, rs);
+    if (size >= 16)
+        range_stats_warp_kernel<<<(unsigned)(((size_t)nranges * 32 + 255) / 256), 256, 0, st>>>(
+            plane, w, h, rows, cols, nranges, size, fp, rs);
+    else
+        range_stats_kernel<<<(nranges + 127) / 128, 128, 0, st>>>(plane, w, h, rows, cols,
+                                                                   nranges, size, fp, rs);
     return cudaGetLastError();
 }
 

@@ -38,7 +38,10 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstring>
+#include <memory>
 
 #include "kernels.cuh"
 #include "tc.cuh"
@@ -127,6 +130,8 @@ struct Smem {
     uint32_t tmem_base;
     int abort_flag;
     int qcount[kGroups];
+    int item;  // the all-levels launch: this CTA's current work item
+    int last;  // this CTA finished the last split of its range tile
     unsigned long long key_rms[kRangesPerTile];  // per-pass winner: f64 bits (rms >= 0)
     uint32_t key_idx[kRangesPerTile];
     double key_sum[kRangesPerTile];
@@ -298,14 +303,140 @@ __device__ __noinline__ void drain_queue(Smem& sm, int grp, int n, bool mark, ui
     group_barrier(grp);
 }
 
+// Final champion of range r over its M-splits' partials; its exact correlation travels with
+// it, so only the (cheap) exact fit is redone to fill in qalfa / qbeta.  The partials are
+// read around L1 (ld.global.cg): in the all-levels launch other CTAs wrote them.
+__device__ __forceinline__ void finish_range(const Partial* partials, int nsplit, int nranges,
+                                             int r, const LevelGeom& g, const RangeStats& rs,
+                                             const DomainStats& ds, const FitParams& fp,
+                                             CandidateOut* out) {
+    double best_rms = 0.0;
+    uint32_t best_idx = UINT32_MAX;
+    int32_t best_t1 = 0;
+    for (int t = 0; t < nsplit; ++t) {
+        const Partial* p = partials + (size_t)t * nranges + r;
+        const double rms = __ldcg(reinterpret_cast<const double*>(p));
+        const uint2 it = __ldcg(reinterpret_cast<const uint2*>(p) + 2);  // idx, t1x4
+        if (t == 0 || rms < best_rms || (rms == best_rms && it.x < best_idx)) {
+            best_rms = rms;
+            best_idx = it.x;
+            best_t1 = (int32_t)it.y;
+        }
+    }
+    if (best_idx == UINT32_MAX) {
+        out[r] = CandidateOut{0, 0, 0, 0, 0, 0, 0.0, 0, 0, 0, 0, 0, 0};
+        return;
+    }
+    const uint32_t dom = best_idx >> 3, k = best_idx & 7u;
+    const int a = (int)(dom / (uint32_t)g.ncol_d), bb = (int)(dom % (uint32_t)g.ncol_d);
+    const int64_t n = (int64_t)g.size * g.size;
+    const int64_t t1 = best_t1;
+    const FitResult f = fit_exact(n, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], t1, rs.t2[r], fp);
+    CandidateOut c;
+    c.dom_row = (uint32_t)a * (uint32_t)g.shift;
+    c.dom_col = (uint32_t)bb * (uint32_t)g.shift;
+    c.isometry = k;
+    c.qalfa = f.qalfa;
+    c.qbeta = f.qbeta;
+    c.valid = 1;
+    c.rms = f.rms;
+    c.s0 = n;
+    c.s1_x4 = ds.s1x4[dom];
+    c.s2_x16 = ds.s2x16[dom];
+    c.t0 = rs.t0[r];
+    c.t1_x4 = t1;
+    c.t2 = rs.t2[r];
+    out[r] = c;
+}
+
+// What one work item reads and writes: a level's B operand, statistics, seeds, its split
+// of the domain tiles and the outputs of its range tile.
+struct ItemArgs {
+    const uint8_t* bglob;
+    LevelGeom g;
+    int nranges;
+    RangeStats rs;
+    DomainStats ds;
+    FitParams fp;
+    const SeedOut* seeds;
+    int m_tiles, m_per_cta, msplit;
+    Partial* partials;        // msplit x nranges
+    unsigned long long* gch;  // 2 x nranges shared champion records, or null
+    int* tickets;             // per range tile: splits done (all-levels launch), or null
+    CandidateOut* out;        // the level's candidates when tickets is set
+};
+
+// Per-thread pipeline state of the roles (each role thread keeps its own copy).  It carries
+// over from one work item to the next, so the mbarriers are initialised once per CTA:
+// bit s of stage_par is the parity of this role's uses of shared-memory stage s so far
+// (fills for the load thread, consumptions for the MMA thread), bit s of stage_used says
+// the load thread filled stage s before; `tiles` counts the accumulator tiles handed over
+// (TMEM buffer tiles & 1, phase (tiles >> 1) & 1); `bres` counts resident-B loads.
+struct PipeState {
+    uint32_t stage_par = 0, stage_used = 0, tiles = 0, bres = 0;
+};
+
+// Shared-memory layout of both correlation kernels: the Smem record first (mbarriers at
+// fixed addresses for every level), then the A stages and the B stages / resident B tile,
+// 1024-byte aligned.
+constexpr size_t kSmemHead = (sizeof(Smem) + 1023) / 1024 * 1024;
+
+__device__ __forceinline__ Smem& smem_record(unsigned char* raw) {
+    return *reinterpret_cast<Smem*>(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
+}
+
+// CTA set-up shared by both kernels: mbarriers, the epilogue's queues and bitmap, TMEM
+// (all 512 columns, held until cta_teardown).
+__device__ __forceinline__ uint32_t cta_setup(Smem& sm) {
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kMaxStages; ++s) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&sm.tfull[b], 1);
+            mbar_init(&sm.tempty[b], kEpiThreads);
+        }
+        mbar_init(&sm.bres, 1);
+        sm.abort_flag = 0;
+        for (int q = 0; q < kGroups; ++q) sm.qcount[q] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = threadIdx.x; i < kM * kN / 32; i += kThreads) sm.evaluated[i] = 0u;
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&sm.tmem_base)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+    return sm.tmem_base;
+}
+
+__device__ __forceinline__ void cta_teardown(Smem& sm, uint32_t tmem, unsigned long long exact,
+                                             unsigned long long* exact_counter) {
+    if (exact_counter && exact) atomicAdd(exact_counter, exact);
+    tmem_fence_before();
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 1) {
+        tmem_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+    }
+}
+
+// One work item: range tile `ntile` of a level against domain tiles [split * m_per_cta,
+// ...) -- the champions seeded, the loads / MMAs / exact-bound epilogue over those domain
+// tiles, the tile's partial champions written.  With tickets set, the last split of the
+// range tile to finish also writes the tile's final candidates.  Every thread of the CTA
+// calls this together; it begins and ends with a CTA barrier.
 template <int S, bool DIG>
-__global__ void __launch_bounds__(kThreads, 1)
-    corr_tc_kernel(const __grid_constant__ TcMaps maps, const uint8_t* __restrict__ bglob,
-                   LevelGeom g, int nranges, RangeStats rs, DomainStats ds, FitParams fp,
-                   const SeedOut* __restrict__ seeds, int m_tiles, int m_per_cta,
-                   Partial* __restrict__ partials, unsigned long long* __restrict__ gch,
-                   int* __restrict__ err,
-                   unsigned long long* __restrict__ exact_counter) {
+__device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs& a, int ntile,
+                                             int split, Smem& sm, unsigned char* stages,
+                                             uint32_t tmem, PipeState& ps, int* err,
+                                             unsigned long long& exact) {
     using C_ = Cfg<S, DIG>;
     constexpr int N = S * S;
     constexpr int NT = C_::kNt;
@@ -320,49 +451,33 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr int kRangesPerWarp = C_::kRw;
     constexpr int kChunks = C_::kCh;
 
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    unsigned char* stA = base;                                  // kStages x (1 or 2) x 16 KB
-    unsigned char* stB = stA + kStages * kStageAll;             // kStages B stages or resident
-    unsigned char* after_b = stB + (kBRes ? KST * kStageB : kStages * kStageB);
-    Smem& sm = *reinterpret_cast<Smem*>(after_b);
+    unsigned char* stA = stages;                     // kStages x (1 or 2) x 16 KB
+    unsigned char* stB = stA + kStages * kStageAll;  // kStages B stages or resident
 
+    const LevelGeom& g = a.g;
+    const DomainStats& ds = a.ds;
+    const FitParams& fp = a.fp;
+    const int nranges = a.nranges;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ntile = blockIdx.x;
-    const int m_begin = blockIdx.y * m_per_cta;
-    const int m_end = min(m_tiles, m_begin + m_per_cta);
+    const int m_begin = split * a.m_per_cta;
+    const int m_end = min(a.m_tiles, m_begin + a.m_per_cta);
     // Phase copies: domains lie shift pixels (fold) or shift / 2 contracted samples
     // (digits) apart; P same-phase copies put each group of 16 / P domains' starts on
     // 16-byte boundaries.
     const int P = DIG ? 32 / g.shift : 16 / g.shift;
     const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
-    const uint8_t* btile = bglob + (size_t)ntile * KST * kStageB;
+    const uint8_t* btile = a.bglob + (size_t)ntile * KST * kStageB;
 
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) {
-            mbar_init(&sm.full[s], 1);
-            mbar_init(&sm.empty[s], 1);
-        }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(&sm.tfull[b], 1);
-            mbar_init(&sm.tempty[b], kEpiThreads);
-        }
-        mbar_init(&sm.bres, 1);
-        sm.abort_flag = 0;
-        for (int q = 0; q < kGroups; ++q) sm.qcount[q] = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    for (int i = threadIdx.x; i < kM * NT / 32; i += kThreads) sm.evaluated[i] = 0u;
     if (threadIdx.x < RT) {
         Champ& C = sm.ch[threadIdx.x];
         const int r = ntile * RT + threadIdx.x;
-        C.valid = r < nranges && seeds[r].idx != UINT32_MAX;
+        C.valid = r < nranges && a.seeds[r].idx != UINT32_MAX;
         if (C.valid) {
-            C.t0 = rs.t0[r];
-            C.t2 = rs.t2[r];
-            C.nrr = rs.nrr[r];
-            C.rms0 = rs.rms0[r];
-            const SeedOut sd = seeds[r];
+            C.t0 = a.rs.t0[r];
+            C.t2 = a.rs.t2[r];
+            C.nrr = a.rs.nrr[r];
+            C.rms0 = a.rs.rms0[r];
+            const SeedOut sd = a.seeds[r];
             C.rms = sd.rms;
             C.sum = sd.sum;
             C.idx = sd.idx;
@@ -378,37 +493,31 @@ __global__ void __launch_bounds__(kThreads, 1)
         sm.key_idx[threadIdx.x] = UINT32_MAX;
         publish_threshold(sm, threadIdx.x, fp, N);
     }
-    if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32(&sm.tmem_base)),
-                     "r"(512));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    tmem_fence_before();
     __syncthreads();
-    tmem_fence_after();
-    const uint32_t tmem = sm.tmem_base;
     volatile int* abort_flag = &sm.abort_flag;
 
     if (warp == 0) {
         // ---------------------------------------------------------------- loads
         if (lane == 0) {
             int s = 0;
-            uint32_t ph = 0;
-            int issued = 0;
             if (kBRes) {
                 mbar_expect_tx(&sm.bres, KST * kStageB);
                 for (int t = 0; t < KST; ++t)
                     bulk_load(stB + t * kStageB, btile + (size_t)t * kStageB, kStageB, &sm.bres);
             }
             for (int mt = m_begin; mt < m_end && !*abort_flag; ++mt) {
-                const int a = mt / tiles_per_row;
+                const int ar = mt / tiles_per_row;
                 const int q0 = (mt % tiles_per_row) * (kM / P);
                 // First row of the domain row's window: a pixel row (fold) or a
                 // contracted-plane row (digits).
-                const int dom_row = DIG ? a * (g.shift / 2) : a * g.shift;
+                const int dom_row = DIG ? ar * (g.shift / 2) : ar * g.shift;
                 for (int t = 0; t < KST; ++t) {
-                    if (issued >= kStages && !mbar_wait(&sm.empty[s], ph ^ 1, abort_flag, err, 1)) break;
+                    const uint32_t bit = 1u << s;
+                    // A stage filled before is refilled once the MMAs of its last fill
+                    // have completed.
+                    if ((ps.stage_used & bit) &&
+                        !mbar_wait(&sm.empty[s], (ps.stage_par & bit) ? 0u : 1u, abort_flag, err, 1))
+                        break;
                     mbar_expect_tx(&sm.full[s], C_::kTx);
                     const int kg0 = t * 8;
                     const int j = kg0 / ROWS, y0 = kg0 % ROWS;
@@ -430,47 +539,53 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     if (!kBRes)
                         bulk_load(stB + s * kStageB, btile + (size_t)t * kStageB, kStageB, &sm.full[s]);
-                    ++issued;
-                    if (++s == kStages) {
-                        s = 0;
-                        ph ^= 1;
-                    }
+                    ps.stage_used |= bit;
+                    ps.stage_par ^= bit;
+                    if (++s == kStages) s = 0;
                 }
             }
-            // Drain: wait (bounded) for the loads still in flight before leaving.
+            // Drain: wait (bounded) for the loads still in flight before leaving -- each
+            // stage's last fill, and the resident B tile.
             if (*abort_flag) {
-                int s2 = s;
-                uint32_t ph2 = ph;
-                for (int i = 0; i < kStages && i < issued; ++i) {
-                    if (--s2 < 0) {
-                        s2 = kStages - 1;
-                        ph2 ^= 1;
-                    }
+                for (int s2 = 0; s2 < kMaxStages; ++s2) {
+                    const uint32_t bit = 1u << s2;
+                    if (!(ps.stage_used & bit)) continue;
+                    const uint32_t par = (ps.stage_par & bit) ? 0u : 1u;  // the last fill's
                     const long long t0 = clock64();
-                    while (!mbar_try_wait(&sm.full[s2], ph2) && clock64() - t0 < kWaitCycles) {
+                    while (!mbar_try_wait(&sm.full[s2], par) && clock64() - t0 < kWaitCycles) {
+                    }
+                }
+                if (kBRes) {
+                    const long long t0 = clock64();
+                    while (!mbar_try_wait(&sm.bres, ps.bres & 1u) && clock64() - t0 < kWaitCycles) {
                     }
                 }
             }
+            if (kBRes) ++ps.bres;
         }
     } else if (warp == 1) {
         // ---------------------------------------------------------------- MMA
         if (lane == 0) {
             int s = 0;
-            uint32_t ph = 0;
             bool ok = true;
-            if (kBRes) ok = mbar_wait(&sm.bres, 0, abort_flag, err, 2);
-            int i = 0;
-            for (int mt = m_begin; ok && mt < m_end; ++mt, ++i) {
-                const int b = i & 1;
-                const uint32_t bph = (uint32_t)((i >> 1) & 1);
+            if (kBRes) {
+                ok = mbar_wait(&sm.bres, ps.bres & 1u, abort_flag, err, 2);
+                ++ps.bres;
+            }
+            for (int mt = m_begin; ok && mt < m_end; ++mt) {
+                const uint32_t i = ps.tiles++;
+                const int b = (int)(i & 1u);
+                const uint32_t bph = (i >> 1) & 1u;
                 if (i >= 2 && !mbar_wait(&sm.tempty[b], bph ^ 1, abort_flag, err, 4)) break;
                 tmem_fence_after();
                 const uint32_t dcol = tmem + (uint32_t)(b * kN);
                 for (int t = 0; t < KST; ++t) {
-                    if (!mbar_wait(&sm.full[s], ph, abort_flag, err, 8)) {
+                    const uint32_t bit = 1u << s;
+                    if (!mbar_wait(&sm.full[s], (ps.stage_par & bit) ? 1u : 0u, abort_flag, err, 8)) {
                         ok = false;
                         break;
                     }
+                    ps.stage_par ^= bit;
                     tmem_fence_after();
                     const uint32_t a_addr = smem_u32(stA + s * kStageAll);
                     const uint32_t b_addr = smem_u32(kBRes ? stB + t * kStageB : stB + s * kStageB);
@@ -483,10 +598,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                             mma_i8<NT>(dcol + NT, smem_desc(a_addr + kStageA + kk * 256), bd, acc);
                     }
                     mma_commit(&sm.empty[s]);
-                    if (++s == kStages) {
-                        s = 0;
-                        ph ^= 1;
-                    }
+                    if (++s == kStages) s = 0;
                 }
                 if (!ok) break;
                 mma_commit(&sm.tfull[b]);
@@ -502,7 +614,6 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int gt = threadIdx.x - 64 - part * kGroupThreads;  // 0..kGroupThreads-1
         const int m = e * 32 + lane;             // this thread's domain lane
         const float four_inv_n = 4.0f / (float)N;
-        unsigned long long exact = 0;
 
         // This lane's domain statistics, prefetched one tile ahead.  The lane's column
         // offset within a tile is fixed (domain_of_lane is P * (q0 + 8h + r8) + p), and
@@ -531,10 +642,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         int n_dom = -1;
         load_dom(m_begin, n_s1, n_det, n_sdet, n_dom);
 
-        int i = 0;
-        for (int mt = m_begin; mt < m_end; ++mt, ++i) {
-            const int b = i & 1;
-            const uint32_t bph = (uint32_t)((i >> 1) & 1);
+        for (int mt = m_begin; mt < m_end; ++mt) {
+            const uint32_t i = ps.tiles++;
+            const int b = (int)(i & 1u);
+            const uint32_t bph = (i >> 1) & 1u;
             const float s1f = n_s1, detf = n_det, sdetf = n_sdet;
             const int dom = n_dom;
             load_dom(mt + 1, n_s1, n_det, n_sdet, n_dom);
@@ -661,13 +772,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const bool last = mt + 1 == m_end;
                 if (queued > kQueueCap) {
                     drain_queue<N, NT, kRangesPerWarp>(sm, part, kQueueCap, true, tag, gt, ds,
-                                                       fp, exact, gch, ntile * RT);
+                                                       fp, exact, a.gch, ntile * RT);
                     rescan = true;
                     continue;  // pass again over the same accumulator (fresh thresholds)
                 }
                 if (queued >= kFlush || (last && queued > 0))
                     drain_queue<N, NT, kRangesPerWarp>(sm, part, queued, false, tag, gt, ds,
-                                                       fp, exact, gch, ntile * RT);
+                                                       fp, exact, a.gch, ntile * RT);
                 break;
             }
             if (rescan) {
@@ -681,15 +792,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             tmem_fence_before();
             mbar_arrive(&sm.tempty[b]);
         }
-        if (exact_counter && exact) atomicAdd(exact_counter, exact);
     }
 
+    // ---------------------------------------------------------------- item end
     tmem_fence_before();
     __syncthreads();
-    if (warp == 1) {
-        tmem_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
-    }
+    tmem_fence_after();
     if (threadIdx.x < RT) {
         const Champ& C = sm.ch[threadIdx.x];
         const int r = ntile * RT + threadIdx.x;
@@ -702,9 +810,107 @@ __global__ void __launch_bounds__(kThreads, 1)
             p.qalfa = 0;
             p.qbeta = 0;
             p.pad = 0;
-            partials[(size_t)blockIdx.y * nranges + r] = p;
+            a.partials[(size_t)split * nranges + r] = p;
         }
     }
+    if (a.tickets) {
+        // The last of the range tile's splits to get here finishes its ranges (the
+        // threadfence-reduction pattern: partials, fence, ticket; the last CTA fences
+        // again and reads every split's partials around L1).
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) sm.last = atomicAdd(&a.tickets[ntile], 1) == a.msplit - 1;
+        __syncthreads();
+        if (sm.last) {
+            __threadfence();
+            const int r = ntile * RT + threadIdx.x;
+            if (threadIdx.x < RT && r < nranges)
+                finish_range(a.partials, a.msplit, nranges, r, g, a.rs, ds, fp, a.out);
+        }
+    }
+}
+
+// The correlation of one level: CTA (x, y) = range tile x against domain-tile split y.
+template <int S, bool DIG>
+__global__ void __launch_bounds__(kThreads, 1)
+    corr_tc_kernel(const __grid_constant__ TcMaps maps, const __grid_constant__ ItemArgs a,
+                   int* __restrict__ err,
+                   unsigned long long* __restrict__ exact_counter) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    Smem& sm = smem_record(smem_raw);
+    unsigned char* stages = reinterpret_cast<unsigned char*>(&sm) + kSmemHead;
+    const uint32_t tmem = cta_setup(sm);
+    PipeState ps;
+    unsigned long long exact = 0;
+    process_item<S, DIG>(maps, a, blockIdx.x, blockIdx.y, sm, stages, tmem, ps, err, exact);
+    cta_teardown(sm, tmem, exact, exact_counter);
+}
+
+// All tensor-core levels of a plane in one persistent launch: one CTA per SM takes work
+// items -- (level job, range tile, domain-tile split) -- from a global counter until none
+// are left.  TMEM, the mbarriers and the epilogue's queues are set up once per CTA; the
+// pipelines' phases carry over from item to item (PipeState).  Jobs are ordered by item
+// cost, largest first, so the cheap items fill the end.  Each range tile's last split
+// writes the tile's final candidates (no finish launch).
+struct AllLevels {
+    TcMaps maps[kMaxLevelJobs];
+    ItemArgs args[kMaxLevelJobs];
+    int kind[kMaxLevelJobs];  // 0: S=4 fold, 1: S=8 fold, 2/3/4: S=16/32/64 digits
+    int tile_begin[kMaxLevelJobs];
+    int tile_count[kMaxLevelJobs];
+    int item_begin[kMaxLevelJobs + 1];
+    int njobs;
+};
+
+static_assert(sizeof(AllLevels) <= 32000, "kernel parameter space");
+
+__global__ void __launch_bounds__(kThreads, 1)
+    corr_tc_all_kernel(const __grid_constant__ AllLevels L, int* __restrict__ work,
+                       int* __restrict__ err, unsigned long long* __restrict__ exact_counter) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    Smem& sm = smem_record(smem_raw);
+    unsigned char* stages = reinterpret_cast<unsigned char*>(&sm) + kSmemHead;
+    const uint32_t tmem = cta_setup(sm);
+    PipeState ps;
+    unsigned long long exact = 0;
+    const int nitems = L.item_begin[L.njobs];
+    volatile int* abort_flag = &sm.abort_flag;
+    if (threadIdx.x == 0) sm.item = (int)blockIdx.x;
+    __syncthreads();
+    for (;;) {
+        const int item = sm.item;
+        if (item >= nitems || *abort_flag) break;
+        int j = 0;
+        while (j + 1 < L.njobs && item >= L.item_begin[j + 1]) ++j;
+        // Parameter-space references: nothing of the job is copied.
+        const TcMaps& maps = L.maps[j];
+        const ItemArgs& a = L.args[j];
+        // Split-major within a job: a range tile's later splits start after its earlier
+        // ones have finished and begin from their champions (the shared records).
+        const int local = item - L.item_begin[j];
+        const int ntile = L.tile_begin[j] + local % L.tile_count[j];
+        const int split = local / L.tile_count[j];
+        switch (L.kind[j]) {
+            case 0:
+                process_item<4, false>(maps, a, ntile, split, sm, stages, tmem, ps, err, exact);
+                break;
+            case 1:
+                process_item<8, false>(maps, a, ntile, split, sm, stages, tmem, ps, err, exact);
+                break;
+            case 2:
+                process_item<16, true>(maps, a, ntile, split, sm, stages, tmem, ps, err, exact);
+                break;
+            case 3:
+                process_item<32, true>(maps, a, ntile, split, sm, stages, tmem, ps, err, exact);
+                break;
+            default:
+                process_item<64, true>(maps, a, ntile, split, sm, stages, tmem, ps, err, exact);
+                break;
+        }
+        if (threadIdx.x == 0) sm.item = (int)gridDim.x + atomicAdd(work, 1);
+        __syncthreads();
+    }
+    cta_teardown(sm, tmem, exact, exact_counter);
 }
 
 // B operand of one level: rows n = range * 8 + isometry; for each N tile (NT rows) and each
@@ -1038,51 +1244,20 @@ __global__ void seed_merge_kernel(const Partial* __restrict__ partials, int nspl
         seeds[r] = SeedOut{best.rms, best.sum, idx, best.t1x4};
 }
 
-// Final champion over the M-splits; its exact correlation travels with it, so only the
-// (cheap) exact fit is redone here to fill in qalfa / qbeta.
+// Final champion over the M-splits of each range (finish_range).
 __global__ void finish_kernel(const Partial* __restrict__ partials, int nsplit, int nranges,
                               LevelGeom g, RangeStats rs, DomainStats ds, FitParams fp,
                               CandidateOut* __restrict__ out) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nranges) return;
-    Partial best = partials[r];
-    for (int t = 1; t < nsplit; ++t) {
-        const Partial p = partials[(size_t)t * nranges + r];
-        if (p.rms < best.rms || (p.rms == best.rms && p.idx < best.idx)) best = p;
-    }
-    if (best.idx == UINT32_MAX) {
-        out[r] = CandidateOut{0, 0, 0, 0, 0, 0, 0.0, 0, 0, 0, 0, 0, 0};
-        return;
-    }
-    const uint32_t dom = best.idx >> 3, k = best.idx & 7u;
-    const int a = (int)(dom / (uint32_t)g.ncol_d), bb = (int)(dom % (uint32_t)g.ncol_d);
-    const int64_t n = (int64_t)g.size * g.size;
-    const int64_t t1 = best.t1x4;
-    const FitResult f = fit_exact(n, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], t1, rs.t2[r], fp);
-    CandidateOut c;
-    c.dom_row = (uint32_t)a * (uint32_t)g.shift;
-    c.dom_col = (uint32_t)bb * (uint32_t)g.shift;
-    c.isometry = k;
-    c.qalfa = f.qalfa;
-    c.qbeta = f.qbeta;
-    c.valid = 1;
-    c.rms = f.rms;
-    c.s0 = n;
-    c.s1_x4 = ds.s1x4[dom];
-    c.s2_x16 = ds.s2x16[dom];
-    c.t0 = rs.t0[r];
-    c.t1_x4 = t1;
-    c.t2 = rs.t2[r];
-    out[r] = c;
+    if (r < nranges) finish_range(partials, nsplit, nranges, r, g, rs, ds, fp, out);
 }
 
 template <int S, bool DIG>
 constexpr size_t smem_bytes() {
     using C_ = Cfg<S, DIG>;
     static_assert(C_::kStages <= kMaxStages, "pipeline depth");
-    return 1024 + (size_t)C_::kStages * C_::kDigits * kStageA +
-           (C_::kBRes ? (size_t)C_::KST * C_::kStageBt : (size_t)C_::kStages * C_::kStageBt) +
-           sizeof(Smem);
+    return 1024 + kSmemHead + (size_t)C_::kStages * C_::kDigits * kStageA +
+           (C_::kBRes ? (size_t)C_::KST * C_::kStageBt : (size_t)C_::kStages * C_::kStageBt);
 }
 static_assert(smem_bytes<4, false>() <= 232448 && smem_bytes<8, false>() <= 232448 &&
                   smem_bytes<16, false>() <= 232448 && smem_bytes<32, false>() <= 232448 &&
@@ -1104,8 +1279,9 @@ cudaError_t launch_t(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& 
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(ntiles, msplit);
-    kern<<<grid, kThreads, smem, st>>>(maps, bglob, g, nranges, rs, ds, fp, seeds, m_tiles,
-                                      m_per_cta, partials, gch, err, counter);
+    const ItemArgs a{bglob, g,        nranges,  rs,       ds,      fp,     seeds,
+                     m_tiles, m_per_cta, msplit, partials, gch, nullptr, nullptr};
+    kern<<<grid, kThreads, smem, st>>>(maps, a, err, counter);
     return cudaGetLastError();
 }
 
@@ -1269,6 +1445,122 @@ cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeo
         default: return cudaErrorInvalidValue;
     }
 #undef MARS_CORR
+}
+
+bool all_levels_supported(int size, bool digits) {
+    return digits ? (size == 16 || size == 32 || size == 64) : (size == 4 || size == 8);
+}
+
+namespace {
+int all_levels_kind(int size, bool digits) {
+    if (!digits) return size == 4 ? 0 : 1;
+    return size == 16 ? 2 : (size == 32 ? 3 : 4);
+}
+
+// Device time of one domain tile of one range tile, by kind (per-level CUDA-event times of a
+// 512 x 512 plane on one B200 / tiles: S = 4 fold 1.48 us, S = 8 fold 1.93, S = 16 digits
+// 2.09, S = 32 digits 8.0; S = 64 digits four times S = 32, K being four times larger).
+double all_levels_tile_us(int size, bool digits) {
+    if (!digits) return size == 4 ? 1.48 : 1.93;
+    return size == 16 ? 2.09 : (size == 32 ? 8.0 : 32.0);
+}
+constexpr double kItemSetupTiles = 4.0;  // B load, champions, pipeline fill: ~4 tiles
+constexpr int kItemsPerSm = 8;           // work items per SM the splits aim at
+}  // namespace
+
+void all_levels_splits(const LevelGeom* g, const int* nranges, const bool* digits, int n,
+                       int num_sms, int* msplit, int* tail_tiles, int* tail_msplit) {
+    double total = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const int tiles_per_row = (g[i].ncol_d + kM - 1) / kM;
+        const double m_tiles = (double)g[i].nrow_d * tiles_per_row;
+        const int rt = ranges_per_tile(digits[i]);
+        const double ntiles = (double)((nranges[i] + rt - 1) / rt);
+        total += ntiles * m_tiles * all_levels_tile_us(g[i].size, digits[i]);
+    }
+    const double target = total / ((double)num_sms * kItemsPerSm);
+    int last = -1;
+    double last_cost = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const int tiles_per_row = (g[i].ncol_d + kM - 1) / kM;
+        const int m_tiles = g[i].nrow_d * tiles_per_row;
+        const double tile_us = all_levels_tile_us(g[i].size, digits[i]);
+        const int ms = (int)((m_tiles * tile_us + target - 1e-9) / target);
+        msplit[i] = std::max(1, std::min(ms, m_tiles));
+        tail_tiles[i] = 0;
+        tail_msplit[i] = msplit[i];
+        const double cost = ((m_tiles + msplit[i] - 1) / msplit[i] + kItemSetupTiles) * tile_us;
+        if (last < 0 || cost < last_cost) {
+            last = i;
+            last_cost = cost;
+        }
+    }
+    if (last < 0) return;
+    // The tail: items a quarter as long, about two per SM.
+    const int tiles_per_row = (g[last].ncol_d + kM - 1) / kM;
+    const int m_tiles = g[last].nrow_d * tiles_per_row;
+    const int rt = ranges_per_tile(digits[last]);
+    const int ntiles = (nranges[last] + rt - 1) / rt;
+    const int fine = std::min(m_tiles, 4 * msplit[last]);
+    if (fine > msplit[last] && ntiles >= 2) {
+        tail_msplit[last] = fine;
+        tail_tiles[last] = std::min(ntiles / 2, (2 * num_sms + fine - 1) / fine);
+    }
+}
+
+cudaError_t launch_corr_all(const LevelJob* jobs, int njobs, int* work, int* err,
+                            unsigned long long* counter, int num_sms, cudaStream_t st) {
+    if (njobs <= 0) return cudaSuccess;
+    if (njobs > kMaxLevelJobs) return cudaErrorInvalidValue;
+    // Largest items first.
+    int order[kMaxLevelJobs];
+    double cost[kMaxLevelJobs];
+    for (int i = 0; i < njobs; ++i) {
+        const LevelJob& J = jobs[i];
+        if (!all_levels_supported(J.g.size, J.digits != 0) || J.msplit < 1) return cudaErrorInvalidValue;
+        const int tiles_per_row = (J.g.ncol_d + kM - 1) / kM;
+        const int m_tiles = J.g.nrow_d * tiles_per_row;
+        const int m_per = (m_tiles + J.msplit - 1) / J.msplit;
+        cost[i] = (m_per + kItemSetupTiles) * all_levels_tile_us(J.g.size, J.digits != 0);
+        order[i] = i;
+    }
+    std::sort(order, order + njobs, [&](int x, int y) { return cost[x] > cost[y]; });
+    std::unique_ptr<AllLevels> hold(new AllLevels());  // the kernel parameter, ~10 KB
+    AllLevels& L = *hold;
+    L.njobs = njobs;
+    L.item_begin[0] = 0;
+    for (int k = 0; k < njobs; ++k) {
+        const LevelJob& J = jobs[order[k]];
+        const int tiles_per_row = (J.g.ncol_d + kM - 1) / kM;
+        const int m_tiles = J.g.nrow_d * tiles_per_row;
+        L.maps[k] = J.maps;
+        L.args[k] = ItemArgs{J.bglob,  J.g,      J.nranges,
+                             J.rs,     J.ds,     J.fp,
+                             J.seeds,  m_tiles,  (m_tiles + J.msplit - 1) / J.msplit,
+                             J.msplit, J.partials, J.gch,
+                             J.tickets, J.out};
+        L.kind[k] = all_levels_kind(J.g.size, J.digits != 0);
+        L.tile_begin[k] = J.tile_begin;
+        L.tile_count[k] = J.tile_count;
+        L.item_begin[k + 1] = L.item_begin[k] + J.tile_count * J.msplit;
+    }
+    const int nitems = L.item_begin[njobs];
+    if (nitems == 0) return cudaSuccess;
+    size_t smem = 0;
+    for (int k = 0; k < njobs; ++k) {
+        constexpr size_t sz[5] = {smem_bytes<4, false>(), smem_bytes<8, false>(),
+                                  smem_bytes<16, true>(), smem_bytes<32, true>(),
+                                  smem_bytes<64, true>()};
+        smem = std::max(smem, sz[L.kind[k]]);
+    }
+    cudaError_t e = cudaFuncSetAttribute(corr_tc_all_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(work, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    const int grid = std::min(nitems, num_sms);
+    corr_tc_all_kernel<<<grid, kThreads, smem, st>>>(L, work, err, counter);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_seed_merge(const Partial* partials, int nsplit, int nranges, int coarse_ncol,

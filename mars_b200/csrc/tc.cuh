@@ -32,6 +32,29 @@ struct SeedOut {
     int32_t t1x4;  // the seed champion's exact correlation (fits int32 for S <= 64)
 };
 
+// One job of the all-levels launch (launch_corr_all): range tiles [tile_begin, tile_begin +
+// tile_count) of a level, each against `msplit` splits of the level's domain tiles, with
+// the operands and outputs launch_corr takes.  gch (2 x nranges) is all ones and tickets
+// (one per range tile of the level) zero before the launch; the last split of a range tile
+// writes the tile's candidates to `out`.
+struct LevelJob {
+    TcMaps maps;
+    const uint8_t* bglob;
+    LevelGeom g;
+    int nranges;
+    RangeStats rs;
+    DomainStats ds;
+    FitParams fp;
+    const SeedOut* seeds;
+    Partial* partials;  // msplit x nranges (or more)
+    unsigned long long* gch;
+    int* tickets;
+    CandidateOut* out;
+    int tile_begin, tile_count, msplit;
+    int digits;
+};
+constexpr int kMaxLevelJobs = 8;
+
 bool supported(int size, int shift);
 // Levels the split-digit contracted operand serves (block sizes 16..64).
 bool digits_supported(int size, int shift);
@@ -44,6 +67,16 @@ int digit_phase_count(int shift);
 size_t digit_plane_bytes(int w, int h, int shift);
 size_t b_bytes(int size, int nranges, bool digits);
 int msplit_for(const LevelGeom& g, int nranges, int num_sms, bool digits);
+// Whether the all-levels kernel holds a level: block sizes 4 and 8 on the fold path, 16, 32
+// and 64 on the split-digit path.
+bool all_levels_supported(int size, bool digits);
+int ranges_per_tile(bool digits);
+// Split counts of the levels of one all-levels launch, from a per-kind cost model, so that
+// the work items are of similar duration and several per SM.  The level with the cheapest
+// items (they run last) also gets a tail: its last tail_tiles[i] range tiles at
+// tail_msplit[i] splits, finer items to even out the end of the launch (0 tiles: none).
+void all_levels_splits(const LevelGeom* g, const int* nranges, const bool* digits, int n,
+                       int num_sms, int* msplit, int* tail_tiles, int* tail_msplit);
 
 cudaError_t launch_phase_planes(const uint8_t* plane, int w, int h, int shift, uint8_t* out,
                                 cudaStream_t st);
@@ -59,6 +92,10 @@ cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeo
                         RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
                         Partial* partials, unsigned long long* gch, int msplit, bool digits,
                         int* err, unsigned long long* counter, cudaStream_t st);
+// The persistent launch over jobs[0..njobs) (njobs <= kMaxLevelJobs); `work` is a device
+// counter it zeroes first.
+cudaError_t launch_corr_all(const LevelJob* jobs, int njobs, int* work, int* err,
+                            unsigned long long* counter, int num_sms, cudaStream_t st);
 cudaError_t launch_seed_merge(const Partial* partials, int nsplit, int nranges, int coarse_ncol,
                               int fine_ncol, int ratio, SeedOut* seeds, cudaStream_t st);
 cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,

@@ -95,3 +95,48 @@ def test_planned_encode_refuses_what_a_plan_cannot_serve(ctx):
                                       mb.C.byref(rn), mb.C.byref(cnt))
     assert rc == -8  # MARS_EUNSUPPORTED
     plan.close()
+
+
+def _grid(w, h, size):
+    r, c = np.meshgrid(np.arange(0, h - size + 1, size), np.arange(0, w - size + 1, size),
+                       indexing="ij")
+    return r.ravel().astype(np.uint32), c.ravel().astype(np.uint32)
+
+
+@pytest.mark.parametrize("w,h,shift,max_size", [(512, 512, 2, 32), (200, 136, 2, 32),
+                                                (129, 127, 4, 16), (256, 256, 8, 64),
+                                                (384, 320, 16, 64), (96, 64, 2, 8)])
+def test_all_levels_launch_equals_per_level_launches(ctx, w, h, shift, max_size):
+    # Tables and plans correlate every tensor-core level in one persistent launch (work items
+    # of every level from one counter, pipelines carried from item to item, each range tile
+    # finished by its last split); one launch per level gives the same candidates, rms bits
+    # and moments for every node, and fewer kernel launches are made.
+    img = synthetic.gray(w, h, 5)
+    params = mb.make_params(min_size=4, max_size=max_size, shift=shift, lam=200.0)
+    per = mb.Context(0)
+    per.set_search_path("per_level")
+    try:
+        a = ctx.search_provider(img, params)
+        b = per.search_provider(img, params)
+        plan = ctx.search_plan(w, h, params)
+        per_plan = per.search_plan(w, h, params)
+        got = plan.run(img)
+        for size in (64, 32, 16, 8, 4):
+            if size > max_size:
+                continue
+            rows, cols = _grid(w, h, size)
+            if len(rows) == 0:
+                continue
+            x, xe = a.search_many(rows, cols, size, shift)
+            y, ye = b.search_many(rows, cols, size, shift)
+            z, ze = got.search_many(rows, cols, size, shift)
+            assert x.tobytes() == y.tobytes(), size
+            assert z.tobytes() == y.tobytes(), size
+            assert np.array_equal(xe, ye) and np.array_equal(ze, ye), size
+        assert plan.launches < per_plan.launches
+        for t in (a, b, got):
+            t.close()
+        plan.close()
+        per_plan.close()
+    finally:
+        per.close()
