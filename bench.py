@@ -53,6 +53,10 @@ WORKLOAD = ("exhaustive search of every RD quadtree node of a 512x512 synthetic 
 # DRAM bytes (read + write) per launch of the dominant search kernel, s=4 level.
 NCU_SOURCE = "profiles/corr_tc_s4_512x512_ncu.md"
 NCU_TRAFFIC = {4: 20_560_000}
+# DRAM bytes (read + write) of one all-levels correlation launch (corr_tc_all_kernel, every
+# level of one 512x512 plane): profiles/corr_tc_all_512x512_ncu.md.
+NCU_ALL_SOURCE = "profiles/corr_tc_all_512x512_ncu.md"
+NCU_ALL_TRAFFIC = 42_626_816 + 299_264
 # Thread instructions per candidate fit of the correlation kernel's level (warp
 # instructions x 32 / fits, same capture): the issue cost behind the epilogue roofline.
 NCU_INSTR_PER_FIT = {4: 0.9722e9 * 32 / 8.52e9, 8: 0.3886e9 * 32 / 2.0e9}
@@ -801,6 +805,8 @@ def run_gpu(args):
     torch.cuda.synchronize(dev)
 
     t_graph = 0.0
+    t_kernel = 0.0  # the all-levels correlation launch inside each replay (events in the graph)
+    kernel_timed = True
     launches0 = ctx.launches
     with ClockSampler(local) as clocks:
         for k in range(args.steps):
@@ -811,6 +817,11 @@ def run_gpu(args):
             e1.record(stream)
             torch.cuda.synchronize(dev)
             t_graph += e0.elapsed_time(e1) / 1e3
+            if kernel_timed:
+                try:
+                    t_kernel += plan.kernel_ms / 1e3
+                except mb.MarsError:  # one launch per level: no all-levels kernel to time
+                    kernel_timed = False
     torch.cuda.synchronize(dev)
     launches = ctx.launches - launches0
     t_total = reduce_max(t_graph, dist, dev)
@@ -829,7 +840,8 @@ def run_gpu(args):
         for s in SIZES:
             per_level[s] += timers[s][0].elapsed_time(timers[s][1]) / 1e3
 
-    # Roofline of the dominant kernel: the level search whose launches take longest.
+    # The dominant level (the one whose per-level launches take longest) for the epilogue
+    # bound; the roofline itself is the all-levels launch when the plan has one.
     dom = max(SIZES, key=lambda s: per_level[s])
     t_launch = per_level[dom] / lvl_steps
     ops = 2.0 * macs_of_level(dom)  # int8-equivalent MAC ops of the correlation
@@ -842,6 +854,21 @@ def run_gpu(args):
         peak_tops = 2.0 * 1590.0
         peak_src = "2 x fallback bf16 1.59 PFLOP/s"
     achieved = ops / t_launch / 1e12
+    level_roofline = {"kernel": f"search level s={dom} (one launch per level)",
+                      "achieved": achieved, "peak": peak_tops, "unit": "TOP/s",
+                      "frac": achieved / peak_tops, "traffic": NCU_TRAFFIC.get(dom),
+                      "traffic_source": f"ncu ({NCU_SOURCE})", "ops_per_launch": ops,
+                      "launch_ms": 1e3 * t_launch}
+    if kernel_timed and t_kernel > 0:
+        roof_kernel = "corr_tc_all_kernel: every tensor-core level of the step, one launch"
+        roof_ops = 2.0 * sum(macs_of_level(s) for s in SIZES)
+        roof_ms = 1e3 * t_kernel / args.steps
+        roof_traffic, roof_src = NCU_ALL_TRAFFIC, NCU_ALL_SOURCE
+    else:
+        roof_kernel = level_roofline["kernel"]
+        roof_ops, roof_ms = ops, 1e3 * t_launch
+        roof_traffic, roof_src = NCU_TRAFFIC.get(dom), NCU_SOURCE
+    roof_achieved = roof_ops / (roof_ms / 1e3) / 1e12
     # The fused epilogue's bound at small s: every candidate costs NCU_INSTR_PER_FIT thread
     # instructions, issued at most one warp instruction per scheduler (4 per SM) per clock.
     epilogue = None
@@ -892,7 +919,7 @@ def run_gpu(args):
     # The single-GPU legs run at N = 1 only: under torchrun the other ranks would sit in
     # the final barrier for their whole duration.
     single = rank == 0 and world == 1
-    encode = run_encode(mb, ctx) if single else None
+    encode = run_encode(mb, ctx) if single and not args.no_encode else None
 
     refine = None
     if single and not args.no_refine:
@@ -921,13 +948,17 @@ def run_gpu(args):
             "config": {"workload": WORKLOAD, "image": "512x512", "sizes": list(SIZES),
                        "shift": SHIFT, "evals_per_step": ev_step, "nodes_per_step": nodes,
                        "parallelism": f"replicas{world}", "l2": "flushed between steps (256 MiB write)"},
-            "roofline": {"bound": "tensor", "kernel": f"search level s={dom}",
-                         "achieved": achieved, "peak": peak_tops, "unit": "TOP/s",
-                         "frac": achieved / peak_tops, "traffic": NCU_TRAFFIC.get(dom),
+            "roofline": {"bound": "tensor", "kernel": roof_kernel,
+                         "achieved": roof_achieved, "peak": peak_tops, "unit": "TOP/s",
+                         "frac": roof_achieved / peak_tops, "traffic": roof_traffic,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                           f"({NCU_SOURCE})",
+                                           f"({roof_src})",
                          "peak_source": peak_src,
-                         "ops_per_launch": ops, "launch_ms": 1e3 * t_launch,
+                         "ops_per_launch": roof_ops, "launch_ms": roof_ms,
+                         "timing": ("CUDA events recorded inside the plan's graph around the "
+                                    "launch (mars_search_plan_kernel_ms), every timed step")
+                                   if kernel_timed else "CUDA events around the level's launches",
+                         "dominant_level": level_roofline,
                          "epilogue": epilogue},
             "per_level_ms": {str(s): 1e3 * per_level[s] / lvl_steps for s in SIZES},
             "launch": "one CUDA-graph launch per step (search plan), "
@@ -964,6 +995,7 @@ def main():
     ap.add_argument("--no-decode", action="store_true", help="skip the decode leg")
     ap.add_argument("--no-refine", action="store_true", help="skip the refinement leg")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
+    ap.add_argument("--no-encode", action="store_true", help="skip the RD encode leg")
     ap.add_argument("--no-classified", action="store_true",
                     help="skip the classified colour leg")
     ap.add_argument("--refine-only", action="store_true",

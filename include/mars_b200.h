@@ -187,6 +187,11 @@ int mars_search_plan_table(mars_search_plan* plan, mars_table** out);
 uint64_t mars_search_plan_evals(const mars_search_plan* plan);
 /* Kernel launches one run replays (the graph's kernel nodes). */
 uint64_t mars_search_plan_launches(const mars_search_plan* plan);
+/* Device time in ms of the last completed replay's all-levels correlation launch (the one
+ * persistent kernel over every tensor-core level), from CUDA events recorded inside the
+ * plan's graph.  MARS_EUNSUPPORTED for plans without that launch (Fisher plans, one launch
+ * per level); MARS_EINVAL before a replay has completed. */
+int mars_search_plan_kernel_ms(const mars_search_plan* plan, float* ms);
 void mars_search_plan_free(mars_search_plan* plan);
 /* mars_encode through a plan (the plan's geometry and parameters): one graph launch for
  * the search, then the walks.  Exhaustive, single-winner, no adaptive density; the

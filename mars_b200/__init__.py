@@ -97,6 +97,7 @@ EXPORTS = (
     "mars_search_plan_create", "mars_search_plan_run", "mars_search_plan_run_device",
     "mars_indexed_plan_create",
     "mars_search_plan_table", "mars_search_plan_evals", "mars_search_plan_launches",
+    "mars_search_plan_kernel_ms",
     "mars_search_plan_free", "mars_decode_until_stable", "mars_decode_plan_run_until_stable",
     "mars_zoom_leaves", "mars_encode_planned",
     "mars_refine_plan_create", "mars_refine_params", "mars_refine_forward",
@@ -148,6 +149,7 @@ def lib():
     L.mars_search_plan_evals.restype = u64
     L.mars_search_plan_launches.argtypes = [vp]
     L.mars_search_plan_launches.restype = u64
+    L.mars_search_plan_kernel_ms.argtypes = [vp, C.POINTER(C.c_float)]
     L.mars_search_plan_free.argtypes = [vp]
     L.mars_search_plan_free.restype = None
     L.mars_search_table_build_ranked.argtypes = [vp, vp, u32, u32, P(Params), C.c_int32, u32, P(vp)]
@@ -627,6 +629,14 @@ class SearchPlan:
     @property
     def launches(self) -> int:
         return lib().mars_search_plan_launches(self._h)
+
+    @property
+    def kernel_ms(self) -> float:
+        """Device time of the last completed replay's all-levels correlation launch
+        (mars_search_plan_kernel_ms)."""
+        v = C.c_float()
+        check(lib().mars_search_plan_kernel_ms(self._h, C.byref(v)))
+        return v.value
 
     def run(self, img) -> GpuSearch:
         a = _plane(img)

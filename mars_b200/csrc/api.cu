@@ -361,12 +361,14 @@ bool tc_digits(const mars_ctx* ctx, const mars::LevelGeom& g) {
 // fits of the 512x512 level 1.09 M -> 0.23 M, 0.98 -> 0.86 ms).  At size 4 its cost
 // outweighs the survivors it saves, and at 16..64 it is neutral or slower.
 constexpr int kCoarseRatio = 4;
+constexpr size_t kCoarseAllLevels = 65536;
 
 // Buffers and tensor maps of a level (g, rs and ds already set).  msplit 0 picks the
 // per-level launch's split count; tickets adds the all-levels launch's per-tile counters;
-// coarse_ok allows the coarse pre-pass (the all-levels launch leaves it out: the pre-pass
-// would sit on the path before the one launch, 0.16 ms at 512 x 512, more than the 0.12 ms
-// of correlation it saves).
+// coarse_ok allows the coarse pre-pass.  The all-levels launch keeps it for large levels
+// only (kCoarseAllLevels ranges and up): the pre-pass sits on the path before the one
+// launch, where at 512 x 512 it costs 0.16 ms, more than the 0.12 ms of correlation it
+// saves; on large planes it is a small part of the step and cuts the level's exact fits.
 // A level whose digit views the driver rejects takes the fold path (L.digits false).
 int tc_level_setup(mars_ctx* ctx, Scratch& sc, uint32_t w, uint32_t h, size_t n, int msplit,
                    bool tickets, bool coarse_ok, TcLevel& L) {
@@ -657,7 +659,8 @@ bool all_levels_eligible(const mars_ctx* ctx, uint32_t w, uint32_t h, const std:
 // holds ctx->mu and has checked all_levels_eligible.
 int run_jobs_all_levels(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w,
                         uint32_t h, const mars::FitParams& fp, const std::vector<Job>& jobs,
-                        mars::CandidateOut* d_out, const uint32_t* d_rc_in) {
+                        mars::CandidateOut* d_out, const uint32_t* d_rc_in,
+                        cudaEvent_t* timing = nullptr) {
     const cudaStream_t main = ctx->stream;
     if (!ctx->fork_ev) {
         MARS_CUDA(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
@@ -727,7 +730,8 @@ int run_jobs_all_levels(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint
         MARS_CUDA(sc.get(&L.ds.detf, ndom));
         MARS_CUDA(sc.get(&L.ds.sdetf, ndom));
         const bool wanted = L.digits;
-        if (int e = tc_level_setup(ctx, sc, w, h, n, std::max(ms[l], tail_ms[l]), true, false, L))
+        if (int e = tc_level_setup(ctx, sc, w, h, n, std::max(ms[l], tail_ms[l]), true,
+                                   n >= kCoarseAllLevels, L))
             return e;
         if (L.digits != wanted)  // the driver rejected the digit views: no fold kernel here
             return fail(MARS_ECUDA, "the split-digit tensor maps were rejected");
@@ -808,8 +812,18 @@ int run_jobs_all_levels(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint
             lj.push_back(J);
         }
     }
+    // Optional timing events around the launch: event-record nodes inside a capture (the
+    // external flag is for captures only), plain records otherwise.
+    unsigned rec_flags = cudaEventRecordDefault;
+    if (timing) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        MARS_CUDA(cudaStreamIsCapturing(main, &cs));
+        if (cs == cudaStreamCaptureStatusActive) rec_flags = cudaEventRecordExternal;
+        MARS_CUDA(cudaEventRecordWithFlags(timing[0], main, rec_flags));
+    }
     MARS_CUDA(mars::tc::launch_corr_all(lj.data(), (int)lj.size(), d_work, ctx->d_err,
                                         ctx->d_counter, ctx->num_sms, main));
+    if (timing) MARS_CUDA(cudaEventRecordWithFlags(timing[1], main, rec_flags));
     ctx->launches += 1;
     return MARS_OK;
 }
@@ -1522,7 +1536,10 @@ mars_search_plan* cached_encode_plan(mars_ctx* ctx, uint32_t w, uint32_t h,
         return nullptr;
     }
     mars_search_plan* plan = nullptr;
-    if (mars_indexed_plan_create(ctx, w, h, p, method, &plan) != MARS_OK) return nullptr;
+    if (mars_indexed_plan_create(ctx, w, h, p, method, &plan) != MARS_OK) {
+        cudaGetLastError();  // the one-shot path serves this call: leave no stale error
+        return nullptr;
+    }
     ctx->plan_cache.emplace_back(key, plan);
     return plan;
 }
@@ -1637,6 +1654,9 @@ struct mars_search_plan {
     double* d_basis = nullptr;
     std::vector<size_t> basis_at;  // per level, into d_basis
     uint64_t nlevels_total = 0;    // sum of size^2 over the nodes
+    // CUDA events recorded inside the graph around the all-levels correlation launch.
+    cudaEvent_t ev_corr[2] = {nullptr, nullptr};
+    bool corr_timed = false;
 };
 
 namespace {
@@ -1662,6 +1682,8 @@ void plan_release(mars_search_plan* p) {
     cudaFree(p->d_wevals);
     cudaFree(p->d_levels_at);
     cudaFree(p->d_basis);
+    if (p->ev_corr[0]) cudaEventDestroy(p->ev_corr[0]);
+    if (p->ev_corr[1]) cudaEventDestroy(p->ev_corr[1]);
     delete p;
 }
 
@@ -1728,9 +1750,14 @@ int plan_enqueue(mars_search_plan* p, bool with_copies) {
                                     p->d_evals, p->d_rc))
             return e;
     } else if (all_levels_eligible(ctx, p->w, p->h, p->jobs)) {
+        if (!p->ev_corr[0]) {
+            MARS_CUDA(cudaEventCreate(&p->ev_corr[0]));
+            MARS_CUDA(cudaEventCreate(&p->ev_corr[1]));
+        }
         if (int e = run_jobs_all_levels(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out,
-                                        p->d_rc))
+                                        p->d_rc, p->ev_corr))
             return e;
+        p->corr_timed = true;
     } else if (int e = run_jobs_branched(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out,
                                          p->d_rc)) {
         return e;
@@ -1911,6 +1938,17 @@ int mars_search_plan_table(mars_search_plan* p, mars_table** out) {
 
 uint64_t mars_search_plan_evals(const mars_search_plan* p) { return p ? p->total_evals : 0; }
 uint64_t mars_search_plan_launches(const mars_search_plan* p) { return p ? p->launches_per_run : 0; }
+
+int mars_search_plan_kernel_ms(const mars_search_plan* p, float* ms) {
+    if (!p || !ms) return fail(MARS_EINVAL, "NULL argument");
+    if (!p->corr_timed)
+        return fail(MARS_EUNSUPPORTED, "this plan has no all-levels correlation launch");
+    MARS_CUDA(cudaSetDevice(p->ctx->device));
+    if (cudaEventQuery(p->ev_corr[1]) != cudaSuccess)
+        return fail(MARS_EINVAL, "no completed replay to time");
+    MARS_CUDA(cudaEventElapsedTime(ms, p->ev_corr[0], p->ev_corr[1]));
+    return MARS_OK;
+}
 
 void mars_search_plan_free(mars_search_plan* p) {
     if (!p) return;

@@ -134,6 +134,9 @@ def test_all_levels_launch_equals_per_level_launches(ctx, w, h, shift, max_size)
             assert z.tobytes() == y.tobytes(), size
             assert np.array_equal(xe, ye) and np.array_equal(ze, ye), size
         assert plan.launches < per_plan.launches
+        assert plan.kernel_ms > 0.0  # events recorded around the launch inside the graph
+        with pytest.raises(mb.MarsError):
+            per_plan.kernel_ms
         for t in (a, b, got):
             t.close()
         plan.close()
