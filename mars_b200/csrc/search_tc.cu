@@ -482,6 +482,22 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
             C.sum = sd.sum;
             C.idx = sd.idx;
             C.t1x4 = sd.t1x4;
+            if (a.gch) {
+                // Start from the range's shared champion when the splits that ran before
+                // this one found a better one than the seed (an atomic 128-bit read).
+                unsigned long long clo, chi;
+                cas128(a.gch + 2 * (size_t)r, 0ull, 0ull, 0ull, 0ull, clo, chi);
+                const uint32_t gidx = (uint32_t)chi;
+                const unsigned long long mlo = (unsigned long long)__double_as_longlong(C.rms);
+                if (clo < mlo || (clo == mlo && gidx < C.idx)) {
+                    const uint32_t dom = gidx >> 3;
+                    C.rms = __longlong_as_double((long long)clo);
+                    C.idx = gidx;
+                    C.t1x4 = (int32_t)(uint32_t)(chi >> 32);
+                    C.sum = fit_exact(N, a.ds.s1x4[dom], a.ds.s2x16[dom], C.t0, (int64_t)C.t1x4,
+                                      C.t2, fp).sum;
+                }
+            }
         } else {
             // Padding of the last N tile, or a block outside the plane: no candidate.
             C.rms = INFINITY;
@@ -1466,6 +1482,10 @@ double all_levels_tile_us(int size, bool digits) {
 }
 constexpr double kItemSetupTiles = 4.0;  // B load, champions, pipeline fill: ~4 tiles
 constexpr int kItemsPerSm = 8;           // work items per SM the splits aim at
+// Longest item the splits allow.  On large planes the levels' phase planes exceed L2; short
+// split-major items keep the CTAs running together inside one band of domain rows (one
+// split), which L2 then holds for all of them.
+constexpr double kMaxItemUs = 1500.0;
 }  // namespace
 
 void all_levels_splits(const LevelGeom* g, const int* nranges, const bool* digits, int n,
@@ -1478,7 +1498,7 @@ void all_levels_splits(const LevelGeom* g, const int* nranges, const bool* digit
         const double ntiles = (double)((nranges[i] + rt - 1) / rt);
         total += ntiles * m_tiles * all_levels_tile_us(g[i].size, digits[i]);
     }
-    const double target = total / ((double)num_sms * kItemsPerSm);
+    const double target = std::min(kMaxItemUs, total / ((double)num_sms * kItemsPerSm));
     int last = -1;
     double last_cost = 0.0;
     for (int i = 0; i < n; ++i) {
