@@ -468,6 +468,52 @@ int run_level_tc(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32
     return MARS_OK;
 }
 
+// The ranked search (k = 2..kMaxTopK) of one level on the tcgen05 path: phase (or digit)
+// planes, the B operand, k seeds per range, the correlation keeping each range's best k,
+// and the merge of the splits' lists (reduce_topk).
+int run_level_tc_topk(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t* d_D,
+                      uint32_t w, uint32_t h, const mars::LevelGeom& g, const mars::FitParams& fp,
+                      const uint32_t* d_rows, const uint32_t* d_cols, size_t n,
+                      mars::RangeStats rs, mars::DomainStats ds, mars::CandidateOut* d_out,
+                      uint32_t k, const uint8_t* d_dplane) {
+    const cudaStream_t st = ctx->stream;
+    uint8_t* d_phases = nullptr;
+    mars::tc::TcMaps maps{};
+    bool digits = tc_digits(ctx, g);
+    if (digits) {
+        MARS_CUDA(sc.get(&d_phases, mars::tc::digit_plane_bytes((int)w, (int)h, g.shift)));
+        digits = make_digit_maps(ctx, d_phases, w, h, (uint32_t)g.shift, &maps);
+    }
+    if (!digits) {
+        MARS_CUDA(sc.get(&d_phases, mars::tc::phase_bytes((int)w, (int)h, g.shift)));
+        if (int e = make_maps(ctx, d_phases, w, h, (uint32_t)g.shift, &maps)) return e;
+    }
+    if (!mars::tc::topk_supported(g.size, digits))
+        return fail(MARS_EUNSUPPORTED, "no ranked tensor-core kernel for this level");
+    uint8_t* d_b = nullptr;
+    mars::tc::SeedOut* d_seed = nullptr;
+    mars::Partial* partials = nullptr;
+    const int msplit = std::min(mars::tc::msplit_for(g, (int)n, ctx->num_sms, digits),
+                                mars::kMaxTopKSplits);
+    MARS_CUDA(sc.get(&d_b, mars::tc::b_bytes(g.size, (int)n, digits)));
+    MARS_CUDA(sc.get(&d_seed, n * k));
+    MARS_CUDA(sc.get(&partials, (size_t)msplit * n * k));
+    if (digits)
+        MARS_CUDA(mars::tc::launch_digit_planes(d_D, (int)w, (int)h, g.shift, d_phases, st));
+    else
+        MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, g.shift, d_phases, st));
+    MARS_CUDA(mars::tc::launch_build_b(g.size, d_plane, (int)w, (int)h, d_rows, d_cols, (int)n,
+                                       d_b, digits, st));
+    MARS_CUDA(mars::tc::launch_seed_topk(d_D, g, d_plane, (int)w, d_rows, d_cols, (int)n, rs, ds,
+                                         fp, (int)k, d_seed, st));
+    MARS_CUDA(mars::tc::launch_corr_topk(maps, d_b, g, (int)n, rs, ds, fp, d_seed, (int)k,
+                                         partials, msplit, digits, ctx->d_err, ctx->d_counter,
+                                         st));
+    MARS_CUDA(mars::launch_reduce_topk(partials, msplit, (int)n, (int)k, g, rs, ds, d_out, st));
+    ctx->launches += 5;
+    return MARS_OK;
+}
+
 // Search every block of one (size, shift) level.  rows/cols/out are device pointers.
 // k > 1: the ranked search (n x k results); k == 1: the single winner.
 // One level of the search: ranges are read from d_plane; domains from d_D (the contracted
@@ -501,6 +547,9 @@ int run_level(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t*
                                        (int)size, fp, rs, st));
     MARS_CUDA(mars::launch_domain_stats(d_D, g, ds, st));
     ctx->launches += 2;
+    if (k > 1 && use_tc(ctx, size, shift) && mars::tc::topk_supported(g.size, tc_digits(ctx, g)))
+        return run_level_tc_topk(ctx, sc, d_plane, d_D, w, h, g, fp, d_rows, d_cols, n, rs, ds,
+                                 d_out, k, d_dplane ? d_dplane : d_plane);
     if (k > 1) {
         const int nsplit = mars::search_topk_splits(g, (int)n, ctx->num_sms);
         mars::Partial* partials;

@@ -78,6 +78,7 @@ cudaError_t launch_reduce(const Partial* partials, int ntiles, int nranges, cons
 // keeping the best k by (rms, reference index); partials are nsplit x nranges x k, the
 // result nranges x k (valid = 0 past the ranked candidates).
 constexpr int kMaxTopK = 8;
+constexpr int kMaxTopKSplits = 64;  // domain-tile splits a ranked search may use
 int search_topk_splits(const LevelGeom& g, int nranges, int num_sms);
 cudaError_t launch_search_topk(const int32_t* D, const uint8_t* plane, int w,
                                const uint32_t* rows, const uint32_t* cols, int nranges,

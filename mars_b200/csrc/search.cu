@@ -28,7 +28,6 @@ constexpr float kHugeSqrtDet = 1.0e15f;
 constexpr int kTileRowsMax = 16;  // domain positions per tile, vertically
 constexpr int kTileColsMax = 32;  // and horizontally
 constexpr size_t kSmemBudget = 200 * 1024;
-constexpr int kMaxTopKSplits = 64;  // domain-tile splits a ranked search may use
 
 // isometry::map (crates/mars-codec/src/isometry.rs:7-19) as a flat range index i*S + j.
 __host__ __device__ constexpr int iso_src(int k, int u, int v, int S) {
@@ -392,10 +391,13 @@ __global__ void reduce_topk_kernel(const Partial* __restrict__ partials, int nsp
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nranges) return;
     const int64_t n = (int64_t)g.size * g.size;
-    // Each split's list is sorted, so one cursor per split walks them in merge order.
+    // Each split's list is sorted, so one cursor per split walks them in merge order.  A
+    // candidate in several splits' lists (the tensor-core kernel's splits all start from the
+    // same seeds) comes out of the merge once: its copies are adjacent in merge order.
     uint8_t cursor[kMaxTopKSplits];
     for (int t = 0; t < nsplit; ++t) cursor[t] = 0;
-    for (int j = 0; j < k; ++j) {
+    uint32_t last = UINT32_MAX;
+    for (int j = 0; j < k;) {
         int bt = -1;
         Partial best;
         best.rms = __longlong_as_double(0x7ff0000000000000ll);
@@ -409,11 +411,16 @@ __global__ void reduce_topk_kernel(const Partial* __restrict__ partials, int nsp
                 bt = t;
             }
         }
+        if (bt >= 0 && best.idx == last) {
+            ++cursor[bt];
+            continue;
+        }
         CandidateOut c;
         if (bt < 0) {
             c = CandidateOut{0, 0, 0, 0, 0, 0, 0.0, 0, 0, 0, 0, 0, 0};
         } else {
             ++cursor[bt];
+            last = best.idx;
             const uint32_t dom = best.idx >> 3;
             c.dom_row = (dom / g.ncol_d) * g.shift;
             c.dom_col = (dom % g.ncol_d) * g.shift;
@@ -430,6 +437,7 @@ __global__ void reduce_topk_kernel(const Partial* __restrict__ partials, int nsp
             c.t2 = rs.t2[r];
         }
         out[(size_t)r * k + j] = c;
+        ++j;
     }
 }
 

@@ -349,6 +349,109 @@ __device__ __forceinline__ void finish_range(const Partial* partials, int nsplit
     out[r] = c;
 }
 
+// The ranked search's lists (search_top_k, encode.rs:695-788): per range of the tile its
+// best k <= kMaxTopK candidates by (rms, reference index), in shared memory after the
+// stages (the ranked kernel only).
+struct TopkLists {
+    double rms[kRangesPerTile][kMaxTopK];
+    double sum[kRangesPerTile][kMaxTopK];
+    uint32_t idx[kRangesPerTile][kMaxTopK];
+    int32_t t1[kRangesPerTile][kMaxTopK];
+    uint32_t q[kRangesPerTile][kMaxTopK];  // qalfa | qbeta << 16
+    int cnt[kRangesPerTile];
+};
+
+// Insert a fitted candidate into range rl's list (capacity k), keeping it sorted by (rms,
+// index) -- retain_top_k's strict-< insertion in encounter order gives the same set.  A
+// candidate already listed (a seed the sweep meets again) is skipped.  True when the list
+// changed.
+__device__ __forceinline__ bool topk_insert(TopkLists& L, int rl, int k, double rms, double sum,
+                                            uint32_t idx, int32_t t1, uint32_t q) {
+    const int c = L.cnt[rl];
+    for (int j = 0; j < c; ++j)
+        if (L.idx[rl][j] == idx) return false;
+    if (c == k && !(rms < L.rms[rl][k - 1] || (rms == L.rms[rl][k - 1] && idx < L.idx[rl][k - 1])))
+        return false;
+    int pos = c < k ? c : k - 1;
+    while (pos > 0 && (rms < L.rms[rl][pos - 1] ||
+                       (rms == L.rms[rl][pos - 1] && idx < L.idx[rl][pos - 1]))) {
+        L.rms[rl][pos] = L.rms[rl][pos - 1];
+        L.sum[rl][pos] = L.sum[rl][pos - 1];
+        L.idx[rl][pos] = L.idx[rl][pos - 1];
+        L.t1[rl][pos] = L.t1[rl][pos - 1];
+        L.q[rl][pos] = L.q[rl][pos - 1];
+        --pos;
+    }
+    L.rms[rl][pos] = rms;
+    L.sum[rl][pos] = sum;
+    L.idx[rl][pos] = idx;
+    L.t1[rl][pos] = t1;
+    L.q[rl][pos] = q;
+    if (c < k) L.cnt[rl] = c + 1;
+    return true;
+}
+
+// The pruning record of a ranked range: against its k-th entry once the list is full (the
+// same bound as the single winner's, fit.cuh); before that every candidate passes (sqrt_w
+// = w2a = -inf: tau = -inf for every domain).
+__device__ __forceinline__ void topk_publish(Smem& sm, const TopkLists& L, int rl, int k,
+                                             const FitParams& fp, int n) {
+    Champ& C = sm.ch[rl];
+    if (!C.valid) {
+        publish_threshold(sm, rl, fp, n);
+        return;
+    }
+    if (L.cnt[rl] < k) {
+        sm.thr[rl] = ThrRec{-INFINITY, -INFINITY, 0.0f, INT32_MAX};
+        return;
+    }
+    C.rms = L.rms[rl][k - 1];
+    C.sum = L.sum[rl][k - 1];
+    C.idx = L.idx[rl][k - 1];
+    publish_threshold(sm, rl, fp, n);
+}
+
+// drain_queue for the ranked search: exact fits of the queued survivors, then one thread per
+// range inserts its range's entries into the range's list and republishes the threshold.
+template <int N, int NT, int RG>
+__device__ __noinline__ void drain_queue_topk(Smem& sm, TopkLists& L, int k, int grp, int n,
+                                              bool mark, uint32_t tag, int gt,
+                                              const DomainStats& ds, const FitParams& fp,
+                                              unsigned long long& exact) {
+    QEntry* const queue = sm.queue[grp];
+    for (int qi = gt; qi < n; qi += kGroupThreads) {
+        QEntry& q = queue[qi];
+        const int col = (int)(q.code & 255u), rl = col >> 3;
+        const Champ& C = sm.ch[rl];
+        const int32_t s1 = ds.s1x4[q.dom];
+        const int64_t t1x4 = (int64_t)q.t1 + 128ll * s1;
+        const FitResult f = fit_exact(N, s1, ds.s2x16[q.dom], C.t0, t1x4, C.t2, fp);
+        q.rms = f.rms;
+        q.sum = f.sum;
+        q.pad = f.qalfa | (f.qbeta << 16);
+        ++exact;
+        if (mark && (q.code >> 16) == tag) {
+            const int qm = (int)(q.code >> 8) & 127;
+            atomicOr(&sm.evaluated[(qm * NT + col) >> 5], 1u << (col & 31));
+        }
+    }
+    group_barrier(grp);
+    const int rl = grp * RG + gt;
+    if (gt < RG && sm.ch[rl].valid) {
+        bool changed = false;
+        for (int qi = 0; qi < n; ++qi) {
+            const QEntry& q = queue[qi];
+            const int col = (int)(q.code & 255u);
+            if ((col >> 3) != rl) continue;
+            changed |= topk_insert(L, rl, k, q.rms, q.sum, q.dom * 8u + (uint32_t)(col & 7),
+                                   q.t1 + 128 * ds.s1x4[q.dom], q.pad);
+        }
+        if (changed) topk_publish(sm, L, rl, k, fp, N);
+    }
+    if (gt == 0) sm.qcount[grp] = 0;
+    group_barrier(grp);
+}
+
 // What one work item reads and writes: a level's B operand, statistics, seeds, its split
 // of the domain tiles and the outputs of its range tile.
 struct ItemArgs {
@@ -364,6 +467,7 @@ struct ItemArgs {
     unsigned long long* gch;  // 2 x nranges shared champion records, or null
     int* tickets;             // per range tile: splits done (all-levels launch), or null
     CandidateOut* out;        // the level's candidates when tickets is set
+    int k;                    // candidates kept per range (> 1: the ranked kernel)
 };
 
 // Per-thread pipeline state of the roles (each role thread keeps its own copy).  It carries
@@ -432,11 +536,12 @@ __device__ __forceinline__ void cta_teardown(Smem& sm, uint32_t tmem, unsigned l
 // tiles, the tile's partial champions written.  With tickets set, the last split of the
 // range tile to finish also writes the tile's final candidates.  Every thread of the CTA
 // calls this together; it begins and ends with a CTA barrier.
-template <int S, bool DIG>
+template <int S, bool DIG, bool TOPK = false>
 __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs& a, int ntile,
                                              int split, Smem& sm, unsigned char* stages,
                                              uint32_t tmem, PipeState& ps, int* err,
-                                             unsigned long long& exact) {
+                                             unsigned long long& exact,
+                                             TopkLists* tk = nullptr) {
     using C_ = Cfg<S, DIG>;
     constexpr int N = S * S;
     constexpr int NT = C_::kNt;
@@ -471,18 +576,32 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
     if (threadIdx.x < RT) {
         Champ& C = sm.ch[threadIdx.x];
         const int r = ntile * RT + threadIdx.x;
-        C.valid = r < nranges && a.seeds[r].idx != UINT32_MAX;
+        const int ks = TOPK ? a.k : 1;  // seeds per range
+        C.valid = r < nranges && a.seeds[(size_t)r * ks].idx != UINT32_MAX;
         if (C.valid) {
             C.t0 = a.rs.t0[r];
             C.t2 = a.rs.t2[r];
             C.nrr = a.rs.nrr[r];
             C.rms0 = a.rs.rms0[r];
-            const SeedOut sd = a.seeds[r];
+            const SeedOut sd = a.seeds[(size_t)r * ks];
             C.rms = sd.rms;
             C.sum = sd.sum;
             C.idx = sd.idx;
             C.t1x4 = sd.t1x4;
-            if (a.gch) {
+            if (TOPK) {
+                // The ranked list starts from the range's k seeds (distinct candidates);
+                // their quantised coefficients come from the same exact fit.
+                tk->cnt[threadIdx.x] = 0;
+                for (int j = 0; j < a.k; ++j) {
+                    const SeedOut sj = a.seeds[(size_t)r * ks + j];
+                    if (sj.idx == UINT32_MAX) continue;
+                    const uint32_t dom = sj.idx >> 3;
+                    const FitResult f = fit_exact(N, a.ds.s1x4[dom], a.ds.s2x16[dom], C.t0,
+                                                  (int64_t)sj.t1x4, C.t2, fp);
+                    topk_insert(*tk, threadIdx.x, a.k, f.rms, f.sum, sj.idx, sj.t1x4,
+                                f.qalfa | (f.qbeta << 16));
+                }
+            } else if (a.gch) {
                 // Start from the range's shared champion when the splits that ran before
                 // this one found a better one than the seed (an atomic 128-bit read).
                 unsigned long long clo, chi;
@@ -507,7 +626,12 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
         }
         sm.key_rms[threadIdx.x] = ~0ull;
         sm.key_idx[threadIdx.x] = UINT32_MAX;
-        publish_threshold(sm, threadIdx.x, fp, N);
+        if (TOPK) {
+            if (!C.valid) tk->cnt[threadIdx.x] = 0;
+            topk_publish(sm, *tk, threadIdx.x, a.k, fp, N);
+        } else {
+            publish_threshold(sm, threadIdx.x, fp, N);
+        }
     }
     __syncthreads();
     volatile int* abort_flag = &sm.abort_flag;
@@ -787,14 +911,23 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
                 const int queued = sm.qcount[part];
                 const bool last = mt + 1 == m_end;
                 if (queued > kQueueCap) {
-                    drain_queue<N, NT, kRangesPerWarp>(sm, part, kQueueCap, true, tag, gt, ds,
-                                                       fp, exact, a.gch, ntile * RT);
+                    if (TOPK)
+                        drain_queue_topk<N, NT, kRangesPerWarp>(sm, *tk, a.k, part, kQueueCap,
+                                                                true, tag, gt, ds, fp, exact);
+                    else
+                        drain_queue<N, NT, kRangesPerWarp>(sm, part, kQueueCap, true, tag, gt,
+                                                           ds, fp, exact, a.gch, ntile * RT);
                     rescan = true;
                     continue;  // pass again over the same accumulator (fresh thresholds)
                 }
-                if (queued >= kFlush || (last && queued > 0))
-                    drain_queue<N, NT, kRangesPerWarp>(sm, part, queued, false, tag, gt, ds,
-                                                       fp, exact, a.gch, ntile * RT);
+                if (queued >= kFlush || (last && queued > 0)) {
+                    if (TOPK)
+                        drain_queue_topk<N, NT, kRangesPerWarp>(sm, *tk, a.k, part, queued,
+                                                                false, tag, gt, ds, fp, exact);
+                    else
+                        drain_queue<N, NT, kRangesPerWarp>(sm, part, queued, false, tag, gt,
+                                                           ds, fp, exact, a.gch, ntile * RT);
+                }
                 break;
             }
             if (rescan) {
@@ -814,7 +947,33 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
     tmem_fence_before();
     __syncthreads();
     tmem_fence_after();
-    if (threadIdx.x < RT) {
+    if (TOPK && threadIdx.x < RT) {
+        // The range's sorted list as this split's k partials (idx UINT32_MAX past its end).
+        const int r = ntile * RT + threadIdx.x;
+        if (r < nranges) {
+            const int c = sm.ch[threadIdx.x].valid ? tk->cnt[threadIdx.x] : 0;
+            for (int j = 0; j < a.k; ++j) {
+                Partial p;
+                if (j < c) {
+                    p.rms = tk->rms[threadIdx.x][j];
+                    p.sum = tk->sum[threadIdx.x][j];
+                    p.idx = tk->idx[threadIdx.x][j];
+                    p.t1x4 = tk->t1[threadIdx.x][j];
+                    p.qalfa = (uint16_t)(tk->q[threadIdx.x][j] & 0xFFFFu);
+                    p.qbeta = (uint16_t)(tk->q[threadIdx.x][j] >> 16);
+                } else {
+                    p.rms = INFINITY;
+                    p.sum = 0.0;
+                    p.idx = UINT32_MAX;
+                    p.t1x4 = 0;
+                    p.qalfa = 0;
+                    p.qbeta = 0;
+                }
+                p.pad = 0;
+                a.partials[((size_t)split * nranges + r) * a.k + j] = p;
+            }
+        }
+    } else if (threadIdx.x < RT) {
         const Champ& C = sm.ch[threadIdx.x];
         const int r = ntile * RT + threadIdx.x;
         if (r < nranges) {
@@ -846,8 +1005,17 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
     }
 }
 
-// The correlation of one level: CTA (x, y) = range tile x against domain-tile split y.
+// Shared-memory bytes of a level's pipeline stages (A, and B stages or the resident B tile).
 template <int S, bool DIG>
+__host__ __device__ constexpr size_t stage_bytes() {
+    using C_ = Cfg<S, DIG>;
+    return (size_t)C_::kStages * C_::kDigits * kStageA +
+           (C_::kBRes ? (size_t)C_::KST * C_::kStageBt : (size_t)C_::kStages * C_::kStageBt);
+}
+
+// The correlation of one level: CTA (x, y) = range tile x against domain-tile split y.
+// TOPK: the ranked search (a.k candidates per range; its lists after the stages).
+template <int S, bool DIG, bool TOPK>
 __global__ void __launch_bounds__(kThreads, 1)
     corr_tc_kernel(const __grid_constant__ TcMaps maps, const __grid_constant__ ItemArgs a,
                    int* __restrict__ err,
@@ -855,10 +1023,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     Smem& sm = smem_record(smem_raw);
     unsigned char* stages = reinterpret_cast<unsigned char*>(&sm) + kSmemHead;
+    TopkLists* tk = TOPK ? reinterpret_cast<TopkLists*>(stages + stage_bytes<S, DIG>()) : nullptr;
     const uint32_t tmem = cta_setup(sm);
     PipeState ps;
     unsigned long long exact = 0;
-    process_item<S, DIG>(maps, a, blockIdx.x, blockIdx.y, sm, stages, tmem, ps, err, exact);
+    process_item<S, DIG, TOPK>(maps, a, blockIdx.x, blockIdx.y, sm, stages, tmem, ps, err, exact,
+                               tk);
     cta_teardown(sm, tmem, exact, exact_counter);
 }
 
@@ -1148,6 +1318,95 @@ __global__ void __launch_bounds__(288) seed_kernel(
     }
 }
 
+// Seeds of the ranked search: the same 72 candidates as seed_kernel (3 x 3 domains around
+// the co-located one x 8 isometries, exact int32 correlations, exact fits), of which the
+// best k distinct ones by (rms, reference index) start the range's list.  The patch is
+// clamped to the pool, so a domain can appear twice; "distinct" drops the repeats.  At least
+// one domain x 8 isometries is always there, so k <= 8 candidates exist.
+template <int S>
+__global__ void __launch_bounds__(288) seed_topk_kernel(
+    const int32_t* __restrict__ D, LevelGeom g, const uint8_t* __restrict__ plane, int w,
+    const uint32_t* rows, const uint32_t* cols, int nranges, RangeStats rs, DomainStats ds,
+    FitParams fp, int k, SeedOut* __restrict__ out) {
+    constexpr int N = S * S;
+    __shared__ uint8_t rsm[N];
+    __shared__ double c_rms[72], c_sum[72];
+    __shared__ uint32_t c_idx[72];
+    __shared__ int32_t c_t1[72];
+    const int r = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (r >= nranges) return;
+    if (rows[r] + (uint32_t)S > (uint32_t)g.h || cols[r] + (uint32_t)S > (uint32_t)g.w) {
+        if (threadIdx.x < k) out[(size_t)r * k + threadIdx.x] = SeedOut{INFINITY, 0.0, UINT32_MAX, 0};
+        return;
+    }
+    const uint8_t* rb = plane + (size_t)rows[r] * w + cols[r];
+    for (int t = threadIdx.x; t < N; t += blockDim.x) rsm[t] = rb[(size_t)(t / S) * w + (t % S)];
+    __syncthreads();
+    const int ac = min(max(((int)rows[r] - S / 2 + g.shift / 2) / g.shift, 0), g.nrow_d - 1);
+    const int bc = min(max(((int)cols[r] - S / 2 + g.shift / 2) / g.shift, 0), g.ncol_d - 1);
+    const int nb = warp;
+    const int a = min(max(ac + nb / 3 - 1, 0), g.nrow_d - 1);
+    const int bb = min(max(bc + nb % 3 - 1, 0), g.ncol_d - 1);
+    const int32_t* db = D + (size_t)(a * g.step_c) * g.dw + bb * g.step_c;
+    int32_t acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] = 0;
+    for (int t = lane; t < N; t += 32) {
+        const int u = t / S, v = t % S;
+        const int32_t d = db[(size_t)u * g.dw + v];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] += (int32_t)rsm[iso_src_rt(q, u, v, S)] * d;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+    if (lane < 8) {
+        int32_t t1 = acc[0];
+#pragma unroll
+        for (int q = 1; q < 8; ++q) t1 = lane == q ? acc[q] : t1;
+        const uint32_t dom = (uint32_t)(a * g.ncol_d + bb);
+        const FitResult f = fit_exact(N, ds.s1x4[dom], ds.s2x16[dom], rs.t0[r], t1, rs.t2[r], fp);
+        c_rms[nb * 8 + lane] = f.rms;
+        c_sum[nb * 8 + lane] = f.sum;
+        c_idx[nb * 8 + lane] = dom * 8u + (uint32_t)lane;
+        c_t1[nb * 8 + lane] = t1;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // k rounds of a warp arg-min over the candidates strictly after the previous pick
+        // in (rms, index) order.
+        double pr = 0.0;
+        uint32_t pi = 0;
+        for (int j = 0; j < k; ++j) {
+            int b = -1;
+            for (int c = lane; c < 72; c += 32) {
+                if (j > 0 && !(c_rms[c] > pr || (c_rms[c] == pr && c_idx[c] > pi))) continue;
+                if (b < 0 || c_rms[c] < c_rms[b] || (c_rms[c] == c_rms[b] && c_idx[c] < c_idx[b]))
+                    b = c;
+            }
+            double br = b < 0 ? INFINITY : c_rms[b];
+            uint32_t bi = b < 0 ? UINT32_MAX : c_idx[b];
+            for (int o = 16; o > 0; o >>= 1) {
+                const double r2 = __shfl_xor_sync(0xffffffffu, br, o);
+                const uint32_t i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+                const int b2 = __shfl_xor_sync(0xffffffffu, b, o);
+                if (r2 < br || (r2 == br && i2 < bi)) {
+                    br = r2;
+                    bi = i2;
+                    b = b2;
+                }
+            }
+            if (lane == 0)
+                out[(size_t)r * k + j] = b < 0 ? SeedOut{INFINITY, 0.0, UINT32_MAX, 0}
+                                               : SeedOut{c_rms[b], c_sum[b], c_idx[b], c_t1[b]};
+            pr = br;
+            pi = bi;
+        }
+    }
+}
+
 constexpr int kSeedSide = 3;                       // seed domains: a 3 x 3 patch
 constexpr int kSeedCands = 8 * kSeedSide * kSeedSide;  // x 8 isometries
 
@@ -1272,31 +1531,34 @@ template <int S, bool DIG>
 constexpr size_t smem_bytes() {
     using C_ = Cfg<S, DIG>;
     static_assert(C_::kStages <= kMaxStages, "pipeline depth");
-    return 1024 + kSmemHead + (size_t)C_::kStages * C_::kDigits * kStageA +
-           (C_::kBRes ? (size_t)C_::KST * C_::kStageBt : (size_t)C_::kStages * C_::kStageBt);
+    return 1024 + kSmemHead + stage_bytes<S, DIG>();
 }
+static_assert(smem_bytes<32, true>() + sizeof(TopkLists) <= 232448 &&
+                  smem_bytes<64, true>() + sizeof(TopkLists) <= 232448 &&
+                  smem_bytes<4, false>() + sizeof(TopkLists) <= 232448,
+              "shared memory per CTA of the ranked kernel (227 KB)");
 static_assert(smem_bytes<4, false>() <= 232448 && smem_bytes<8, false>() <= 232448 &&
                   smem_bytes<16, false>() <= 232448 && smem_bytes<32, false>() <= 232448 &&
                   smem_bytes<16, true>() <= 232448 && smem_bytes<32, true>() <= 232448 &&
                   smem_bytes<64, true>() <= 232448,
               "shared memory per CTA (227 KB)");
 
-template <int S, bool DIG>
+template <int S, bool DIG, bool TOPK = false>
 cudaError_t launch_t(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g, int nranges,
                      RangeStats rs, DomainStats ds, const FitParams& fp, const SeedOut* seeds,
                      Partial* partials, unsigned long long* gch, int msplit, int* err,
-                     unsigned long long* counter, cudaStream_t st) {
+                     unsigned long long* counter, cudaStream_t st, int k = 1) {
     const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
     const int m_tiles = g.nrow_d * tiles_per_row;
     const int m_per_cta = (m_tiles + msplit - 1) / msplit;
     const int ntiles = (nranges + Cfg<S, DIG>::kRt - 1) / Cfg<S, DIG>::kRt;
-    const size_t smem = smem_bytes<S, DIG>();
-    auto kern = corr_tc_kernel<S, DIG>;
+    const size_t smem = smem_bytes<S, DIG>() + (TOPK ? sizeof(TopkLists) : 0);
+    auto kern = corr_tc_kernel<S, DIG, TOPK>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 grid(ntiles, msplit);
     const ItemArgs a{bglob, g,        nranges,  rs,       ds,      fp,     seeds,
-                     m_tiles, m_per_cta, msplit, partials, gch, nullptr, nullptr};
+                     m_tiles, m_per_cta, msplit, partials, gch, nullptr, nullptr, k};
     kern<<<grid, kThreads, smem, st>>>(maps, a, err, counter);
     return cudaGetLastError();
 }
@@ -1558,7 +1820,7 @@ cudaError_t launch_corr_all(const LevelJob* jobs, int njobs, int* work, int* err
                              J.rs,     J.ds,     J.fp,
                              J.seeds,  m_tiles,  (m_tiles + J.msplit - 1) / J.msplit,
                              J.msplit, J.partials, J.gch,
-                             J.tickets, J.out};
+                             J.tickets, J.out, 1};
         L.kind[k] = all_levels_kind(J.g.size, J.digits != 0);
         L.tile_begin[k] = J.tile_begin;
         L.tile_count[k] = J.tile_count;
@@ -1580,6 +1842,54 @@ cudaError_t launch_corr_all(const LevelJob* jobs, int njobs, int* work, int* err
     if (e != cudaSuccess) return e;
     const int grid = std::min(nitems, num_sms);
     corr_tc_all_kernel<<<grid, kThreads, smem, st>>>(L, work, err, counter);
+    return cudaGetLastError();
+}
+
+bool topk_supported(int size, bool digits) { return all_levels_supported(size, digits); }
+
+cudaError_t launch_corr_topk(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g,
+                             int nranges, RangeStats rs, DomainStats ds, const FitParams& fp,
+                             const SeedOut* seeds, int k, Partial* partials, int msplit,
+                             bool digits, int* err, unsigned long long* counter,
+                             cudaStream_t st) {
+    if (k < 2 || k > kMaxTopK) return cudaErrorInvalidValue;
+#define MARS_CORR_TOPK(S_, D_)                                                                  \
+    launch_t<S_, D_, true>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, nullptr, msplit, \
+                           err, counter, st, k)
+    if (digits) {
+        switch (g.size) {
+            case 16: return MARS_CORR_TOPK(16, true);
+            case 32: return MARS_CORR_TOPK(32, true);
+            case 64: return MARS_CORR_TOPK(64, true);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (g.size) {
+        case 4: return MARS_CORR_TOPK(4, false);
+        case 8: return MARS_CORR_TOPK(8, false);
+        default: return cudaErrorInvalidValue;
+    }
+#undef MARS_CORR_TOPK
+}
+
+cudaError_t launch_seed_topk(const int32_t* D, const LevelGeom& g, const uint8_t* plane, int w,
+                             const uint32_t* rows, const uint32_t* cols, int nranges,
+                             RangeStats rs, DomainStats ds, const FitParams& fp, int k,
+                             SeedOut* out, cudaStream_t st) {
+    if (nranges == 0) return cudaSuccess;
+    if (k < 1 || k > kMaxTopK) return cudaErrorInvalidValue;
+#define MARS_SEED_TOPK(S_)                                                                   \
+    seed_topk_kernel<S_><<<nranges, 288, 0, st>>>(D, g, plane, w, rows, cols, nranges, rs, ds, \
+                                                  fp, k, out)
+    switch (g.size) {
+        case 4: MARS_SEED_TOPK(4); break;
+        case 8: MARS_SEED_TOPK(8); break;
+        case 16: MARS_SEED_TOPK(16); break;
+        case 32: MARS_SEED_TOPK(32); break;
+        case 64: MARS_SEED_TOPK(64); break;
+        default: return cudaErrorInvalidValue;
+    }
+#undef MARS_SEED_TOPK
     return cudaGetLastError();
 }
 

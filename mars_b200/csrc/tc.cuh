@@ -96,6 +96,20 @@ cudaError_t launch_corr(const TcMaps& maps, const uint8_t* bglob, const LevelGeo
 // counter it zeroes first.
 cudaError_t launch_corr_all(const LevelJob* jobs, int njobs, int* work, int* err,
                             unsigned long long* counter, int num_sms, cudaStream_t st);
+// The ranked search (k = 2..kMaxTopK candidates per range) on the tcgen05 path, for the
+// kinds the all-levels kernel holds: seeds (n x k, the best k distinct of the 72 seed
+// candidates), then the correlation, whose partials are msplit x n x k sorted lists
+// (launch_reduce_topk merges them).
+bool topk_supported(int size, bool digits);
+cudaError_t launch_seed_topk(const int32_t* D, const LevelGeom& g, const uint8_t* plane, int w,
+                             const uint32_t* rows, const uint32_t* cols, int nranges,
+                             RangeStats rs, DomainStats ds, const FitParams& fp, int k,
+                             SeedOut* out, cudaStream_t st);
+cudaError_t launch_corr_topk(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g,
+                             int nranges, RangeStats rs, DomainStats ds, const FitParams& fp,
+                             const SeedOut* seeds, int k, Partial* partials, int msplit,
+                             bool digits, int* err, unsigned long long* counter,
+                             cudaStream_t st);
 cudaError_t launch_seed_merge(const Partial* partials, int nsplit, int nranges, int coarse_ncol,
                               int fine_ncol, int ratio, SeedOut* seeds, cudaStream_t st);
 cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,
