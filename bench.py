@@ -607,6 +607,42 @@ def run_uneven(mb, ctx, dev, large=True):
     return out
 
 
+RANKED_K = 3  # candidates per node of the ranked-search leg (rd_candidates)
+
+
+def run_ranked(mb, ctx, dev):
+    """Ranked search (search_candidates, k = RANKED_K): every RD-quadtree node of the 512x512
+    planes of the search leg through the ranked provider factory, host plane in and host
+    table out, on the tensor-core kernel and (beside it) the CUDA-core kernel."""
+    import torch
+    params = mb.make_params(min_size=4, max_size=32, shift=SHIFT)
+    imgs = [synthetic.gray(W, H, s) for s in (1, 2, 3)]
+
+    def timed(c):
+        c.search_provider(imgs[0], params, k=RANKED_K).close()
+        torch.cuda.synchronize(dev)
+        ev = 0
+        t0 = time.perf_counter()
+        for im in imgs:
+            prov = c.search_provider(im, params, k=RANKED_K)
+            ev += int(mb.lib().mars_search_table_evals(prov._h))
+            prov.close()
+        return ev / (time.perf_counter() - t0)
+
+    tc = timed(ctx)
+    simt_ctx = mb.Context(dev.index)
+    simt_ctx.set_search_path("simt")
+    try:
+        simt = timed(simt_ctx)
+    finally:
+        simt_ctx.close()
+    return {"workload": f"ranked search (k = {RANKED_K}) of every RD quadtree node of 512x512 "
+                        "synthetic gray planes (seeds 1-3), sizes 32..4, domain stride 2",
+            "value": tc, "unit": "fits/s", "cuda_core_value": simt,
+            "timing": "host wall clock around the ranked provider factory "
+                      "(mars_search_table_build_ranked: host plane in, k-lists out)"}
+
+
 LARGE_BLOCKS = 1024  # range blocks per level of the large-plane profile case
 
 
@@ -933,6 +969,8 @@ def run_gpu(args):
     if single and not args.no_classified:
         classified = run_classified(mb, ctx)
 
+    ranked = run_ranked(mb, ctx, dev) if single and not args.no_ranked else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, desc, ns1, secs = cpu_baseline()
@@ -976,6 +1014,7 @@ def run_gpu(args):
             "refine": refine,
             "uneven": uneven,
             "classified": classified,
+            "ranked": ranked,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -996,6 +1035,7 @@ def main():
     ap.add_argument("--no-refine", action="store_true", help="skip the refinement leg")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg")
     ap.add_argument("--no-encode", action="store_true", help="skip the RD encode leg")
+    ap.add_argument("--no-ranked", action="store_true", help="skip the ranked-search leg")
     ap.add_argument("--no-classified", action="store_true",
                     help="skip the classified colour leg")
     ap.add_argument("--refine-only", action="store_true",
