@@ -341,6 +341,8 @@ struct TcLevel {
     mars::Partial* partials = nullptr;
     unsigned long long* gch = nullptr;
     int* tickets = nullptr;  // all-levels launch only
+    int* coarse_tickets = nullptr;  // all-levels launch: the in-kernel coarse pre-pass
+    int* ready = nullptr;
     int tail_tiles = 0, tail_msplit = 0;  // all-levels launch: the finer-split tail
     bool coarse = false;
     mars::LevelGeom g1{};
@@ -413,8 +415,9 @@ int tc_level_setup(mars_ctx* ctx, Scratch& sc, uint32_t w, uint32_t h, size_t n,
 }
 
 // Everything of a level before its correlation, on stream st: phase (or digit phase)
-// copies, the B operand, seed champions, the coarse pre-pass, the shared champion records
-// and tickets.
+// copies, the B operand, seed champions, the coarse pre-pass (its statistics and planes
+// only when the all-levels launch runs it: L.ready set), the shared champion records and
+// tickets.
 int tc_level_prep(mars_ctx* ctx, const TcLevel& L, const uint8_t* d_plane, const int32_t* d_D,
                   const uint8_t* d_dplane, uint32_t w, uint32_t h, const mars::FitParams& fp,
                   const uint32_t* d_rows, const uint32_t* d_cols, cudaStream_t st) {
@@ -432,12 +435,20 @@ int tc_level_prep(mars_ctx* ctx, const TcLevel& L, const uint8_t* d_plane, const
     if (L.coarse) {
         MARS_CUDA(mars::launch_domain_stats(d_D, L.g1, L.ds1, st));
         MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, L.g1.shift, L.d_ph1, st));
-        MARS_CUDA(mars::tc::launch_corr(L.maps1, L.d_b, L.g1, n, L.rs, L.ds1, fp, L.d_seed,
-                                        L.part1, nullptr, L.ms1, false, ctx->d_err,
-                                        ctx->d_counter, st));
-        MARS_CUDA(mars::tc::launch_seed_merge(L.part1, L.ms1, n, L.g1.ncol_d, g.ncol_d,
-                                              kCoarseRatio, L.d_seed, st));
-        ctx->launches += 4;
+        ctx->launches += 2;
+        if (L.ready) {
+            const int rt = mars::tc::ranges_per_tile(false);
+            const size_t nt = (L.n + rt - 1) / rt;
+            MARS_CUDA(cudaMemsetAsync(L.ready, 0, nt * sizeof(int), st));
+            MARS_CUDA(cudaMemsetAsync(L.coarse_tickets, 0, nt * sizeof(int), st));
+        } else {
+            MARS_CUDA(mars::tc::launch_corr(L.maps1, L.d_b, L.g1, n, L.rs, L.ds1, fp, L.d_seed,
+                                            L.part1, nullptr, L.ms1, false, ctx->d_err,
+                                            ctx->d_counter, st));
+            MARS_CUDA(mars::tc::launch_seed_merge(L.part1, L.ms1, n, L.g1.ncol_d, g.ncol_d,
+                                                  kCoarseRatio, L.d_seed, st));
+            ctx->launches += 2;
+        }
     }
     MARS_CUDA(cudaMemsetAsync(L.gch, 0xFF, 2 * L.n * sizeof(unsigned long long), st));
     if (L.tickets) {
@@ -697,7 +708,8 @@ bool all_levels_eligible(const mars_ctx* ctx, uint32_t w, uint32_t h, const std:
         if (!mars::tc::all_levels_supported(g.size, tc_digits(ctx, g))) return false;
         ++levels;
     }
-    return levels > 0 && levels < mars::tc::kMaxLevelJobs;  // a level may add a tail job
+    // A level may add a tail job, and the block-size-8 level a coarse pre-pass job.
+    return levels > 0 && levels + 2 <= mars::tc::kMaxLevelJobs;
 }
 
 // run_jobs for the exhaustive single-candidate search with the correlation of every
@@ -787,6 +799,12 @@ int run_jobs_all_levels(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint
         L.msplit = ms[l];
         L.tail_tiles = tail_t[l];
         L.tail_msplit = tail_ms[l];
+        if (L.coarse) {
+            // The coarse pre-pass runs inside the launch, ahead of this level's items.
+            const int rt = mars::tc::ranges_per_tile(false);
+            MARS_CUDA(sc.get(&L.ready, (n + rt - 1) / rt));
+            MARS_CUDA(sc.get(&L.coarse_tickets, (n + rt - 1) / rt));
+        }
     }
     int* d_work = nullptr;
     MARS_CUDA(sc.get(&d_work, 1));
@@ -853,6 +871,27 @@ int run_jobs_all_levels(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint
         J.tile_begin = 0;
         J.tile_count = ntiles - L.tail_tiles;
         J.msplit = L.msplit;
+        if (L.coarse) {
+            // The pre-pass job: the same B operand and ranges, the coarse grid's planes and
+            // statistics; its last split of each tile merges the tile's seeds.
+            mars::tc::LevelJob C = J;
+            C.maps = L.maps1;
+            C.g = L.g1;
+            C.ds = L.ds1;
+            C.partials = L.part1;
+            C.gch = nullptr;
+            C.tickets = L.coarse_tickets;
+            C.out = nullptr;
+            C.tile_begin = 0;
+            C.tile_count = ntiles;
+            C.msplit = L.ms1;
+            C.merge_seeds = L.d_seed;
+            C.merge_ratio = kCoarseRatio;
+            C.fine_ncol = L.g.ncol_d;
+            C.ready = L.ready;
+            lj.push_back(C);
+            J.wait_ready = L.ready;
+        }
         lj.push_back(J);
         if (L.tail_tiles > 0) {
             J.tile_begin = ntiles - L.tail_tiles;

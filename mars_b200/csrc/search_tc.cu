@@ -452,6 +452,62 @@ __device__ __noinline__ void drain_queue_topk(Smem& sm, TopkLists& L, int k, int
     group_barrier(grp);
 }
 
+// A seed read around L1: in the all-levels launch another CTA may have just merged it.
+__device__ __forceinline__ SeedOut load_seed(const SeedOut* p) {
+    const uint2 it = __ldcg(reinterpret_cast<const uint2*>(p) + 2);
+    return SeedOut{__ldcg(reinterpret_cast<const double*>(p)),
+                   __ldcg(reinterpret_cast<const double*>(p) + 1), it.x, (int32_t)it.y};
+}
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// The coarse pre-pass's champion of range r (the best of its M-splits over every
+// `ratio`-th domain position of each axis) as a seed on the full grid: its domain index is
+// mapped to the fine grid, and it replaces the seed when it is better by (rms, index).
+// Any real candidate is a valid seed; a better one prunes more from the first tile.
+__device__ __forceinline__ void seed_merge_range(const Partial* partials, int nsplit, int nranges,
+                                                 int r, int coarse_ncol, int fine_ncol,
+                                                 int ratio, SeedOut* seeds) {
+    const SeedOut s = load_seed(seeds + r);
+    if (s.idx == UINT32_MAX) return;  // no range block here
+    // The pre-pass started from this seed, whose index is on the fine grid.  A split's
+    // champion only ever changes to a strictly better (rms, index) pair, so a partial equal
+    // to the seed's pair is the seed itself; every other one is a coarse-grid candidate.
+    bool have = false;
+    double best_rms = 0.0, best_sum = 0.0;
+    uint32_t best_idx = UINT32_MAX;
+    int32_t best_t1 = 0;
+    for (int t = 0; t < nsplit; ++t) {
+        const Partial* p = partials + (size_t)t * nranges + r;
+        const double rms = __ldcg(reinterpret_cast<const double*>(p));
+        const double sum = __ldcg(reinterpret_cast<const double*>(p) + 1);
+        const uint2 it = __ldcg(reinterpret_cast<const uint2*>(p) + 2);
+        if (it.x == UINT32_MAX || (rms == s.rms && it.x == s.idx)) continue;
+        if (!have || rms < best_rms || (rms == best_rms && it.x < best_idx)) {
+            best_rms = rms;
+            best_sum = sum;
+            best_idx = it.x;
+            best_t1 = (int32_t)it.y;
+        }
+        have = true;
+    }
+    if (!have) return;
+    const uint32_t dom1 = best_idx >> 3;
+    const uint32_t a1 = dom1 / (uint32_t)coarse_ncol, b1 = dom1 % (uint32_t)coarse_ncol;
+    const uint32_t idx =
+        ((a1 * (uint32_t)ratio) * (uint32_t)fine_ncol + b1 * (uint32_t)ratio) * 8u + (best_idx & 7u);
+    if (best_rms < s.rms || (best_rms == s.rms && idx < s.idx))
+        seeds[r] = SeedOut{best_rms, best_sum, idx, best_t1};
+}
+
 // What one work item reads and writes: a level's B operand, statistics, seeds, its split
 // of the domain tiles and the outputs of its range tile.
 struct ItemArgs {
@@ -468,6 +524,13 @@ struct ItemArgs {
     int* tickets;             // per range tile: splits done (all-levels launch), or null
     CandidateOut* out;        // the level's candidates when tickets is set
     int k;                    // candidates kept per range (> 1: the ranked kernel)
+    // The all-levels launch's coarse pre-pass job: the last split of a range tile merges
+    // the tile's champions into merge_seeds (the fine level's seeds) and sets ready[tile];
+    // the fine level's items wait for wait_ready[tile] before reading their seeds.
+    SeedOut* merge_seeds;
+    int merge_ratio, fine_ncol;
+    int* ready;
+    const int* wait_ready;
 };
 
 // Per-thread pipeline state of the roles (each role thread keeps its own copy).  It carries
@@ -573,17 +636,33 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
     const int tiles_per_row = (g.ncol_d + kM - 1) / kM;
     const uint8_t* btile = a.bglob + (size_t)ntile * KST * kStageB;
 
+    if (a.wait_ready) {
+        // The coarse pre-pass items of this range tile were claimed before any item of this
+        // level, by CTAs that are running them: the wait ends (bounded all the same).
+        if (threadIdx.x == 0) {
+            const long long t0 = clock64();
+            while (ld_acquire_gpu(a.wait_ready + ntile) == 0) {
+                if (clock64() - t0 > kWaitCycles) {
+                    sm.abort_flag = 1;
+                    atomicOr(err, 32);
+                    break;
+                }
+                __nanosleep(256);
+            }
+        }
+        __syncthreads();
+    }
     if (threadIdx.x < RT) {
         Champ& C = sm.ch[threadIdx.x];
         const int r = ntile * RT + threadIdx.x;
         const int ks = TOPK ? a.k : 1;  // seeds per range
-        C.valid = r < nranges && a.seeds[(size_t)r * ks].idx != UINT32_MAX;
+        C.valid = r < nranges && load_seed(a.seeds + (size_t)r * ks).idx != UINT32_MAX;
         if (C.valid) {
             C.t0 = a.rs.t0[r];
             C.t2 = a.rs.t2[r];
             C.nrr = a.rs.nrr[r];
             C.rms0 = a.rs.rms0[r];
-            const SeedOut sd = a.seeds[(size_t)r * ks];
+            const SeedOut sd = load_seed(a.seeds + (size_t)r * ks);
             C.rms = sd.rms;
             C.sum = sd.sum;
             C.idx = sd.idx;
@@ -999,8 +1078,16 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
         if (sm.last) {
             __threadfence();
             const int r = ntile * RT + threadIdx.x;
-            if (threadIdx.x < RT && r < nranges)
+            if (a.merge_seeds) {
+                if (threadIdx.x < RT && r < nranges)
+                    seed_merge_range(a.partials, a.msplit, nranges, r, g.ncol_d, a.fine_ncol,
+                                     a.merge_ratio, a.merge_seeds);
+                __threadfence();
+                __syncthreads();
+                if (threadIdx.x == 0) st_release_gpu(a.ready + ntile, 1);
+            } else if (threadIdx.x < RT && r < nranges) {
                 finish_range(a.partials, a.msplit, nranges, r, g, a.rs, ds, fp, a.out);
+            }
         }
     }
 }
@@ -1488,35 +1575,14 @@ __global__ void __launch_bounds__(256) seed_small_kernel(
     if (lane == bl) out[r] = SeedOut{best, best_sum, best_idx, best_t1};
 }
 
-// The coarse pre-pass's champion of each range (the best of its M-splits over every
-// `ratio`-th domain position of each axis) as a seed on the full grid: its domain index is
-// mapped to the fine grid, and it replaces the seed when it is better by (rms, index).
-// Any real candidate is a valid seed; a better one prunes more from the first tile.
+// The coarse pre-pass's seeds merged into the full grid's (seed_merge_range), one thread
+// per range.
 __global__ void seed_merge_kernel(const Partial* __restrict__ partials, int nsplit, int nranges,
                                   int coarse_ncol, int fine_ncol, int ratio,
                                   SeedOut* __restrict__ seeds) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nranges) return;
-    const SeedOut s = seeds[r];
-    if (s.idx == UINT32_MAX) return;  // no range block here
-    // The pre-pass started from this seed, whose index is on the fine grid.  A split's
-    // champion only ever changes to a strictly better (rms, index) pair, so a partial equal
-    // to the seed's pair is the seed itself; every other one is a coarse-grid candidate.
-    bool have = false;
-    Partial best{};
-    for (int t = 0; t < nsplit; ++t) {
-        const Partial p = partials[(size_t)t * nranges + r];
-        if (p.idx == UINT32_MAX || (p.rms == s.rms && p.idx == s.idx)) continue;
-        if (!have || p.rms < best.rms || (p.rms == best.rms && p.idx < best.idx)) best = p;
-        have = true;
-    }
-    if (!have) return;
-    const uint32_t dom1 = best.idx >> 3;
-    const uint32_t a1 = dom1 / (uint32_t)coarse_ncol, b1 = dom1 % (uint32_t)coarse_ncol;
-    const uint32_t idx =
-        ((a1 * (uint32_t)ratio) * (uint32_t)fine_ncol + b1 * (uint32_t)ratio) * 8u + (best.idx & 7u);
-    if (best.rms < s.rms || (best.rms == s.rms && idx < s.idx))
-        seeds[r] = SeedOut{best.rms, best.sum, idx, best.t1x4};
+    if (r < nranges)
+        seed_merge_range(partials, nsplit, nranges, r, coarse_ncol, fine_ncol, ratio, seeds);
 }
 
 // Final champion over the M-splits of each range (finish_range).
@@ -1558,7 +1624,8 @@ cudaError_t launch_t(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& 
     if (e != cudaSuccess) return e;
     dim3 grid(ntiles, msplit);
     const ItemArgs a{bglob, g,        nranges,  rs,       ds,      fp,     seeds,
-                     m_tiles, m_per_cta, msplit, partials, gch, nullptr, nullptr, k};
+                     m_tiles, m_per_cta, msplit, partials, gch, nullptr, nullptr, k,
+                     nullptr, 0, 0, nullptr, nullptr};
     kern<<<grid, kThreads, smem, st>>>(maps, a, err, counter);
     return cudaGetLastError();
 }
@@ -1804,6 +1871,7 @@ cudaError_t launch_corr_all(const LevelJob* jobs, int njobs, int* work, int* err
         const int m_tiles = J.g.nrow_d * tiles_per_row;
         const int m_per = (m_tiles + J.msplit - 1) / J.msplit;
         cost[i] = (m_per + kItemSetupTiles) * all_levels_tile_us(J.g.size, J.digits != 0);
+        if (J.merge_seeds) cost[i] = 1e30;  // coarse pre-pass jobs first: others wait on them
         order[i] = i;
     }
     std::sort(order, order + njobs, [&](int x, int y) { return cost[x] > cost[y]; });
@@ -1820,7 +1888,9 @@ cudaError_t launch_corr_all(const LevelJob* jobs, int njobs, int* work, int* err
                              J.rs,     J.ds,     J.fp,
                              J.seeds,  m_tiles,  (m_tiles + J.msplit - 1) / J.msplit,
                              J.msplit, J.partials, J.gch,
-                             J.tickets, J.out, 1};
+                             J.tickets, J.out, 1,
+                             J.merge_seeds, J.merge_ratio, J.fine_ncol,
+                             J.ready, J.wait_ready};
         L.kind[k] = all_levels_kind(J.g.size, J.digits != 0);
         L.tile_begin[k] = J.tile_begin;
         L.tile_count[k] = J.tile_count;

@@ -52,6 +52,14 @@ struct LevelJob {
     CandidateOut* out;
     int tile_begin, tile_count, msplit;
     int digits;
+    // A coarse pre-pass job (merge_seeds set) runs before every other job: the last split
+    // of each range tile merges its champions into merge_seeds (the fine level's seeds, fine
+    // grid fine_ncol, coarse stride merge_ratio times the fine one) and sets ready[tile]
+    // (zero before the launch); the fine level's jobs pass the same array as wait_ready.
+    SeedOut* merge_seeds = nullptr;
+    int merge_ratio = 0, fine_ncol = 0;
+    int* ready = nullptr;
+    const int* wait_ready = nullptr;
 };
 constexpr int kMaxLevelJobs = 8;
 
