@@ -341,6 +341,7 @@ struct TcLevel {
     mars::Partial* partials = nullptr;
     unsigned long long* gch = nullptr;
     int* tickets = nullptr;  // all-levels launch only
+    int32_t* dtmp = nullptr;  // the separable domain statistics' scratch (all-levels launch)
     int* coarse_tickets = nullptr;  // all-levels launch: the in-kernel coarse pre-pass
     int* ready = nullptr;
     int tail_tiles = 0, tail_msplit = 0;  // all-levels launch: the finer-split tail
@@ -352,6 +353,10 @@ struct TcLevel {
     int ms1 = 1;
     mars::Partial* part1 = nullptr;
 };
+
+// The separable domain statistics take scratch up to this many words (256 MiB); larger
+// levels use the direct kernel.
+constexpr size_t kDomainTmpWords = 64ull << 20;
 
 // Whether a level takes the split-digit operand (block sizes 16..64 unless pinned off).
 bool tc_digits(const mars_ctx* ctx, const mars::LevelGeom& g) {
@@ -556,7 +561,10 @@ int run_level(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const int32_t*
     MARS_CUDA(sc.get(&ds.sdetf, ndom));
     MARS_CUDA(mars::launch_range_stats(d_plane, (int)w, (int)h, d_rows, d_cols, (int)n,
                                        (int)size, fp, rs, st));
-    MARS_CUDA(mars::launch_domain_stats(d_D, g, ds, st));
+    int32_t* dtmp = nullptr;
+    const size_t dwords = mars::domain_stats_tmp_words(g);
+    if (dwords > 0 && dwords <= kDomainTmpWords) MARS_CUDA(sc.get(&dtmp, dwords));
+    MARS_CUDA(mars::launch_domain_stats(d_D, g, ds, st, dtmp));
     ctx->launches += 2;
     if (k > 1 && use_tc(ctx, size, shift) && mars::tc::topk_supported(g.size, tc_digits(ctx, g)))
         return run_level_tc_topk(ctx, sc, d_plane, d_D, w, h, g, fp, d_rows, d_cols, n, rs, ds,
@@ -790,6 +798,8 @@ int run_jobs_all_levels(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint
         MARS_CUDA(sc.get(&L.ds.s2x16, ndom));
         MARS_CUDA(sc.get(&L.ds.detf, ndom));
         MARS_CUDA(sc.get(&L.ds.sdetf, ndom));
+        const size_t dwords = mars::domain_stats_tmp_words(L.g);
+        if (dwords > 0 && dwords <= kDomainTmpWords) MARS_CUDA(sc.get(&L.dtmp, dwords));
         const bool wanted = L.digits;
         if (int e = tc_level_setup(ctx, sc, w, h, n, std::max(ms[l], tail_ms[l]), true,
                                    n >= kCoarseAllLevels, L))
@@ -826,7 +836,7 @@ int run_jobs_all_levels(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint
             if (cudaError_t ce = mars::launch_range_stats(d_plane, (int)w, (int)h, rows, cols,
                                                           (int)L.n, g.size, fp, L.rs, bs)) {
                 err = fail(MARS_ECUDA, cudaGetErrorString(ce));
-            } else if (cudaError_t ce2 = mars::launch_domain_stats(d_D, g, L.ds, bs)) {
+            } else if (cudaError_t ce2 = mars::launch_domain_stats(d_D, g, L.ds, bs, L.dtmp)) {
                 err = fail(MARS_ECUDA, cudaGetErrorString(ce2));
             } else {
                 ctx->launches += 2;

@@ -59,8 +59,11 @@ struct CandidateOut {
 // ---- launchers (search.cu) ----
 cudaError_t launch_contract(const uint8_t* plane, int w, int h, int32_t* d_out,
                             cudaStream_t st);
+// tmp (domain_stats_tmp_words(g) int32 words, or null): scratch of the separable form, used
+// for block sizes >= 8; without it the direct kernel runs.  Same results either way.
+size_t domain_stats_tmp_words(const LevelGeom& g);
 cudaError_t launch_domain_stats(const int32_t* D, const LevelGeom& g, DomainStats ds,
-                                cudaStream_t st);
+                                cudaStream_t st, int32_t* tmp = nullptr);
 cudaError_t launch_range_stats(const uint8_t* plane, int w, int h, const uint32_t* rows,
                                const uint32_t* cols, int nranges, int size, const FitParams& fp,
                                RangeStats rs, cudaStream_t st);
