@@ -423,23 +423,27 @@ int tc_level_setup(mars_ctx* ctx, Scratch& sc, uint32_t w, uint32_t h, size_t n,
 // copies, the B operand, seed champions, the coarse pre-pass (its statistics and planes
 // only when the all-levels launch runs it: L.ready set), the shared champion records and
 // tickets.
+// st_planes (all-levels launch only): a second stream for the phase planes and the B
+// operand, which do not depend on the statistics the seeds need.
 int tc_level_prep(mars_ctx* ctx, const TcLevel& L, const uint8_t* d_plane, const int32_t* d_D,
                   const uint8_t* d_dplane, uint32_t w, uint32_t h, const mars::FitParams& fp,
-                  const uint32_t* d_rows, const uint32_t* d_cols, cudaStream_t st) {
+                  const uint32_t* d_rows, const uint32_t* d_cols, cudaStream_t st,
+                  cudaStream_t st_planes = nullptr) {
     const mars::LevelGeom& g = L.g;
     const int n = (int)L.n;
+    const cudaStream_t sp = st_planes ? st_planes : st;
     if (L.digits)
-        MARS_CUDA(mars::tc::launch_digit_planes(d_D, (int)w, (int)h, g.shift, L.d_phases, st));
+        MARS_CUDA(mars::tc::launch_digit_planes(d_D, (int)w, (int)h, g.shift, L.d_phases, sp));
     else
-        MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, g.shift, L.d_phases, st));
+        MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, g.shift, L.d_phases, sp));
     MARS_CUDA(mars::tc::launch_build_b(g.size, d_plane, (int)w, (int)h, d_rows, d_cols, n, L.d_b,
-                                       L.digits, st));
+                                       L.digits, sp));
     MARS_CUDA(mars::tc::launch_seed(d_D, g, d_plane, (int)w, d_rows, d_cols, n, L.rs, L.ds, fp,
                                     L.d_seed, st));
     ctx->launches += 3;
     if (L.coarse) {
         MARS_CUDA(mars::launch_domain_stats(d_D, L.g1, L.ds1, st));
-        MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, L.g1.shift, L.d_ph1, st));
+        MARS_CUDA(mars::tc::launch_phase_planes(d_dplane, (int)w, (int)h, L.g1.shift, L.d_ph1, sp));
         ctx->launches += 2;
         if (L.ready) {
             const int rt = mars::tc::ranges_per_tile(false);
@@ -818,14 +822,17 @@ int run_jobs_all_levels(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint
     }
     int* d_work = nullptr;
     MARS_CUDA(sc.get(&d_work, 1));
+    // Every branch is forked: a level's statistics and seeds run on branch b, its planes and
+    // B operand on branch b + kBranches / 2.
     MARS_CUDA(cudaEventRecord(ctx->fork_ev, main));
-    const int nb = (int)std::min<size_t>(jobs.size(), mars_ctx::kBranches);
+    const int nb = mars_ctx::kBranches;
+    constexpr int kHalf = mars_ctx::kBranches / 2;
     for (int b = 0; b < nb; ++b) MARS_CUDA(cudaStreamWaitEvent(ctx->branch[b], ctx->fork_ev, 0));
     int err = MARS_OK;
     size_t off = 0;
     for (size_t i = 0; i < jobs.size() && !err; ++i) {
         const Job& j = jobs[i];
-        const int b = (int)(i % mars_ctx::kBranches);
+        const int b = (int)(i % kHalf);
         const cudaStream_t bs = ctx->branch[b];
         const uint32_t* rows = d_rc + off;
         const uint32_t* cols = d_rc + total + off;
@@ -840,7 +847,8 @@ int run_jobs_all_levels(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint
                 err = fail(MARS_ECUDA, cudaGetErrorString(ce2));
             } else {
                 ctx->launches += 2;
-                err = tc_level_prep(ctx, L, d_plane, d_D, d_plane, w, h, fp, rows, cols, bs);
+                err = tc_level_prep(ctx, L, d_plane, d_D, d_plane, w, h, fp, rows, cols, bs,
+                                    ctx->branch[b + kHalf]);
             }
         } else {
             ctx->stream = bs;

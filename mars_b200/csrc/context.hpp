@@ -31,7 +31,7 @@ struct mars_ctx {
     PFN_cuTensorMapEncodeTiled_v12000 encode_tiled = nullptr;
     // Streams and events a search plan's capture forks its levels onto (created on first use;
     // the levels of a plane run as parallel branches of the plan's graph).
-    static constexpr int kBranches = 4;
+    static constexpr int kBranches = 8;
     cudaStream_t branch[kBranches] = {};
     cudaEvent_t fork_ev = nullptr;
     cudaEvent_t join_ev[kBranches] = {};
