@@ -526,9 +526,13 @@ int run_level_tc_topk(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, const 
                                        d_b, digits, st));
     MARS_CUDA(mars::tc::launch_seed_topk(d_D, g, d_plane, (int)w, d_rows, d_cols, (int)n, rs, ds,
                                          fp, (int)k, d_seed, st));
+    // The splits share each range's best k-th entry (rms bits, index, t1_x4) as a bound.
+    unsigned long long* gch = nullptr;
+    MARS_CUDA(sc.get(&gch, 2 * n));
+    MARS_CUDA(cudaMemsetAsync(gch, 0xFF, 2 * n * sizeof(unsigned long long), st));
     MARS_CUDA(mars::tc::launch_corr_topk(maps, d_b, g, (int)n, rs, ds, fp, d_seed, (int)k,
-                                         partials, msplit, digits, ctx->d_err, ctx->d_counter,
-                                         st));
+                                         partials, gch, msplit, digits, ctx->d_err,
+                                         ctx->d_counter, st));
     MARS_CUDA(mars::launch_reduce_topk(partials, msplit, (int)n, (int)k, g, rs, ds, d_out, st));
     ctx->launches += 5;
     return MARS_OK;

@@ -368,10 +368,10 @@ struct TopkLists {
 __device__ __forceinline__ bool topk_insert(TopkLists& L, int rl, int k, double rms, double sum,
                                             uint32_t idx, int32_t t1, uint32_t q) {
     const int c = L.cnt[rl];
-    for (int j = 0; j < c; ++j)
-        if (L.idx[rl][j] == idx) return false;
     if (c == k && !(rms < L.rms[rl][k - 1] || (rms == L.rms[rl][k - 1] && idx < L.idx[rl][k - 1])))
         return false;
+    for (int j = 0; j < c; ++j)
+        if (L.idx[rl][j] == idx) return false;
     int pos = c < k ? c : k - 1;
     while (pos > 0 && (rms < L.rms[rl][pos - 1] ||
                        (rms == L.rms[rl][pos - 1] && idx < L.idx[rl][pos - 1]))) {
@@ -393,21 +393,61 @@ __device__ __forceinline__ bool topk_insert(TopkLists& L, int rl, int k, double 
 
 // The pruning record of a ranked range: against its k-th entry once the list is full (the
 // same bound as the single winner's, fit.cuh); before that every candidate passes (sqrt_w
-// = w2a = -inf: tau = -inf for every domain).
+// = w2a = -inf: tau = -inf for every domain).  With a shared record (rec, the range's
+// 128-bit record of the best k-th entry any split holds) the bound is the better of the two:
+// a candidate that k others of one split beat is not among the k best at all.  The list
+// keeps this split's own candidates either way.
 __device__ __forceinline__ void topk_publish(Smem& sm, const TopkLists& L, int rl, int k,
-                                             const FitParams& fp, int n) {
+                                             const FitParams& fp, int n,
+                                             unsigned long long* rec = nullptr,
+                                             const DomainStats* ds = nullptr) {
     Champ& C = sm.ch[rl];
     if (!C.valid) {
         publish_threshold(sm, rl, fp, n);
         return;
     }
-    if (L.cnt[rl] < k) {
+    bool have = L.cnt[rl] == k;
+    if (have) {
+        C.rms = L.rms[rl][k - 1];
+        C.sum = L.sum[rl][k - 1];
+        C.idx = L.idx[rl][k - 1];
+        C.t1x4 = L.t1[rl][k - 1];
+    }
+    if (rec) {
+        unsigned long long clo, chi;
+        cas128(rec, 0ull, 0ull, 0ull, 0ull, clo, chi);
+        for (int tries = 0; tries < 64; ++tries) {
+            const uint32_t gidx = (uint32_t)chi;
+            const unsigned long long mlo =
+                have ? (unsigned long long)__double_as_longlong(C.rms) : ~0ull;
+            if (have && (mlo < clo || (mlo == clo && C.idx < gidx))) {
+                // Publish this split's k-th entry.
+                const unsigned long long vhi = (unsigned long long)C.idx |
+                                               (unsigned long long)(uint32_t)C.t1x4 << 32;
+                unsigned long long olo, ohi;
+                cas128(rec, clo, chi, mlo, vhi, olo, ohi);
+                if (olo == clo && ohi == chi) break;
+                clo = olo;
+                chi = ohi;
+            } else {
+                if (clo != ~0ull && (!have || clo < mlo || (clo == mlo && gidx < C.idx))) {
+                    // Another split's k-th entry is the tighter bound.
+                    const uint32_t dom = gidx >> 3;
+                    C.rms = __longlong_as_double((long long)clo);
+                    C.idx = gidx;
+                    C.t1x4 = (int32_t)(uint32_t)(chi >> 32);
+                    C.sum = fit_exact(n, ds->s1x4[dom], ds->s2x16[dom], C.t0, (int64_t)C.t1x4,
+                                      C.t2, fp).sum;
+                    have = true;
+                }
+                break;
+            }
+        }
+    }
+    if (!have) {
         sm.thr[rl] = ThrRec{-INFINITY, -INFINITY, 0.0f, INT32_MAX};
         return;
     }
-    C.rms = L.rms[rl][k - 1];
-    C.sum = L.sum[rl][k - 1];
-    C.idx = L.idx[rl][k - 1];
     publish_threshold(sm, rl, fp, n);
 }
 
@@ -417,7 +457,8 @@ template <int N, int NT, int RG>
 __device__ __noinline__ void drain_queue_topk(Smem& sm, TopkLists& L, int k, int grp, int n,
                                               bool mark, uint32_t tag, int gt,
                                               const DomainStats& ds, const FitParams& fp,
-                                              unsigned long long& exact) {
+                                              unsigned long long& exact, unsigned long long* gch,
+                                              int rbase) {
     QEntry* const queue = sm.queue[grp];
     for (int qi = gt; qi < n; qi += kGroupThreads) {
         QEntry& q = queue[qi];
@@ -446,7 +487,11 @@ __device__ __noinline__ void drain_queue_topk(Smem& sm, TopkLists& L, int k, int
             changed |= topk_insert(L, rl, k, q.rms, q.sum, q.dom * 8u + (uint32_t)(col & 7),
                                    q.t1 + 128 * ds.s1x4[q.dom], q.pad);
         }
-        if (changed) topk_publish(sm, L, rl, k, fp, N);
+        // With shared records the bound is refreshed after every drain: another split may
+        // have tightened it.
+        if (changed || gch)
+            topk_publish(sm, L, rl, k, fp, N, gch ? gch + 2 * (size_t)(rbase + rl) : nullptr,
+                         &ds);
     }
     if (gt == 0) sm.qcount[grp] = 0;
     group_barrier(grp);
@@ -707,7 +752,8 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
         sm.key_idx[threadIdx.x] = UINT32_MAX;
         if (TOPK) {
             if (!C.valid) tk->cnt[threadIdx.x] = 0;
-            topk_publish(sm, *tk, threadIdx.x, a.k, fp, N);
+            topk_publish(sm, *tk, threadIdx.x, a.k, fp, N,
+                         (a.gch && C.valid) ? a.gch + 2 * (size_t)r : nullptr, &a.ds);
         } else {
             publish_threshold(sm, threadIdx.x, fp, N);
         }
@@ -992,7 +1038,8 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
                 if (queued > kQueueCap) {
                     if (TOPK)
                         drain_queue_topk<N, NT, kRangesPerWarp>(sm, *tk, a.k, part, kQueueCap,
-                                                                true, tag, gt, ds, fp, exact);
+                                                                true, tag, gt, ds, fp, exact,
+                                                                a.gch, ntile * RT);
                     else
                         drain_queue<N, NT, kRangesPerWarp>(sm, part, kQueueCap, true, tag, gt,
                                                            ds, fp, exact, a.gch, ntile * RT);
@@ -1002,7 +1049,8 @@ __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs&
                 if (queued >= kFlush || (last && queued > 0)) {
                     if (TOPK)
                         drain_queue_topk<N, NT, kRangesPerWarp>(sm, *tk, a.k, part, queued,
-                                                                false, tag, gt, ds, fp, exact);
+                                                                false, tag, gt, ds, fp, exact,
+                                                                a.gch, ntile * RT);
                     else
                         drain_queue<N, NT, kRangesPerWarp>(sm, part, queued, false, tag, gt,
                                                            ds, fp, exact, a.gch, ntile * RT);
@@ -1919,12 +1967,12 @@ bool topk_supported(int size, bool digits) { return all_levels_supported(size, d
 
 cudaError_t launch_corr_topk(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g,
                              int nranges, RangeStats rs, DomainStats ds, const FitParams& fp,
-                             const SeedOut* seeds, int k, Partial* partials, int msplit,
-                             bool digits, int* err, unsigned long long* counter,
-                             cudaStream_t st) {
+                             const SeedOut* seeds, int k, Partial* partials,
+                             unsigned long long* gch, int msplit, bool digits, int* err,
+                             unsigned long long* counter, cudaStream_t st) {
     if (k < 2 || k > kMaxTopK) return cudaErrorInvalidValue;
-#define MARS_CORR_TOPK(S_, D_)                                                                  \
-    launch_t<S_, D_, true>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, nullptr, msplit, \
+#define MARS_CORR_TOPK(S_, D_)                                                               \
+    launch_t<S_, D_, true>(maps, bglob, g, nranges, rs, ds, fp, seeds, partials, gch, msplit, \
                            err, counter, st, k)
     if (digits) {
         switch (g.size) {

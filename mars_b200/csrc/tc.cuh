@@ -115,9 +115,9 @@ cudaError_t launch_seed_topk(const int32_t* D, const LevelGeom& g, const uint8_t
                              SeedOut* out, cudaStream_t st);
 cudaError_t launch_corr_topk(const TcMaps& maps, const uint8_t* bglob, const LevelGeom& g,
                              int nranges, RangeStats rs, DomainStats ds, const FitParams& fp,
-                             const SeedOut* seeds, int k, Partial* partials, int msplit,
-                             bool digits, int* err, unsigned long long* counter,
-                             cudaStream_t st);
+                             const SeedOut* seeds, int k, Partial* partials,
+                             unsigned long long* gch, int msplit, bool digits, int* err,
+                             unsigned long long* counter, cudaStream_t st);
 cudaError_t launch_seed_merge(const Partial* partials, int nsplit, int nranges, int coarse_ncol,
                               int fine_ncol, int ratio, SeedOut* seeds, cudaStream_t st);
 cudaError_t launch_finish(const Partial* partials, int nsplit, int nranges, const LevelGeom& g,
