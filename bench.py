@@ -52,14 +52,14 @@ WORKLOAD = ("exhaustive search of every RD quadtree node of a 512x512 synthetic 
 # committed captures named beside them; re-captured whenever the kernel changes.
 # DRAM bytes (read + write) per launch of the dominant search kernel, s=4 level.
 NCU_SOURCE = "profiles/corr_tc_s4_512x512_ncu.md"
-NCU_TRAFFIC = {4: 20_560_000}
+NCU_TRAFFIC = {4: 21_360_000}
 # DRAM bytes (read + write) of one all-levels correlation launch (corr_tc_all_kernel, every
 # level of one 512x512 plane): profiles/corr_tc_all_512x512_ncu.md.
 NCU_ALL_SOURCE = "profiles/corr_tc_all_512x512_ncu.md"
 NCU_ALL_TRAFFIC = 42_626_816 + 299_264
 # Thread instructions per candidate fit of the correlation kernel's level (warp
 # instructions x 32 / fits, same capture): the issue cost behind the epilogue roofline.
-NCU_INSTR_PER_FIT = {4: 0.9722e9 * 32 / 8.52e9, 8: 0.3886e9 * 32 / 2.0e9}
+NCU_INSTR_PER_FIT = {4: 0.8684e9 * 32 / 8.52e9, 8: 0.3886e9 * 32 / 2.0e9}
 # DRAM bytes of one decode iteration, by plane side (profiles/decode_cell_4096x4096_ncu.md;
 # profiles/decode_sorted_16384x16384_ncu.md: dram__bytes.sum.per_second x
 # gpu__time_duration.sum of the gather and the place launch of one iteration).
