@@ -67,3 +67,13 @@ def test_ifs_write_rejects_duplicate_leaves():
     dup = np.concatenate([leaves, leaves[:1]])
     with pytest.raises(mb.MarsError):
         mb.ifs_write(h, dup)
+
+
+def test_null_arguments_are_refused_without_a_device():
+    # Entry points that take a plan or a context check their arguments before touching a
+    # device: no CUDA call, no crash, MARS_EINVAL.
+    import ctypes as C
+    L = mb.lib()
+    ms = C.c_float()
+    assert L.mars_search_plan_kernel_ms(None, C.byref(ms)) == -1
+    assert L.mars_ctx_set_search_path(None, 5) == -1
