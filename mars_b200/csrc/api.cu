@@ -176,6 +176,12 @@ int sync_bounded(mars_ctx* ctx, cudaStream_t stream = nullptr) {
         const char* e = std::getenv("MARS_SYNC_TIMEOUT_S");
         return e ? std::atof(e) : 300.0;
     }();
+    // On the context's stream (its callers hold ctx->mu) the kernel error word travels back
+    // with the work, ahead of the event; other streams read it after the wait.
+    const bool err_async = !stream && ctx->h_err;
+    if (err_async)
+        MARS_CUDA(cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
     cudaEvent_t ev;
     MARS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     MARS_CUDA(cudaEventRecord(ev, stream ? stream : ctx->stream));
@@ -193,11 +199,19 @@ int sync_bounded(mars_ctx* ctx, cudaStream_t stream = nullptr) {
             cudaEventDestroy(ev);
             return fail(MARS_ETIMEOUT, "device work did not finish within MARS_SYNC_TIMEOUT_S");
         }
-        std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 20 : 500));
+        // The first milliseconds poll without sleeping (a short sleep overshoots by tens of
+        // microseconds, a search step's whole host overhead), then every 20 us, then 500 us.
+        if (el < 0.005)
+            std::this_thread::yield();
+        else
+            std::this_thread::sleep_for(std::chrono::microseconds(el < 0.05 ? 20 : 500));
     }
     cudaEventDestroy(ev);
     int kerr = 0;
-    MARS_CUDA(cudaMemcpy(&kerr, ctx->d_err, sizeof kerr, cudaMemcpyDeviceToHost));
+    if (err_async)
+        kerr = *reinterpret_cast<volatile int*>(ctx->h_err);
+    else
+        MARS_CUDA(cudaMemcpy(&kerr, ctx->d_err, sizeof kerr, cudaMemcpyDeviceToHost));
     if (kerr) {
         cudaMemset(ctx->d_err, 0, sizeof(int));
         return fail(MARS_ETIMEOUT, "a bounded wait inside the search kernel expired (code " +
@@ -1217,6 +1231,7 @@ int mars_ctx_create(mars_ctx** out, int device) {
     if (e == cudaSuccess) e = cudaMalloc(&c->d_counter, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&c->h_err, sizeof(int));
     if (e == cudaSuccess) {
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q;
@@ -1234,6 +1249,7 @@ int mars_ctx_create(mars_ctx** out, int device) {
     }
     if (e != cudaSuccess) {
         if (c->own_stream) cudaStreamDestroy(c->own_stream);
+        if (c->h_err) cudaFreeHost(c->h_err);
         delete c;
         return fail(MARS_ECUDA, std::string("context setup: ") + cudaGetErrorString(e));
     }
@@ -1250,6 +1266,7 @@ void mars_ctx_destroy(mars_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->h_err) cudaFreeHost(ctx->h_err);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     for (int b = 0; b < mars_ctx::kBranches; ++b) {
         if (ctx->branch[b]) cudaStreamDestroy(ctx->branch[b]);

@@ -24,6 +24,7 @@ struct mars_ctx {
     std::mutex mu;
     unsigned long long* d_counter = nullptr;  // survivors that took the exact f64 fit
     int* d_err = nullptr;                     // kernel-side error bits (bounded waits)
+    int* h_err = nullptr;                     // pinned copy of d_err, read by sync_bounded
     int search_path = 0;                      // 0 auto, 1 CUDA cores only, 2 tensor cores
     bool tma_16_boxes = false;                // load A stages as 16 2-D boxes (A/B checks)
     bool fold_only = false;                   // no split-digit operand at sizes 16..64 (A/B)
