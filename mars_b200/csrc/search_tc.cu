@@ -642,8 +642,11 @@ __device__ __forceinline__ void cta_teardown(Smem& sm, uint32_t tmem, unsigned l
 // One work item: range tile `ntile` of a level against domain tiles [split * m_per_cta,
 // ...) -- the champions seeded, the loads / MMAs / exact-bound epilogue over those domain
 // tiles, the tile's partial champions written.  With tickets set, the last split of the
-// range tile to finish also writes the tile's final candidates.  Every thread of the CTA
-// calls this together; it begins and ends with a CTA barrier.
+// range tile to finish also writes the tile's final candidates, or, for a coarse pre-pass
+// job, merges them into the fine level's seeds and sets the tile's ready flag; with
+// wait_ready set the item first waits for that flag.  TOPK: the ranked search, a k-list
+// per range in *tk.  Every thread of the CTA calls this together; it begins and ends with a
+// CTA barrier.
 template <int S, bool DIG, bool TOPK = false>
 __device__ __forceinline__ void process_item(const TcMaps& maps, const ItemArgs& a, int ntile,
                                              int split, Smem& sm, unsigned char* stages,
