@@ -35,6 +35,11 @@
 // and thresholds.
 // Every mbarrier wait is bounded (clock64 deadline): on expiry the kernel records an
 // error, stops issuing work, waits (bounded) for its own loads, frees TMEM and returns.
+//
+// One body (process_item) serves three kernels: corr_tc_kernel<S, DIG, false>, one level
+// per launch (CTA = range tile x domain-tile split); corr_tc_kernel<S, DIG, true>, the
+// ranked search keeping each range's best k; and corr_tc_all_kernel, every tensor-core
+// level of a plane in one persistent launch over (level, range tile, split) work items.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
