@@ -1112,6 +1112,10 @@ int run_jobs_fisher(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t
     return MARS_OK;
 }
 
+int run_jobs_branched(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uint32_t h,
+                      const mars::FitParams& fp, const std::vector<Job>& jobs,
+                      mars::CandidateOut* d_out, const uint32_t* d_rc, uint32_t k);
+
 int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, uint32_t w,
                 uint32_t h, const mars_params* params, bool adaptive, mars_table** out,
                 int method = MARS_METHOD_EXHAUSTIVE, uint32_t k = 1) {
@@ -1173,6 +1177,16 @@ int build_table(mars_ctx* ctx, const uint8_t* plane, const uint8_t* d_plane_in, 
                                       cudaMemcpyDeviceToHost, ctx->stream));
         } else if (k == 1 && all_levels_eligible(ctx, w, h, jobs)) {
             if (int e = run_jobs_all_levels(ctx, sc, d_plane, w, h, fp, jobs, d_out, nullptr))
+                return e;
+        } else if (k > 1) {
+            // The ranked search: the levels as parallel branches (run_jobs_branched).
+            size_t tot = 0;
+            const std::vector<uint32_t> rc = job_origins(jobs, &tot);
+            uint32_t* d_rc = nullptr;
+            MARS_CUDA(sc.get(&d_rc, rc.size()));
+            MARS_CUDA(cudaMemcpyAsync(d_rc, rc.data(), rc.size() * 4, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+            if (int e = run_jobs_branched(ctx, sc, d_plane, w, h, fp, jobs, d_out, d_rc, k))
                 return e;
         } else {
             if (int e = run_jobs(ctx, sc, d_plane, w, h, fp, jobs, d_out, k)) return e;
@@ -1823,7 +1837,7 @@ void plan_release(mars_search_plan* p) {
 // overlap another level's correlation.  The caller holds ctx->mu.
 int run_jobs_branched(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32_t w, uint32_t h,
                       const mars::FitParams& fp, const std::vector<Job>& jobs,
-                      mars::CandidateOut* d_out, const uint32_t* d_rc) {
+                      mars::CandidateOut* d_out, const uint32_t* d_rc, uint32_t k) {
     const cudaStream_t main = ctx->stream;
     if (!ctx->fork_ev) {
         MARS_CUDA(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
@@ -1850,7 +1864,7 @@ int run_jobs_branched(mars_ctx* ctx, Scratch& sc, const uint8_t* d_plane, uint32
         {
             Scratch sb(ctx->branch[b]);
             err = run_level(ctx, sb, d_plane, d_D, w, h, j.size, j.shift, fp, d_rc + off,
-                            d_rc + total + off, j.rows.size(), d_out + off, 1);
+                            d_rc + total + off, j.rows.size(), d_out + off * k, k);
         }
         ctx->stream = main;
         off += j.rows.size();
@@ -1886,7 +1900,7 @@ int plan_enqueue(mars_search_plan* p, bool with_copies) {
             return e;
         p->corr_timed = true;
     } else if (int e = run_jobs_branched(ctx, sc, p->d_plane, p->w, p->h, fp, p->jobs, p->d_out,
-                                         p->d_rc)) {
+                                         p->d_rc, 1)) {
         return e;
     }
     if (with_copies) {
